@@ -1,0 +1,351 @@
+"""SSB recon/s at 128^4 u16 on B200 (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload: plain SSB at production size - scan 128x128, detector 128x128,
+uint16 (537 MB), ~1784 bright-field pixels, synthetic weak-phase data
+(seeded; the reference's own benchmarks use private acquisitions). One step
+is one cold reconstruction: u16 counts resident in HBM -> u64 mean DP -> BF
+selection -> BF gather -> Hermitian scan FFT -> corrected Fourier sum ->
+inverse FFT -> float32 object phase, through ``B200SSBBackend`` and the C ABI.
+Inputs (537 MB per step) are larger than the 126 MB L2.
+
+``--impl reference`` times the reference's CPU path for the same workload:
+the reference has no CPU SSB implementation, so this is the CPU torch
+restatement of its executable specification (docs/kernels/ssb.md) from
+``oracle/ssb_torch_spec.py``, run with every host thread, rank 0 only.
+
+Multi-GPU: replicas (each rank reconstructs its own scan; no collective on the
+data path), ``scaling: weak``, time = max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "SSB recon/s at 128^4 u16"
+UNIT = "recon/s"
+SPEC_NAME = "plain_128x128_det128"
+KW = dict(semiangle=20.0, scan_sampling=0.5, det_sampling=20.0 / 24.0, voltage_kV=300)
+WORKLOAD = ("plain SSB, scan 128x128 x detector 128x128 uint16 (537 MB), ~1784 BF pixels, "
+            "cold u16->object phase per step")
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def _barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def _max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except ValueError:
+                continue
+            for name, v in zip(names, r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def _peaks() -> tuple[float, str]:
+    p = REPO / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def _traffic(kernel: str) -> float | None:
+    p = REPO / "profiles" / "traffic.json"
+    if p.exists():
+        v = json.loads(p.read_text()).get(kernel)
+        return None if v is None else float(v)
+    return None
+
+
+def cpu_baseline(counts_host: np.ndarray, budget_s: float = 15.0) -> dict:
+    """Reference-spec CPU recon on the host cores, bounded to ~budget_s."""
+    from oracle import ssb_torch_spec as spec
+
+    kw = dict(voltage_kV=300, semiangle_mrad=KW["semiangle"], scan_sampling=KW["scan_sampling"],
+              det_sampling=KW["det_sampling"])
+    spec.reconstruct(counts_host, bf_stride=8, **kw)  # warm-up (allocator, threads)
+    t0 = time.perf_counter()
+    n = 0
+    while True:
+        spec.reconstruct(counts_host, **kw)
+        n += 1
+        if time.perf_counter() - t0 > budget_s or n >= 20:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": UNIT, "cores": spec.host_threads(), "kind": "port",
+            "sample": f"{n} full 128^4 reconstructions (all BF pixels) of the same workload"}
+
+
+def run_reference(args, world, rank) -> None:
+    if rank != 0:
+        return
+    from oracle import ssb_torch_spec as spec
+    from quantem.gpu_b200.synthetic import CONFIGS, generate
+
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    counts = generate(CONFIGS[SPEC_NAME], device=dev).counts.cpu().numpy()
+    kw = dict(voltage_kV=300, semiangle_mrad=KW["semiangle"], scan_sampling=KW["scan_sampling"],
+              det_sampling=KW["det_sampling"])
+    for _ in range(args.warmup):
+        spec.reconstruct(counts, **kw)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        spec.reconstruct(counts, **kw)
+    dt = time.perf_counter() - t0
+    value = args.steps / dt
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "impl": "reference",
+        "config": {"workload": WORKLOAD, "path": "CPU torch restatement of docs/kernels/ssb.md"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": spec.host_threads(), "kind": "port",
+                         "sample": "one full 128^4 reconstruction per step"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_b200(args, world, rank, local) -> None:
+    from quantem.gpu_b200 import SSB, B200SSBBackend, ops
+    from quantem.gpu_b200.synthetic import CONFIGS, generate
+    from dataclasses import replace
+
+    dev = torch.device("cuda", local)
+    spec = replace(CONFIGS[SPEC_NAME], seed=CONFIGS[SPEC_NAME].seed + rank)
+    counts = generate(spec, device=dev).counts.contiguous()
+    ab = dict(C10=0.0, C12=0.0, phi12=0.0)
+    stream = torch.cuda.current_stream(dev)
+
+    def cold_step():
+        be = B200SSBBackend(counts, device=dev, **KW)
+        obj, ph = be.object_and_phase(ab["C10"], ab["C12"], ab["phi12"])
+        return be, ph
+
+    for _ in range(max(3, args.warmup)):
+        be, ph = cold_step()
+    torch.cuda.synchronize(dev)
+    n_bf = be.num_bf
+    clocks = Clocks(dev.index)
+    _barrier(world)
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    launches0 = ops.LAUNCH_COUNT
+    with ops.profile_ops() as prof:
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(args.steps):
+            be, ph = cold_step()
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+    clock_info = clocks.stop()
+    launches = ops.LAUNCH_COUNT - launches0
+    _barrier(world)
+    elapsed_ms = _max_over_ranks(start.elapsed_time(end), world)
+    value = world * args.steps / (elapsed_ms / 1e3)
+    per_op: dict[str, list[float]] = {}
+    for name, s, e in prof:
+        per_op.setdefault(name, []).append(s.elapsed_time(e))
+
+    # warm redraw (object from resident G) and loss evaluations: secondary figures
+    torch.cuda.synchronize(dev)
+    for _ in range(5):
+        be.object_and_phase(10.0, 5.0, 0.1)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    n_warm = 50
+    for i in range(n_warm):
+        be.object_and_phase(10.0 + i, 5.0, 0.1)
+    e.record(stream)
+    torch.cuda.synchronize(dev)
+    warm_ms = s.elapsed_time(e) / n_warm
+    cands = torch.zeros((64, 4), dtype=torch.float32, device=dev)
+    cands[:, 0] = torch.linspace(-50, 50, 64, device=dev)
+    be.variance_loss_batch(cands[:, 0].cpu().numpy(), 0.0, 0.0)
+    torch.cuda.synchronize(dev)
+    s.record(stream)
+    for _ in range(3):
+        be.variance_loss_batch(cands[:, 0].cpu().numpy(), 0.0, 0.0)
+    e.record(stream)
+    torch.cuda.synchronize(dev)
+    loss_batch_ms = s.elapsed_time(e) / 3
+
+    # end to end through the public API: pinned host counts -> SSB -> host phase
+    host = counts.cpu().pin_memory()
+    h2d = host.numel() * host.element_size()
+    d2h = 0
+    def e2e_step():
+        with SSB.from_array(host, voltage_kV=300, semiangle_mrad=KW["semiangle"],
+                            scan_sampling_A=KW["scan_sampling"],
+                            det_sampling=KW["det_sampling"]) as ssb:
+            res = ssb.reconstruct(compute_loss=False)
+            return res.phase.cpu()
+    for _ in range(2):
+        out = e2e_step()
+    d2h = out.numel() * out.element_size() + 128 * 128 * (4 + 8)  # phase + mean DP + u64 sums
+    torch.cuda.synchronize(dev)
+    _barrier(world)
+    t0 = time.perf_counter()
+    n_e2e = max(3, min(args.steps, 10))
+    for _ in range(n_e2e):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    e2e_s = _max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = world * n_e2e / e2e_s
+
+    if rank != 0:
+        return
+    peak, peak_kind = _peaks()
+    mean_dp_ms = float(np.mean(per_op.get("qssb_mean_dp_u64", [float("nan")])))
+    alg_bytes = 2 * 128 * 128 * 128 * 128  # u16 counts read once
+    achieved = alg_bytes / (mean_dp_ms / 1e3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(3, args.warmup), "ms_per_step": elapsed_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_bf": n_bf, "scan": [128, 128], "detector": [128, 128],
+                   "l2": "inputs larger than L2 (537 MB u16 per step)",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": "qssb_mean_dp_u64 (k_sum_frames_vec8 + k_mean_from_sums)",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": f"{peak_kind} hbm_gbs",
+                     "traffic": _traffic("k_sum_frames_vec8"),
+                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": mean_dp_ms},
+        "stage_ms": {k: float(np.mean(v)) for k, v in per_op.items()},
+        "warm_recon_per_s": 1e3 / warm_ms,
+        "loss_evals_per_s_batch64": 64 * 1e3 / loss_batch_ms,
+        "gpu_launches": launches,
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "api": "SSB.from_array(pinned host u16).reconstruct()"},
+        "clocks": clock_info,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(counts.cpu().numpy())
+    if world == 1 and not args.no_oracle:
+        from oracle import ssb_oracle as so
+
+        hostc = counts.cpu().numpy()
+        prep = so.prepare(hostc, voltage_kV=300, semiangle_mrad=KW["semiangle"],
+                          scan_sampling=KW["scan_sampling"], det_sampling=KW["det_sampling"])
+        _, ref_ph = so.reconstruct(prep, so.Aberrations(0.0, 0.0, 0.0))
+        err = so.wrapped_phase_error(ph.cpu().numpy(), ref_ph)
+        line["phase_rms_rad_vs_fp64"] = float(np.sqrt(np.mean(err ** 2)))
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-oracle", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = _dist()
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_b200(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

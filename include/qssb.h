@@ -1,0 +1,139 @@
+/*
+ * qssb.h - C ABI of the B200-native single-sideband (SSB) ptychography engine.
+ *
+ * Every entry point is a plain C function: raw device pointers, sizes and a
+ * cudaStream_t passed as void*. No PyTorch or CuPy types cross this boundary.
+ * Each returns QSSB_OK (0) or a negative QSSB_ERR_* code and never aborts;
+ * qssb_last_error() gives a message for the calling thread's last failure.
+ * All kernels are enqueued on the given stream; nothing synchronises it.
+ *
+ * The entry points replace the device work of the reference backend
+ * (bobleesj/quantem.gpu 0.0.1rc6, src/quantem/gpu/ssb/compute/cuda/), as
+ * cited on each declaration. Complex arrays are interleaved float32 pairs
+ * (complex64); the Hermitian spectrum layout is the reference's
+ * G_qk[n_bf][scan_rows][scan_cols/2 + 1].
+ */
+#ifndef QSSB_H
+#define QSSB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QSSB_VERSION 1
+
+#define QSSB_OK 0
+#define QSSB_ERR_INVALID (-1)     /* bad argument, shape, alignment or size */
+#define QSSB_ERR_CUDA (-2)        /* a CUDA launch or runtime call failed */
+#define QSSB_ERR_UNSUPPORTED (-3) /* valid request this build cannot serve */
+#define QSSB_ERR_WORKSPACE (-4)   /* workspace smaller than the query said */
+
+/* Flags for qssb_object / qssb_loss_batch. */
+#define QSSB_FLAG_CHI_FP64 1      /* chi polynomial and its 2*pi reduction in FP64 */
+#define QSSB_FLAG_FULL_PLANE 2    /* evaluate every scan frequency; no +-q symmetry */
+
+/* Calibration shared by the object and loss entry points. Scalars follow
+ * SSBEngine's cache (engine.py:784-848): wavelength in Angstrom, angles in
+ * radians, the per-axis detector angular sampling in radians per pixel, the
+ * scan step in Angstrom. The float32 kernels use these rounded to float32,
+ * as the reference passes them (np.float32 kernel arguments); the FP64
+ * aperture evaluation at near-tied overlaps uses them as given. */
+typedef struct qssb_calibration {
+    int32_t n_bf;                 /* selected BF pixels (B), >= 1 */
+    int32_t scan_rows;            /* R0: 64, 128 or 256 */
+    int32_t scan_cols;            /* R1: == scan_rows */
+    int32_t reserved;             /* must be 0 */
+    double wavelength_A;
+    double semiangle_rad;
+    double det_sampling_row_rad;  /* reference "ang_y" */
+    double det_sampling_col_rad;  /* reference "ang_x" */
+    double scan_sampling_row_A;   /* q_row = fftfreq(R0, scan_sampling_row_A) */
+    double scan_sampling_col_A;
+    double dc_re;                 /* dc = mean_b G_b(0,0) (backend.py:587) */
+    double dc_im;
+} qssb_calibration_t;
+
+/* Layout of bf_geom (device float32 [8][n_bf]): rows 0-5 are cache_rotation's
+ * kx, ky, alpha_k2, cos2phi_k, sin2phi_k, aperture_k (engine.py:784-830, in
+ * float32 like the reference); rows 6-7 are kx_lo, ky_lo with
+ * kx_fp64 = (double)kx + (double)kx_lo. */
+#define QSSB_GEOM_ROWS 8
+
+/* One aberration candidate in the reference's numeric convention: C10, C12
+ * and C30 enter chi as Angstrom values, phi12 in radians
+ * (engine.py:217-231, common.py:410-471 slot 4 for C30). */
+typedef struct qssb_aberrations {
+    float C10;
+    float C12;
+    float phi12;
+    float C30;
+} qssb_aberrations_t;
+
+int qssb_version(void);
+const char* qssb_last_error(void);
+
+/* Mean diffraction pattern: sums[k] = sum over frames of counts[f][k] in
+ * exact u64 arithmetic, mean_dp[k] = float32(sums[k]) / n_frames (IEEE
+ * round-to-nearest). Replaces CudaSSBBackend._compute_bf_mask's reduction
+ * (backend.py:432-441) and probe.mean_dp (detector/compute/cuda/probe.py:
+ * 122-147). counts: [n_frames][det_pixels] u16; sums: [det_pixels]
+ * (overwritten); mean_dp: [det_pixels] or NULL. */
+int qssb_mean_dp_u64(const uint16_t* counts, int64_t n_frames, int32_t det_pixels,
+                     uint64_t* sums, float* mean_dp, void* stream);
+
+/* BF-column gather: columns[b][f] = counts[f][bf_linear[b]] (exact u16).
+ * Replaces the fancy-index + transpose of _extract_gqk (backend.py:561-572).
+ * bf_linear: device int32 [n_bf], each in [0, det_pixels). */
+int qssb_gather_bf_columns(const uint16_t* counts, int64_t n_frames, int32_t det_pixels,
+                           const int32_t* bf_linear, int32_t n_bf, uint16_t* columns,
+                           void* stream);
+
+/* Forward scan FFT of each BF image, Hermitian half plane:
+ * g_half[b][r][c] = sum_R columns[b][R] exp(-2 pi i (r R_r/R0 + c R_c/R1)),
+ * c in [0, R1/2]. Replaces cp.fft.fft2 + the half-plane slice of
+ * _extract_gqk (backend.py:573-585). columns: u16 [n_bf][R0*R1];
+ * g_half: complex64 [n_bf][R0][R1/2+1]. */
+int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t scan_rows,
+                       int32_t scan_cols, float* g_half, void* stream);
+
+/* Workspace bytes needed by qssb_object for this calibration. */
+int qssb_object_workspace_bytes(const qssb_calibration_t* cal, int32_t flags, size_t* bytes);
+
+/* Object wave O = ifft2((1/B) sum_b G_b conj(Gamma_hat_b)), DC := dc, and
+ * phase = atan2(Im O, Re O). Replaces SSBEngine.reconstruct_object
+ * (engine.py:1109-1151; identical by IFFT linearity to its per-BF fused
+ * path K5+K6+K7+mean, and to _reconstruct_object_fourier_sum,
+ * engine.py:1047-1107). bf_geom: device float32 [QSSB_GEOM_ROWS][n_bf]
+ * (layout above); q_row/q_col: device float32 fftfreq grids; object: complex64 [R0][R1];
+ * phase: float32 [R0][R1] or NULL. */
+int qssb_object(const float* g_half, const float* bf_geom, const float* q_row,
+                const float* q_col, const qssb_calibration_t* cal,
+                const qssb_aberrations_t* ab, int32_t flags, void* workspace,
+                size_t workspace_bytes, float* object, float* phase, void* stream);
+
+/* Workspace bytes needed by qssb_loss_batch for n_cand candidates. */
+int qssb_loss_workspace_bytes(const qssb_calibration_t* cal, int32_t n_cand, int32_t flags,
+                              size_t* bytes);
+
+/* Phase-variance loss for n_cand candidates in one launch sequence:
+ * phi_b = atan2(ifft2(C_b)), L = mean_R[(1/B) sum phi_b^2 - ((1/B) sum phi_b)^2].
+ * Replaces SSBEngine.reconstruct_with_loss (engine.py:1464-1514) and
+ * variance_loss_batch (engine.py:2120-2295). candidates: DEVICE array of
+ * n_cand qssb_aberrations_t; losses: device float32 [n_cand];
+ * mean_phase: device float32 [n_cand][R0][R1] (mean over b of phi_b) or NULL.
+ * The per-candidate reduction order is fixed: repeated calls return
+ * identical bits. */
+int qssb_loss_batch(const float* g_half, const float* bf_geom, const float* q_row,
+                    const float* q_col, const qssb_calibration_t* cal,
+                    const qssb_aberrations_t* candidates, int32_t n_cand, int32_t flags,
+                    void* workspace, size_t workspace_bytes, float* losses,
+                    float* mean_phase, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QSSB_H */

@@ -1,0 +1,116 @@
+"""ctypes binding of ``libqssb.so`` (the C ABI declared in ``include/qssb.h``).
+
+The shared library is built in-tree by ``quantem.gpu_b200.build`` (nvcc,
+sm_100a). There is no fallback: if the library is missing or a symbol is
+absent, loading raises, and every entry point's nonzero status becomes a
+Python exception carrying ``qssb_last_error()``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libqssb.so"
+
+QSSB_OK = 0
+QSSB_ERR_INVALID = -1
+QSSB_ERR_CUDA = -2
+QSSB_ERR_UNSUPPORTED = -3
+QSSB_ERR_WORKSPACE = -4
+QSSB_FLAG_CHI_FP64 = 1
+QSSB_FLAG_FULL_PLANE = 2
+
+
+class Calibration(ctypes.Structure):
+    """``qssb_calibration_t``."""
+
+    _fields_ = [
+        ("n_bf", ctypes.c_int32),
+        ("scan_rows", ctypes.c_int32),
+        ("scan_cols", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("wavelength_A", ctypes.c_double),
+        ("semiangle_rad", ctypes.c_double),
+        ("det_sampling_row_rad", ctypes.c_double),
+        ("det_sampling_col_rad", ctypes.c_double),
+        ("scan_sampling_row_A", ctypes.c_double),
+        ("scan_sampling_col_A", ctypes.c_double),
+        ("dc_re", ctypes.c_double),
+        ("dc_im", ctypes.c_double),
+    ]
+
+
+GEOM_ROWS = 8
+
+
+class Aberrations(ctypes.Structure):
+    """``qssb_aberrations_t`` (reference numeric convention: Angstrom, rad)."""
+
+    _fields_ = [
+        ("C10", ctypes.c_float),
+        ("C12", ctypes.c_float),
+        ("phi12", ctypes.c_float),
+        ("C30", ctypes.c_float),
+    ]
+
+
+_P = ctypes.c_void_p
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+_SZ = ctypes.c_size_t
+
+# name -> (restype, argtypes); must match include/qssb.h exactly.
+SIGNATURES = {
+    "qssb_version": (ctypes.c_int, []),
+    "qssb_last_error": (ctypes.c_char_p, []),
+    "qssb_mean_dp_u64": (ctypes.c_int, [_P, _I64, _I32, _P, _P, _P]),
+    "qssb_gather_bf_columns": (ctypes.c_int, [_P, _I64, _I32, _P, _I32, _P, _P]),
+    "qssb_scan_fft_half": (ctypes.c_int, [_P, _I32, _I32, _I32, _P, _P]),
+    "qssb_object_workspace_bytes": (
+        ctypes.c_int, [ctypes.POINTER(Calibration), _I32, ctypes.POINTER(_SZ)]),
+    "qssb_object": (ctypes.c_int, [
+        _P, _P, _P, _P, ctypes.POINTER(Calibration), ctypes.POINTER(Aberrations), _I32, _P, _SZ,
+        _P, _P, _P]),
+    "qssb_loss_workspace_bytes": (
+        ctypes.c_int, [ctypes.POINTER(Calibration), _I32, _I32, ctypes.POINTER(_SZ)]),
+    "qssb_loss_batch": (ctypes.c_int, [
+        _P, _P, _P, _P, ctypes.POINTER(Calibration), _P, _I32, _I32, _P, _SZ, _P, _P, _P]),
+}
+
+_lib = None
+
+
+class QssbError(RuntimeError):
+    """A nonzero status from the native library."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"qssb error {code}: {message}")
+        self.code = code
+
+
+def load() -> ctypes.CDLL:
+    """Load ``libqssb.so`` once; raise if it is missing (no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = Path(os.environ.get("QSSB_LIBRARY", LIB_PATH))
+    if not path.exists():
+        raise ImportError(
+            f"{path} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+            "or `python -m quantem.gpu_b200.build`. The SSB engine has no CPU fallback."
+        )
+    lib = ctypes.CDLL(str(path))
+    for name, (restype, argtypes) in SIGNATURES.items():
+        fn = getattr(lib, name)  # AttributeError if a symbol is absent
+        fn.restype = restype
+        fn.argtypes = argtypes
+    _lib = lib
+    return lib
+
+
+def check(code: int) -> None:
+    """Raise :class:`QssbError` for a nonzero status."""
+    if code != QSSB_OK:
+        msg = load().qssb_last_error()
+        raise QssbError(code, msg.decode() if msg else "")

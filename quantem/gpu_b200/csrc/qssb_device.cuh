@@ -1,0 +1,364 @@
+// qssb_device.cuh - device building blocks of the SSB engine (sm_100a).
+//
+// * complex helpers and radix-2/4/8 butterflies;
+// * a warp-cooperative Stockham FFT over one line held in shared memory
+//   (any stride), N in {64, 128, 256}, forward (exp(-2 pi i nk/N)) or
+//   inverse (exp(+2 pi i nk/N), unnormalised);
+// * the probe transfer function P(u) = A(u) exp(-i chi(u)) and the
+//   normalised double-overlap correction of the reference SSB kernels
+//   (bobleesj/quantem.gpu src/quantem/gpu/ssb/compute/cuda/kernels/
+//   common.py:115-236), restated.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../../include/qssb.h"
+
+namespace qssb {
+
+// ---------------------------------------------------------------- complex
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+__device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
+__device__ __forceinline__ float2 cneg_conj(float2 a) { return make_float2(-a.x, a.y); }
+// multiply by DIR * i  (DIR = -1: -i, DIR = +1: +i)
+template <int DIR>
+__device__ __forceinline__ float2 mul_dir_i(float2 a) {
+    return DIR < 0 ? make_float2(a.y, -a.x) : make_float2(-a.y, a.x);
+}
+
+// Twiddles tw[m] = exp(-2 pi i m / N), correctly rounded from FP64.
+template <int N>
+__device__ __forceinline__ void fill_twiddles(float2* tw, int tid, int nthreads) {
+    for (int m = tid; m < N; m += nthreads) {
+        double s, c;
+        sincospi(-2.0 * (double)m / (double)N, &s, &c);
+        tw[m] = make_float2((float)c, (float)s);
+    }
+}
+
+// ------------------------------------------------------------- butterflies
+template <int DIR>
+__device__ __forceinline__ void dft2(float2& a, float2& b) {
+    float2 t = a;
+    a = cadd(t, b);
+    b = csub(t, b);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft4(float2* v) {
+    float2 s02 = cadd(v[0], v[2]), d02 = csub(v[0], v[2]);
+    float2 s13 = cadd(v[1], v[3]), d13 = mul_dir_i<DIR>(csub(v[1], v[3]));
+    v[0] = cadd(s02, s13);
+    v[2] = csub(s02, s13);
+    v[1] = cadd(d02, d13);
+    v[3] = csub(d02, d13);
+}
+
+template <int DIR>
+__device__ __forceinline__ void dft8(float2* v) {
+    float2 e[4] = {v[0], v[2], v[4], v[6]};
+    float2 o[4] = {v[1], v[3], v[5], v[7]};
+    dft4<DIR>(e);
+    dft4<DIR>(o);
+    const float h = 0.70710678118654752440f;
+    // W8^k = exp(DIR 2 pi i k / 8)
+    float2 w1o = cmul(o[1], make_float2(h, DIR * h));
+    float2 w2o = mul_dir_i<DIR>(o[2]);
+    float2 w3o = cmul(o[3], make_float2(-h, DIR * h));
+    v[0] = cadd(e[0], o[0]);
+    v[4] = csub(e[0], o[0]);
+    v[1] = cadd(e[1], w1o);
+    v[5] = csub(e[1], w1o);
+    v[2] = cadd(e[2], w2o);
+    v[6] = csub(e[2], w2o);
+    v[3] = cadd(e[3], w3o);
+    v[7] = csub(e[3], w3o);
+}
+
+template <int R, int DIR>
+__device__ __forceinline__ void dft_r(float2* v) {
+    if constexpr (R == 2) {
+        dft2<DIR>(v[0], v[1]);
+    } else if constexpr (R == 4) {
+        dft4<DIR>(v);
+    } else {
+        static_assert(R == 8, "radix 2, 4 or 8");
+        dft8<DIR>(v);
+    }
+}
+
+// --------------------------------------------------------- Stockham stage
+// One radix-R pass of the self-sorting (Stockham) FFT over a line of N
+// complex values at x[i * stride], executed by the 32 lanes of one warp.
+// Butterfly j (of N/R) reads x[j + r N/R], twiddles by W_{Ns R}^{k r}
+// (k = j mod Ns), transforms and writes x[(j - k) R + k + r Ns]. All lanes
+// read before any lane writes (the __syncwarp between), so it runs in place.
+template <int N, int R, int NS, int DIR>
+__device__ __forceinline__ void stockham_stage(float2* x, int stride, const float2* tw, int lane) {
+    constexpr int NB = N / R;
+    constexpr int PER = (NB + 31) / 32;
+    constexpr int TWS = N / (NS * R);
+    float2 v[PER][R];
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int j = lane + 32 * t;
+        if (NB % 32 == 0 || j < NB) {
+            const int k = j & (NS - 1);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                float2 a = x[(j + r * NB) * stride];
+                if (NS > 1 && r > 0) {
+                    float2 w = tw[k * r * TWS];
+                    if (DIR > 0) w.y = -w.y;
+                    a = cmul(a, w);
+                }
+                v[t][r] = a;
+            }
+            dft_r<R, DIR>(v[t]);
+        }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int j = lane + 32 * t;
+        if (NB % 32 == 0 || j < NB) {
+            const int k = j & (NS - 1);
+            const int base = (j - k) * R + k;
+#pragma unroll
+            for (int r = 0; r < R; ++r) x[(base + r * NS) * stride] = v[t][r];
+        }
+    }
+    __syncwarp();
+}
+
+// Whole line FFT of length N (natural order in, natural order out).
+template <int N, int DIR>
+__device__ __forceinline__ void line_fft(float2* x, int stride, const float2* tw, int lane) {
+    if constexpr (N == 64) {
+        stockham_stage<64, 4, 1, DIR>(x, stride, tw, lane);
+        stockham_stage<64, 4, 4, DIR>(x, stride, tw, lane);
+        stockham_stage<64, 4, 16, DIR>(x, stride, tw, lane);
+    } else if constexpr (N == 128) {
+        stockham_stage<128, 4, 1, DIR>(x, stride, tw, lane);
+        stockham_stage<128, 4, 4, DIR>(x, stride, tw, lane);
+        stockham_stage<128, 4, 16, DIR>(x, stride, tw, lane);
+        stockham_stage<128, 2, 64, DIR>(x, stride, tw, lane);
+    } else {
+        static_assert(N == 256, "line FFT sizes 64, 128, 256");
+        stockham_stage<256, 8, 1, DIR>(x, stride, tw, lane);
+        stockham_stage<256, 8, 8, DIR>(x, stride, tw, lane);
+        stockham_stage<256, 4, 64, DIR>(x, stride, tw, lane);
+    }
+}
+
+// --------------------------------------------------------------- physics
+// Per-candidate probe constants. chi(u) = factor * alpha^2 *
+// (C10 + C12 (cos2phi cos2phi12 + sin2phi sin2phi12)) + c30_half * alpha^4,
+// factor = pi / lambda, c30_half = (pi / (2 lambda)) C30.
+struct Probe {
+    float wavelength;
+    float semiangle;
+    float ang_r;
+    float ang_c;
+    float inner2;     // (|u| <= inner) => aperture == 1 exactly; <= 0 disables
+    float outer2;     // (|u| >= outer) => aperture == 0 exactly
+    float factor;
+    float C10;
+    float C12;
+    float cos2p;
+    float sin2p;
+    float c30_half;
+    // FP64 calibration for near-tied aperture pairs (soft_aperture_fp64)
+    double semi_d, lam_d, ang_r_d, ang_c_d;
+    double qval_r, qval_c;  // 1 / (R d): q = fftfreq index * qval
+    int n_r, n_c;
+    double factor_d;  // FP64 copies for QSSB_FLAG_CHI_FP64
+    double C10_d;
+    double C12_d;
+    double cos2p_d;
+    double sin2p_d;
+    double c30_half_d;
+};
+
+// Soft aperture at displacement (dx, dy) with r2 = dx^2 + dy^2:
+// clip((alpha_max - lambda |u|) / denom + 0.5, 0, 1),
+// denom = sqrt((dx d_row)^2 + (dy d_col)^2) / |u|. Both shortcuts are exact:
+// denom <= max(d_row, d_col) makes the clipped edge 1 inside `inner` and 0
+// outside `outer`; only the band between them is evaluated.
+__device__ __forceinline__ float soft_aperture(float dx, float dy, float r2, const Probe& p) {
+    if (p.inner2 > 0.0f && r2 <= p.inner2) return 1.0f;
+    if (r2 >= p.outer2) return 0.0f;
+    const float r = sqrtf(r2);
+    const float alpha = r * p.wavelength;
+    const float num2 = fmaf(dx * p.ang_r, dx * p.ang_r, (dy * p.ang_c) * (dy * p.ang_c));
+    const float inv_r = r > 1e-15f ? 1.0f / r : 0.0f;
+    const float denom = sqrtf(num2) * inv_r;
+    const float edge = denom > 1e-15f ? (p.semiangle - alpha) / denom + 0.5f : 1.0f;
+    return fminf(fmaxf(edge, 0.0f), 1.0f);
+}
+
+__device__ __forceinline__ bool in_edge_band(float r2, const Probe& p) {
+    return !(p.inner2 > 0.0f && r2 <= p.inner2) && r2 < p.outer2;
+}
+
+// The same aperture in FP64 at displacement (dx, dy) (u = q -+ k from FP64
+// q and k), with the FP64 calibration.
+static __device__ __noinline__ float soft_aperture_fp64(double dx, double dy, double semiangle,
+                                                        double wavelength, double ang_r,
+                                                        double ang_c) {
+    const double r = sqrt(dx * dx + dy * dy);
+    const double ar = dx * ang_r;
+    const double ac = dy * ang_c;
+    const double num = sqrt(ar * ar + ac * ac);
+    if (!(r > 1e-300) || !(num > 0.0)) return 1.0f;
+    const double edge = (semiangle - r * wavelength) / (num / r) + 0.5;
+    return (float)fmin(fmax(edge, 0.0), 1.0);
+}
+
+// numpy.fft.fftfreq(n, d)[i] in FP64: (i < n/2 ? i : i - n) * (1 / (n d)).
+__device__ __forceinline__ double fftfreq_d(int i, int n, double val) {
+    return (double)(i < (n >> 1) ? i : i - n) * val;
+}
+
+// chi from (alpha^2, cos 2phi, sin 2phi).
+template <bool CHI64>
+__device__ __forceinline__ float chi_value(float alpha2, float cos2, float sin2, const Probe& p) {
+    if constexpr (CHI64) {
+        const double a2 = (double)alpha2;
+        const double term = fma(p.C12_d, fma((double)cos2, p.cos2p_d, (double)sin2 * p.sin2p_d), p.C10_d);
+        double chi = p.factor_d * a2 * term + p.c30_half_d * a2 * a2;
+        // exact reduction to [-pi, pi] in FP64
+        chi -= 6.283185307179586476925 * rint(chi * 0.15915494309189533577);
+        return (float)chi;
+    } else {
+        const float term = fmaf(p.C12, fmaf(cos2, p.cos2p, sin2 * p.sin2p), p.C10);
+        return fmaf(p.c30_half * alpha2, alpha2, p.factor * alpha2 * term);
+    }
+}
+
+// Geometry of one displacement as compute_geometry (common.py:115-157):
+// alpha^2 = r2 lambda^2, cos 2phi = (dx^2 - dy^2)/r2, sin 2phi = 2 dx dy / r2
+// (0 at the origin).
+struct Disp {
+    float r2, alpha2, cos2, sin2;
+};
+
+__device__ __forceinline__ Disp displacement(float dx, float dy, const Probe& p) {
+    Disp d;
+    const float dx2 = dx * dx;
+    const float dy2 = dy * dy;
+    d.r2 = dx2 + dy2;
+    d.alpha2 = (d.r2 * p.wavelength) * p.wavelength;
+    const float inv_r2 = d.r2 > 1e-30f ? 1.0f / d.r2 : 0.0f;
+    d.cos2 = (dx2 - dy2) * inv_r2;
+    d.sin2 = 2.0f * dx * dy * inv_r2;
+    return d;
+}
+
+template <bool CHI64>
+__device__ __forceinline__ float2 probe_from(const Disp& d, float ap, const Probe& p) {
+    if (ap == 0.0f) return make_float2(0.0f, 0.0f);
+    float s, c;
+    __sincosf(chi_value<CHI64>(d.alpha2, d.cos2, d.sin2, p), &s, &c);
+    return make_float2(ap * c, -ap * s);
+}
+
+// P(k_b) from the cached BF geometry (engine.py:217-231, _pk_kernel).
+template <bool CHI64>
+__device__ __forceinline__ float2 probe_at_bf(float alpha2, float cos2, float sin2, float aperture,
+                                              const Probe& p) {
+    float s, c;
+    __sincosf(chi_value<CHI64>(alpha2, cos2, sin2, p), &s, &c);
+    return make_float2(aperture * c, -aperture * s);
+}
+
+// Aperture pairs closer than this are re-evaluated in FP64 when either lies
+// in the edge band. For an aberration-free (real) Gamma = A(k)(A(q-k) -
+// A(q+k)) the sign of the unit-normalised Gamma is decided by that
+// difference; where q is (nearly) perpendicular to k it is pure float32
+// rounding (the edge carries ~1e-6 absolute), and on an integer-centred BF
+// lattice exactly perpendicular pairs are common. Evaluating both apertures
+// from FP64 q and k (k = kx + kx_lo) reproduces the FP64 result there.
+constexpr float kApertureTie = 1.0e-4f;
+
+// C = G conj(Gamma_hat), Gamma = P(q-k) conj(P(k)) - conj(P(q+k)) P(k),
+// Gamma_hat = Gamma * (|Gamma|^2 > 1e-16 ? 1/|Gamma| : 1e8)
+// (gamma_mul_pk_onthefly, common.py:173-236). (r, c) index the scan
+// frequency (qx, qy); kx_lo/ky_lo are the FP64 residuals of k.
+template <bool CHI64>
+__device__ __forceinline__ float2 corrected(float qx, float qy, int r, int c, float kx, float ky,
+                                            float kx_lo, float ky_lo, float2 pk, float2 g,
+                                            const Probe& p) {
+    const Disp dm = displacement(qx - kx, qy - ky, p);
+    const Disp dp = displacement(qx + kx, qy + ky, p);
+    float am = soft_aperture(qx - kx, qy - ky, dm.r2, p);
+    float ap = soft_aperture(qx + kx, qy + ky, dp.r2, p);
+    if (fabsf(am - ap) < kApertureTie && (in_edge_band(dm.r2, p) || in_edge_band(dp.r2, p))) {
+        const double qx64 = fftfreq_d(r, p.n_r, p.qval_r);
+        const double qy64 = fftfreq_d(c, p.n_c, p.qval_c);
+        const double kx64 = (double)kx + (double)kx_lo;
+        const double ky64 = (double)ky + (double)ky_lo;
+        am = soft_aperture_fp64(qx64 - kx64, qy64 - ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
+        ap = soft_aperture_fp64(qx64 + kx64, qy64 + ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
+    }
+    const float2 pm = probe_from<CHI64>(dm, am, p);
+    const float2 pp = probe_from<CHI64>(dp, ap, p);
+    // t1 = pm * conj(pk); t2 = conj(pp) * pk
+    const float t1r = fmaf(pm.x, pk.x, pm.y * pk.y);
+    const float t1i = fmaf(pm.y, pk.x, -pm.x * pk.y);
+    const float t2r = fmaf(pp.x, pk.x, pp.y * pk.y);
+    const float t2i = fmaf(pp.x, pk.y, -pp.y * pk.x);
+    float gr = t1r - t2r;
+    float gi = t1i - t2i;
+    const float m2 = fmaf(gr, gr, gi * gi);
+    const float inv = m2 > 1e-16f ? rsqrtf(m2) : 1e8f;
+    gr *= inv;
+    gi *= inv;
+    return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
+}
+
+// Probe constants of one candidate from the calibration (FP64 trig of phi12).
+__host__ __device__ inline Probe make_probe_common(const qssb_calibration_t& cal, float C10,
+                                                   float C12, float phi12, float C30) {
+    Probe p;
+    p.wavelength = (float)cal.wavelength_A;
+    p.semiangle = (float)cal.semiangle_rad;
+    p.ang_r = (float)cal.det_sampling_row_rad;
+    p.ang_c = (float)cal.det_sampling_col_rad;
+    const float max_ang = fmaxf(p.ang_r, p.ang_c);
+    const float inner = (p.semiangle - 0.5f * max_ang) / p.wavelength;
+    p.inner2 = inner > 0.0f ? inner * inner : 0.0f;
+    const float outer = (p.semiangle + 0.5f * max_ang) / p.wavelength;
+    p.outer2 = outer * outer;
+    p.semi_d = cal.semiangle_rad;
+    p.lam_d = cal.wavelength_A;
+    p.ang_r_d = cal.det_sampling_row_rad;
+    p.ang_c_d = cal.det_sampling_col_rad;
+    p.n_r = cal.scan_rows;
+    p.n_c = cal.scan_cols;
+    p.qval_r = 1.0 / ((double)cal.scan_rows * cal.scan_sampling_row_A);
+    p.qval_c = 1.0 / ((double)cal.scan_cols * cal.scan_sampling_col_A);
+    const double factor = 3.14159265358979323846 / cal.wavelength_A;
+    const double c2 = cos(2.0 * (double)phi12);
+    const double s2 = sin(2.0 * (double)phi12);
+    p.factor = (float)factor;
+    p.C10 = C10;
+    p.C12 = C12;
+    p.cos2p = (float)c2;
+    p.sin2p = (float)s2;
+    p.c30_half = (float)(0.5 * factor * (double)C30);
+    p.factor_d = factor;
+    p.C10_d = C10;
+    p.C12_d = C12;
+    p.cos2p_d = c2;
+    p.sin2p_d = s2;
+    p.c30_half_d = 0.5 * factor * (double)C30;
+    return p;
+}
+
+}  // namespace qssb

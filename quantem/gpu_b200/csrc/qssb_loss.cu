@@ -1,0 +1,269 @@
+// qssb_loss.cu - SSB phase-variance loss for a batch of aberration candidates.
+//
+// L(theta) = mean_R[(1/B) sum_b phi_b^2 - ((1/B) sum_b phi_b)^2],
+// phi_b = atan2(ifft2(C_b)) (docs/kernels/ssb.md:256-266 of the reference;
+// engine.py:1464-1514 and 2120-2295). Unlike the object, this needs one
+// inverse FFT per (candidate, BF pixel).
+//
+// k_loss_moments: grid (BF chunks, candidates), one CTA per SM (the N x N+1
+// complex plane lives in shared memory). Per BF pixel the CTA
+//   A) evaluates C_b on the +-q half set and mirrors it (C(-q) = -conj C(q),
+//      see qssb_object.cu), DC := dc;
+//   B) inverse-FFTs all rows, then all columns, in shared memory;
+//   C) takes atan2 of its owned pixels and accumulates sum / sum of squares
+//      in registers.
+// Partial moment planes per chunk are folded in a fixed order in FP64
+// (k_loss_reduce), and the per-pixel variance is averaged (k_loss_final):
+// repeated calls give identical bits.
+#include <math.h>
+
+#include "qssb_internal.h"
+
+namespace qssb {
+
+constexpr int kLossThreads = 512;
+constexpr int kLossWarps = kLossThreads / 32;
+
+template <int N>
+struct LossSmem {
+    static constexpr int P = N + 1;  // odd pitch: conflict-free column access
+    static constexpr size_t bytes = sizeof(float2) * ((size_t)N * P + N);
+};
+
+template <int N, bool SYM, bool CHI64>
+__global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments(
+    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
+    const float* __restrict__ q_row, const float* __restrict__ q_col,
+    const qssb_aberrations_t* __restrict__ cands, qssb_calibration_t cal, int bf_per_chunk, int n_chunks,
+    float* __restrict__ part) {
+    constexpr int H = N / 2 + 1;
+    constexpr int P = LossSmem<N>::P;
+    constexpr int CPW = N / kLossWarps;  // columns owned per warp
+    constexpr int RPL = N / 32;          // rows owned per lane
+    constexpr int NEVAL = SYM ? (N / 2 + 1) * N + (N / 2 - 1) : N * N;
+    extern __shared__ float2 smem[];
+    float2* plane = smem;
+    float2* tw = smem + N * P;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int chunk = blockIdx.x;
+    const int cand = blockIdx.y;
+    const qssb_aberrations_t ab = cands[cand];
+    const Probe p = make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
+    fill_twiddles<N>(tw, tid, kLossThreads);
+    float as[CPW][RPL], aq[CPW][RPL];
+#pragma unroll
+    for (int i = 0; i < CPW; ++i)
+#pragma unroll
+        for (int t = 0; t < RPL; ++t) as[i][t] = aq[i][t] = 0.0f;
+    const int b0 = chunk * bf_per_chunk;
+    int nb = n_bf - b0;
+    if (nb > bf_per_chunk) nb = bf_per_chunk;
+    const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
+    for (int i = 0; i < nb; ++i) {
+        const int b = b0 + i;
+        const float kx = __ldg(geom + b);
+        const float ky = __ldg(geom + n_bf + b);
+        const float kxlo = __ldg(geom + 6 * n_bf + b);
+        const float kylo = __ldg(geom + 7 * n_bf + b);
+        const float2 pk = probe_at_bf<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
+                                             __ldg(geom + 4 * n_bf + b), __ldg(geom + 5 * n_bf + b), p);
+        const float2* gb = g + (size_t)b * N * H;
+        // A) corrected spectrum into shared memory
+        for (int e = tid; e < NEVAL; e += kLossThreads) {
+            int r, c;
+            bool mirror = false;
+            if (!SYM || e < (N / 2 + 1) * N) {
+                r = e / N;
+                c = e - r * N;
+                mirror = SYM && r >= 1 && r < N / 2 && c != N / 2;
+            } else {
+                r = N / 2 + 1 + (e - (N / 2 + 1) * N);
+                c = N / 2;
+            }
+            float2 gv;
+            if (c <= N / 2) {
+                gv = __ldg(gb + r * H + c);
+            } else {
+                gv = cconj(__ldg(gb + ((N - r) & (N - 1)) * H + (N - c)));
+            }
+            float2 v = corrected<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c, kx, ky, kxlo, kylo,
+                                        pk, gv, p);
+            if (r == 0 && c == 0) v = dc;
+            plane[r * P + c] = v;
+            if (mirror) plane[(N - r) * P + ((N - c) & (N - 1))] = cneg_conj(v);
+        }
+        __syncthreads();
+        // B) rows, then columns (inverse, unnormalised: atan2 is scale-free)
+        for (int row = warp; row < N; row += kLossWarps) line_fft<N, +1>(plane + row * P, 1, tw, lane);
+        __syncthreads();
+#pragma unroll
+        for (int ci = 0; ci < CPW; ++ci) {
+            const int col = warp + ci * kLossWarps;
+            line_fft<N, +1>(plane + col, P, tw, lane);
+            // C) phase moments of the owned pixels
+#pragma unroll
+            for (int t = 0; t < RPL; ++t) {
+                const float2 v = plane[(lane + 32 * t) * P + col];
+                const float ph = atan2f(v.y, v.x);
+                as[ci][t] += ph;
+                aq[ci][t] = fmaf(ph, ph, aq[ci][t]);
+            }
+        }
+        __syncthreads();
+    }
+    // column-major partial planes: part[((cand * n_chunks + chunk) * 2 + m) * N * N + col * N + row]
+    float* ps = part + ((size_t)(cand * n_chunks + chunk) * 2) * N * N;
+    float* pq = ps + (size_t)N * N;
+#pragma unroll
+    for (int ci = 0; ci < CPW; ++ci) {
+        const int col = warp + ci * kLossWarps;
+#pragma unroll
+        for (int t = 0; t < RPL; ++t) {
+            ps[col * N + lane + 32 * t] = as[ci][t];
+            pq[col * N + lane + 32 * t] = aq[ci][t];
+        }
+    }
+}
+
+template <int N>
+__global__ void k_loss_reduce(const float* __restrict__ part, int n_chunks, int n_bf,
+                              double* __restrict__ var, float* __restrict__ mean_phase) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;  // col * N + row
+    const int cand = blockIdx.y;
+    if (j >= N * N) return;
+    double s1 = 0.0, s2 = 0.0;
+    for (int k = 0; k < n_chunks; ++k) {
+        const float* base = part + ((size_t)(cand * n_chunks + k) * 2) * N * N;
+        s1 += (double)base[j];
+        s2 += (double)base[(size_t)N * N + j];
+    }
+    const double inv_b = 1.0 / (double)n_bf;
+    const double mean = s1 * inv_b;
+    var[(size_t)cand * N * N + j] = s2 * inv_b - mean * mean;
+    if (mean_phase) {
+        const int col = j / N;
+        const int row = j - col * N;
+        mean_phase[(size_t)cand * N * N + row * N + col] = (float)mean;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_loss_final(const double* __restrict__ var, int npos,
+                                                    float* __restrict__ losses) {
+    __shared__ double red[256];
+    const int cand = blockIdx.x;
+    const double* v = var + (size_t)cand * npos;
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < npos; i += 256) acc += v[i];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) losses[cand] = (float)(red[0] / (double)npos);
+}
+
+struct LossPlan {
+    int bf_per_chunk;
+    int n_chunks;
+    size_t part_bytes;
+    size_t var_bytes;
+};
+
+// Deterministic: about 296 CTAs in total (two per B200 SM), at least one BF
+// pixel each.
+static LossPlan plan_loss(int n, int n_bf, int n_cand) {
+    LossPlan pl;
+    int chunks = (296 + n_cand - 1) / n_cand;
+    if (chunks < 1) chunks = 1;
+    if (chunks > n_bf) chunks = n_bf;
+    pl.bf_per_chunk = (n_bf + chunks - 1) / chunks;
+    pl.n_chunks = (n_bf + pl.bf_per_chunk - 1) / pl.bf_per_chunk;
+    pl.part_bytes = sizeof(float) * 2 * (size_t)n * n * pl.n_chunks * n_cand;
+    pl.part_bytes = (pl.part_bytes + 255) & ~(size_t)255;
+    pl.var_bytes = sizeof(double) * (size_t)n * n * n_cand;
+    return pl;
+}
+
+template <int N, bool SYM, bool CHI64>
+static int launch_loss(const float* g_half, const float* geom, const float* q_row,
+                       const float* q_col, const qssb_calibration_t& cal,
+                       const qssb_aberrations_t* cands, int n_cand, char* ws, float* losses,
+                       float* mean_phase, cudaStream_t s) {
+    const LossPlan pl = plan_loss(N, cal.n_bf, n_cand);
+    float* part = reinterpret_cast<float*>(ws);
+    double* var = reinterpret_cast<double*>(ws + pl.part_bytes);
+    const size_t smem = LossSmem<N>::bytes;
+    CUDA_TRY(cudaFuncSetAttribute(k_loss_moments<N, SYM, CHI64>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_loss_moments<N, SYM, CHI64><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
+        reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal,
+        pl.bf_per_chunk, pl.n_chunks, part);
+    CUDA_TRY(cudaGetLastError());
+    k_loss_reduce<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(part, pl.n_chunks, cal.n_bf,
+                                                                       var, mean_phase);
+    CUDA_TRY(cudaGetLastError());
+    k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N, losses);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+template <int N>
+static int dispatch_loss(bool sym, bool chi64, const float* g_half, const float* geom,
+                         const float* q_row, const float* q_col, const qssb_calibration_t& cal,
+                         const qssb_aberrations_t* cands, int n_cand, char* ws, float* losses,
+                         float* mean_phase, cudaStream_t s) {
+    if (sym)
+        return chi64 ? launch_loss<N, true, true>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
+                     : launch_loss<N, true, false>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
+    return chi64 ? launch_loss<N, false, true>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
+                 : launch_loss<N, false, false>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
+}
+
+}  // namespace qssb
+
+using namespace qssb;
+
+extern "C" int qssb_loss_workspace_bytes(const qssb_calibration_t* cal, int32_t n_cand,
+                                         int32_t flags, size_t* bytes) {
+    (void)flags;
+    int rc = validate_calibration(cal, "qssb_loss_workspace_bytes: null calibration");
+    if (rc) return rc;
+    if (!bytes || n_cand <= 0 || n_cand > 65535)
+        return set_error(QSSB_ERR_INVALID, "qssb_loss_workspace_bytes: n_cand must be in [1, 65535]");
+    const int n = cal->scan_rows;
+    if (n != 64 && n != 128)
+        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64 or 128");
+    const LossPlan pl = plan_loss(n, cal->n_bf, n_cand);
+    *bytes = pl.part_bytes + pl.var_bytes;
+    return QSSB_OK;
+}
+
+extern "C" int qssb_loss_batch(const float* g_half, const float* bf_geom, const float* q_row,
+                               const float* q_col, const qssb_calibration_t* cal,
+                               const qssb_aberrations_t* candidates, int32_t n_cand, int32_t flags,
+                               void* workspace, size_t workspace_bytes, float* losses,
+                               float* mean_phase, void* stream) {
+    int rc = validate_calibration(cal, "qssb_loss_batch: null calibration");
+    if (rc) return rc;
+    if (!g_half || !bf_geom || !q_row || !q_col || !candidates || !workspace || !losses)
+        return set_error(QSSB_ERR_INVALID, "qssb_loss_batch: null pointer");
+    size_t need = 0;
+    rc = qssb_loss_workspace_bytes(cal, n_cand, flags, &need);
+    if (rc) return rc;
+    if (workspace_bytes < need)
+        return set_error(QSSB_ERR_WORKSPACE, "qssb_loss_batch: workspace too small");
+    if (((uintptr_t)workspace & 255u) != 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_loss_batch: workspace must be 256-byte aligned");
+    const bool sym = !(flags & QSSB_FLAG_FULL_PLANE);
+    const bool chi64 = (flags & QSSB_FLAG_CHI_FP64) != 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    char* ws = static_cast<char*>(workspace);
+    switch (cal->scan_rows) {
+        case 64: return dispatch_loss<64>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, ws, losses, mean_phase, s);
+        case 128: return dispatch_loss<128>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, ws, losses, mean_phase, s);
+        default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64 or 128");
+    }
+}

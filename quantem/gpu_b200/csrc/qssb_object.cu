@@ -1,0 +1,329 @@
+// qssb_object.cu - SSB object wave by the corrected Fourier ("trotter") sum.
+//
+// O = ifft2((1/B) sum_b C_b), C_b(q) = G_b(q) conj(Gamma_hat_b(q)), DC := dc.
+// By IFFT linearity this equals the reference's per-BF path
+// (ifft2 of every C_b, then mean over b; engine.py:1109-1151) and its
+// Fourier-sum path (engine.py:1047-1107), but runs no per-BF inverse FFT.
+//
+// +-q symmetry: for aberrations whose chi is even in u (C10, C12, C30 - the
+// only ones this entry point takes) and the point-symmetric soft aperture,
+// P(-u) = P(u), hence Gamma_b(-q) = -conj(Gamma_b(q)) bit for bit, and with
+// G_b(-q) = conj(G_b(q)) (real scan images) C_b(-q) = -conj(C_b(q)). The
+// frequencies computed are the stored half plane (all rows, columns 0..N/2)
+// plus the Nyquist row's remaining columns (whose mirror frequency +N/2 is not
+// on the fftfreq grid); the rest is filled by the mirror relation after the
+// sum. That is N(N/2+1) + N/2 - 1 of the N^2 overlap evaluations.
+//
+// Kernels: k_trotter_partial (per BF chunk, Kahan-compensated FP32 sums per
+// frequency) -> k_trotter_plane (fixed-order FP64 fold of the chunks, mirror
+// fill, DC, 1/B) -> k_ifft_rows -> k_ifft_cols_phase (1/N^2, atan2).
+#include <math.h>
+
+#include "qssb_internal.h"
+
+namespace qssb {
+
+constexpr int kMaxBfChunk = 256;
+constexpr int kTrotterThreads = 256;
+
+struct QMap {
+    int r, c, gr, gc;  // scan-frequency (r, c); stored half-plane element (gr, gc)
+    bool conj;         // load conj(G[gr][gc])
+};
+
+// Index -> frequency for the evaluated set.
+template <int N, bool SYM>
+__device__ __forceinline__ QMap qmap(int qi) {
+    constexpr int H = N / 2 + 1;
+    QMap m;
+    if constexpr (SYM) {
+        if (qi < N * H) {
+            m.r = qi / H;
+            m.c = qi - m.r * H;
+            m.gr = m.r;
+            m.gc = m.c;
+            m.conj = false;
+        } else {
+            m.r = N / 2;
+            m.c = H + (qi - N * H);
+            m.gr = N / 2;
+            m.gc = N - m.c;
+            m.conj = true;
+        }
+    } else {
+        m.r = qi / N;
+        m.c = qi - m.r * N;
+        if (m.c <= N / 2) {
+            m.gr = m.r;
+            m.gc = m.c;
+            m.conj = false;
+        } else {
+            m.gr = (N - m.r) & (N - 1);
+            m.gc = N - m.c;
+            m.conj = true;
+        }
+    }
+    return m;
+}
+
+template <int N, bool SYM>
+__host__ __device__ constexpr int n_eval_q() {
+    return SYM ? N * (N / 2 + 1) + N / 2 - 1 : N * N;
+}
+
+template <int N, bool SYM, bool CHI64>
+__global__ void __launch_bounds__(kTrotterThreads) k_trotter_partial(
+    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
+    const float* __restrict__ q_row, const float* __restrict__ q_col, Probe p, int bf_per_chunk,
+    float2* __restrict__ partial) {
+    constexpr int H = N / 2 + 1;
+    constexpr int NQ = n_eval_q<N, SYM>();
+    __shared__ float s_kx[kMaxBfChunk];
+    __shared__ float s_ky[kMaxBfChunk];
+    __shared__ float s_kxlo[kMaxBfChunk];
+    __shared__ float s_kylo[kMaxBfChunk];
+    __shared__ float2 s_pk[kMaxBfChunk];
+    const int tid = threadIdx.x;
+    const int chunk = blockIdx.y;
+    const int b0 = chunk * bf_per_chunk;
+    int nb = n_bf - b0;
+    if (nb > bf_per_chunk) nb = bf_per_chunk;
+    for (int i = tid; i < nb; i += kTrotterThreads) {
+        const int b = b0 + i;
+        s_kx[i] = __ldg(geom + b);
+        s_ky[i] = __ldg(geom + n_bf + b);
+        s_kxlo[i] = __ldg(geom + 6 * n_bf + b);
+        s_kylo[i] = __ldg(geom + 7 * n_bf + b);
+        s_pk[i] = probe_at_bf<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
+                                     __ldg(geom + 4 * n_bf + b), __ldg(geom + 5 * n_bf + b), p);
+    }
+    __syncthreads();
+    const int qi = blockIdx.x * kTrotterThreads + tid;
+    if (qi >= NQ) return;
+    const QMap m = qmap<N, SYM>(qi);
+    const float qx = __ldg(q_row + m.r);
+    const float qy = __ldg(q_col + m.c);
+    const float2* gp = g + (size_t)b0 * N * H + m.gr * H + m.gc;
+    float sr = 0.f, si = 0.f, er = 0.f, ei = 0.f;  // Kahan sums and compensations
+#pragma unroll 2
+    for (int i = 0; i < nb; ++i) {
+        float2 gv = __ldg(gp + (size_t)i * N * H);
+        if (m.conj) gv.y = -gv.y;
+        const float2 v = corrected<CHI64>(qx, qy, m.r, m.c, s_kx[i], s_ky[i], s_kxlo[i], s_kylo[i],
+                                          s_pk[i], gv, p);
+        const float yr = v.x - er;
+        const float tr = sr + yr;
+        er = (tr - sr) - yr;
+        sr = tr;
+        const float yi = v.y - ei;
+        const float ti = si + yi;
+        ei = (ti - si) - yi;
+        si = ti;
+    }
+    partial[(size_t)chunk * NQ + qi] = make_float2(sr, si);
+}
+
+// Full N x N corrected-mean plane from the chunk partials.
+template <int N, bool SYM>
+__global__ void k_trotter_plane(const float2* __restrict__ partial, int n_chunks, int n_bf,
+                                float2 dc, float2* __restrict__ plane) {
+    constexpr int H = N / 2 + 1;
+    constexpr int NQ = n_eval_q<N, SYM>();
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= N * N) return;
+    const int r = idx / N;
+    const int c = idx - r * N;
+    int qi;
+    bool mirror = false;
+    if constexpr (SYM) {
+        if (c <= N / 2) {
+            qi = r * H + c;
+        } else if (r == N / 2) {
+            qi = N * H + (c - H);
+        } else {
+            qi = ((N - r) & (N - 1)) * H + (N - c);
+            mirror = true;
+        }
+    } else {
+        qi = idx;
+    }
+    double sr = 0.0, si = 0.0;
+    for (int k = 0; k < n_chunks; ++k) {
+        const float2 v = partial[(size_t)k * NQ + qi];
+        sr += (double)v.x;
+        si += (double)v.y;
+    }
+    if (mirror) sr = -sr;  // S(-q) = -conj(S(q)): real part flips, imaginary part stays
+    const double inv_b = 1.0 / (double)n_bf;
+    float2 out = make_float2((float)(sr * inv_b), (float)(si * inv_b));
+    if (r == 0 && c == 0) out = dc;
+    plane[idx] = out;
+}
+
+// In-place inverse FFT of every row of a N x N plane (one warp per row).
+template <int N>
+__global__ void __launch_bounds__(256) k_ifft_rows(float2* __restrict__ plane) {
+    __shared__ float2 tw[N];
+    __shared__ float2 line[8][N];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    fill_twiddles<N>(tw, tid, 256);
+    const int row = blockIdx.x * 8 + warp;
+    __syncthreads();
+    if (row >= N) return;
+    float2* src = plane + (size_t)row * N;
+    for (int i = lane; i < N; i += 32) line[warp][i] = src[i];
+    __syncwarp();
+    line_fft<N, +1>(line[warp], 1, tw, lane);
+    for (int i = lane; i < N; i += 32) src[i] = line[warp][i];
+}
+
+// Inverse FFT of every column, 1/N^2, object and atan2 phase.
+template <int N>
+__global__ void __launch_bounds__(256) k_ifft_cols_phase(const float2* __restrict__ plane,
+                                                         float2* __restrict__ object,
+                                                         float* __restrict__ phase) {
+    __shared__ float2 tw[N];
+    __shared__ float2 line[8][N];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    fill_twiddles<N>(tw, tid, 256);
+    const int col = blockIdx.x * 8 + warp;
+    __syncthreads();
+    if (col >= N) return;
+    for (int i = lane; i < N; i += 32) line[warp][i] = plane[(size_t)i * N + col];
+    __syncwarp();
+    line_fft<N, +1>(line[warp], 1, tw, lane);
+    const float scale = 1.0f / (float)(N * N);
+    for (int i = lane; i < N; i += 32) {
+        float2 v = line[warp][i];
+        v.x *= scale;
+        v.y *= scale;
+        object[(size_t)i * N + col] = v;
+        if (phase) phase[(size_t)i * N + col] = atan2f(v.y, v.x);
+    }
+}
+
+struct ObjectPlan {
+    int n_q;
+    int bf_per_chunk;
+    int n_chunks;
+    size_t partial_bytes;
+    size_t plane_bytes;
+};
+
+// Deterministic chunking (independent of the GPU's SM count): about 40 BF
+// chunks, 4..256 BF pixels each.
+static ObjectPlan plan_object(int n, int n_bf, bool sym) {
+    ObjectPlan pl;
+    pl.n_q = sym ? n * (n / 2 + 1) + n / 2 - 1 : n * n;
+    int bpc = (n_bf + 39) / 40;
+    if (bpc < 4) bpc = 4;
+    if (bpc > kMaxBfChunk) bpc = kMaxBfChunk;
+    pl.bf_per_chunk = bpc;
+    pl.n_chunks = (n_bf + bpc - 1) / bpc;
+    pl.partial_bytes = sizeof(float2) * (size_t)pl.n_chunks * pl.n_q;
+    pl.partial_bytes = (pl.partial_bytes + 255) & ~(size_t)255;
+    pl.plane_bytes = sizeof(float2) * (size_t)n * n;
+    return pl;
+}
+
+Probe make_probe(const qssb_calibration_t& cal, const qssb_aberrations_t& ab) {
+    return make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
+}
+
+int validate_calibration(const qssb_calibration_t* cal, const char* who) {
+    if (!cal) return set_error(QSSB_ERR_INVALID, who);
+    if (cal->n_bf <= 0 || cal->scan_rows != cal->scan_cols)
+        return set_error(QSSB_ERR_INVALID, "calibration: n_bf must be >= 1 and the scan square");
+    if (!(cal->wavelength_A > 0.0) || !(cal->semiangle_rad >= 0.0) ||
+        !(cal->det_sampling_row_rad > 0.0) || !(cal->det_sampling_col_rad > 0.0) ||
+        !(cal->scan_sampling_row_A > 0.0) || !(cal->scan_sampling_col_A > 0.0))
+        return set_error(QSSB_ERR_INVALID, "calibration: wavelength and samplings must be positive");
+    if (cal->reserved != 0) return set_error(QSSB_ERR_INVALID, "calibration: reserved must be 0");
+    if (!isfinite(cal->dc_re) || !isfinite(cal->dc_im))
+        return set_error(QSSB_ERR_INVALID, "calibration: dc must be finite");
+    return QSSB_OK;
+}
+
+template <int N, bool SYM, bool CHI64>
+static int launch_object(const float* g_half, const float* geom, const float* q_row,
+                         const float* q_col, const qssb_calibration_t& cal, const Probe& p,
+                         char* ws, float* object, float* phase, cudaStream_t s) {
+    const ObjectPlan pl = plan_object(N, cal.n_bf, SYM);
+    float2* partial = reinterpret_cast<float2*>(ws);
+    float2* plane = reinterpret_cast<float2*>(ws + pl.partial_bytes);
+    const dim3 grid((pl.n_q + kTrotterThreads - 1) / kTrotterThreads, pl.n_chunks);
+    k_trotter_partial<N, SYM, CHI64><<<grid, kTrotterThreads, 0, s>>>(
+        reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, p, pl.bf_per_chunk,
+        partial);
+    CUDA_TRY(cudaGetLastError());
+    k_trotter_plane<N, SYM><<<(N * N + 255) / 256, 256, 0, s>>>(
+        partial, pl.n_chunks, cal.n_bf, make_float2((float)cal.dc_re, (float)cal.dc_im), plane);
+    CUDA_TRY(cudaGetLastError());
+    k_ifft_rows<N><<<N / 8, 256, 0, s>>>(plane);
+    CUDA_TRY(cudaGetLastError());
+    k_ifft_cols_phase<N><<<N / 8, 256, 0, s>>>(plane, reinterpret_cast<float2*>(object), phase);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+template <int N>
+static int dispatch_object(bool sym, bool chi64, const float* g_half, const float* geom,
+                           const float* q_row, const float* q_col, const qssb_calibration_t& cal,
+                           const Probe& p, char* ws, float* object, float* phase, cudaStream_t s) {
+    if (sym) {
+        return chi64 ? launch_object<N, true, true>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s)
+                     : launch_object<N, true, false>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s);
+    }
+    return chi64 ? launch_object<N, false, true>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s)
+                 : launch_object<N, false, false>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s);
+}
+
+}  // namespace qssb
+
+using namespace qssb;
+
+extern "C" int qssb_object_workspace_bytes(const qssb_calibration_t* cal, int32_t flags,
+                                           size_t* bytes) {
+    int rc = validate_calibration(cal, "qssb_object_workspace_bytes: null calibration");
+    if (rc) return rc;
+    if (!bytes) return set_error(QSSB_ERR_INVALID, "qssb_object_workspace_bytes: null output");
+    const int n = cal->scan_rows;
+    if (n != 64 && n != 128 && n != 256)
+        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_object: scan size must be 64, 128 or 256");
+    const ObjectPlan pl = plan_object(n, cal->n_bf, !(flags & QSSB_FLAG_FULL_PLANE));
+    *bytes = pl.partial_bytes + pl.plane_bytes;
+    return QSSB_OK;
+}
+
+extern "C" int qssb_object(const float* g_half, const float* bf_geom, const float* q_row,
+                           const float* q_col, const qssb_calibration_t* cal,
+                           const qssb_aberrations_t* ab, int32_t flags, void* workspace,
+                           size_t workspace_bytes, float* object, float* phase, void* stream) {
+    int rc = validate_calibration(cal, "qssb_object: null calibration");
+    if (rc) return rc;
+    if (!g_half || !bf_geom || !q_row || !q_col || !ab || !workspace || !object)
+        return set_error(QSSB_ERR_INVALID, "qssb_object: null pointer");
+    if (!isfinite(ab->C10) || !isfinite(ab->C12) || !isfinite(ab->phi12) || !isfinite(ab->C30))
+        return set_error(QSSB_ERR_INVALID, "qssb_object: aberrations must be finite");
+    size_t need = 0;
+    rc = qssb_object_workspace_bytes(cal, flags, &need);
+    if (rc) return rc;
+    if (workspace_bytes < need) return set_error(QSSB_ERR_WORKSPACE, "qssb_object: workspace too small");
+    if (((uintptr_t)workspace & 255u) != 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_object: workspace must be 256-byte aligned");
+    const Probe p = make_probe(*cal, *ab);
+    const bool sym = !(flags & QSSB_FLAG_FULL_PLANE);
+    const bool chi64 = (flags & QSSB_FLAG_CHI_FP64) != 0;
+    cudaStream_t s = (cudaStream_t)stream;
+    char* ws = static_cast<char*>(workspace);
+    switch (cal->scan_rows) {
+        case 64: return dispatch_object<64>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, ws, object, phase, s);
+        case 128: return dispatch_object<128>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, ws, object, phase, s);
+        case 256: return dispatch_object<256>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, ws, object, phase, s);
+        default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_object: scan size must be 64, 128 or 256");
+    }
+}

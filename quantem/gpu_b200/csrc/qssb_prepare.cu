@@ -1,0 +1,286 @@
+// qssb_prepare.cu - dataset preparation: exact u64 mean diffraction pattern,
+// BF-column gather and the per-BF Hermitian scan FFT (sm_100a).
+//
+// HBM layout: counts[f][k] u16 with k = k_row * K1 + k_col contiguous per
+// frame (the reference's data.reshape(-1, K0, K1), backend.py:432); BF
+// columns [b][f] u16 (BF-major, one 32 KB scan image per BF pixel at 128^2);
+// spectra [b][r][c] complex64 with c in [0, R1/2] (backend.py:547-554).
+#include "qssb_internal.h"
+
+namespace qssb {
+
+// --------------------------------------------------------------- mean DP
+// Each thread owns 8 detector pixels (one 16-byte vector per frame) and a
+// contiguous range of frames; u32 partials (<= 65536 frames * 65535 fits)
+// are folded into the u64 sums with one atomic per pixel per chunk. Integer
+// addition commutes, so the result is exact and order-independent.
+constexpr int kSumThreads = 256;
+
+__global__ void __launch_bounds__(kSumThreads) k_sum_frames_vec8(
+    const uint4* __restrict__ counts, long long n_frames, int nvec, int frames_per_chunk,
+    unsigned long long* __restrict__ sums) {
+    const int vec = blockIdx.x * kSumThreads + threadIdx.x;
+    if (vec >= nvec) return;
+    const long long f0 = (long long)blockIdx.y * frames_per_chunk;
+    long long f1 = f0 + frames_per_chunk;
+    if (f1 > n_frames) f1 = n_frames;
+    uint32_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const uint4* p = counts + f0 * (long long)nvec + vec;
+    long long f = f0;
+    auto add = [&](uint4 v) {
+        acc[0] += v.x & 0xffffu; acc[1] += v.x >> 16;
+        acc[2] += v.y & 0xffffu; acc[3] += v.y >> 16;
+        acc[4] += v.z & 0xffffu; acc[5] += v.z >> 16;
+        acc[6] += v.w & 0xffffu; acc[7] += v.w >> 16;
+    };
+    for (; f + 4 <= f1; f += 4) {
+        const uint4 v0 = __ldcs(p);
+        const uint4 v1 = __ldcs(p + nvec);
+        const uint4 v2 = __ldcs(p + 2 * (long long)nvec);
+        const uint4 v3 = __ldcs(p + 3 * (long long)nvec);
+        p += 4 * (long long)nvec;
+        add(v0); add(v1); add(v2); add(v3);
+    }
+    for (; f < f1; ++f) {
+        add(__ldcs(p));
+        p += nvec;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        if (acc[i]) atomicAdd(&sums[vec * 8 + i], (unsigned long long)acc[i]);
+}
+
+// Fallback for detector sizes that are not a multiple of 8 pixels or
+// unaligned bases: one pixel per thread.
+__global__ void k_sum_frames_scalar(const uint16_t* __restrict__ counts, long long n_frames,
+                                    int npix, int frames_per_chunk,
+                                    unsigned long long* __restrict__ sums) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= npix) return;
+    const long long f0 = (long long)blockIdx.y * frames_per_chunk;
+    long long f1 = f0 + frames_per_chunk;
+    if (f1 > n_frames) f1 = n_frames;
+    uint32_t acc = 0;
+    for (long long f = f0; f < f1; ++f) acc += counts[f * npix + k];
+    if (acc) atomicAdd(&sums[k], (unsigned long long)acc);
+}
+
+__global__ void k_mean_from_sums(const unsigned long long* __restrict__ sums, int npix,
+                                 float n_frames_f, float* __restrict__ mean_dp) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < npix) mean_dp[k] = __fdiv_rn(__ull2float_rn(sums[k]), n_frames_f);
+}
+
+// ---------------------------------------------------------------- gather
+// Tile of 64 frames x 64 BF pixels through shared memory: each warp reads 32
+// BF entries of one frame (mostly contiguous within a detector row) and
+// writes 64 consecutive frames (128 bytes) of one BF column.
+constexpr int kGatherF = 64;
+constexpr int kGatherB = 64;
+
+__global__ void __launch_bounds__(256) k_gather_columns(
+    const uint16_t* __restrict__ counts, long long n_frames, int npix,
+    const int32_t* __restrict__ bf_linear, int n_bf, uint16_t* __restrict__ columns) {
+    __shared__ uint16_t tile[kGatherB][kGatherF + 2];
+    const int tid = threadIdx.x;
+    const long long f0 = (long long)blockIdx.x * kGatherF;
+    const int b0 = blockIdx.y * kGatherB;
+    const int bl = tid & (kGatherB - 1);
+    const int b = b0 + bl;
+    const int lin = b < n_bf ? __ldg(bf_linear + b) : 0;
+    // an index outside the detector reads nothing (its column stays zero);
+    // the host wrapper rejects such indices before launch
+    const bool ok = b < n_bf && lin >= 0 && lin < npix;
+    for (int fl = tid >> 6; fl < kGatherF; fl += 4) {
+        const long long f = f0 + fl;
+        uint16_t v = 0;
+        if (ok && f < n_frames) v = __ldcs(counts + f * npix + lin);
+        tile[bl][fl] = v;
+    }
+    __syncthreads();
+    // write: 64 BF rows x 32 u32 words (2 frames each)
+    const bool full = (f0 + kGatherF <= n_frames) && ((n_frames & 1) == 0);
+    for (int w = tid; w < kGatherB * (kGatherF / 2); w += 256) {
+        const int row = w >> 5;
+        const int word = w & 31;
+        const int bb = b0 + row;
+        if (bb >= n_bf) continue;
+        const long long f = f0 + 2 * word;
+        uint16_t* dst = columns + (long long)bb * n_frames + f;
+        if (full) {
+            const uint32_t packed = (uint32_t)tile[row][2 * word] | ((uint32_t)tile[row][2 * word + 1] << 16);
+            *reinterpret_cast<uint32_t*>(dst) = packed;
+        } else {
+            if (f < n_frames) dst[0] = tile[row][2 * word];
+            if (f + 1 < n_frames) dst[1] = tile[row][2 * word + 1];
+        }
+    }
+}
+
+// ----------------------------------------------------- Hermitian scan FFT
+// One CTA per BF image (N x N real). Rows 2j and 2j+1 are packed as the real
+// and imaginary parts of one complex line, transformed together and split:
+// X_2j(c) = (Z(c) + conj Z(-c)) / 2, X_2j+1(c) = (Z(c) - conj Z(-c)) / (2i),
+// keeping c in [0, N/2]. The N/2+1 columns are then transformed along rows.
+template <int N>
+struct ScanFftSmem {
+    static constexpr int H = N / 2 + 1;
+    static constexpr int PP = N + 1;          // packed-line pitch (odd)
+    static constexpr int HP = H;              // half-plane pitch (odd for N=128,256)
+    static constexpr size_t bytes = sizeof(float2) * ((size_t)(N / 2) * PP + (size_t)N * HP + N);
+};
+
+template <int N>
+__global__ void __launch_bounds__(512, 1) k_scan_fft_half(const uint16_t* __restrict__ columns,
+                                                          int n_bf, float2* __restrict__ g_half) {
+    using S = ScanFftSmem<N>;
+    extern __shared__ float2 smem[];
+    float2* packed = smem;                         // [N/2][PP]
+    float2* half = packed + (N / 2) * S::PP;       // [N][HP]
+    float2* tw = half + N * S::HP;                 // [N]
+    const int b = blockIdx.x;
+    if (b >= n_bf) return;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    constexpr int NW = 16;
+    fill_twiddles<N>(tw, tid, 512);
+    // load N*N u16 as uint4 (8 values), pack row pairs
+    const uint4* src = reinterpret_cast<const uint4*>(columns + (size_t)b * N * N);
+    constexpr int NV = N * N / 8;
+    for (int i = tid; i < NV; i += 512) {
+        const uint4 v = __ldcs(src + i);
+        const int e = i * 8;
+        const int row = e / N;
+        const int col = e % N;
+        const int j = row >> 1;
+        const bool odd = row & 1;
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float lo = (float)(w[q] & 0xffffu);
+            const float hi = (float)(w[q] >> 16);
+            float* d0 = reinterpret_cast<float*>(&packed[j * S::PP + col + 2 * q]);
+            float* d1 = reinterpret_cast<float*>(&packed[j * S::PP + col + 2 * q + 1]);
+            d0[odd ? 1 : 0] = lo;
+            d1[odd ? 1 : 0] = hi;
+        }
+    }
+    __syncthreads();
+    for (int j = warp; j < N / 2; j += NW) {
+        float2* line = packed + j * S::PP;
+        line_fft<N, -1>(line, 1, tw, lane);
+        for (int c = lane; c < S::H; c += 32) {
+            const float2 z = line[c];
+            const float2 zm = line[(N - c) & (N - 1)];
+            // even = (z + conj zm)/2 ; odd = (z - conj zm)/(2i)
+            const float2 ev = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+            const float2 od = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+            half[(2 * j) * S::HP + c] = ev;
+            half[(2 * j + 1) * S::HP + c] = od;
+        }
+    }
+    __syncthreads();
+    for (int c = warp; c < S::H; c += NW) line_fft<N, -1>(half + c, S::HP, tw, lane);
+    __syncthreads();
+    float2* dst = g_half + (size_t)b * N * S::H;
+    for (int i = tid; i < N * S::H; i += 512) {
+        const int r = i / S::H;
+        const int c = i - r * S::H;
+        dst[i] = half[r * S::HP + c];
+    }
+}
+
+}  // namespace qssb
+
+using namespace qssb;
+
+extern "C" int qssb_mean_dp_u64(const uint16_t* counts, int64_t n_frames, int32_t det_pixels,
+                                uint64_t* sums, float* mean_dp, void* stream) {
+    if (!counts || !sums || n_frames <= 0 || det_pixels <= 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_mean_dp_u64: null pointer or empty shape");
+    if (n_frames > (int64_t)1 << 40)
+        return set_error(QSSB_ERR_INVALID, "qssb_mean_dp_u64: n_frames too large");
+    cudaStream_t s = (cudaStream_t)stream;
+    CUDA_TRY(cudaMemsetAsync(sums, 0, sizeof(uint64_t) * (size_t)det_pixels, s));
+    const int sms = device_sm_count();
+    const bool vec = (det_pixels % 8 == 0) && (((uintptr_t)counts & 15u) == 0);
+    if (vec) {
+        const int nvec = det_pixels / 8;
+        const int gx = (nvec + kSumThreads - 1) / kSumThreads;
+        // about 8 resident CTAs per SM, two waves
+        long long want = (long long)sms * 16 / gx;
+        if (want < 1) want = 1;
+        long long chunk = (n_frames + want - 1) / want;
+        if (chunk > 32768) chunk = 32768;
+        if (chunk < 4) chunk = 4;
+        const long long gy = (n_frames + chunk - 1) / chunk;
+        if (gy > 65535) return set_error(QSSB_ERR_INVALID, "qssb_mean_dp_u64: too many frames");
+        k_sum_frames_vec8<<<dim3(gx, (unsigned)gy), kSumThreads, 0, s>>>(
+            reinterpret_cast<const uint4*>(counts), n_frames, nvec, (int)chunk,
+            reinterpret_cast<unsigned long long*>(sums));
+    } else {
+        const int gx = (det_pixels + 255) / 256;
+        long long want = (long long)sms * 16 / gx;
+        if (want < 1) want = 1;
+        long long chunk = (n_frames + want - 1) / want;
+        if (chunk > 32768) chunk = 32768;
+        const long long gy = (n_frames + chunk - 1) / chunk;
+        if (gy > 65535) return set_error(QSSB_ERR_INVALID, "qssb_mean_dp_u64: too many frames");
+        k_sum_frames_scalar<<<dim3(gx, (unsigned)gy), 256, 0, s>>>(
+            counts, n_frames, det_pixels, (int)chunk, reinterpret_cast<unsigned long long*>(sums));
+    }
+    CUDA_TRY(cudaGetLastError());
+    if (mean_dp) {
+        k_mean_from_sums<<<(det_pixels + 255) / 256, 256, 0, s>>>(
+            reinterpret_cast<const unsigned long long*>(sums), det_pixels, (float)n_frames, mean_dp);
+        CUDA_TRY(cudaGetLastError());
+    }
+    return QSSB_OK;
+}
+
+extern "C" int qssb_gather_bf_columns(const uint16_t* counts, int64_t n_frames, int32_t det_pixels,
+                                      const int32_t* bf_linear, int32_t n_bf, uint16_t* columns,
+                                      void* stream) {
+    if (!counts || !bf_linear || !columns || n_frames <= 0 || det_pixels <= 0 || n_bf <= 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_gather_bf_columns: null pointer or empty shape");
+    if (((uintptr_t)columns & 3u) != 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_gather_bf_columns: columns must be 4-byte aligned");
+    const long long gx = (n_frames + kGatherF - 1) / kGatherF;
+    const int gy = (n_bf + kGatherB - 1) / kGatherB;
+    if (gx > 0x7fffffffLL || gy > 65535)
+        return set_error(QSSB_ERR_INVALID, "qssb_gather_bf_columns: grid too large");
+    k_gather_columns<<<dim3((unsigned)gx, gy), 256, 0, (cudaStream_t)stream>>>(
+        counts, n_frames, det_pixels, bf_linear, n_bf, columns);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+template <int N>
+static int launch_scan_fft(const uint16_t* columns, int n_bf, float* g_half, cudaStream_t s) {
+    const size_t smem = ScanFftSmem<N>::bytes;
+    CUDA_TRY(cudaFuncSetAttribute(k_scan_fft_half<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    k_scan_fft_half<N><<<n_bf, 512, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half));
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+extern "C" int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t scan_rows,
+                                  int32_t scan_cols, float* g_half, void* stream) {
+    if (!columns || !g_half || n_bf <= 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_scan_fft_half: null pointer or empty shape");
+    if (scan_rows != scan_cols)
+        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_scan_fft_half: square scans only");
+    if (((uintptr_t)columns & 15u) != 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_scan_fft_half: columns must be 16-byte aligned");
+    if (n_bf > 0x7fffffff)
+        return set_error(QSSB_ERR_INVALID, "qssb_scan_fft_half: too many BF pixels");
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (scan_rows) {
+        case 64: return launch_scan_fft<64>(columns, n_bf, g_half, s);
+        case 128: return launch_scan_fft<128>(columns, n_bf, g_half, s);
+        default:
+            return set_error(QSSB_ERR_UNSUPPORTED, "qssb_scan_fft_half: scan size must be 64 or 128");
+    }
+}

@@ -1,0 +1,198 @@
+"""Device operations of the SSB engine, called through the C ABI.
+
+Thin wrappers that check shapes/dtypes on the host, allocate outputs as
+torch CUDA tensors (torch is the allocator and stream provider only) and
+call ``libqssb.so``. Every computation runs in the native sm_100a kernels;
+a CPU tensor is rejected rather than computed elsewhere.
+"""
+from __future__ import annotations
+
+import contextlib
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import Aberrations, Calibration, check
+
+# Kernel launches each entry point enqueues (the evidence counted by bench.py).
+LAUNCHES_PER_CALL = {
+    "qssb_mean_dp_u64": 2,
+    "qssb_gather_bf_columns": 1,
+    "qssb_scan_fft_half": 1,
+    "qssb_object": 4,
+    "qssb_loss_batch": 3,
+}
+LAUNCH_COUNT = 0
+_PROFILE: list | None = None
+
+
+@contextlib.contextmanager
+def profile_ops():
+    """Record (entry point, start event, end event) around every C-ABI call.
+
+    Events are recorded on the calling stream, so their elapsed time is the
+    device time of the kernels that call enqueued.
+    """
+    global _PROFILE
+    prev = _PROFILE
+    _PROFILE = []
+    try:
+        yield _PROFILE
+    finally:
+        _PROFILE = prev
+
+
+def _call(name: str, device: torch.device, *args) -> None:
+    global LAUNCH_COUNT
+    fn = getattr(_lib.load(), name)
+    if _PROFILE is None:
+        check(fn(*args))
+    else:
+        stream = torch.cuda.current_stream(device)
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        check(fn(*args))
+        end.record(stream)
+        _PROFILE.append((name, start, end))
+    LAUNCH_COUNT += LAUNCHES_PER_CALL.get(name, 0)
+
+
+def _require_cuda(t: torch.Tensor, name: str, dtype: torch.dtype) -> None:
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise ValueError(f"{name} must be a CUDA tensor (the SSB engine has no CPU path)")
+    if t.dtype != dtype:
+        raise TypeError(f"{name} must be {dtype}, got {t.dtype}")
+    if not t.is_contiguous():
+        raise ValueError(f"{name} must be contiguous")
+
+
+def _stream(t: torch.Tensor) -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream(t.device).cuda_stream)
+
+
+def _ptr(t: torch.Tensor | None) -> ctypes.c_void_p:
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+class Workspace:
+    """A reusable, growing device scratch buffer (256-byte aligned)."""
+
+    def __init__(self, device: torch.device | str = "cuda"):
+        self.device = torch.device(device)
+        self._buf: torch.Tensor | None = None
+
+    def get(self, nbytes: int) -> torch.Tensor:
+        if self._buf is None or self._buf.numel() < nbytes:
+            self._buf = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=self.device)
+        return self._buf
+
+    def release(self) -> None:
+        self._buf = None
+
+
+def mean_dp_u64(counts: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor]:
+    """Exact u64 detector sums and float32 mean DP of ``counts[..., K0, K1]``.
+
+    Returns (sums as int64 [K0, K1] holding the u64 values, mean_dp f32 [K0, K1]).
+    """
+    _require_cuda(counts, "counts", torch.uint16)
+    k0, k1 = int(counts.shape[-2]), int(counts.shape[-1])
+    n_frames = counts.numel() // (k0 * k1)
+    sums = torch.empty((k0, k1), dtype=torch.int64, device=counts.device)
+    mean = torch.empty((k0, k1), dtype=torch.float32, device=counts.device)
+    _call("qssb_mean_dp_u64", counts.device, _ptr(counts), n_frames, k0 * k1, _ptr(sums),
+          _ptr(mean), _stream(counts))
+    return sums, mean
+
+
+def gather_bf_columns(counts: torch.Tensor, bf_linear: torch.Tensor) -> torch.Tensor:
+    """columns[b, f] = counts[f, bf_linear[b]] (u16, BF-major)."""
+    _require_cuda(counts, "counts", torch.uint16)
+    _require_cuda(bf_linear, "bf_linear", torch.int32)
+    k0, k1 = int(counts.shape[-2]), int(counts.shape[-1])
+    n_frames = counts.numel() // (k0 * k1)
+    n_bf = int(bf_linear.numel())
+    if n_bf and (int(bf_linear.min()) < 0 or int(bf_linear.max()) >= k0 * k1):
+        raise ValueError("bf_linear indices must lie in [0, K0*K1)")
+    out = torch.empty((n_bf, n_frames), dtype=torch.uint16, device=counts.device)
+    _call("qssb_gather_bf_columns", counts.device, _ptr(counts), n_frames, k0 * k1,
+          _ptr(bf_linear), n_bf, _ptr(out), _stream(counts))
+    return out
+
+
+def scan_fft_half(columns: torch.Tensor, scan_shape: tuple[int, int]) -> torch.Tensor:
+    """Hermitian half-plane scan spectra G[b, r, c], c in [0, R1/2] (complex64)."""
+    _require_cuda(columns, "columns", torch.uint16)
+    r0, r1 = int(scan_shape[0]), int(scan_shape[1])
+    n_bf = int(columns.shape[0])
+    if columns.shape[1] != r0 * r1:
+        raise ValueError("columns must hold R0*R1 frames per BF pixel")
+    g = torch.empty((n_bf, r0, r1 // 2 + 1), dtype=torch.complex64, device=columns.device)
+    _call("qssb_scan_fft_half", columns.device, _ptr(columns), n_bf, r0, r1, _ptr(g),
+          _stream(columns))
+    return g
+
+
+def object_workspace_bytes(cal: Calibration, flags: int = 0) -> int:
+    n = ctypes.c_size_t(0)
+    check(_lib.load().qssb_object_workspace_bytes(ctypes.byref(cal), int(flags), ctypes.byref(n)))
+    return int(n.value)
+
+
+def object_wave(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
+                q_col: torch.Tensor, cal: Calibration, ab: Aberrations, *, flags: int = 0,
+                workspace: Workspace | None = None, want_phase: bool = True
+                ) -> tuple[torch.Tensor, torch.Tensor | None]:
+    """Object wave (complex64 [R0, R1]) and its phase (float32) for one candidate."""
+    _require_cuda(g_half, "g_half", torch.complex64)
+    _require_cuda(bf_geom, "bf_geom", torch.float32)
+    _require_cuda(q_row, "q_row", torch.float32)
+    _require_cuda(q_col, "q_col", torch.float32)
+    r0, r1 = int(cal.scan_rows), int(cal.scan_cols)
+    if (tuple(g_half.shape) != (cal.n_bf, r0, r1 // 2 + 1)
+            or tuple(bf_geom.shape) != (_lib.GEOM_ROWS, cal.n_bf)):
+        raise ValueError("g_half / bf_geom shapes do not match the calibration")
+    ws = workspace or Workspace(g_half.device)
+    need = object_workspace_bytes(cal, flags)
+    buf = ws.get(need)
+    obj = torch.empty((r0, r1), dtype=torch.complex64, device=g_half.device)
+    ph = torch.empty((r0, r1), dtype=torch.float32, device=g_half.device) if want_phase else None
+    _call("qssb_object", g_half.device, _ptr(g_half), _ptr(bf_geom), _ptr(q_row), _ptr(q_col),
+          ctypes.byref(cal), ctypes.byref(ab), int(flags), _ptr(buf), buf.numel(), _ptr(obj),
+          _ptr(ph), _stream(g_half))
+    return obj, ph
+
+
+def loss_workspace_bytes(cal: Calibration, n_cand: int, flags: int = 0) -> int:
+    n = ctypes.c_size_t(0)
+    check(_lib.load().qssb_loss_workspace_bytes(ctypes.byref(cal), int(n_cand), int(flags),
+                                                ctypes.byref(n)))
+    return int(n.value)
+
+
+def loss_batch(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
+               q_col: torch.Tensor, cal: Calibration, candidates: torch.Tensor, *,
+               flags: int = 0, workspace: Workspace | None = None, want_mean_phase: bool = False
+               ) -> tuple[torch.Tensor, torch.Tensor | None]:
+    """Phase-variance losses for ``candidates`` (float32 CUDA [n, 4]: C10, C12, phi12, C30)."""
+    _require_cuda(g_half, "g_half", torch.complex64)
+    _require_cuda(bf_geom, "bf_geom", torch.float32)
+    _require_cuda(candidates, "candidates", torch.float32)
+    if candidates.ndim != 2 or candidates.shape[1] != 4:
+        raise ValueError("candidates must have shape (n, 4): C10, C12, phi12, C30")
+    if (tuple(g_half.shape) != (cal.n_bf, int(cal.scan_rows), int(cal.scan_cols) // 2 + 1)
+            or tuple(bf_geom.shape) != (_lib.GEOM_ROWS, cal.n_bf)):
+        raise ValueError("g_half / bf_geom shapes do not match the calibration")
+    n = int(candidates.shape[0])
+    r0, r1 = int(cal.scan_rows), int(cal.scan_cols)
+    ws = workspace or Workspace(g_half.device)
+    buf = ws.get(loss_workspace_bytes(cal, n, flags))
+    losses = torch.empty(n, dtype=torch.float32, device=g_half.device)
+    mp = (torch.empty((n, r0, r1), dtype=torch.float32, device=g_half.device)
+          if want_mean_phase else None)
+    _call("qssb_loss_batch", g_half.device, _ptr(g_half), _ptr(bf_geom), _ptr(q_row),
+          _ptr(q_col), ctypes.byref(cal), _ptr(candidates), n, int(flags), _ptr(buf), buf.numel(),
+          _ptr(losses), _ptr(mp), _stream(g_half))
+    return losses, mp

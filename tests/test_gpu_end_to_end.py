@@ -1,0 +1,115 @@
+"""End-to-end: u16 counts -> B200SSBBackend / SSB -> object phase, vs the oracle.
+
+Covers the CPU-runnable plain workload (32x32 scan, 64x64 detector, padded
+to 128 by the reference rule) and the production workload (128x128 scan,
+128x128 detector, ~1800 BF pixels) with the north-star bar of 1e-4 rad RMS
+phase error against the FP64 oracle, exact integer selection and an exact dc.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import ssb_oracle as so
+from quantem.gpu_b200 import SSB, B200SSBBackend, SSBProtocol
+from quantem.gpu_b200.synthetic import CONFIGS, generate
+from recipes import disk_input
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+
+
+def _compare(backend: B200SSBBackend, host: np.ndarray, kw: dict, ab: so.Aberrations,
+             check_loss: bool = True):
+    prep = so.prepare(host, **kw)
+    np.testing.assert_array_equal(backend.bf_inds_row, prep.bf.rows)
+    np.testing.assert_array_equal(backend.bf_inds_col, prep.bf.cols)
+    assert backend.bf_center == prep.bf.center
+    # both are means of exact integer sums; only the summation order differs
+    assert abs(backend.dc_value - prep.dc) <= 1e-14 * abs(prep.dc)
+    g = backend.G_qk.cpu().numpy()
+    assert np.abs(g - prep.g_half).max() <= 2e-6 * np.abs(prep.g_half).max()
+    obj, ph = backend.object_and_phase(ab.C10, ab.C12, ab.phi12)
+    ref_obj, ref_ph = so.reconstruct(prep, ab)
+    err = so.wrapped_phase_error(ph.cpu().numpy(), ref_ph)
+    rms = float(np.sqrt(np.mean(err ** 2)))
+    assert rms < 1e-4, rms
+    if check_loss:
+        ref_loss, _ = so.phase_variance_loss(prep.g_half, prep.geo, ab, prep.dc)
+        loss = backend.variance_loss(ab.C10, ab.C12, ab.phi12)
+        assert loss == pytest.approx(ref_loss, rel=1e-5, abs=1e-6)
+    return rms
+
+
+def test_plain_32x32_det64_end_to_end():
+    spec = CONFIGS["plain_32x32_det64"]
+    counts = generate(spec, device="cpu").counts.numpy()
+    kw = dict(voltage_kV=300, semiangle_mrad=20.0, scan_sampling=0.5, det_sampling=20.0 / 12.0)
+    backend = B200SSBBackend(counts, semiangle=20.0, scan_sampling=0.5, det_sampling=20.0 / 12.0,
+                             voltage_kV=300)
+    assert isinstance(backend, SSBProtocol)
+    assert backend.scan_shape == (128, 128)
+    _compare(backend, counts, kw, so.Aberrations(50.0, 20.0, 0.3))
+    backend.close()
+
+
+def test_disk_case_matches_reference_golden():
+    """The reference test's own end-to-end input, bf_radius=3."""
+    counts = disk_input(123)
+    kw = dict(voltage_kV=300, semiangle_mrad=21.4, scan_sampling=0.5, det_sampling=1.0, bf_radius=3)
+    backend = B200SSBBackend(torch.as_tensor(counts, device=DEV), semiangle=21.4, scan_sampling=0.5,
+                             det_sampling=1.0, voltage_kV=300, bf_radius=3,
+                             aberrations={"C10": -120.0, "C12": 55.0, "phi12": math.radians(17.0)})
+    _compare(backend, counts, kw, so.Aberrations(-120.0, 55.0, math.radians(17.0)))
+    with np.load("tests/golden/ref_disk128_bfr3.npz") as z:
+        ref_obj = z["object"].astype(np.complex128)
+        ref_loss = float(z["loss"])
+    res = backend.result()
+    obj = res.object_wave.cpu().numpy()
+    assert np.abs(obj - ref_obj).max() <= 1e-5 * np.abs(ref_obj).max()
+    assert res.loss == pytest.approx(ref_loss, rel=1e-4, abs=1e-6)
+    assert res.num_bf == 27
+
+
+def test_uneven_96_scan_is_padded_like_the_reference():
+    counts = disk_input(124, scan=(96, 96))
+    kw = dict(voltage_kV=300, semiangle_mrad=21.4, scan_sampling=0.5, det_sampling=1.0, bf_radius=3)
+    backend = B200SSBBackend(counts, semiangle=21.4, scan_sampling=0.5, det_sampling=1.0,
+                             voltage_kV=300, bf_radius=3)
+    assert backend.scan_shape == (128, 128)
+    _compare(backend, counts, kw, so.Aberrations(10.0, 5.0, 0.1))
+
+
+def test_production_128x128_det128_end_to_end():
+    spec = CONFIGS["plain_128x128_det128"]
+    data = generate(spec, device=DEV)
+    counts = data.counts
+    host = counts.cpu().numpy()
+    kw = dict(voltage_kV=300, semiangle_mrad=20.0, scan_sampling=0.5, det_sampling=20.0 / 24.0)
+    backend = B200SSBBackend(counts, semiangle=20.0, scan_sampling=0.5, det_sampling=20.0 / 24.0,
+                             voltage_kV=300)
+    assert 1700 <= backend.num_bf <= 1900
+    rms = _compare(backend, host, kw, so.Aberrations(0.0, 0.0, 0.0), check_loss=False)
+    assert rms < 1e-4
+
+
+def test_ssb_session_fit_recovers_defocus():
+    """A short sweep + Nelder-Mead on data made with C10 = 100 A finds it.
+
+    1e6 e per position: at 1000 e on a 32x32 scan the phase-variance
+    objective is noise-dominated and its global minimum is the degenerate
+    C10 ~ 0 (Gamma vanishes where both q-k and q+k are inside the aperture)."""
+    spec = CONFIGS["plain_32x32_det64"]
+    from dataclasses import replace
+
+    counts = generate(replace(spec, C10=100.0, dose=1e6, seed=3), device="cpu").counts.numpy()
+    with SSB.from_array(counts, voltage_kV=300, semiangle_mrad=20.0, scan_sampling_A=0.5,
+                        det_sampling=20.0 / 12.0) as ssb:
+        res = ssb.fit(trials=64, search_ranges={"C10_nm": (-200.0, 200.0), "C12_nm": 0.0,
+                                                "phi12_deg": 0.0}, verbose=False)
+    assert abs(res.aberrations["C10"] - 100.0) < 15.0
+    assert res.refine_method == "nelder-mead"
+    assert res.loss is not None

@@ -1,0 +1,220 @@
+"""Parity of the sm_100a kernels (through the C ABI) with the FP64 oracle.
+
+Integer work (sums, gathers) must be bit-exact. Floating-point results use
+the reference's precision contract (tests/ssb_precision.py:7-10 of
+bobleesj/quantem.gpu: phase 2e-4 rad, loss rel 1e-5 / abs 1e-6) or, where
+stated, the north-star target of 1e-4 rad RMS phase error vs FP64.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import ssb_oracle as so
+from quantem.gpu_b200 import ops
+from quantem.gpu_b200._lib import (
+    QSSB_FLAG_CHI_FP64,
+    QSSB_FLAG_FULL_PLANE,
+    Aberrations,
+    Calibration,
+    QssbError,
+)
+from quantem.gpu_b200.calibration import bf_geometry, scan_frequencies
+from recipes import disk_input
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+PHASE_ATOL = 2.0e-4
+LOSS_RTOL = 1.0e-5
+LOSS_ATOL = 1.0e-6
+
+
+def _dev(a: np.ndarray, dtype=None) -> torch.Tensor:
+    t = torch.as_tensor(np.ascontiguousarray(a), device=DEV)
+    return t if dtype is None else t.to(dtype)
+
+
+def _prep_case(data: np.ndarray, **kw):
+    prep = so.prepare(data, **kw)
+    det = prep.detector_shape
+    ang = kw["det_sampling"]
+    ang = (ang, ang) if isinstance(ang, (int, float)) else ang
+    geo = bf_geometry(prep.bf.rows, prep.bf.cols, prep.bf.center, det, prep.sampling,
+                      prep.wavelength, kw["semiangle_mrad"], ang, 0.0)
+    q_row, q_col = scan_frequencies(prep.scan_shape, (kw["scan_sampling"],) * 2)
+    cal = Calibration(
+        n_bf=prep.g_half.shape[0], scan_rows=prep.scan_shape[0], scan_cols=prep.scan_shape[1],
+        reserved=0, wavelength_A=prep.wavelength, semiangle_rad=kw["semiangle_mrad"] * 1e-3,
+        det_sampling_row_rad=ang[0] * 1e-3, det_sampling_col_rad=ang[1] * 1e-3,
+        scan_sampling_row_A=kw["scan_sampling"], scan_sampling_col_A=kw["scan_sampling"],
+        dc_re=prep.dc.real, dc_im=prep.dc.imag)
+    dev = dict(
+        g=_dev(prep.g_half.astype(np.complex64)),
+        geom=_dev(geo.stacked()),
+        q_row=_dev(q_row),
+        q_col=_dev(q_col),
+    )
+    return prep, cal, dev
+
+
+DISK_KW = dict(voltage_kV=300, semiangle_mrad=21.4, scan_sampling=0.5, det_sampling=1.0, bf_radius=3)
+
+
+@pytest.fixture(scope="module")
+def disk_case():
+    return _prep_case(disk_input(123), **DISK_KW)
+
+
+# ------------------------------------------------------------------ integer
+@pytest.mark.parametrize("shape", [(16, 16, 16, 16), (7, 9, 24, 40), (3, 5, 13, 11), (128, 128, 8, 8)])
+def test_mean_dp_is_bit_exact(shape):
+    rng = np.random.default_rng(sum(shape))
+    data = rng.integers(0, 65536, size=shape, dtype=np.uint16)
+    sums, mean = ops.mean_dp_u64(_dev(data))
+    ref_sums, ref_mean = so.mean_dp_u64(data)
+    np.testing.assert_array_equal(sums.cpu().numpy().view(np.uint64), ref_sums)
+    np.testing.assert_array_equal(mean.cpu().numpy(), ref_mean)
+
+
+def test_mean_dp_saturated_counts_exact():
+    data = np.full((64, 64, 8, 8), 65535, dtype=np.uint16)
+    sums, mean = ops.mean_dp_u64(_dev(data))
+    assert int(sums.cpu().numpy().view(np.uint64).max()) == 65535 * 4096
+    np.testing.assert_array_equal(mean.cpu().numpy(), np.full((8, 8), 65535.0, np.float32))
+
+
+@pytest.mark.parametrize("n_frames,npix,n_bf", [(16384, 16384, 1810), (1000, 37, 5), (65, 64, 64), (1, 8, 1)])
+def test_gather_is_bit_exact(n_frames, npix, n_bf):
+    rng = np.random.default_rng(n_frames + npix)
+    data = rng.integers(0, 65536, size=(n_frames, npix), dtype=np.uint16)
+    lin = np.sort(rng.choice(npix, size=n_bf, replace=False)).astype(np.int32)
+    cols = ops.gather_bf_columns(_dev(data.reshape(n_frames, 1, npix)), _dev(lin))
+    np.testing.assert_array_equal(cols.cpu().numpy(), data[:, lin].T)
+
+
+# -------------------------------------------------------------- scan FFT
+@pytest.mark.parametrize("n", [64, 128])
+def test_scan_fft_half_matches_fp64(n):
+    rng = np.random.default_rng(n)
+    images = rng.integers(0, 4000, size=(9, n, n), dtype=np.uint16)
+    g = ops.scan_fft_half(_dev(images.reshape(9, n * n)), (n, n)).cpu().numpy()
+    ref = np.fft.rfft2(images.astype(np.float64))
+    err = np.abs(g - ref).max() / np.abs(ref).max()
+    assert err < 2e-6, err
+    # DC of an integer image is exact in FP32 while the sum stays below 2^24
+    np.testing.assert_array_equal(g[:, 0, 0].real, images.reshape(9, -1).sum(axis=1).astype(np.float32))
+
+
+# ---------------------------------------------------------------- object
+@pytest.mark.parametrize("flags", [0, QSSB_FLAG_FULL_PLANE, QSSB_FLAG_CHI_FP64])
+def test_object_matches_oracle(disk_case, flags):
+    prep, cal, d = disk_case
+    ab = so.Aberrations(C10=-120.0, C12=55.0, phi12=math.radians(17.0))
+    obj, ph = ops.object_wave(d["g"], d["geom"], d["q_row"], d["q_col"], cal,
+                              Aberrations(ab.C10, ab.C12, ab.phi12, 0.0), flags=flags)
+    ref_obj, ref_ph = so.reconstruct(prep, ab)
+    obj = obj.cpu().numpy().astype(np.complex128)
+    assert np.abs(obj - ref_obj).max() <= 2e-6 * np.abs(ref_obj).max()
+    err = so.wrapped_phase_error(ph.cpu().numpy(), ref_ph)
+    assert np.sqrt(np.mean(err ** 2)) < 1e-4
+    assert np.abs(err).max() < PHASE_ATOL
+
+
+def test_symmetric_and_full_plane_agree(disk_case):
+    prep, cal, d = disk_case
+    ab = Aberrations(35.0, 12.0, 0.4, 0.0)
+    a, _ = ops.object_wave(d["g"], d["geom"], d["q_row"], d["q_col"], cal, ab, flags=0)
+    b, _ = ops.object_wave(d["g"], d["geom"], d["q_row"], d["q_col"], cal, ab, flags=QSSB_FLAG_FULL_PLANE)
+    a = a.cpu().numpy()
+    b = b.cpu().numpy()
+    assert np.abs(a - b).max() <= 1e-6 * np.abs(b).max()
+
+
+def test_object_with_spherical_aberration_matches_oracle(disk_case):
+    prep, cal, d = disk_case
+    ab = so.Aberrations(C10=40.0, C12=10.0, phi12=0.2, C30=2.0e5)
+    obj, ph = ops.object_wave(d["g"], d["geom"], d["q_row"], d["q_col"], cal,
+                              Aberrations(ab.C10, ab.C12, ab.phi12, ab.C30), flags=QSSB_FLAG_CHI_FP64)
+    ref_obj, ref_ph = so.reconstruct(prep, ab)
+    assert np.abs(obj.cpu().numpy() - ref_obj).max() <= 2e-6 * np.abs(ref_obj).max()
+
+
+def test_zero_input_known_answer():
+    """G = 0, one BF pixel, dc = 1 -> object 1/N^2 everywhere, loss 0."""
+    n = 128
+    g = torch.zeros((1, n, n // 2 + 1), dtype=torch.complex64, device=DEV)
+    geo = bf_geometry(np.asarray([16], np.int32), np.asarray([17], np.int32), (16.0, 16.0), (32, 32),
+                      (1.0, 1.0), 0.0197, 21.4, (1.0, 1.0), 0.0)
+    q_row, q_col = scan_frequencies((n, n), (0.5, 0.5))
+    cal = Calibration(n_bf=1, scan_rows=n, scan_cols=n, reserved=0, wavelength_A=0.0197,
+                      semiangle_rad=0.0214, det_sampling_row_rad=1e-3, det_sampling_col_rad=1e-3,
+                      scan_sampling_row_A=0.5, scan_sampling_col_A=0.5, dc_re=1.0, dc_im=0.0)
+    obj, ph = ops.object_wave(g, _dev(geo.stacked()), _dev(q_row), _dev(q_col), cal,
+                              Aberrations(0.0, 0.0, 0.0, 0.0))
+    np.testing.assert_allclose(obj.cpu().numpy(), np.full((n, n), 1.0 / n ** 2), atol=2e-7)
+    np.testing.assert_array_equal(ph.cpu().numpy(), 0.0)
+    losses, _ = ops.loss_batch(g, _dev(geo.stacked()), _dev(q_row), _dev(q_col), cal,
+                               torch.zeros((2, 4), device=DEV))
+    np.testing.assert_array_equal(losses.cpu().numpy(), 0.0)
+
+
+# ------------------------------------------------------------------- loss
+CANDS = [(-120.0, 55.0, math.radians(17.0)), (-80.0, 30.0, math.radians(-5.0)),
+         (20.0, 40.0, math.radians(11.0)), (100.0, 10.0, math.radians(43.0))]
+
+
+@pytest.mark.parametrize("flags", [0, QSSB_FLAG_FULL_PLANE])
+def test_loss_batch_matches_oracle(disk_case, flags):
+    """variance_loss_batch vs the explicit reference (test_ssb_cuda_128.py:726-744)."""
+    prep, cal, d = disk_case
+    cands = torch.tensor([[a, b, c, 0.0] for a, b, c in CANDS], dtype=torch.float32, device=DEV)
+    losses, mp = ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands, flags=flags,
+                                want_mean_phase=True)
+    losses = losses.cpu().numpy()
+    mp = mp.cpu().numpy()
+    for i, (a, b, c) in enumerate(CANDS):
+        ref_loss, ref_mean = so.phase_variance_loss(prep.g_half, prep.geo, so.Aberrations(a, b, c), prep.dc)
+        assert losses[i] == pytest.approx(ref_loss, rel=LOSS_RTOL, abs=LOSS_ATOL)
+        err = np.abs(so.wrapped_phase_error(mp[i], ref_mean))
+        assert np.percentile(err, 99.9) < PHASE_ATOL
+
+
+def test_loss_batch_is_bitwise_repeatable(disk_case):
+    prep, cal, d = disk_case
+    cands = torch.tensor([[a, b, c, 0.0] for a, b, c in CANDS] * 3, dtype=torch.float32, device=DEV)
+    first, _ = ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands)
+    for _ in range(3):
+        again, _ = ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands)
+        assert torch.equal(first, again)
+    # identical candidates give identical bits regardless of batch position
+    first = first.cpu().numpy()
+    np.testing.assert_array_equal(first[:4], first[4:8])
+
+
+# ------------------------------------------------------------ boundaries
+def test_invalid_arguments_raise_without_launching(disk_case):
+    prep, cal, d = disk_case
+    bad = Calibration(**{f: getattr(cal, f) for f, _ in Calibration._fields_})
+    bad.scan_rows = 96
+    bad.scan_cols = 96
+    with pytest.raises(QssbError):
+        ops.object_workspace_bytes(bad)
+    bad2 = Calibration(**{f: getattr(cal, f) for f, _ in Calibration._fields_})
+    bad2.wavelength_A = 0.0
+    with pytest.raises(QssbError):
+        ops.object_wave(d["g"], d["geom"], d["q_row"], d["q_col"], bad2, Aberrations(0, 0, 0, 0))
+    with pytest.raises(QssbError):
+        ops.object_wave(d["g"], d["geom"], d["q_row"], d["q_col"], cal,
+                        Aberrations(float("nan"), 0, 0, 0))
+    with pytest.raises(ValueError):
+        ops.mean_dp_u64(torch.zeros((4, 4), dtype=torch.uint16))  # CPU tensor: no CPU path
+    torch.cuda.synchronize()
+
+
+def test_empty_bf_rejected():
+    with pytest.raises(QssbError):
+        ops.gather_bf_columns(torch.zeros((4, 8), dtype=torch.uint16, device=DEV),
+                              torch.zeros((0,), dtype=torch.int32, device=DEV))
