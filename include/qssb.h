@@ -34,6 +34,9 @@ extern "C" {
 /* Flags for qssb_object / qssb_loss_batch. */
 #define QSSB_FLAG_CHI_FP64 1      /* chi polynomial and its 2*pi reduction in FP64 */
 #define QSSB_FLAG_FULL_PLANE 2    /* evaluate every scan frequency; no +-q symmetry */
+#define QSSB_FLAG_QUADRATIC 4     /* qssb_loss_batch: every candidate has C30 == 0, so the
+                                     factorised quadratic-chi overlap applies (qssb_object
+                                     decides this itself from its host-side candidate) */
 
 /* Calibration shared by the object and loss entry points. Scalars follow
  * SSBEngine's cache (engine.py:784-848): wavelength in Angstrom, angles in

@@ -20,6 +20,7 @@ QSSB_ERR_UNSUPPORTED = -3
 QSSB_ERR_WORKSPACE = -4
 QSSB_FLAG_CHI_FP64 = 1
 QSSB_FLAG_FULL_PLANE = 2
+QSSB_FLAG_QUADRATIC = 4
 
 
 class Calibration(ctypes.Structure):

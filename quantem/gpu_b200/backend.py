@@ -32,7 +32,7 @@ import numpy as np
 import torch
 
 from . import ops
-from ._lib import QSSB_FLAG_CHI_FP64, Aberrations, Calibration
+from ._lib import QSSB_FLAG_CHI_FP64, QSSB_FLAG_QUADRATIC, Aberrations, Calibration
 from .calibration import (
     BFGeometry,
     bf_geometry,
@@ -151,9 +151,12 @@ class B200SSBBackend:
                 f"padding rule; got {scan_gpts}."
             )
         self.wavelength = electron_wavelength_angstrom(energy)
-        # (a3) exact u64 mean diffraction pattern on the GPU
-        sums, mean_dp = ops.mean_dp_u64(counts)
-        mean_host = mean_dp.cpu().numpy()
+        # (a3) exact u64 mean diffraction pattern on the GPU; the one host sync
+        # of preparation reads the 128 KB of sums back
+        sums_dev, _ = ops.mean_dp_u64(counts, want_mean=False)
+        sums_host = sums_dev.cpu().numpy().view(np.uint64).reshape(det_gpts)
+        n_frames = scan_gpts[0] * scan_gpts[1]
+        mean_host = ops.mean_from_sums(sums_host, n_frames)
         self._detected_radius_px = None
         if det_sampling is None:
             _, r = detect_bf_radius(mean_host)
@@ -173,22 +176,22 @@ class B200SSBBackend:
         self.bf_inds_col = sel.cols
         self.bf_center = sel.center
         self._bf_radius_selected = sel.radius
-        lin_host = sel.rows.astype(np.int64) * det_gpts[1] + sel.cols
-        self._bf_linear = torch.as_tensor(lin_host.astype(np.int32), device=self.device)
-        # (a6) gather + Hermitian scan FFT; dc exact from the integer sums
-        columns = ops.gather_bf_columns(counts, self._bf_linear)
-        self.G_qk = ops.scan_fft_half(columns, scan_gpts)
-        del columns
-        sums_host = sums.cpu().numpy().view(np.uint64).reshape(-1)
-        self.dc_value = complex(float(sums_host[lin_host].astype(np.float64).mean()), 0.0)
+        lin_host = (sel.rows.astype(np.int64) * det_gpts[1] + sel.cols).astype(np.int32)
+        self.dc_value = complex(float(sums_host.reshape(-1)[lin_host].astype(np.float64).mean()), 0.0)
         q_row, q_col = scan_frequencies(scan_gpts, self.scan_sampling)
         self._q_row_host, self._q_col_host = q_row, q_col
-        self._q_row = torch.as_tensor(q_row, device=self.device)
-        self._q_col = torch.as_tensor(q_col, device=self.device)
+        geo = bf_geometry(sel.rows, sel.cols, sel.center, det_gpts, self.sampling, self.wavelength,
+                          self.semiangle_cutoff, self.angular_sampling, self._rotation_angle_rad)
+        # one pinned upload: BF indices, geometry, scan frequencies
+        self._bf_linear, self._geom_dev, self._q_row, self._q_col = ops.STAGING.upload(
+            [lin_host, geo.stacked(), q_row, q_col], self.device)
+        self._geometry = geo
+        self._cached_rotation = self._rotation_angle_rad
+        # (a6) gather + Hermitian scan FFT; dc exact from the integer sums
+        columns = ops.gather_bf_columns(counts, self._bf_linear, validate=False)
+        self.G_qk = ops.scan_fft_half(columns, scan_gpts)
+        del columns
         self._workspace = ops.Workspace(self.device)
-        self._geometry: BFGeometry | None = None
-        self._geom_dev: torch.Tensor | None = None
-        self._cached_rotation: float | None = None
         self._subset_stack: list = []
         self._best_loss = float("inf")
         self._elapsed_optimize = 0.0
@@ -199,7 +202,6 @@ class B200SSBBackend:
         self._refine_nfev: int | None = None
         self._optuna_trials: list[dict] = []
         self.timings = {"prepare_s": time.perf_counter() - t0}
-        self.cache_rotation(self._rotation_angle_rad)
 
     # ------------------------------------------------------------ preparation
     def _pad_or_crop(self, counts: torch.Tensor) -> torch.Tensor:
@@ -215,7 +217,7 @@ class B200SSBBackend:
             counts = counts[r0:r0 + min(t, h), c0:c0 + min(t, w)].contiguous()
             h, w = int(counts.shape[0]), int(counts.shape[1])
         if h < t or w < t:
-            sums, _ = ops.mean_dp_u64(counts)
+            sums, _ = ops.mean_dp_u64(counts, want_mean=False)
             n = h * w
             fill = (sums.cpu().numpy().view(np.uint64).astype(np.float64) / n).astype(np.uint16)
             padded = torch.as_tensor(fill, device=self.device).expand(t, t, *fill.shape).contiguous()
@@ -249,6 +251,8 @@ class B200SSBBackend:
         c30 = np.zeros(n, np.float32) if c30 is None else np.broadcast_to(np.asarray(c30, np.float32), (n,))
         host = np.stack([c10, c12, phi12, c30], axis=1).astype(np.float32)
         return torch.as_tensor(host, device=self.device)
+
+
 
     def _require_loss_size(self) -> None:
         if self._scan_shape[0] not in LOSS_SCAN_SIZES:
@@ -301,8 +305,9 @@ class B200SSBBackend:
         """Phase-variance losses (float32 CUDA [n]) for a candidate batch."""
         self._require_loss_size()
         cands = self._candidates(C10, C12, phi12, C30)
+        flags = self._flags | (QSSB_FLAG_QUADRATIC if C30 is None or not np.any(np.asarray(C30)) else 0)
         losses, _ = ops.loss_batch(self.G_qk, self._geom_dev, self._q_row, self._q_col,
-                                   self._calibration(), cands, flags=self._flags,
+                                   self._calibration(), cands, flags=flags,
                                    workspace=self._workspace)
         return losses
 
@@ -314,7 +319,8 @@ class B200SSBBackend:
         self._require_loss_size()
         cands = self._candidates([C10], [C12], [phi12])
         losses, mp = ops.loss_batch(self.G_qk, self._geom_dev, self._q_row, self._q_col,
-                                    self._calibration(), cands, flags=self._flags,
+                                    self._calibration(), cands,
+                                    flags=self._flags | QSSB_FLAG_QUADRATIC,
                                     workspace=self._workspace, want_mean_phase=True)
         return mp[0], float(losses[0])
 

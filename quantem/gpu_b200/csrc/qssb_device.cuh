@@ -177,6 +177,10 @@ struct Probe {
     double semi_d, lam_d, ang_r_d, ang_c_d;
     double qval_r, qval_c;  // 1 / (R d): q = fftfreq index * qval
     int n_r, n_c;
+    // chi(u) = u^T M u for the quadratic (C10, C12) part; M symmetric
+    float mxx, mxy, myy;
+    double mxx_d, mxy_d, myy_d;
+    bool quadratic;   // C30 == 0: the factorised overlap applies
     double factor_d;  // FP64 copies for QSSB_FLAG_CHI_FP64
     double C10_d;
     double C12_d;
@@ -358,7 +362,96 @@ __host__ __device__ inline Probe make_probe_common(const qssb_calibration_t& cal
     p.cos2p_d = c2;
     p.sin2p_d = s2;
     p.c30_half_d = 0.5 * factor * (double)C30;
+    // M = (pi / lambda) lambda^2 [[C10 + C12 c2, C12 s2], [C12 s2, C10 - C12 c2]]
+    const double fl2 = factor * cal.wavelength_A * cal.wavelength_A;
+    p.mxx_d = fl2 * ((double)C10 + (double)C12 * c2);
+    p.mxy_d = fl2 * (double)C12 * s2;
+    p.myy_d = fl2 * ((double)C10 - (double)C12 * c2);
+    p.mxx = (float)p.mxx_d;
+    p.mxy = (float)p.mxy_d;
+    p.myy = (float)p.myy_d;
+    p.quadratic = (C30 == 0.0f);
     return p;
+}
+
+// Reduce an FP64 angle to [-pi, pi] and round to float32.
+__device__ __forceinline__ float reduce_angle(double a) {
+    return (float)(a - 6.283185307179586476925 * rint(a * 0.15915494309189533577));
+}
+
+// (cos Q(q), sin Q(q)), Q(q) = q^T M q, from the FP64 grid value of q.
+__device__ __forceinline__ float2 eq_value(int r, int c, const Probe& p) {
+    const double qx = fftfreq_d(r, p.n_r, p.qval_r);
+    const double qy = fftfreq_d(c, p.n_c, p.qval_c);
+    const double q = fma(p.mxx_d * qx, qx, fma(2.0 * p.mxy_d * qx, qy, p.myy_d * qy * qy));
+    float s, co;
+    sincosf(reduce_angle(q), &s, &co);
+    return make_float2(co, s);
+}
+
+// Per-BF constants of the factorised overlap: (u, v) = M k.
+struct BFQuad {
+    float kx, ky, kx_lo, ky_lo, ak, u, v;
+    double ud, vd;  // FP64 M k (QSSB_FLAG_CHI_FP64)
+};
+
+__device__ __forceinline__ BFQuad bf_quad(const float* __restrict__ geom, int n_bf, int b,
+                                          const Probe& p) {
+    BFQuad q;
+    q.kx = __ldg(geom + b);
+    q.ky = __ldg(geom + n_bf + b);
+    q.ak = __ldg(geom + 5 * n_bf + b);
+    q.kx_lo = __ldg(geom + 6 * n_bf + b);
+    q.ky_lo = __ldg(geom + 7 * n_bf + b);
+    q.u = fmaf(p.mxx, q.kx, p.mxy * q.ky);
+    q.v = fmaf(p.mxy, q.kx, p.myy * q.ky);
+    const double kx = (double)q.kx + (double)q.kx_lo;
+    const double ky = (double)q.ky + (double)q.ky_lo;
+    q.ud = fma(p.mxx_d, kx, p.mxy_d * ky);
+    q.vd = fma(p.mxy_d, kx, p.myy_d * ky);
+    return q;
+}
+
+// Factorised C = G conj(Gamma_hat) for quadratic chi (C10, C12). With
+// chi(u) = u^T M u: chi(q -+ k) = Q(q) -+ 2 q^T M k + Q(k), so
+// Gamma = A(k) e^{i theta} [(A(q-k) - A(q+k)) cos Q(q) - i (A(q-k) + A(q+k)) sin Q(q)],
+// theta = 2 q^T M k: one sincos per (b, q) and no polar geometry. The
+// normalisation threshold is applied to |Gamma|^2 as in the reference.
+template <bool CHI64>
+__device__ __forceinline__ float2 corrected_quad(float qx, float qy, int r, int c, float2 eq,
+                                                 const BFQuad& k, float2 g, const Probe& p) {
+    const float dxm = qx - k.kx, dym = qy - k.ky;
+    const float dxp = qx + k.kx, dyp = qy + k.ky;
+    const float r2m = fmaf(dxm, dxm, dym * dym);
+    const float r2p = fmaf(dxp, dxp, dyp * dyp);
+    float am = soft_aperture(dxm, dym, r2m, p);
+    float ap = soft_aperture(dxp, dyp, r2p, p);
+    if (fabsf(am - ap) < kApertureTie && (in_edge_band(r2m, p) || in_edge_band(r2p, p))) {
+        const double qx64 = fftfreq_d(r, p.n_r, p.qval_r);
+        const double qy64 = fftfreq_d(c, p.n_c, p.qval_c);
+        const double kx64 = (double)k.kx + (double)k.kx_lo;
+        const double ky64 = (double)k.ky + (double)k.ky_lo;
+        am = soft_aperture_fp64(qx64 - kx64, qy64 - ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
+        ap = soft_aperture_fp64(qx64 + kx64, qy64 + ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
+    }
+    if (am == 0.0f && ap == 0.0f) return make_float2(0.0f, 0.0f);  // Gamma == 0
+    const float dr = (am - ap) * eq.x;
+    const float di = -(am + ap) * eq.y;
+    float st, ct;
+    if constexpr (CHI64) {
+        const double qx64 = fftfreq_d(r, p.n_r, p.qval_r);
+        const double qy64 = fftfreq_d(c, p.n_c, p.qval_c);
+        __sincosf(reduce_angle(2.0 * fma(qx64, k.ud, qy64 * k.vd)), &st, &ct);
+    } else {
+        __sincosf(2.0f * fmaf(qx, k.u, qy * k.v), &st, &ct);
+    }
+    float gr = k.ak * fmaf(ct, dr, -st * di);
+    float gi = k.ak * fmaf(ct, di, st * dr);
+    const float m2 = fmaf(gr, gr, gi * gi);
+    const float inv = m2 > 1e-16f ? rsqrtf(m2) : 1e8f;
+    gr *= inv;
+    gi *= inv;
+    return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
 }
 
 }  // namespace qssb

@@ -30,18 +30,31 @@ struct LossSmem {
     static constexpr size_t bytes = sizeof(float2) * ((size_t)N * P + N);
 };
 
-template <int N, bool SYM, bool CHI64>
+// e^{-i Q(q)} for every scan frequency of every candidate (quadratic chi).
+template <int N>
+__global__ void k_eq_table(const qssb_aberrations_t* __restrict__ cands, qssb_calibration_t cal,
+                           float2* __restrict__ eq) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    const int cand = blockIdx.y;
+    if (idx >= N * N) return;
+    const qssb_aberrations_t ab = cands[cand];
+    const Probe p = make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
+    eq[(size_t)cand * N * N + idx] = eq_value(idx / N, idx % N, p);
+}
+
+template <int N, bool SYM, bool CHI64, bool QUAD>
 __global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments(
     const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
     const float* __restrict__ q_row, const float* __restrict__ q_col,
-    const qssb_aberrations_t* __restrict__ cands, qssb_calibration_t cal, int bf_per_chunk, int n_chunks,
-    float* __restrict__ part) {
+    const qssb_aberrations_t* __restrict__ cands, qssb_calibration_t cal,
+    const float2* __restrict__ eq_table, int bf_per_chunk, int n_chunks, float* __restrict__ part) {
     constexpr int H = N / 2 + 1;
     constexpr int P = LossSmem<N>::P;
     constexpr int CPW = N / kLossWarps;  // columns owned per warp
     constexpr int RPL = N / 32;          // rows owned per lane
     constexpr int NEVAL = SYM ? (N / 2 + 1) * N + (N / 2 - 1) : N * N;
     extern __shared__ float2 smem[];
+    __shared__ Probe sp;
     float2* plane = smem;
     float2* tw = smem + N * P;
     const int tid = threadIdx.x;
@@ -49,9 +62,14 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments(
     const int warp = tid >> 5;
     const int chunk = blockIdx.x;
     const int cand = blockIdx.y;
-    const qssb_aberrations_t ab = cands[cand];
-    const Probe p = make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
+    if (tid == 0) {
+        const qssb_aberrations_t ab = cands[cand];
+        sp = make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
+    }
     fill_twiddles<N>(tw, tid, kLossThreads);
+    __syncthreads();
+    const Probe& p = sp;
+    const float2* eqc = eq_table + (size_t)cand * N * N;
     float as[CPW][RPL], aq[CPW][RPL];
 #pragma unroll
     for (int i = 0; i < CPW; ++i)
@@ -63,12 +81,11 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments(
     const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
     for (int i = 0; i < nb; ++i) {
         const int b = b0 + i;
-        const float kx = __ldg(geom + b);
-        const float ky = __ldg(geom + n_bf + b);
-        const float kxlo = __ldg(geom + 6 * n_bf + b);
-        const float kylo = __ldg(geom + 7 * n_bf + b);
-        const float2 pk = probe_at_bf<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
-                                             __ldg(geom + 4 * n_bf + b), __ldg(geom + 5 * n_bf + b), p);
+        const BFQuad kq = bf_quad(geom, n_bf, b, p);
+        float2 pk = make_float2(0.0f, 0.0f);
+        if constexpr (!QUAD)
+            pk = probe_at_bf<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
+                                    __ldg(geom + 4 * n_bf + b), __ldg(geom + 5 * n_bf + b), p);
         const float2* gb = g + (size_t)b * N * H;
         // A) corrected spectrum into shared memory
         for (int e = tid; e < NEVAL; e += kLossThreads) {
@@ -88,8 +105,14 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments(
             } else {
                 gv = cconj(__ldg(gb + ((N - r) & (N - 1)) * H + (N - c)));
             }
-            float2 v = corrected<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c, kx, ky, kxlo, kylo,
-                                        pk, gv, p);
+            float2 v;
+            if constexpr (QUAD) {
+                v = corrected_quad<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c,
+                                          __ldg(eqc + r * N + c), kq, gv, p);
+            } else {
+                v = corrected<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c, kq.kx, kq.ky, kq.kx_lo,
+                                     kq.ky_lo, pk, gv, p);
+            }
             if (r == 0 && c == 0) v = dc;
             plane[r * P + c] = v;
             if (mirror) plane[(N - r) * P + ((N - c) & (N - 1))] = cneg_conj(v);
@@ -170,6 +193,7 @@ struct LossPlan {
     int n_chunks;
     size_t part_bytes;
     size_t var_bytes;
+    size_t eq_bytes;
 };
 
 // Deterministic: about 296 CTAs in total (two per B200 SM), at least one BF
@@ -184,10 +208,11 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand) {
     pl.part_bytes = sizeof(float) * 2 * (size_t)n * n * pl.n_chunks * n_cand;
     pl.part_bytes = (pl.part_bytes + 255) & ~(size_t)255;
     pl.var_bytes = sizeof(double) * (size_t)n * n * n_cand;
+    pl.eq_bytes = sizeof(float2) * (size_t)n * n * n_cand;
     return pl;
 }
 
-template <int N, bool SYM, bool CHI64>
+template <int N, bool SYM, bool CHI64, bool QUAD>
 static int launch_loss(const float* g_half, const float* geom, const float* q_row,
                        const float* q_col, const qssb_calibration_t& cal,
                        const qssb_aberrations_t* cands, int n_cand, char* ws, float* losses,
@@ -195,11 +220,16 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
     const LossPlan pl = plan_loss(N, cal.n_bf, n_cand);
     float* part = reinterpret_cast<float*>(ws);
     double* var = reinterpret_cast<double*>(ws + pl.part_bytes);
+    float2* eq = reinterpret_cast<float2*>(ws + pl.part_bytes + pl.var_bytes);
+    if (QUAD) {
+        k_eq_table<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(cands, cal, eq);
+        CUDA_TRY(cudaGetLastError());
+    }
     const size_t smem = LossSmem<N>::bytes;
-    CUDA_TRY(cudaFuncSetAttribute(k_loss_moments<N, SYM, CHI64>,
+    CUDA_TRY(cudaFuncSetAttribute(k_loss_moments<N, SYM, CHI64, QUAD>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_loss_moments<N, SYM, CHI64><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
-        reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal,
+    k_loss_moments<N, SYM, CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
+        reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal, eq,
         pl.bf_per_chunk, pl.n_chunks, part);
     CUDA_TRY(cudaGetLastError());
     k_loss_reduce<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(part, pl.n_chunks, cal.n_bf,
@@ -210,16 +240,28 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
     return QSSB_OK;
 }
 
+template <int N, bool QUAD>
+static int dispatch_loss_q(bool sym, bool chi64, const float* g_half, const float* geom,
+                           const float* q_row, const float* q_col, const qssb_calibration_t& cal,
+                           const qssb_aberrations_t* cands, int n_cand, char* ws, float* losses,
+                           float* mean_phase, cudaStream_t s) {
+    if (sym)
+        return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
+                     : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
+    return chi64 ? launch_loss<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
+                 : launch_loss<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
+}
+
+// Candidates live on the device, so the path is chosen by a flag: the
+// general (C30) path unless QSSB_FLAG_QUADRATIC promises C30 == 0 for all.
 template <int N>
-static int dispatch_loss(bool sym, bool chi64, const float* g_half, const float* geom,
+static int dispatch_loss(bool sym, bool chi64, bool quad, const float* g_half, const float* geom,
                          const float* q_row, const float* q_col, const qssb_calibration_t& cal,
                          const qssb_aberrations_t* cands, int n_cand, char* ws, float* losses,
                          float* mean_phase, cudaStream_t s) {
-    if (sym)
-        return chi64 ? launch_loss<N, true, true>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
-                     : launch_loss<N, true, false>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
-    return chi64 ? launch_loss<N, false, true>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
-                 : launch_loss<N, false, false>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
+    if (quad)
+        return dispatch_loss_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
+    return dispatch_loss_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
 }
 
 }  // namespace qssb
@@ -237,7 +279,7 @@ extern "C" int qssb_loss_workspace_bytes(const qssb_calibration_t* cal, int32_t 
     if (n != 64 && n != 128)
         return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64 or 128");
     const LossPlan pl = plan_loss(n, cal->n_bf, n_cand);
-    *bytes = pl.part_bytes + pl.var_bytes;
+    *bytes = pl.part_bytes + pl.var_bytes + pl.eq_bytes;
     return QSSB_OK;
 }
 
@@ -259,11 +301,12 @@ extern "C" int qssb_loss_batch(const float* g_half, const float* bf_geom, const 
         return set_error(QSSB_ERR_INVALID, "qssb_loss_batch: workspace must be 256-byte aligned");
     const bool sym = !(flags & QSSB_FLAG_FULL_PLANE);
     const bool chi64 = (flags & QSSB_FLAG_CHI_FP64) != 0;
+    const bool quad = (flags & QSSB_FLAG_QUADRATIC) != 0;
     cudaStream_t s = (cudaStream_t)stream;
     char* ws = static_cast<char*>(workspace);
     switch (cal->scan_rows) {
-        case 64: return dispatch_loss<64>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, ws, losses, mean_phase, s);
-        case 128: return dispatch_loss<128>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, ws, losses, mean_phase, s);
+        case 64: return dispatch_loss<64>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, ws, losses, mean_phase, s);
+        case 128: return dispatch_loss<128>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, ws, losses, mean_phase, s);
         default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64 or 128");
     }
 }

@@ -71,18 +71,15 @@ __host__ __device__ constexpr int n_eval_q() {
     return SYM ? N * (N / 2 + 1) + N / 2 - 1 : N * N;
 }
 
-template <int N, bool SYM, bool CHI64>
+template <int N, bool SYM, bool CHI64, bool QUAD>
 __global__ void __launch_bounds__(kTrotterThreads) k_trotter_partial(
     const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
     const float* __restrict__ q_row, const float* __restrict__ q_col, Probe p, int bf_per_chunk,
     float2* __restrict__ partial) {
     constexpr int H = N / 2 + 1;
     constexpr int NQ = n_eval_q<N, SYM>();
-    __shared__ float s_kx[kMaxBfChunk];
-    __shared__ float s_ky[kMaxBfChunk];
-    __shared__ float s_kxlo[kMaxBfChunk];
-    __shared__ float s_kylo[kMaxBfChunk];
-    __shared__ float2 s_pk[kMaxBfChunk];
+    __shared__ BFQuad s_bf[kMaxBfChunk];
+    __shared__ float2 s_pk[QUAD ? 1 : kMaxBfChunk];
     const int tid = threadIdx.x;
     const int chunk = blockIdx.y;
     const int b0 = chunk * bf_per_chunk;
@@ -90,12 +87,10 @@ __global__ void __launch_bounds__(kTrotterThreads) k_trotter_partial(
     if (nb > bf_per_chunk) nb = bf_per_chunk;
     for (int i = tid; i < nb; i += kTrotterThreads) {
         const int b = b0 + i;
-        s_kx[i] = __ldg(geom + b);
-        s_ky[i] = __ldg(geom + n_bf + b);
-        s_kxlo[i] = __ldg(geom + 6 * n_bf + b);
-        s_kylo[i] = __ldg(geom + 7 * n_bf + b);
-        s_pk[i] = probe_at_bf<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
-                                     __ldg(geom + 4 * n_bf + b), __ldg(geom + 5 * n_bf + b), p);
+        s_bf[i] = bf_quad(geom, n_bf, b, p);
+        if constexpr (!QUAD)
+            s_pk[i] = probe_at_bf<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
+                                         __ldg(geom + 4 * n_bf + b), __ldg(geom + 5 * n_bf + b), p);
     }
     __syncthreads();
     const int qi = blockIdx.x * kTrotterThreads + tid;
@@ -103,14 +98,20 @@ __global__ void __launch_bounds__(kTrotterThreads) k_trotter_partial(
     const QMap m = qmap<N, SYM>(qi);
     const float qx = __ldg(q_row + m.r);
     const float qy = __ldg(q_col + m.c);
+    const float2 eq = QUAD ? eq_value(m.r, m.c, p) : make_float2(1.0f, 0.0f);
     const float2* gp = g + (size_t)b0 * N * H + m.gr * H + m.gc;
     float sr = 0.f, si = 0.f, er = 0.f, ei = 0.f;  // Kahan sums and compensations
 #pragma unroll 2
     for (int i = 0; i < nb; ++i) {
         float2 gv = __ldg(gp + (size_t)i * N * H);
         if (m.conj) gv.y = -gv.y;
-        const float2 v = corrected<CHI64>(qx, qy, m.r, m.c, s_kx[i], s_ky[i], s_kxlo[i], s_kylo[i],
-                                          s_pk[i], gv, p);
+        float2 v;
+        if constexpr (QUAD) {
+            v = corrected_quad<CHI64>(qx, qy, m.r, m.c, eq, s_bf[i], gv, p);
+        } else {
+            const BFQuad& k = s_bf[i];
+            v = corrected<CHI64>(qx, qy, m.r, m.c, k.kx, k.ky, k.kx_lo, k.ky_lo, s_pk[i], gv, p);
+        }
         const float yr = v.x - er;
         const float tr = sr + yr;
         er = (tr - sr) - yr;
@@ -248,7 +249,7 @@ int validate_calibration(const qssb_calibration_t* cal, const char* who) {
     return QSSB_OK;
 }
 
-template <int N, bool SYM, bool CHI64>
+template <int N, bool SYM, bool CHI64, bool QUAD>
 static int launch_object(const float* g_half, const float* geom, const float* q_row,
                          const float* q_col, const qssb_calibration_t& cal, const Probe& p,
                          char* ws, float* object, float* phase, cudaStream_t s) {
@@ -256,7 +257,7 @@ static int launch_object(const float* g_half, const float* geom, const float* q_
     float2* partial = reinterpret_cast<float2*>(ws);
     float2* plane = reinterpret_cast<float2*>(ws + pl.partial_bytes);
     const dim3 grid((pl.n_q + kTrotterThreads - 1) / kTrotterThreads, pl.n_chunks);
-    k_trotter_partial<N, SYM, CHI64><<<grid, kTrotterThreads, 0, s>>>(
+    k_trotter_partial<N, SYM, CHI64, QUAD><<<grid, kTrotterThreads, 0, s>>>(
         reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, p, pl.bf_per_chunk,
         partial);
     CUDA_TRY(cudaGetLastError());
@@ -270,16 +271,25 @@ static int launch_object(const float* g_half, const float* geom, const float* q_
     return QSSB_OK;
 }
 
+template <int N, bool QUAD>
+static int dispatch_object_q(bool sym, bool chi64, const float* g_half, const float* geom,
+                             const float* q_row, const float* q_col, const qssb_calibration_t& cal,
+                             const Probe& p, char* ws, float* object, float* phase, cudaStream_t s) {
+    if (sym) {
+        return chi64 ? launch_object<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s)
+                     : launch_object<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s);
+    }
+    return chi64 ? launch_object<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s)
+                 : launch_object<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s);
+}
+
 template <int N>
 static int dispatch_object(bool sym, bool chi64, const float* g_half, const float* geom,
                            const float* q_row, const float* q_col, const qssb_calibration_t& cal,
                            const Probe& p, char* ws, float* object, float* phase, cudaStream_t s) {
-    if (sym) {
-        return chi64 ? launch_object<N, true, true>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s)
-                     : launch_object<N, true, false>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s);
-    }
-    return chi64 ? launch_object<N, false, true>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s)
-                 : launch_object<N, false, false>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s);
+    if (p.quadratic)
+        return dispatch_object_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, p, ws, object, phase, s);
+    return dispatch_object_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, p, ws, object, phase, s);
 }
 
 }  // namespace qssb

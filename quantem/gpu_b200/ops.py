@@ -76,6 +76,49 @@ def _ptr(t: torch.Tensor | None) -> ctypes.c_void_p:
     return ctypes.c_void_p(0 if t is None else t.data_ptr())
 
 
+class PinnedStaging:
+    """A reusable pinned host buffer for batching small host->device uploads."""
+
+    def __init__(self):
+        self._buf: torch.Tensor | None = None
+
+    def upload(self, arrays, device: torch.device) -> list[torch.Tensor]:
+        """Copy numpy arrays to ``device`` with one pinned H2D transfer.
+
+        Returns device tensors (views into one allocation) with the arrays'
+        dtypes and shapes; each array starts on a 256-byte boundary.
+        """
+        import numpy as np
+
+        offsets, total = [], 0
+        for a in arrays:
+            offsets.append(total)
+            total += (a.nbytes + 255) & ~255
+        self.wait()  # the previous upload must have left the pinned buffer
+        if self._buf is None or self._buf.numel() < total:
+            self._buf = torch.empty(max(total, 1 << 16), dtype=torch.uint8, pin_memory=True)
+        host = self._buf.numpy()
+        for a, off in zip(arrays, offsets):
+            host[off:off + a.nbytes] = np.ascontiguousarray(a).view(np.uint8).reshape(-1)
+        dev = self._buf[:total].to(device, non_blocking=True)
+        out = []
+        for a, off in zip(arrays, offsets):
+            t = dev[off:off + a.nbytes].view(getattr(torch, str(a.dtype)))
+            out.append(t.reshape(a.shape))
+        # the pinned buffer may be rewritten only after this copy has run
+        self._event = torch.cuda.Event()
+        self._event.record(torch.cuda.current_stream(device))
+        return out
+
+    def wait(self) -> None:
+        ev = getattr(self, "_event", None)
+        if ev is not None:
+            ev.synchronize()
+
+
+STAGING = PinnedStaging()
+
+
 class Workspace:
     """A reusable, growing device scratch buffer (256-byte aligned)."""
 
@@ -92,29 +135,46 @@ class Workspace:
         self._buf = None
 
 
-def mean_dp_u64(counts: torch.Tensor) -> tuple[torch.Tensor, torch.Tensor]:
+def mean_dp_u64(counts: torch.Tensor, want_mean: bool = True
+                ) -> tuple[torch.Tensor, torch.Tensor | None]:
     """Exact u64 detector sums and float32 mean DP of ``counts[..., K0, K1]``.
 
-    Returns (sums as int64 [K0, K1] holding the u64 values, mean_dp f32 [K0, K1]).
+    Returns (sums as int64 [K0, K1] holding the u64 values, mean_dp f32 [K0, K1]
+    or None when ``want_mean`` is False).
     """
     _require_cuda(counts, "counts", torch.uint16)
     k0, k1 = int(counts.shape[-2]), int(counts.shape[-1])
     n_frames = counts.numel() // (k0 * k1)
     sums = torch.empty((k0, k1), dtype=torch.int64, device=counts.device)
-    mean = torch.empty((k0, k1), dtype=torch.float32, device=counts.device)
+    mean = torch.empty((k0, k1), dtype=torch.float32, device=counts.device) if want_mean else None
     _call("qssb_mean_dp_u64", counts.device, _ptr(counts), n_frames, k0 * k1, _ptr(sums),
           _ptr(mean), _stream(counts))
+    if not want_mean:
+        global LAUNCH_COUNT
+        LAUNCH_COUNT -= 1  # the mean kernel is skipped
     return sums, mean
 
 
-def gather_bf_columns(counts: torch.Tensor, bf_linear: torch.Tensor) -> torch.Tensor:
-    """columns[b, f] = counts[f, bf_linear[b]] (u16, BF-major)."""
+def mean_from_sums(sums_u64, n_frames: int):
+    """float32(sum) / n_frames with IEEE rounding: the kernel's mean, on the host."""
+    import numpy as np
+
+    return np.asarray(sums_u64, dtype=np.uint64).astype(np.float32) / np.float32(n_frames)
+
+
+def gather_bf_columns(counts: torch.Tensor, bf_linear: torch.Tensor, validate: bool = True
+                      ) -> torch.Tensor:
+    """columns[b, f] = counts[f, bf_linear[b]] (u16, BF-major).
+
+    ``validate`` checks the index range on the device (two host syncs); the
+    backend passes indices it built itself and skips it.
+    """
     _require_cuda(counts, "counts", torch.uint16)
     _require_cuda(bf_linear, "bf_linear", torch.int32)
     k0, k1 = int(counts.shape[-2]), int(counts.shape[-1])
     n_frames = counts.numel() // (k0 * k1)
     n_bf = int(bf_linear.numel())
-    if n_bf and (int(bf_linear.min()) < 0 or int(bf_linear.max()) >= k0 * k1):
+    if validate and n_bf and (int(bf_linear.min()) < 0 or int(bf_linear.max()) >= k0 * k1):
         raise ValueError("bf_linear indices must lie in [0, K0*K1)")
     out = torch.empty((n_bf, n_frames), dtype=torch.uint16, device=counts.device)
     _call("qssb_gather_bf_columns", counts.device, _ptr(counts), n_frames, k0 * k1,

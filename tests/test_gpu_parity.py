@@ -18,6 +18,7 @@ from quantem.gpu_b200 import ops
 from quantem.gpu_b200._lib import (
     QSSB_FLAG_CHI_FP64,
     QSSB_FLAG_FULL_PLANE,
+    QSSB_FLAG_QUADRATIC,
     Aberrations,
     Calibration,
     QssbError,
@@ -166,7 +167,8 @@ CANDS = [(-120.0, 55.0, math.radians(17.0)), (-80.0, 30.0, math.radians(-5.0)),
          (20.0, 40.0, math.radians(11.0)), (100.0, 10.0, math.radians(43.0))]
 
 
-@pytest.mark.parametrize("flags", [0, QSSB_FLAG_FULL_PLANE])
+@pytest.mark.parametrize("flags", [0, QSSB_FLAG_FULL_PLANE, QSSB_FLAG_QUADRATIC,
+                                   QSSB_FLAG_QUADRATIC | QSSB_FLAG_CHI_FP64])
 def test_loss_batch_matches_oracle(disk_case, flags):
     """variance_loss_batch vs the explicit reference (test_ssb_cuda_128.py:726-744)."""
     prep, cal, d = disk_case
