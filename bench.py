@@ -325,6 +325,25 @@ def run_b200(args, world, rank, local) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_profile_once(local: int) -> None:
+    """One cold reconstruction, one warm object, one loss and one 64-candidate
+    loss batch on the 128^4 workload, untimed: the launch sequence the ncu
+    summaries under profiles/ are captured from."""
+    from quantem.gpu_b200 import B200SSBBackend
+    from quantem.gpu_b200.synthetic import CONFIGS, generate
+
+    dev = torch.device("cuda", local)
+    counts = generate(CONFIGS[SPEC_NAME], device=dev).counts
+    torch.cuda.synchronize(dev)
+    be = B200SSBBackend(counts, device=dev, **KW)
+    be.object_and_phase(10.0, 5.0, 0.1)
+    loss = be.variance_loss(10.0, 5.0, 0.1)
+    losses = be.variance_loss_batch(np.linspace(-50.0, 50.0, 64), 0.0, 0.0)
+    torch.cuda.synchronize(dev)
+    print(json.dumps({"profile_once": True, "n_bf": be.num_bf, "loss": loss,
+                      "loss_batch0": float(losses[0])}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -333,10 +352,14 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-oracle", action="store_true")
+    ap.add_argument("--profile-once", action="store_true",
+                    help="run the untimed launch sequence used for ncu captures")
     args = ap.parse_args()
     world, rank, local = _dist()
     try:
-        if args.impl == "reference":
+        if args.profile_once:
+            run_profile_once(local)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
             run_b200(args, world, rank, local)
