@@ -117,6 +117,33 @@ int qssb_object(const float* g_half, const float* bf_geom, const float* q_row,
                 const qssb_aberrations_t* ab, int32_t flags, void* workspace,
                 size_t workspace_bytes, float* object, float* phase, void* stream);
 
+/* Capacity of the fixed device scratch used by qssb_object_noalloc. */
+#define QSSB_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* qssb_object without a workspace argument and without allocating: for
+ * callers that cannot allocate device memory where they call us - a host
+ * application whose own memory pool already owns the whole device, a
+ * real-time acquisition loop that must not enter the CUDA allocator (an
+ * allocation can synchronise the device and stall the stream), or a plugin
+ * host that forbids third-party allocations. No counterpart in the reference
+ * (its CuPy engine always allocates through CuPy's memory pool).
+ *
+ * The scratch (partial Fourier sums and the spectrum plane) is one
+ * QSSB_NOALLOC_SCRATCH_BYTES (16 MiB) array inside this library; every GPU
+ * that loads the library holds it until the process exits. Requests whose
+ * qssb_object_workspace_bytes exceed it fail with QSSB_ERR_WORKSPACE (up to
+ * 63488 BF pixels fit at 128^2 scans, 15616 at 256^2).
+ * The first call on each device looks up the array's device address; make
+ * that first call before any stream capture. All calls share the one array:
+ * calls whose work overlaps on the GPU (other streams, other host threads)
+ * race and corrupt each other's results, so serialise them. Each call writes
+ * every scratch byte it reads, so nothing has to be cleared between calls.
+ * Arguments and results are those of qssb_object. */
+int qssb_object_noalloc(const float* g_half, const float* bf_geom, const float* q_row,
+                        const float* q_col, const qssb_calibration_t* cal,
+                        const qssb_aberrations_t* ab, int32_t flags, float* object,
+                        float* phase, void* stream);
+
 /* Workspace bytes needed by qssb_loss_batch for n_cand candidates. */
 int qssb_loss_workspace_bytes(const qssb_calibration_t* cal, int32_t n_cand, int32_t flags,
                               size_t* bytes);

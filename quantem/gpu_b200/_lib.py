@@ -21,6 +21,7 @@ QSSB_ERR_WORKSPACE = -4
 QSSB_FLAG_CHI_FP64 = 1
 QSSB_FLAG_FULL_PLANE = 2
 QSSB_FLAG_QUADRATIC = 4
+QSSB_NOALLOC_SCRATCH_BYTES = 16 << 20
 
 
 class Calibration(ctypes.Structure):
@@ -73,6 +74,8 @@ SIGNATURES = {
     "qssb_object": (ctypes.c_int, [
         _P, _P, _P, _P, ctypes.POINTER(Calibration), ctypes.POINTER(Aberrations), _I32, _P, _SZ,
         _P, _P, _P]),
+    "qssb_object_noalloc": (ctypes.c_int, [
+        _P, _P, _P, _P, ctypes.POINTER(Calibration), ctypes.POINTER(Aberrations), _I32, _P, _P, _P]),
     "qssb_loss_workspace_bytes": (
         ctypes.c_int, [ctypes.POINTER(Calibration), _I32, _I32, ctypes.POINTER(_SZ)]),
     "qssb_loss_batch": (ctypes.c_int, [

@@ -19,6 +19,8 @@
 // fill, DC, 1/B) -> k_ifft_rows -> k_ifft_cols_phase (1/N^2, atan2).
 #include <math.h>
 
+#include <mutex>
+
 #include "qssb_internal.h"
 
 namespace qssb {
@@ -336,4 +338,50 @@ extern "C" int qssb_object(const float* g_half, const float* bf_geom, const floa
         case 256: return dispatch_object<256>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, ws, object, phase, s);
         default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_object: scan size must be 64, 128 or 256");
     }
+}
+
+// ---------------------------------------------------------------------------
+// qssb_object_noalloc: the same launch sequence with its scratch in a fixed
+// file-scope device array (see include/qssb.h for the callers it serves and
+// the sharing rules). The host must not pass the array's name to a kernel:
+// in host code it is a stand-in, not a device address. Its device address is
+// looked up once per device with cudaGetSymbolAddress and cached.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[QSSB_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_addr[kMaxDevices] = {nullptr};
+}  // namespace
+
+extern "C" int qssb_object_noalloc(const float* g_half, const float* bf_geom, const float* q_row,
+                                   const float* q_col, const qssb_calibration_t* cal,
+                                   const qssb_aberrations_t* ab, int32_t flags, float* object,
+                                   float* phase, void* stream) {
+    int rc = validate_calibration(cal, "qssb_object_noalloc: null calibration");
+    if (rc) return rc;
+    size_t need = 0;
+    rc = qssb_object_workspace_bytes(cal, flags, &need);
+    if (rc) return rc;
+    if (need > (size_t)QSSB_NOALLOC_SCRATCH_BYTES)
+        return set_error(QSSB_ERR_WORKSPACE,
+                         "qssb_object_noalloc: this scan size and BF count need more than the "
+                         "16 MiB fixed scratch; use qssb_object with a caller workspace");
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices)
+        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_object_noalloc: device ordinal out of range");
+    void* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (g_noalloc_addr[dev] == nullptr) {
+            void* addr = nullptr;
+            const cudaError_t err = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+            if (err != cudaSuccess) return set_cuda_error(err, "qssb_object_noalloc: cudaGetSymbolAddress");
+            g_noalloc_addr[dev] = addr;
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    return qssb_object(g_half, bf_geom, q_row, q_col, cal, ab, flags, scratch,
+                       (size_t)QSSB_NOALLOC_SCRATCH_BYTES, object, phase, stream);
 }
