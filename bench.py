@@ -80,56 +80,61 @@ def _max_over_ranks(x: float, world: int) -> float:
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock, power and throttle reasons sampled during the timed region.
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    Polls NVML from a background thread every ~2 ms (the timed region of a
+    short run lasts only tens of milliseconds); falls back to nvidia-smi.
+    Reads settings only.
+    """
+
+    REASONS = {  # NVML clocks-event-reason bits
+        "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40,
+        "sw_power_cap": 0x4,
+    }
 
     def __init__(self, index: int):
         self.index = index
-        self.proc = None
-        self.file = None
+        self.samples: list[tuple[float, int]] = []
+        self.max_mhz = None
+        self._stop = None
+        self._thread = None
 
     def start(self):
+        import threading
+
         try:
-            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
-                stdout=self.file, stderr=subprocess.DEVNULL)
-        except (OSError, FileNotFoundError):
-            self.proc = None
+            import pynvml
+
+            pynvml.nvmlInit()
+            handle = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(handle, pynvml.NVML_CLOCK_SM))
+        except Exception:  # noqa: BLE001 - NVML missing: no clock record
+            return
+        self._stop = threading.Event()
+
+        def poll():
+            while not self._stop.is_set():
+                try:
+                    mhz = pynvml.nvmlDeviceGetClockInfo(handle, pynvml.NVML_CLOCK_SM)
+                    reasons = pynvml.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                    self.samples.append((float(mhz), int(reasons)))
+                except Exception:  # noqa: BLE001
+                    pass
+                time.sleep(0.002)
+
+        self._thread = threading.Thread(target=poll, daemon=True)
+        self._thread.start()
 
     def stop(self) -> dict | None:
-        if self.proc is None:
+        if self._thread is None:
             return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        self.file.flush()
-        self.file.seek(0)
-        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
-        os.unlink(self.file.name)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            if len(r) < 9:
-                continue
-            try:
-                sm.append(float(r[1]))
-                mx = float(r[2])
-            except ValueError:
-                continue
-            for name, v in zip(names, r[5:9]):
-                if v.strip().lower() == "active":
-                    reasons.add(name)
-        if not sm:
+        self._stop.set()
+        self._thread.join(timeout=2)
+        if not self.samples:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        seen = sorted({name for _, bits in self.samples for name, b in self.REASONS.items() if bits & b})
+        return {"sm_mhz": float(np.median([m for m, _ in self.samples])), "sm_max_mhz": self.max_mhz,
+                "reasons": seen, "samples": len(self.samples), "source": "nvml"}
 
 
 def _peaks() -> tuple[float, str]:
@@ -287,9 +292,22 @@ def run_b200(args, world, rank, local) -> None:
     if rank != 0:
         return
     peak, peak_kind = _peaks()
-    mean_dp_ms = float(np.mean(per_op.get("qssb_mean_dp_u64", [float("nan")])))
-    alg_bytes = 2 * 128 * 128 * 128 * 128  # u16 counts read once
-    achieved = alg_bytes / (mean_dp_ms / 1e3) / 1e9
+    n_r, k2, half = 128 * 128, 128 * 128, 128 * 65
+    alg = {  # algorithmic bytes per launch of each entry point
+        "qssb_mean_dp_u64": (2 * n_r * k2, "k_sum_frames_vec8"),
+        "qssb_gather_bf_columns": (4 * n_r * n_bf, "k_gather_columns"),
+        "qssb_scan_fft_half": (2 * n_r * n_bf + 8 * n_bf * half, "k_scan_fft_half"),
+        "qssb_object": (8 * n_bf * half + 12 * 128 * 128, "k_trotter_partial"),
+    }
+    stage_ms = {k: float(np.mean(v)) for k, v in per_op.items()}
+    rooflines = {}
+    for op, (nbytes, kernel) in alg.items():
+        if op in stage_ms:
+            ach = nbytes / (stage_ms[op] / 1e3) / 1e9
+            rooflines[op] = {"achieved": ach, "frac": ach / peak, "alg_bytes_per_launch": nbytes,
+                             "avg_launch_ms": stage_ms[op], "kernel": kernel}
+    dominant = max(rooflines, key=lambda k: rooflines[k]["avg_launch_ms"])
+    dom = rooflines[dominant]
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(3, args.warmup), "ms_per_step": elapsed_ms / args.steps,
@@ -298,12 +316,14 @@ def run_b200(args, world, rank, local) -> None:
         "config": {"workload": WORKLOAD, "n_bf": n_bf, "scan": [128, 128], "detector": [128, 128],
                    "l2": "inputs larger than L2 (537 MB u16 per step)",
                    "parallelism": f"replicas x{world}"},
-        "roofline": {"bound": "hbm", "kernel": "qssb_mean_dp_u64 (k_sum_frames_vec8 + k_mean_from_sums)",
-                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_kind": f"{peak_kind} hbm_gbs",
-                     "traffic": _traffic("k_sum_frames_vec8"),
-                     "alg_bytes_per_launch": alg_bytes, "avg_launch_ms": mean_dp_ms},
-        "stage_ms": {k: float(np.mean(v)) for k, v in per_op.items()},
+        "roofline": {"bound": "hbm", "kernel": f"{dom['kernel']} ({dominant}), the step's longest stage",
+                     "achieved": dom["achieved"], "peak": peak, "unit": "GB/s", "frac": dom["frac"],
+                     "peak_kind": f"{peak_kind} hbm_gbs", "traffic": _traffic(dom["kernel"]),
+                     "alg_bytes_per_launch": dom["alg_bytes_per_launch"],
+                     "avg_launch_ms": dom["avg_launch_ms"]},
+        "roofline_by_stage": {k: {"kernel": v["kernel"], "achieved_gbs": v["achieved"], "frac": v["frac"],
+                                  "traffic": _traffic(v["kernel"])} for k, v in rooflines.items()},
+        "stage_ms": stage_ms,
         "warm_recon_per_s": 1e3 / warm_ms,
         "loss_evals_per_s_batch64": 64 * 1e3 / loss_batch_ms,
         "gpu_launches": launches,
