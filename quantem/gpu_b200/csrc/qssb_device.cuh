@@ -136,6 +136,80 @@ __device__ __forceinline__ void stockham_stage(float2* x, int stride, const floa
     __syncwarp();
 }
 
+// 16-point DFT in registers (natural order in and out): 4 x 4 with the
+// W16 twiddles between the two radix-4 passes.
+template <int DIR>
+__device__ __forceinline__ void dft16(float2* x) {
+    const float c1 = 0.92387953251128675613f;  // cos(pi/8)
+    const float s1 = 0.38268343236508977173f;  // sin(pi/8)
+    const float h = 0.70710678118654752440f;
+    float2 y[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        float2 t[4] = {x[a], x[a + 4], x[a + 8], x[a + 12]};
+        dft4<DIR>(t);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) y[a][c] = t[c];
+    }
+    // W16^m = (cos(2 pi m / 16), DIR sin(2 pi m / 16)), m = a * c
+    y[1][1] = cmul(y[1][1], make_float2(c1, DIR * s1));   // m = 1
+    y[1][2] = cmul(y[1][2], make_float2(h, DIR * h));     // m = 2
+    y[1][3] = cmul(y[1][3], make_float2(s1, DIR * c1));   // m = 3
+    y[2][1] = cmul(y[2][1], make_float2(h, DIR * h));     // m = 2
+    y[2][2] = mul_dir_i<DIR>(y[2][2]);                    // m = 4
+    y[2][3] = cmul(y[2][3], make_float2(-h, DIR * h));    // m = 6
+    y[3][1] = cmul(y[3][1], make_float2(s1, DIR * c1));   // m = 3
+    y[3][2] = cmul(y[3][2], make_float2(-h, DIR * h));    // m = 6
+    y[3][3] = cmul(y[3][3], make_float2(-c1, -DIR * s1)); // m = 9
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float2 t[4] = {y[0][c], y[1][c], y[2][c], y[3][c]};
+        dft4<DIR>(t);
+#pragma unroll
+        for (int d = 0; d < 4; ++d) x[c + 4 * d] = t[d];
+    }
+}
+
+// A 128-point FFT by a group of 8 lanes (sub-lane s), 16 values per lane:
+// four-step 128 = 16 x 8. In: v[n1] = x[s + 8 n1]. DFT-16 over n1 in
+// registers, twiddle W128^(s k1), transpose through the group's scratch T
+// (16 rows of pitch 9, conflict-free for two groups per half-warp when the
+// groups' T bases differ by 8 mod 16 float2), DFT-8 over s for k1 = s and
+// s + 8. Out: v[t] = X[fft128_g8_index(s, t)] = X[s + 8 (t / 8) + 16 (t % 8)].
+// The 8 lanes of a group must belong to one warp; all 32 lanes call it.
+constexpr int kG8Pitch = 9;
+constexpr int kG8Scratch = 16 * kG8Pitch + 8;  // float2 per group (152)
+
+__device__ __forceinline__ int fft128_g8_index(int s, int t) { return s + 8 * (t >> 3) + 16 * (t & 7); }
+
+template <int DIR>
+__device__ __forceinline__ void fft128_g8(float2 (&v)[16], float2* T, int s, const float2* tw) {
+    dft16<DIR>(v);
+#pragma unroll
+    for (int k1 = 1; k1 < 16; ++k1) {
+        float2 w = tw[s * k1];
+        if (DIR > 0) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < 16; ++k1) T[k1 * kG8Pitch + s] = v[k1];
+    __syncwarp();
+    float2 u0[8], u1[8];
+#pragma unroll
+    for (int n2 = 0; n2 < 8; ++n2) {
+        u0[n2] = T[s * kG8Pitch + n2];
+        u1[n2] = T[(s + 8) * kG8Pitch + n2];
+    }
+    __syncwarp();
+    dft8<DIR>(u0);
+    dft8<DIR>(u1);
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) {
+        v[k2] = u0[k2];
+        v[8 + k2] = u1[k2];
+    }
+}
+
 // Whole line FFT of length N (natural order in, natural order out).
 template <int N, int DIR>
 __device__ __forceinline__ void line_fft(float2* x, int stride, const float2* tw, int lane) {

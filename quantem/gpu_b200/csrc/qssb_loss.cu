@@ -150,10 +150,177 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments(
     }
 }
 
+// ------------------------------------------------------------ N = 128 path
+// One CTA (16 warps = 64 groups of 8 lanes) per (BF chunk, candidate). Per BF:
+//  A) C_b on rows 0..64 (all columns) into Hp, C_b(-r, 64) for r = 1..63;
+//     then delta_r = conj(C(r,64)) + C(-r,64), the Nyquist-column deviation
+//     from C(-q) = -conj(C(q));
+//  B) row IFFTs of rows 0..64 only: after them row -r is
+//     -conj(row r) + delta_r (-1)^x, so the lower half is never stored;
+//  C) column IFFTs of all 128 columns, reading rows 65..127 through that
+//     relation; atan2 of each output, sum in registers, sum of squares in
+//     shared memory (each pixel owned by one lane for the whole launch).
+// Row/column -> group maps keep the two groups of a half-warp 8 apart mod 16
+// in bank space (conflict-free 8-byte accesses) and the four groups of a
+// warp 8 apart mod 32 (conflict-free 4-byte accesses to the squares).
+constexpr int kL128P = 129;  // Hp and squares pitch
+struct Loss128Smem {
+    static constexpr size_t hp = sizeof(float2) * 65 * kL128P;
+    static constexpr size_t t = sizeof(float2) * 64 * kG8Scratch;
+    static constexpr size_t sq = sizeof(float) * 128 * kL128P;
+    static constexpr size_t misc = sizeof(float2) * (128 + 64 + 64);  // tw, cneg, delta
+    static constexpr size_t bytes = hp + t + sq + misc;
+};
+
+template <bool CHI64, bool QUAD>
+__global__ void __launch_bounds__(512, 1) k_loss_moments128(
+    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
+    const float* __restrict__ q_row, const float* __restrict__ q_col,
+    const qssb_aberrations_t* __restrict__ cands, qssb_calibration_t cal,
+    const float2* __restrict__ eq_table, int bf_per_chunk, int n_chunks, float* __restrict__ part) {
+    constexpr int N = 128;
+    constexpr int H = N / 2 + 1;
+    extern __shared__ float4 smem4[];
+    char* base = reinterpret_cast<char*>(smem4);
+    float2* Hp = reinterpret_cast<float2*>(base);
+    float2* T = reinterpret_cast<float2*>(base + Loss128Smem::hp);
+    float* sq = reinterpret_cast<float*>(base + Loss128Smem::hp + Loss128Smem::t);
+    float2* tw = reinterpret_cast<float2*>(base + Loss128Smem::hp + Loss128Smem::t + Loss128Smem::sq);
+    float2* cneg = tw + 128;
+    float2* delta = cneg + 64;
+    __shared__ Probe sp;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int grp = lane >> 3;
+    const int s = lane & 7;
+    float2* Tg = T + (warp * 4 + grp) * kG8Scratch;
+    const int chunk = blockIdx.x;
+    const int cand = blockIdx.y;
+    if (tid == 0) {
+        const qssb_aberrations_t ab = cands[cand];
+        sp = make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
+    }
+    fill_twiddles<N>(tw, tid, 512);
+    for (int i = tid; i < 128 * kL128P; i += 512) sq[i] = 0.0f;
+    __syncthreads();
+    const Probe& p = sp;
+    const float2* eqc = eq_table + (size_t)cand * N * N;
+    // the line (row or column) of this group within a round of 64
+    const int line = (warp & 7) + 8 * grp + 32 * (warp >> 3);
+    float acc[2][16];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int t = 0; t < 16; ++t) acc[r][t] = 0.0f;
+    const int b0 = chunk * bf_per_chunk;
+    int nb = n_bf - b0;
+    if (nb > bf_per_chunk) nb = bf_per_chunk;
+    const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
+    for (int i = 0; i < nb; ++i) {
+        const int b = b0 + i;
+        const BFQuad kq = bf_quad(geom, n_bf, b, p);
+        float2 pk = make_float2(0.0f, 0.0f);
+        if constexpr (!QUAD)
+            pk = probe_at_bf<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
+                                    __ldg(geom + 4 * n_bf + b), __ldg(geom + 5 * n_bf + b), p);
+        const float2* gb = g + (size_t)b * N * H;
+        // A) rows 0..64 and the lower Nyquist column
+        for (int e = tid; e < 65 * N + 63; e += 512) {
+            int r, c;
+            if (e < 65 * N) {
+                r = e >> 7;
+                c = e & 127;
+            } else {
+                r = N - 1 - (e - 65 * N);  // 127 .. 65
+                c = 64;
+            }
+            const float2 gv = c <= 64 ? __ldg(gb + r * H + c)
+                                      : cconj(__ldg(gb + ((N - r) & (N - 1)) * H + (N - c)));
+            float2 v;
+            if constexpr (QUAD) {
+                v = corrected_quad<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c,
+                                          __ldg(eqc + r * N + c), kq, gv, p);
+            } else {
+                v = corrected<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c, kq.kx, kq.ky,
+                                     kq.kx_lo, kq.ky_lo, pk, gv, p);
+            }
+            if (e < 65 * N) {
+                Hp[r * kL128P + c] = (r == 0 && c == 0) ? dc : v;
+            } else {
+                cneg[N - r] = v;  // C(-r', 64), r' = N - r in 1..63
+            }
+        }
+        __syncthreads();
+        if (tid >= 1 && tid < 64) delta[tid] = cadd(cconj(Hp[tid * kL128P + 64]), cneg[tid]);
+        __syncthreads();
+        // B) row IFFTs of rows 0..63, then row 64
+        {
+            float2 v[16];
+            float2* rowp = Hp + line * kL128P;
+#pragma unroll
+            for (int n1 = 0; n1 < 16; ++n1) v[n1] = rowp[s + 8 * n1];
+            fft128_g8<+1>(v, Tg, s, tw);
+#pragma unroll
+            for (int t = 0; t < 16; ++t) rowp[fft128_g8_index(s, t)] = v[t];
+            if (warp == 0) {
+                float2* r64 = Hp + 64 * kL128P;
+#pragma unroll
+                for (int n1 = 0; n1 < 16; ++n1) v[n1] = lane < 8 ? r64[s + 8 * n1] : make_float2(0.f, 0.f);
+                fft128_g8<+1>(v, Tg, s, tw);
+                if (lane < 8) {
+#pragma unroll
+                    for (int t = 0; t < 16; ++t) r64[fft128_g8_index(s, t)] = v[t];
+                }
+            }
+        }
+        __syncthreads();
+        // C) column IFFTs, two rounds of 64 columns
+#pragma unroll
+        for (int round = 0; round < 2; ++round) {
+            const int x = line + 64 * round;
+            const float sign = (x & 1) ? -1.0f : 1.0f;
+            float2 v[16];
+#pragma unroll
+            for (int n1 = 0; n1 < 16; ++n1) {
+                const int r = s + 8 * n1;
+                if (r <= 64) {
+                    v[n1] = Hp[r * kL128P + x];
+                } else {
+                    const float2 m = Hp[(N - r) * kL128P + x];
+                    const float2 d = delta[N - r];
+                    v[n1] = make_float2(fmaf(sign, d.x, -m.x), fmaf(sign, d.y, m.y));
+                }
+            }
+            fft128_g8<+1>(v, Tg, s, tw);
+#pragma unroll
+            for (int t = 0; t < 16; ++t) {
+                const int y = fft128_g8_index(s, t);
+                const float ph = atan2f(v[t].y, v[t].x);
+                acc[round][t] += ph;
+                float* q2 = sq + y * kL128P + x;
+                *q2 = fmaf(ph, ph, *q2);
+            }
+        }
+        __syncthreads();
+    }
+    // row-major partial planes: part[((cand * n_chunks + chunk) * 2 + m) * N * N + y * N + x]
+    float* ps = part + ((size_t)(cand * n_chunks + chunk) * 2) * N * N;
+    float* pq = ps + (size_t)N * N;
+#pragma unroll
+    for (int round = 0; round < 2; ++round) {
+        const int x = line + 64 * round;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) ps[fft128_g8_index(s, t) * N + x] = acc[round][t];
+    }
+    for (int i = tid; i < N * N; i += 512) pq[i] = sq[(i >> 7) * kL128P + (i & 127)];
+}
+
 template <int N>
 __global__ void k_loss_reduce(const float* __restrict__ part, int n_chunks, int n_bf,
-                              double* __restrict__ var, float* __restrict__ mean_phase) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;  // col * N + row
+                              double* __restrict__ var, float* __restrict__ mean_phase,
+                              int row_major) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;  // col * N + row, or row * N + col
     const int cand = blockIdx.y;
     if (j >= N * N) return;
     double s1 = 0.0, s2 = 0.0;
@@ -166,9 +333,9 @@ __global__ void k_loss_reduce(const float* __restrict__ part, int n_chunks, int 
     const double mean = s1 * inv_b;
     var[(size_t)cand * N * N + j] = s2 * inv_b - mean * mean;
     if (mean_phase) {
-        const int col = j / N;
-        const int row = j - col * N;
-        mean_phase[(size_t)cand * N * N + row * N + col] = (float)mean;
+        const int hi = j / N;
+        const int lo = j - hi * N;
+        mean_phase[(size_t)cand * N * N + (row_major ? j : lo * N + hi)] = (float)mean;
     }
 }
 
@@ -225,15 +392,24 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
         k_eq_table<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(cands, cal, eq);
         CUDA_TRY(cudaGetLastError());
     }
-    const size_t smem = LossSmem<N>::bytes;
-    CUDA_TRY(cudaFuncSetAttribute(k_loss_moments<N, SYM, CHI64, QUAD>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_loss_moments<N, SYM, CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
-        reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal, eq,
-        pl.bf_per_chunk, pl.n_chunks, part);
+    if constexpr (N == 128) {
+        const size_t smem = Loss128Smem::bytes;
+        CUDA_TRY(cudaFuncSetAttribute(k_loss_moments128<CHI64, QUAD>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_loss_moments128<CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), 512, smem, s>>>(
+            reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal, eq,
+            pl.bf_per_chunk, pl.n_chunks, part);
+    } else {
+        const size_t smem = LossSmem<N>::bytes;
+        CUDA_TRY(cudaFuncSetAttribute(k_loss_moments<N, SYM, CHI64, QUAD>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_loss_moments<N, SYM, CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
+            reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal, eq,
+            pl.bf_per_chunk, pl.n_chunks, part);
+    }
     CUDA_TRY(cudaGetLastError());
     k_loss_reduce<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(part, pl.n_chunks, cal.n_bf,
-                                                                       var, mean_phase);
+                                                                       var, mean_phase, N == 128);
     CUDA_TRY(cudaGetLastError());
     k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N, losses);
     CUDA_TRY(cudaGetLastError());
