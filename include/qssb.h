@@ -94,6 +94,55 @@ int qssb_gather_bf_columns(const uint16_t* counts, int64_t n_frames, int32_t det
                            const int32_t* bf_linear, int32_t n_bf, uint16_t* columns,
                            void* stream);
 
+/* Result of qssb_select_bf (device memory, written by the kernel). */
+typedef struct qssb_bf_info {
+    int32_t n_bf;        /* selected BF pixels B (0: nothing selected) */
+    int32_t n_mask;      /* pixels with mean_dp > max(mean_dp) * threshold */
+    double center_row;   /* selection centre in detector pixels (float32 values) */
+    double center_col;
+    double radius;       /* selection radius in pixels */
+    double dc_re;        /* dc = mean over the B pixels of their exact frame sums */
+    double dc_im;        /* 0 (the scan images are real) */
+} qssb_bf_info_t;
+
+/* Bright-field selection from the exact frame sums (the reference's
+ * _compute_bf_mask_from_mean_dp, backend.py:448-518, and the dc of
+ * _extract_gqk, backend.py:587): mean_dp = float32(sums) / n_frames; mask =
+ * mean_dp > max(mean_dp) * threshold; with bf_radius <= 0 the probe disk
+ * mean_dp > mean + std gives the centre (its centroid) and the radius
+ * sqrt(|disk| / pi), otherwise the centre is the intensity-weighted centroid
+ * of the mask and the radius bf_radius; the kept pixels are the mask pixels
+ * within the radius, in row-major order. sums: device u64 [det_rows*det_cols];
+ * mean_dp: device float32 [det_rows*det_cols] or NULL; bf_linear: device
+ * int32 with room for det_rows*det_cols entries (the first info->n_bf are
+ * written); info: device. One CTA; nothing is read back. */
+int qssb_select_bf(const uint64_t* sums, int32_t det_rows, int32_t det_cols, int64_t n_frames,
+                   float threshold, float bf_radius, float* mean_dp, int32_t* bf_linear,
+                   qssb_bf_info_t* info, void* stream);
+
+/* Detector-to-k calibration of qssb_bf_geometry. rot_cos / rot_sin are
+ * cos(-theta) and sin(-theta) of the scan rotation theta (the passive
+ * rotation of engine.py:800-805). */
+typedef struct qssb_geometry_params {
+    double k_step_row_inv_A;      /* detector pixel pitch in 1/A: 1 / (sampling_row * det_rows) */
+    double k_step_col_inv_A;
+    double rot_cos;
+    double rot_sin;
+    double wavelength_A;
+    double semiangle_rad;
+    double det_sampling_row_rad;
+    double det_sampling_col_rad;
+} qssb_geometry_params_t;
+
+/* Per-BF geometry of SSBEngine.cache_rotation (engine.py:784-830) for the
+ * info->n_bf pixels of bf_linear, relative to info's centre, written as
+ * bf_geom [QSSB_GEOM_ROWS][n_bf] (rows n_bf floats apart; bf_geom must hold
+ * QSSB_GEOM_ROWS * capacity floats, capacity >= n_bf, else nothing is
+ * written). Needs no host copy of n_bf: launch it right after qssb_select_bf. */
+int qssb_bf_geometry(const int32_t* bf_linear, const qssb_bf_info_t* info, int32_t det_rows,
+                     int32_t det_cols, int32_t capacity, const qssb_geometry_params_t* params,
+                     float* bf_geom, void* stream);
+
 /* Forward scan FFT of each BF image, Hermitian half plane:
  * g_half[b][r][c] = sum_R columns[b][R] exp(-2 pi i (r R_r/R0 + c R_c/R1)),
  * c in [0, R1/2]. Replaces cp.fft.fft2 + the half-plane slice of

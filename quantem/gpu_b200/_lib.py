@@ -57,6 +57,35 @@ class Aberrations(ctypes.Structure):
     ]
 
 
+class BFInfo(ctypes.Structure):
+    """``qssb_bf_info_t`` (written on the device by ``qssb_select_bf``)."""
+
+    _fields_ = [
+        ("n_bf", ctypes.c_int32),
+        ("n_mask", ctypes.c_int32),
+        ("center_row", ctypes.c_double),
+        ("center_col", ctypes.c_double),
+        ("radius", ctypes.c_double),
+        ("dc_re", ctypes.c_double),
+        ("dc_im", ctypes.c_double),
+    ]
+
+
+class GeometryParams(ctypes.Structure):
+    """``qssb_geometry_params_t``."""
+
+    _fields_ = [
+        ("k_step_row_inv_A", ctypes.c_double),
+        ("k_step_col_inv_A", ctypes.c_double),
+        ("rot_cos", ctypes.c_double),
+        ("rot_sin", ctypes.c_double),
+        ("wavelength_A", ctypes.c_double),
+        ("semiangle_rad", ctypes.c_double),
+        ("det_sampling_row_rad", ctypes.c_double),
+        ("det_sampling_col_rad", ctypes.c_double),
+    ]
+
+
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
 _I64 = ctypes.c_int64
@@ -68,6 +97,10 @@ SIGNATURES = {
     "qssb_last_error": (ctypes.c_char_p, []),
     "qssb_mean_dp_u64": (ctypes.c_int, [_P, _I64, _I32, _P, _P, _P]),
     "qssb_gather_bf_columns": (ctypes.c_int, [_P, _I64, _I32, _P, _I32, _P, _P]),
+    "qssb_select_bf": (ctypes.c_int, [_P, _I32, _I32, _I64, ctypes.c_float, ctypes.c_float,
+                                      _P, _P, _P, _P]),
+    "qssb_bf_geometry": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, ctypes.POINTER(GeometryParams),
+                                        _P, _P]),
     "qssb_scan_fft_half": (ctypes.c_int, [_P, _I32, _I32, _I32, _P, _P]),
     "qssb_object_workspace_bytes": (
         ctypes.c_int, [ctypes.POINTER(Calibration), _I32, ctypes.POINTER(_SZ)]),

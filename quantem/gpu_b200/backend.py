@@ -32,7 +32,7 @@ import numpy as np
 import torch
 
 from . import ops
-from ._lib import QSSB_FLAG_CHI_FP64, QSSB_FLAG_QUADRATIC, Aberrations, Calibration
+from ._lib import GEOM_ROWS, QSSB_FLAG_CHI_FP64, QSSB_FLAG_QUADRATIC, Aberrations, Calibration
 from .calibration import (
     BFGeometry,
     bf_geometry,
@@ -66,6 +66,20 @@ def _as_device_counts(data, device: torch.device) -> torch.Tensor:
     if not t.is_cuda or t.device != device:
         t = t.to(device, non_blocking=False)
     return t.contiguous()
+
+
+_FREQ_CACHE: dict = {}
+
+
+def _device_frequencies(scan_shape, scan_sampling, device) -> tuple[torch.Tensor, torch.Tensor]:
+    """Device fftfreq grids of the scan axes, uploaded once per shape/sampling/device."""
+    key = (tuple(scan_shape), tuple(float(s) for s in scan_sampling), str(device))
+    hit = _FREQ_CACHE.get(key)
+    if hit is None:
+        q_row, q_col = scan_frequencies(scan_shape, scan_sampling)
+        hit = tuple(t.clone() for t in ops.STAGING.upload([q_row, q_col], torch.device(device)))
+        _FREQ_CACHE[key] = hit
+    return hit
 
 
 class B200SSBBackend:
@@ -151,15 +165,15 @@ class B200SSBBackend:
                 f"padding rule; got {scan_gpts}."
             )
         self.wavelength = electron_wavelength_angstrom(energy)
-        # (a3) exact u64 mean diffraction pattern on the GPU; the one host sync
-        # of preparation reads the 128 KB of sums back
-        sums_dev, _ = ops.mean_dp_u64(counts, want_mean=False)
-        sums_host = sums_dev.cpu().numpy().view(np.uint64).reshape(det_gpts)
         n_frames = scan_gpts[0] * scan_gpts[1]
-        mean_host = ops.mean_from_sums(sums_host, n_frames)
+        # (a3) exact u64 frame sums on the GPU
+        sums_dev, _ = ops.mean_dp_u64(counts, want_mean=False)
         self._detected_radius_px = None
+        sums_host = None
         if det_sampling is None:
-            _, r = detect_bf_radius(mean_host)
+            # (a5) the half-max radius detector runs on the host mean pattern
+            sums_host = sums_dev.cpu().numpy().view(np.uint64).reshape(det_gpts)
+            _, r = detect_bf_radius(ops.mean_from_sums(sums_host, n_frames))
             self._detected_radius_px = float(r)
             det_sampling = (2 * semiangle) / r
             det_sampling = (det_sampling, det_sampling)
@@ -170,22 +184,48 @@ class B200SSBBackend:
         self.sampling = (1.0 / (recip[0] * det_gpts[0]), 1.0 / (recip[1] * det_gpts[1]))
         self.gpts = det_gpts
         self._scan_shape = scan_gpts
-        # (a4) BF selection on the 64 KB mean DP
-        sel = select_bf(mean_host, self.bf_intensity_threshold, bf_radius)
-        self.bf_inds_row = sel.rows
-        self.bf_inds_col = sel.cols
-        self.bf_center = sel.center
-        self._bf_radius_selected = sel.radius
-        lin_host = (sel.rows.astype(np.int64) * det_gpts[1] + sel.cols).astype(np.int32)
-        self.dc_value = complex(float(sums_host.reshape(-1)[lin_host].astype(np.float64).mean()), 0.0)
-        q_row, q_col = scan_frequencies(scan_gpts, self.scan_sampling)
-        self._q_row_host, self._q_col_host = q_row, q_col
-        geo = bf_geometry(sel.rows, sel.cols, sel.center, det_gpts, self.sampling, self.wavelength,
-                          self.semiangle_cutoff, self.angular_sampling, self._rotation_angle_rad)
-        # one pinned upload: BF indices, geometry, scan frequencies
-        self._bf_linear, self._geom_dev, self._q_row, self._q_col = ops.STAGING.upload(
-            [lin_host, geo.stacked(), q_row, q_col], self.device)
-        self._geometry = geo
+        self._bf_rows_host = self._bf_cols_host = None
+        self._geometry_host = None
+        if sums_host is None and (bf_radius is None or bf_radius > 0):
+            # (a4) selection and (a8) geometry on the device; the one host sync
+            # of preparation reads the 48-byte selection result
+            sel = ops.select_bf(sums_dev, det_gpts, n_frames, self.bf_intensity_threshold, bf_radius)
+            geom_buf = ops.bf_geometry(
+                sel, det_gpts, self._k_step(), self._rotation_angle_rad, self.wavelength,
+                self.semiangle_cutoff * 1e-3,
+                (self.angular_sampling[0] * 1e-3, self.angular_sampling[1] * 1e-3))
+            info = ops.read_bf_info(sel)
+            if info.n_mask == 0:
+                raise ValueError(
+                    f"No bright-field pixels found with threshold {self.bf_intensity_threshold:.2f}. "
+                    "Check that the data contains a visible BF disk, or lower the threshold.")
+            if info.n_bf == 0:
+                raise ValueError(
+                    f"No bright-field pixels within bf_radius={info.radius}. Increase bf_radius or "
+                    "check detector geometry.")
+            n_bf = int(info.n_bf)
+            self._bf_linear = sel.bf_linear[:n_bf]
+            self._geom_dev = geom_buf[:GEOM_ROWS * n_bf].view(GEOM_ROWS, n_bf)
+            self.bf_center = (float(info.center_row), float(info.center_col))
+            self._bf_radius_selected = float(info.radius)
+            self.dc_value = complex(float(info.dc_re), float(info.dc_im))
+        else:
+            if sums_host is None:
+                sums_host = sums_dev.cpu().numpy().view(np.uint64).reshape(det_gpts)
+            # (a4) BF selection on the host mean pattern (radius-detection path)
+            sel = select_bf(ops.mean_from_sums(sums_host, n_frames), self.bf_intensity_threshold,
+                            bf_radius)
+            self._bf_rows_host, self._bf_cols_host = sel.rows, sel.cols
+            self.bf_center = sel.center
+            self._bf_radius_selected = sel.radius
+            lin_host = (sel.rows.astype(np.int64) * det_gpts[1] + sel.cols).astype(np.int32)
+            self.dc_value = complex(float(sums_host.reshape(-1)[lin_host].astype(np.float64).mean()), 0.0)
+            geo = bf_geometry(sel.rows, sel.cols, sel.center, det_gpts, self.sampling, self.wavelength,
+                              self.semiangle_cutoff, self.angular_sampling, self._rotation_angle_rad)
+            self._geometry_host = geo
+            self._bf_linear, self._geom_dev = ops.STAGING.upload([lin_host, geo.stacked()], self.device)
+        self._q_row_host, self._q_col_host = scan_frequencies(scan_gpts, self.scan_sampling)
+        self._q_row, self._q_col = _device_frequencies(scan_gpts, self.scan_sampling, self.device)
         self._cached_rotation = self._rotation_angle_rad
         # (a6) gather + Hermitian scan FFT; dc exact from the integer sums
         columns = ops.gather_bf_columns(counts, self._bf_linear, validate=False)
@@ -227,6 +267,48 @@ class B200SSBBackend:
         return counts
 
     # ---------------------------------------------------------------- helpers
+    def _k_step(self) -> tuple[float, float]:
+        """Detector pixel pitch in 1/A, as cache_rotation derives it from the sampling."""
+        return (1.0 / (self.sampling[0] * self.gpts[0]), 1.0 / (self.sampling[1] * self.gpts[1]))
+
+    def _host_selection(self) -> None:
+        if self._bf_rows_host is None:
+            lin = self._bf_linear.cpu().numpy().astype(np.int64)
+            self._bf_rows_host = (lin // self.gpts[1]).astype(np.int32)
+            self._bf_cols_host = (lin % self.gpts[1]).astype(np.int32)
+
+    @property
+    def bf_inds_row(self) -> np.ndarray:
+        """Selected BF detector rows (int32, row-major order); host copy made on first use."""
+        self._host_selection()
+        return self._bf_rows_host
+
+    @bf_inds_row.setter
+    def bf_inds_row(self, value) -> None:
+        self._bf_rows_host = value
+
+    @property
+    def bf_inds_col(self) -> np.ndarray:
+        """Selected BF detector columns (int32); host copy made on first use."""
+        self._host_selection()
+        return self._bf_cols_host
+
+    @bf_inds_col.setter
+    def bf_inds_col(self, value) -> None:
+        self._bf_cols_host = value
+
+    @property
+    def _geometry(self) -> BFGeometry:
+        """Host copy of the per-BF geometry (reference cache names), made on first use."""
+        if self._geometry_host is None:
+            g = self._geom_dev.cpu().numpy()
+            self._geometry_host = BFGeometry(*[g[i].copy() for i in range(GEOM_ROWS)])
+        return self._geometry_host
+
+    @_geometry.setter
+    def _geometry(self, value) -> None:
+        self._geometry_host = value
+
     def _calibration(self) -> Calibration:
         return Calibration(
             n_bf=int(self.G_qk.shape[0]), scan_rows=self._scan_shape[0], scan_cols=self._scan_shape[1],

@@ -241,6 +241,8 @@ struct Probe {
     float ang_c;
     float inner2;     // (|u| <= inner) => aperture == 1 exactly; <= 0 disables
     float outer2;     // (|u| >= outer) => aperture == 0 exactly
+    float inv_ang;    // 1 / d_row (isotropic detector sampling)
+    bool iso;         // d_row == d_col: denom == d_row for every direction
     float factor;
     float C10;
     float C12;
@@ -278,6 +280,29 @@ __device__ __forceinline__ float soft_aperture(float dx, float dy, float r2, con
     const float denom = sqrtf(num2) * inv_r;
     const float edge = denom > 1e-15f ? (p.semiangle - alpha) / denom + 0.5f : 1.0f;
     return fminf(fmaxf(edge, 0.0f), 1.0f);
+}
+
+// The same aperture without branches and with reciprocal square roots only
+// (the arithmetic class of a --use_fast_math build): r = r2 rsqrt(r2); with
+// isotropic sampling denom == d exactly, so one MUFU op per call. The exact
+// 1 inside `inner` and 0 outside `outer` are kept by selects: the tied-overlap
+// refinement depends on them.
+__device__ __forceinline__ float soft_aperture_fast(float dx, float dy, float r2, const Probe& p) {
+    const float r = r2 * rsqrtf(r2);
+    const float num = p.semiangle - r * p.wavelength;
+    float edge;
+    if (p.iso) {
+        edge = fmaf(num, p.inv_ang, 0.5f);
+    } else {
+        const float ar = dx * p.ang_r;
+        const float ac = dy * p.ang_c;
+        edge = fmaf(num * r, rsqrtf(fmaf(ar, ar, ac * ac)), 0.5f);
+    }
+    float a = fminf(fmaxf(edge, 0.0f), 1.0f);
+    a = r2 > 0.0f ? a : 1.0f;
+    a = r2 >= p.outer2 ? 0.0f : a;
+    a = (p.inner2 > 0.0f && r2 <= p.inner2) ? 1.0f : a;
+    return a;
 }
 
 __device__ __forceinline__ bool in_edge_band(float r2, const Probe& p) {
@@ -413,6 +438,8 @@ __host__ __device__ inline Probe make_probe_common(const qssb_calibration_t& cal
     p.inner2 = inner > 0.0f ? inner * inner : 0.0f;
     const float outer = (p.semiangle + 0.5f * max_ang) / p.wavelength;
     p.outer2 = outer * outer;
+    p.iso = cal.det_sampling_row_rad == cal.det_sampling_col_rad;
+    p.inv_ang = (float)(1.0 / cal.det_sampling_row_rad);
     p.semi_d = cal.semiangle_rad;
     p.lam_d = cal.wavelength_A;
     p.ang_r_d = cal.det_sampling_row_rad;
@@ -526,6 +553,51 @@ __device__ __forceinline__ float2 corrected_quad(float qx, float qy, int r, int 
     gr *= inv;
     gi *= inv;
     return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
+}
+
+// corrected_quad (FP32 chi) with e^{i theta} supplied by the caller (a phase
+// recurrence or a separable table) and the branch-free aperture. Gamma == 0
+// (both apertures 0) gives m2 == 0 and C == 0 without a branch.
+__device__ __forceinline__ float2 corrected_quad_e(float qx, float qy, int r, int c, float2 eq,
+                                                   float kx, float ky, float ak,
+                                                   const float2* lo, float2 e, float2 g,
+                                                   const Probe& p) {
+    const float dxm = qx - kx, dym = qy - ky;
+    const float dxp = qx + kx, dyp = qy + ky;
+    const float r2m = fmaf(dxm, dxm, dym * dym);
+    const float r2p = fmaf(dxp, dxp, dyp * dyp);
+    float am = soft_aperture_fast(dxm, dym, r2m, p);
+    float ap = soft_aperture_fast(dxp, dyp, r2p, p);
+    if (fabsf(am - ap) < kApertureTie && (in_edge_band(r2m, p) || in_edge_band(r2p, p))) {
+        const float2 l = *lo;
+        const double qx64 = fftfreq_d(r, p.n_r, p.qval_r);
+        const double qy64 = fftfreq_d(c, p.n_c, p.qval_c);
+        const double kx64 = (double)kx + (double)l.x;
+        const double ky64 = (double)ky + (double)l.y;
+        am = soft_aperture_fp64(qx64 - kx64, qy64 - ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
+        ap = soft_aperture_fp64(qx64 + kx64, qy64 + ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
+    }
+    const float dr = (am - ap) * eq.x;
+    const float di = -(am + ap) * eq.y;
+    float gr = ak * fmaf(e.x, dr, -e.y * di);
+    float gi = ak * fmaf(e.x, di, e.y * dr);
+    const float m2 = fmaf(gr, gr, gi * gi);
+    const float inv = m2 > 1e-16f ? rsqrtf(m2) : 1e8f;
+    gr *= inv;
+    gi *= inv;
+    return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
+}
+
+// Kahan-compensated complex accumulation: (s.x, s.y) sums, (s.z, s.w) compensations.
+__device__ __forceinline__ void kahan_add(float4& s, float2 v) {
+    const float yr = v.x - s.z;
+    const float tr = s.x + yr;
+    s.z = (tr - s.x) - yr;
+    s.x = tr;
+    const float yi = v.y - s.w;
+    const float ti = s.y + yi;
+    s.w = (ti - s.y) - yi;
+    s.y = ti;
 }
 
 }  // namespace qssb

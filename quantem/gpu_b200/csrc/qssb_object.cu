@@ -126,6 +126,127 @@ __global__ void __launch_bounds__(kTrotterThreads) k_trotter_partial(
     partial[(size_t)chunk * NQ + qi] = make_float2(sr, si);
 }
 
+// The C10/C12 (quadratic chi, FP32) path with four adjacent frequencies per
+// thread. theta = 2 q^T M k is linear in q, so along a row of the stored half
+// plane e^{i theta} advances by the per-BF factor w = e^{i 2 dq v}: one sincos
+// per four overlap evaluations. Threads t < N * N/8 take (r, 4j .. 4j+3) of
+// columns 0..N/2-1; the rest take column N/2 of every row and the Nyquist
+// row's columns N/2+1..N-1 one at a time. The partial layout is the same as
+// k_trotter_partial's.
+struct BFRow {
+    float4 a;  // kx, ky, u, v   with (u, v) = M k
+    float4 b;  // A(k), w.x, w.y, unused
+};
+
+template <int N>
+__global__ void __launch_bounds__(kTrotterThreads) k_trotter_quad4(
+    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
+    const float* __restrict__ q_row, const float* __restrict__ q_col, Probe p, int bf_per_chunk,
+    float2* __restrict__ partial) {
+    constexpr int H = N / 2 + 1;
+    constexpr int NQ = n_eval_q<N, true>();
+    constexpr int GPR = N / 8;   // groups of four per row
+    constexpr int NG = N * GPR;
+    constexpr int NT = N + N / 2 - 1;
+    __shared__ BFRow s_bf[kMaxBfChunk];
+    __shared__ float2 s_lo[kMaxBfChunk];
+    const int tid = threadIdx.x;
+    const int chunk = blockIdx.y;
+    const int b0 = chunk * bf_per_chunk;
+    int nb = n_bf - b0;
+    if (nb > bf_per_chunk) nb = bf_per_chunk;
+    const float dq = __ldg(q_col + 1);  // fftfreq step 1 / (N d)
+    for (int i = tid; i < nb; i += kTrotterThreads) {
+        const int b = b0 + i;
+        const float kx = __ldg(geom + b);
+        const float ky = __ldg(geom + n_bf + b);
+        const float u = fmaf(p.mxx, kx, p.mxy * ky);
+        const float v = fmaf(p.mxy, kx, p.myy * ky);
+        float sw, cw;
+        sincosf(2.0f * dq * v, &sw, &cw);
+        s_bf[i].a = make_float4(kx, ky, u, v);
+        s_bf[i].b = make_float4(__ldg(geom + 5 * n_bf + b), cw, sw, 0.0f);
+        s_lo[i] = make_float2(__ldg(geom + 6 * n_bf + b), __ldg(geom + 7 * n_bf + b));
+    }
+    __syncthreads();
+    const int t = blockIdx.x * kTrotterThreads + tid;
+    if (t < NG) {
+        const int r = t / GPR;
+        const int c0 = 4 * (t - r * GPR);
+        const float qx = __ldg(q_row + r);
+        float qy[4];
+        float2 eq[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            qy[j] = __ldg(q_col + c0 + j);
+            eq[j] = eq_value(r, c0 + j, p);
+        }
+        const float2* gp = g + (size_t)b0 * N * H + r * H + c0;
+        float4 acc[4];
+        float2 gc[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            acc[j] = make_float4(0.f, 0.f, 0.f, 0.f);
+            gc[j] = nb > 0 ? __ldg(gp + j) : make_float2(0.f, 0.f);
+        }
+        for (int i = 0; i < nb; ++i) {
+            float2 gn[4];
+            const bool more = i + 1 < nb;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                gn[j] = more ? __ldg(gp + (size_t)(i + 1) * N * H + j) : make_float2(0.f, 0.f);
+            const float4 a = s_bf[i].a;
+            const float4 bb = s_bf[i].b;
+            float st, ct;
+            __sincosf(2.0f * fmaf(qx, a.z, qy[0] * a.w), &st, &ct);
+            float2 e = make_float2(ct, st);
+            const float2 w = make_float2(bb.y, bb.z);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const float2 v = corrected_quad_e(qx, qy[j], r, c0 + j, eq[j], a.x, a.y, bb.x,
+                                                  &s_lo[i], e, gc[j], p);
+                kahan_add(acc[j], v);
+                if (j < 3) e = cmul(e, w);
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) gc[j] = gn[j];
+        }
+        float2* out = partial + (size_t)chunk * NQ + r * H + c0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) out[j] = make_float2(acc[j].x, acc[j].y);
+    } else if (t < NG + NT) {
+        const int tt = t - NG;
+        int r, c, gr, gcol, qi;
+        bool cj;
+        if (tt < N) {
+            r = tt; c = N / 2; gr = r; gcol = c; cj = false; qi = r * H + c;
+        } else {
+            r = N / 2; c = H + (tt - N); gr = N / 2; gcol = N - c; cj = true; qi = N * H + (tt - N);
+        }
+        const float qx = __ldg(q_row + r);
+        const float qy = __ldg(q_col + c);
+        const float2 eq = eq_value(r, c, p);
+        const float2* gp = g + (size_t)b0 * N * H + gr * H + gcol;
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int i = 0; i < nb; ++i) {
+            float2 gv = __ldg(gp + (size_t)i * N * H);
+            if (cj) gv.y = -gv.y;
+            const float4 a = s_bf[i].a;
+            float st, ct;
+            __sincosf(2.0f * fmaf(qx, a.z, qy * a.w), &st, &ct);
+            const float2 v = corrected_quad_e(qx, qy, r, c, eq, a.x, a.y, s_bf[i].b.x, &s_lo[i],
+                                              make_float2(ct, st), gv, p);
+            kahan_add(acc, v);
+        }
+        partial[(size_t)chunk * NQ + qi] = make_float2(acc.x, acc.y);
+    }
+}
+
+template <int N>
+__host__ __device__ constexpr int quad4_threads() {
+    return N * (N / 8) + N + N / 2 - 1;
+}
+
 // Full N x N corrected-mean plane from the chunk partials.
 template <int N, bool SYM>
 __global__ void k_trotter_plane(const float2* __restrict__ partial, int n_chunks, int n_bf,
@@ -150,15 +271,30 @@ __global__ void k_trotter_plane(const float2* __restrict__ partial, int n_chunks
     } else {
         qi = idx;
     }
-    double sr = 0.0, si = 0.0;
-    for (int k = 0; k < n_chunks; ++k) {
-        const float2 v = partial[(size_t)k * NQ + qi];
-        sr += (double)v.x;
-        si += (double)v.y;
+    // eight independent FP64 lanes over the chunks (loads in flight
+    // together), folded in a fixed order: deterministic for a given plan
+    double lr[8], li[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) lr[j] = li[j] = 0.0;
+    int k = 0;
+    for (; k + 8 <= n_chunks; k += 8) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const float2 v = __ldg(partial + (size_t)(k + j) * NQ + qi);
+            lr[j] += (double)v.x;
+            li[j] += (double)v.y;
+        }
     }
-    if (mirror) sr = -sr;  // S(-q) = -conj(S(q)): real part flips, imaginary part stays
+    for (; k < n_chunks; ++k) {
+        const float2 v = __ldg(partial + (size_t)k * NQ + qi);
+        lr[0] += (double)v.x;
+        li[0] += (double)v.y;
+    }
+    const double sr = ((lr[0] + lr[1]) + (lr[2] + lr[3])) + ((lr[4] + lr[5]) + (lr[6] + lr[7]));
+    const double si = ((li[0] + li[1]) + (li[2] + li[3])) + ((li[4] + li[5]) + (li[6] + li[7]));
     const double inv_b = 1.0 / (double)n_bf;
-    float2 out = make_float2((float)(sr * inv_b), (float)(si * inv_b));
+    // S(-q) = -conj(S(q)): real part flips, imaginary part stays
+    float2 out = make_float2((float)((mirror ? -sr : sr) * inv_b), (float)(si * inv_b));
     if (r == 0 && c == 0) out = dc;
     plane[idx] = out;
 }
@@ -217,12 +353,14 @@ struct ObjectPlan {
     size_t plane_bytes;
 };
 
-// Deterministic chunking (independent of the GPU's SM count): about 40 BF
-// chunks, 4..256 BF pixels each.
+// Deterministic chunking (independent of the GPU's SM count): about 128 BF
+// chunks at N <= 128 and 32 at N = 256 (N^2/4-thread grids per chunk fill
+// the GPU), 4..256 BF pixels each.
 static ObjectPlan plan_object(int n, int n_bf, bool sym) {
     ObjectPlan pl;
     pl.n_q = sym ? n * (n / 2 + 1) + n / 2 - 1 : n * n;
-    int bpc = (n_bf + 39) / 40;
+    const int target = n >= 256 ? 32 : 128;
+    int bpc = (n_bf + target - 1) / target;
     if (bpc < 4) bpc = 4;
     if (bpc > kMaxBfChunk) bpc = kMaxBfChunk;
     pl.bf_per_chunk = bpc;
@@ -258,12 +396,19 @@ static int launch_object(const float* g_half, const float* geom, const float* q_
     const ObjectPlan pl = plan_object(N, cal.n_bf, SYM);
     float2* partial = reinterpret_cast<float2*>(ws);
     float2* plane = reinterpret_cast<float2*>(ws + pl.partial_bytes);
-    const dim3 grid((pl.n_q + kTrotterThreads - 1) / kTrotterThreads, pl.n_chunks);
-    k_trotter_partial<N, SYM, CHI64, QUAD><<<grid, kTrotterThreads, 0, s>>>(
-        reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, p, pl.bf_per_chunk,
-        partial);
+    if constexpr (SYM && QUAD && !CHI64) {
+        const dim3 grid((quad4_threads<N>() + kTrotterThreads - 1) / kTrotterThreads, pl.n_chunks);
+        k_trotter_quad4<N><<<grid, kTrotterThreads, 0, s>>>(
+            reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, p,
+            pl.bf_per_chunk, partial);
+    } else {
+        const dim3 grid((pl.n_q + kTrotterThreads - 1) / kTrotterThreads, pl.n_chunks);
+        k_trotter_partial<N, SYM, CHI64, QUAD><<<grid, kTrotterThreads, 0, s>>>(
+            reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, p,
+            pl.bf_per_chunk, partial);
+    }
     CUDA_TRY(cudaGetLastError());
-    k_trotter_plane<N, SYM><<<(N * N + 255) / 256, 256, 0, s>>>(
+    k_trotter_plane<N, SYM><<<(N * N + 127) / 128, 128, 0, s>>>(
         partial, pl.n_chunks, cal.n_bf, make_float2((float)cal.dc_re, (float)cal.dc_im), plane);
     CUDA_TRY(cudaGetLastError());
     k_ifft_rows<N><<<N / 8, 256, 0, s>>>(plane);

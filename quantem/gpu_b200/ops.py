@@ -18,6 +18,8 @@ from ._lib import Aberrations, Calibration, check
 # Kernel launches each entry point enqueues (the evidence counted by bench.py).
 LAUNCHES_PER_CALL = {
     "qssb_mean_dp_u64": 2,
+    "qssb_select_bf": 1,
+    "qssb_bf_geometry": 1,
     "qssb_gather_bf_columns": 1,
     "qssb_scan_fft_half": 1,
     "qssb_object": 4,
@@ -160,6 +162,69 @@ def mean_from_sums(sums_u64, n_frames: int):
     import numpy as np
 
     return np.asarray(sums_u64, dtype=np.uint64).astype(np.float32) / np.float32(n_frames)
+
+
+BF_INFO_BYTES = ctypes.sizeof(_lib.BFInfo)
+
+
+class DeviceSelection:
+    """Device outputs of :func:`select_bf`: BF indices (capacity K0*K1), the
+    ``qssb_bf_info_t`` bytes and the float32 mean pattern (or None)."""
+
+    def __init__(self, bf_linear: torch.Tensor, info: torch.Tensor, mean_dp: torch.Tensor | None):
+        self.bf_linear = bf_linear
+        self.info = info
+        self.mean_dp = mean_dp
+
+
+def select_bf(sums: torch.Tensor, det_shape: tuple[int, int], n_frames: int,
+              threshold: float = 0.0, bf_radius: float | None = None,
+              want_mean: bool = False) -> DeviceSelection:
+    """BF selection on the device from the exact u64 sums (no host sync)."""
+    _require_cuda(sums, "sums", torch.int64)
+    k0, k1 = int(det_shape[0]), int(det_shape[1])
+    if sums.numel() != k0 * k1:
+        raise ValueError("sums must hold det_rows * det_cols entries")
+    radius = 0.0 if bf_radius is None else float(bf_radius)
+    if bf_radius is not None and not radius > 0:
+        raise ValueError("bf_radius must be positive")
+    dev = sums.device
+    lin = torch.empty(k0 * k1, dtype=torch.int32, device=dev)
+    info = torch.empty(BF_INFO_BYTES, dtype=torch.uint8, device=dev)
+    mean = torch.empty((k0, k1), dtype=torch.float32, device=dev) if want_mean else None
+    _call("qssb_select_bf", dev, _ptr(sums), k0, k1, int(n_frames), float(threshold), radius,
+          _ptr(mean), _ptr(lin), _ptr(info), _stream(sums))
+    return DeviceSelection(lin, info, mean)
+
+
+def read_bf_info(sel: DeviceSelection) -> "_lib.BFInfo":
+    """Copy the 48-byte selection result to the host (the one sync of a cold
+    preparation)."""
+    host = torch.empty(BF_INFO_BYTES, dtype=torch.uint8, pin_memory=True)
+    host.copy_(sel.info, non_blocking=True)
+    torch.cuda.current_stream(sel.info.device).synchronize()
+    return _lib.BFInfo.from_buffer_copy(host.numpy().tobytes())
+
+
+def bf_geometry(sel: DeviceSelection, det_shape: tuple[int, int], k_step: tuple[float, float],
+                rotation_rad: float, wavelength_A: float, semiangle_rad: float,
+                det_sampling_rad: tuple[float, float]) -> torch.Tensor:
+    """Float32 buffer of 8*capacity whose first 8*n_bf floats are the
+    ``[8][n_bf]`` geometry of the selected pixels (written on the device)."""
+    import math
+
+    k0, k1 = int(det_shape[0]), int(det_shape[1])
+    cap = int(sel.bf_linear.numel())
+    geom = torch.empty(_lib.GEOM_ROWS * cap, dtype=torch.float32, device=sel.bf_linear.device)
+    gp = _lib.GeometryParams(
+        k_step_row_inv_A=float(k_step[0]), k_step_col_inv_A=float(k_step[1]),
+        rot_cos=math.cos(-rotation_rad), rot_sin=math.sin(-rotation_rad),
+        wavelength_A=float(wavelength_A), semiangle_rad=float(semiangle_rad),
+        det_sampling_row_rad=float(det_sampling_rad[0]),
+        det_sampling_col_rad=float(det_sampling_rad[1]))
+    _call("qssb_bf_geometry", sel.bf_linear.device, _ptr(sel.bf_linear), _ptr(sel.info), k0, k1,
+          cap, ctypes.byref(gp), _ptr(geom), _stream(geom))
+    return geom
 
 
 def gather_bf_columns(counts: torch.Tensor, bf_linear: torch.Tensor, validate: bool = True

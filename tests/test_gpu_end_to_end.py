@@ -27,7 +27,13 @@ def _compare(backend: B200SSBBackend, host: np.ndarray, kw: dict, ab: so.Aberrat
     prep = so.prepare(host, **kw)
     np.testing.assert_array_equal(backend.bf_inds_row, prep.bf.rows)
     np.testing.assert_array_equal(backend.bf_inds_col, prep.bf.cols)
-    assert backend.bf_center == prep.bf.center
+    if kw.get("bf_radius") is None:  # centroid of integer indices: exact
+        assert backend.bf_center == prep.bf.center
+    else:
+        # intensity-weighted float32 centroid: the oracle sums in numpy's pairwise
+        # float32 order, the reference's CuPy in its tree order, the device in FP64
+        # rounded once; they agree to a few float32 ulps
+        np.testing.assert_allclose(backend.bf_center, prep.bf.center, rtol=5e-7)
     # both are means of exact integer sums; only the summation order differs
     assert abs(backend.dc_value - prep.dc) <= 1e-14 * abs(prep.dc)
     g = backend.G_qk.cpu().numpy()

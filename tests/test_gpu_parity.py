@@ -69,6 +69,103 @@ def disk_case():
     return _prep_case(disk_input(123), **DISK_KW)
 
 
+# ------------------------------------------------------- device selection
+GOLDEN = __import__("pathlib").Path(__file__).resolve().parent / "golden"
+
+
+def _device_selection(data: np.ndarray, threshold: float, bf_radius, det_sampling, semiangle,
+                      wavelength, sampling, rotation=0.0):
+    counts = _dev(data)
+    det = data.shape[2:]
+    n_frames = data.shape[0] * data.shape[1]
+    sums, _ = ops.mean_dp_u64(counts, want_mean=False)
+    sel = ops.select_bf(sums, det, n_frames, threshold, bf_radius, want_mean=True)
+    k_step = (1.0 / (sampling[0] * det[0]), 1.0 / (sampling[1] * det[1]))
+    geom = ops.bf_geometry(sel, det, k_step, rotation, wavelength, semiangle * 1e-3,
+                           (det_sampling * 1e-3, det_sampling * 1e-3))
+    info = ops.read_bf_info(sel)
+    n = info.n_bf
+    lin = sel.bf_linear[:n].cpu().numpy()
+    g = geom[:8 * n].view(8, n).cpu().numpy()
+    return info, lin // det[1], lin % det[1], g, sel.mean_dp.cpu().numpy(), sums
+
+
+@pytest.mark.parametrize("name", ["ref_disk128_bfr3", "ref_disk96_padded", "ref_plain32_auto"])
+def test_device_selection_matches_reference_golden(name):
+    """qssb_select_bf + qssb_bf_geometry against the reference's own outputs."""
+    from recipes import synthetic_plain_32
+
+    data = {"ref_disk128_bfr3": lambda: disk_input(123),
+            "ref_disk96_padded": lambda: disk_input(124, scan=(96, 96)),
+            "ref_plain32_auto": synthetic_plain_32}[name]()
+    with np.load(GOLDEN / f"{name}.npz") as z:
+        gold = {k: z[k] for k in z.files}
+    data = so.pad_or_crop_scan(data)
+    bf_radius = float(gold["kw_bf_radius"]) if "kw_bf_radius" in gold else None
+    det = float(gold["kw_det_sampling"])
+    info, rows, cols, g, mean_dp, _ = _device_selection(
+        data, 0.0, bf_radius, det, float(gold["kw_semiangle"]), float(gold["wavelength"]),
+        tuple(gold["sampling"]))
+    np.testing.assert_array_equal(mean_dp, so.mean_dp_u64(data)[1])
+    np.testing.assert_array_equal(rows, gold["rows"])
+    np.testing.assert_array_equal(cols, gold["cols"])
+    if bf_radius is None:  # centroid of integer indices: exact
+        assert (info.center_row, info.center_col) == tuple(gold["center"])
+    else:  # weighted float32 centroid: summation order differs (a few ulps)
+        np.testing.assert_allclose((info.center_row, info.center_col), gold["center"], rtol=5e-7)
+    np.testing.assert_allclose(g[0], gold["kx_bf"], rtol=1e-6, atol=1e-7)
+    np.testing.assert_allclose(g[1], gold["ky_bf"], rtol=1e-6, atol=1e-7)
+    np.testing.assert_allclose(g[2], gold["alpha_k2"], rtol=1e-5, atol=1e-12)
+    # a centroid a few ulps apart turns the direction of pixels within ~0.1 px of
+    # the centre by up to ~1e-5 rad (where alpha^2 ~ 0 makes cos/sin 2phi moot)
+    angle_tol = 1e-6 if bf_radius is None else 5e-5
+    np.testing.assert_allclose(g[3], gold["cos2phi_k"], atol=angle_tol)
+    np.testing.assert_allclose(g[4], gold["sin2phi_k"], atol=angle_tol)
+    np.testing.assert_allclose(g[5], gold["aperture_k"], atol=1e-6)
+
+
+@pytest.mark.parametrize("threshold,bf_radius,rotation", [(0.0, None, 0.0), (0.0, 20.0, 0.3),
+                                                          (0.3, None, -1.1), (0.5, 24.0, 0.0)])
+def test_device_selection_matches_host_restatement(threshold, bf_radius, rotation):
+    """Device selection/geometry vs the host float32 restatement (64^2 detector)."""
+    from quantem.gpu_b200.calibration import select_bf
+    from quantem.gpu_b200.synthetic import CONFIGS, generate
+
+    spec = CONFIGS["plain_32x32_det64"]
+    data = generate(spec, DEV).counts.cpu().numpy()
+    det_sampling, semi = spec.det_sampling_mrad, spec.semiangle_mrad
+    lam = so.wavelength_angstrom(spec.voltage_kV)
+    det = data.shape[2:]
+    recip = det_sampling * 1e-3 / lam
+    sampling = (1.0 / (recip * det[0]), 1.0 / (recip * det[1]))
+    info, rows, cols, g, mean_dp, sums = _device_selection(
+        data, threshold, bf_radius, det_sampling, semi, lam, sampling, rotation)
+    sel = select_bf(mean_dp, threshold, bf_radius)
+    np.testing.assert_array_equal(rows, sel.rows)
+    np.testing.assert_array_equal(cols, sel.cols)
+    if bf_radius is None:
+        assert (info.center_row, info.center_col) == sel.center
+    else:  # FP64-accumulated vs pairwise float32 centroid: a few ulps
+        np.testing.assert_allclose((info.center_row, info.center_col), sel.center, rtol=5e-7)
+    assert info.radius == pytest.approx(sel.radius, rel=1e-15)
+    geo = bf_geometry(rows.astype(np.int32), cols.astype(np.int32),
+                      (info.center_row, info.center_col), det, sampling, lam, semi,
+                      (det_sampling, det_sampling), rotation)
+    host = geo.stacked()
+    for row in (0, 1, 2, 6, 7):  # per-op IEEE rounding on both sides: identical
+        np.testing.assert_array_equal(g[row], host[row])
+    np.testing.assert_allclose(g[3:6], host[3:6], atol=1e-6)  # atan2f/cosf/sinf ulps
+    s = sums.cpu().numpy().view(np.uint64).reshape(-1)
+    dc = float(s[rows * det[1] + cols].astype(np.float64).mean())
+    assert abs(info.dc_re - dc) <= 1e-14 * abs(dc) and info.dc_im == 0.0
+
+
+def test_device_selection_reports_empty_masks():
+    data = np.zeros((4, 4, 8, 8), np.uint16)
+    info, *_ = _device_selection(data, 0.0, None, 1.0, 20.0, 0.0197, (0.5, 0.5))
+    assert info.n_mask == 0 and info.n_bf == 0
+
+
 # ------------------------------------------------------------------ integer
 @pytest.mark.parametrize("shape", [(16, 16, 16, 16), (7, 9, 24, 40), (3, 5, 13, 11), (128, 128, 8, 8)])
 def test_mean_dp_is_bit_exact(shape):

@@ -59,6 +59,9 @@ def test_version_and_error_reporting_without_gpu():
     assert lib.qssb_mean_dp_u64(None, 10, 10, None, None, None) == _lib.QSSB_ERR_INVALID
     assert lib.qssb_gather_bf_columns(None, 1, 1, None, 1, None, None) == _lib.QSSB_ERR_INVALID
     assert lib.qssb_scan_fft_half(None, 1, 128, 128, None, None) == _lib.QSSB_ERR_INVALID
+    assert lib.qssb_select_bf(None, 128, 128, 10, 0.0, 0.0, None, None, None, None) == _lib.QSSB_ERR_INVALID
+    gp = _lib.GeometryParams(1.0, 1.0, 1.0, 0.0, 0.0197, 0.02, 1e-3, 1e-3)
+    assert lib.qssb_bf_geometry(None, None, 128, 128, 10, ctypes.byref(gp), None, None) == _lib.QSSB_ERR_INVALID
 
 
 def test_check_raises_with_message():
