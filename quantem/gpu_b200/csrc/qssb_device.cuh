@@ -298,10 +298,9 @@ __device__ __forceinline__ float soft_aperture_fast(float dx, float dy, float r2
         const float ac = dy * p.ang_c;
         edge = fmaf(num * r, rsqrtf(fmaf(ar, ar, ac * ac)), 0.5f);
     }
-    float a = fminf(fmaxf(edge, 0.0f), 1.0f);
-    a = r2 > 0.0f ? a : 1.0f;
+    float a = __saturatef(edge);          // clip to [0, 1]; NaN (r2 == 0) -> 0
     a = r2 >= p.outer2 ? 0.0f : a;
-    a = (p.inner2 > 0.0f && r2 <= p.inner2) ? 1.0f : a;
+    a = r2 <= p.inner2 ? 1.0f : a;        // inner2 >= 0, so r2 == 0 gives 1
     return a;
 }
 

@@ -189,6 +189,11 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
     float2* cneg = tw + 128;
     float2* delta = cneg + 64;
     __shared__ Probe sp;
+    // FP32-chi path: theta = 2 (q_row u + q_col v) is separable, so
+    // e^{i theta} = s_phr[r] * s_phc[c] from 256 sincos per BF pixel
+    constexpr bool kSep = QUAD && !CHI64;
+    __shared__ float2 s_phr[kSep ? 128 : 1];
+    __shared__ float2 s_phc[kSep ? 128 : 1];
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -206,6 +211,21 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
     __syncthreads();
     const Probe& p = sp;
     const float2* eqc = eq_table + (size_t)cand * N * N;
+    // e^{i 2 q_row(r) u}, e^{i 2 q_col(c) v} of BF pixel b, (u, v) = M k
+    auto fill_phase = [&](int b) {
+        if (tid < 256) {
+            const float kx = __ldg(geom + b);
+            const float ky = __ldg(geom + n_bf + b);
+            float sn, cs;
+            if (tid < 128) {
+                sincosf(2.0f * __ldg(q_row + tid) * fmaf(p.mxx, kx, p.mxy * ky), &sn, &cs);
+                s_phr[tid] = make_float2(cs, sn);
+            } else {
+                sincosf(2.0f * __ldg(q_col + tid - 128) * fmaf(p.mxy, kx, p.myy * ky), &sn, &cs);
+                s_phc[tid - 128] = make_float2(cs, sn);
+            }
+        }
+    };
     // the line (row or column) of this group within a round of 64
     const int line = (warp & 7) + 8 * grp + 32 * (warp >> 3);
     float acc[2][16];
@@ -217,6 +237,10 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
     int nb = n_bf - b0;
     if (nb > bf_per_chunk) nb = bf_per_chunk;
     const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
+    if constexpr (kSep) {
+        if (nb > 0) fill_phase(b0);
+        __syncthreads();
+    }
     for (int i = 0; i < nb; ++i) {
         const int b = b0 + i;
         const BFQuad kq = bf_quad(geom, n_bf, b, p);
@@ -238,7 +262,12 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
             const float2 gv = c <= 64 ? __ldg(gb + r * H + c)
                                       : cconj(__ldg(gb + ((N - r) & (N - 1)) * H + (N - c)));
             float2 v;
-            if constexpr (QUAD) {
+            if constexpr (kSep) {
+                const float2 lo = make_float2(kq.kx_lo, kq.ky_lo);
+                v = corrected_quad_e(__ldg(q_row + r), __ldg(q_col + c), r, c,
+                                     __ldg(eqc + r * N + c), kq.kx, kq.ky, kq.ak, &lo,
+                                     cmul(s_phr[r], s_phc[c]), gv, p);
+            } else if constexpr (QUAD) {
                 v = corrected_quad<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c,
                                           __ldg(eqc + r * N + c), kq, gv, p);
             } else {
@@ -253,6 +282,10 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
         }
         __syncthreads();
         if (tid >= 1 && tid < 64) delta[tid] = cadd(cconj(Hp[tid * kL128P + 64]), cneg[tid]);
+        // every thread is past A: the next BF pixel's phase rows can be written
+        if constexpr (kSep) {
+            if (i + 1 < nb) fill_phase(b + 1);
+        }
         __syncthreads();
         // B) row IFFTs of rows 0..63, then row 64
         {

@@ -247,17 +247,25 @@ __host__ __device__ constexpr int quad4_threads() {
     return N * (N / 8) + N + N / 2 - 1;
 }
 
-// Full N x N corrected-mean plane from the chunk partials.
+// Full N x N corrected-mean plane from the chunk partials. A block takes 32
+// frequencies; its 8 warps fold every 8th chunk each in FP64 and the 8 slice
+// sums are added in a fixed order: deterministic for a given plan.
+constexpr int kFoldSlices = 8;
+
 template <int N, bool SYM>
-__global__ void k_trotter_plane(const float2* __restrict__ partial, int n_chunks, int n_bf,
-                                float2 dc, float2* __restrict__ plane) {
+__global__ void __launch_bounds__(32 * kFoldSlices) k_trotter_plane(
+    const float2* __restrict__ partial, int n_chunks, int n_bf, float2 dc,
+    float2* __restrict__ plane) {
     constexpr int H = N / 2 + 1;
     constexpr int NQ = n_eval_q<N, SYM>();
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= N * N) return;
+    __shared__ double2 red[kFoldSlices][32];
+    const int ql = threadIdx.x & 31;
+    const int sl = threadIdx.x >> 5;
+    const int idx = blockIdx.x * 32 + ql;
+    const bool valid = idx < N * N;
     const int r = idx / N;
     const int c = idx - r * N;
-    int qi;
+    int qi = idx;
     bool mirror = false;
     if constexpr (SYM) {
         if (c <= N / 2) {
@@ -268,33 +276,28 @@ __global__ void k_trotter_plane(const float2* __restrict__ partial, int n_chunks
             qi = ((N - r) & (N - 1)) * H + (N - c);
             mirror = true;
         }
-    } else {
-        qi = idx;
     }
-    // eight independent FP64 lanes over the chunks (loads in flight
-    // together), folded in a fixed order: deterministic for a given plan
-    double lr[8], li[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) lr[j] = li[j] = 0.0;
-    int k = 0;
-    for (; k + 8 <= n_chunks; k += 8) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const float2 v = __ldg(partial + (size_t)(k + j) * NQ + qi);
-            lr[j] += (double)v.x;
-            li[j] += (double)v.y;
+    double sr = 0.0, si = 0.0;
+    if (valid) {
+#pragma unroll 4
+        for (int k = sl; k < n_chunks; k += kFoldSlices) {
+            const float2 v = __ldg(partial + (size_t)k * NQ + qi);
+            sr += (double)v.x;
+            si += (double)v.y;
         }
     }
-    for (; k < n_chunks; ++k) {
-        const float2 v = __ldg(partial + (size_t)k * NQ + qi);
-        lr[0] += (double)v.x;
-        li[0] += (double)v.y;
+    red[sl][ql] = make_double2(sr, si);
+    __syncthreads();
+    if (sl != 0 || !valid) return;
+    double tr = 0.0, ti = 0.0;
+#pragma unroll
+    for (int j = 0; j < kFoldSlices; ++j) {
+        tr += red[j][ql].x;
+        ti += red[j][ql].y;
     }
-    const double sr = ((lr[0] + lr[1]) + (lr[2] + lr[3])) + ((lr[4] + lr[5]) + (lr[6] + lr[7]));
-    const double si = ((li[0] + li[1]) + (li[2] + li[3])) + ((li[4] + li[5]) + (li[6] + li[7]));
     const double inv_b = 1.0 / (double)n_bf;
     // S(-q) = -conj(S(q)): real part flips, imaginary part stays
-    float2 out = make_float2((float)((mirror ? -sr : sr) * inv_b), (float)(si * inv_b));
+    float2 out = make_float2((float)((mirror ? -tr : tr) * inv_b), (float)(ti * inv_b));
     if (r == 0 && c == 0) out = dc;
     plane[idx] = out;
 }
@@ -408,7 +411,7 @@ static int launch_object(const float* g_half, const float* geom, const float* q_
             pl.bf_per_chunk, partial);
     }
     CUDA_TRY(cudaGetLastError());
-    k_trotter_plane<N, SYM><<<(N * N + 127) / 128, 128, 0, s>>>(
+    k_trotter_plane<N, SYM><<<(N * N + 31) / 32, 32 * kFoldSlices, 0, s>>>(
         partial, pl.n_chunks, cal.n_bf, make_float2((float)cal.dc_re, (float)cal.dc_im), plane);
     CUDA_TRY(cudaGetLastError());
     k_ifft_rows<N><<<N / 8, 256, 0, s>>>(plane);

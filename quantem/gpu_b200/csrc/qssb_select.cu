@@ -29,25 +29,6 @@ __device__ __forceinline__ T warp_sum(T v) {
     return v;
 }
 
-// Block-wide sum in a fixed order (lane tree, then warp tree); every thread
-// gets the result.
-template <typename T>
-__device__ T block_sum(T v, T* sh) {
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5;
-    v = warp_sum(v);
-    __syncthreads();
-    if (lane == 0) sh[warp] = v;
-    __syncthreads();
-    if (warp == 0) {
-        T x = lane < (int)(blockDim.x >> 5) ? sh[lane] : T(0);
-        x = warp_sum(x);
-        if (lane == 0) sh[0] = x;
-    }
-    __syncthreads();
-    return sh[0];
-}
-
 __device__ float block_max(float v, float* sh) {
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
@@ -70,156 +51,190 @@ __device__ __forceinline__ float mean_at(const unsigned long long* sums, int i, 
     return __fdiv_rn(__ull2float_rn(sums[i]), n_frames_f);
 }
 
-// One CTA. Each thread owns the contiguous pixel segment [t*seg, (t+1)*seg)
-// so the compaction below keeps row-major (np.nonzero) order.
+// Sums NV values over the block at once (one pass of barriers); every thread
+// gets the results in v. Fixed order: lane tree, then warp tree.
+template <typename T, int NV>
+__device__ void block_sums(T (&v)[NV], T* sh /* [NV][32] */) {
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] = warp_sum(v[j]);
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int j = 0; j < NV; ++j) sh[j * 32 + warp] = v[j];
+    }
+    __syncthreads();
+    if (warp < NV) {
+        T x = lane < (int)(blockDim.x >> 5) ? sh[warp * 32 + lane] : T(0);
+        x = warp_sum(x);
+        if (lane == 0) sh[warp * 32] = x;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < NV; ++j) v[j] = sh[j * 32];
+}
+
+// Mean patterns up to this many pixels are cached in shared memory.
+constexpr int kSelSmemPixels = 16384;
+
+// One CTA of 32 warps. Warp w owns the contiguous pixel range
+// [w*S, (w+1)*S), S a multiple of 32, read 32 consecutive pixels at a time:
+// loads are coalesced and the ballot compaction keeps row-major
+// (np.nonzero) order.
 __global__ void __launch_bounds__(kSelThreads) k_select_bf(
     const unsigned long long* __restrict__ sums, int k0, int k1, float n_frames_f,
     float threshold, float bf_radius, float* __restrict__ mean_dp,
     int32_t* __restrict__ bf_linear, qssb_bf_info_t* __restrict__ info) {
-    __shared__ double sh_d[32];
+    extern __shared__ float s_m[];  // [npix] when npix <= kSelSmemPixels
+    __shared__ double sh_d[4 * 32];
     __shared__ float sh_f[32];
-    __shared__ long long sh_l[32];
+    __shared__ long long sh_l[4 * 32];
     __shared__ unsigned long long sh_u[32];
     __shared__ int s_off[kSelThreads / 32];
-    const int tid = threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     const int npix = k0 * k1;
-    const int seg = (npix + kSelThreads - 1) / kSelThreads;
-    const int p0 = tid * seg;
-    const int p1 = min(p0 + seg, npix);
+    const bool cached = npix <= kSelSmemPixels;
+    const int span = ((npix + 32 * 32 - 1) / (32 * 32)) * 32;  // pixels per warp
+    const int base = warp * span;
+    const int end = min(base + span, npix);
+    const float inv_k1 = 1.0f / (float)k1;
+    // exact for npix <= 2^20: (i + 0.5) / k1 is >= 0.5 / k1 away from an integer
+#define QSSB_ROW(i) __float2int_rz(((float)(i) + 0.5f) * inv_k1)
+#define QSSB_VAL(i) (cached ? s_m[i] : mean_at(sums, (i), n_frames_f))
 
-    // mean pattern, its maximum and mean
+    // pass 1: mean pattern, its maximum and mean
     float vmax = -INFINITY;
-    double vsum = 0.0;
-    for (int i = p0; i < p1; ++i) {
+    double vsum[1] = {0.0};
+    for (int i = base + lane; i < end; i += 32) {
         const float m = mean_at(sums, i, n_frames_f);
+        if (cached) s_m[i] = m;
         if (mean_dp) mean_dp[i] = m;
         vmax = fmaxf(vmax, m);
-        vsum += (double)m;
+        vsum[0] += (double)m;
     }
     vmax = block_max(vmax, sh_f);
-    vsum = block_sum(vsum, sh_d);
-    const float mean_f = (float)(vsum / (double)npix);
+    block_sums(vsum, sh_d);
+    const float mean_f = (float)(vsum[0] / (double)npix);
     const float thr = __fmul_rn(vmax, threshold);
+    const bool auto_radius = !(bf_radius > 0.0f);
 
-    // intensity mask (dp > max * threshold)
-    long long n_mask = 0;
-    for (int i = p0; i < p1; ++i) n_mask += mean_at(sums, i, n_frames_f) > thr;
-    n_mask = block_sum(n_mask, sh_l);
+    // pass 2: mask count, variance (auto radius) or weighted centroid sums
+    double dsum[3] = {0.0, 0.0, 0.0};   // auto: v2 | explicit: w, w*row, w*col
+    long long lsum[3] = {0, 0, 0};      // n_mask, sum row, sum col (explicit)
+    for (int i = base + lane; i < end; i += 32) {
+        const float m = QSSB_VAL(i);
+        const bool in_mask = m > thr;
+        lsum[0] += in_mask;
+        if (auto_radius) {
+            const float d = __fsub_rn(m, mean_f);
+            dsum[0] += (double)__fmul_rn(d, d);
+        } else if (in_mask) {
+            const int row = QSSB_ROW(i);
+            const int col = i - row * k1;
+            dsum[0] += (double)m;
+            dsum[1] += (double)__fmul_rn((float)row, m);
+            dsum[2] += (double)__fmul_rn((float)col, m);
+            lsum[1] += row;
+            lsum[2] += col;
+        }
+    }
+    block_sums(dsum, sh_d);
+    block_sums(lsum, sh_l);
+    const long long n_mask = lsum[0];
 
     float cr, cc;  // selection centre (float32 values)
     double radius;
-    if (!(bf_radius > 0.0f)) {
+    if (auto_radius) {
         // probe disk: dp > mean + std; centre = its centroid, radius = sqrt(|disk| / pi)
-        double v2 = 0.0;
-        for (int i = p0; i < p1; ++i) {
-            const float d = __fsub_rn(mean_at(sums, i, n_frames_f), mean_f);
-            v2 += (double)__fmul_rn(d, d);
-        }
-        v2 = block_sum(v2, sh_d);
-        const float std_f = __fsqrt_rn((float)(v2 / (double)npix));
+        const float std_f = __fsqrt_rn((float)(dsum[0] / (double)npix));
         const float pthr = __fadd_rn(mean_f, std_f);
-        long long cnt = 0, sr = 0, sc = 0;
-        for (int i = p0; i < p1; ++i) {
-            if (mean_at(sums, i, n_frames_f) > pthr) {
-                ++cnt;
-                sr += i / k1;
-                sc += i % k1;
+        long long c3[3] = {0, 0, 0};
+        for (int i = base + lane; i < end; i += 32) {
+            if (QSSB_VAL(i) > pthr) {
+                const int row = QSSB_ROW(i);
+                c3[0] += 1;
+                c3[1] += row;
+                c3[2] += i - row * k1;
             }
         }
-        cnt = block_sum(cnt, sh_l);
-        sr = block_sum(sr, sh_l);
-        sc = block_sum(sc, sh_l);
-        if (cnt > 0) {
-            cr = __fdiv_rn((float)sr, (float)cnt);
-            cc = __fdiv_rn((float)sc, (float)cnt);
-            radius = sqrt((double)cnt / 3.14159265358979323846);
+        block_sums(c3, sh_l);
+        if (c3[0] > 0) {
+            cr = __fdiv_rn((float)c3[1], (float)c3[0]);
+            cc = __fdiv_rn((float)c3[2], (float)c3[0]);
+            radius = sqrt((double)c3[0] / 3.14159265358979323846);
         } else {
             cr = (float)(k0 / 2.0);
             cc = (float)(k1 / 2.0);
             radius = (double)min(k0, k1) * 0.25;
         }
     } else {
-        // explicit radius: intensity-weighted centroid of the mask
-        double w = 0.0, wr = 0.0, wc = 0.0;
-        long long nr = 0, nc = 0;
-        for (int i = p0; i < p1; ++i) {
-            const float m = mean_at(sums, i, n_frames_f);
-            if (m > thr) {
-                w += (double)m;
-                wr += (double)__fmul_rn((float)(i / k1), m);
-                wc += (double)__fmul_rn((float)(i % k1), m);
-                nr += i / k1;
-                nc += i % k1;
-            }
-        }
-        w = block_sum(w, sh_d);
-        wr = block_sum(wr, sh_d);
-        wc = block_sum(wc, sh_d);
-        nr = block_sum(nr, sh_l);
-        nc = block_sum(nc, sh_l);
-        const float wf = (float)w;
+        const float wf = (float)dsum[0];
         if (wf > 0.0f) {
-            cr = __fdiv_rn((float)wr, wf);
-            cc = __fdiv_rn((float)wc, wf);
+            cr = __fdiv_rn((float)dsum[1], wf);
+            cc = __fdiv_rn((float)dsum[2], wf);
         } else {
-            cr = (float)((double)nr / (double)max(n_mask, 1LL));
-            cc = (float)((double)nc / (double)max(n_mask, 1LL));
+            cr = (float)((double)lsum[1] / (double)max(n_mask, 1LL));
+            cc = (float)((double)lsum[2] / (double)max(n_mask, 1LL));
         }
         radius = (double)bf_radius;
     }
     const float r2 = (float)(radius * radius);
 
-    // keep = mask && (row - cr)^2 + (col - cc)^2 <= r^2, compacted in order
-    int mine = 0;
-    for (int i = p0; i < p1; ++i) {
-        const float dr = __fsub_rn((float)(i / k1), cr);
-        const float dc = __fsub_rn((float)(i % k1), cc);
+    // pass 3: keep = mask && (row - cr)^2 + (col - cc)^2 <= r^2; each warp
+    // counts its kept pixels, an exclusive scan over the warps gives their
+    // offsets, then every warp writes its pixels in order
+    auto keep = [&](int i) -> bool {
+        const int row = QSSB_ROW(i);
+        const float dr = __fsub_rn((float)row, cr);
+        const float dc = __fsub_rn((float)(i - row * k1), cc);
         const float d2 = __fadd_rn(__fmul_rn(dr, dr), __fmul_rn(dc, dc));
-        mine += (mean_at(sums, i, n_frames_f) > thr) && (d2 <= r2);
+        return (QSSB_VAL(i) > thr) && (d2 <= r2);
+    };
+    int count = 0;
+    for (int i0 = base; i0 < end; i0 += 32) {
+        const int i = i0 + lane;
+        count += __popc(__ballot_sync(0xffffffffu, i < end && keep(i)));
     }
-    // exclusive scan of `mine` over the block
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
-    int incl = mine;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    if (lane == 31) s_off[warp] = incl;
+    if (lane == 0) s_off[warp] = count;
     __syncthreads();
     if (warp == 0) {
-        const int x = lane < kSelThreads / 32 ? s_off[lane] : 0;
+        const int x = s_off[lane];
         int xi = x;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, xi, o);
             if (lane >= o) xi += y;
         }
-        if (lane < kSelThreads / 32) s_off[lane] = xi - x;
+        s_off[lane] = xi - x;
+        if (lane == 31) sh_l[0] = xi;  // total, read after the barrier
     }
     __syncthreads();
-    int pos = s_off[warp] + incl - mine;
-    unsigned long long dc_sum = 0;
-    for (int i = p0; i < p1; ++i) {
-        const float dr = __fsub_rn((float)(i / k1), cr);
-        const float dc = __fsub_rn((float)(i % k1), cc);
-        const float d2 = __fadd_rn(__fmul_rn(dr, dr), __fmul_rn(dc, dc));
-        if ((mean_at(sums, i, n_frames_f) > thr) && (d2 <= r2)) {
-            bf_linear[pos++] = i;
-            dc_sum += sums[i];
+    const int n_bf = (int)sh_l[0];
+    int pos = s_off[warp];
+    unsigned long long dc_sum[1] = {0};
+    for (int i0 = base; i0 < end; i0 += 32) {
+        const int i = i0 + lane;
+        const bool k = i < end && keep(i);
+        const unsigned ball = __ballot_sync(0xffffffffu, k);
+        if (k) {
+            bf_linear[pos + __popc(ball & ((1u << lane) - 1u))] = i;
+            dc_sum[0] += sums[i];
         }
+        pos += __popc(ball);
     }
-    dc_sum = block_sum(dc_sum, sh_u);
-    const int n_bf = (int)block_sum((long long)mine, sh_l);
-    if (tid == 0) {
+#undef QSSB_ROW
+#undef QSSB_VAL
+    block_sums(dc_sum, sh_u);
+    if (threadIdx.x == 0) {
         info->n_bf = n_bf;
         info->n_mask = (int32_t)n_mask;
         info->center_row = (double)cr;
         info->center_col = (double)cc;
         info->radius = radius;
         // dc = mean over the selected pixels of G_b(0,0) = sum over frames (exact integers)
-        info->dc_re = n_bf > 0 ? (double)dc_sum / (double)n_bf : 0.0;
+        info->dc_re = n_bf > 0 ? (double)dc_sum[0] / (double)n_bf : 0.0;
         info->dc_im = 0.0;
     }
 }
@@ -287,7 +302,11 @@ extern "C" int qssb_select_bf(const uint64_t* sums, int32_t det_rows, int32_t de
         return set_error(QSSB_ERR_INVALID, "qssb_select_bf: threshold and radius must be finite");
     if (((uintptr_t)sums & 7u) != 0 || ((uintptr_t)info & 7u) != 0)
         return set_error(QSSB_ERR_INVALID, "qssb_select_bf: sums and info must be 8-byte aligned");
-    k_select_bf<<<1, kSelThreads, 0, (cudaStream_t)stream>>>(
+    const int npix = det_rows * det_cols;
+    const size_t smem = npix <= kSelSmemPixels ? sizeof(float) * (size_t)npix : 0;
+    CUDA_TRY(cudaFuncSetAttribute(k_select_bf, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(float) * kSelSmemPixels)));
+    k_select_bf<<<1, kSelThreads, smem, (cudaStream_t)stream>>>(
         reinterpret_cast<const unsigned long long*>(sums), det_rows, det_cols, (float)n_frames,
         threshold, bf_radius, mean_dp, bf_linear, info);
     CUDA_TRY(cudaGetLastError());
