@@ -171,6 +171,53 @@ def cpu_baseline(counts_host: np.ndarray, budget_s: float = 15.0) -> dict:
             "sample": f"{n} full 128^4 reconstructions (all BF pixels) of the same workload"}
 
 
+def reference_cuda_baseline(counts: torch.Tensor, be, steps: int, warmup: int) -> dict:
+    """The reference's own 128x128 object kernels (built from its CUDA sources
+    into oracle/_ref/) timed on this GPU beside ours: warm object redraws from
+    the same resident G, and cold reconstructions with its G construction
+    replayed through torch's gather/cuFFT (its CuPy steps)."""
+    from oracle.ref_cuda import build_ref
+
+    if not build_ref.available():
+        return {"unavailable": "oracle/_ref/ssb_fft128.cubin not built (needs the reference tree)"}
+    from oracle.ref_cuda.harness import ReferenceObject128, reference_cold_object
+
+    dev = counts.device
+    stream = torch.cuda.current_stream(dev)
+    ref = ReferenceObject128(dev)
+    semi = KW["semiangle"] * 1e-3
+    ang = KW["det_sampling"] * 1e-3
+    wargs = (be.G_qk, be._geom_dev, be._q_row, be._q_col, be.wavelength, semi, ang, ang)
+
+    def timed(fn, n):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(n):
+            fn()
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        return s.elapsed_time(e) / n
+
+    warm_ms = timed(lambda: torch.angle(ref.object(*wargs, 10.0, 5.0, 0.1, be.dc_value)), steps)
+    cold = dict(wavelength=be.wavelength, semiangle_mrad=KW["semiangle"],
+                det_sampling_mrad=KW["det_sampling"], scan_sampling_A=KW["scan_sampling"],
+                C10=0.0, C12=0.0, phi12=0.0)
+    cold_ms = timed(lambda: reference_cold_object(counts, ref, **cold), max(3, steps // 4))
+    ref_obj = ref.object(*wargs, 0.0, 0.0, 0.0, be.dc_value)
+    our_obj, _ = be.object_and_phase(0.0, 0.0, 0.0)
+    d = torch.angle(our_obj * torch.conj(ref_obj)).double()
+    return {
+        "warm_recon_per_s": 1e3 / warm_ms, "cold_recon_per_s": 1e3 / cold_ms,
+        "phase_rms_rad_vs_ours": float(torch.sqrt(torch.mean(d * d))),
+        "kind": "reference CUDA kernels ifft128_rows_fused_pk_t32_mr8_packed + ifft128_cols_t32_mr8 "
+                "(its sources, its nvrtc options, sm_100a; oracle/_ref) with its gather/cuFFT/mean "
+                "steps as torch library calls",
+    }
+
+
 def run_reference(args, world, rank) -> None:
     if rank != 0:
         return
@@ -296,8 +343,8 @@ def run_b200(args, world, rank, local) -> None:
     alg = {  # algorithmic bytes per launch of each entry point
         "qssb_mean_dp_u64": (2 * n_r * k2, "k_sum_frames_vec8"),
         "qssb_gather_bf_columns": (4 * n_r * n_bf, "k_gather_columns"),
-        "qssb_scan_fft_half": (2 * n_r * n_bf + 8 * n_bf * half, "k_scan_fft_half"),
-        "qssb_object": (8 * n_bf * half + 12 * 128 * 128, "k_trotter_partial"),
+        "qssb_scan_fft_half": (2 * n_r * n_bf + 8 * n_bf * half, "k_scan_fft128"),
+        "qssb_object": (8 * n_bf * half + 12 * 128 * 128, "k_trotter_quad4"),
     }
     stage_ms = {k: float(np.mean(v)) for k, v in per_op.items()}
     rooflines = {}
@@ -331,6 +378,13 @@ def run_b200(args, world, rank, local) -> None:
                 "d2h_bytes_per_step": d2h, "api": "SSB.from_array(pinned host u16).reconstruct()"},
         "clocks": clock_info,
     }
+    if world == 1 and not args.no_reference_cuda:
+        rc = reference_cuda_baseline(counts, be, min(args.steps, 20), 3)
+        line["reference_cuda"] = rc
+        if "cold_recon_per_s" in rc:
+            line["speedup_vs_reference_cuda"] = {
+                "cold": value / rc["cold_recon_per_s"],
+                "warm": line["warm_recon_per_s"] / rc["warm_recon_per_s"]}
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(counts.cpu().numpy())
     if world == 1 and not args.no_oracle:
@@ -372,6 +426,8 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-oracle", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true",
+                    help="skip timing the reference's own CUDA object kernels")
     ap.add_argument("--profile-once", action="store_true",
                     help="run the untimed launch sequence used for ncu captures")
     args = ap.parse_args()

@@ -1,0 +1,101 @@
+"""Compile the reference's 128x128 SSB CUDA module into oracle/_ref/.
+
+Run in the build container, where the reference tree exists:
+
+    python -m oracle.ref_cuda.build_ref [--reference /root/reference]
+
+Reads the CUDA source strings of
+``src/quantem/gpu/ssb/compute/cuda/kernels/common.py`` (``_DEVICE_FUNCTIONS_CUDA``)
+and ``.../fft128.py`` (``_TWIDDLE_DECL``, ``_FFT128_KERNELS``) with ``ast``
+(the modules import CuPy, so they are not imported), assembles them as
+``build_cuda_code`` does (common.py:620-622) in a temporary directory, and
+compiles with the reference's NVRTC options (common.py:708: c++11, fast math,
+96 registers, -dlcm=ca) for sm_100a. Only the cubin and a manifest are written
+under ``oracle/_ref/``; no reference source is kept.
+"""
+from __future__ import annotations
+
+import argparse
+import ast
+import hashlib
+import json
+import shutil
+import subprocess
+import tempfile
+from pathlib import Path
+
+ORACLE = Path(__file__).resolve().parents[1]
+OUT_DIR = ORACLE / "_ref"
+CUBIN = OUT_DIR / "ssb_fft128.cubin"
+MANIFEST = OUT_DIR / "ssb_fft128.json"
+KERNELS_REL = Path("src/quantem/gpu/ssb/compute/cuda/kernels")
+DEFAULT_REFERENCE = Path("/root/reference")
+KERNEL_NAMES = ("ifft128_rows_fused_pk_t32_mr8_packed", "ifft128_cols_t32_mr8")
+TWIDDLE_NAME = "TWIDDLE_128"
+
+
+def _string_constants(path: Path, names: set[str]) -> dict[str, str]:
+    tree = ast.parse(path.read_text())
+    found = {}
+    for node in tree.body:
+        if isinstance(node, ast.Assign) and len(node.targets) == 1:
+            tgt = node.targets[0]
+            if isinstance(tgt, ast.Name) and tgt.id in names and isinstance(node.value, ast.Constant) \
+                    and isinstance(node.value.value, str):
+                found[tgt.id] = node.value.value
+    missing = names - set(found)
+    if missing:
+        raise RuntimeError(f"{path}: string constants not found: {sorted(missing)}")
+    return found
+
+
+def module_source(reference: Path) -> str:
+    """The CUDA module text the reference's CustomFFT128 hands to NVRTC."""
+    kdir = reference / KERNELS_REL
+    common = _string_constants(kdir / "common.py", {"_DEVICE_FUNCTIONS_CUDA"})
+    fft = _string_constants(kdir / "fft128.py", {"_TWIDDLE_DECL", "_FFT128_KERNELS"})
+    return ('extern "C" {\n' + fft["_TWIDDLE_DECL"] + "\n" + common["_DEVICE_FUNCTIONS_CUDA"]
+            + "\n" + fft["_FFT128_KERNELS"] + "\n}")
+
+
+def available() -> bool:
+    return CUBIN.exists() and MANIFEST.exists()
+
+
+def build(reference: Path = DEFAULT_REFERENCE, force: bool = False, verbose: bool = False) -> Path | None:
+    """Compile the cubin; returns its path, or None when the reference tree is absent."""
+    if not (reference / KERNELS_REL / "fft128.py").exists():
+        return CUBIN if available() else None
+    src = module_source(reference)
+    digest = hashlib.sha256(src.encode()).hexdigest()
+    if not force and available():
+        if json.loads(MANIFEST.read_text()).get("source_sha256") == digest:
+            return CUBIN
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    OUT_DIR.mkdir(parents=True, exist_ok=True)
+    with tempfile.TemporaryDirectory() as td:
+        cu = Path(td) / "ssb_fft128.cu"
+        cu.write_text(src)
+        cmd = [nvcc, "-cubin", "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++11",
+               "--use_fast_math", "-maxrregcount=96", "-Xptxas", "-dlcm=ca",
+               "-o", str(CUBIN) + ".tmp", str(cu)]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    Path(str(CUBIN) + ".tmp").replace(CUBIN)
+    MANIFEST.write_text(json.dumps({
+        "source_sha256": digest,
+        "reference_files": [str(KERNELS_REL / "common.py"), str(KERNELS_REL / "fft128.py")],
+        "options": "nvcc -cubin sm_100a -std=c++11 --use_fast_math -maxrregcount=96 -Xptxas -dlcm=ca",
+        "kernels": list(KERNEL_NAMES),
+        "twiddle": TWIDDLE_NAME,
+    }, indent=1))
+    return CUBIN
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--reference", type=Path, default=DEFAULT_REFERENCE)
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    print(build(a.reference, force=a.force, verbose=True))

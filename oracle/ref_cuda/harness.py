@@ -1,0 +1,142 @@
+"""Launch the reference's own 128x128 SSB object kernels (checker and baseline).
+
+Test infrastructure: imported only by tests/ and by bench.py's baseline legs.
+The kernels come from ``oracle/_ref/ssb_fft128.cubin`` (built by
+``build_ref.py`` from the reference's sources); this file holds only the
+launch sequence of ``SSBEngine._run_correction_pipeline`` (engine.py:934-971)
+and ``CustomFFTBase.ifft2_inplace_fused_pk`` (common.py:768-816), and the
+restated pk element-wise kernel (engine.py:217-231).
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from .build_ref import CUBIN, KERNEL_NAMES, TWIDDLE_NAME, available
+
+N = 128
+
+
+def _check(res):
+    err = res[0] if isinstance(res, tuple) else res
+    if int(err) != 0:
+        raise RuntimeError(f"CUDA driver call failed: {err}")
+    return res[1:] if isinstance(res, tuple) and len(res) > 1 else None
+
+
+class ReferenceObject128:
+    """The reference's per-BF fused IFFT object path for 128x128 scans."""
+
+    def __init__(self, device: torch.device | str = "cuda:0"):
+        if not available():
+            raise FileNotFoundError(f"{CUBIN} is missing: run python -m oracle.ref_cuda.build_ref")
+        from cuda.bindings import driver as cu
+
+        self.cu = cu
+        self.device = torch.device(device)
+        torch.cuda.set_device(self.device)
+        torch.zeros(1, device=self.device)  # make torch's primary context current
+        (self.module,) = _check(cu.cuModuleLoad(str(CUBIN).encode()))
+        (self.rows,) = _check(cu.cuModuleGetFunction(self.module, KERNEL_NAMES[0].encode()))
+        (self.cols,) = _check(cu.cuModuleGetFunction(self.module, KERNEL_NAMES[1].encode()))
+        dptr, nbytes = _check(cu.cuModuleGetGlobal(self.module, TWIDDLE_NAME.encode()))
+        # CustomFFTBase._init_twiddles (common.py:725-730): exp(+2 pi i n / N), complex64
+        w = np.exp(2j * math.pi * np.arange(N) / N).astype(np.complex64)
+        assert int(nbytes) == w.nbytes
+        tw = torch.from_numpy(w.view(np.float32)).to(self.device)
+        torch.cuda.synchronize(self.device)
+        _check(cu.cuMemcpyDtoD(dptr, cu.CUdeviceptr(tw.data_ptr()), w.nbytes))
+        self._buf: torch.Tensor | None = None
+
+    @staticmethod
+    def pk(geom: torch.Tensor, C10: float, C12: float, phi12: float, factor: float) -> torch.Tensor:
+        """pk = A(k) exp(-i chi(k)) per BF pixel: the reference's _pk_kernel
+        (engine.py:217-231) restated with torch float32 operations."""
+        alpha2, c2, s2, ap = geom[2], geom[3], geom[4], geom[5]
+        cos_term = c2 * np.float32(math.cos(2 * phi12)) + s2 * np.float32(math.sin(2 * phi12))
+        chi = np.float32(factor) * alpha2 * (np.float32(C12) * cos_term + np.float32(C10))
+        return torch.complex(ap * torch.cos(chi), -ap * torch.sin(chi))
+
+    def _launch(self, fn, grid, block, args, stream) -> None:
+        values = tuple(a[0] for a in args)
+        types = tuple(a[1] for a in args)
+        _check(self.cu.cuLaunchKernel(fn, *grid, *block, 0, stream, (values, types), 0))
+
+    def corrected_images(self, g_half: torch.Tensor, geom: torch.Tensor, q_row: torch.Tensor,
+                         q_col: torch.Tensor, wavelength: float, semiangle_rad: float,
+                         ang_y_rad: float, ang_x_rad: float, C10: float, C12: float,
+                         phi12: float, dc: complex) -> torch.Tensor:
+        """[B, 128, 128] corrected BF images O_b (rows kernel + columns kernel)."""
+        n_bf = int(g_half.shape[0])
+        assert g_half.shape == (n_bf, N, N // 2 + 1) and g_half.dtype == torch.complex64
+        assert geom.shape[0] >= 6 and geom.shape[1] == n_bf and n_bf * N * N < 2 ** 31
+        g_half = g_half.contiguous()
+        factor = math.pi / wavelength
+        pk = self.pk(geom, C10, C12, phi12, factor).contiguous()
+        kx = geom[0].contiguous()
+        ky = geom[1].contiguous()
+        if self._buf is None or self._buf.shape[0] != n_bf:
+            self._buf = torch.empty((n_bf, N, N), dtype=torch.complex64, device=self.device)
+        out = self._buf
+        stream = self.cu.CUstream(torch.cuda.current_stream(self.device).cuda_stream)
+        P, F, I = ctypes.c_void_p, ctypes.c_float, ctypes.c_int
+        f32 = lambda x: float(np.float32(x))  # noqa: E731  (np.float32 kernel arguments)
+        args = [(kx.data_ptr(), P), (ky.data_ptr(), P), (q_row.data_ptr(), P), (q_col.data_ptr(), P),
+                (f32(wavelength), F), (f32(semiangle_rad), F), (f32(ang_y_rad), F),
+                (f32(ang_x_rad), F), (f32(C10), F), (f32(C12), F),
+                (f32(math.cos(2.0 * phi12)), F), (f32(math.sin(2.0 * phi12)), F), (f32(factor), F),
+                (pk.data_ptr(), P), (g_half.data_ptr(), P), (out.data_ptr(), P),
+                (f32(dc.real), F), (f32(dc.imag), F), (n_bf, I), (N // 2 + 1, I)]
+        # grids of ifft2_inplace_fused_pk: (1, 16, B) x (32, 8, 1), both kernels
+        self._launch(self.rows, (1, 16, n_bf), (32, 8, 1), args, stream)
+        self._launch(self.cols, (1, 16, n_bf), (32, 8, 1),
+                     [(out.data_ptr(), P), (n_bf, I), (f32(1.0 / (N * N)), F)], stream)
+        return out
+
+    def object(self, *args, **kw) -> torch.Tensor:
+        """reconstruct_object for B > 1024 (engine.py:1148-1151): mean over BF pixels."""
+        return self.corrected_images(*args, **kw).mean(dim=0)
+
+
+def reference_cold_object(counts: torch.Tensor, ref: ReferenceObject128, *, wavelength: float,
+                          semiangle_mrad: float, det_sampling_mrad: float,
+                          scan_sampling_A: float, C10: float, C12: float, phi12: float,
+                          threshold: float = 0.0, bf_radius=None):
+    """One cold reconstruction the way CudaSSBBackend + SSBEngine do it for a
+    128^4 u16 device tensor: u64 frame sums and float32 mean
+    (backend.py:432-441, torch.sum standing in for CuPy's reduction), the BF
+    selection and the rotation cache (host restatements of backend.py:448-518
+    and engine.py:784-830, which the reference evaluates with CuPy and host
+    syncs), the gather / transpose / complex64 cast / cuFFT fft2 / half-plane
+    slice / dc of _extract_gqk (backend.py:520-589) as torch library calls,
+    then the reference's own object kernels. Returns (object, phase, n_bf)."""
+    from quantem.gpu_b200.calibration import bf_geometry, scan_frequencies, select_bf
+
+    r0, r1, k0, k1 = (int(s) for s in counts.shape)
+    assert r0 == r1 == N
+    frames = counts.reshape(-1, k0, k1)
+    sums = frames.sum(dim=0, dtype=torch.int64)
+    mean_dp = sums.to(torch.float32) / float(frames.shape[0])
+    sel = select_bf(mean_dp.cpu().numpy(), threshold, bf_radius)
+    rows = torch.as_tensor(sel.rows, device=counts.device, dtype=torch.int64)
+    cols = torch.as_tensor(sel.cols, device=counts.device, dtype=torch.int64)
+    n_bf = int(rows.numel())
+    # torch's CUDA gather has no uint16 kernel: gather the same bits as int16
+    vbf = frames.view(torch.int16)[:, rows, cols]                 # [N_R, B]
+    vbf_int = vbf.T.reshape(n_bf, r0, r1).contiguous()
+    vbf_c = (vbf_int.to(torch.int32) & 0xFFFF).to(torch.complex64)
+    g_half = torch.fft.fft2(vbf_c)[:, :, : r1 // 2 + 1].contiguous()
+    dc = complex(g_half[:, 0, 0].mean().item())
+    recip = det_sampling_mrad * 1e-3 / wavelength
+    sampling = (1.0 / (recip * k0), 1.0 / (recip * k1))
+    geo = bf_geometry(sel.rows, sel.cols, sel.center, (k0, k1), sampling, wavelength,
+                      semiangle_mrad, (det_sampling_mrad, det_sampling_mrad), 0.0)
+    geom = torch.as_tensor(geo.stacked(), device=counts.device)
+    q_row, q_col = (torch.as_tensor(q, device=counts.device)
+                    for q in scan_frequencies((r0, r1), (scan_sampling_A, scan_sampling_A)))
+    obj = ref.object(g_half, geom, q_row, q_col, wavelength, semiangle_mrad * 1e-3,
+                     det_sampling_mrad * 1e-3, det_sampling_mrad * 1e-3, C10, C12, phi12, dc)
+    return obj, torch.angle(obj), n_bf
