@@ -45,7 +45,7 @@ from .optimizer import batch_nelder_mead, batch_sweep, search_box
 from .physics import electron_wavelength_angstrom
 from .protocol import BrightfieldDisk, SSBExportState, SSBPrecision, SSBResult
 
-NATIVE_SCAN_SIZES = (128,)
+NATIVE_SCAN_SIZES = (128, 256)
 LOSS_SCAN_SIZES = (128,)
 
 

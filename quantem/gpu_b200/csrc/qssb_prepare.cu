@@ -351,6 +351,77 @@ extern "C" int qssb_gather_bf_columns(const uint16_t* counts, int64_t n_frames, 
     return QSSB_OK;
 }
 
+// ------------------------------------------------- 256 x 256 scan FFT
+// The 256^2 half plane (264 KB per BF image) does not fit one CTA's shared
+// memory, so the transform is two passes through G itself:
+//   k_scan_rows256: rows 2j, 2j+1 of a BF image as one complex line (one warp
+//     per pair), forward FFT, split into the two real rows' spectra
+//     X_2j(c) = (Z(c) + conj Z(-c)) / 2, X_2j+1(c) = (Z(c) - conj Z(-c)) / 2i,
+//     c = 0..128, written to G[b][row][c];
+//   k_scan_cols256: 16 columns of G[b] staged in shared memory (pitch 257:
+//     the 16 columns of one row land on distinct banks), forward FFT of each
+//     column along the rows, written back in place.
+constexpr int kS256 = 256;
+constexpr int kS256H = kS256 / 2 + 1;
+constexpr int kS256ColTile = 16;
+
+__global__ void __launch_bounds__(256) k_scan_rows256(const uint16_t* __restrict__ columns,
+                                                      int n_bf, float2* __restrict__ g_half) {
+    __shared__ float2 tw[kS256];
+    __shared__ float2 line[8][kS256];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    fill_twiddles<kS256>(tw, tid, 256);
+    __syncthreads();
+    const int b = blockIdx.x;
+    const int pair = blockIdx.y * 8 + warp;  // 0 .. 127
+    if (b >= n_bf || pair >= kS256 / 2) return;
+    const uint16_t* img = columns + (size_t)b * kS256 * kS256;
+    const uint16_t* r0 = img + (size_t)(2 * pair) * kS256;
+    const uint16_t* r1 = r0 + kS256;
+    float2* x = line[warp];
+    for (int i = lane; i < kS256; i += 32) x[i] = make_float2((float)__ldg(r0 + i), (float)__ldg(r1 + i));
+    __syncwarp();
+    line_fft<kS256, -1>(x, 1, tw, lane);
+    float2* g0 = g_half + ((size_t)b * kS256 + 2 * pair) * kS256H;
+    float2* g1 = g0 + kS256H;
+    for (int c = lane; c < kS256H; c += 32) {
+        const float2 z = x[c];
+        const float2 m = x[(kS256 - c) & (kS256 - 1)];
+        g0[c] = make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y));
+        g1[c] = make_float2(0.5f * (z.y + m.y), -0.5f * (z.x - m.x));
+    }
+}
+
+__global__ void __launch_bounds__(256) k_scan_cols256(int n_bf, float2* __restrict__ g_half) {
+    constexpr int P = kS256 + 1;
+    __shared__ float2 tw[kS256];
+    __shared__ float2 tile[kS256ColTile * P];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    fill_twiddles<kS256>(tw, tid, 256);
+    const int b = blockIdx.x;
+    const int c0 = blockIdx.y * kS256ColTile;
+    const int nc = min(kS256ColTile, kS256H - c0);
+    if (b >= n_bf) return;  // uniform per block: before any barrier
+    float2* g = g_half + (size_t)b * kS256 * kS256H;
+    for (int e = tid; e < kS256 * kS256ColTile; e += 256) {
+        const int r = e / kS256ColTile;
+        const int c = e - r * kS256ColTile;
+        if (c < nc) tile[c * P + r] = g[(size_t)r * kS256H + c0 + c];
+    }
+    __syncthreads();
+    for (int c = warp; c < nc; c += 8) line_fft<kS256, -1>(tile + c * P, 1, tw, lane);
+    __syncthreads();
+    for (int e = tid; e < kS256 * kS256ColTile; e += 256) {
+        const int r = e / kS256ColTile;
+        const int c = e - r * kS256ColTile;
+        if (c < nc) g[(size_t)r * kS256H + c0 + c] = tile[c * P + r];
+    }
+}
+
 template <int N>
 static int launch_scan_fft(const uint16_t* columns, int n_bf, float* g_half, cudaStream_t s) {
     const size_t smem = ScanFftSmem<N>::bytes;
@@ -382,7 +453,17 @@ extern "C" int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t
             CUDA_TRY(cudaGetLastError());
             return QSSB_OK;
         }
+        case 256: {
+            k_scan_rows256<<<dim3(n_bf, kS256 / 2 / 8), 256, 0, s>>>(
+                columns, n_bf, reinterpret_cast<float2*>(g_half));
+            CUDA_TRY(cudaGetLastError());
+            k_scan_cols256<<<dim3(n_bf, (kS256H + kS256ColTile - 1) / kS256ColTile), 256, 0, s>>>(
+                n_bf, reinterpret_cast<float2*>(g_half));
+            CUDA_TRY(cudaGetLastError());
+            return QSSB_OK;
+        }
         default:
-            return set_error(QSSB_ERR_UNSUPPORTED, "qssb_scan_fft_half: scan size must be 64 or 128");
+            return set_error(QSSB_ERR_UNSUPPORTED,
+                             "qssb_scan_fft_half: scan size must be 64, 128 or 256");
     }
 }

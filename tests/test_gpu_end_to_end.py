@@ -119,3 +119,29 @@ def test_ssb_session_fit_recovers_defocus():
     assert abs(res.aberrations["C10"] - 100.0) < 15.0
     assert res.refine_method == "nelder-mead"
     assert res.loss is not None
+
+
+@pytest.mark.parametrize("dose", [1000.0])
+def test_stress_256_matches_fp64_gpu_path(dose):
+    """256^2 scan x 128^2 detector (2.1 GB u16), defocus 20 nm: the float32
+    kernels (Kahan trotter sum) against the FP64 GPU restatement of the oracle,
+    target 1e-4 rad RMS."""
+    from dataclasses import replace
+
+    from oracle import ssb_torch_fp64 as tf
+
+    spec = replace(CONFIGS["stress_256x256_det128"], dose=dose)
+    counts = generate(spec, DEV).counts
+    kw = dict(voltage_kV=spec.voltage_kV, semiangle_mrad=spec.semiangle_mrad,
+              scan_sampling=spec.scan_step_A, det_sampling=spec.det_sampling_mrad)
+    backend = B200SSBBackend(counts, semiangle=spec.semiangle_mrad, scan_sampling=spec.scan_step_A,
+                             det_sampling=spec.det_sampling_mrad, voltage_kV=spec.voltage_kV,
+                             device=DEV)
+    assert backend.G_qk.shape[1:] == (256, 129)
+    _, ph = backend.object_and_phase(spec.C10, 0.0, 0.0)
+    prep = tf.prepare(counts, **kw)
+    np.testing.assert_array_equal(backend.bf_inds_row, prep.bf.rows)
+    _, ref = tf.reconstruct(prep, so.Aberrations(spec.C10, 0.0, 0.0))
+    err = so.wrapped_phase_error(ph.cpu().numpy(), ref.cpu().numpy())
+    rms = float(np.sqrt(np.mean(err ** 2)))
+    assert rms <= 1e-4, rms

@@ -194,10 +194,11 @@ def test_gather_is_bit_exact(n_frames, npix, n_bf):
 
 
 # -------------------------------------------------------------- scan FFT
-@pytest.mark.parametrize("n", [64, 128])
+@pytest.mark.parametrize("n", [64, 128, 256])
 def test_scan_fft_half_matches_fp64(n):
     rng = np.random.default_rng(n)
-    images = rng.integers(0, 4000, size=(9, n, n), dtype=np.uint16)
+    top = 4000 if n <= 128 else 256  # keeps every image sum below 2^24
+    images = rng.integers(0, top, size=(9, n, n), dtype=np.uint16)
     g = ops.scan_fft_half(_dev(images.reshape(9, n * n)), (n, n)).cpu().numpy()
     ref = np.fft.rfft2(images.astype(np.float64))
     err = np.abs(g - ref).max() / np.abs(ref).max()
