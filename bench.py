@@ -218,6 +218,55 @@ def reference_cuda_baseline(counts: torch.Tensor, be, steps: int, warmup: int) -
     }
 
 
+def stress_256(dev: torch.device, steps: int) -> dict:
+    """Precision and scale stress: 256^2 scan x 128^2 detector u16 (2.1 GB),
+    defocus 20 nm (C10 = 200 A), doses 50 / 1000 / 20000 e per position. Per
+    dose: the float32 path (FP32 FFTs, Kahan trotter sum) against the FP64 GPU
+    restatement of the oracle at the true aberrations (phase RMS), and the cold
+    recon time at 256^2."""
+    from dataclasses import replace
+
+    from oracle import ssb_oracle as so
+    from oracle import ssb_torch_fp64 as tf
+    from quantem.gpu_b200 import B200SSBBackend
+    from quantem.gpu_b200.synthetic import CONFIGS, generate
+
+    base = CONFIGS["stress_256x256_det128"]
+    out = {"workload": "scan 256x256 x detector 128x128 uint16 (2.1 GB), C10 = 200 A",
+           "doses": {}}
+    stream = torch.cuda.current_stream(dev)
+    for dose in (50.0, 1000.0, 20000.0):
+        spec = replace(base, dose=dose)
+        counts = generate(spec, dev).counts.contiguous()
+        kw = dict(semiangle=spec.semiangle_mrad, scan_sampling=spec.scan_step_A,
+                  det_sampling=spec.det_sampling_mrad, voltage_kV=spec.voltage_kV)
+
+        def cold():
+            be = B200SSBBackend(counts, device=dev, **kw)
+            return be, be.object_and_phase(spec.C10, 0.0, 0.0)[1]
+
+        for _ in range(2):
+            be, ph = cold()
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(steps):
+            be, ph = cold()
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        prep = tf.prepare(counts, voltage_kV=spec.voltage_kV, semiangle_mrad=spec.semiangle_mrad,
+                          scan_sampling=spec.scan_step_A, det_sampling=spec.det_sampling_mrad)
+        _, ref = tf.reconstruct(prep, so.Aberrations(spec.C10, 0.0, 0.0))
+        err = so.wrapped_phase_error(ph.cpu().numpy(), ref.cpu().numpy())
+        out["doses"][str(int(dose))] = {
+            "phase_rms_rad_vs_fp64_gpu": float(np.sqrt(np.mean(err ** 2))),
+            "phase_max_rad_vs_fp64_gpu": float(np.abs(err).max()),
+            "cold_recon_per_s": 1e3 * steps / s.elapsed_time(e), "n_bf": be.num_bf}
+        del counts, be, prep
+        torch.cuda.empty_cache()
+    return out
+
+
 def run_reference(args, world, rank) -> None:
     if rank != 0:
         return
@@ -385,6 +434,8 @@ def run_b200(args, world, rank, local) -> None:
             line["speedup_vs_reference_cuda"] = {
                 "cold": value / rc["cold_recon_per_s"],
                 "warm": line["warm_recon_per_s"] / rc["warm_recon_per_s"]}
+    if world == 1 and not args.no_stress:
+        line["stress_256"] = stress_256(dev, 5)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(counts.cpu().numpy())
     if world == 1 and not args.no_oracle:
@@ -426,6 +477,8 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-oracle", action="store_true")
+    ap.add_argument("--no-stress", action="store_true",
+                    help="skip the 256^2 dose sweep against the FP64 GPU path")
     ap.add_argument("--no-reference-cuda", action="store_true",
                     help="skip timing the reference's own CUDA object kernels")
     ap.add_argument("--profile-once", action="store_true",

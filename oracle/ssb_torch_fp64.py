@@ -12,9 +12,10 @@ device:
   ``rfft2`` of the gathered BF images;
 * corrected spectra and trotter sum - ``ssb_oracle.corrected_spectra`` /
   ``fourier_sum`` (kernels/common.py:115-236, engine.py:1047-1107);
-* object wave - ``ssb_oracle.object_wave`` (engine.py:1109-1151).
+* object wave - ``ssb_oracle.object_wave`` (engine.py:1109-1151);
+* phase-variance loss - ``ssb_oracle.phase_variance_loss`` (engine.py:1464-1514).
 
-Pinned against the numpy oracle in tests/test_gpu_fp64_path.py.
+Pinned against the numpy oracle in tests/test_fp64_path.py.
 """
 from __future__ import annotations
 
@@ -93,8 +94,9 @@ def _chi(alpha2, cos2, sin2, ab: so.Aberrations, lam: float):
     return out
 
 
-def fourier_sum(prep: PreparedGPU, ab: so.Aberrations, chunk: int = 32) -> torch.Tensor:
-    """Sum over BF pixels of C_b(q) on the full plane (complex128), DC := dc."""
+def _corrected_chunks(prep: PreparedGPU, ab: so.Aberrations, chunk: int):
+    """C_b(q) = G_b(q) conj(Gamma_hat_b(q)), full plane, DC := dc, per BF chunk
+    (``ssb_oracle.corrected_spectra``)."""
     geo, d = prep.geo, prep.dev
     r0, r1 = prep.scan_shape
     half = r1 // 2 + 1
@@ -103,7 +105,6 @@ def fourier_sum(prep: PreparedGPU, ab: so.Aberrations, chunk: int = 32) -> torch
     mirror_cols = torch.as_tensor(r1 - np.arange(half, r1), device=prep.g_half.device)
     qx = d["q_row"][None, :, None]
     qy = d["q_col"][None, None, :]
-    total = torch.zeros((r0, r1), dtype=torch.complex128, device=prep.g_half.device)
     for s in range(0, n_bf, chunk):
         e = min(n_bf, s + chunk)
         gh = prep.g_half[s:e]
@@ -125,8 +126,31 @@ def fourier_sum(prep: PreparedGPU, ab: so.Aberrations, chunk: int = 32) -> torch
                             torch.full_like(mag2, 1e8))
         corrected = g * torch.conj(gamma * scale)
         corrected[:, 0, 0] = prep.dc
+        yield corrected
+
+
+def fourier_sum(prep: PreparedGPU, ab: so.Aberrations, chunk: int = 32) -> torch.Tensor:
+    """Sum over BF pixels of C_b(q) on the full plane (complex128)."""
+    r0, r1 = prep.scan_shape
+    total = torch.zeros((r0, r1), dtype=torch.complex128, device=prep.g_half.device)
+    for corrected in _corrected_chunks(prep, ab, chunk):
         total += corrected.sum(dim=0)
     return total
+
+
+def phase_variance_loss(prep: PreparedGPU, ab: so.Aberrations, chunk: int = 32):
+    """``ssb_oracle.phase_variance_loss``: (loss, mean phase [R0, R1])."""
+    r0, r1 = prep.scan_shape
+    s1 = torch.zeros((r0, r1), dtype=torch.float64, device=prep.g_half.device)
+    s2 = torch.zeros_like(s1)
+    for corrected in _corrected_chunks(prep, ab, chunk):
+        ang = torch.angle(torch.fft.ifft2(corrected))
+        s1 += ang.sum(dim=0)
+        s2 += (ang * ang).sum(dim=0)
+    n_b = prep.g_half.shape[0]
+    mean_phase = s1 / n_b
+    var = s2 / n_b - mean_phase * mean_phase
+    return float(var.mean().item()), mean_phase
 
 
 def reconstruct(prep: PreparedGPU, ab: so.Aberrations) -> tuple[torch.Tensor, torch.Tensor]:

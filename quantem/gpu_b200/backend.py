@@ -46,7 +46,7 @@ from .physics import electron_wavelength_angstrom
 from .protocol import BrightfieldDisk, SSBExportState, SSBPrecision, SSBResult
 
 NATIVE_SCAN_SIZES = (128, 256)
-LOSS_SCAN_SIZES = (128,)
+LOSS_SCAN_SIZES = (128, 256)
 
 
 def _as_device_counts(data, device: torch.device) -> torch.Tensor:

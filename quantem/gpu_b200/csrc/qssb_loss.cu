@@ -349,6 +349,172 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
     for (int i = tid; i < N * N; i += 512) pq[i] = sq[(i >> 7) * kL128P + (i & 127)];
 }
 
+// ------------------------------------------------------------- N = 256
+// The 256^2 half plane (264 KB) does not fit shared memory. Per BF pixel:
+//   rows: each warp evaluates C on rows 0..128 one line at a time in its own
+//     shared line (the value C(r, 128) saved first), inverse-FFTs the line
+//     and writes it to the CTA's staging plane in global memory (L2);
+//     C(-r', 128), r' = 1..127, is evaluated directly;
+//   columns: after a barrier each warp rebuilds its columns from the staging
+//     plane (rows 129..255 by row(-r) = -conj(row(r)) + (-1)^x delta_r,
+//     delta_r = conj C(r, 128) + C(-r, 128)), inverse-FFTs them and adds
+//     phi and phi^2 to the CTA's own partial planes, stored column-major
+//     (x * N + y): every element belongs to one lane, so no atomics.
+constexpr int kL256 = 256;
+constexpr int kL256Rows = kL256 / 2 + 1;  // 129 evaluated rows
+
+struct Loss256Smem {
+    static constexpr size_t lines = sizeof(float2) * kLossWarps * kL256;
+    static constexpr size_t misc = sizeof(float2) * (kL256 + 3 * 128);  // tw, cpos, cneg, delta
+    static constexpr size_t bytes = lines + misc;
+    static constexpr size_t stage_per_cta = sizeof(float2) * kL256Rows * kL256;
+};
+
+template <bool CHI64, bool QUAD>
+__global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments256(
+    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
+    const float* __restrict__ q_row, const float* __restrict__ q_col,
+    const qssb_aberrations_t* __restrict__ cands, qssb_calibration_t cal,
+    const float2* __restrict__ eq_table, int bf_per_chunk, int n_chunks, float* __restrict__ part,
+    float2* __restrict__ stage) {
+    constexpr int N = kL256;
+    constexpr int H = N / 2 + 1;
+    constexpr bool kSep = QUAD && !CHI64;
+    extern __shared__ float4 smem4[];
+    float2* lines = reinterpret_cast<float2*>(smem4);
+    float2* tw = lines + kLossWarps * N;
+    float2* cpos = tw + N;
+    float2* cneg = cpos + 128;
+    float2* delta = cneg + 128;
+    __shared__ Probe sp;
+    __shared__ float2 s_phr[kSep ? N : 1];
+    __shared__ float2 s_phc[kSep ? N : 1];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int chunk = blockIdx.x;
+    const int cand = blockIdx.y;
+    const size_t cta = (size_t)cand * n_chunks + chunk;
+    float2* S = stage + cta * (size_t)kL256Rows * N;
+    float* ps = part + cta * 2 * (size_t)N * N;
+    float* pq = ps + (size_t)N * N;
+    float2* line = lines + warp * N;
+    if (tid == 0) {
+        const qssb_aberrations_t ab = cands[cand];
+        sp = make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
+    }
+    fill_twiddles<N>(tw, tid, kLossThreads);
+    // this lane's accumulator elements: columns warp + 16 j, rows lane + 32 t
+    for (int j = 0; j < N / kLossWarps; ++j) {
+        const int x = warp + kLossWarps * j;
+#pragma unroll
+        for (int t = 0; t < N / 32; ++t) {
+            ps[(size_t)x * N + lane + 32 * t] = 0.0f;
+            pq[(size_t)x * N + lane + 32 * t] = 0.0f;
+        }
+    }
+    __syncthreads();
+    const Probe& p = sp;
+    const float2* eqc = eq_table + (size_t)cand * N * N;
+    auto fill_phase = [&](int b) {  // e^{i 2 q_row(r) u}, e^{i 2 q_col(c) v}
+        const float kx = __ldg(geom + b);
+        const float ky = __ldg(geom + n_bf + b);
+        float sn, cs;
+        if (tid < N) {
+            sincosf(2.0f * __ldg(q_row + tid) * fmaf(p.mxx, kx, p.mxy * ky), &sn, &cs);
+            s_phr[tid] = make_float2(cs, sn);
+        } else {
+            sincosf(2.0f * __ldg(q_col + tid - N) * fmaf(p.mxy, kx, p.myy * ky), &sn, &cs);
+            s_phc[tid - N] = make_float2(cs, sn);
+        }
+    };
+    const int b0 = chunk * bf_per_chunk;
+    int nb = n_bf - b0;
+    if (nb > bf_per_chunk) nb = bf_per_chunk;
+    const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
+    if constexpr (kSep) {
+        if (nb > 0) fill_phase(b0);
+        __syncthreads();
+    }
+    auto eval = [&](int b, const BFQuad& kq, const float2& pk, int r, int c) -> float2 {
+        const float2* gb = g + (size_t)b * N * H;
+        const float2 gv = c <= N / 2 ? __ldg(gb + r * H + c)
+                                     : cconj(__ldg(gb + ((N - r) & (N - 1)) * H + (N - c)));
+        if constexpr (kSep) {
+            const float2 lo = make_float2(kq.kx_lo, kq.ky_lo);
+            return corrected_quad_e(__ldg(q_row + r), __ldg(q_col + c), r, c, __ldg(eqc + r * N + c),
+                                    kq.kx, kq.ky, kq.ak, &lo, cmul(s_phr[r], s_phc[c]), gv, p);
+        } else if constexpr (QUAD) {
+            return corrected_quad<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c,
+                                         __ldg(eqc + r * N + c), kq, gv, p);
+        } else {
+            return corrected<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c, kq.kx, kq.ky,
+                                    kq.kx_lo, kq.ky_lo, pk, gv, p);
+        }
+    };
+    for (int i = 0; i < nb; ++i) {
+        const int b = b0 + i;
+        const BFQuad kq = bf_quad(geom, n_bf, b, p);
+        float2 pk = make_float2(0.0f, 0.0f);
+        if constexpr (!QUAD)
+            pk = probe_at_bf<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
+                                    __ldg(geom + 4 * n_bf + b), __ldg(geom + 5 * n_bf + b), p);
+        // C(-r', N/2) for r' = 1..127 (row N - r')
+        if (tid >= 1 && tid < N / 2) cneg[tid] = eval(b, kq, pk, N - tid, N / 2);
+        // rows 0..128: evaluate, keep C(r, N/2), inverse FFT, stage
+        for (int r = warp; r < kL256Rows; r += kLossWarps) {
+#pragma unroll
+            for (int t = 0; t < N / 32; ++t) {
+                const int c = lane + 32 * t;
+                float2 v = (r == 0 && c == 0) ? dc : eval(b, kq, pk, r, c);
+                if (c == N / 2 && r >= 1 && r < N / 2) cpos[r] = v;
+                line[c] = v;
+            }
+            __syncwarp();
+            line_fft<N, +1>(line, 1, tw, lane);
+#pragma unroll
+            for (int t = 0; t < N / 32; ++t) S[(size_t)r * N + lane + 32 * t] = line[lane + 32 * t];
+            __syncwarp();
+        }
+        __syncthreads();
+        if (tid >= 1 && tid < N / 2) delta[tid] = cadd(cconj(cpos[tid]), cneg[tid]);
+        __syncthreads();
+        // columns
+        for (int j = 0; j < N / kLossWarps; ++j) {
+            const int x = warp + kLossWarps * j;
+            const float sign = (x & 1) ? -1.0f : 1.0f;
+#pragma unroll
+            for (int t = 0; t < N / 32; ++t) {
+                const int r = lane + 32 * t;
+                float2 v;
+                if (r < kL256Rows) {
+                    v = S[(size_t)r * N + x];
+                } else {
+                    const float2 m = S[(size_t)(N - r) * N + x];
+                    const float2 d = delta[N - r];
+                    v = make_float2(fmaf(sign, d.x, -m.x), fmaf(sign, d.y, m.y));
+                }
+                line[r] = v;
+            }
+            __syncwarp();
+            line_fft<N, +1>(line, 1, tw, lane);
+#pragma unroll
+            for (int t = 0; t < N / 32; ++t) {
+                const int y = lane + 32 * t;
+                const float2 v = line[y];
+                const float ph = atan2f(v.y, v.x);
+                ps[(size_t)x * N + y] += ph;
+                pq[(size_t)x * N + y] = fmaf(ph, ph, pq[(size_t)x * N + y]);
+            }
+            __syncwarp();
+        }
+        if constexpr (kSep) {
+            if (i + 1 < nb) fill_phase(b + 1);
+        }
+        __syncthreads();
+    }
+}
+
 template <int N>
 __global__ void k_loss_reduce(const float* __restrict__ part, int n_chunks, int n_bf,
                               double* __restrict__ var, float* __restrict__ mean_phase,
@@ -394,6 +560,7 @@ struct LossPlan {
     size_t part_bytes;
     size_t var_bytes;
     size_t eq_bytes;
+    size_t stage_bytes;  // N = 256: one staging half plane per CTA
 };
 
 // Deterministic: about 296 CTAs in total (two per B200 SM), at least one BF
@@ -409,6 +576,7 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand) {
     pl.part_bytes = (pl.part_bytes + 255) & ~(size_t)255;
     pl.var_bytes = sizeof(double) * (size_t)n * n * n_cand;
     pl.eq_bytes = sizeof(float2) * (size_t)n * n * n_cand;
+    pl.stage_bytes = n == kL256 ? Loss256Smem::stage_per_cta * (size_t)pl.n_chunks * n_cand : 0;
     return pl;
 }
 
@@ -425,7 +593,16 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
         k_eq_table<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(cands, cal, eq);
         CUDA_TRY(cudaGetLastError());
     }
-    if constexpr (N == 128) {
+    if constexpr (N == kL256) {
+        static_assert(SYM, "the 256^2 loss evaluates the half plane");
+        float2* stage = reinterpret_cast<float2*>(ws + pl.part_bytes + pl.var_bytes + pl.eq_bytes);
+        const size_t smem = Loss256Smem::bytes;
+        CUDA_TRY(cudaFuncSetAttribute(k_loss_moments256<CHI64, QUAD>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_loss_moments256<CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
+            reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal, eq,
+            pl.bf_per_chunk, pl.n_chunks, part, stage);
+    } else if constexpr (N == 128) {
         const size_t smem = Loss128Smem::bytes;
         CUDA_TRY(cudaFuncSetAttribute(k_loss_moments128<CHI64, QUAD>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -442,7 +619,7 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
     }
     CUDA_TRY(cudaGetLastError());
     k_loss_reduce<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(part, pl.n_chunks, cal.n_bf,
-                                                                       var, mean_phase, N == 128);
+                                                                       var, mean_phase, N == 128 ? 1 : 0);
     CUDA_TRY(cudaGetLastError());
     k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N, losses);
     CUDA_TRY(cudaGetLastError());
@@ -454,11 +631,19 @@ static int dispatch_loss_q(bool sym, bool chi64, const float* g_half, const floa
                            const float* q_row, const float* q_col, const qssb_calibration_t& cal,
                            const qssb_aberrations_t* cands, int n_cand, char* ws, float* losses,
                            float* mean_phase, cudaStream_t s) {
-    if (sym)
+    if constexpr (N == kL256) {
+        if (!sym)
+            return set_error(QSSB_ERR_UNSUPPORTED,
+                             "qssb_loss_batch: QSSB_FLAG_FULL_PLANE is not offered at 256^2");
         return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
                      : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
-    return chi64 ? launch_loss<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
-                 : launch_loss<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
+    } else {
+        if (sym)
+            return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
+                         : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
+        return chi64 ? launch_loss<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
+                     : launch_loss<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
+    }
 }
 
 // Candidates live on the device, so the path is chosen by a flag: the
@@ -485,10 +670,10 @@ extern "C" int qssb_loss_workspace_bytes(const qssb_calibration_t* cal, int32_t 
     if (!bytes || n_cand <= 0 || n_cand > 65535)
         return set_error(QSSB_ERR_INVALID, "qssb_loss_workspace_bytes: n_cand must be in [1, 65535]");
     const int n = cal->scan_rows;
-    if (n != 64 && n != 128)
-        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64 or 128");
+    if (n != 64 && n != 128 && n != 256)
+        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64, 128 or 256");
     const LossPlan pl = plan_loss(n, cal->n_bf, n_cand);
-    *bytes = pl.part_bytes + pl.var_bytes + pl.eq_bytes;
+    *bytes = pl.part_bytes + pl.var_bytes + pl.eq_bytes + pl.stage_bytes;
     return QSSB_OK;
 }
 
@@ -516,6 +701,7 @@ extern "C" int qssb_loss_batch(const float* g_half, const float* bf_geom, const 
     switch (cal->scan_rows) {
         case 64: return dispatch_loss<64>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, ws, losses, mean_phase, s);
         case 128: return dispatch_loss<128>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, ws, losses, mean_phase, s);
-        default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64 or 128");
+        case 256: return dispatch_loss<256>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, ws, losses, mean_phase, s);
+        default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64, 128 or 256");
     }
 }

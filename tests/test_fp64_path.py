@@ -33,3 +33,7 @@ def test_torch_fp64_path_matches_numpy_oracle(case):
         o2, p2 = tf.reconstruct(pg, ab)
         assert np.abs(o1 - o2.numpy()).max() <= 1e-10 * np.abs(o1).max()
         assert np.abs(so.wrapped_phase_error(p1, p2.numpy())).max() <= 1e-10
+        l1, m1 = so.phase_variance_loss(prep.g_half, prep.geo, ab, prep.dc)
+        l2, m2 = tf.phase_variance_loss(pg, ab)
+        assert abs(l1 - l2) <= 1e-10 * abs(l1)
+        assert np.abs(m1 - m2.numpy()).max() <= 1e-10

@@ -145,3 +145,12 @@ def test_stress_256_matches_fp64_gpu_path(dose):
     err = so.wrapped_phase_error(ph.cpu().numpy(), ref.cpu().numpy())
     rms = float(np.sqrt(np.mean(err ** 2)))
     assert rms <= 1e-4, rms
+    # phase-variance loss at 256^2 (the staged-rows kernel), quadratic and C30 paths
+    c10 = np.asarray([spec.C10, spec.C10 - 40.0, spec.C10 + 25.0])
+    losses = backend.variance_loss_batch(c10, 0.0, 0.0).cpu().numpy()
+    for c, got in zip(c10, losses):
+        want, _ = tf.phase_variance_loss(prep, so.Aberrations(float(c), 0.0, 0.0))
+        assert abs(got - want) <= 1e-5 * abs(want) + 1e-6, (c, got, want)
+    got = backend.variance_loss_batch([spec.C10], [5.0], [0.3], C30=[2e4]).cpu().numpy()[0]
+    want, _ = tf.phase_variance_loss(prep, so.Aberrations(spec.C10, 5.0, 0.3, C30=2e4))
+    assert abs(got - want) <= 1e-5 * abs(want) + 1e-6, (got, want)
