@@ -267,6 +267,58 @@ def stress_256(dev: torch.device, steps: int) -> dict:
     return out
 
 
+def sweep_3scans(dev: torch.device, steps: int) -> dict:
+    """Batched aberration sweep: scans of 96^2, 128^2 and 160x120 positions
+    (128^2 detector, padded by the reference's rule to 128^2, 128^2, 256^2),
+    64 candidates each with C1, A1 and C3, all three scored in one CUDA-graph
+    launch with autotuned loss partitions."""
+    from quantem.gpu_b200 import B200SSBBackend
+    from quantem.gpu_b200.sweep import MultiScanSweep
+    from quantem.gpu_b200.synthetic import draw_aberrations, generate, sweep_specs
+
+    specs = sweep_specs()
+    backends = []
+    for spec in specs:
+        counts = generate(spec, dev).counts
+        backends.append(B200SSBBackend(counts, semiangle=spec.semiangle_mrad,
+                                       scan_sampling=spec.scan_step_A,
+                                       det_sampling=spec.det_sampling_mrad,
+                                       voltage_kV=spec.voltage_kV, device=dev))
+        del counts
+    rng = np.random.default_rng(5)
+    cands = [draw_aberrations(rng, 64) for _ in specs]
+    for i, spec in enumerate(specs):
+        cands[i][17] = (spec.C10, spec.C12, spec.phi12, spec.C30)
+    sw = MultiScanSweep(backends, 64)
+    losses = sw(cands)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        fn()
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(steps):
+            fn()
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        return s.elapsed_time(e) / steps
+
+    graph_ms = timed(sw.replay)
+    direct_ms = timed(sw._launch_all)
+    n = sum(c.shape[0] for c in cands)
+    return {
+        "workload": "scans 96x96, 128x128, 160x120 (padded to 128, 128, 256) x 128^2 detector, "
+                    "64 candidates each (C1 in +-50 nm, |A1| <= 10 nm, C3 <= 1 um)",
+        "n_bf": [be.num_bf for be in backends],
+        "graph_launch_ms": graph_ms, "evals_per_s_graph": n * 1e3 / graph_ms,
+        "evals_per_s_direct": n * 1e3 / direct_ms,
+        "kernel_launches_per_graph": sw.launches_per_replay,
+        "autotuned_chunks_per_candidate": [s["chunks"] for s in sw._slots],
+        "truth_ranked_first": [bool(int(np.argmin(l)) == 17) for l in losses],
+    }
+
+
 def run_reference(args, world, rank) -> None:
     if rank != 0:
         return
@@ -436,6 +488,7 @@ def run_b200(args, world, rank, local) -> None:
                 "warm": line["warm_recon_per_s"] / rc["warm_recon_per_s"]}
     if world == 1 and not args.no_stress:
         line["stress_256"] = stress_256(dev, 5)
+        line["sweep_3scans"] = sweep_3scans(dev, 5)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(counts.cpu().numpy())
     if world == 1 and not args.no_oracle:

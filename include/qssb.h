@@ -37,6 +37,14 @@ extern "C" {
 #define QSSB_FLAG_QUADRATIC 4     /* qssb_loss_batch: every candidate has C30 == 0, so the
                                      factorised quadratic-chi overlap applies (qssb_object
                                      decides this itself from its host-side candidate) */
+/* Work partition (the tuning knob of an autotuner): bits 16..30 of flags hold
+ * the number of BF chunks - per candidate for qssb_loss_batch, in total for
+ * qssb_object. 0 keeps the built-in plan. Any value gives the same result up
+ * to float32 summation order, and the same bits on every repeat of that value;
+ * query the workspace with the same flags. */
+#define QSSB_FLAG_CHUNKS_SHIFT 16
+#define QSSB_FLAG_CHUNKS(n) ((int32_t)(n) << QSSB_FLAG_CHUNKS_SHIFT)
+#define QSSB_FLAG_CHUNKS_MAX 32767
 
 /* Calibration shared by the object and loss entry points. Scalars follow
  * SSBEngine's cache (engine.py:784-848): wavelength in Angstrom, angles in

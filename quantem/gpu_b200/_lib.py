@@ -22,6 +22,15 @@ QSSB_FLAG_CHI_FP64 = 1
 QSSB_FLAG_FULL_PLANE = 2
 QSSB_FLAG_QUADRATIC = 4
 QSSB_NOALLOC_SCRATCH_BYTES = 16 << 20
+QSSB_FLAG_CHUNKS_SHIFT = 16
+QSSB_FLAG_CHUNKS_MAX = 32767
+
+
+def flag_chunks(n: int) -> int:
+    """``QSSB_FLAG_CHUNKS(n)``: the work partition knob (0 = built-in plan)."""
+    if not 0 <= int(n) <= QSSB_FLAG_CHUNKS_MAX:
+        raise ValueError(f"chunk count must be in [0, {QSSB_FLAG_CHUNKS_MAX}]")
+    return int(n) << QSSB_FLAG_CHUNKS_SHIFT
 
 
 class Calibration(ctypes.Structure):

@@ -31,8 +31,15 @@ from typing import Literal
 import numpy as np
 import torch
 
-from . import ops
-from ._lib import GEOM_ROWS, QSSB_FLAG_CHI_FP64, QSSB_FLAG_QUADRATIC, Aberrations, Calibration
+from . import autotune, ops
+from ._lib import (
+    GEOM_ROWS,
+    QSSB_FLAG_CHI_FP64,
+    QSSB_FLAG_QUADRATIC,
+    Aberrations,
+    Calibration,
+    flag_chunks,
+)
 from .calibration import (
     BFGeometry,
     bf_geometry,
@@ -309,6 +316,21 @@ class B200SSBBackend:
     def _geometry(self, value) -> None:
         self._geometry_host = value
 
+    def _object_flags(self) -> int:
+        """Flags of the object kernels: the session's, plus the autotuned work
+        partition when one is cached for this scan size and BF count."""
+        chunks = autotune.cached_object(self.device, self._scan_shape[0], int(self.G_qk.shape[0]),
+                                        self._flags)
+        return self._flags | flag_chunks(chunks)
+
+    def autotune(self) -> dict:
+        """Time the object kernels' work partitions on this dataset and cache the
+        fastest for every later session with the same scan size and BF count."""
+        c = autotune.tune_object(self.G_qk, self._geom_dev, self._q_row, self._q_col,
+                                 self._calibration(), Aberrations(0.0, 0.0, 0.0, 0.0), self._flags,
+                                 self._workspace)
+        return {"object_chunks": c}
+
     def _calibration(self) -> Calibration:
         return Calibration(
             n_bf=int(self.G_qk.shape[0]), scan_rows=self._scan_shape[0], scan_cols=self._scan_shape[1],
@@ -373,7 +395,8 @@ class B200SSBBackend:
             self.cache_rotation(rotation_angle_rad)
         obj, _ = ops.object_wave(self.G_qk, self._geom_dev, self._q_row, self._q_col,
                                  self._calibration(), Aberrations(C10, C12, phi12, C30),
-                                 flags=self._flags, workspace=self._workspace, want_phase=False)
+                                 flags=self._object_flags(), workspace=self._workspace,
+                                 want_phase=False)
         return obj
 
     def object_and_phase(self, C10: float, C12: float, phi12: float, C30: float = 0.0
@@ -381,7 +404,7 @@ class B200SSBBackend:
         """Object wave and its float32 phase from one launch sequence."""
         return ops.object_wave(self.G_qk, self._geom_dev, self._q_row, self._q_col,
                                self._calibration(), Aberrations(C10, C12, phi12, C30),
-                               flags=self._flags, workspace=self._workspace)
+                               flags=self._object_flags(), workspace=self._workspace)
 
     def variance_loss_batch(self, C10, C12, phi12, C30=None) -> torch.Tensor:
         """Phase-variance losses (float32 CUDA [n]) for a candidate batch."""

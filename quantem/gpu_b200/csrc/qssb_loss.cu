@@ -565,9 +565,9 @@ struct LossPlan {
 
 // Deterministic: about 296 CTAs in total (two per B200 SM), at least one BF
 // pixel each.
-static LossPlan plan_loss(int n, int n_bf, int n_cand) {
+static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0) {
     LossPlan pl;
-    int chunks = (296 + n_cand - 1) / n_cand;
+    int chunks = chunks_req > 0 ? chunks_req : (296 + n_cand - 1) / n_cand;
     if (chunks < 1) chunks = 1;
     if (chunks > n_bf) chunks = n_bf;
     pl.bf_per_chunk = (n_bf + chunks - 1) / chunks;
@@ -583,9 +583,9 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand) {
 template <int N, bool SYM, bool CHI64, bool QUAD>
 static int launch_loss(const float* g_half, const float* geom, const float* q_row,
                        const float* q_col, const qssb_calibration_t& cal,
-                       const qssb_aberrations_t* cands, int n_cand, char* ws, float* losses,
-                       float* mean_phase, cudaStream_t s) {
-    const LossPlan pl = plan_loss(N, cal.n_bf, n_cand);
+                       const qssb_aberrations_t* cands, int n_cand, int chunks, char* ws,
+                       float* losses, float* mean_phase, cudaStream_t s) {
+    const LossPlan pl = plan_loss(N, cal.n_bf, n_cand, chunks);
     float* part = reinterpret_cast<float*>(ws);
     double* var = reinterpret_cast<double*>(ws + pl.part_bytes);
     float2* eq = reinterpret_cast<float2*>(ws + pl.part_bytes + pl.var_bytes);
@@ -629,20 +629,20 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
 template <int N, bool QUAD>
 static int dispatch_loss_q(bool sym, bool chi64, const float* g_half, const float* geom,
                            const float* q_row, const float* q_col, const qssb_calibration_t& cal,
-                           const qssb_aberrations_t* cands, int n_cand, char* ws, float* losses,
-                           float* mean_phase, cudaStream_t s) {
+                           const qssb_aberrations_t* cands, int n_cand, int chunks, char* ws,
+                           float* losses, float* mean_phase, cudaStream_t s) {
     if constexpr (N == kL256) {
         if (!sym)
             return set_error(QSSB_ERR_UNSUPPORTED,
                              "qssb_loss_batch: QSSB_FLAG_FULL_PLANE is not offered at 256^2");
-        return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
-                     : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
+        return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s)
+                     : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
     } else {
         if (sym)
-            return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
-                         : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
-        return chi64 ? launch_loss<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s)
-                     : launch_loss<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
+            return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s)
+                         : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
+        return chi64 ? launch_loss<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s)
+                     : launch_loss<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
     }
 }
 
@@ -651,11 +651,11 @@ static int dispatch_loss_q(bool sym, bool chi64, const float* g_half, const floa
 template <int N>
 static int dispatch_loss(bool sym, bool chi64, bool quad, const float* g_half, const float* geom,
                          const float* q_row, const float* q_col, const qssb_calibration_t& cal,
-                         const qssb_aberrations_t* cands, int n_cand, char* ws, float* losses,
-                         float* mean_phase, cudaStream_t s) {
+                         const qssb_aberrations_t* cands, int n_cand, int chunks, char* ws,
+                         float* losses, float* mean_phase, cudaStream_t s) {
     if (quad)
-        return dispatch_loss_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
-    return dispatch_loss_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, ws, losses, mean_phase, s);
+        return dispatch_loss_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
+    return dispatch_loss_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
 }
 
 }  // namespace qssb
@@ -664,7 +664,6 @@ using namespace qssb;
 
 extern "C" int qssb_loss_workspace_bytes(const qssb_calibration_t* cal, int32_t n_cand,
                                          int32_t flags, size_t* bytes) {
-    (void)flags;
     int rc = validate_calibration(cal, "qssb_loss_workspace_bytes: null calibration");
     if (rc) return rc;
     if (!bytes || n_cand <= 0 || n_cand > 65535)
@@ -672,7 +671,7 @@ extern "C" int qssb_loss_workspace_bytes(const qssb_calibration_t* cal, int32_t 
     const int n = cal->scan_rows;
     if (n != 64 && n != 128 && n != 256)
         return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64, 128 or 256");
-    const LossPlan pl = plan_loss(n, cal->n_bf, n_cand);
+    const LossPlan pl = plan_loss(n, cal->n_bf, n_cand, flag_chunks(flags));
     *bytes = pl.part_bytes + pl.var_bytes + pl.eq_bytes + pl.stage_bytes;
     return QSSB_OK;
 }
@@ -696,12 +695,13 @@ extern "C" int qssb_loss_batch(const float* g_half, const float* bf_geom, const 
     const bool sym = !(flags & QSSB_FLAG_FULL_PLANE);
     const bool chi64 = (flags & QSSB_FLAG_CHI_FP64) != 0;
     const bool quad = (flags & QSSB_FLAG_QUADRATIC) != 0;
+    const int chunks = flag_chunks(flags);
     cudaStream_t s = (cudaStream_t)stream;
     char* ws = static_cast<char*>(workspace);
     switch (cal->scan_rows) {
-        case 64: return dispatch_loss<64>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, ws, losses, mean_phase, s);
-        case 128: return dispatch_loss<128>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, ws, losses, mean_phase, s);
-        case 256: return dispatch_loss<256>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, ws, losses, mean_phase, s);
+        case 64: return dispatch_loss<64>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
+        case 128: return dispatch_loss<128>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
+        case 256: return dispatch_loss<256>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
         default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64, 128 or 256");
     }
 }

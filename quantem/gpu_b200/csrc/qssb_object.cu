@@ -359,12 +359,12 @@ struct ObjectPlan {
 // Deterministic chunking (independent of the GPU's SM count): about 128 BF
 // chunks at N <= 128 and 32 at N = 256 (N^2/4-thread grids per chunk fill
 // the GPU), 4..256 BF pixels each.
-static ObjectPlan plan_object(int n, int n_bf, bool sym) {
+static ObjectPlan plan_object(int n, int n_bf, bool sym, int chunks_req = 0) {
     ObjectPlan pl;
     pl.n_q = sym ? n * (n / 2 + 1) + n / 2 - 1 : n * n;
-    const int target = n >= 256 ? 32 : 128;
+    const int target = chunks_req > 0 ? chunks_req : (n >= 256 ? 32 : 128);
     int bpc = (n_bf + target - 1) / target;
-    if (bpc < 4) bpc = 4;
+    if (bpc < (chunks_req > 0 ? 1 : 4)) bpc = chunks_req > 0 ? 1 : 4;
     if (bpc > kMaxBfChunk) bpc = kMaxBfChunk;
     pl.bf_per_chunk = bpc;
     pl.n_chunks = (n_bf + bpc - 1) / bpc;
@@ -395,8 +395,8 @@ int validate_calibration(const qssb_calibration_t* cal, const char* who) {
 template <int N, bool SYM, bool CHI64, bool QUAD>
 static int launch_object(const float* g_half, const float* geom, const float* q_row,
                          const float* q_col, const qssb_calibration_t& cal, const Probe& p,
-                         char* ws, float* object, float* phase, cudaStream_t s) {
-    const ObjectPlan pl = plan_object(N, cal.n_bf, SYM);
+                         int chunks, char* ws, float* object, float* phase, cudaStream_t s) {
+    const ObjectPlan pl = plan_object(N, cal.n_bf, SYM, chunks);
     float2* partial = reinterpret_cast<float2*>(ws);
     float2* plane = reinterpret_cast<float2*>(ws + pl.partial_bytes);
     if constexpr (SYM && QUAD && !CHI64) {
@@ -424,22 +424,24 @@ static int launch_object(const float* g_half, const float* geom, const float* q_
 template <int N, bool QUAD>
 static int dispatch_object_q(bool sym, bool chi64, const float* g_half, const float* geom,
                              const float* q_row, const float* q_col, const qssb_calibration_t& cal,
-                             const Probe& p, char* ws, float* object, float* phase, cudaStream_t s) {
+                             const Probe& p, int chunks, char* ws, float* object, float* phase,
+                             cudaStream_t s) {
     if (sym) {
-        return chi64 ? launch_object<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s)
-                     : launch_object<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s);
+        return chi64 ? launch_object<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, ws, object, phase, s)
+                     : launch_object<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, ws, object, phase, s);
     }
-    return chi64 ? launch_object<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s)
-                 : launch_object<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, p, ws, object, phase, s);
+    return chi64 ? launch_object<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, ws, object, phase, s)
+                 : launch_object<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, ws, object, phase, s);
 }
 
 template <int N>
 static int dispatch_object(bool sym, bool chi64, const float* g_half, const float* geom,
                            const float* q_row, const float* q_col, const qssb_calibration_t& cal,
-                           const Probe& p, char* ws, float* object, float* phase, cudaStream_t s) {
+                           const Probe& p, int chunks, char* ws, float* object, float* phase,
+                           cudaStream_t s) {
     if (p.quadratic)
-        return dispatch_object_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, p, ws, object, phase, s);
-    return dispatch_object_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, p, ws, object, phase, s);
+        return dispatch_object_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, p, chunks, ws, object, phase, s);
+    return dispatch_object_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, p, chunks, ws, object, phase, s);
 }
 
 }  // namespace qssb
@@ -454,7 +456,7 @@ extern "C" int qssb_object_workspace_bytes(const qssb_calibration_t* cal, int32_
     const int n = cal->scan_rows;
     if (n != 64 && n != 128 && n != 256)
         return set_error(QSSB_ERR_UNSUPPORTED, "qssb_object: scan size must be 64, 128 or 256");
-    const ObjectPlan pl = plan_object(n, cal->n_bf, !(flags & QSSB_FLAG_FULL_PLANE));
+    const ObjectPlan pl = plan_object(n, cal->n_bf, !(flags & QSSB_FLAG_FULL_PLANE), flag_chunks(flags));
     *bytes = pl.partial_bytes + pl.plane_bytes;
     return QSSB_OK;
 }
@@ -478,12 +480,13 @@ extern "C" int qssb_object(const float* g_half, const float* bf_geom, const floa
     const Probe p = make_probe(*cal, *ab);
     const bool sym = !(flags & QSSB_FLAG_FULL_PLANE);
     const bool chi64 = (flags & QSSB_FLAG_CHI_FP64) != 0;
+    const int chunks = flag_chunks(flags);
     cudaStream_t s = (cudaStream_t)stream;
     char* ws = static_cast<char*>(workspace);
     switch (cal->scan_rows) {
-        case 64: return dispatch_object<64>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, ws, object, phase, s);
-        case 128: return dispatch_object<128>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, ws, object, phase, s);
-        case 256: return dispatch_object<256>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, ws, object, phase, s);
+        case 64: return dispatch_object<64>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, ws, object, phase, s);
+        case 128: return dispatch_object<128>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, ws, object, phase, s);
+        case 256: return dispatch_object<256>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, ws, object, phase, s);
         default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_object: scan size must be 64, 128 or 256");
     }
 }

@@ -302,7 +302,8 @@ def loss_workspace_bytes(cal: Calibration, n_cand: int, flags: int = 0) -> int:
 
 def loss_batch(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
                q_col: torch.Tensor, cal: Calibration, candidates: torch.Tensor, *,
-               flags: int = 0, workspace: Workspace | None = None, want_mean_phase: bool = False
+               flags: int = 0, workspace: Workspace | None = None, want_mean_phase: bool = False,
+               out: torch.Tensor | None = None
                ) -> tuple[torch.Tensor, torch.Tensor | None]:
     """Phase-variance losses for ``candidates`` (float32 CUDA [n, 4]: C10, C12, phi12, C30)."""
     _require_cuda(g_half, "g_half", torch.complex64)
@@ -317,7 +318,11 @@ def loss_batch(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
     r0, r1 = int(cal.scan_rows), int(cal.scan_cols)
     ws = workspace or Workspace(g_half.device)
     buf = ws.get(loss_workspace_bytes(cal, n, flags))
-    losses = torch.empty(n, dtype=torch.float32, device=g_half.device)
+    if out is not None:
+        _require_cuda(out, "out", torch.float32)
+        if out.numel() != n:
+            raise ValueError("out must hold one loss per candidate")
+    losses = out if out is not None else torch.empty(n, dtype=torch.float32, device=g_half.device)
     mp = (torch.empty((n, r0, r1), dtype=torch.float32, device=g_half.device)
           if want_mean_phase else None)
     _call("qssb_loss_batch", g_half.device, _ptr(g_half), _ptr(bf_geom), _ptr(q_row),

@@ -200,3 +200,28 @@ def generate(spec: SyntheticSpec, device: torch.device | str = "cpu",
     counts = counts.reshape(r0, r1, k0, k1)
     return SyntheticData(counts=counts, spec=spec, object_phase=phi,
                          extra={"probe_pixel_A": dx, "canvas": canvas})
+
+
+# Batched-sweep workload: three 128^2-detector scans of uneven size; true
+# aberrations and candidates drawn from C1 in [-50, 50] nm, |A1| in [0, 10] nm
+# at a random angle, C3 in [0, 1] um - in the reference's numeric convention
+# (Angstrom values): C10 in [-500, 500], C12 in [0, 100], C30 in [0, 1e4].
+SWEEP_SCANS = ((96, 96), (128, 128), (160, 120))
+SWEEP_RANGES = {"C10": (-500.0, 500.0), "C12": (0.0, 100.0), "phi12": (0.0, math.pi),
+                "C30": (0.0, 1.0e4)}
+
+
+def draw_aberrations(rng: np.random.Generator, n: int) -> np.ndarray:
+    """[n, 4] float32 (C10, C12, phi12, C30) uniform in SWEEP_RANGES."""
+    cols = [rng.uniform(*SWEEP_RANGES[k], size=n) for k in ("C10", "C12", "phi12", "C30")]
+    return np.stack(cols, axis=1).astype(np.float32)
+
+
+def sweep_specs(seed: int = 7, dose: float = 2.0e4) -> list[SyntheticSpec]:
+    """The three scans of the batched sweep, each with its own true aberrations."""
+    rng = np.random.default_rng(seed)
+    truth = draw_aberrations(rng, len(SWEEP_SCANS))
+    return [SyntheticSpec(scan_shape=shape, detector_shape=(128, 128),
+                          det_sampling_mrad=20.0 / 24.0, dose=dose, C10=float(t[0]),
+                          C12=float(t[1]), phi12=float(t[2]), C30=float(t[3]), seed=seed + i)
+            for i, (shape, t) in enumerate(zip(SWEEP_SCANS, truth))]

@@ -1,0 +1,79 @@
+"""Batched aberration sweep over three uneven scans in one CUDA-graph launch.
+
+Scans of 96x96, 128x128 and 160x120 positions (128^2 detector) are padded by
+the reference's rule (backend.py:229-269) to 128^2, 128^2 and 256^2, and
+scored with candidates that include C3 (C30). Checks: the graph replay gives
+the same bits as direct calls with the same (autotuned) partition and on
+every replay; the losses match the FP64 GPU restatement of the oracle within
+the reference's loss tolerance (tests/ssb_precision.py:7-10 of
+bobleesj/quantem.gpu: rel 1e-5, abs 1e-6); the true aberrations, hidden among
+random candidates, give the lowest loss of each scan.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import ssb_oracle as so
+from oracle import ssb_torch_fp64 as tf
+from quantem.gpu_b200 import B200SSBBackend, ops
+from quantem.gpu_b200.sweep import MultiScanSweep
+from quantem.gpu_b200.synthetic import draw_aberrations, generate, sweep_specs
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+N_CAND = 8
+
+
+@pytest.fixture(scope="module")
+def scans():
+    out = []
+    for spec in sweep_specs():
+        counts = generate(spec, DEV).counts
+        be = B200SSBBackend(counts, semiangle=spec.semiangle_mrad, scan_sampling=spec.scan_step_A,
+                            det_sampling=spec.det_sampling_mrad, voltage_kV=spec.voltage_kV,
+                            device=DEV)
+        out.append((spec, counts, be))
+    return out
+
+
+@pytest.fixture(scope="module")
+def candidates(scans):
+    rng = np.random.default_rng(11)
+    cands = []
+    for i, (spec, _, _) in enumerate(scans):
+        c = draw_aberrations(rng, N_CAND)
+        c[i % N_CAND] = (spec.C10, spec.C12, spec.phi12, spec.C30)  # hide the truth
+        cands.append(c)
+    return cands
+
+
+def test_reference_padding_of_uneven_scans(scans):
+    assert [be.scan_shape for _, _, be in scans] == [(128, 128), (128, 128), (256, 256)]
+
+
+def test_graph_sweep_matches_direct_calls_and_repeats(scans, candidates):
+    sw = MultiScanSweep([be for _, _, be in scans], N_CAND)
+    first = sw(candidates)
+    second = sw(candidates)
+    assert sw.launches_per_replay == 3 * len(scans)  # moments, reduce, mean per scan
+    for a, b in zip(first, second):
+        np.testing.assert_array_equal(a, b)
+    for (_, _, be), slot, c, got in zip(scans, sw._slots, candidates, first):
+        direct, _ = ops.loss_batch(be.G_qk, be._geom_dev, be._q_row, be._q_col, slot["cal"],
+                                   torch.as_tensor(c, device=DEV), flags=slot["flags"])
+        np.testing.assert_array_equal(direct.cpu().numpy(), got)
+
+
+def test_sweep_losses_match_fp64_and_find_the_truth(scans, candidates):
+    sw = MultiScanSweep([be for _, _, be in scans], N_CAND)
+    got = sw(candidates)
+    for i, ((spec, counts, be), c, losses) in enumerate(zip(scans, candidates, got)):
+        assert int(np.argmin(losses)) == i % N_CAND, (spec.scan_shape, losses)
+        padded = torch.as_tensor(so.pad_or_crop_scan(counts.cpu().numpy()), device=DEV)
+        prep = tf.prepare(padded, voltage_kV=spec.voltage_kV, semiangle_mrad=spec.semiangle_mrad,
+                          scan_sampling=spec.scan_step_A, det_sampling=spec.det_sampling_mrad)
+        for j in (i % N_CAND, (i + 3) % N_CAND):
+            want, _ = tf.phase_variance_loss(prep, so.Aberrations(*map(float, c[j])))
+            assert abs(losses[j] - want) <= 1e-5 * abs(want) + 1e-6, (spec.scan_shape, j, losses[j], want)
