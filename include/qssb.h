@@ -219,6 +219,64 @@ int qssb_loss_batch(const float* g_half, const float* bf_geom, const float* q_ro
                     void* workspace, size_t workspace_bytes, float* losses,
                     float* mean_phase, void* stream);
 
+/* ------------------------------------------------------------------------
+ * Learned aberration proposer (no counterpart in the reference, which has no
+ * learned component). Features: trotter amplitudes |G_b(Q)| at n_q scan
+ * frequencies, resampled onto a k grid through a caller-built CSR table
+ * (cells x BF pixels: csr_off [cells+1], csr_idx, csr_w with row sums 1) and
+ * divided by their mean over covered cells. scratch: float [n_q * n_bf]
+ * (times n_samples for qssb_synth_features). Outputs [n_samples][n_q][cells]
+ * as float32 and/or BF16 (either pointer may be NULL, not both).
+ */
+/* Inference features from a resident Hermitian G [n_bf][scan_n][scan_n/2+1];
+ * q_idx: device int32 [n_q][2] fftfreq indices (row, col), any sign. */
+int qssb_trotter_features(const float* g_half, int32_t n_bf, int32_t scan_n, const int32_t* q_idx,
+                          int32_t n_q, const int32_t* csr_off, const int32_t* csr_idx,
+                          const float* csr_w, int32_t cells, float* scratch, float* out_f32,
+                          void* out_bf16, void* stream);
+
+/* Training features from the SSB forward model of a weak object:
+ * v = |Gamma(Q, k_b) phi + Gamma+(Q, k_b) phi_a + n|,
+ * Gamma = P(Q-k) conj P(k) - conj P(Q+k) P(k) (kernels/common.py:115-236),
+ * Gamma+ = P(Q-k) conj P(k) + conj P(Q+k) P(k) (amplitude contrast), phi:
+ * complex64 [n_samples][n_q][2] = (phi, phi_a) per map, n complex
+ * Gaussian of standard deviation sigma[s][q] |phi| (float [n_samples][n_q])
+ * from a counter-based hash of (seed, index). bf_geom: the [8][n_bf] geometry of the training detector
+ * lattice; q_vec: device float [n_q][2] in 1/A; cal supplies wavelength,
+ * aperture and detector sampling (n_bf and dc unused). */
+int qssb_synth_features(const float* bf_geom, int32_t n_bf, const float* q_vec, int32_t n_q,
+                        const qssb_aberrations_t* aberrations, const float* phi,
+                        const float* sigma, int32_t n_samples, const qssb_calibration_t* cal,
+                        uint64_t seed, const int32_t* csr_off, const int32_t* csr_idx,
+                        const float* csr_w, int32_t cells, float* scratch, float* out_f32,
+                        void* out_bf16, void* stream);
+
+/* C[M][N] (+)= op(A)[M][K] op(B)[K][N] on the tensor cores: A, B BF16
+ * (op = transpose when trans_*), FP32 accumulation; M, N, K multiples of 16,
+ * leading dimensions multiples of 8, A and B 32-byte aligned. Epilogue: + bias
+ * [N] (or NULL); C (FP32, NULL allowed) stores or, with accumulate, adds;
+ * act_bf16 (NULL allowed) receives BF16 GELU(result) (tanh form). */
+int qssb_gemm_bf16(const void* A, int32_t lda, int32_t trans_a, const void* B, int32_t ldb,
+                   int32_t trans_b, int32_t M, int32_t N, int32_t K, const float* bias,
+                   int32_t accumulate, float* C, int32_t ldc, void* act_bf16, int32_t ld_act,
+                   void* stream);
+/* dz = dy * GELU'(pre) (FP32 and BF16 copies), n elements. */
+int qssb_gelu_backward(const float* dy, const float* pre, int64_t n, void* dz_bf16, float* dz,
+                       void* stream);
+/* db[c] = sum over rows of dz[r][c] (fixed order, FP64 accumulation). */
+int qssb_bias_grad(const float* dz, int32_t rows, int32_t cols, float* db, void* stream);
+/* Mean squared error over the first n_out of ld columns and its gradient dy
+ * (zero in columns n_out..ld-1); loss (device float) may be NULL. */
+int qssb_mse(const float* y, const float* target, int32_t rows, int32_t n_out, int32_t ld,
+             float* dy, float* loss, void* stream);
+/* Adam (bias-corrected, decoupled weight decay) on FP32 master weights; the
+ * BF16 copy w_bf16 (may be NULL) is refreshed. step counts from 1. */
+int qssb_adam(float* w, float* m, float* v, const float* grad, int64_t n, float lr, float beta1,
+              float beta2, float eps, float weight_decay, int32_t step, void* w_bf16,
+              void* stream);
+/* y = BF16(x), n elements. */
+int qssb_to_bf16(const float* x, int64_t n, void* y, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -120,6 +120,19 @@ SIGNATURES = {
         _P, _P, _P, _P, ctypes.POINTER(Calibration), ctypes.POINTER(Aberrations), _I32, _P, _P, _P]),
     "qssb_loss_workspace_bytes": (
         ctypes.c_int, [ctypes.POINTER(Calibration), _I32, _I32, ctypes.POINTER(_SZ)]),
+    "qssb_trotter_features": (ctypes.c_int, [_P, _I32, _I32, _P, _I32, _P, _P, _P, _I32, _P, _P,
+                                             _P, _P]),
+    "qssb_synth_features": (ctypes.c_int, [_P, _I32, _P, _I32, _P, _P, _P, _I32,
+                                           ctypes.POINTER(Calibration), ctypes.c_uint64, _P, _P,
+                                           _P, _I32, _P, _P, _P, _P]),
+    "qssb_gemm_bf16": (ctypes.c_int, [_P, _I32, _I32, _P, _I32, _I32, _I32, _I32, _I32, _P, _I32,
+                                      _P, _I32, _P, _I32, _P]),
+    "qssb_gelu_backward": (ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
+    "qssb_bias_grad": (ctypes.c_int, [_P, _I32, _I32, _P, _P]),
+    "qssb_mse": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _P, _P, _P]),
+    "qssb_adam": (ctypes.c_int, [_P, _P, _P, _P, _I64, ctypes.c_float, ctypes.c_float,
+                                 ctypes.c_float, ctypes.c_float, ctypes.c_float, _I32, _P, _P]),
+    "qssb_to_bf16": (ctypes.c_int, [_P, _I64, _P, _P]),
     "qssb_loss_batch": (ctypes.c_int, [
         _P, _P, _P, _P, ctypes.POINTER(Calibration), _P, _I32, _I32, _P, _SZ, _P, _P, _P]),
 }

@@ -1,0 +1,272 @@
+// qssb_mlp.cu - training and inference kernels of the learned aberration
+// proposer: BF16 tensor-core GEMMs with FP32 accumulation and fused bias/GELU
+// epilogues, the GELU backward, the MSE loss and its gradient, bias-gradient
+// reductions and an Adam step on FP32 master weights that refreshes the BF16
+// copies. No counterpart in the reference (it has no learned component).
+//
+// GEMM: C[M][N] = op(A)[M][K] * op(B)[K][N] (+ C when accumulate), A and B
+// BF16 with a per-operand transpose flag, FP32 accumulation in the tensor
+// cores (warp-level 16x16x16 BF16 MMA), M, N, K multiples of 16. Each warp
+// owns a 32x32 output tile; each CTA of 4 warps a 64x64 tile. The epilogue
+// adds a bias, stores the FP32 pre-activation and/or a BF16 copy of
+// GELU(pre) for the next layer.
+#include <cuda_bf16.h>
+#include <math.h>
+#include <mma.h>
+
+#include "qssb_internal.h"
+
+namespace qssb {
+
+using namespace nvcuda;
+
+constexpr int kGemmWarpTile = 32;
+constexpr int kGemmCtaTile = 64;
+
+// GELU with the tanh form: 0.5 x (1 + tanh(s (x + 0.044715 x^3))), s = sqrt(2/pi).
+__device__ __forceinline__ float gelu_f(float x) {
+    const float s = 0.7978845608028654f;
+    const float u = s * fmaf(0.044715f * x * x, x, x);
+    return 0.5f * x * (1.0f + tanhf(u));
+}
+
+__device__ __forceinline__ float gelu_grad(float x) {
+    const float s = 0.7978845608028654f;
+    const float x2 = x * x;
+    const float u = s * fmaf(0.044715f * x2, x, x);
+    const float t = tanhf(u);
+    const float du = s * fmaf(3.0f * 0.044715f, x2, 1.0f);
+    return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * du;
+}
+
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(128) k_gemm_bf16(
+    const __nv_bfloat16* __restrict__ A, int lda, const __nv_bfloat16* __restrict__ B, int ldb,
+    int M, int N, int K, const float* __restrict__ bias, int accumulate,
+    float* __restrict__ C, int ldc, __nv_bfloat16* __restrict__ act, int ld_act) {
+    using LA = typename std::conditional<TA, wmma::col_major, wmma::row_major>::type;
+    using LB = typename std::conditional<TB, wmma::col_major, wmma::row_major>::type;
+    __shared__ float stage[4][16 * 16];
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * kGemmCtaTile + (warp >> 1) * kGemmWarpTile;
+    const int n0 = blockIdx.x * kGemmCtaTile + (warp & 1) * kGemmWarpTile;
+    if (m0 >= M || n0 >= N) return;  // warp-uniform; no block barrier below
+    wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[2][2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 2; ++j) wmma::fill_fragment(acc[i][j], 0.0f);
+    const bool mi1 = m0 + 16 < M;
+    const bool nj1 = n0 + 16 < N;
+    for (int k = 0; k < K; k += 16) {
+        wmma::fragment<wmma::matrix_a, 16, 16, 16, __nv_bfloat16, LA> fa[2];
+        wmma::fragment<wmma::matrix_b, 16, 16, 16, __nv_bfloat16, LB> fb[2];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            if (i == 1 && !mi1) break;
+            const int m = m0 + 16 * i;
+            const __nv_bfloat16* pa = TA ? A + (size_t)k * lda + m : A + (size_t)m * lda + k;
+            wmma::load_matrix_sync(fa[i], pa, lda);
+        }
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            if (j == 1 && !nj1) break;
+            const int n = n0 + 16 * j;
+            const __nv_bfloat16* pb = TB ? B + (size_t)n * ldb + k : B + (size_t)k * ldb + n;
+            wmma::load_matrix_sync(fb[j], pb, ldb);
+        }
+#pragma unroll
+        for (int i = 0; i < 2; ++i)
+#pragma unroll
+            for (int j = 0; j < 2; ++j)
+                if ((i == 0 || mi1) && (j == 0 || nj1)) wmma::mma_sync(acc[i][j], fa[i], fb[j], acc[i][j]);
+    }
+    float* st = stage[warp];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            if ((i == 1 && !mi1) || (j == 1 && !nj1)) continue;
+            wmma::store_matrix_sync(st, acc[i][j], 16, wmma::mem_row_major);
+            __syncwarp();
+            for (int e = lane; e < 256; e += 32) {
+                const int r = m0 + 16 * i + (e >> 4);
+                const int c = n0 + 16 * j + (e & 15);
+                float v = st[e];
+                if (bias) v += bias[c];
+                if (C) {
+                    float* pc = C + (size_t)r * ldc + c;
+                    *pc = accumulate ? *pc + v : v;
+                }
+                if (act) act[(size_t)r * ld_act + c] = __float2bfloat16_rn(gelu_f(v));
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// dZ = dY * GELU'(pre), as BF16 for the next GEMMs and FP32 for the bias gradient.
+__global__ void k_gelu_backward(const float* __restrict__ dy, const float* __restrict__ pre,
+                                long long n, __nv_bfloat16* __restrict__ dz_bf,
+                                float* __restrict__ dz) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float g = dy[i] * gelu_grad(pre[i]);
+        dz[i] = g;
+        dz_bf[i] = __float2bfloat16_rn(g);
+    }
+}
+
+// db[c] = sum over rows of dz[r][c] (fixed order: one thread per column).
+__global__ void k_bias_grad(const float* __restrict__ dz, int rows, int cols,
+                            float* __restrict__ db) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= cols) return;
+    double s = 0.0;
+    for (int r = 0; r < rows; ++r) s += (double)dz[(size_t)r * cols + c];
+    db[c] = (float)s;
+}
+
+// MSE over the first n_out of ld columns: loss = mean (y - t)^2 over rows x n_out,
+// dy = 2 (y - t) / (rows * n_out) (zero in the padding columns).
+__global__ void __launch_bounds__(256) k_mse(const float* __restrict__ y, const float* __restrict__ t,
+                                             int rows, int n_out, int ld, float* __restrict__ dy,
+                                             float* __restrict__ loss) {
+    __shared__ double red[256];
+    const double scale = 1.0 / ((double)rows * n_out);
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < rows * ld; i += 256) {
+        const int r = i / ld;
+        const int c = i - r * ld;
+        float g = 0.0f;
+        if (c < n_out) {
+            const float d = y[i] - t[(size_t)r * n_out + c];
+            acc += (double)d * d;
+            g = (float)(2.0 * scale) * d;
+        }
+        dy[i] = g;
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && loss) *loss = (float)(red[0] * scale);
+}
+
+// Adam on FP32 master weights (bias-corrected), then the BF16 copy.
+__global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
+                       const float* __restrict__ g, long long n, float lr, float b1, float b2,
+                       float eps, float wd, float c1, float c2, __nv_bfloat16* __restrict__ w_bf) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = fmaf(b1, m[i], (1.0f - b1) * gi);
+        const float vi = fmaf(b2, v[i], (1.0f - b2) * gi * gi);
+        m[i] = mi;
+        v[i] = vi;
+        const float upd = (mi / c1) / (sqrtf(vi / c2) + eps) + wd * w[i];
+        const float wi = w[i] - lr * upd;
+        w[i] = wi;
+        if (w_bf) w_bf[i] = __float2bfloat16_rn(wi);
+    }
+}
+
+__global__ void k_to_bf16(const float* __restrict__ x, long long n, __nv_bfloat16* __restrict__ y) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        y[i] = __float2bfloat16_rn(x[i]);
+}
+
+static int grid_for(long long n) {
+    long long g = (n + 255) / 256;
+    const long long cap = 148LL * 16;
+    return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
+}  // namespace qssb
+
+using namespace qssb;
+
+extern "C" int qssb_gemm_bf16(const void* A, int32_t lda, int32_t trans_a, const void* B,
+                              int32_t ldb, int32_t trans_b, int32_t M, int32_t N, int32_t K,
+                              const float* bias, int32_t accumulate, float* C, int32_t ldc,
+                              void* act_bf16, int32_t ld_act, void* stream) {
+    if (!A || !B || (!C && !act_bf16))
+        return set_error(QSSB_ERR_INVALID, "qssb_gemm_bf16: null operand or no output");
+    if (M <= 0 || N <= 0 || K <= 0 || (M % 16) || (N % 16) || (K % 16))
+        return set_error(QSSB_ERR_INVALID, "qssb_gemm_bf16: M, N, K must be positive multiples of 16");
+    const int rows_a = trans_a ? K : M, cols_a = trans_a ? M : K;
+    const int rows_b = trans_b ? N : K, cols_b = trans_b ? K : N;
+    (void)rows_a;
+    (void)rows_b;
+    if (lda < cols_a || ldb < cols_b || (C && ldc < N) || (act_bf16 && ld_act < N) ||
+        (lda % 8) || (ldb % 8))
+        return set_error(QSSB_ERR_INVALID, "qssb_gemm_bf16: leading dimensions too small or not multiples of 8");
+    if (((uintptr_t)A & 31u) || ((uintptr_t)B & 31u))
+        return set_error(QSSB_ERR_INVALID, "qssb_gemm_bf16: A and B must be 32-byte aligned");
+    const dim3 grid((N + kGemmCtaTile - 1) / kGemmCtaTile, (M + kGemmCtaTile - 1) / kGemmCtaTile);
+    const auto* a = static_cast<const __nv_bfloat16*>(A);
+    const auto* b = static_cast<const __nv_bfloat16*>(B);
+    auto* act = static_cast<__nv_bfloat16*>(act_bf16);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (trans_a) {
+        if (trans_b) k_gemm_bf16<true, true><<<grid, 128, 0, s>>>(a, lda, b, ldb, M, N, K, bias, accumulate, C, ldc, act, ld_act);
+        else k_gemm_bf16<true, false><<<grid, 128, 0, s>>>(a, lda, b, ldb, M, N, K, bias, accumulate, C, ldc, act, ld_act);
+    } else {
+        if (trans_b) k_gemm_bf16<false, true><<<grid, 128, 0, s>>>(a, lda, b, ldb, M, N, K, bias, accumulate, C, ldc, act, ld_act);
+        else k_gemm_bf16<false, false><<<grid, 128, 0, s>>>(a, lda, b, ldb, M, N, K, bias, accumulate, C, ldc, act, ld_act);
+    }
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+extern "C" int qssb_gelu_backward(const float* dy, const float* pre, int64_t n, void* dz_bf16,
+                                  float* dz, void* stream) {
+    if (!dy || !pre || !dz_bf16 || !dz || n <= 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_gelu_backward: null pointer or empty");
+    k_gelu_backward<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+        dy, pre, n, static_cast<__nv_bfloat16*>(dz_bf16), dz);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+extern "C" int qssb_bias_grad(const float* dz, int32_t rows, int32_t cols, float* db, void* stream) {
+    if (!dz || !db || rows <= 0 || cols <= 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_bias_grad: null pointer or empty");
+    k_bias_grad<<<(cols + 127) / 128, 128, 0, (cudaStream_t)stream>>>(dz, rows, cols, db);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+extern "C" int qssb_mse(const float* y, const float* target, int32_t rows, int32_t n_out,
+                        int32_t ld, float* dy, float* loss, void* stream) {
+    if (!y || !target || !dy || rows <= 0 || n_out <= 0 || ld < n_out)
+        return set_error(QSSB_ERR_INVALID, "qssb_mse: null pointer or bad shape");
+    k_mse<<<1, 256, 0, (cudaStream_t)stream>>>(y, target, rows, n_out, ld, dy, loss);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+extern "C" int qssb_adam(float* w, float* m, float* v, const float* grad, int64_t n, float lr,
+                         float beta1, float beta2, float eps, float weight_decay, int32_t step,
+                         void* w_bf16, void* stream) {
+    if (!w || !m || !v || !grad || n <= 0 || step < 1)
+        return set_error(QSSB_ERR_INVALID, "qssb_adam: null pointer, empty or step < 1");
+    const float c1 = 1.0f - powf(beta1, (float)step);
+    const float c2 = 1.0f - powf(beta2, (float)step);
+    k_adam<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+        w, m, v, grad, n, lr, beta1, beta2, eps, weight_decay, c1, c2,
+        static_cast<__nv_bfloat16*>(w_bf16));
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+extern "C" int qssb_to_bf16(const float* x, int64_t n, void* y, void* stream) {
+    if (!x || !y || n <= 0) return set_error(QSSB_ERR_INVALID, "qssb_to_bf16: null pointer or empty");
+    k_to_bf16<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(x, n, static_cast<__nv_bfloat16*>(y));
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}

@@ -1,0 +1,513 @@
+"""Learned aberration proposer: trotter-amplitude features, an MLP trained on
+the SSB forward model with the library's own CUDA kernels, and the short
+batched SSB refinement its proposal seeds.
+
+No counterpart in the reference, whose fits search the whole prior box
+(Optuna TPE + Nelder-Mead, backend.py:958-1374). The pieces:
+
+* Features (``qssb_trotter_features`` / ``qssb_synth_features``): |G_b(Q)|
+  at 16 fixed scan frequencies Q = (m, n) / 32 A^-1 (on the fftfreq grid of
+  every scan whose extent N d is a multiple of 32 A), resampled onto a 32x32
+  grid over the aperture disk with a tent of the training detector's pitch
+  and normalised per Q: 16384 inputs, independent of dose and object contrast.
+* Training data: the SSB forward model of a weak-phase object,
+  G_b(Q) = Gamma(Q, k_b) Phi(Q) + noise, on a 64x64-scan x 64x64-detector
+  lattice (300 kV, 20 mrad, 20/12 mrad per pixel), aberrations uniform in the
+  sweep ranges (C1 +-50 nm, |A1| <= 10 nm, C3 <= 1 um), random Phi and noise;
+  each sample leaves a random subset of its 16 maps noise-dominated, as a
+  crystal does between its reflections.
+* Network: 16384 -> 512 -> 512 -> 512 -> 4, GELU, BF16 weights and
+  activations on the tensor cores with FP32 accumulation, FP32 master weights
+  and Adam (``qssb_gemm_bf16``, ``qssb_gelu_backward``, ``qssb_bias_grad``,
+  ``qssb_mse``, ``qssb_adam``). Outputs (C1, |A1| cos 2phi, |A1| sin 2phi, C3)
+  scaled to O(1).
+* Sign: trotter amplitudes are unchanged when every aberration flips sign
+  (Gamma -> conj Gamma), so targets are canonical (C1 >= 0) and a proposal
+  is two hypotheses, p and -p; the refinement tests both.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib, ops
+from ._lib import Calibration, check
+from .calibration import bf_geometry
+from .physics import electron_wavelength_angstrom
+from .synthetic import SWEEP_RANGES
+
+Q_UNITS = np.array([(4, 0), (8, 0), (12, 0), (16, 0), (0, 4), (0, 8), (0, 12), (0, 16),
+                    (3, 3), (6, 6), (9, 9), (12, 12), (3, -3), (6, -6), (9, -9), (12, -12)],
+                   dtype=np.int32)
+Q_PERIOD_A = 32.0          # Q = units / 32 A^-1
+GRID = 32
+K_MAX_FACTOR = 1.05        # grid half-width in units of the aperture radius alpha/lambda
+CELL_RADIUS_FACTOR = 0.9   # cells beyond 0.9 alpha/lambda stay empty: the BF sets of the
+                           # training lattice and of a selected dataset differ at the rim
+N_IN = len(Q_UNITS) * GRID * GRID
+HIDDEN = 512
+N_OUT = 4
+N_OUT_PAD = 16
+OUT_SCALE = np.array([500.0, 100.0, 100.0, 1.0e4], dtype=np.float32)
+
+# the training lattice (64x64 detector)
+TRAIN_VOLTAGE_KV = 300.0
+TRAIN_SEMIANGLE_MRAD = 20.0
+TRAIN_DET_SAMPLING_MRAD = 20.0 / 12.0
+TRAIN_DET = 64
+
+
+def _ptr(t):
+    return ctypes.c_void_p(0 if t is None else t.data_ptr())
+
+
+def _stream(dev):
+    return ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+
+def _call(name, dev, *args):
+    ops._call(name, dev, *args)
+
+
+# --------------------------------------------------------------- features
+def tent_half_width() -> float:
+    """Tent half-width (1/A): the training detector's pixel pitch."""
+    lam = electron_wavelength_angstrom(TRAIN_VOLTAGE_KV * 1e3)
+    return TRAIN_DET_SAMPLING_MRAD * 1e-3 / lam
+
+
+def k_max(semiangle_mrad: float, wavelength_A: float) -> float:
+    return K_MAX_FACTOR * semiangle_mrad * 1e-3 / wavelength_A
+
+
+def resample_table(kx: np.ndarray, ky: np.ndarray, kmax: float, h: float,
+                   grid: int = GRID, cell_radius: float | None = None
+                   ) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """CSR (cell -> BF pixels) tent weights, rows normalised to sum 1; cells whose
+    centre lies beyond ``cell_radius`` (1/A) are left empty."""
+    kx = np.asarray(kx, np.float64)
+    ky = np.asarray(ky, np.float64)
+    step = 2.0 * kmax / grid
+    centres = -kmax + (np.arange(grid) + 0.5) * step
+    rmax2 = np.inf if cell_radius is None else cell_radius * cell_radius
+    wx = 1.0 - np.abs(kx[None, :] - centres[:, None]) / h          # [grid, B]
+    wy = 1.0 - np.abs(ky[None, :] - centres[:, None]) / h
+    wx = np.where(wx > 0, wx, 0.0)
+    wy = np.where(wy > 0, wy, 0.0)
+    off = [0]
+    idx, wts = [], []
+    for i in range(grid):
+        nzx = np.nonzero(wx[i])[0]
+        for j in range(grid):
+            if centres[i] ** 2 + centres[j] ** 2 > rmax2:
+                off.append(off[-1])
+                continue
+            w = wx[i, nzx] * wy[j, nzx]
+            keep = w > 0
+            b = nzx[keep]
+            w = w[keep]
+            if w.size:
+                idx.append(b)
+                wts.append(w / w.sum())
+            off.append(off[-1] + int(w.size))
+    idx = np.concatenate(idx) if idx else np.zeros(0, np.int64)
+    wts = np.concatenate(wts) if wts else np.zeros(0)
+    return (np.asarray(off, np.int32), idx.astype(np.int32), wts.astype(np.float32))
+
+
+@dataclass
+class Lattice:
+    """Geometry of one feature source on the device: BF k-vectors and the CSR table."""
+
+    n_bf: int
+    off: torch.Tensor
+    idx: torch.Tensor
+    w: torch.Tensor
+
+
+def _lattice(kx: np.ndarray, ky: np.ndarray, kmax: float, device) -> Lattice:
+    off, idx, w = resample_table(kx, ky, kmax, tent_half_width(),
+                                 cell_radius=CELL_RADIUS_FACTOR * kmax / K_MAX_FACTOR)
+    if idx.size == 0:
+        idx = np.zeros(1, np.int32)
+        w = np.zeros(1, np.float32)
+    t = lambda a: torch.as_tensor(a, device=device)  # noqa: E731
+    return Lattice(int(len(kx)), t(off), t(idx), t(w))
+
+
+def backend_features(be) -> torch.Tensor:
+    """Features [1, N_IN] (BF16) of a prepared ``B200SSBBackend`` dataset."""
+    n = be.scan_shape[0]
+    extent = n * be.scan_sampling[0]
+    scale = extent / Q_PERIOD_A
+    if abs(scale - round(scale)) > 1e-6 or abs(be.scan_sampling[0] - be.scan_sampling[1]) > 1e-12:
+        raise ValueError("the proposer needs square scans whose extent is a multiple of 32 A")
+    q_idx = torch.as_tensor((Q_UNITS * int(round(scale))).astype(np.int32), device=be.device)
+    lat = getattr(be, "_proposer_lattice", None)
+    if lat is None:
+        geo = be._geom_dev[:2].cpu().numpy()
+        lat = _lattice(geo[0], geo[1], k_max(be.semiangle_cutoff, be.wavelength), be.device)
+        be._proposer_lattice = lat
+    nq = len(Q_UNITS)
+    scratch = torch.empty(nq * lat.n_bf, dtype=torch.float32, device=be.device)
+    out = torch.empty((1, N_IN), dtype=torch.bfloat16, device=be.device)
+    _call("qssb_trotter_features", be.device, _ptr(be.G_qk), lat.n_bf, n, _ptr(q_idx), nq,
+          _ptr(lat.off), _ptr(lat.idx), _ptr(lat.w), GRID * GRID, _ptr(scratch), None, _ptr(out),
+          _stream(be.device))
+    return out
+
+
+class TrainingLattice:
+    """The 64x64-detector lattice of the forward-model training data."""
+
+    def __init__(self, device):
+        self.device = torch.device(device)
+        lam = electron_wavelength_angstrom(TRAIN_VOLTAGE_KV * 1e3)
+        self.wavelength = lam
+        dk = TRAIN_DET_SAMPLING_MRAD * 1e-3 / lam
+        c = TRAIN_DET / 2.0
+        ii, jj = np.meshgrid(np.arange(TRAIN_DET), np.arange(TRAIN_DET), indexing="ij")
+        kr = (ii - c) * dk
+        kc = (jj - c) * dk
+        edge = (TRAIN_SEMIANGLE_MRAD * 1e-3 + 0.5 * TRAIN_DET_SAMPLING_MRAD * 1e-3) / lam
+        inside = (kr * kr + kc * kc) < edge * edge
+        rows, cols = np.nonzero(inside)
+        sampling = (1.0 / (dk * TRAIN_DET),) * 2
+        geo = bf_geometry(rows.astype(np.int32), cols.astype(np.int32), (c, c),
+                          (TRAIN_DET, TRAIN_DET), sampling, lam, TRAIN_SEMIANGLE_MRAD,
+                          (TRAIN_DET_SAMPLING_MRAD,) * 2, 0.0)
+        self.geom = torch.as_tensor(geo.stacked(), device=self.device).contiguous()
+        self.lattice = _lattice(geo.kx_bf, geo.ky_bf, k_max(TRAIN_SEMIANGLE_MRAD, lam), self.device)
+        self.q_vec = torch.as_tensor((Q_UNITS / Q_PERIOD_A).astype(np.float32), device=self.device)
+        self.cal = Calibration(
+            n_bf=self.lattice.n_bf, scan_rows=64, scan_cols=64, reserved=0, wavelength_A=lam,
+            semiangle_rad=TRAIN_SEMIANGLE_MRAD * 1e-3,
+            det_sampling_row_rad=TRAIN_DET_SAMPLING_MRAD * 1e-3,
+            det_sampling_col_rad=TRAIN_DET_SAMPLING_MRAD * 1e-3,
+            scan_sampling_row_A=0.5, scan_sampling_col_A=0.5, dc_re=1.0, dc_im=0.0)
+
+    def features(self, aberrations: np.ndarray, rng: np.random.Generator,
+                 sigma: tuple[float, float] = (0.02, 1.0), seed: int = 0,
+                 chunk: int = 4096) -> torch.Tensor:
+        """BF16 features [n, N_IN] of the forward model at ``aberrations`` [n, 4]."""
+        n = int(aberrations.shape[0])
+        nq = len(Q_UNITS)
+        out = torch.empty((n, N_IN), dtype=torch.bfloat16, device=self.device)
+        lat = self.lattice
+        for s in range(0, n, chunk):
+            e = min(n, s + chunk)
+            m = e - s
+            ab = torch.as_tensor(np.ascontiguousarray(aberrations[s:e], np.float32), device=self.device)
+            amp = np.exp(rng.uniform(np.log(0.2), np.log(5.0), size=(m, nq)))
+            ph = rng.uniform(0, 2 * np.pi, size=(m, nq))
+            # amplitude contrast: 0 .. 0.5 of the phase part, random phase
+            amp_a = amp * rng.uniform(0.0, 0.5, size=(m, nq))
+            ph_a = rng.uniform(0, 2 * np.pi, size=(m, nq))
+            phi = np.stack([np.stack([amp * np.cos(ph), amp * np.sin(ph)], axis=-1),
+                            np.stack([amp_a * np.cos(ph_a), amp_a * np.sin(ph_a)], axis=-1)],
+                           axis=2).astype(np.float32)     # [m, nq, 2, 2]
+            # one noise level per map: a crystal puts its signal into a few
+            # frequencies (reflections) and leaves the others noise-dominated,
+            # so each sample has 2..16 informative maps, the rest drowned
+            n_good = rng.integers(2, nq + 1, size=m)
+            good = rng.random((m, nq)).argsort(axis=1) < n_good[:, None]
+            lo = rng.uniform(np.log(sigma[0]), np.log(sigma[1]), size=(m, nq))
+            hi = rng.uniform(np.log(2.0), np.log(50.0), size=(m, nq))
+            sig = np.exp(np.where(good, lo, hi)).astype(np.float32)
+            phi_d = torch.as_tensor(phi, device=self.device)
+            sig_d = torch.as_tensor(sig, device=self.device)
+            scratch = torch.empty(m * nq * lat.n_bf, dtype=torch.float32, device=self.device)
+            _call("qssb_synth_features", self.device, _ptr(self.geom), lat.n_bf, _ptr(self.q_vec),
+                  nq, _ptr(ab), _ptr(phi_d), _ptr(sig_d), m, ctypes.byref(self.cal),
+                  ctypes.c_uint64(seed * 1_000_003 + s), _ptr(lat.off), _ptr(lat.idx), _ptr(lat.w),
+                  GRID * GRID, _ptr(scratch), None, _ptr(out[s:e]), _stream(self.device))
+        return out
+
+
+# ---------------------------------------------------------------- targets
+def canonical_targets(ab: np.ndarray) -> np.ndarray:
+    """(C10, C12, phi12, C30) -> scaled (C1, A1 cos 2phi, A1 sin 2phi, C3), with
+    every aberration's sign flipped where C1 < 0."""
+    ab = np.asarray(ab, np.float64)
+    s = np.where(ab[:, 0] < 0, -1.0, 1.0)
+    t = np.stack([s * ab[:, 0], s * ab[:, 1] * np.cos(2 * ab[:, 2]),
+                  s * ab[:, 1] * np.sin(2 * ab[:, 2]), s * ab[:, 3]], axis=1)
+    return (t / OUT_SCALE).astype(np.float32)
+
+
+def decode(pred: np.ndarray) -> np.ndarray:
+    """Scaled outputs [n, 4] -> aberrations (C10, C12, phi12, C30) [n, 4]."""
+    p = np.asarray(pred, np.float64) * OUT_SCALE
+    c12 = np.hypot(p[:, 1], p[:, 2])
+    phi = 0.5 * np.arctan2(p[:, 2], p[:, 1])
+    return np.stack([p[:, 0], c12, np.mod(phi, np.pi), p[:, 3]], axis=1)
+
+
+def flipped(ab: np.ndarray) -> np.ndarray:
+    """Every aberration negated: C10 -> -C10, A1 -> -A1 (phi12 + pi/2), C30 -> -C30."""
+    ab = np.array(ab, np.float64, ndmin=2)
+    return np.stack([-ab[:, 0], ab[:, 1], np.mod(ab[:, 2] + np.pi / 2, np.pi), -ab[:, 3]], axis=1)
+
+
+# -------------------------------------------------------------------- MLP
+class MLP:
+    """16384 -> 512 -> 512 -> 512 -> 4 (padded to 16), GELU, BF16 weights on the
+    tensor cores, FP32 master weights and Adam; every step in the C ABI."""
+
+    def __init__(self, device, seed: int = 0):
+        self.device = torch.device(device)
+        g = torch.Generator(device=self.device).manual_seed(seed)
+        dims = [N_IN, HIDDEN, HIDDEN, HIDDEN, N_OUT_PAD]
+        self.w, self.b = [], []
+        for i in range(4):
+            fan_in = dims[i]
+            w = torch.randn((dims[i], dims[i + 1]), generator=g, device=self.device) * math.sqrt(2.0 / fan_in)
+            if i == 3:
+                w[:, N_OUT:] = 0.0
+                w *= 0.1
+            self.w.append(w.contiguous())
+            self.b.append(torch.zeros(dims[i + 1], device=self.device))
+        self.dims = dims
+        self.w_bf = [w.to(torch.bfloat16).contiguous() for w in self.w]
+        self.m = [torch.zeros_like(t) for t in self.w + self.b]
+        self.v = [torch.zeros_like(t) for t in self.w + self.b]
+        self.t = 0
+        self._bufs: dict = {}
+
+    # buffers per batch size
+    def _buf(self, m: int) -> dict:
+        b = self._bufs.get(m)
+        if b is None:
+            dev = self.device
+            b = {
+                "z": [torch.empty((m, d), device=dev) for d in self.dims[1:]],
+                "a": [torch.empty((m, d), dtype=torch.bfloat16, device=dev) for d in self.dims[1:4]],
+                "dy": torch.empty((m, N_OUT_PAD), device=dev),
+                "dy_bf": torch.empty((m, N_OUT_PAD), dtype=torch.bfloat16, device=dev),
+                "da": [torch.empty((m, d), device=dev) for d in self.dims[1:4]],
+                "dz": [torch.empty((m, d), device=dev) for d in self.dims[1:4]],
+                "dz_bf": [torch.empty((m, d), dtype=torch.bfloat16, device=dev) for d in self.dims[1:4]],
+                "gw": [torch.empty_like(w) for w in self.w],
+                "gb": [torch.empty_like(x) for x in self.b],
+                "loss": torch.empty(1, device=dev),
+            }
+            self._bufs[m] = b
+        return b
+
+    def _gemm(self, a, lda, ta, bmat, ldb, tb, m, n, k, bias=None, c=None, ldc=0, act=None,
+              ld_act=0, accumulate=False):
+        _call("qssb_gemm_bf16", self.device, _ptr(a), lda, int(ta), _ptr(bmat), ldb, int(tb), m, n,
+              k, _ptr(bias), int(accumulate), _ptr(c), ldc, _ptr(act), ld_act, _stream(self.device))
+
+    def forward(self, x: torch.Tensor) -> torch.Tensor:
+        """x: BF16 [m, N_IN] (m a multiple of 16) -> FP32 [m, N_OUT_PAD]."""
+        m = int(x.shape[0])
+        if m % 16 or x.dtype != torch.bfloat16 or x.shape[1] != N_IN:
+            raise ValueError("x must be BF16 [m, 16384] with m a multiple of 16")
+        bf = self._buf(m)
+        inp = x
+        for i in range(4):
+            k, n = self.dims[i], self.dims[i + 1]
+            act = bf["a"][i] if i < 3 else None
+            self._gemm(inp, k, False, self.w_bf[i], n, False, m, n, k, bias=self.b[i],
+                       c=bf["z"][i], ldc=n, act=act, ld_act=n)
+            inp = act
+        self._x = x
+        return bf["z"][3]
+
+    def backward_and_step(self, target: torch.Tensor, lr: float, wd: float = 1e-5) -> torch.Tensor:
+        """MSE against target [m, N_OUT] (FP32), gradients, one Adam step; returns the loss (device)."""
+        bf = self._buf(int(target.shape[0]))
+        m = int(target.shape[0])
+        dev = self.device
+        _call("qssb_mse", dev, _ptr(bf["z"][3]), _ptr(target), m, N_OUT, N_OUT_PAD, _ptr(bf["dy"]),
+              _ptr(bf["loss"]), _stream(dev))
+        _call("qssb_to_bf16", dev, _ptr(bf["dy"]), m * N_OUT_PAD, _ptr(bf["dy_bf"]), _stream(dev))
+        grad_bf, grad_f = bf["dy_bf"], bf["dy"]
+        for i in (3, 2, 1, 0):
+            k, n = self.dims[i], self.dims[i + 1]
+            a_in = self._x if i == 0 else bf["a"][i - 1]
+            # dW_i = A_in^T dZ_i ; db_i = colsum dZ_i
+            self._gemm(a_in, k, True, grad_bf, n, False, k, n, m, c=bf["gw"][i], ldc=n)
+            _call("qssb_bias_grad", dev, _ptr(grad_f), m, n, _ptr(bf["gb"][i]), _stream(dev))
+            if i > 0:
+                # dA_{i-1} = dZ_i W_i^T, then through GELU'
+                self._gemm(grad_bf, n, False, self.w_bf[i], n, True, m, k, n, c=bf["da"][i - 1], ldc=k)
+                _call("qssb_gelu_backward", dev, _ptr(bf["da"][i - 1]), _ptr(bf["z"][i - 1]), m * k,
+                      _ptr(bf["dz_bf"][i - 1]), _ptr(bf["dz"][i - 1]), _stream(dev))
+                grad_bf, grad_f = bf["dz_bf"][i - 1], bf["dz"][i - 1]
+        self.t += 1
+        params = self.w + self.b
+        grads = bf["gw"] + bf["gb"]
+        for j, (p, gr) in enumerate(zip(params, grads)):
+            wbf = self.w_bf[j] if j < 4 else None
+            _call("qssb_adam", dev, _ptr(p), _ptr(self.m[j]), _ptr(self.v[j]), _ptr(gr), p.numel(),
+                  ctypes.c_float(lr), ctypes.c_float(0.9), ctypes.c_float(0.999),
+                  ctypes.c_float(1e-8), ctypes.c_float(wd if j < 4 else 0.0), self.t, _ptr(wbf),
+                  _stream(dev))
+        return bf["loss"]
+
+    def predict(self, x: torch.Tensor) -> np.ndarray:
+        m = int(x.shape[0])
+        pad = (-m) % 16
+        if pad:
+            x = torch.cat([x, torch.zeros((pad, N_IN), dtype=x.dtype, device=x.device)])
+        return self.forward(x)[:m, :N_OUT].cpu().numpy()
+
+
+class Proposer:
+    """Trains the MLP on forward-model features and proposes aberrations."""
+
+    def __init__(self, device, seed: int = 0):
+        self.device = torch.device(device)
+        self.lattice = TrainingLattice(self.device)
+        self.mlp = MLP(self.device, seed)
+        self.seed = seed
+        self.history: list[float] = []
+
+    def make_data(self, n: int, seed: int) -> tuple[torch.Tensor, torch.Tensor, np.ndarray]:
+        from .synthetic import draw_aberrations
+
+        rng = np.random.default_rng(seed)
+        ab = draw_aberrations(rng, n)
+        x = self.lattice.features(ab, rng, seed=seed)
+        t = torch.as_tensor(canonical_targets(ab), device=self.device)
+        return x, t, ab
+
+    def train(self, n_samples: int = 50_000, epochs: int = 40, batch: int = 256,
+              lr: float = 1e-3) -> dict:
+        x, t, _ = self.make_data(n_samples, self.seed)
+        steps_per_epoch = n_samples // batch
+        total = epochs * steps_per_epoch
+        g = torch.Generator(device=self.device).manual_seed(self.seed + 1)
+        step = 0
+        losses = []
+        for _ in range(epochs):
+            perm = torch.randperm(n_samples, generator=g, device=self.device)
+            for s in range(steps_per_epoch):
+                sel = perm[s * batch:(s + 1) * batch]
+                xb = x.index_select(0, sel).contiguous()
+                tb = t.index_select(0, sel).contiguous()
+                self.mlp.forward(xb)
+                cur = lr * 0.5 * (1.0 + math.cos(math.pi * step / total))
+                loss = self.mlp.backward_and_step(tb, cur)
+                step += 1
+                if s == steps_per_epoch - 1:
+                    losses.append(float(loss.item()))
+        self.history = losses
+        return {"epochs": epochs, "steps": step, "final_train_mse": losses[-1] if losses else None}
+
+    def validate(self, n: int = 2048, seed: int = 12345) -> dict:
+        x, t, _ = self.make_data(n, seed)
+        pred = self.mlp.predict(x)
+        err = pred - t.cpu().numpy()
+        return {"rmse_scaled": np.sqrt(np.mean(err ** 2, axis=0)).tolist(),
+                "rmse_units": (np.sqrt(np.mean(err ** 2, axis=0)) * OUT_SCALE).tolist()}
+
+    def propose(self, be) -> np.ndarray:
+        """Two hypotheses [2, 4] (C10, C12, phi12, C30): the canonical proposal and its flip."""
+        p = decode(self.mlp.predict(backend_features(be)))[0]
+        return np.stack([p, flipped(p)[0]])
+
+
+# ------------------------------------------------------------- refinement
+# Searches move in x = (C10, a, b, C30) with the astigmatism in Cartesian form
+# (a, b) = C12 (cos 2 phi12, sin 2 phi12), so a box around a point is a box.
+BOX_LO = np.array([SWEEP_RANGES["C10"][0], -SWEEP_RANGES["C12"][1], -SWEEP_RANGES["C12"][1],
+                   SWEEP_RANGES["C30"][0]])
+BOX_HI = np.array([SWEEP_RANGES["C10"][1], SWEEP_RANGES["C12"][1], SWEEP_RANGES["C12"][1],
+                   SWEEP_RANGES["C30"][1]])
+
+
+def to_x(ab: np.ndarray) -> np.ndarray:
+    ab = np.array(ab, np.float64, ndmin=2)
+    return np.stack([ab[:, 0], ab[:, 1] * np.cos(2 * ab[:, 2]), ab[:, 1] * np.sin(2 * ab[:, 2]),
+                     ab[:, 3]], axis=1)
+
+
+def from_x(x: np.ndarray) -> np.ndarray:
+    x = np.array(x, np.float64, ndmin=2)
+    return np.stack([x[:, 0], np.hypot(x[:, 1], x[:, 2]),
+                     np.mod(0.5 * np.arctan2(x[:, 2], x[:, 1]), np.pi), x[:, 3]], axis=1)
+
+
+def zoom_search(be, centres: np.ndarray | None, half_widths: np.ndarray, batch: int, rounds: int,
+                shrink: float, rng: np.random.Generator, done=None, lo=None, hi=None):
+    """Batched zoom search on the phase-variance loss in x = (C10, a, b, C30):
+    each round scores ``batch`` candidates in one ``qssb_loss_batch`` call (the
+    current best plus uniform draws in a box around it; the first round splits
+    them over ``centres``), keeps the best and shrinks the box by ``shrink``.
+    ``done(best_aberrations)`` ends it early. Returns (best (C10, C12, phi12,
+    C30), SSB evaluations, rounds)."""
+    lo = BOX_LO if lo is None else np.asarray(lo, np.float64)
+    hi = BOX_HI if hi is None else np.asarray(hi, np.float64)
+    w = np.asarray(half_widths, np.float64).copy()
+    if centres is None:  # no prior point: the first round spreads over the whole box
+        centres = np.empty((0, 4))
+    centres = np.clip(np.array(centres, np.float64, ndmin=2).reshape(-1, 4), lo, hi)
+    best_x, best_loss = (centres[0].copy() if len(centres) else (lo + hi) / 2), np.inf
+    evals = 0
+    for r in range(rounds):
+        if r == 0 and len(centres) == 0:
+            cand = lo + rng.random((batch, 4)) * (hi - lo)
+        elif r == 0:
+            per = max(1, batch // len(centres))
+            cand = []
+            for c in centres:
+                cand.append(c)
+                cand.extend(c + rng.uniform(-1, 1, size=(per - 1, 4)) * w)
+            cand = np.array(cand[:batch])
+            if len(cand) < batch:
+                cand = np.vstack([cand, centres[0] + rng.uniform(-1, 1, size=(batch - len(cand), 4)) * w])
+        else:
+            cand = np.vstack([best_x, best_x + rng.uniform(-1, 1, size=(batch - 1, 4)) * w])
+        cand = np.clip(cand, lo, hi)
+        ab = from_x(cand)
+        losses = be.variance_loss_batch(ab[:, 0], ab[:, 1], ab[:, 2], ab[:, 3]).cpu().numpy()
+        evals += batch
+        j = int(np.argmin(losses))
+        if losses[j] < best_loss:
+            best_x, best_loss = cand[j].copy(), float(losses[j])
+        w *= shrink
+        if done is not None and done(from_x(best_x)[0]):
+            return from_x(best_x)[0], evals, r + 1
+    return from_x(best_x)[0], evals, rounds
+
+
+def compass_search(be, start: np.ndarray, steps: np.ndarray, rounds: int, done=None,
+                   lo=None, hi=None, grow: float = 1.0, shrink: float = 0.5):
+    """Batched pattern search for the 8-candidate refinement: each round scores
+    the 8 points x +- s_i e_i (one ``qssb_loss_batch`` call); the best point
+    becomes the centre if it beats it, otherwise every step halves. The start
+    points (the proposal's two sign hypotheses) are scored first in one batch.
+    Returns (best (C10, C12, phi12, C30), SSB evaluations, rounds)."""
+    lo = BOX_LO if lo is None else np.asarray(lo, np.float64)
+    hi = BOX_HI if hi is None else np.asarray(hi, np.float64)
+    starts = np.clip(np.array(start, np.float64, ndmin=2).reshape(-1, 4), lo, hi)
+    ab = from_x(starts)
+    losses = be.variance_loss_batch(ab[:, 0], ab[:, 1], ab[:, 2], ab[:, 3]).cpu().numpy()
+    evals = len(starts)
+    j = int(np.argmin(losses))
+    x, fx = starts[j].copy(), float(losses[j])
+    s = np.asarray(steps, np.float64).copy()
+    if done is not None and done(from_x(x)[0]):
+        return from_x(x)[0], evals, 0
+    eye = np.eye(4)
+    for r in range(rounds):
+        cand = np.clip(np.vstack([x + s * eye, x - s * eye]), lo, hi)
+        ab = from_x(cand)
+        losses = be.variance_loss_batch(ab[:, 0], ab[:, 1], ab[:, 2], ab[:, 3]).cpu().numpy()
+        evals += len(cand)
+        j = int(np.argmin(losses))
+        if losses[j] < fx:
+            x, fx = cand[j].copy(), float(losses[j])
+            s *= grow
+        else:
+            s *= shrink
+        if done is not None and done(from_x(x)[0]):
+            return from_x(x)[0], evals, r + 1
+    return from_x(x)[0], evals, rounds

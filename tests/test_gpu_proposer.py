@@ -1,0 +1,150 @@
+"""The learned proposer's CUDA kernels against the FP64 oracle
+(oracle/proposer_oracle.py): forward-model features, features from a
+resident G, and the MLP's outputs and gradients; plus a short training run
+that must cut the validation error."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import proposer_oracle as po
+from oracle import ssb_oracle as so
+from quantem.gpu_b200 import _lib, proposer as pr
+from quantem.gpu_b200.synthetic import draw_aberrations
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+
+
+def _ptr(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _host_csr(lat):
+    return lat.off.cpu().numpy(), lat.idx.cpu().numpy(), lat.w.cpu().numpy()
+
+
+def test_synth_features_match_oracle():
+    tl = pr.TrainingLattice(DEV)
+    rng = np.random.default_rng(2)
+    ab = draw_aberrations(rng, 3)
+    nq = len(pr.Q_UNITS)
+    phi = np.zeros((3, nq, 2, 2), np.float32)
+    phi[:, :, 0, 0] = 1.0  # unit phase-object spectrum, no amplitude part
+    sig = np.zeros((3, nq), np.float32)
+    lat = tl.lattice
+    scratch = torch.empty(3 * nq * lat.n_bf, device=DEV)
+    out = torch.empty((3, pr.N_IN), device=DEV)
+    ab_d, phi_d, sig_d = (torch.as_tensor(a, device=DEV) for a in (ab, phi, sig))
+    _lib.check(_lib.load().qssb_synth_features(
+        _ptr(tl.geom), lat.n_bf, _ptr(tl.q_vec), nq, _ptr(ab_d), _ptr(phi_d), _ptr(sig_d), 3,
+        ctypes.byref(tl.cal), 0, _ptr(lat.off), _ptr(lat.idx), _ptr(lat.w), pr.GRID * pr.GRID,
+        _ptr(scratch), _ptr(out), None, ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)))
+    got = out.cpu().numpy().reshape(3, nq, -1)
+    g = tl.geom.cpu().numpy().astype(np.float64)
+    geo = so.Geometry(g[0], g[1], g[2], g[3], g[4], g[5], np.zeros(1), np.zeros(1), tl.wavelength,
+                      pr.TRAIN_SEMIANGLE_MRAD * 1e-3, pr.TRAIN_DET_SAMPLING_MRAD * 1e-3,
+                      pr.TRAIN_DET_SAMPLING_MRAD * 1e-3)
+    off, idx, w = _host_csr(lat)
+    qv = tl.q_vec.cpu().numpy().astype(np.float64)
+    for s in range(3):
+        a = so.Aberrations(*map(float, ab[s]))
+        vals = np.stack([np.abs(po.gamma(qv[q, 0], qv[q, 1], g[0] + g[6], g[1] + g[7], g[2], g[3],
+                                         g[4], g[5], a, geo)) for q in range(nq)])
+        want = po.resample(vals, off, idx, w)
+        np.testing.assert_allclose(got[s], want, atol=2e-3)
+
+
+def test_backend_features_match_oracle():
+    from quantem.gpu_b200 import B200SSBBackend
+    from quantem.gpu_b200.synthetic import CONFIGS, generate
+
+    spec = CONFIGS["plain_128x128_det128"]
+    be = B200SSBBackend(generate(spec, DEV).counts, semiangle=spec.semiangle_mrad,
+                        scan_sampling=spec.scan_step_A, det_sampling=spec.det_sampling_mrad,
+                        voltage_kV=spec.voltage_kV, device=DEV)
+    got = pr.backend_features(be).float().cpu().numpy().reshape(len(pr.Q_UNITS), -1)
+    g = be.G_qk.cpu().numpy()
+    n = be.scan_shape[0]
+    vals = []
+    for m, k in pr.Q_UNITS * 2:
+        r, c = m % n, k % n
+        if c > n // 2:
+            r, c = (n - r) % n, n - c
+        vals.append(np.abs(g[:, r, c]).astype(np.float64))
+    off, idx, w = _host_csr(be._proposer_lattice)
+    want = po.resample(np.stack(vals), off, idx, w)
+    np.testing.assert_allclose(got, want, rtol=1e-2, atol=1e-2)  # BF16 output
+
+
+def test_mlp_outputs_and_gradients_match_oracle():
+    mlp = pr.MLP(DEV, seed=3)
+    rng = np.random.default_rng(4)
+    m = 32
+    x = torch.as_tensor(rng.uniform(0, 2, size=(m, pr.N_IN)).astype(np.float32), device=DEV).to(torch.bfloat16)
+    t = torch.as_tensor(rng.normal(size=(m, pr.N_OUT)).astype(np.float32), device=DEV)
+    ws = [w.float().cpu().numpy().astype(np.float64) for w in mlp.w_bf]
+    bs = [b.cpu().numpy().astype(np.float64) for b in mlp.b]
+    loss_ref, y_ref, dws, dbs = po.mlp_loss_and_grads(x.float().cpu().numpy(), ws, bs,
+                                                       t.cpu().numpy(), pr.N_OUT)
+    y = mlp.forward(x).cpu().numpy()
+    np.testing.assert_allclose(y[:, :pr.N_OUT], y_ref[:, :pr.N_OUT], rtol=2e-2, atol=2e-2)
+    loss = mlp.backward_and_step(t, lr=0.0).item()
+    assert abs(loss - loss_ref) <= 2e-2 * loss_ref
+    bufs = mlp._buf(m)
+    for i in range(4):
+        for got, want in ((bufs["gw"][i].cpu().numpy(), dws[i]), (bufs["gb"][i].cpu().numpy(), dbs[i])):
+            rel = np.linalg.norm(got - want) / max(np.linalg.norm(want), 1e-30)
+            assert rel <= 3e-2, (i, rel)
+
+
+def test_short_training_cuts_validation_error():
+    prop = pr.Proposer(DEV, seed=5)
+    before = prop.validate(1024)["rmse_scaled"]
+    prop.train(n_samples=20_000, epochs=10, batch=256, lr=1e-3)
+    after = prop.validate(1024)["rmse_scaled"]
+    assert after[0] < 0.5 * before[0], (before, after)       # C1
+    assert np.mean(after[:3]) < 0.8 * np.mean(before[:3])     # C1 and A1
+
+
+def test_learned_proposal_needs_fewer_evaluations_than_plain_sweep():
+    """What the trained network gains: proposal + 8-candidate refinement reaches
+    a phase within 1e-3 rad RMS of the FP64 oracle (at the true aberrations)
+    with fewer SSB evaluations than the plain 64-candidate sweep."""
+    from oracle import ssb_torch_fp64 as tf
+    from quantem.gpu_b200 import B200SSBBackend
+    from quantem.gpu_b200.synthetic import SyntheticSpec, generate
+
+    prop = pr.Proposer(DEV, seed=0)
+    prop.train(n_samples=50_000, epochs=40)
+    rng = np.random.default_rng(77)
+    plain_total = learned_total = 0
+    for i in range(2):
+        ab = draw_aberrations(rng, 1)[0]
+        spec = SyntheticSpec(scan_shape=(64, 64), detector_shape=(64, 64),
+                             det_sampling_mrad=20.0 / 12.0, dose=1e6, C10=float(ab[0]),
+                             C12=float(ab[1]), phi12=float(ab[2]), C30=float(ab[3]), seed=100 + i)
+        counts = generate(spec, DEV).counts
+        be = B200SSBBackend(counts, semiangle=20.0, scan_sampling=0.5, det_sampling=20.0 / 12.0,
+                            voltage_kV=300, device=DEV)
+        padded = torch.as_tensor(so.pad_or_crop_scan(counts.cpu().numpy()), device=DEV)
+        prep = tf.prepare(padded, voltage_kV=300, semiangle_mrad=20.0, scan_sampling=0.5,
+                          det_sampling=20.0 / 12.0)
+        truth = tf.reconstruct(prep, so.Aberrations(*map(float, ab)))[1].cpu().numpy()
+
+        def ok(est):
+            ph = be.object_and_phase(*map(float, est))[1].cpu().numpy()
+            return float(np.sqrt(np.mean(so.wrapped_phase_error(ph, truth) ** 2))) <= 1e-3
+
+        _, pe, _ = pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64, 30, 0.75,
+                                  np.random.default_rng(1), done=ok)
+        best, le, _ = pr.zoom_search(be, pr.to_x(prop.propose(be)),
+                                     np.array([120.0, 40.0, 40.0, 5000.0]), 8, 60, 0.9,
+                                     np.random.default_rng(2), done=ok)
+        assert ok(best)
+        plain_total += pe
+        learned_total += le
+    assert learned_total * 2 <= plain_total, (learned_total, plain_total)
