@@ -151,6 +151,13 @@ int qssb_bf_geometry(const int32_t* bf_linear, const qssb_bf_info_t* info, int32
                      int32_t det_cols, int32_t capacity, const qssb_geometry_params_t* params,
                      float* bf_geom, void* stream);
 
+/* The same gather with the detector shape known: reads each frame's BF
+ * bounding box with 16-byte loads (det_cols a multiple of 8, counts and
+ * columns 16-byte aligned; otherwise it runs qssb_gather_bf_columns). */
+int qssb_gather_bf_columns_2d(const uint16_t* counts, int64_t n_frames, int32_t det_rows,
+                              int32_t det_cols, const int32_t* bf_linear, int32_t n_bf,
+                              uint16_t* columns, void* stream);
+
 /* Forward scan FFT of each BF image, Hermitian half plane:
  * g_half[b][r][c] = sum_R columns[b][R] exp(-2 pi i (r R_r/R0 + c R_c/R1)),
  * c in [0, R1/2]. Replaces cp.fft.fft2 + the half-plane slice of

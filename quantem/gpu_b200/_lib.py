@@ -106,6 +106,7 @@ SIGNATURES = {
     "qssb_last_error": (ctypes.c_char_p, []),
     "qssb_mean_dp_u64": (ctypes.c_int, [_P, _I64, _I32, _P, _P, _P]),
     "qssb_gather_bf_columns": (ctypes.c_int, [_P, _I64, _I32, _P, _I32, _P, _P]),
+    "qssb_gather_bf_columns_2d": (ctypes.c_int, [_P, _I64, _I32, _I32, _P, _I32, _P, _P]),
     "qssb_select_bf": (ctypes.c_int, [_P, _I32, _I32, _I64, ctypes.c_float, ctypes.c_float,
                                       _P, _P, _P, _P]),
     "qssb_bf_geometry": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, ctypes.POINTER(GeometryParams),

@@ -286,6 +286,112 @@ __global__ void __launch_bounds__(512, 1) k_scan_fft128(const uint16_t* __restri
     for (int i = tid; i < 128 * kScanHalf / 2; i += 512) dst[i] = h4[i];
 }
 
+// Persistent form of k_scan_fft128: one CTA per SM loops over BF images; the
+// next image is copied into a second staging buffer with cp.async (16-byte
+// global -> shared copies, L1 bypassed) while the current one is transformed,
+// so the 32 KB load of each image is off the critical path. Same arithmetic
+// and output as k_scan_fft128.
+struct ScanFft128PSmem {
+    static constexpr size_t t_bytes = sizeof(float2) * 64 * kG8Scratch;
+    static constexpr size_t h_bytes = sizeof(float2) * 128 * kScanHalf;
+    static constexpr size_t tw_bytes = sizeof(float2) * 128;
+    static constexpr size_t img_bytes = sizeof(uint16_t) * 128 * kImgPitch;
+    static constexpr size_t bytes = t_bytes + h_bytes + tw_bytes + 2 * img_bytes;
+};
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+__device__ __forceinline__ void stage_image_async(uint16_t* img, const uint16_t* columns, int b,
+                                                  int tid) {
+    const uint4* src = reinterpret_cast<const uint4*>(columns + (size_t)b * 128 * 128);
+    for (int i = tid; i < 128 * 128 / 8; i += 512) {
+        const int row = i >> 4;
+        const int col = (i & 15) * 8;
+        cp_async16(img + row * kImgPitch + col, src + i);
+    }
+    cp_async_commit();
+}
+
+__global__ void __launch_bounds__(512, 1) k_scan_fft128p(const uint16_t* __restrict__ columns,
+                                                         int n_bf, float2* __restrict__ g_half) {
+    extern __shared__ float4 smem4[];
+    char* base = reinterpret_cast<char*>(smem4);
+    float2* T = reinterpret_cast<float2*>(base);
+    float2* H = reinterpret_cast<float2*>(base + ScanFft128PSmem::t_bytes);
+    float2* tw = H + 128 * kScanHalf;
+    uint16_t* imgs = reinterpret_cast<uint16_t*>(base + ScanFft128PSmem::t_bytes +
+                                                 ScanFft128PSmem::h_bytes + ScanFft128PSmem::tw_bytes);
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int g = tid >> 3;  // group 0..63
+    const int s = tid & 7;   // sub-lane
+    fill_twiddles<128>(tw, tid, 512);
+    int buf = 0;
+    if (blockIdx.x < n_bf) stage_image_async(imgs, columns, blockIdx.x, tid);
+    for (int b = blockIdx.x; b < n_bf; b += gridDim.x) {
+        uint16_t* img = imgs + buf * 128 * kImgPitch;
+        cp_async_wait_all();
+        __syncthreads();  // the image is complete; the previous copy-out of H is done
+        const int nb = b + gridDim.x;
+        if (nb < n_bf) stage_image_async(imgs + (buf ^ 1) * 128 * kImgPitch, columns, nb, tid);
+        // row pairs
+        float2 v[16];
+        {
+            const uint16_t* r0 = img + (2 * g) * kImgPitch + s;
+            const uint16_t* r1 = r0 + kImgPitch;
+#pragma unroll
+            for (int n1 = 0; n1 < 16; ++n1) v[n1] = make_float2((float)r0[8 * n1], (float)r1[8 * n1]);
+        }
+        float2* Tg = T + g * kG8Scratch;
+        fft128_g8<-1>(v, Tg, s, tw);
+#pragma unroll
+        for (int t = 0; t < 16; ++t) Tg[fft128_g8_index(s, t)] = v[t];
+        __syncwarp();
+#pragma unroll
+        for (int m = 0; m < 9; ++m) {
+            const int c = s + 8 * m;
+            if (c <= 64) {
+                const float2 z = Tg[c];
+                const float2 zm = Tg[(128 - c) & 127];
+                H[(2 * g) * kScanHalf + c] = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+                H[(2 * g + 1) * kScanHalf + c] = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+            }
+        }
+        __syncthreads();
+        {
+            const int grp = lane >> 3;
+            const int col = 16 * (warp & 3) + 8 * (grp & 1) + 2 * (warp >> 2) + (grp >> 1);
+#pragma unroll
+            for (int n1 = 0; n1 < 16; ++n1) v[n1] = H[(s + 8 * n1) * kScanHalf + col];
+            fft128_g8<-1>(v, Tg, s, tw);
+#pragma unroll
+            for (int t = 0; t < 16; ++t) H[fft128_g8_index(s, t) * kScanHalf + col] = v[t];
+        }
+        if (warp == 0) {
+            const bool act = lane < 8;
+#pragma unroll
+            for (int n1 = 0; n1 < 16; ++n1) v[n1] = act ? H[(s + 8 * n1) * kScanHalf + 64] : make_float2(0.f, 0.f);
+            fft128_g8<-1>(v, Tg, s, tw);
+            if (act) {
+#pragma unroll
+                for (int t = 0; t < 16; ++t) H[fft128_g8_index(s, t) * kScanHalf + 64] = v[t];
+            }
+        }
+        __syncthreads();
+        const float4* h4 = reinterpret_cast<const float4*>(H);
+        float4* dst = reinterpret_cast<float4*>(g_half + (size_t)b * 128 * kScanHalf);
+        for (int i = tid; i < 128 * kScanHalf / 2; i += 512) dst[i] = h4[i];
+        buf ^= 1;
+    }
+    cp_async_wait_all();  // nothing left in flight at exit
+}
+
 }  // namespace qssb
 
 using namespace qssb;
@@ -334,6 +440,126 @@ extern "C" int qssb_mean_dp_u64(const uint16_t* counts, int64_t n_frames, int32_
     return QSSB_OK;
 }
 
+// Bounding-box gather. The BF pixels' bounding box (rows x columns rounded
+// out to 8 pixels = 16 bytes) is read per frame with coalesced 16-byte copies
+// into shared memory, 8 frames per tile; each BF column then receives its 8
+// frames as one 16-byte store. Persistent CTAs (two per SM) loop over frame
+// tiles with the next tile's box arriving by cp.async into a second buffer
+// while the current tile is written out. (DRAM fetches whole 128-byte lines,
+// so the box rows are read in full either way: ~12.5 KB per 128^2 frame.) A
+// box larger than the tile buffer falls back to direct element loads.
+constexpr int kGbF = 8;
+constexpr int kGbThreads = 256;
+constexpr int kGbMaxPix = 3072;  // box pixels per frame held in one buffer
+
+__device__ __forceinline__ void gb_cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+
+__global__ void __launch_bounds__(kGbThreads) k_gather_bbox(
+    const uint16_t* __restrict__ counts, long long n_frames, int det_rows, int det_cols,
+    const int32_t* __restrict__ bf_linear, int n_bf, uint16_t* __restrict__ columns) {
+    extern __shared__ uint4 smem_u4[];
+    uint16_t* tiles = reinterpret_cast<uint16_t*>(smem_u4);  // [2][kGbF][area]
+    __shared__ int s_box[4][kGbThreads / 32];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int npix = det_rows * det_cols;
+    int rmin = det_rows, rmax = -1, cmin = det_cols, cmax = -1;
+    for (int b = tid; b < n_bf; b += kGbThreads) {
+        const int lin = __ldg(bf_linear + b);
+        if (lin < 0 || lin >= npix) continue;
+        const int r = lin / det_cols, c = lin - (lin / det_cols) * det_cols;
+        rmin = min(rmin, r); rmax = max(rmax, r); cmin = min(cmin, c); cmax = max(cmax, c);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        rmin = min(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+        rmax = max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+        cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
+        cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+    }
+    if (lane == 0) {
+        s_box[0][warp] = rmin; s_box[1][warp] = rmax; s_box[2][warp] = cmin; s_box[3][warp] = cmax;
+    }
+    __syncthreads();
+    rmin = det_rows; rmax = -1; cmin = det_cols; cmax = -1;
+#pragma unroll
+    for (int w = 0; w < kGbThreads / 32; ++w) {
+        rmin = min(rmin, s_box[0][w]); rmax = max(rmax, s_box[1][w]);
+        cmin = min(cmin, s_box[2][w]); cmax = max(cmax, s_box[3][w]);
+    }
+    const long long n_tiles = (n_frames + kGbF - 1) / kGbF;
+    const int c0 = cmin & ~7;
+    const int width = rmax >= 0 ? ((cmax + 8) & ~7) - c0 : 0;   // multiple of 8 pixels
+    const int nr = rmax >= 0 ? rmax - rmin + 1 : 0;
+    const int area = nr * width;
+    if (area == 0 || area > kGbMaxPix) {
+        // direct path: one element per (frame, BF pixel)
+        for (long long t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+            const long long f0 = t * kGbF;
+            const int nf = (int)min((long long)kGbF, n_frames - f0);
+            for (int e = tid; e < nf * n_bf; e += kGbThreads) {
+                const int f = e / n_bf, b = e - (e / n_bf) * n_bf;
+                const int lin = __ldg(bf_linear + b);
+                const bool ok = lin >= 0 && lin < npix;
+                columns[(size_t)b * n_frames + f0 + f] =
+                    ok ? __ldcs(counts + (size_t)(f0 + f) * npix + lin) : (uint16_t)0;
+            }
+        }
+        return;
+    }
+    const int vpr = width / 8;
+    const int per_frame = nr * vpr;
+    auto stage = [&](long long t, uint16_t* dst) {
+        const long long f0 = t * kGbF;
+        const int nf = (int)min((long long)kGbF, n_frames - f0);
+        for (int e = tid; e < nf * per_frame; e += kGbThreads) {
+            const int f = e / per_frame;
+            const int rem = e - f * per_frame;
+            const int i = rem / vpr;
+            const int v = rem - i * vpr;
+            const uint4* src = reinterpret_cast<const uint4*>(
+                counts + (size_t)(f0 + f) * npix + (size_t)(rmin + i) * det_cols + c0) + v;
+            gb_cp_async16(reinterpret_cast<uint4*>(dst + (size_t)f * area + i * width) + v, src);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    const bool vec_out = (n_frames & 7) == 0;
+    int buf = 0;
+    if (blockIdx.x < n_tiles) stage(blockIdx.x, tiles);
+    for (long long t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();  // tile t is in; everyone is done with the other buffer
+        const long long tn = t + gridDim.x;
+        if (tn < n_tiles) stage(tn, tiles + (size_t)(buf ^ 1) * kGbF * kGbMaxPix);
+        const uint16_t* tile = tiles + (size_t)buf * kGbF * kGbMaxPix;
+        const long long f0 = t * kGbF;
+        const int nf = (int)min((long long)kGbF, n_frames - f0);
+        for (int b = tid; b < n_bf; b += kGbThreads) {
+            const int lin = __ldg(bf_linear + b);
+            const bool ok = lin >= 0 && lin < npix;
+            const int r = ok ? lin / det_cols : rmin;
+            const int c = ok ? lin - r * det_cols : c0;
+            const int pos = (r - rmin) * width + (c - c0);
+            uint16_t* dst = columns + (size_t)b * n_frames + f0;
+            if (vec_out && nf == kGbF) {
+                uint32_t w[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    w[k] = ok ? ((uint32_t)tile[(2 * k) * area + pos] |
+                                 ((uint32_t)tile[(2 * k + 1) * area + pos] << 16)) : 0u;
+                *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+            } else {
+                for (int f = 0; f < nf; ++f) dst[f] = ok ? tile[f * area + pos] : (uint16_t)0;
+            }
+        }
+        buf ^= 1;
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 extern "C" int qssb_gather_bf_columns(const uint16_t* counts, int64_t n_frames, int32_t det_pixels,
                                       const int32_t* bf_linear, int32_t n_bf, uint16_t* columns,
                                       void* stream) {
@@ -347,6 +573,31 @@ extern "C" int qssb_gather_bf_columns(const uint16_t* counts, int64_t n_frames, 
         return set_error(QSSB_ERR_INVALID, "qssb_gather_bf_columns: grid too large");
     k_gather_columns<<<dim3((unsigned)gx, gy), 256, 0, (cudaStream_t)stream>>>(
         counts, n_frames, det_pixels, bf_linear, n_bf, columns);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+extern "C" int qssb_gather_bf_columns_2d(const uint16_t* counts, int64_t n_frames,
+                                         int32_t det_rows, int32_t det_cols,
+                                         const int32_t* bf_linear, int32_t n_bf,
+                                         uint16_t* columns, void* stream) {
+    if (!counts || !bf_linear || !columns || n_frames <= 0 || det_rows <= 0 || det_cols <= 0 ||
+        n_bf <= 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_gather_bf_columns_2d: null pointer or empty shape");
+    if ((int64_t)det_rows * det_cols > 0x7fffffff)
+        return set_error(QSSB_ERR_INVALID, "qssb_gather_bf_columns_2d: detector too large");
+    const bool vec_ok = (det_cols % 8) == 0 && ((uintptr_t)counts & 15u) == 0 &&
+                        ((uintptr_t)columns & 15u) == 0;
+    if (!vec_ok)  // rows not 16-byte aligned: the tile gather
+        return qssb_gather_bf_columns(counts, n_frames, det_rows * det_cols, bf_linear, n_bf,
+                                      columns, stream);
+    const long long n_tiles = (n_frames + kGbF - 1) / kGbF;
+    long long gx = 2LL * device_sm_count();
+    if (gx > n_tiles) gx = n_tiles;
+    const int smem = (int)(sizeof(uint16_t) * 2 * kGbF * kGbMaxPix);
+    CUDA_TRY(cudaFuncSetAttribute(k_gather_bbox, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_gather_bbox<<<(unsigned)gx, kGbThreads, smem, (cudaStream_t)stream>>>(
+        counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns);
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -446,10 +697,11 @@ extern "C" int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t
     switch (scan_rows) {
         case 64: return launch_scan_fft<64>(columns, n_bf, g_half, s);
         case 128: {
-            const size_t smem = ScanFft128Smem::bytes;
-            CUDA_TRY(cudaFuncSetAttribute(k_scan_fft128, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            const size_t smem = ScanFft128PSmem::bytes;
+            CUDA_TRY(cudaFuncSetAttribute(k_scan_fft128p, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
-            k_scan_fft128<<<n_bf, 512, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half));
+            const int grid = n_bf < device_sm_count() ? n_bf : device_sm_count();
+            k_scan_fft128p<<<grid, 512, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half));
             CUDA_TRY(cudaGetLastError());
             return QSSB_OK;
         }

@@ -21,6 +21,7 @@ LAUNCHES_PER_CALL = {
     "qssb_select_bf": 1,
     "qssb_bf_geometry": 1,
     "qssb_gather_bf_columns": 1,
+    "qssb_gather_bf_columns_2d": 1,
     "qssb_scan_fft_half": 1,
     "qssb_object": 4,
     "qssb_loss_batch": 3,
@@ -242,7 +243,7 @@ def gather_bf_columns(counts: torch.Tensor, bf_linear: torch.Tensor, validate: b
     if validate and n_bf and (int(bf_linear.min()) < 0 or int(bf_linear.max()) >= k0 * k1):
         raise ValueError("bf_linear indices must lie in [0, K0*K1)")
     out = torch.empty((n_bf, n_frames), dtype=torch.uint16, device=counts.device)
-    _call("qssb_gather_bf_columns", counts.device, _ptr(counts), n_frames, k0 * k1,
+    _call("qssb_gather_bf_columns_2d", counts.device, _ptr(counts), n_frames, k0, k1,
           _ptr(bf_linear), n_bf, _ptr(out), _stream(counts))
     return out
 

@@ -193,6 +193,20 @@ def test_gather_is_bit_exact(n_frames, npix, n_bf):
     np.testing.assert_array_equal(cols.cpu().numpy(), data[:, lin].T)
 
 
+@pytest.mark.parametrize("n_frames,det,radius", [(16384, 128, 24.0), (1000, 64, 12.0),
+                                                 (77, 128, 40.0), (4096, 96, 70.0)])
+def test_bbox_gather_is_bit_exact(n_frames, det, radius):
+    """The bounding-box gather (qssb_gather_bf_columns_2d) on disk-shaped BF
+    sets: full and ragged frame tiles, a box too large for the shared tile."""
+    rng = np.random.default_rng(n_frames + det)
+    counts = rng.integers(0, 65536, size=(n_frames, det, det), dtype=np.uint16)
+    rr, cc = np.meshgrid(np.arange(det), np.arange(det), indexing="ij")
+    disk = (rr - det / 2 + 0.3) ** 2 + (cc - det / 2 - 0.2) ** 2 <= radius ** 2
+    lin = np.nonzero(disk.reshape(-1))[0].astype(np.int32)
+    cols = ops.gather_bf_columns(_dev(counts), _dev(lin)).cpu().numpy()
+    np.testing.assert_array_equal(cols, counts.reshape(n_frames, -1)[:, lin].T)
+
+
 # -------------------------------------------------------------- scan FFT
 @pytest.mark.parametrize("n", [64, 128, 256])
 def test_scan_fft_half_matches_fp64(n):
