@@ -181,6 +181,16 @@ int qssb_object(const float* g_half, const float* bf_geom, const float* q_row,
                 const qssb_aberrations_t* ab, int32_t flags, void* workspace,
                 size_t workspace_bytes, float* object, float* phase, void* stream);
 
+/* qssb_object with dc read from device memory at run time: dc_device points
+ * to two doubles (re, im) - e.g. &info->dc_re of a qssb_bf_info_t written by
+ * qssb_select_bf - or is NULL to use cal->dc_re/dc_im. Lets a captured CUDA
+ * graph serve datasets whose dc differs. */
+int qssb_object_ex(const float* g_half, const float* bf_geom, const float* q_row,
+                   const float* q_col, const qssb_calibration_t* cal,
+                   const qssb_aberrations_t* ab, int32_t flags, const double* dc_device,
+                   void* workspace, size_t workspace_bytes, float* object, float* phase,
+                   void* stream);
+
 /* Capacity of the fixed device scratch used by qssb_object_noalloc. */
 #define QSSB_NOALLOC_SCRATCH_BYTES (16u << 20)
 

@@ -117,6 +117,9 @@ SIGNATURES = {
     "qssb_object": (ctypes.c_int, [
         _P, _P, _P, _P, ctypes.POINTER(Calibration), ctypes.POINTER(Aberrations), _I32, _P, _SZ,
         _P, _P, _P]),
+    "qssb_object_ex": (ctypes.c_int, [
+        _P, _P, _P, _P, ctypes.POINTER(Calibration), ctypes.POINTER(Aberrations), _I32, _P, _P, _SZ,
+        _P, _P, _P]),
     "qssb_object_noalloc": (ctypes.c_int, [
         _P, _P, _P, _P, ctypes.POINTER(Calibration), ctypes.POINTER(Aberrations), _I32, _P, _P, _P]),
     "qssb_loss_workspace_bytes": (

@@ -255,7 +255,7 @@ constexpr int kFoldSlices = 8;
 template <int N, bool SYM>
 __global__ void __launch_bounds__(32 * kFoldSlices) k_trotter_plane(
     const float2* __restrict__ partial, int n_chunks, int n_bf, float2 dc,
-    float2* __restrict__ plane) {
+    const double* __restrict__ dc_dev, float2* __restrict__ plane) {
     constexpr int H = N / 2 + 1;
     constexpr int NQ = n_eval_q<N, SYM>();
     __shared__ double2 red[kFoldSlices][32];
@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(32 * kFoldSlices) k_trotter_plane(
     const double inv_b = 1.0 / (double)n_bf;
     // S(-q) = -conj(S(q)): real part flips, imaginary part stays
     float2 out = make_float2((float)((mirror ? -tr : tr) * inv_b), (float)(ti * inv_b));
-    if (r == 0 && c == 0) out = dc;
+    if (r == 0 && c == 0) out = dc_dev ? make_float2((float)dc_dev[0], (float)dc_dev[1]) : dc;
     plane[idx] = out;
 }
 
@@ -395,7 +395,8 @@ int validate_calibration(const qssb_calibration_t* cal, const char* who) {
 template <int N, bool SYM, bool CHI64, bool QUAD>
 static int launch_object(const float* g_half, const float* geom, const float* q_row,
                          const float* q_col, const qssb_calibration_t& cal, const Probe& p,
-                         int chunks, char* ws, float* object, float* phase, cudaStream_t s) {
+                         int chunks, const double* dc_dev, char* ws, float* object, float* phase,
+                         cudaStream_t s) {
     const ObjectPlan pl = plan_object(N, cal.n_bf, SYM, chunks);
     float2* partial = reinterpret_cast<float2*>(ws);
     float2* plane = reinterpret_cast<float2*>(ws + pl.partial_bytes);
@@ -412,7 +413,8 @@ static int launch_object(const float* g_half, const float* geom, const float* q_
     }
     CUDA_TRY(cudaGetLastError());
     k_trotter_plane<N, SYM><<<(N * N + 31) / 32, 32 * kFoldSlices, 0, s>>>(
-        partial, pl.n_chunks, cal.n_bf, make_float2((float)cal.dc_re, (float)cal.dc_im), plane);
+        partial, pl.n_chunks, cal.n_bf, make_float2((float)cal.dc_re, (float)cal.dc_im), dc_dev,
+        plane);
     CUDA_TRY(cudaGetLastError());
     k_ifft_rows<N><<<N / 8, 256, 0, s>>>(plane);
     CUDA_TRY(cudaGetLastError());
@@ -424,24 +426,24 @@ static int launch_object(const float* g_half, const float* geom, const float* q_
 template <int N, bool QUAD>
 static int dispatch_object_q(bool sym, bool chi64, const float* g_half, const float* geom,
                              const float* q_row, const float* q_col, const qssb_calibration_t& cal,
-                             const Probe& p, int chunks, char* ws, float* object, float* phase,
-                             cudaStream_t s) {
+                             const Probe& p, int chunks, const double* dc_dev, char* ws,
+                             float* object, float* phase, cudaStream_t s) {
     if (sym) {
-        return chi64 ? launch_object<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, ws, object, phase, s)
-                     : launch_object<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, ws, object, phase, s);
+        return chi64 ? launch_object<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, dc_dev, ws, object, phase, s)
+                     : launch_object<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, dc_dev, ws, object, phase, s);
     }
-    return chi64 ? launch_object<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, ws, object, phase, s)
-                 : launch_object<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, ws, object, phase, s);
+    return chi64 ? launch_object<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, dc_dev, ws, object, phase, s)
+                 : launch_object<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, dc_dev, ws, object, phase, s);
 }
 
 template <int N>
 static int dispatch_object(bool sym, bool chi64, const float* g_half, const float* geom,
                            const float* q_row, const float* q_col, const qssb_calibration_t& cal,
-                           const Probe& p, int chunks, char* ws, float* object, float* phase,
-                           cudaStream_t s) {
+                           const Probe& p, int chunks, const double* dc_dev, char* ws,
+                           float* object, float* phase, cudaStream_t s) {
     if (p.quadratic)
-        return dispatch_object_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, p, chunks, ws, object, phase, s);
-    return dispatch_object_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, p, chunks, ws, object, phase, s);
+        return dispatch_object_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, p, chunks, dc_dev, ws, object, phase, s);
+    return dispatch_object_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, p, chunks, dc_dev, ws, object, phase, s);
 }
 
 }  // namespace qssb
@@ -461,10 +463,13 @@ extern "C" int qssb_object_workspace_bytes(const qssb_calibration_t* cal, int32_
     return QSSB_OK;
 }
 
-extern "C" int qssb_object(const float* g_half, const float* bf_geom, const float* q_row,
-                           const float* q_col, const qssb_calibration_t* cal,
-                           const qssb_aberrations_t* ab, int32_t flags, void* workspace,
-                           size_t workspace_bytes, float* object, float* phase, void* stream) {
+extern "C" int qssb_object_ex(const float* g_half, const float* bf_geom, const float* q_row,
+                              const float* q_col, const qssb_calibration_t* cal,
+                              const qssb_aberrations_t* ab, int32_t flags, const double* dc_device,
+                              void* workspace, size_t workspace_bytes, float* object, float* phase,
+                              void* stream) {
+    if (dc_device && ((uintptr_t)dc_device & 7u) != 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_object_ex: dc_device must be 8-byte aligned");
     int rc = validate_calibration(cal, "qssb_object: null calibration");
     if (rc) return rc;
     if (!g_half || !bf_geom || !q_row || !q_col || !ab || !workspace || !object)
@@ -481,14 +486,23 @@ extern "C" int qssb_object(const float* g_half, const float* bf_geom, const floa
     const bool sym = !(flags & QSSB_FLAG_FULL_PLANE);
     const bool chi64 = (flags & QSSB_FLAG_CHI_FP64) != 0;
     const int chunks = flag_chunks(flags);
+    const double* dc_dev = dc_device;
     cudaStream_t s = (cudaStream_t)stream;
     char* ws = static_cast<char*>(workspace);
     switch (cal->scan_rows) {
-        case 64: return dispatch_object<64>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, ws, object, phase, s);
-        case 128: return dispatch_object<128>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, ws, object, phase, s);
-        case 256: return dispatch_object<256>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, ws, object, phase, s);
+        case 64: return dispatch_object<64>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
+        case 128: return dispatch_object<128>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
+        case 256: return dispatch_object<256>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
         default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_object: scan size must be 64, 128 or 256");
     }
+}
+
+extern "C" int qssb_object(const float* g_half, const float* bf_geom, const float* q_row,
+                           const float* q_col, const qssb_calibration_t* cal,
+                           const qssb_aberrations_t* ab, int32_t flags, void* workspace,
+                           size_t workspace_bytes, float* object, float* phase, void* stream) {
+    return qssb_object_ex(g_half, bf_geom, q_row, q_col, cal, ab, flags, nullptr, workspace,
+                          workspace_bytes, object, phase, stream);
 }
 
 // ---------------------------------------------------------------------------

@@ -24,6 +24,7 @@ LAUNCHES_PER_CALL = {
     "qssb_gather_bf_columns_2d": 1,
     "qssb_scan_fft_half": 1,
     "qssb_object": 4,
+    "qssb_object_ex": 4,
     "qssb_loss_batch": 3,
 }
 LAUNCH_COUNT = 0
@@ -272,7 +273,8 @@ def object_workspace_bytes(cal: Calibration, flags: int = 0) -> int:
 
 def object_wave(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
                 q_col: torch.Tensor, cal: Calibration, ab: Aberrations, *, flags: int = 0,
-                workspace: Workspace | None = None, want_phase: bool = True
+                workspace: Workspace | None = None, want_phase: bool = True,
+                dc_device: torch.Tensor | None = None, out: tuple | None = None
                 ) -> tuple[torch.Tensor, torch.Tensor | None]:
     """Object wave (complex64 [R0, R1]) and its phase (float32) for one candidate."""
     _require_cuda(g_half, "g_half", torch.complex64)
@@ -286,11 +288,19 @@ def object_wave(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor
     ws = workspace or Workspace(g_half.device)
     need = object_workspace_bytes(cal, flags)
     buf = ws.get(need)
-    obj = torch.empty((r0, r1), dtype=torch.complex64, device=g_half.device)
-    ph = torch.empty((r0, r1), dtype=torch.float32, device=g_half.device) if want_phase else None
-    _call("qssb_object", g_half.device, _ptr(g_half), _ptr(bf_geom), _ptr(q_row), _ptr(q_col),
-          ctypes.byref(cal), ctypes.byref(ab), int(flags), _ptr(buf), buf.numel(), _ptr(obj),
-          _ptr(ph), _stream(g_half))
+    if out is not None:
+        obj, ph = out
+    else:
+        obj = torch.empty((r0, r1), dtype=torch.complex64, device=g_half.device)
+        ph = torch.empty((r0, r1), dtype=torch.float32, device=g_half.device) if want_phase else None
+    if dc_device is None:
+        _call("qssb_object", g_half.device, _ptr(g_half), _ptr(bf_geom), _ptr(q_row), _ptr(q_col),
+              ctypes.byref(cal), ctypes.byref(ab), int(flags), _ptr(buf), buf.numel(), _ptr(obj),
+              _ptr(ph), _stream(g_half))
+    else:
+        _call("qssb_object_ex", g_half.device, _ptr(g_half), _ptr(bf_geom), _ptr(q_row),
+              _ptr(q_col), ctypes.byref(cal), ctypes.byref(ab), int(flags), _ptr(dc_device),
+              _ptr(buf), buf.numel(), _ptr(obj), _ptr(ph), _stream(g_half))
     return obj, ph
 
 
