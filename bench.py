@@ -635,7 +635,7 @@ def run_b200(args, world, rank, local) -> None:
     print(json.dumps(line), flush=True)
 
 
-def run_profile_once(local: int) -> None:
+def run_profile_once(local: int, with_256: bool = False) -> None:
     """One cold reconstruction, one warm object, one loss and one 64-candidate
     loss batch on the 128^4 workload, untimed: the launch sequence the ncu
     summaries under profiles/ are captured from."""
@@ -650,8 +650,15 @@ def run_profile_once(local: int) -> None:
     loss = be.variance_loss(10.0, 5.0, 0.1)
     losses = be.variance_loss_batch(np.linspace(-50.0, 50.0, 64), 0.0, 0.0)
     torch.cuda.synchronize(dev)
-    print(json.dumps({"profile_once": True, "n_bf": be.num_bf, "loss": loss,
-                      "loss_batch0": float(losses[0])}))
+    out = {"profile_once": True, "n_bf": be.num_bf, "loss": loss, "loss_batch0": float(losses[0])}
+    if with_256:
+        del be, counts
+        spec = CONFIGS["stress_256x256_det128"]
+        c256 = generate(spec, device=dev).counts
+        be = B200SSBBackend(c256, device=dev, **KW)
+        out["loss256"] = float(be.variance_loss_batch([spec.C10], [0.0], [0.0])[0])
+        torch.cuda.synchronize(dev)
+    print(json.dumps(out))
 
 
 def main() -> None:
@@ -662,6 +669,8 @@ def main() -> None:
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-oracle", action="store_true")
+    ap.add_argument("--with-256", action="store_true",
+                    help="--profile-once: also one 256^2 scan loss evaluation")
     ap.add_argument("--no-stress", action="store_true",
                     help="skip the 256^2 dose sweep against the FP64 GPU path")
     ap.add_argument("--no-reference-cuda", action="store_true",
@@ -672,7 +681,7 @@ def main() -> None:
     world, rank, local = _dist()
     try:
         if args.profile_once:
-            run_profile_once(local)
+            run_profile_once(local, args.with_256)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
