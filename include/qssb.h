@@ -236,6 +236,35 @@ int qssb_loss_batch(const float* g_half, const float* bf_geom, const float* q_ro
                     void* workspace, size_t workspace_bytes, float* losses,
                     float* mean_phase, void* stream);
 
+/* The 14 Krivanek coefficients of one candidate, slots C10, C12, C21, C23,
+ * C30, C32, C34, C41, C43, C45, C50, C52, C54, C56 (aberration.py:63,
+ * engine.py:1244-1262): magnitudes in the length unit of C10 (Angstrom, as
+ * qssb_aberrations_t), angles phi_nm in radians (ignored for m = 0 slots).
+ * chi = (2 pi / lambda) sum alpha^(n+1) C_nm / (n+1) cos(m (phi - phi_nm))
+ * (chi_full and pack_aberration_coefs, common.py:410-471, 646-674). */
+#define QSSB_FULL_TERMS 14
+typedef struct qssb_full_aberrations {
+    float magnitude[QSSB_FULL_TERMS];
+    float angle_rad[QSSB_FULL_TERMS];
+} qssb_full_aberrations_t;
+
+/* Workspace bytes needed by qssb_loss_batch_full for n_cand candidates. */
+int qssb_loss_full_workspace_bytes(const qssb_calibration_t* cal, int32_t n_cand,
+                                   int32_t flags, size_t* bytes);
+
+/* qssb_loss_batch with the 14-term chi: replaces reconstruct_full /
+ * reconstruct_full_with_loss (engine.py:1244-1458; the reference raises
+ * NotImplementedError at 128, engine.py:1276-1280, 1373-1377 - this entry
+ * serves 64, 128 and 256). Odd-m terms break C(-q) = -conj C(q), so every
+ * scan frequency is evaluated. candidates: DEVICE array of n_cand
+ * qssb_full_aberrations_t. Flags: QSSB_FLAG_CHI_FP64 (chi from FP64 q and k,
+ * reduced in FP64) and QSSB_FLAG_CHUNKS; the others are ignored. */
+int qssb_loss_batch_full(const float* g_half, const float* bf_geom, const float* q_row,
+                         const float* q_col, const qssb_calibration_t* cal,
+                         const qssb_full_aberrations_t* candidates, int32_t n_cand,
+                         int32_t flags, void* workspace, size_t workspace_bytes,
+                         float* losses, float* mean_phase, void* stream);
+
 /* ------------------------------------------------------------------------
  * Learned aberration proposer (no counterpart in the reference, which has no
  * learned component). Features: trotter amplitudes |G_b(Q)| at n_q scan

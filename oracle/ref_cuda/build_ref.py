@@ -49,13 +49,37 @@ def _string_constants(path: Path, names: set[str]) -> dict[str, str]:
     return found
 
 
+# Our probe kernel (not reference code): evaluates the reference's own device
+# functions chi_full and gamma_mul_pk_onthefly_full (common.py:410-532)
+# element-wise, so the 14-term chi convention can be checked on a GPU.
+FULL_PROBE_NAME = "qref_full_chi_probe"
+FULL_PROBE_SOURCE = """
+__global__ void qref_full_chi_probe(
+    const float* qx, const float* qy, const float* kx, const float* ky, int n,
+    float wavelength, float semiangle_rad, float ang_y_rad, float ang_x_rad,
+    const float* mag_scaled, const float* cm, const float* sm, const float* pk,
+    const float* g, float* chi_qmk, float* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    chi_qmk[i] = chi_full(qx[i] - kx[i], qy[i] - ky[i], wavelength, mag_scaled, cm, sm);
+    const float2 v = gamma_mul_pk_onthefly_full(
+        qx[i], qy[i], kx[i], ky[i], wavelength, semiangle_rad, ang_y_rad, ang_x_rad,
+        mag_scaled, cm, sm, pk[2 * i], pk[2 * i + 1], make_float2(g[2 * i], g[2 * i + 1]));
+    out[2 * i] = v.x;
+    out[2 * i + 1] = v.y;
+}
+"""
+
+
 def module_source(reference: Path) -> str:
-    """The CUDA module text the reference's CustomFFT128 hands to NVRTC."""
+    """The CUDA module text the reference's CustomFFT128 hands to NVRTC, plus
+    the element-wise probe of its 14-term chi functions."""
     kdir = reference / KERNELS_REL
     common = _string_constants(kdir / "common.py", {"_DEVICE_FUNCTIONS_CUDA"})
     fft = _string_constants(kdir / "fft128.py", {"_TWIDDLE_DECL", "_FFT128_KERNELS"})
     return ('extern "C" {\n' + fft["_TWIDDLE_DECL"] + "\n" + common["_DEVICE_FUNCTIONS_CUDA"]
-            + "\n" + fft["_FFT128_KERNELS"] + "\n}")
+            + "\n" + fft["_FFT128_KERNELS"] + "\n" + FULL_PROBE_SOURCE + "\n}")
 
 
 def available() -> bool:
@@ -87,7 +111,7 @@ def build(reference: Path = DEFAULT_REFERENCE, force: bool = False, verbose: boo
         "source_sha256": digest,
         "reference_files": [str(KERNELS_REL / "common.py"), str(KERNELS_REL / "fft128.py")],
         "options": "nvcc -cubin sm_100a -std=c++11 --use_fast_math -maxrregcount=96 -Xptxas -dlcm=ca",
-        "kernels": list(KERNEL_NAMES),
+        "kernels": list(KERNEL_NAMES) + [FULL_PROBE_NAME],
         "twiddle": TWIDDLE_NAME,
     }, indent=1))
     return CUBIN

@@ -15,7 +15,7 @@ import math
 import numpy as np
 import torch
 
-from .build_ref import CUBIN, KERNEL_NAMES, TWIDDLE_NAME, available
+from .build_ref import CUBIN, FULL_PROBE_NAME, KERNEL_NAMES, TWIDDLE_NAME, available
 
 N = 128
 
@@ -95,6 +95,39 @@ class ReferenceObject128:
         self._launch(self.cols, (1, 16, n_bf), (32, 8, 1),
                      [(out.data_ptr(), P), (n_bf, I), (f32(1.0 / (N * N)), F)], stream)
         return out
+
+    def full_chi_probe(self, qx, qy, kx, ky, *, wavelength: float, semiangle_rad: float,
+                       ang_y_rad: float, ang_x_rad: float, magnitudes, angles, pk, g):
+        """The reference's chi_full(q - k) and gamma_mul_pk_onthefly_full
+        (common.py:410-532) at n points (float32 CUDA [n] inputs; pk, g
+        complex64 [n]). Coefficients packed as pack_aberration_coefs does
+        (common.py:646-674): mag / (n+1), cos(m angle), sin(m angle) in float32."""
+        nm = ((1, 0), (1, 2), (2, 1), (2, 3), (3, 0), (3, 2), (3, 4),
+              (4, 1), (4, 3), (4, 5), (5, 0), (5, 2), (5, 4), (5, 6))
+        mags = np.asarray(magnitudes, np.float32)
+        angs = np.asarray(angles, np.float32)
+        n1 = np.array([n + 1 for n, _ in nm], np.float32)
+        m = np.array([m for _, m in nm], np.float32)
+        packed = [torch.as_tensor(a, device=self.device) for a in
+                  (mags * (np.float32(1.0) / n1), np.cos(m * angs, dtype=np.float32),
+                   np.sin(m * angs, dtype=np.float32))]
+        if not hasattr(self, "probe"):
+            (self.probe,) = _check(self.cu.cuModuleGetFunction(self.module, FULL_PROBE_NAME.encode()))
+        n = int(qx.numel())
+        chi = torch.empty(n, dtype=torch.float32, device=self.device)
+        out = torch.empty(n, dtype=torch.complex64, device=self.device)
+        pk = pk.contiguous()
+        g = g.contiguous()
+        P, F, I = ctypes.c_void_p, ctypes.c_float, ctypes.c_int
+        f32 = lambda x: float(np.float32(x))  # noqa: E731
+        args = [(qx.data_ptr(), P), (qy.data_ptr(), P), (kx.data_ptr(), P), (ky.data_ptr(), P),
+                (n, I), (f32(wavelength), F), (f32(semiangle_rad), F), (f32(ang_y_rad), F),
+                (f32(ang_x_rad), F), *[(t.data_ptr(), P) for t in packed],
+                (pk.data_ptr(), P), (g.data_ptr(), P), (chi.data_ptr(), P), (out.data_ptr(), P)]
+        stream = self.cu.CUstream(torch.cuda.current_stream(self.device).cuda_stream)
+        self._launch(self.probe, ((n + 255) // 256, 1, 1), (256, 1, 1), args, stream)
+        torch.cuda.synchronize(self.device)
+        return chi, out
 
     def object(self, *args, **kw) -> torch.Tensor:
         """reconstruct_object for B > 1024 (engine.py:1148-1151): mean over BF pixels."""

@@ -333,6 +333,54 @@ def chi(alpha2, cos2phi, sin2phi, ab: Aberrations, wavelength: float):
     return out
 
 
+# Slot layout of the 14-term chi (aberration.py:63 of the reference):
+# (n, m) of C10, C12, C21, C23, C30, C32, C34, C41, C43, C45, C50, C52, C54, C56.
+FULL_NM = ((1, 0), (1, 2), (2, 1), (2, 3), (3, 0), (3, 2), (3, 4),
+           (4, 1), (4, 3), (4, 5), (5, 0), (5, 2), (5, 4), (5, 6))
+
+
+@dataclass(frozen=True)
+class FullAberrations:
+    """The 14 Krivanek coefficients: magnitudes (length unit of C10) and
+    angles phi_nm in radians, slot order ``FULL_NM`` (engine.py:1244-1262)."""
+
+    magnitudes: tuple
+    angles: tuple
+
+
+def chi_full(dx, dy, ab: FullAberrations, wavelength: float):
+    """chi = (2 pi / lambda) sum_i alpha^(n_i+1) C_i / (n_i+1) cos(m_i (phi - phi_i)).
+
+    Follows ``chi_full`` and ``pack_aberration_coefs`` (kernels/common.py:
+    410-471, 646-674) in FP64, with alpha = lambda |u| and phi = atan2(dy, dx)
+    evaluated directly (the reference reaches cos(m phi) by a Chebyshev
+    recurrence from dx / |u|; at |u| = 0 both give chi = 0).
+    """
+    r = np.sqrt(dx * dx + dy * dy)
+    alpha = r * wavelength
+    phi = np.arctan2(dy, dx)
+    out = np.zeros(np.broadcast(dx, dy).shape)
+    for (n, m), mag, ang in zip(FULL_NM, ab.magnitudes, ab.angles):
+        if mag == 0.0:
+            continue
+        out = out + alpha ** (n + 1) * (mag / (n + 1)) * np.cos(m * (phi - ang))
+    return (2.0 * math.pi / wavelength) * out
+
+
+def full_from_two_term(ab: Aberrations) -> FullAberrations:
+    """The same chi as ``ab`` in the 14-slot layout."""
+    mags = [0.0] * 14
+    angs = [0.0] * 14
+    mags[0], mags[1], angs[1], mags[4] = ab.C10, ab.C12, ab.phi12, ab.C30
+    return FullAberrations(tuple(mags), tuple(angs))
+
+
+def _chi_at(dx, dy, alpha2, cos2, sin2, ab, wavelength: float):
+    if isinstance(ab, FullAberrations):
+        return chi_full(dx, dy, ab, wavelength)
+    return chi(alpha2, cos2, sin2, ab, wavelength)
+
+
 def corrected_spectra(
     g_half: np.ndarray,
     geo: Geometry,
@@ -355,12 +403,13 @@ def corrected_spectra(
     ky = geo.ky[bf][:, None, None]
     qx = geo.q_row[None, :, None]
     qy = geo.q_col[None, None, :]
-    chi_k = chi(geo.alpha_k2[bf], geo.cos2phi_k[bf], geo.sin2phi_k[bf], ab, geo.wavelength)
+    chi_k = _chi_at(geo.kx[bf], geo.ky[bf], geo.alpha_k2[bf], geo.cos2phi_k[bf],
+                    geo.sin2phi_k[bf], ab, geo.wavelength)
     pk = (geo.aperture_k[bf] * np.exp(-1j * chi_k))[:, None, None]
     am2, cm, sm, apm = _aperture_and_angles(qx - kx, qy - ky, geo)
     ap2, cp_, sp, app = _aperture_and_angles(qx + kx, qy + ky, geo)
-    pm = apm * np.exp(-1j * chi(am2, cm, sm, ab, geo.wavelength))
-    pp = app * np.exp(-1j * chi(ap2, cp_, sp, ab, geo.wavelength))
+    pm = apm * np.exp(-1j * _chi_at(qx - kx, qy - ky, am2, cm, sm, ab, geo.wavelength))
+    pp = app * np.exp(-1j * _chi_at(qx + kx, qy + ky, ap2, cp_, sp, ab, geo.wavelength))
     gamma = pm * np.conj(pk) - np.conj(pp) * pk
     mag2 = gamma.real ** 2 + gamma.imag ** 2
     scale = np.where(mag2 > 1e-16, 1.0 / np.sqrt(np.where(mag2 > 1e-16, mag2, 1.0)), 1e8)

@@ -53,6 +53,10 @@ class Calibration(ctypes.Structure):
 
 
 GEOM_ROWS = 8
+FULL_TERMS = 14  # QSSB_FULL_TERMS
+# slot order of qssb_full_aberrations_t (aberration.py:63 of the reference)
+FULL_TERM_NAMES = ("C10", "C12", "C21", "C23", "C30", "C32", "C34", "C41", "C43", "C45", "C50",
+                   "C52", "C54", "C56")
 
 
 class Aberrations(ctypes.Structure):
@@ -138,6 +142,10 @@ SIGNATURES = {
                                  ctypes.c_float, ctypes.c_float, ctypes.c_float, _I32, _P, _P]),
     "qssb_to_bf16": (ctypes.c_int, [_P, _I64, _P, _P]),
     "qssb_loss_batch": (ctypes.c_int, [
+        _P, _P, _P, _P, ctypes.POINTER(Calibration), _P, _I32, _I32, _P, _SZ, _P, _P, _P]),
+    "qssb_loss_full_workspace_bytes": (
+        ctypes.c_int, [ctypes.POINTER(Calibration), _I32, _I32, ctypes.POINTER(_SZ)]),
+    "qssb_loss_batch_full": (ctypes.c_int, [
         _P, _P, _P, _P, ctypes.POINTER(Calibration), _P, _I32, _I32, _P, _SZ, _P, _P, _P]),
 }
 

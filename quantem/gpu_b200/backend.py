@@ -33,6 +33,8 @@ import torch
 
 from . import autotune, ops
 from ._lib import (
+    FULL_TERM_NAMES,
+    FULL_TERMS,
     GEOM_ROWS,
     QSSB_FLAG_CHI_FP64,
     QSSB_FLAG_QUADRATIC,
@@ -439,11 +441,63 @@ class B200SSBBackend:
             self.cache_rotation(rotation_angle_rad)
         return self.reconstruct(C10, C12, phi12)
 
-    def reconstruct_full(self, mags_m, angles_rad):
-        raise NotImplementedError("14-coefficient chi is not supported on the 128 path "
-                                  "(the reference raises the same at 128, engine.py:1276-1280).")
+    # ---------------------------------------------------- 14-term chi
+    def _full_candidates(self, mags, angles) -> torch.Tensor:
+        """float32 CUDA [n, 28] rows (14 magnitudes, 14 angles) from [14] or [n, 14]."""
+        m = np.atleast_2d(np.asarray(mags, dtype=np.float32))
+        a = np.atleast_2d(np.asarray(angles, dtype=np.float32))
+        if m.shape[-1] != FULL_TERMS or a.shape != m.shape:
+            raise ValueError("magnitudes and angles must each have shape (14,) or (n, 14)")
+        rows = np.ascontiguousarray(np.concatenate([m, a], axis=1))
+        return torch.as_tensor(rows, device=self.device)
 
-    reconstruct_full_with_loss = reconstruct_full
+    def variance_loss_batch_full(self, mags, angles) -> torch.Tensor:
+        """Phase-variance losses (float32 CUDA [n]) with the 14-term chi."""
+        self._require_loss_size()
+        losses, _ = ops.loss_batch_full(self.G_qk, self._geom_dev, self._q_row, self._q_col,
+                                        self._calibration(), self._full_candidates(mags, angles),
+                                        flags=self._flags, workspace=self._workspace)
+        return losses
+
+    def reconstruct_full_with_loss(self, mags_m, angles_rad):
+        """Mean per-BF phase and loss with the 14-term chi (engine.py:1350-1458).
+
+        The reference raises NotImplementedError at 128 (engine.py:1373-1377);
+        this path serves 128 and 256.
+        """
+        self._require_loss_size()
+        losses, mp = ops.loss_batch_full(self.G_qk, self._geom_dev, self._q_row, self._q_col,
+                                         self._calibration(),
+                                         self._full_candidates(mags_m, angles_rad),
+                                         flags=self._flags, workspace=self._workspace,
+                                         want_mean_phase=True)
+        return mp[0], float(losses[0])
+
+    def reconstruct_full(self, mags_m, angles_rad):
+        """Mean per-BF phase with the 14-term chi (engine.py:1244-1292)."""
+        return self.reconstruct_full_with_loss(mags_m, angles_rad)[0]
+
+    def _higher_order_arrays(self) -> tuple[np.ndarray, np.ndarray, bool]:
+        """(magnitudes [14], angles [14] rad, any higher order active) from the
+        aberrations dict: C10, C12, phi12 (rad); Cn0 scalars; Cnm_mag with
+        Cnm_angle in degrees (backend.py:730-771)."""
+        a = self.aberrations
+        mags = np.zeros(FULL_TERMS, dtype=np.float32)
+        angs = np.zeros(FULL_TERMS, dtype=np.float32)
+        mags[0] = a.get("C10", 0.0)
+        mags[1] = a.get("C12", 0.0)
+        angs[1] = a.get("phi12", 0.0)
+        active = False
+        for idx, name in enumerate(FULL_TERM_NAMES[2:], start=2):
+            if name.endswith("0"):
+                mag, ang = float(a.get(name, 0.0)), 0.0
+            else:
+                mag = float(a.get(f"{name}_mag", 0.0))
+                ang = math.radians(float(a.get(f"{name}_angle", 0.0)))
+            active = active or mag != 0.0
+            mags[idx] = mag
+            angs[idx] = ang
+        return mags, angs, active
 
     @staticmethod
     def phase_to_numpy(phase) -> np.ndarray:
@@ -461,9 +515,16 @@ class B200SSBBackend:
 
     def result(self, *, compute_loss: bool = True) -> SSBResult:
         C10, C12, phi12 = self._resolve_coefs()
-        obj = self.reconstruct_object(C10, C12, phi12)
+        mags, angs, higher = self._higher_order_arrays()
+        if higher:
+            # 14-term chi: the mean per-BF phase as a unit-amplitude object
+            # and no diagnostic loss (backend.py:795-820)
+            phase = self.reconstruct_full(mags, angs)
+            obj = torch.polar(torch.ones_like(phase), phase)
+        else:
+            obj = self.reconstruct_object(C10, C12, phi12)
         loss = None
-        if compute_loss and self._scan_shape[0] in LOSS_SCAN_SIZES:
+        if compute_loss and not higher and self._scan_shape[0] in LOSS_SCAN_SIZES:
             try:
                 loss = self.variance_loss(C10, C12, phi12)
             except (ValueError, ZeroDivisionError, FloatingPointError):
@@ -494,7 +555,12 @@ class B200SSBBackend:
                 higher_order_magnitudes: np.ndarray | None,
                 higher_order_angles: np.ndarray | None) -> tuple[np.ndarray, float | None]:
         if higher_order_magnitudes is not None:
-            return self.reconstruct_full(higher_order_magnitudes, higher_order_angles)
+            if compute_loss:
+                phase, loss = self.reconstruct_full_with_loss(higher_order_magnitudes,
+                                                              higher_order_angles)
+                return self.phase_to_numpy(phase), float(loss)
+            return self.phase_to_numpy(self.reconstruct_full(higher_order_magnitudes,
+                                                             higher_order_angles)), None
         if compute_loss:
             phase, loss = self.reconstruct_with_loss(aberrations["C10"], aberrations["C12"],
                                                      aberrations["phi12"])

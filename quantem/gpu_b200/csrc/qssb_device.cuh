@@ -587,6 +587,152 @@ __device__ __forceinline__ float2 corrected_quad_e(float qx, float qy, int r, in
     return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
 }
 
+// ------------------------------------------------ 14-term Krivanek chi
+// chi(u) = (2 pi / lambda) sum_i alpha^(n_i+1) C_i / (n_i+1) cos(m_i (phi - phi_i)),
+// alpha = lambda |u|, phi = atan2(dy, dx) (chi_full, common.py:410-471 of the
+// reference; slots C10, C12, C21, C23, C30, C32, C34, C41, C43, C45, C50, C52,
+// C54, C56). Every term has n + 1 - m even, so with z = dx + i dy and
+// r2 = |z|^2,
+//   alpha^(n+1) cos(m (phi - phi_i)) = lambda^(n+1) r2^j Re(e^{-i m phi_i} z^m),
+//   j = (n + 1 - m) / 2,
+// and chi is a polynomial in (dx, dy):
+//   chi = r2 (K10 + r2 (K30 + r2 K50)) + Re(sum_{m=1..6} w_m(r2) z^m),
+//   w_m(r2) = sum_j K_{m,j} e^{-i m phi_{m,j}} r2^j,  K = 2 pi lambda^n C / (n + 1),
+// evaluated by Horner in r2 and in z: no angle, no square root, no division.
+constexpr int kFullTerms = 14;
+
+template <typename T, typename T2>
+struct FullChiT {
+    T c0[3];     // r2 coefficients of the m = 0 terms: K10, K30, K50
+    T2 w[6][3];  // w[m - 1][j] = K e^{-i m phi}; zero where no term exists
+};
+using FullChi = FullChiT<float, float2>;
+using FullChi64 = FullChiT<double, double2>;
+
+// Coefficients from magnitudes (length unit of 1 / q, as C10) and angles.
+__host__ __device__ inline void make_full_chi(const float* mag, const float* ang, double wavelength,
+                                              FullChi& f, FullChi64& d) {
+    const int kn[kFullTerms] = {1, 1, 2, 2, 3, 3, 3, 4, 4, 4, 5, 5, 5, 5};
+    const int km[kFullTerms] = {0, 2, 1, 3, 0, 2, 4, 1, 3, 5, 0, 2, 4, 6};
+    for (int j = 0; j < 3; ++j) {
+        d.c0[j] = 0.0;
+        for (int m = 0; m < 6; ++m) d.w[m][j] = make_double2(0.0, 0.0);
+    }
+    for (int i = 0; i < kFullTerms; ++i) {
+        const int n = kn[i];
+        const int m = km[i];
+        const int j = (n + 1 - m) / 2;
+        double lam_n = 1.0;
+        for (int e = 0; e < n; ++e) lam_n *= wavelength;
+        const double k = 6.283185307179586476925 * lam_n * (double)mag[i] / (double)(n + 1);
+        if (m == 0) {
+            d.c0[j - 1] += k;
+        } else {
+            const double a = (double)m * (double)ang[i];
+            d.w[m - 1][j].x += k * cos(a);
+            d.w[m - 1][j].y -= k * sin(a);
+        }
+    }
+    for (int j = 0; j < 3; ++j) {
+        f.c0[j] = (float)d.c0[j];
+        for (int m = 0; m < 6; ++m) f.w[m][j] = make_float2((float)d.w[m][j].x, (float)d.w[m][j].y);
+    }
+}
+
+template <typename T, typename T2>
+__device__ __forceinline__ T chi_full_poly(T dx, T dy, const FullChiT<T, T2>& f) {
+    const T r2 = dx * dx + dy * dy;
+    T sr = 0, si = 0;  // complex Horner in z over m = 6 .. 1
+    auto step = [&](int m) {
+        const T2* w = f.w[m - 1];
+        const T wr = w[0].x + r2 * (w[1].x + r2 * w[2].x);
+        const T wi = w[0].y + r2 * (w[1].y + r2 * w[2].y);
+        const T tr = sr * dx - si * dy + wr;
+        const T ti = sr * dy + si * dx + wi;
+        sr = tr;
+        si = ti;
+    };
+    if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int m = 6; m >= 1; --m) step(m);
+    } else {
+        // FP64 coefficients stay in shared memory (a rolled loop keeps them
+        // from being hoisted into 72 registers)
+#pragma unroll 1
+        for (int m = 6; m >= 1; --m) step(m);
+    }
+    const T re = sr * dx - si * dy;  // Re(S z)
+    return r2 * (f.c0[0] + r2 * (f.c0[1] + r2 * f.c0[2])) + re;
+}
+
+// C = G conj(Gamma_hat) (as `corrected`) with the 14-term chi at q -+ k.
+// CHI64: chi from FP64 q and k (k = kx + kx_lo), reduced to [-pi, pi] in FP64.
+template <bool CHI64>
+__device__ __forceinline__ float2 corrected_full(float qx, float qy, int r, int c, float kx,
+                                                 float ky, float kx_lo, float ky_lo, float2 pk,
+                                                 float2 g, const Probe& p, const FullChi& f,
+                                                 const FullChi64& fd) {
+    const float dxm = qx - kx, dym = qy - ky;
+    const float dxp = qx + kx, dyp = qy + ky;
+    const float r2m = dxm * dxm + dym * dym;
+    const float r2p = dxp * dxp + dyp * dyp;
+    float am = soft_aperture(dxm, dym, r2m, p);
+    float ap = soft_aperture(dxp, dyp, r2p, p);
+    const bool tie = fabsf(am - ap) < kApertureTie && (in_edge_band(r2m, p) || in_edge_band(r2p, p));
+    if (CHI64 || tie) {
+        const double qx64 = fftfreq_d(r, p.n_r, p.qval_r);
+        const double qy64 = fftfreq_d(c, p.n_c, p.qval_c);
+        const double kx64 = (double)kx + (double)kx_lo;
+        const double ky64 = (double)ky + (double)ky_lo;
+        if (tie) {
+            am = soft_aperture_fp64(qx64 - kx64, qy64 - ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
+            ap = soft_aperture_fp64(qx64 + kx64, qy64 + ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
+        }
+        if constexpr (CHI64) {
+            float s, co;
+            sincosf(reduce_angle(chi_full_poly(qx64 - kx64, qy64 - ky64, fd)), &s, &co);
+            const float2 pm = make_float2(am * co, -am * s);
+            sincosf(reduce_angle(chi_full_poly(qx64 + kx64, qy64 + ky64, fd)), &s, &co);
+            const float2 pp = make_float2(ap * co, -ap * s);
+            const float t1r = fmaf(pm.x, pk.x, pm.y * pk.y);
+            const float t1i = fmaf(pm.y, pk.x, -pm.x * pk.y);
+            const float t2r = fmaf(pp.x, pk.x, pp.y * pk.y);
+            const float t2i = fmaf(pp.x, pk.y, -pp.y * pk.x);
+            float gr = t1r - t2r;
+            float gi = t1i - t2i;
+            const float m2 = fmaf(gr, gr, gi * gi);
+            const float inv = m2 > 1e-16f ? rsqrtf(m2) : 1e8f;
+            gr *= inv;
+            gi *= inv;
+            return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
+        }
+    }
+    float s, co;
+    sincosf(chi_full_poly(dxm, dym, f), &s, &co);
+    const float2 pm = make_float2(am * co, -am * s);
+    sincosf(chi_full_poly(dxp, dyp, f), &s, &co);
+    const float2 pp = make_float2(ap * co, -ap * s);
+    const float t1r = fmaf(pm.x, pk.x, pm.y * pk.y);
+    const float t1i = fmaf(pm.y, pk.x, -pm.x * pk.y);
+    const float t2r = fmaf(pp.x, pk.x, pp.y * pk.y);
+    const float t2i = fmaf(pp.x, pk.y, -pp.y * pk.x);
+    float gr = t1r - t2r;
+    float gi = t1i - t2i;
+    const float m2 = fmaf(gr, gr, gi * gi);
+    const float inv = m2 > 1e-16f ? rsqrtf(m2) : 1e8f;
+    gr *= inv;
+    gi *= inv;
+    return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
+}
+
+// P(k_b) with the 14-term chi from FP64 k (once per BF pixel).
+__device__ __forceinline__ float2 probe_full_at_bf(double kx, double ky, float aperture,
+                                                   const FullChi64& fd) {
+    float s, c;
+    sincosf(reduce_angle(chi_full_poly(kx, ky, fd)), &s, &c);
+    return make_float2(aperture * c, -aperture * s);
+}
+
 // Kahan-compensated complex accumulation: (s.x, s.y) sums, (s.z, s.w) compensations.
 __device__ __forceinline__ void kahan_add(float4& s, float2 v) {
     const float yr = v.x - s.z;

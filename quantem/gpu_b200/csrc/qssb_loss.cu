@@ -658,6 +658,235 @@ static int dispatch_loss(bool sym, bool chi64, bool quad, const float* g_half, c
     return dispatch_loss_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
 }
 
+// ------------------------------------------------------ 14-term chi
+// Odd-m terms (C21, C23, C41, C43, C45) make chi odd in part, which breaks
+// C(-q) = -conj C(q): every scan frequency is evaluated. N <= 128: the whole
+// N x (N+1) plane in shared memory (k_loss_moments without the mirror).
+// N = 256: each warp evaluates, inverse-FFTs and stages full rows in the
+// CTA's global plane, then rebuilds its columns from it (k_loss_moments256
+// without the row(-r) reconstruction). Partial planes are column-major.
+struct FullConsts {
+    Probe p;
+    FullChi f;
+    FullChi64 d;
+};
+
+__device__ __forceinline__ void load_full_consts(FullConsts& sh, const qssb_full_aberrations_t* cands,
+                                                 int cand, const qssb_calibration_t& cal) {
+    sh.p = make_probe_common(cal, 0.0f, 0.0f, 0.0f, 0.0f);
+    make_full_chi(cands[cand].magnitude, cands[cand].angle_rad, cal.wavelength_A, sh.f, sh.d);
+}
+
+template <int N, bool CHI64>
+__global__ void __launch_bounds__(kLossThreads, 1) k_loss_full(
+    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
+    const float* __restrict__ q_row, const float* __restrict__ q_col,
+    const qssb_full_aberrations_t* __restrict__ cands, qssb_calibration_t cal, int bf_per_chunk,
+    int n_chunks, float* __restrict__ part) {
+    constexpr int H = N / 2 + 1;
+    constexpr int P = LossSmem<N>::P;
+    constexpr int CPW = N / kLossWarps;
+    constexpr int RPL = N / 32;
+    extern __shared__ float2 smem[];
+    __shared__ FullConsts sh;
+    float2* plane = smem;
+    float2* tw = smem + N * P;
+    float* sq = reinterpret_cast<float*>(tw + N);  // [col][row] sums of squares
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int chunk = blockIdx.x;
+    const int cand = blockIdx.y;
+    if (tid == 0) load_full_consts(sh, cands, cand, cal);
+    fill_twiddles<N>(tw, tid, kLossThreads);
+    for (int i = tid; i < N * N; i += kLossThreads) sq[i] = 0.0f;
+    __syncthreads();
+    float as[CPW][RPL];
+#pragma unroll
+    for (int i = 0; i < CPW; ++i)
+#pragma unroll
+        for (int t = 0; t < RPL; ++t) as[i][t] = 0.0f;
+    const int b0 = chunk * bf_per_chunk;
+    int nb = n_bf - b0;
+    if (nb > bf_per_chunk) nb = bf_per_chunk;
+    const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
+    for (int i = 0; i < nb; ++i) {
+        const int b = b0 + i;
+        const float kx = __ldg(geom + b);
+        const float ky = __ldg(geom + n_bf + b);
+        const float kx_lo = __ldg(geom + 6 * n_bf + b);
+        const float ky_lo = __ldg(geom + 7 * n_bf + b);
+        const float2 pk = probe_full_at_bf((double)kx + (double)kx_lo, (double)ky + (double)ky_lo,
+                                           __ldg(geom + 5 * n_bf + b), sh.d);
+        const float2* gb = g + (size_t)b * N * H;
+        for (int e = tid; e < N * N; e += kLossThreads) {
+            const int r = e / N;
+            const int c = e - r * N;
+            const float2 gv = c <= N / 2 ? __ldg(gb + r * H + c)
+                                         : cconj(__ldg(gb + ((N - r) & (N - 1)) * H + (N - c)));
+            float2 v = corrected_full<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c, kx, ky, kx_lo,
+                                             ky_lo, pk, gv, sh.p, sh.f, sh.d);
+            if (e == 0) v = dc;
+            plane[r * P + c] = v;
+        }
+        __syncthreads();
+        for (int row = warp; row < N; row += kLossWarps) line_fft<N, +1>(plane + row * P, 1, tw, lane);
+        __syncthreads();
+#pragma unroll
+        for (int ci = 0; ci < CPW; ++ci) {
+            const int col = warp + ci * kLossWarps;
+            line_fft<N, +1>(plane + col, P, tw, lane);
+#pragma unroll
+            for (int t = 0; t < RPL; ++t) {
+                const float2 v = plane[(lane + 32 * t) * P + col];
+                const float ph = atan2f(v.y, v.x);
+                as[ci][t] += ph;
+                float* q2 = sq + col * N + lane + 32 * t;
+                *q2 = fmaf(ph, ph, *q2);
+            }
+        }
+        __syncthreads();
+    }
+    float* ps = part + ((size_t)(cand * n_chunks + chunk) * 2) * N * N;
+    float* pq = ps + (size_t)N * N;
+#pragma unroll
+    for (int ci = 0; ci < CPW; ++ci) {
+        const int col = warp + ci * kLossWarps;
+#pragma unroll
+        for (int t = 0; t < RPL; ++t) ps[col * N + lane + 32 * t] = as[ci][t];
+    }
+    for (int i = tid; i < N * N; i += kLossThreads) pq[i] = sq[i];
+}
+
+template <bool CHI64>
+__global__ void __launch_bounds__(kLossThreads, 1) k_loss_full256(
+    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
+    const float* __restrict__ q_row, const float* __restrict__ q_col,
+    const qssb_full_aberrations_t* __restrict__ cands, qssb_calibration_t cal, int bf_per_chunk,
+    int n_chunks, float* __restrict__ part, float2* __restrict__ stage) {
+    constexpr int N = kL256;
+    constexpr int H = N / 2 + 1;
+    extern __shared__ float4 smem4[];
+    float2* lines = reinterpret_cast<float2*>(smem4);
+    float2* tw = lines + kLossWarps * N;
+    __shared__ FullConsts sh;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int chunk = blockIdx.x;
+    const int cand = blockIdx.y;
+    const size_t cta = (size_t)cand * n_chunks + chunk;
+    float2* S = stage + cta * (size_t)N * N;
+    float* ps = part + cta * 2 * (size_t)N * N;
+    float* pq = ps + (size_t)N * N;
+    float2* line = lines + warp * N;
+    if (tid == 0) load_full_consts(sh, cands, cand, cal);
+    fill_twiddles<N>(tw, tid, kLossThreads);
+    for (int j = 0; j < N / kLossWarps; ++j) {
+        const int x = warp + kLossWarps * j;
+#pragma unroll
+        for (int t = 0; t < N / 32; ++t) {
+            ps[(size_t)x * N + lane + 32 * t] = 0.0f;
+            pq[(size_t)x * N + lane + 32 * t] = 0.0f;
+        }
+    }
+    __syncthreads();
+    const int b0 = chunk * bf_per_chunk;
+    int nb = n_bf - b0;
+    if (nb > bf_per_chunk) nb = bf_per_chunk;
+    const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
+    for (int i = 0; i < nb; ++i) {
+        const int b = b0 + i;
+        const float kx = __ldg(geom + b);
+        const float ky = __ldg(geom + n_bf + b);
+        const float kx_lo = __ldg(geom + 6 * n_bf + b);
+        const float ky_lo = __ldg(geom + 7 * n_bf + b);
+        const float2 pk = probe_full_at_bf((double)kx + (double)kx_lo, (double)ky + (double)ky_lo,
+                                           __ldg(geom + 5 * n_bf + b), sh.d);
+        const float2* gb = g + (size_t)b * N * H;
+        for (int r = warp; r < N; r += kLossWarps) {
+#pragma unroll
+            for (int t = 0; t < N / 32; ++t) {
+                const int c = lane + 32 * t;
+                const float2 gv = c <= N / 2 ? __ldg(gb + r * H + c)
+                                             : cconj(__ldg(gb + ((N - r) & (N - 1)) * H + (N - c)));
+                float2 v = corrected_full<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c, kx, ky,
+                                                 kx_lo, ky_lo, pk, gv, sh.p, sh.f, sh.d);
+                if (r == 0 && c == 0) v = dc;
+                line[c] = v;
+            }
+            __syncwarp();
+            line_fft<N, +1>(line, 1, tw, lane);
+#pragma unroll
+            for (int t = 0; t < N / 32; ++t) S[(size_t)r * N + lane + 32 * t] = line[lane + 32 * t];
+            __syncwarp();
+        }
+        __syncthreads();
+        for (int j = 0; j < N / kLossWarps; ++j) {
+            const int x = warp + kLossWarps * j;
+#pragma unroll
+            for (int t = 0; t < N / 32; ++t) line[lane + 32 * t] = S[(size_t)(lane + 32 * t) * N + x];
+            __syncwarp();
+            line_fft<N, +1>(line, 1, tw, lane);
+#pragma unroll
+            for (int t = 0; t < N / 32; ++t) {
+                const int y = lane + 32 * t;
+                const float2 v = line[y];
+                const float ph = atan2f(v.y, v.x);
+                ps[(size_t)x * N + y] += ph;
+                pq[(size_t)x * N + y] = fmaf(ph, ph, pq[(size_t)x * N + y]);
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+}
+
+static size_t full_stage_bytes(int n, const LossPlan& pl, int n_cand) {
+    return n == kL256 ? sizeof(float2) * (size_t)n * n * pl.n_chunks * n_cand : 0;
+}
+
+template <int N, bool CHI64>
+static int launch_loss_full(const float* g_half, const float* geom, const float* q_row,
+                            const float* q_col, const qssb_calibration_t& cal,
+                            const qssb_full_aberrations_t* cands, int n_cand, int chunks, char* ws,
+                            float* losses, float* mean_phase, cudaStream_t s) {
+    const LossPlan pl = plan_loss(N, cal.n_bf, n_cand, chunks);
+    float* part = reinterpret_cast<float*>(ws);
+    double* var = reinterpret_cast<double*>(ws + pl.part_bytes);
+    const auto* gh = reinterpret_cast<const float2*>(g_half);
+    if constexpr (N == kL256) {
+        float2* stage = reinterpret_cast<float2*>(ws + pl.part_bytes + pl.var_bytes);
+        const size_t smem = sizeof(float2) * (kLossWarps * N + N);
+        CUDA_TRY(cudaFuncSetAttribute(k_loss_full256<CHI64>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_loss_full256<CHI64><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
+            gh, cal.n_bf, geom, q_row, q_col, cands, cal, pl.bf_per_chunk, pl.n_chunks, part, stage);
+    } else {
+        const size_t smem = LossSmem<N>::bytes + sizeof(float) * N * N;
+        CUDA_TRY(cudaFuncSetAttribute(k_loss_full<N, CHI64>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_loss_full<N, CHI64><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
+            gh, cal.n_bf, geom, q_row, q_col, cands, cal, pl.bf_per_chunk, pl.n_chunks, part);
+    }
+    CUDA_TRY(cudaGetLastError());
+    k_loss_reduce<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(part, pl.n_chunks, cal.n_bf,
+                                                                       var, mean_phase, 0);
+    CUDA_TRY(cudaGetLastError());
+    k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N, losses);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+template <int N>
+static int dispatch_loss_full(bool chi64, const float* g_half, const float* geom,
+                              const float* q_row, const float* q_col, const qssb_calibration_t& cal,
+                              const qssb_full_aberrations_t* cands, int n_cand, int chunks, char* ws,
+                              float* losses, float* mean_phase, cudaStream_t s) {
+    return chi64 ? launch_loss_full<N, true>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s)
+                 : launch_loss_full<N, false>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
+}
+
 }  // namespace qssb
 
 using namespace qssb;
@@ -703,5 +932,47 @@ extern "C" int qssb_loss_batch(const float* g_half, const float* bf_geom, const 
         case 128: return dispatch_loss<128>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
         case 256: return dispatch_loss<256>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
         default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64, 128 or 256");
+    }
+}
+
+extern "C" int qssb_loss_full_workspace_bytes(const qssb_calibration_t* cal, int32_t n_cand,
+                                              int32_t flags, size_t* bytes) {
+    int rc = validate_calibration(cal, "qssb_loss_full_workspace_bytes: null calibration");
+    if (rc) return rc;
+    if (!bytes || n_cand <= 0 || n_cand > 65535)
+        return set_error(QSSB_ERR_INVALID, "qssb_loss_full_workspace_bytes: n_cand must be in [1, 65535]");
+    const int n = cal->scan_rows;
+    if (n != 64 && n != 128 && n != 256)
+        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch_full: scan size must be 64, 128 or 256");
+    const LossPlan pl = plan_loss(n, cal->n_bf, n_cand, flag_chunks(flags));
+    *bytes = pl.part_bytes + pl.var_bytes + full_stage_bytes(n, pl, n_cand);
+    return QSSB_OK;
+}
+
+extern "C" int qssb_loss_batch_full(const float* g_half, const float* bf_geom, const float* q_row,
+                                    const float* q_col, const qssb_calibration_t* cal,
+                                    const qssb_full_aberrations_t* candidates, int32_t n_cand,
+                                    int32_t flags, void* workspace, size_t workspace_bytes,
+                                    float* losses, float* mean_phase, void* stream) {
+    int rc = validate_calibration(cal, "qssb_loss_batch_full: null calibration");
+    if (rc) return rc;
+    if (!g_half || !bf_geom || !q_row || !q_col || !candidates || !workspace || !losses)
+        return set_error(QSSB_ERR_INVALID, "qssb_loss_batch_full: null pointer");
+    size_t need = 0;
+    rc = qssb_loss_full_workspace_bytes(cal, n_cand, flags, &need);
+    if (rc) return rc;
+    if (workspace_bytes < need)
+        return set_error(QSSB_ERR_WORKSPACE, "qssb_loss_batch_full: workspace too small");
+    if (((uintptr_t)workspace & 255u) != 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_loss_batch_full: workspace must be 256-byte aligned");
+    const bool chi64 = (flags & QSSB_FLAG_CHI_FP64) != 0;
+    const int chunks = flag_chunks(flags);
+    cudaStream_t s = (cudaStream_t)stream;
+    char* ws = static_cast<char*>(workspace);
+    switch (cal->scan_rows) {
+        case 64: return dispatch_loss_full<64>(chi64, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
+        case 128: return dispatch_loss_full<128>(chi64, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
+        case 256: return dispatch_loss_full<256>(chi64, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
+        default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch_full: scan size must be 64, 128 or 256");
     }
 }

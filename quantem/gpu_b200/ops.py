@@ -26,6 +26,7 @@ LAUNCHES_PER_CALL = {
     "qssb_object": 4,
     "qssb_object_ex": 4,
     "qssb_loss_batch": 3,
+    "qssb_loss_batch_full": 3,
 }
 LAUNCH_COUNT = 0
 _PROFILE: list | None = None
@@ -309,6 +310,41 @@ def loss_workspace_bytes(cal: Calibration, n_cand: int, flags: int = 0) -> int:
     check(_lib.load().qssb_loss_workspace_bytes(ctypes.byref(cal), int(n_cand), int(flags),
                                                 ctypes.byref(n)))
     return int(n.value)
+
+
+def loss_full_workspace_bytes(cal: Calibration, n_cand: int, flags: int = 0) -> int:
+    n = ctypes.c_size_t(0)
+    check(_lib.load().qssb_loss_full_workspace_bytes(ctypes.byref(cal), int(n_cand), int(flags),
+                                                     ctypes.byref(n)))
+    return int(n.value)
+
+
+def loss_batch_full(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
+                    q_col: torch.Tensor, cal: Calibration, candidates: torch.Tensor, *,
+                    flags: int = 0, workspace: Workspace | None = None,
+                    want_mean_phase: bool = False
+                    ) -> tuple[torch.Tensor, torch.Tensor | None]:
+    """Losses with the 14-term chi: ``candidates`` float32 CUDA [n, 28] holding
+    14 magnitudes then 14 angles per row (``qssb_full_aberrations_t``)."""
+    _require_cuda(g_half, "g_half", torch.complex64)
+    _require_cuda(bf_geom, "bf_geom", torch.float32)
+    _require_cuda(candidates, "candidates", torch.float32)
+    if candidates.ndim != 2 or candidates.shape[1] != 2 * _lib.FULL_TERMS:
+        raise ValueError("candidates must have shape (n, 28): 14 magnitudes, then 14 angles")
+    if (tuple(g_half.shape) != (cal.n_bf, int(cal.scan_rows), int(cal.scan_cols) // 2 + 1)
+            or tuple(bf_geom.shape) != (_lib.GEOM_ROWS, cal.n_bf)):
+        raise ValueError("g_half / bf_geom shapes do not match the calibration")
+    n = int(candidates.shape[0])
+    r0, r1 = int(cal.scan_rows), int(cal.scan_cols)
+    ws = workspace or Workspace(g_half.device)
+    buf = ws.get(loss_full_workspace_bytes(cal, n, flags))
+    losses = torch.empty(n, dtype=torch.float32, device=g_half.device)
+    mp = (torch.empty((n, r0, r1), dtype=torch.float32, device=g_half.device)
+          if want_mean_phase else None)
+    _call("qssb_loss_batch_full", g_half.device, _ptr(g_half), _ptr(bf_geom), _ptr(q_row),
+          _ptr(q_col), ctypes.byref(cal), _ptr(candidates), n, int(flags), _ptr(buf), buf.numel(),
+          _ptr(losses), _ptr(mp), _stream(g_half))
+    return losses, mp
 
 
 def loss_batch(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
