@@ -544,6 +544,19 @@ def run_b200(args, world, rank, local) -> None:
     e.record(stream)
     torch.cuda.synchronize(dev)
     loss_batch_ms = s.elapsed_time(e) / 3
+    # 14-term chi (full plane, per-element polynomial chi): 8-candidate batches
+    rng = np.random.default_rng(5)
+    fm = np.tile(np.array([10.0, 5.0, 1500.0, 1000.0, 5e4, 3e4, 4e4, 3e6, 2e6, 2e6, 1e8, 5e7, 5e7,
+                           5e7], np.float32), (8, 1)) * rng.uniform(0.5, 1.0, (8, 14)).astype(np.float32)
+    fa = rng.uniform(-np.pi, np.pi, (8, 14)).astype(np.float32)
+    be.variance_loss_batch_full(fm, fa)
+    torch.cuda.synchronize(dev)
+    s.record(stream)
+    for _ in range(3):
+        be.variance_loss_batch_full(fm, fa)
+    e.record(stream)
+    torch.cuda.synchronize(dev)
+    loss_full_ms = s.elapsed_time(e) / 3
 
     # end to end through the public API: pinned host counts -> SSB -> host phase
     host = counts.cpu().pin_memory()
@@ -605,6 +618,7 @@ def run_b200(args, world, rank, local) -> None:
         "cold_backend_recon_per_s": backend_cold,
         "warm_recon_per_s": 1e3 / warm_ms,
         "loss_evals_per_s_batch64": 64 * 1e3 / loss_batch_ms,
+        "loss_full_chi_evals_per_s_batch8": 8 * 1e3 / loss_full_ms,
         "gpu_launches": launches,
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "api": "SSB.from_array(pinned host u16).reconstruct()"},

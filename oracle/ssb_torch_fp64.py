@@ -94,6 +94,23 @@ def _chi(alpha2, cos2, sin2, ab: so.Aberrations, lam: float):
     return out
 
 
+def _chi_full(dx, dy, ab: so.FullAberrations, lam: float):
+    """``ssb_oracle.chi_full`` in torch float64."""
+    alpha = torch.sqrt(dx * dx + dy * dy) * lam
+    phi = torch.atan2(dy, dx)
+    out = torch.zeros_like(alpha)
+    for (n, m), mag, ang in zip(so.FULL_NM, ab.magnitudes, ab.angles):
+        if mag != 0.0:
+            out = out + alpha ** (n + 1) * (mag / (n + 1)) * torch.cos(m * (phi - ang))
+    return (2.0 * math.pi / lam) * out
+
+
+def _chi_at(dx, dy, alpha2, cos2, sin2, ab, lam: float):
+    if isinstance(ab, so.FullAberrations):
+        return _chi_full(dx, dy, ab, lam)
+    return _chi(alpha2, cos2, sin2, ab, lam)
+
+
 def _corrected_chunks(prep: PreparedGPU, ab: so.Aberrations, chunk: int):
     """C_b(q) = G_b(q) conj(Gamma_hat_b(q)), full plane, DC := dc, per BF chunk
     (``ssb_oracle.corrected_spectra``)."""
@@ -113,12 +130,13 @@ def _corrected_chunks(prep: PreparedGPU, ab: so.Aberrations, chunk: int):
         g[:, :, half:] = torch.conj(gh[:, mirror_rows][:, :, mirror_cols])
         kx = d["kx"][s:e, None, None]
         ky = d["ky"][s:e, None, None]
-        chi_k = _chi(d["alpha_k2"][s:e], d["cos2phi_k"][s:e], d["sin2phi_k"][s:e], ab, geo.wavelength)
+        chi_k = _chi_at(d["kx"][s:e], d["ky"][s:e], d["alpha_k2"][s:e], d["cos2phi_k"][s:e],
+                        d["sin2phi_k"][s:e], ab, geo.wavelength)
         pk = (d["aperture_k"][s:e] * torch.exp(-1j * chi_k))[:, None, None]
         am2, cm, sm, apm = _aperture_and_angles(qx - kx, qy - ky, geo)
         ap2, cp, sp, app = _aperture_and_angles(qx + kx, qy + ky, geo)
-        pm = apm * torch.exp(-1j * _chi(am2, cm, sm, ab, geo.wavelength))
-        pp = app * torch.exp(-1j * _chi(ap2, cp, sp, ab, geo.wavelength))
+        pm = apm * torch.exp(-1j * _chi_at(qx - kx, qy - ky, am2, cm, sm, ab, geo.wavelength))
+        pp = app * torch.exp(-1j * _chi_at(qx + kx, qy + ky, ap2, cp, sp, ab, geo.wavelength))
         gamma = pm * torch.conj(pk) - torch.conj(pp) * pk
         mag2 = gamma.real ** 2 + gamma.imag ** 2
         big = mag2 > 1e-16

@@ -54,8 +54,8 @@ from .optimizer import batch_nelder_mead, batch_sweep, search_box
 from .physics import electron_wavelength_angstrom
 from .protocol import BrightfieldDisk, SSBExportState, SSBPrecision, SSBResult
 
-NATIVE_SCAN_SIZES = (128, 256)
-LOSS_SCAN_SIZES = (128, 256)
+NATIVE_SCAN_SIZES = (128, 256, 512, 1024)
+LOSS_SCAN_SIZES = (128, 256, 512, 1024)
 
 
 def _as_device_counts(data, device: torch.device) -> torch.Tensor:

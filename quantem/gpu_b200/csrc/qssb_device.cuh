@@ -2,7 +2,7 @@
 //
 // * complex helpers and radix-2/4/8 butterflies;
 // * a warp-cooperative Stockham FFT over one line held in shared memory
-//   (any stride), N in {64, 128, 256}, forward (exp(-2 pi i nk/N)) or
+//   (any stride), N in {64, 128, 256, 512, 1024}, forward (exp(-2 pi i nk/N)) or
 //   inverse (exp(+2 pi i nk/N), unnormalised);
 // * the probe transfer function P(u) = A(u) exp(-i chi(u)) and the
 //   normalised double-overlap correction of the reference SSB kernels
@@ -222,11 +222,20 @@ __device__ __forceinline__ void line_fft(float2* x, int stride, const float2* tw
         stockham_stage<128, 4, 4, DIR>(x, stride, tw, lane);
         stockham_stage<128, 4, 16, DIR>(x, stride, tw, lane);
         stockham_stage<128, 2, 64, DIR>(x, stride, tw, lane);
-    } else {
-        static_assert(N == 256, "line FFT sizes 64, 128, 256");
+    } else if constexpr (N == 256) {
         stockham_stage<256, 8, 1, DIR>(x, stride, tw, lane);
         stockham_stage<256, 8, 8, DIR>(x, stride, tw, lane);
         stockham_stage<256, 4, 64, DIR>(x, stride, tw, lane);
+    } else if constexpr (N == 512) {
+        stockham_stage<512, 8, 1, DIR>(x, stride, tw, lane);
+        stockham_stage<512, 8, 8, DIR>(x, stride, tw, lane);
+        stockham_stage<512, 8, 64, DIR>(x, stride, tw, lane);
+    } else {
+        static_assert(N == 1024, "line FFT sizes 64, 128, 256, 512, 1024");
+        stockham_stage<1024, 8, 1, DIR>(x, stride, tw, lane);
+        stockham_stage<1024, 8, 8, DIR>(x, stride, tw, lane);
+        stockham_stage<1024, 4, 64, DIR>(x, stride, tw, lane);
+        stockham_stage<1024, 4, 256, DIR>(x, stride, tw, lane);
     }
 }
 

@@ -360,32 +360,43 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
 //     delta_r = conj C(r, 128) + C(-r, 128)), inverse-FFTs them and adds
 //     phi and phi^2 to the CTA's own partial planes, stored column-major
 //     (x * N + y): every element belongs to one lane, so no atomics.
+// The same scheme serves 512^2 and 1024^2 (N/2 + 1 evaluated rows).
 constexpr int kL256 = 256;
-constexpr int kL256Rows = kL256 / 2 + 1;  // 129 evaluated rows
 
-struct Loss256Smem {
-    static constexpr size_t lines = sizeof(float2) * kLossWarps * kL256;
-    static constexpr size_t misc = sizeof(float2) * (kL256 + 3 * 128);  // tw, cpos, cneg, delta
+template <int N>
+struct LossStagedSmem {
+    static constexpr int rows = N / 2 + 1;
+    static constexpr size_t lines = sizeof(float2) * kLossWarps * N;
+    static constexpr size_t misc = sizeof(float2) * (N + 3 * (N / 2));  // tw, cpos, cneg, delta
     static constexpr size_t bytes = lines + misc;
-    static constexpr size_t stage_per_cta = sizeof(float2) * kL256Rows * kL256;
+    static constexpr size_t stage_per_cta = sizeof(float2) * rows * N;
 };
 
-template <bool CHI64, bool QUAD>
-__global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments256(
+static size_t staged_stage_per_cta(int n) {
+    switch (n) {
+        case 256: return LossStagedSmem<256>::stage_per_cta;
+        case 512: return LossStagedSmem<512>::stage_per_cta;
+        case 1024: return LossStagedSmem<1024>::stage_per_cta;
+        default: return 0;
+    }
+}
+
+template <int N, bool CHI64, bool QUAD>
+__global__ void __launch_bounds__(kLossThreads, 1) k_loss_staged(
     const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
     const float* __restrict__ q_row, const float* __restrict__ q_col,
     const qssb_aberrations_t* __restrict__ cands, qssb_calibration_t cal,
     const float2* __restrict__ eq_table, int bf_per_chunk, int n_chunks, float* __restrict__ part,
     float2* __restrict__ stage) {
-    constexpr int N = kL256;
     constexpr int H = N / 2 + 1;
+    constexpr int kRows = LossStagedSmem<N>::rows;
     constexpr bool kSep = QUAD && !CHI64;
     extern __shared__ float4 smem4[];
     float2* lines = reinterpret_cast<float2*>(smem4);
     float2* tw = lines + kLossWarps * N;
     float2* cpos = tw + N;
-    float2* cneg = cpos + 128;
-    float2* delta = cneg + 128;
+    float2* cneg = cpos + N / 2;
+    float2* delta = cneg + N / 2;
     __shared__ Probe sp;
     __shared__ float2 s_phr[kSep ? N : 1];
     __shared__ float2 s_phc[kSep ? N : 1];
@@ -395,7 +406,7 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments256(
     const int chunk = blockIdx.x;
     const int cand = blockIdx.y;
     const size_t cta = (size_t)cand * n_chunks + chunk;
-    float2* S = stage + cta * (size_t)kL256Rows * N;
+    float2* S = stage + cta * (size_t)kRows * N;
     float* ps = part + cta * 2 * (size_t)N * N;
     float* pq = ps + (size_t)N * N;
     float2* line = lines + warp * N;
@@ -420,12 +431,14 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments256(
         const float kx = __ldg(geom + b);
         const float ky = __ldg(geom + n_bf + b);
         float sn, cs;
-        if (tid < N) {
-            sincosf(2.0f * __ldg(q_row + tid) * fmaf(p.mxx, kx, p.mxy * ky), &sn, &cs);
-            s_phr[tid] = make_float2(cs, sn);
-        } else {
-            sincosf(2.0f * __ldg(q_col + tid - N) * fmaf(p.mxy, kx, p.myy * ky), &sn, &cs);
-            s_phc[tid - N] = make_float2(cs, sn);
+        for (int i = tid; i < 2 * N; i += kLossThreads) {
+            if (i < N) {
+                sincosf(2.0f * __ldg(q_row + i) * fmaf(p.mxx, kx, p.mxy * ky), &sn, &cs);
+                s_phr[i] = make_float2(cs, sn);
+            } else {
+                sincosf(2.0f * __ldg(q_col + i - N) * fmaf(p.mxy, kx, p.myy * ky), &sn, &cs);
+                s_phc[i - N] = make_float2(cs, sn);
+            }
         }
     };
     const int b0 = chunk * bf_per_chunk;
@@ -459,10 +472,11 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments256(
         if constexpr (!QUAD)
             pk = probe_at_bf<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
                                     __ldg(geom + 4 * n_bf + b), __ldg(geom + 5 * n_bf + b), p);
-        // C(-r', N/2) for r' = 1..127 (row N - r')
-        if (tid >= 1 && tid < N / 2) cneg[tid] = eval(b, kq, pk, N - tid, N / 2);
-        // rows 0..128: evaluate, keep C(r, N/2), inverse FFT, stage
-        for (int r = warp; r < kL256Rows; r += kLossWarps) {
+        // C(-r', N/2) for r' = 1..N/2-1 (row N - r')
+        for (int j = tid; j < N / 2; j += kLossThreads)
+            if (j >= 1) cneg[j] = eval(b, kq, pk, N - j, N / 2);
+        // rows 0..N/2: evaluate, keep C(r, N/2), inverse FFT, stage
+        for (int r = warp; r < kRows; r += kLossWarps) {
 #pragma unroll
             for (int t = 0; t < N / 32; ++t) {
                 const int c = lane + 32 * t;
@@ -477,7 +491,8 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments256(
             __syncwarp();
         }
         __syncthreads();
-        if (tid >= 1 && tid < N / 2) delta[tid] = cadd(cconj(cpos[tid]), cneg[tid]);
+        for (int j = tid; j < N / 2; j += kLossThreads)
+            if (j >= 1) delta[j] = cadd(cconj(cpos[j]), cneg[j]);
         __syncthreads();
         // columns
         for (int j = 0; j < N / kLossWarps; ++j) {
@@ -487,7 +502,7 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments256(
             for (int t = 0; t < N / 32; ++t) {
                 const int r = lane + 32 * t;
                 float2 v;
-                if (r < kL256Rows) {
+                if (r < kRows) {
                     v = S[(size_t)r * N + x];
                 } else {
                     const float2 m = S[(size_t)(N - r) * N + x];
@@ -576,7 +591,7 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0) {
     pl.part_bytes = (pl.part_bytes + 255) & ~(size_t)255;
     pl.var_bytes = sizeof(double) * (size_t)n * n * n_cand;
     pl.eq_bytes = sizeof(float2) * (size_t)n * n * n_cand;
-    pl.stage_bytes = n == kL256 ? Loss256Smem::stage_per_cta * (size_t)pl.n_chunks * n_cand : 0;
+    pl.stage_bytes = staged_stage_per_cta(n) * (size_t)pl.n_chunks * n_cand;
     return pl;
 }
 
@@ -593,13 +608,13 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
         k_eq_table<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(cands, cal, eq);
         CUDA_TRY(cudaGetLastError());
     }
-    if constexpr (N == kL256) {
-        static_assert(SYM, "the 256^2 loss evaluates the half plane");
+    if constexpr (N >= kL256) {
+        static_assert(SYM, "the staged loss evaluates the half plane");
         float2* stage = reinterpret_cast<float2*>(ws + pl.part_bytes + pl.var_bytes + pl.eq_bytes);
-        const size_t smem = Loss256Smem::bytes;
-        CUDA_TRY(cudaFuncSetAttribute(k_loss_moments256<CHI64, QUAD>,
+        const size_t smem = LossStagedSmem<N>::bytes;
+        CUDA_TRY(cudaFuncSetAttribute(k_loss_staged<N, CHI64, QUAD>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_loss_moments256<CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
+        k_loss_staged<N, CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
             reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal, eq,
             pl.bf_per_chunk, pl.n_chunks, part, stage);
     } else if constexpr (N == 128) {
@@ -631,10 +646,10 @@ static int dispatch_loss_q(bool sym, bool chi64, const float* g_half, const floa
                            const float* q_row, const float* q_col, const qssb_calibration_t& cal,
                            const qssb_aberrations_t* cands, int n_cand, int chunks, char* ws,
                            float* losses, float* mean_phase, cudaStream_t s) {
-    if constexpr (N == kL256) {
+    if constexpr (N >= kL256) {
         if (!sym)
             return set_error(QSSB_ERR_UNSUPPORTED,
-                             "qssb_loss_batch: QSSB_FLAG_FULL_PLANE is not offered at 256^2");
+                             "qssb_loss_batch: QSSB_FLAG_FULL_PLANE is offered up to 128^2");
         return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s)
                      : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
     } else {
@@ -662,8 +677,8 @@ static int dispatch_loss(bool sym, bool chi64, bool quad, const float* g_half, c
 // Odd-m terms (C21, C23, C41, C43, C45) make chi odd in part, which breaks
 // C(-q) = -conj C(q): every scan frequency is evaluated. N <= 128: the whole
 // N x (N+1) plane in shared memory (k_loss_moments without the mirror).
-// N = 256: each warp evaluates, inverse-FFTs and stages full rows in the
-// CTA's global plane, then rebuilds its columns from it (k_loss_moments256
+// N >= 256: each warp evaluates, inverse-FFTs and stages full rows in the
+// CTA's global plane, then rebuilds its columns from it (k_loss_staged
 // without the row(-r) reconstruction). Partial planes are column-major.
 struct FullConsts {
     Probe p;
@@ -758,13 +773,12 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_full(
     for (int i = tid; i < N * N; i += kLossThreads) pq[i] = sq[i];
 }
 
-template <bool CHI64>
-__global__ void __launch_bounds__(kLossThreads, 1) k_loss_full256(
+template <int N, bool CHI64>
+__global__ void __launch_bounds__(kLossThreads, 1) k_loss_full_staged(
     const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
     const float* __restrict__ q_row, const float* __restrict__ q_col,
     const qssb_full_aberrations_t* __restrict__ cands, qssb_calibration_t cal, int bf_per_chunk,
     int n_chunks, float* __restrict__ part, float2* __restrict__ stage) {
-    constexpr int N = kL256;
     constexpr int H = N / 2 + 1;
     extern __shared__ float4 smem4[];
     float2* lines = reinterpret_cast<float2*>(smem4);
@@ -843,7 +857,7 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_full256(
 }
 
 static size_t full_stage_bytes(int n, const LossPlan& pl, int n_cand) {
-    return n == kL256 ? sizeof(float2) * (size_t)n * n * pl.n_chunks * n_cand : 0;
+    return n >= kL256 ? sizeof(float2) * (size_t)n * n * pl.n_chunks * n_cand : 0;
 }
 
 template <int N, bool CHI64>
@@ -855,12 +869,12 @@ static int launch_loss_full(const float* g_half, const float* geom, const float*
     float* part = reinterpret_cast<float*>(ws);
     double* var = reinterpret_cast<double*>(ws + pl.part_bytes);
     const auto* gh = reinterpret_cast<const float2*>(g_half);
-    if constexpr (N == kL256) {
+    if constexpr (N >= kL256) {
         float2* stage = reinterpret_cast<float2*>(ws + pl.part_bytes + pl.var_bytes);
         const size_t smem = sizeof(float2) * (kLossWarps * N + N);
-        CUDA_TRY(cudaFuncSetAttribute(k_loss_full256<CHI64>,
+        CUDA_TRY(cudaFuncSetAttribute(k_loss_full_staged<N, CHI64>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_loss_full256<CHI64><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
+        k_loss_full_staged<N, CHI64><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
             gh, cal.n_bf, geom, q_row, q_col, cands, cal, pl.bf_per_chunk, pl.n_chunks, part, stage);
     } else {
         const size_t smem = LossSmem<N>::bytes + sizeof(float) * N * N;
@@ -898,8 +912,9 @@ extern "C" int qssb_loss_workspace_bytes(const qssb_calibration_t* cal, int32_t 
     if (!bytes || n_cand <= 0 || n_cand > 65535)
         return set_error(QSSB_ERR_INVALID, "qssb_loss_workspace_bytes: n_cand must be in [1, 65535]");
     const int n = cal->scan_rows;
-    if (n != 64 && n != 128 && n != 256)
-        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64, 128 or 256");
+    if (n != 64 && n != 128 && n != 256 && n != 512 && n != 1024)
+        return set_error(QSSB_ERR_UNSUPPORTED,
+                         "qssb_loss_batch: scan size must be 64, 128, 256, 512 or 1024");
     const LossPlan pl = plan_loss(n, cal->n_bf, n_cand, flag_chunks(flags));
     *bytes = pl.part_bytes + pl.var_bytes + pl.eq_bytes + pl.stage_bytes;
     return QSSB_OK;
@@ -931,7 +946,10 @@ extern "C" int qssb_loss_batch(const float* g_half, const float* bf_geom, const 
         case 64: return dispatch_loss<64>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
         case 128: return dispatch_loss<128>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
         case 256: return dispatch_loss<256>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
-        default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: scan size must be 64, 128 or 256");
+        case 512: return dispatch_loss<512>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
+        case 1024: return dispatch_loss<1024>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
+        default: return set_error(QSSB_ERR_UNSUPPORTED,
+                                  "qssb_loss_batch: scan size must be 64, 128, 256, 512 or 1024");
     }
 }
 
@@ -942,8 +960,9 @@ extern "C" int qssb_loss_full_workspace_bytes(const qssb_calibration_t* cal, int
     if (!bytes || n_cand <= 0 || n_cand > 65535)
         return set_error(QSSB_ERR_INVALID, "qssb_loss_full_workspace_bytes: n_cand must be in [1, 65535]");
     const int n = cal->scan_rows;
-    if (n != 64 && n != 128 && n != 256)
-        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch_full: scan size must be 64, 128 or 256");
+    if (n != 64 && n != 128 && n != 256 && n != 512 && n != 1024)
+        return set_error(QSSB_ERR_UNSUPPORTED,
+                         "qssb_loss_batch_full: scan size must be 64, 128, 256, 512 or 1024");
     const LossPlan pl = plan_loss(n, cal->n_bf, n_cand, flag_chunks(flags));
     *bytes = pl.part_bytes + pl.var_bytes + full_stage_bytes(n, pl, n_cand);
     return QSSB_OK;
@@ -973,6 +992,9 @@ extern "C" int qssb_loss_batch_full(const float* g_half, const float* bf_geom, c
         case 64: return dispatch_loss_full<64>(chi64, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
         case 128: return dispatch_loss_full<128>(chi64, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
         case 256: return dispatch_loss_full<256>(chi64, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
-        default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch_full: scan size must be 64, 128 or 256");
+        case 512: return dispatch_loss_full<512>(chi64, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
+        case 1024: return dispatch_loss_full<1024>(chi64, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
+        default: return set_error(QSSB_ERR_UNSUPPORTED,
+                                  "qssb_loss_batch_full: scan size must be 64, 128, 256, 512 or 1024");
     }
 }

@@ -302,16 +302,22 @@ __global__ void __launch_bounds__(32 * kFoldSlices) k_trotter_plane(
     plane[idx] = out;
 }
 
+// Lines (warps) per block of the plane IFFTs: 8, or 4 at 1024 (static
+// shared memory stays under 48 KB).
+template <int N>
+__host__ __device__ constexpr int ifft_lines() { return N >= 1024 ? 4 : 8; }
+
 // In-place inverse FFT of every row of a N x N plane (one warp per row).
 template <int N>
-__global__ void __launch_bounds__(256) k_ifft_rows(float2* __restrict__ plane) {
+__global__ void __launch_bounds__(32 * ifft_lines<N>()) k_ifft_rows(float2* __restrict__ plane) {
+    constexpr int W = ifft_lines<N>();
     __shared__ float2 tw[N];
-    __shared__ float2 line[8][N];
+    __shared__ float2 line[W][N];
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
-    fill_twiddles<N>(tw, tid, 256);
-    const int row = blockIdx.x * 8 + warp;
+    fill_twiddles<N>(tw, tid, 32 * W);
+    const int row = blockIdx.x * W + warp;
     __syncthreads();
     if (row >= N) return;
     float2* src = plane + (size_t)row * N;
@@ -323,16 +329,16 @@ __global__ void __launch_bounds__(256) k_ifft_rows(float2* __restrict__ plane) {
 
 // Inverse FFT of every column, 1/N^2, object and atan2 phase.
 template <int N>
-__global__ void __launch_bounds__(256) k_ifft_cols_phase(const float2* __restrict__ plane,
-                                                         float2* __restrict__ object,
-                                                         float* __restrict__ phase) {
+__global__ void __launch_bounds__(32 * ifft_lines<N>()) k_ifft_cols_phase(
+    const float2* __restrict__ plane, float2* __restrict__ object, float* __restrict__ phase) {
+    constexpr int W = ifft_lines<N>();
     __shared__ float2 tw[N];
-    __shared__ float2 line[8][N];
+    __shared__ float2 line[W][N];
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
-    fill_twiddles<N>(tw, tid, 256);
-    const int col = blockIdx.x * 8 + warp;
+    fill_twiddles<N>(tw, tid, 32 * W);
+    const int col = blockIdx.x * W + warp;
     __syncthreads();
     if (col >= N) return;
     for (int i = lane; i < N; i += 32) line[warp][i] = plane[(size_t)i * N + col];
@@ -357,7 +363,7 @@ struct ObjectPlan {
 };
 
 // Deterministic chunking (independent of the GPU's SM count): about 128 BF
-// chunks at N <= 128 and 32 at N = 256 (N^2/4-thread grids per chunk fill
+// chunks at N <= 128 and 32 at N >= 256 (N^2/4-thread grids per chunk fill
 // the GPU), 4..256 BF pixels each.
 static ObjectPlan plan_object(int n, int n_bf, bool sym, int chunks_req = 0) {
     ObjectPlan pl;
@@ -416,9 +422,10 @@ static int launch_object(const float* g_half, const float* geom, const float* q_
         partial, pl.n_chunks, cal.n_bf, make_float2((float)cal.dc_re, (float)cal.dc_im), dc_dev,
         plane);
     CUDA_TRY(cudaGetLastError());
-    k_ifft_rows<N><<<N / 8, 256, 0, s>>>(plane);
+    constexpr int W = ifft_lines<N>();
+    k_ifft_rows<N><<<N / W, 32 * W, 0, s>>>(plane);
     CUDA_TRY(cudaGetLastError());
-    k_ifft_cols_phase<N><<<N / 8, 256, 0, s>>>(plane, reinterpret_cast<float2*>(object), phase);
+    k_ifft_cols_phase<N><<<N / W, 32 * W, 0, s>>>(plane, reinterpret_cast<float2*>(object), phase);
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -456,8 +463,9 @@ extern "C" int qssb_object_workspace_bytes(const qssb_calibration_t* cal, int32_
     if (rc) return rc;
     if (!bytes) return set_error(QSSB_ERR_INVALID, "qssb_object_workspace_bytes: null output");
     const int n = cal->scan_rows;
-    if (n != 64 && n != 128 && n != 256)
-        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_object: scan size must be 64, 128 or 256");
+    if (n != 64 && n != 128 && n != 256 && n != 512 && n != 1024)
+        return set_error(QSSB_ERR_UNSUPPORTED,
+                         "qssb_object: scan size must be 64, 128, 256, 512 or 1024");
     const ObjectPlan pl = plan_object(n, cal->n_bf, !(flags & QSSB_FLAG_FULL_PLANE), flag_chunks(flags));
     *bytes = pl.partial_bytes + pl.plane_bytes;
     return QSSB_OK;
@@ -493,7 +501,10 @@ extern "C" int qssb_object_ex(const float* g_half, const float* bf_geom, const f
         case 64: return dispatch_object<64>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
         case 128: return dispatch_object<128>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
         case 256: return dispatch_object<256>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
-        default: return set_error(QSSB_ERR_UNSUPPORTED, "qssb_object: scan size must be 64, 128 or 256");
+        case 512: return dispatch_object<512>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
+        case 1024: return dispatch_object<1024>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
+        default: return set_error(QSSB_ERR_UNSUPPORTED,
+                                  "qssb_object: scan size must be 64, 128, 256, 512 or 1024");
     }
 }
 

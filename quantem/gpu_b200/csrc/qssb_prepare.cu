@@ -602,75 +602,100 @@ extern "C" int qssb_gather_bf_columns_2d(const uint16_t* counts, int64_t n_frame
     return QSSB_OK;
 }
 
-// ------------------------------------------------- 256 x 256 scan FFT
-// The 256^2 half plane (264 KB per BF image) does not fit one CTA's shared
-// memory, so the transform is two passes through G itself:
-//   k_scan_rows256: rows 2j, 2j+1 of a BF image as one complex line (one warp
+// ------------------------------------------ 256^2 .. 1024^2 scan FFT
+// The half plane (264 KB per BF image at 256^2) does not fit one CTA's
+// shared memory, so the transform is two passes through G itself:
+//   k_scan_rows<N>: rows 2j, 2j+1 of a BF image as one complex line (one warp
 //     per pair), forward FFT, split into the two real rows' spectra
 //     X_2j(c) = (Z(c) + conj Z(-c)) / 2, X_2j+1(c) = (Z(c) - conj Z(-c)) / 2i,
-//     c = 0..128, written to G[b][row][c];
-//   k_scan_cols256: 16 columns of G[b] staged in shared memory (pitch 257:
-//     the 16 columns of one row land on distinct banks), forward FFT of each
+//     c = 0..N/2, written to G[b][row][c];
+//   k_scan_cols<N>: T columns of G[b] staged in shared memory (pitch N+1:
+//     the T columns of one row land on distinct banks), forward FFT of each
 //     column along the rows, written back in place.
-constexpr int kS256 = 256;
-constexpr int kS256H = kS256 / 2 + 1;
-constexpr int kS256ColTile = 16;
+template <int N>
+struct ScanLines {
+    static constexpr int H = N / 2 + 1;
+    static constexpr int kWarps = N >= 1024 ? 4 : 8;       // row pairs per block
+    static constexpr int kTile = N >= 1024 ? 8 : 16;       // columns per block
+    static constexpr size_t cols_smem = sizeof(float2) * ((size_t)kTile * (N + 1) + N);
+};
 
-__global__ void __launch_bounds__(256) k_scan_rows256(const uint16_t* __restrict__ columns,
-                                                      int n_bf, float2* __restrict__ g_half) {
-    __shared__ float2 tw[kS256];
-    __shared__ float2 line[8][kS256];
+template <int N>
+__global__ void __launch_bounds__(32 * ScanLines<N>::kWarps) k_scan_rows(
+    const uint16_t* __restrict__ columns, int n_bf, float2* __restrict__ g_half) {
+    constexpr int W = ScanLines<N>::kWarps;
+    constexpr int H = ScanLines<N>::H;
+    __shared__ float2 tw[N];
+    __shared__ float2 line[W][N];
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
-    fill_twiddles<kS256>(tw, tid, 256);
+    fill_twiddles<N>(tw, tid, 32 * W);
     __syncthreads();
     const int b = blockIdx.x;
-    const int pair = blockIdx.y * 8 + warp;  // 0 .. 127
-    if (b >= n_bf || pair >= kS256 / 2) return;
-    const uint16_t* img = columns + (size_t)b * kS256 * kS256;
-    const uint16_t* r0 = img + (size_t)(2 * pair) * kS256;
-    const uint16_t* r1 = r0 + kS256;
+    const int pair = blockIdx.y * W + warp;  // 0 .. N/2 - 1
+    if (b >= n_bf || pair >= N / 2) return;
+    const uint16_t* img = columns + (size_t)b * N * N;
+    const uint16_t* r0 = img + (size_t)(2 * pair) * N;
+    const uint16_t* r1 = r0 + N;
     float2* x = line[warp];
-    for (int i = lane; i < kS256; i += 32) x[i] = make_float2((float)__ldg(r0 + i), (float)__ldg(r1 + i));
+    for (int i = lane; i < N; i += 32) x[i] = make_float2((float)__ldg(r0 + i), (float)__ldg(r1 + i));
     __syncwarp();
-    line_fft<kS256, -1>(x, 1, tw, lane);
-    float2* g0 = g_half + ((size_t)b * kS256 + 2 * pair) * kS256H;
-    float2* g1 = g0 + kS256H;
-    for (int c = lane; c < kS256H; c += 32) {
+    line_fft<N, -1>(x, 1, tw, lane);
+    float2* g0 = g_half + ((size_t)b * N + 2 * pair) * H;
+    float2* g1 = g0 + H;
+    for (int c = lane; c < H; c += 32) {
         const float2 z = x[c];
-        const float2 m = x[(kS256 - c) & (kS256 - 1)];
+        const float2 m = x[(N - c) & (N - 1)];
         g0[c] = make_float2(0.5f * (z.x + m.x), 0.5f * (z.y - m.y));
         g1[c] = make_float2(0.5f * (z.y + m.y), -0.5f * (z.x - m.x));
     }
 }
 
-__global__ void __launch_bounds__(256) k_scan_cols256(int n_bf, float2* __restrict__ g_half) {
-    constexpr int P = kS256 + 1;
-    __shared__ float2 tw[kS256];
-    __shared__ float2 tile[kS256ColTile * P];
+template <int N>
+__global__ void __launch_bounds__(256) k_scan_cols(int n_bf, float2* __restrict__ g_half) {
+    constexpr int P = N + 1;
+    constexpr int T = ScanLines<N>::kTile;
+    constexpr int H = ScanLines<N>::H;
+    extern __shared__ float2 scan_cols_smem[];
+    float2* tile = scan_cols_smem;
+    float2* tw = tile + T * P;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
-    fill_twiddles<kS256>(tw, tid, 256);
+    fill_twiddles<N>(tw, tid, 256);
     const int b = blockIdx.x;
-    const int c0 = blockIdx.y * kS256ColTile;
-    const int nc = min(kS256ColTile, kS256H - c0);
+    const int c0 = blockIdx.y * T;
+    const int nc = min(T, H - c0);
     if (b >= n_bf) return;  // uniform per block: before any barrier
-    float2* g = g_half + (size_t)b * kS256 * kS256H;
-    for (int e = tid; e < kS256 * kS256ColTile; e += 256) {
-        const int r = e / kS256ColTile;
-        const int c = e - r * kS256ColTile;
-        if (c < nc) tile[c * P + r] = g[(size_t)r * kS256H + c0 + c];
+    float2* g = g_half + (size_t)b * N * H;
+    for (int e = tid; e < N * T; e += 256) {
+        const int r = e / T;
+        const int c = e - r * T;
+        if (c < nc) tile[c * P + r] = g[(size_t)r * H + c0 + c];
     }
     __syncthreads();
-    for (int c = warp; c < nc; c += 8) line_fft<kS256, -1>(tile + c * P, 1, tw, lane);
+    for (int c = warp; c < nc; c += 8) line_fft<N, -1>(tile + c * P, 1, tw, lane);
     __syncthreads();
-    for (int e = tid; e < kS256 * kS256ColTile; e += 256) {
-        const int r = e / kS256ColTile;
-        const int c = e - r * kS256ColTile;
-        if (c < nc) g[(size_t)r * kS256H + c0 + c] = tile[c * P + r];
+    for (int e = tid; e < N * T; e += 256) {
+        const int r = e / T;
+        const int c = e - r * T;
+        if (c < nc) g[(size_t)r * H + c0 + c] = tile[c * P + r];
     }
+}
+
+template <int N>
+static int launch_scan_lines(const uint16_t* columns, int n_bf, float* g_half, cudaStream_t s) {
+    using L = ScanLines<N>;
+    auto* g = reinterpret_cast<float2*>(g_half);
+    k_scan_rows<N><<<dim3(n_bf, (N / 2 + L::kWarps - 1) / L::kWarps), 32 * L::kWarps, 0, s>>>(
+        columns, n_bf, g);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaFuncSetAttribute(k_scan_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)L::cols_smem));
+    k_scan_cols<N><<<dim3(n_bf, (L::H + L::kTile - 1) / L::kTile), 256, L::cols_smem, s>>>(n_bf, g);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
 }
 
 template <int N>
@@ -705,17 +730,11 @@ extern "C" int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t
             CUDA_TRY(cudaGetLastError());
             return QSSB_OK;
         }
-        case 256: {
-            k_scan_rows256<<<dim3(n_bf, kS256 / 2 / 8), 256, 0, s>>>(
-                columns, n_bf, reinterpret_cast<float2*>(g_half));
-            CUDA_TRY(cudaGetLastError());
-            k_scan_cols256<<<dim3(n_bf, (kS256H + kS256ColTile - 1) / kS256ColTile), 256, 0, s>>>(
-                n_bf, reinterpret_cast<float2*>(g_half));
-            CUDA_TRY(cudaGetLastError());
-            return QSSB_OK;
-        }
+        case 256: return launch_scan_lines<256>(columns, n_bf, g_half, s);
+        case 512: return launch_scan_lines<512>(columns, n_bf, g_half, s);
+        case 1024: return launch_scan_lines<1024>(columns, n_bf, g_half, s);
         default:
             return set_error(QSSB_ERR_UNSUPPORTED,
-                             "qssb_scan_fft_half: scan size must be 64, 128 or 256");
+                             "qssb_scan_fft_half: scan size must be 64, 128, 256, 512 or 1024");
     }
 }

@@ -41,8 +41,8 @@ class ColdReconstructor:
         if counts.ndim != 4 or counts.dtype != torch.uint16 or not counts.is_cuda:
             raise ValueError("counts must be a CUDA uint16 tensor [R0, R1, K0, K1]")
         r0, r1, k0, k1 = (int(x) for x in counts.shape)
-        if r0 != r1 or r0 not in (128, 256):
-            raise NotImplementedError("ColdReconstructor takes native 128^2 or 256^2 scans")
+        if r0 != r1 or r0 not in (128, 256, 512, 1024):
+            raise NotImplementedError("ColdReconstructor takes native 128^2 .. 1024^2 scans")
         self.device = counts.device
         self.counts = counts  # the input buffer: load() copies new data into it
         self.scan_shape = (r0, r1)

@@ -27,8 +27,12 @@ def test_torch_fp64_path_matches_numpy_oracle(case):
     pg = tf.prepare(torch.as_tensor(data), **kw)
     np.testing.assert_array_equal(pg.bf.rows, prep.bf.rows)
     assert abs(pg.dc - prep.dc) <= 1e-13 * abs(prep.dc)
+    full = so.FullAberrations((-120.0, 55.0, 1500.0, 1000.0, 5.0e4, 3.0e4, 4.0e4, 3.0e6, 2.0e6,
+                               2.0e6, 1.0e8, 5.0e7, 5.0e7, 5.0e7),
+                              (0.0, 0.3, 0.5, -0.7, 0.0, 1.1, -0.35, 0.17, 1.4, -0.96, 0.0, 0.09,
+                               0.79, -1.2))
     for ab in (so.Aberrations(0.0, 0.0, 0.0), so.Aberrations(-120.0, 55.0, math.radians(17.0)),
-               so.Aberrations(30.0, 10.0, 0.2, C30=5e4)):
+               so.Aberrations(30.0, 10.0, 0.2, C30=5e4), full):
         o1, p1 = so.reconstruct(prep, ab)
         o2, p2 = tf.reconstruct(pg, ab)
         assert np.abs(o1 - o2.numpy()).max() <= 1e-10 * np.abs(o1).max()
