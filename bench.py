@@ -270,6 +270,67 @@ def stress_256(dev: torch.device, steps: int) -> dict:
     return out
 
 
+def large_512(dev: torch.device, steps: int = 5) -> dict:
+    """The reference's 512^2 timing shape: 512 x 512 scan x 192 x 192 detector
+    u16 (19.3 GB on the device), ~8.9k BF pixels, synthetic. Cold u16 -> phase
+    through the graph pipeline; the backend's G construction; then, from the
+    resident G, the warm complex object, the exact mean phase, and phase +
+    loss - the three figures the reference publishes for this shape."""
+    from quantem.gpu_b200 import B200SSBBackend
+    from quantem.gpu_b200.pipeline import ColdReconstructor
+    from quantem.gpu_b200.synthetic import CONFIGS, generate
+
+    spec = CONFIGS["large_512x512_det192"]
+    t0 = time.perf_counter()
+    counts = generate(spec, dev).counts
+    torch.cuda.synchronize(dev)
+    gen_s = time.perf_counter() - t0
+    kw = dict(semiangle=spec.semiangle_mrad, scan_sampling=spec.scan_step_A,
+              det_sampling=spec.det_sampling_mrad, voltage_kV=spec.voltage_kV)
+    stream = torch.cuda.current_stream(dev)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def timed(fn, n):
+        fn()
+        torch.cuda.synchronize(dev)
+        s.record(stream)
+        for _ in range(n):
+            fn()
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        return s.elapsed_time(e) / n
+
+    rec = ColdReconstructor(counts, **kw)
+    cold_ms = timed(rec.run, steps)
+    n_bf = rec.last_info.n_bf
+    del rec
+    torch.cuda.empty_cache()
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    be = B200SSBBackend(counts, device=dev, **kw)
+    torch.cuda.synchronize(dev)
+    construct_s = time.perf_counter() - t0
+    obj_ms = timed(lambda: be.reconstruct_object(spec.C10, 0.0, 0.0), steps)
+    phase_ms = timed(lambda: be.reconstruct(spec.C10, 0.0, 0.0), max(2, steps // 2))
+    loss_ms = timed(lambda: be.reconstruct_with_loss(spec.C10, 0.0, 0.0), max(2, steps // 2))
+    out = {
+        "workload": "scan 512x512 x detector 192x192 uint16 (19.3 GB), synthetic, C10 = 100 A",
+        "n_bf": n_bf, "generate_s": gen_s,
+        "cold_u16_to_phase_ms": cold_ms,
+        "backend_construct_s": construct_s,
+        "warm_complex_object_ms": obj_ms,
+        "exact_mean_phase_ms": phase_ms,
+        "exact_phase_plus_loss_ms": loss_ms,
+        "reference_published_ms": {
+            "gpu": "RTX PRO 6000 Blackwell Max-Q, real data with 8928 BF",
+            "complex_object": 13.883, "exact_phase": 32.035, "exact_phase_plus_loss": 32.335,
+            "g_construction_s": 0.27},
+    }
+    del be, counts
+    torch.cuda.empty_cache()
+    return out
+
+
 def sweep_3scans(dev: torch.device, steps: int) -> dict:
     """Batched aberration sweep: scans of 96^2, 128^2 and 160x120 positions
     (128^2 detector, padded by the reference's rule to 128^2, 128^2, 256^2),
@@ -633,6 +694,8 @@ def run_b200(args, world, rank, local) -> None:
                 "warm": line["warm_recon_per_s"] / rc["warm_recon_per_s"]}
     if world == 1 and not args.no_stress:
         line["stress_256"] = stress_256(dev, 5)
+        if not args.no_large:
+            line["large_512"] = large_512(dev)
         line["sweep_3scans"] = sweep_3scans(dev, 5)
         line["learned_fits"] = learned_fits(dev)
     if world == 1 and not args.no_cpu_baseline:
@@ -685,6 +748,8 @@ def main() -> None:
     ap.add_argument("--no-oracle", action="store_true")
     ap.add_argument("--with-256", action="store_true",
                     help="--profile-once: also one 256^2 scan loss evaluation")
+    ap.add_argument("--no-large", action="store_true",
+                    help="skip the 512^2 x 192^2 (19.3 GB) leg")
     ap.add_argument("--no-stress", action="store_true",
                     help="skip the 256^2 dose sweep against the FP64 GPU path")
     ap.add_argument("--no-reference-cuda", action="store_true",

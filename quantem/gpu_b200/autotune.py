@@ -72,12 +72,16 @@ def _time_ms(fn, device: torch.device, reps: int) -> float:
     return best
 
 
-def loss_chunk_options(n_bf: int, n_cand: int, sms: int) -> list[int]:
-    """Chunks per candidate whose CTA count fills whole waves, plus neighbours."""
+def loss_chunk_options(n_bf: int, n_cand: int, sms: int, scan: int = 128) -> list[int]:
+    """Chunks per candidate whose CTA count fills whole waves, plus neighbours.
+
+    At 256^2 and above the knob is the column pass's interleave, whose CTA
+    count is (scan / strip width) x chunks x candidates."""
     opts = set()
+    strips = 1 if scan < 256 else scan // (8 if scan >= 1024 else 16)
     for waves in (1, 2, 3, 4):
-        c = max(1, (waves * sms) // n_cand)
-        opts.update({c, c + 1} if c * n_cand < waves * sms else {c})
+        c = max(1, (waves * sms) // (n_cand * strips))
+        opts.update({c, c + 1} if c * n_cand * strips < waves * sms else {c})
     return sorted(c for c in opts if 1 <= c <= min(n_bf, _lib.QSSB_FLAG_CHUNKS_MAX))
 
 
@@ -93,7 +97,7 @@ def tune_loss(g_half, bf_geom, q_row, q_col, cal, candidates: torch.Tensor, flag
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     out = torch.empty(n_cand, dtype=torch.float32, device=dev)
     timings = {}
-    for c in loss_chunk_options(int(cal.n_bf), n_cand, sms):
+    for c in loss_chunk_options(int(cal.n_bf), n_cand, sms, int(cal.scan_rows)):
         f = flags | _lib.flag_chunks(c)
         timings[c] = _time_ms(lambda: ops.loss_batch(g_half, bf_geom, q_row, q_col, cal, candidates,
                                                      flags=f, workspace=workspace, out=out), dev, reps)

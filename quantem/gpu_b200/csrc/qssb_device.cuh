@@ -239,6 +239,126 @@ __device__ __forceinline__ void line_fft(float2* x, int stride, const float2* tw
     }
 }
 
+// ------------------------------------------- register-resident warp FFT
+// N = R * 32 (N in {256, 512, 1024}; R = 8, 16, 32 values per lane), four
+// steps with one shared-memory transpose:
+//   in:  v[n1] = x[32 n1 + lane];
+//   DFT-R over n1 in registers, twiddle W_N^(lane k1);
+//   transpose through T[k1][n2] (pitch 32 + G: conflict-free both ways);
+//   lane (k1 = lane / G, h = lane % G), G = 32 / R, takes n2 = h + G m:
+//   DFT-R over m, twiddle W_32^(h k2'), DFT-G across the G lanes of k1
+//   (warp shuffles);
+//   out: v[j] = X[warp_fft_index<N>(lane, j)] = X[k1 + R (j + R (lane % G))].
+// tw: the N-entry table of fill_twiddles<N>. T: warp_fft_scratch<N>() float2.
+template <int DIR>
+__device__ __forceinline__ void dft32(float2* x, const float2* tw, int step) {
+    float2 e[16], o[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        e[i] = x[2 * i];
+        o[i] = x[2 * i + 1];
+    }
+    dft16<DIR>(e);
+    dft16<DIR>(o);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        float2 w = tw[k * step];
+        if (DIR > 0) w.y = -w.y;
+        const float2 t = cmul(o[k], w);
+        x[k] = cadd(e[k], t);
+        x[k + 16] = csub(e[k], t);
+    }
+}
+
+template <int R, int DIR>
+__device__ __forceinline__ void dft_reg(float2* v, const float2* tw, int step32) {
+    if constexpr (R == 8) {
+        dft8<DIR>(v);
+    } else if constexpr (R == 16) {
+        dft16<DIR>(v);
+    } else {
+        static_assert(R == 32, "warp FFT radix 8, 16 or 32");
+        dft32<DIR>(v, tw, step32);
+    }
+}
+
+template <int N>
+__host__ __device__ constexpr int warp_fft_scratch() {
+    return (N / 32) * (32 + 32 / (N / 32));
+}
+
+template <int N>
+__device__ __forceinline__ int warp_fft_index(int lane, int j) {
+    constexpr int R = N / 32;
+    constexpr int G = 32 / R;
+    return lane / G + R * (j + R * (lane % G));
+}
+
+template <int N, int DIR>
+__device__ __forceinline__ void warp_fft(float2 (&v)[N / 32], float2* T, const float2* tw, int lane) {
+    constexpr int R = N / 32;
+    constexpr int G = 32 / R;
+    constexpr int P = 32 + G;
+    constexpr int S32 = N / 32;  // W_32^e = tw[e * S32]
+    dft_reg<R, DIR>(v, tw, S32);
+#pragma unroll
+    for (int k1 = 1; k1 < R; ++k1) {
+        float2 w = tw[lane * k1];
+        if (DIR > 0) w.y = -w.y;
+        v[k1] = cmul(v[k1], w);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < R; ++k1) T[k1 * P + lane] = v[k1];
+    __syncwarp();
+    const int k1 = lane / G;
+    const int h = lane % G;
+#pragma unroll
+    for (int m = 0; m < R; ++m) v[m] = T[k1 * P + h + G * m];
+    __syncwarp();
+    dft_reg<R, DIR>(v, tw, S32);
+    if constexpr (G > 1) {
+#pragma unroll
+        for (int k2 = 1; k2 < R; ++k2) {
+            float2 w = tw[((h * k2) & 31) * S32];
+            if (DIR > 0) w.y = -w.y;
+            v[k2] = cmul(v[k2], w);
+        }
+        if constexpr (G == 2) {
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                float2 o;
+                o.x = __shfl_xor_sync(0xffffffffu, v[j].x, 1);
+                o.y = __shfl_xor_sync(0xffffffffu, v[j].y, 1);
+                v[j] = h == 0 ? cadd(v[j], o) : csub(o, v[j]);
+            }
+        } else {
+            static_assert(G == 4, "cross-lane radix 2 or 4");
+            const int base = lane & ~3;
+#pragma unroll
+            for (int j = 0; j < R; ++j) {
+                float2 s[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    s[i].x = __shfl_sync(0xffffffffu, v[j].x, base + i);
+                    s[i].y = __shfl_sync(0xffffffffu, v[j].y, base + i);
+                }
+                // X_h = sum_i W4^(i h) s_i, W4 = exp(DIR 2 pi i / 4) = DIR i
+                float2 acc = s[0];
+#pragma unroll
+                for (int i = 1; i < 4; ++i) {
+                    const int e = (i * h) & 3;
+                    float2 t = s[i];
+                    if (e == 1) t = mul_dir_i<DIR>(t);
+                    else if (e == 2) t = make_float2(-t.x, -t.y);
+                    else if (e == 3) t = mul_dir_i<-DIR>(t);
+                    acc = cadd(acc, t);
+                }
+                v[j] = acc;
+            }
+        }
+    }
+}
+
 // --------------------------------------------------------------- physics
 // Per-candidate probe constants. chi(u) = factor * alpha^2 *
 // (C10 + C12 (cos2phi cos2phi12 + sin2phi sin2phi12)) + c30_half * alpha^4,

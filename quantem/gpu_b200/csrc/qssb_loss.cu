@@ -349,187 +349,6 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
     for (int i = tid; i < N * N; i += 512) pq[i] = sq[(i >> 7) * kL128P + (i & 127)];
 }
 
-// ------------------------------------------------------------- N = 256
-// The 256^2 half plane (264 KB) does not fit shared memory. Per BF pixel:
-//   rows: each warp evaluates C on rows 0..128 one line at a time in its own
-//     shared line (the value C(r, 128) saved first), inverse-FFTs the line
-//     and writes it to the CTA's staging plane in global memory (L2);
-//     C(-r', 128), r' = 1..127, is evaluated directly;
-//   columns: after a barrier each warp rebuilds its columns from the staging
-//     plane (rows 129..255 by row(-r) = -conj(row(r)) + (-1)^x delta_r,
-//     delta_r = conj C(r, 128) + C(-r, 128)), inverse-FFTs them and adds
-//     phi and phi^2 to the CTA's own partial planes, stored column-major
-//     (x * N + y): every element belongs to one lane, so no atomics.
-// The same scheme serves 512^2 and 1024^2 (N/2 + 1 evaluated rows).
-constexpr int kL256 = 256;
-
-template <int N>
-struct LossStagedSmem {
-    static constexpr int rows = N / 2 + 1;
-    static constexpr size_t lines = sizeof(float2) * kLossWarps * N;
-    static constexpr size_t misc = sizeof(float2) * (N + 3 * (N / 2));  // tw, cpos, cneg, delta
-    static constexpr size_t bytes = lines + misc;
-    static constexpr size_t stage_per_cta = sizeof(float2) * rows * N;
-};
-
-static size_t staged_stage_per_cta(int n) {
-    switch (n) {
-        case 256: return LossStagedSmem<256>::stage_per_cta;
-        case 512: return LossStagedSmem<512>::stage_per_cta;
-        case 1024: return LossStagedSmem<1024>::stage_per_cta;
-        default: return 0;
-    }
-}
-
-template <int N, bool CHI64, bool QUAD>
-__global__ void __launch_bounds__(kLossThreads, 1) k_loss_staged(
-    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
-    const float* __restrict__ q_row, const float* __restrict__ q_col,
-    const qssb_aberrations_t* __restrict__ cands, qssb_calibration_t cal,
-    const float2* __restrict__ eq_table, int bf_per_chunk, int n_chunks, float* __restrict__ part,
-    float2* __restrict__ stage) {
-    constexpr int H = N / 2 + 1;
-    constexpr int kRows = LossStagedSmem<N>::rows;
-    constexpr bool kSep = QUAD && !CHI64;
-    extern __shared__ float4 smem4[];
-    float2* lines = reinterpret_cast<float2*>(smem4);
-    float2* tw = lines + kLossWarps * N;
-    float2* cpos = tw + N;
-    float2* cneg = cpos + N / 2;
-    float2* delta = cneg + N / 2;
-    __shared__ Probe sp;
-    __shared__ float2 s_phr[kSep ? N : 1];
-    __shared__ float2 s_phc[kSep ? N : 1];
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
-    const int chunk = blockIdx.x;
-    const int cand = blockIdx.y;
-    const size_t cta = (size_t)cand * n_chunks + chunk;
-    float2* S = stage + cta * (size_t)kRows * N;
-    float* ps = part + cta * 2 * (size_t)N * N;
-    float* pq = ps + (size_t)N * N;
-    float2* line = lines + warp * N;
-    if (tid == 0) {
-        const qssb_aberrations_t ab = cands[cand];
-        sp = make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
-    }
-    fill_twiddles<N>(tw, tid, kLossThreads);
-    // this lane's accumulator elements: columns warp + 16 j, rows lane + 32 t
-    for (int j = 0; j < N / kLossWarps; ++j) {
-        const int x = warp + kLossWarps * j;
-#pragma unroll
-        for (int t = 0; t < N / 32; ++t) {
-            ps[(size_t)x * N + lane + 32 * t] = 0.0f;
-            pq[(size_t)x * N + lane + 32 * t] = 0.0f;
-        }
-    }
-    __syncthreads();
-    const Probe& p = sp;
-    const float2* eqc = eq_table + (size_t)cand * N * N;
-    auto fill_phase = [&](int b) {  // e^{i 2 q_row(r) u}, e^{i 2 q_col(c) v}
-        const float kx = __ldg(geom + b);
-        const float ky = __ldg(geom + n_bf + b);
-        float sn, cs;
-        for (int i = tid; i < 2 * N; i += kLossThreads) {
-            if (i < N) {
-                sincosf(2.0f * __ldg(q_row + i) * fmaf(p.mxx, kx, p.mxy * ky), &sn, &cs);
-                s_phr[i] = make_float2(cs, sn);
-            } else {
-                sincosf(2.0f * __ldg(q_col + i - N) * fmaf(p.mxy, kx, p.myy * ky), &sn, &cs);
-                s_phc[i - N] = make_float2(cs, sn);
-            }
-        }
-    };
-    const int b0 = chunk * bf_per_chunk;
-    int nb = n_bf - b0;
-    if (nb > bf_per_chunk) nb = bf_per_chunk;
-    const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
-    if constexpr (kSep) {
-        if (nb > 0) fill_phase(b0);
-        __syncthreads();
-    }
-    auto eval = [&](int b, const BFQuad& kq, const float2& pk, int r, int c) -> float2 {
-        const float2* gb = g + (size_t)b * N * H;
-        const float2 gv = c <= N / 2 ? __ldg(gb + r * H + c)
-                                     : cconj(__ldg(gb + ((N - r) & (N - 1)) * H + (N - c)));
-        if constexpr (kSep) {
-            const float2 lo = make_float2(kq.kx_lo, kq.ky_lo);
-            return corrected_quad_e(__ldg(q_row + r), __ldg(q_col + c), r, c, __ldg(eqc + r * N + c),
-                                    kq.kx, kq.ky, kq.ak, &lo, cmul(s_phr[r], s_phc[c]), gv, p);
-        } else if constexpr (QUAD) {
-            return corrected_quad<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c,
-                                         __ldg(eqc + r * N + c), kq, gv, p);
-        } else {
-            return corrected<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c, kq.kx, kq.ky,
-                                    kq.kx_lo, kq.ky_lo, pk, gv, p);
-        }
-    };
-    for (int i = 0; i < nb; ++i) {
-        const int b = b0 + i;
-        const BFQuad kq = bf_quad(geom, n_bf, b, p);
-        float2 pk = make_float2(0.0f, 0.0f);
-        if constexpr (!QUAD)
-            pk = probe_at_bf<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
-                                    __ldg(geom + 4 * n_bf + b), __ldg(geom + 5 * n_bf + b), p);
-        // C(-r', N/2) for r' = 1..N/2-1 (row N - r')
-        for (int j = tid; j < N / 2; j += kLossThreads)
-            if (j >= 1) cneg[j] = eval(b, kq, pk, N - j, N / 2);
-        // rows 0..N/2: evaluate, keep C(r, N/2), inverse FFT, stage
-        for (int r = warp; r < kRows; r += kLossWarps) {
-#pragma unroll
-            for (int t = 0; t < N / 32; ++t) {
-                const int c = lane + 32 * t;
-                float2 v = (r == 0 && c == 0) ? dc : eval(b, kq, pk, r, c);
-                if (c == N / 2 && r >= 1 && r < N / 2) cpos[r] = v;
-                line[c] = v;
-            }
-            __syncwarp();
-            line_fft<N, +1>(line, 1, tw, lane);
-#pragma unroll
-            for (int t = 0; t < N / 32; ++t) S[(size_t)r * N + lane + 32 * t] = line[lane + 32 * t];
-            __syncwarp();
-        }
-        __syncthreads();
-        for (int j = tid; j < N / 2; j += kLossThreads)
-            if (j >= 1) delta[j] = cadd(cconj(cpos[j]), cneg[j]);
-        __syncthreads();
-        // columns
-        for (int j = 0; j < N / kLossWarps; ++j) {
-            const int x = warp + kLossWarps * j;
-            const float sign = (x & 1) ? -1.0f : 1.0f;
-#pragma unroll
-            for (int t = 0; t < N / 32; ++t) {
-                const int r = lane + 32 * t;
-                float2 v;
-                if (r < kRows) {
-                    v = S[(size_t)r * N + x];
-                } else {
-                    const float2 m = S[(size_t)(N - r) * N + x];
-                    const float2 d = delta[N - r];
-                    v = make_float2(fmaf(sign, d.x, -m.x), fmaf(sign, d.y, m.y));
-                }
-                line[r] = v;
-            }
-            __syncwarp();
-            line_fft<N, +1>(line, 1, tw, lane);
-#pragma unroll
-            for (int t = 0; t < N / 32; ++t) {
-                const int y = lane + 32 * t;
-                const float2 v = line[y];
-                const float ph = atan2f(v.y, v.x);
-                ps[(size_t)x * N + y] += ph;
-                pq[(size_t)x * N + y] = fmaf(ph, ph, pq[(size_t)x * N + y]);
-            }
-            __syncwarp();
-        }
-        if constexpr (kSep) {
-            if (i + 1 < nb) fill_phase(b + 1);
-        }
-        __syncthreads();
-    }
-}
-
 template <int N>
 __global__ void k_loss_reduce(const float* __restrict__ part, int n_chunks, int n_bf,
                               double* __restrict__ var, float* __restrict__ mean_phase,
@@ -569,30 +388,319 @@ __global__ void __launch_bounds__(256) k_loss_final(const double* __restrict__ v
     if (threadIdx.x == 0) losses[cand] = (float)(red[0] / (double)npos);
 }
 
+// ---------------------------------------------- N >= 256: two passes
+// A 256^2 .. 1024^2 plane does not fit one CTA's shared memory. The BF pixels
+// are taken in chunks whose row-transformed planes stay in L2 (about 48 MB
+// for all candidates of the call):
+//   k_loss_rows: one warp per row of C_b (rows 0..N/2 on the +-q half set, all
+//     N rows for the 14-term chi): evaluate, inverse-FFT, store the row in the
+//     chunk's staging planes; the half-set path also stores
+//     delta_r = conj C(r, N/2) + C(-r, N/2), r = 1..N/2-1, the Nyquist-column
+//     deviation from C(-q) = -conj C(q) (row(-r) = -conj row(r) + (-1)^x delta_r
+//     after the row transforms);
+//   k_loss_cols: a CTA owns a strip of 16 columns (8 at 1024) and every n_sub-th BF pixel
+//     of the chunk: it loads the strip (coalesced 128-byte rows), rebuilds the
+//     lower half rows, inverse-FFTs one column per warp and keeps phi and phi^2
+//     of its pixels in registers; at the end of the chunk it adds them to its
+//     own partial planes (column-major), so every element has one writer.
+constexpr int kL256 = 256;
+constexpr size_t kStageBudget = 32u << 20;
+
+// Rows per CTA of the row pass and columns per CTA of the column pass (one
+// warp each): 16, or 8 at 1024 where a lane holds 32 values of its line.
+__host__ __device__ constexpr int row_warps(int n) { return n >= 1024 ? 8 : 16; }
+__host__ __device__ constexpr int col_tile(int n) { return n >= 1024 ? 8 : 16; }
+
+template <int N, bool FULL>
+struct TwoPass {
+    static constexpr int rows = FULL ? N : N / 2 + 1;
+    static constexpr int rwarps = row_warps(N);
+    static constexpr int tile = col_tile(N);
+    static constexpr int scratch = warp_fft_scratch<N>();
+    // column line pitch: odd mod 16 (conflict-free strip loads), and room for
+    // the warp FFT's transpose once the line is in registers
+    static constexpr int pitch = (scratch > N ? scratch : N) | 1;
+    static constexpr size_t row_smem = sizeof(float2) * ((size_t)rwarps * scratch + N);
+    static constexpr size_t col_smem = sizeof(float2) * ((size_t)tile * pitch + N);
+};
+
+struct TwoPassPlan {
+    int chunk_bf;  // BF pixels per (rows, columns) launch pair
+    int n_sub;     // column-pass interleave = partial planes per candidate
+};
+
+static TwoPassPlan plan_two_pass(int n, bool full, int n_bf, int n_cand, int chunks_req) {
+    TwoPassPlan tp;
+    const size_t per_bf = sizeof(float2) * (size_t)(full ? n : n / 2 + 1) * n;
+    long long c = (long long)(kStageBudget / (per_bf * (size_t)n_cand));
+    if (c < 1) c = 1;
+    if (c > n_bf) c = n_bf;
+    tp.chunk_bf = (int)c;
+    const int strips = n / col_tile(n);
+    int sub = chunks_req > 0 ? chunks_req : (296 + strips * n_cand - 1) / (strips * n_cand);
+    if (sub < 1) sub = 1;
+    if (sub > tp.chunk_bf) sub = tp.chunk_bf;
+    tp.n_sub = sub;
+    return tp;
+}
+
+template <int N, bool CHI64, bool QUAD, bool FULL>
+__global__ void __launch_bounds__(32 * row_warps(N)) k_loss_rows(
+    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
+    const float* __restrict__ q_row, const float* __restrict__ q_col, const void* __restrict__ cands,
+    qssb_calibration_t cal, const float2* __restrict__ eq_table, int b0, int nb_chunk,
+    float2* __restrict__ stage, float2* __restrict__ delta) {
+    using TP = TwoPass<N, FULL>;
+    constexpr int H = N / 2 + 1;
+    constexpr int RW = TP::rwarps;
+    constexpr int RPL = N / 32;
+    constexpr bool kSep = !FULL && QUAD && !CHI64;
+    extern __shared__ float4 smem4[];
+    float2* scr = reinterpret_cast<float2*>(smem4);
+    float2* tw = scr + RW * TP::scratch;
+    __shared__ Probe sp;
+    __shared__ FullChi sf;
+    __shared__ FullChi64 sd;
+    __shared__ float2 s_phc[kSep ? N : 1];
+    __shared__ float2 s_phr[kSep ? RW : 1];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int bi = blockIdx.y;
+    const int b = b0 + bi;
+    const int cand = blockIdx.z;
+    const int r0 = blockIdx.x * RW;
+    const int r = r0 + warp;
+    if (tid == 0) {
+        if constexpr (FULL) {
+            const auto* fc = static_cast<const qssb_full_aberrations_t*>(cands) + cand;
+            sp = make_probe_common(cal, 0.0f, 0.0f, 0.0f, 0.0f);
+            make_full_chi(fc->magnitude, fc->angle_rad, cal.wavelength_A, sf, sd);
+        } else {
+            const qssb_aberrations_t ab = static_cast<const qssb_aberrations_t*>(cands)[cand];
+            sp = make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
+        }
+    }
+    fill_twiddles<N>(tw, tid, 32 * RW);
+    __syncthreads();
+    const Probe& p = sp;
+    const BFQuad kq = bf_quad(geom, n_bf, b, p);
+    float2 pk = make_float2(0.0f, 0.0f);
+    if constexpr (FULL) {
+        pk = probe_full_at_bf((double)kq.kx + (double)kq.kx_lo, (double)kq.ky + (double)kq.ky_lo,
+                              kq.ak, sd);
+    } else if constexpr (!QUAD) {
+        pk = probe_at_bf<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
+                                __ldg(geom + 4 * n_bf + b), __ldg(geom + 5 * n_bf + b), p);
+    }
+    if constexpr (kSep) {  // e^{i 2 q_col(c) v} for all columns, e^{i 2 q_row(r) u} for this CTA's rows
+        for (int i = tid; i < N + RW; i += 32 * RW) {
+            float sn, cs;
+            if (i < N) {
+                sincosf(2.0f * __ldg(q_col + i) * kq.v, &sn, &cs);
+                s_phc[i] = make_float2(cs, sn);
+            } else if (r0 + i - N < N) {
+                sincosf(2.0f * __ldg(q_row + r0 + i - N) * kq.u, &sn, &cs);
+                s_phr[i - N] = make_float2(cs, sn);
+            }
+        }
+        __syncthreads();
+    }
+    if (r >= TP::rows) return;  // warp-uniform; no block barrier follows
+    const float2* gb = g + (size_t)b * N * H;
+    const float2* eqc = eq_table + (size_t)cand * N * N;
+    const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
+    // G is read once per candidate: streaming loads keep the chunk's staged
+    // rows in L2 for the column pass
+    auto eval = [&](int rr, int c, float2 e_row) -> float2 {
+        const float2 gv = c <= N / 2 ? __ldcs(gb + rr * H + c)
+                                     : cconj(__ldcs(gb + ((N - rr) & (N - 1)) * H + (N - c)));
+        if constexpr (FULL) {
+            return corrected_full<CHI64>(__ldg(q_row + rr), __ldg(q_col + c), rr, c, kq.kx, kq.ky,
+                                         kq.kx_lo, kq.ky_lo, pk, gv, p, sf, sd);
+        } else if constexpr (kSep) {
+            const float2 lo = make_float2(kq.kx_lo, kq.ky_lo);
+            return corrected_quad_e(__ldg(q_row + rr), __ldg(q_col + c), rr, c,
+                                    __ldg(eqc + rr * N + c), kq.kx, kq.ky, kq.ak, &lo,
+                                    cmul(e_row, s_phc[c]), gv, p);
+        } else if constexpr (QUAD) {
+            return corrected_quad<CHI64>(__ldg(q_row + rr), __ldg(q_col + c), rr, c,
+                                         __ldg(eqc + rr * N + c), kq, gv, p);
+        } else {
+            return corrected<CHI64>(__ldg(q_row + rr), __ldg(q_col + c), rr, c, kq.kx, kq.ky,
+                                    kq.kx_lo, kq.ky_lo, pk, gv, p);
+        }
+    };
+    const float2 e_row = kSep ? s_phr[warp] : make_float2(1.0f, 0.0f);
+    float2 v[RPL];
+#pragma unroll
+    for (int t = 0; t < RPL; ++t) {
+        const int c = lane + 32 * t;
+        v[t] = (r == 0 && c == 0) ? dc : eval(r, c, e_row);
+        if (!FULL && t == N / 64 && lane == 0 && r >= 1 && r < N / 2) {  // c == N/2
+            float2 e_neg = make_float2(1.0f, 0.0f);
+            if constexpr (kSep) {
+                float sn, cs;
+                sincosf(2.0f * __ldg(q_row + N - r) * kq.u, &sn, &cs);
+                e_neg = make_float2(cs, sn);
+            }
+            delta[((size_t)cand * nb_chunk + bi) * (N / 2) + r] =
+                cadd(cconj(v[t]), eval(N - r, N / 2, e_neg));
+        }
+    }
+    warp_fft<N, +1>(v, scr + warp * TP::scratch, tw, lane);
+    float2* out = stage + (((size_t)cand * nb_chunk + bi) * TP::rows + r) * N;
+#pragma unroll
+    for (int j = 0; j < RPL; ++j) out[warp_fft_index<N>(lane, j)] = v[j];
+}
+
+template <int N, bool FULL>
+__global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
+    const float2* __restrict__ stage, const float2* __restrict__ delta, int nb_chunk, int n_sub,
+    int first, float* __restrict__ part) {
+    using TP = TwoPass<N, FULL>;
+    constexpr int P = TP::pitch;
+    constexpr int RPL = N / 32;
+    constexpr int kColTile = TP::tile;
+    constexpr int NT = 32 * kColTile;
+    extern __shared__ float4 smem4[];
+    float2* tile = reinterpret_cast<float2*>(smem4);
+    float2* tw = tile + kColTile * P;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int x0 = blockIdx.x * kColTile;
+    const int sub = blockIdx.y;
+    const int cand = blockIdx.z;
+    const int x = x0 + warp;
+    const float sign = (x & 1) ? -1.0f : 1.0f;
+    float2* line = tile + warp * P;
+    fill_twiddles<N>(tw, tid, NT);
+    float as[RPL], aq[RPL];
+#pragma unroll
+    for (int t = 0; t < RPL; ++t) as[t] = aq[t] = 0.0f;
+    for (int bi = sub; bi < nb_chunk; bi += n_sub) {
+        const float2* S = stage + ((size_t)cand * nb_chunk + bi) * TP::rows * N + x0;
+        __syncthreads();  // the previous pixel's columns are done (and tw is filled)
+        for (int e = tid; e < TP::rows * kColTile; e += NT) {
+            const int rr = e / kColTile;
+            const int c = e - rr * kColTile;
+            tile[c * P + rr] = __ldcs(S + (size_t)rr * N + c);
+        }
+        __syncthreads();
+        if constexpr (!FULL) {
+            const float2* d = delta + ((size_t)cand * nb_chunk + bi) * (N / 2);
+#pragma unroll
+            for (int t = 0; t < RPL; ++t) {
+                const int rr = lane + 32 * t;
+                if (rr > N / 2) {
+                    const float2 m = line[N - rr];
+                    const float2 dd = __ldg(d + N - rr);
+                    line[rr] = make_float2(fmaf(sign, dd.x, -m.x), fmaf(sign, dd.y, m.y));
+                }
+            }
+            __syncwarp();
+        }
+        float2 v[RPL];
+#pragma unroll
+        for (int t = 0; t < RPL; ++t) v[t] = line[lane + 32 * t];
+        __syncwarp();  // the line becomes the FFT's transpose scratch
+        warp_fft<N, +1>(v, line, tw, lane);
+#pragma unroll
+        for (int j = 0; j < RPL; ++j) {
+            const float ph = atan2f(v[j].y, v[j].x);
+            as[j] += ph;
+            aq[j] = fmaf(ph, ph, aq[j]);
+        }
+    }
+    float* ps = part + ((size_t)(cand * n_sub + sub) * 2) * N * N + (size_t)x * N;
+    float* pq = ps + (size_t)N * N;
+#pragma unroll
+    for (int j = 0; j < RPL; ++j) {
+        const int y = warp_fft_index<N>(lane, j);
+        if (first) {
+            ps[y] = as[j];
+            pq[y] = aq[j];
+        } else {
+            ps[y] += as[j];
+            pq[y] += aq[j];
+        }
+    }
+}
+
 struct LossPlan {
     int bf_per_chunk;
-    int n_chunks;
+    int n_chunks;      // partial planes per candidate
+    int chunk_bf;      // N >= 256: BF pixels per row/column launch pair
     size_t part_bytes;
     size_t var_bytes;
     size_t eq_bytes;
-    size_t stage_bytes;  // N = 256: one staging half plane per CTA
+    size_t stage_bytes;  // N >= 256: row-transformed planes of one chunk
+    size_t delta_bytes;  // N >= 256, half set: Nyquist-column deviations
 };
 
 // Deterministic: about 296 CTAs in total (two per B200 SM), at least one BF
-// pixel each.
-static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0) {
+// pixel each. N >= 256: the two-pass plan (n_chunks = its column interleave).
+static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool full = false) {
     LossPlan pl;
-    int chunks = chunks_req > 0 ? chunks_req : (296 + n_cand - 1) / n_cand;
-    if (chunks < 1) chunks = 1;
-    if (chunks > n_bf) chunks = n_bf;
-    pl.bf_per_chunk = (n_bf + chunks - 1) / chunks;
-    pl.n_chunks = (n_bf + pl.bf_per_chunk - 1) / pl.bf_per_chunk;
+    if (n >= kL256) {
+        const TwoPassPlan tp = plan_two_pass(n, full, n_bf, n_cand, chunks_req);
+        pl.chunk_bf = tp.chunk_bf;
+        pl.n_chunks = tp.n_sub;
+        pl.bf_per_chunk = 0;
+        const size_t rows = full ? (size_t)n : (size_t)(n / 2 + 1);
+        pl.stage_bytes = sizeof(float2) * rows * n * (size_t)tp.chunk_bf * n_cand;
+        pl.delta_bytes = full ? 0 : sizeof(float2) * (size_t)(n / 2) * tp.chunk_bf * n_cand;
+    } else {
+        int chunks = chunks_req > 0 ? chunks_req : (296 + n_cand - 1) / n_cand;
+        if (chunks < 1) chunks = 1;
+        if (chunks > n_bf) chunks = n_bf;
+        pl.bf_per_chunk = (n_bf + chunks - 1) / chunks;
+        pl.n_chunks = (n_bf + pl.bf_per_chunk - 1) / pl.bf_per_chunk;
+        pl.chunk_bf = 0;
+        pl.stage_bytes = 0;
+        pl.delta_bytes = 0;
+    }
     pl.part_bytes = sizeof(float) * 2 * (size_t)n * n * pl.n_chunks * n_cand;
     pl.part_bytes = (pl.part_bytes + 255) & ~(size_t)255;
     pl.var_bytes = sizeof(double) * (size_t)n * n * n_cand;
-    pl.eq_bytes = sizeof(float2) * (size_t)n * n * n_cand;
-    pl.stage_bytes = staged_stage_per_cta(n) * (size_t)pl.n_chunks * n_cand;
+    pl.eq_bytes = full ? 0 : sizeof(float2) * (size_t)n * n * n_cand;
+    pl.stage_bytes = (pl.stage_bytes + 255) & ~(size_t)255;
     return pl;
+}
+
+static size_t loss_workspace(const LossPlan& pl) {
+    return pl.part_bytes + pl.var_bytes + pl.eq_bytes + pl.stage_bytes + pl.delta_bytes;
+}
+
+// The N >= 256 launch sequence after the eq table: row and column passes per
+// BF chunk; the partial planes then go through k_loss_reduce.
+template <int N, bool CHI64, bool QUAD, bool FULL>
+static int launch_two_pass(const float* g_half, const float* geom, const float* q_row,
+                           const float* q_col, const qssb_calibration_t& cal, const void* cands,
+                           int n_cand, const LossPlan& pl, const float2* eq, float* part,
+                           char* stage_base, cudaStream_t s) {
+    using TP = TwoPass<N, FULL>;
+    float2* stage = reinterpret_cast<float2*>(stage_base);
+    float2* delta = reinterpret_cast<float2*>(stage_base + pl.stage_bytes);
+    CUDA_TRY(cudaFuncSetAttribute(k_loss_rows<N, CHI64, QUAD, FULL>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP::row_smem));
+    CUDA_TRY(cudaFuncSetAttribute(k_loss_cols<N, FULL>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP::col_smem));
+    const auto* g = reinterpret_cast<const float2*>(g_half);
+    for (int b0 = 0; b0 < cal.n_bf; b0 += pl.chunk_bf) {
+        const int nb = cal.n_bf - b0 < pl.chunk_bf ? cal.n_bf - b0 : pl.chunk_bf;
+        k_loss_rows<N, CHI64, QUAD, FULL>
+            <<<dim3((TP::rows + TP::rwarps - 1) / TP::rwarps, nb, n_cand), 32 * TP::rwarps,
+               TP::row_smem, s>>>(g, cal.n_bf, geom, q_row, q_col, cands, cal, eq, b0, nb, stage,
+                                  delta);
+        CUDA_TRY(cudaGetLastError());
+        k_loss_cols<N, FULL><<<dim3(N / TP::tile, pl.n_chunks, n_cand), 32 * TP::tile,
+                               TP::col_smem, s>>>(stage, delta, nb, pl.n_chunks, b0 == 0 ? 1 : 0,
+                                                  part);
+        CUDA_TRY(cudaGetLastError());
+    }
+    return QSSB_OK;
 }
 
 template <int N, bool SYM, bool CHI64, bool QUAD>
@@ -609,14 +717,11 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
         CUDA_TRY(cudaGetLastError());
     }
     if constexpr (N >= kL256) {
-        static_assert(SYM, "the staged loss evaluates the half plane");
-        float2* stage = reinterpret_cast<float2*>(ws + pl.part_bytes + pl.var_bytes + pl.eq_bytes);
-        const size_t smem = LossStagedSmem<N>::bytes;
-        CUDA_TRY(cudaFuncSetAttribute(k_loss_staged<N, CHI64, QUAD>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_loss_staged<N, CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
-            reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal, eq,
-            pl.bf_per_chunk, pl.n_chunks, part, stage);
+        static_assert(SYM, "the two-pass loss evaluates the half set");
+        const int rc = launch_two_pass<N, CHI64, QUAD, false>(
+            g_half, geom, q_row, q_col, cal, cands, n_cand, pl, eq, part,
+            ws + pl.part_bytes + pl.var_bytes + pl.eq_bytes, s);
+        if (rc) return rc;
     } else if constexpr (N == 128) {
         const size_t smem = Loss128Smem::bytes;
         CUDA_TRY(cudaFuncSetAttribute(k_loss_moments128<CHI64, QUAD>,
@@ -774,116 +879,27 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_full(
 }
 
 template <int N, bool CHI64>
-__global__ void __launch_bounds__(kLossThreads, 1) k_loss_full_staged(
-    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
-    const float* __restrict__ q_row, const float* __restrict__ q_col,
-    const qssb_full_aberrations_t* __restrict__ cands, qssb_calibration_t cal, int bf_per_chunk,
-    int n_chunks, float* __restrict__ part, float2* __restrict__ stage) {
-    constexpr int H = N / 2 + 1;
-    extern __shared__ float4 smem4[];
-    float2* lines = reinterpret_cast<float2*>(smem4);
-    float2* tw = lines + kLossWarps * N;
-    __shared__ FullConsts sh;
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
-    const int chunk = blockIdx.x;
-    const int cand = blockIdx.y;
-    const size_t cta = (size_t)cand * n_chunks + chunk;
-    float2* S = stage + cta * (size_t)N * N;
-    float* ps = part + cta * 2 * (size_t)N * N;
-    float* pq = ps + (size_t)N * N;
-    float2* line = lines + warp * N;
-    if (tid == 0) load_full_consts(sh, cands, cand, cal);
-    fill_twiddles<N>(tw, tid, kLossThreads);
-    for (int j = 0; j < N / kLossWarps; ++j) {
-        const int x = warp + kLossWarps * j;
-#pragma unroll
-        for (int t = 0; t < N / 32; ++t) {
-            ps[(size_t)x * N + lane + 32 * t] = 0.0f;
-            pq[(size_t)x * N + lane + 32 * t] = 0.0f;
-        }
-    }
-    __syncthreads();
-    const int b0 = chunk * bf_per_chunk;
-    int nb = n_bf - b0;
-    if (nb > bf_per_chunk) nb = bf_per_chunk;
-    const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
-    for (int i = 0; i < nb; ++i) {
-        const int b = b0 + i;
-        const float kx = __ldg(geom + b);
-        const float ky = __ldg(geom + n_bf + b);
-        const float kx_lo = __ldg(geom + 6 * n_bf + b);
-        const float ky_lo = __ldg(geom + 7 * n_bf + b);
-        const float2 pk = probe_full_at_bf((double)kx + (double)kx_lo, (double)ky + (double)ky_lo,
-                                           __ldg(geom + 5 * n_bf + b), sh.d);
-        const float2* gb = g + (size_t)b * N * H;
-        for (int r = warp; r < N; r += kLossWarps) {
-#pragma unroll
-            for (int t = 0; t < N / 32; ++t) {
-                const int c = lane + 32 * t;
-                const float2 gv = c <= N / 2 ? __ldg(gb + r * H + c)
-                                             : cconj(__ldg(gb + ((N - r) & (N - 1)) * H + (N - c)));
-                float2 v = corrected_full<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c, kx, ky,
-                                                 kx_lo, ky_lo, pk, gv, sh.p, sh.f, sh.d);
-                if (r == 0 && c == 0) v = dc;
-                line[c] = v;
-            }
-            __syncwarp();
-            line_fft<N, +1>(line, 1, tw, lane);
-#pragma unroll
-            for (int t = 0; t < N / 32; ++t) S[(size_t)r * N + lane + 32 * t] = line[lane + 32 * t];
-            __syncwarp();
-        }
-        __syncthreads();
-        for (int j = 0; j < N / kLossWarps; ++j) {
-            const int x = warp + kLossWarps * j;
-#pragma unroll
-            for (int t = 0; t < N / 32; ++t) line[lane + 32 * t] = S[(size_t)(lane + 32 * t) * N + x];
-            __syncwarp();
-            line_fft<N, +1>(line, 1, tw, lane);
-#pragma unroll
-            for (int t = 0; t < N / 32; ++t) {
-                const int y = lane + 32 * t;
-                const float2 v = line[y];
-                const float ph = atan2f(v.y, v.x);
-                ps[(size_t)x * N + y] += ph;
-                pq[(size_t)x * N + y] = fmaf(ph, ph, pq[(size_t)x * N + y]);
-            }
-            __syncwarp();
-        }
-        __syncthreads();
-    }
-}
-
-static size_t full_stage_bytes(int n, const LossPlan& pl, int n_cand) {
-    return n >= kL256 ? sizeof(float2) * (size_t)n * n * pl.n_chunks * n_cand : 0;
-}
-
-template <int N, bool CHI64>
 static int launch_loss_full(const float* g_half, const float* geom, const float* q_row,
                             const float* q_col, const qssb_calibration_t& cal,
                             const qssb_full_aberrations_t* cands, int n_cand, int chunks, char* ws,
                             float* losses, float* mean_phase, cudaStream_t s) {
-    const LossPlan pl = plan_loss(N, cal.n_bf, n_cand, chunks);
+    const LossPlan pl = plan_loss(N, cal.n_bf, n_cand, chunks, true);
     float* part = reinterpret_cast<float*>(ws);
     double* var = reinterpret_cast<double*>(ws + pl.part_bytes);
-    const auto* gh = reinterpret_cast<const float2*>(g_half);
     if constexpr (N >= kL256) {
-        float2* stage = reinterpret_cast<float2*>(ws + pl.part_bytes + pl.var_bytes);
-        const size_t smem = sizeof(float2) * (kLossWarps * N + N);
-        CUDA_TRY(cudaFuncSetAttribute(k_loss_full_staged<N, CHI64>,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_loss_full_staged<N, CHI64><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
-            gh, cal.n_bf, geom, q_row, q_col, cands, cal, pl.bf_per_chunk, pl.n_chunks, part, stage);
+        const int rc = launch_two_pass<N, CHI64, false, true>(
+            g_half, geom, q_row, q_col, cal, cands, n_cand, pl, nullptr, part,
+            ws + pl.part_bytes + pl.var_bytes, s);
+        if (rc) return rc;
     } else {
         const size_t smem = LossSmem<N>::bytes + sizeof(float) * N * N;
         CUDA_TRY(cudaFuncSetAttribute(k_loss_full<N, CHI64>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         k_loss_full<N, CHI64><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
-            gh, cal.n_bf, geom, q_row, q_col, cands, cal, pl.bf_per_chunk, pl.n_chunks, part);
+            reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal,
+            pl.bf_per_chunk, pl.n_chunks, part);
+        CUDA_TRY(cudaGetLastError());
     }
-    CUDA_TRY(cudaGetLastError());
     k_loss_reduce<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(part, pl.n_chunks, cal.n_bf,
                                                                        var, mean_phase, 0);
     CUDA_TRY(cudaGetLastError());
@@ -916,7 +932,7 @@ extern "C" int qssb_loss_workspace_bytes(const qssb_calibration_t* cal, int32_t 
         return set_error(QSSB_ERR_UNSUPPORTED,
                          "qssb_loss_batch: scan size must be 64, 128, 256, 512 or 1024");
     const LossPlan pl = plan_loss(n, cal->n_bf, n_cand, flag_chunks(flags));
-    *bytes = pl.part_bytes + pl.var_bytes + pl.eq_bytes + pl.stage_bytes;
+    *bytes = loss_workspace(pl);
     return QSSB_OK;
 }
 
@@ -963,8 +979,8 @@ extern "C" int qssb_loss_full_workspace_bytes(const qssb_calibration_t* cal, int
     if (n != 64 && n != 128 && n != 256 && n != 512 && n != 1024)
         return set_error(QSSB_ERR_UNSUPPORTED,
                          "qssb_loss_batch_full: scan size must be 64, 128, 256, 512 or 1024");
-    const LossPlan pl = plan_loss(n, cal->n_bf, n_cand, flag_chunks(flags));
-    *bytes = pl.part_bytes + pl.var_bytes + full_stage_bytes(n, pl, n_cand);
+    const LossPlan pl = plan_loss(n, cal->n_bf, n_cand, flag_chunks(flags), true);
+    *bytes = loss_workspace(pl);
     return QSSB_OK;
 }
 

@@ -75,6 +75,12 @@ CONFIGS: dict[str, SyntheticSpec] = {
         scan_shape=(256, 256), detector_shape=(128, 128), det_sampling_mrad=20.0 / 24.0,
         C10=200.0,
     ),
+    # the reference's 512^2 timing shape (512 x 512 x 192 x 192 u16, ~8.9k BF
+    # pixels): a 53.3 px BF radius on the 192^2 detector
+    "large_512x512_det192": SyntheticSpec(
+        scan_shape=(512, 512), detector_shape=(192, 192), det_sampling_mrad=25.0 / 53.3,
+        semiangle_mrad=25.0, C10=100.0,
+    ),
 }
 
 
@@ -146,6 +152,10 @@ def object_phase_canvas(spec: SyntheticSpec, canvas: int, dx: float,
     return phase
 
 
+# Above this many detector samples the counts are drawn batch by batch.
+_WHOLE_ARRAY_LIMIT = 1 << 31
+
+
 def generate(spec: SyntheticSpec, device: torch.device | str = "cpu",
              batch: int = 1024) -> SyntheticData:
     """Generate uint16 counts I[R0, R1, K0, K1] for ``spec`` on ``device``."""
@@ -178,9 +188,8 @@ def generate(spec: SyntheticSpec, device: torch.device | str = "cpu",
     fr = pr - orr
     fc = pc - occ
     ar = torch.arange(k0, device=device)
-    intens = torch.empty((r0 * r1, k0, k1), device=device, dtype=torch.float32)
-    for s in range(0, r0 * r1, batch):
-        e = min(r0 * r1, s + batch)
+
+    def intensities(s: int, e: int) -> torch.Tensor:
         # Sub-pixel probe shift by a Fourier phase ramp, window at integer offset.
         ramp_r = torch.exp(-2j * math.pi * fr[s:e, None] * dx * kr[None, :])
         ramp_c = torch.exp(-2j * math.pi * fc[s:e, None] * dx * kc[None, :])
@@ -190,13 +199,33 @@ def generate(spec: SyntheticSpec, device: torch.device | str = "cpu",
         cols = occ[s:e, None, None] + ar[None, None, :]
         window = trans[rows, cols]
         psi = torch.fft.fftshift(torch.fft.fft2(probe * window), dim=(-2, -1))
-        intens[s:e] = (psi.abs() ** 2).to(torch.float32)
-    scale = spec.dose / intens.sum(dim=(1, 2)).mean()
-    intens *= scale
+        return (psi.abs() ** 2).to(torch.float32)
+
     gen = torch.Generator(device=device)
     gen.manual_seed(int(spec.seed) + 7919)
-    counts = torch.poisson(intens, generator=gen)
-    counts = torch.clamp(counts, max=65535).to(torch.int32).to(torch.uint16)
+    n_frames = r0 * r1
+    if n_frames * k0 * k1 <= _WHOLE_ARRAY_LIMIT:
+        intens = torch.empty((n_frames, k0, k1), device=device, dtype=torch.float32)
+        for s in range(0, n_frames, batch):
+            e = min(n_frames, s + batch)
+            intens[s:e] = intensities(s, e)
+        scale = spec.dose / intens.sum(dim=(1, 2)).mean()
+        intens *= scale
+        counts = torch.poisson(intens, generator=gen)
+        counts = torch.clamp(counts, max=65535).to(torch.int32).to(torch.uint16)
+    else:
+        # large acquisitions: two streaming passes (frame totals, then counts
+        # drawn batch by batch straight into the u16 array)
+        total = torch.zeros((), device=device, dtype=torch.float64)
+        for s in range(0, n_frames, batch):
+            total += intensities(s, min(n_frames, s + batch)).sum(dim=(1, 2), dtype=torch.float64).sum()
+        scale = spec.dose / (total / n_frames)
+        counts = torch.empty((n_frames, k0, k1), device=device, dtype=torch.uint16)
+        for s in range(0, n_frames, batch):
+            e = min(n_frames, s + batch)
+            lam_b = intensities(s, e) * scale.to(torch.float32)
+            c = torch.poisson(lam_b, generator=gen)
+            counts[s:e] = torch.clamp(c, max=65535).to(torch.int32).to(torch.uint16)
     counts = counts.reshape(r0, r1, k0, k1)
     return SyntheticData(counts=counts, spec=spec, object_phase=phi,
                          extra={"probe_pixel_A": dx, "canvas": canvas})
