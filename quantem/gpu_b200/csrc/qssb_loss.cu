@@ -349,13 +349,16 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
     for (int i = tid; i < N * N; i += 512) pq[i] = sq[(i >> 7) * kL128P + (i & 127)];
 }
 
+// Per pixel: fold the partial planes in FP64 (fixed order), write the mean
+// phase, and sum the variance over this block's 256 pixels (fixed tree):
+// block_var[cand][blockIdx.x]. N^2 is a multiple of 256 for every size.
 template <int N>
-__global__ void k_loss_reduce(const float* __restrict__ part, int n_chunks, int n_bf,
-                              double* __restrict__ var, float* __restrict__ mean_phase,
-                              int row_major) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;  // col * N + row, or row * N + col
+__global__ void __launch_bounds__(256) k_loss_reduce(const float* __restrict__ part, int n_chunks,
+                                                     int n_bf, double* __restrict__ block_var,
+                                                     float* __restrict__ mean_phase, int row_major) {
+    __shared__ double red[256];
+    const int j = blockIdx.x * 256 + threadIdx.x;  // col * N + row, or row * N + col
     const int cand = blockIdx.y;
-    if (j >= N * N) return;
     double s1 = 0.0, s2 = 0.0;
     for (int k = 0; k < n_chunks; ++k) {
         const float* base = part + ((size_t)(cand * n_chunks + k) * 2) * N * N;
@@ -364,21 +367,29 @@ __global__ void k_loss_reduce(const float* __restrict__ part, int n_chunks, int 
     }
     const double inv_b = 1.0 / (double)n_bf;
     const double mean = s1 * inv_b;
-    var[(size_t)cand * N * N + j] = s2 * inv_b - mean * mean;
+    red[threadIdx.x] = s2 * inv_b - mean * mean;
     if (mean_phase) {
         const int hi = j / N;
         const int lo = j - hi * N;
         mean_phase[(size_t)cand * N * N + (row_major ? j : lo * N + hi)] = (float)mean;
     }
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) block_var[(size_t)cand * (N * N / 256) + blockIdx.x] = red[0];
 }
 
-__global__ void __launch_bounds__(256) k_loss_final(const double* __restrict__ var, int npos,
+// L = (sum of the block sums, fixed order) / N^2.
+__global__ void __launch_bounds__(256) k_loss_final(const double* __restrict__ block_var,
+                                                    int n_blocks, int npos,
                                                     float* __restrict__ losses) {
     __shared__ double red[256];
     const int cand = blockIdx.x;
-    const double* v = var + (size_t)cand * npos;
+    const double* v = block_var + (size_t)cand * n_blocks;
     double acc = 0.0;
-    for (int i = threadIdx.x; i < npos; i += 256) acc += v[i];
+    for (int i = threadIdx.x; i < n_blocks; i += 256) acc += v[i];
     red[threadIdx.x] = acc;
     __syncthreads();
     for (int w = 128; w > 0; w >>= 1) {
@@ -421,7 +432,7 @@ struct TwoPass {
     // the warp FFT's transpose once the line is in registers
     static constexpr int pitch = (scratch > N ? scratch : N) | 1;
     static constexpr size_t row_smem = sizeof(float2) * ((size_t)rwarps * scratch + N);
-    static constexpr size_t col_smem = sizeof(float2) * ((size_t)tile * pitch + N);
+    static constexpr size_t col_smem = sizeof(float2) * ((size_t)2 * tile * pitch + N);
 };
 
 struct TwoPassPlan {
@@ -437,7 +448,8 @@ static TwoPassPlan plan_two_pass(int n, bool full, int n_bf, int n_cand, int chu
     if (c > n_bf) c = n_bf;
     tp.chunk_bf = (int)c;
     const int strips = n / col_tile(n);
-    int sub = chunks_req > 0 ? chunks_req : (296 + strips * n_cand - 1) / (strips * n_cand);
+    // whole waves of two CTAs per SM (148 SMs), not a last partial wave
+    int sub = chunks_req > 0 ? chunks_req : 296 / (strips * n_cand);
     if (sub < 1) sub = 1;
     if (sub > tp.chunk_bf) sub = tp.chunk_bf;
     tp.n_sub = sub;
@@ -512,46 +524,68 @@ __global__ void __launch_bounds__(32 * row_warps(N)) k_loss_rows(
     const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
     // G is read once per candidate: streaming loads keep the chunk's staged
     // rows in L2 for the column pass
-    auto eval = [&](int rr, int c, float2 e_row) -> float2 {
-        const float2 gv = c <= N / 2 ? __ldcs(gb + rr * H + c)
-                                     : cconj(__ldcs(gb + ((N - rr) & (N - 1)) * H + (N - c)));
+    auto load_g = [&](int rr, int c) -> float2 {
+        return c <= N / 2 ? __ldcs(gb + rr * H + c)
+                          : cconj(__ldcs(gb + ((N - rr) & (N - 1)) * H + (N - c)));
+    };
+    auto eval = [&](int rr, int c, float qx, float qy, float2 gv, float2 eq,
+                    float2 e_row) -> float2 {
         if constexpr (FULL) {
-            return corrected_full<CHI64>(__ldg(q_row + rr), __ldg(q_col + c), rr, c, kq.kx, kq.ky,
-                                         kq.kx_lo, kq.ky_lo, pk, gv, p, sf, sd);
+            return corrected_full<CHI64>(qx, qy, rr, c, kq.kx, kq.ky, kq.kx_lo, kq.ky_lo, pk, gv, p,
+                                         sf, sd);
         } else if constexpr (kSep) {
             const float2 lo = make_float2(kq.kx_lo, kq.ky_lo);
-            return corrected_quad_e(__ldg(q_row + rr), __ldg(q_col + c), rr, c,
-                                    __ldg(eqc + rr * N + c), kq.kx, kq.ky, kq.ak, &lo,
+            return corrected_quad_e(qx, qy, rr, c, eq, kq.kx, kq.ky, kq.ak, &lo,
                                     cmul(e_row, s_phc[c]), gv, p);
         } else if constexpr (QUAD) {
-            return corrected_quad<CHI64>(__ldg(q_row + rr), __ldg(q_col + c), rr, c,
-                                         __ldg(eqc + rr * N + c), kq, gv, p);
+            return corrected_quad<CHI64>(qx, qy, rr, c, eq, kq, gv, p);
         } else {
-            return corrected<CHI64>(__ldg(q_row + rr), __ldg(q_col + c), rr, c, kq.kx, kq.ky,
-                                    kq.kx_lo, kq.ky_lo, pk, gv, p);
+            return corrected<CHI64>(qx, qy, rr, c, kq.kx, kq.ky, kq.kx_lo, kq.ky_lo, pk, gv, p);
         }
     };
     const float2 e_row = kSep ? s_phr[warp] : make_float2(1.0f, 0.0f);
+    const float qx = __ldg(q_row + r);
     float2 v[RPL];
+    constexpr int kBatch = 8;  // loads of 8 elements issued before their math
 #pragma unroll
-    for (int t = 0; t < RPL; ++t) {
-        const int c = lane + 32 * t;
-        v[t] = (r == 0 && c == 0) ? dc : eval(r, c, e_row);
-        if (!FULL && t == N / 64 && lane == 0 && r >= 1 && r < N / 2) {  // c == N/2
-            float2 e_neg = make_float2(1.0f, 0.0f);
-            if constexpr (kSep) {
-                float sn, cs;
-                sincosf(2.0f * __ldg(q_row + N - r) * kq.u, &sn, &cs);
-                e_neg = make_float2(cs, sn);
+    for (int t0 = 0; t0 < RPL; t0 += kBatch) {
+        float2 gv[kBatch], eq[kBatch];
+        float qy[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int c = lane + 32 * (t0 + u);
+            gv[u] = load_g(r, c);
+            qy[u] = __ldg(q_col + c);
+            eq[u] = QUAD && !FULL ? __ldg(eqc + r * N + c) : make_float2(1.0f, 0.0f);
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int t = t0 + u;
+            const int c = lane + 32 * t;
+            v[t] = (r == 0 && c == 0) ? dc : eval(r, c, qx, qy[u], gv[u], eq[u], e_row);
+            if (!FULL && t == N / 64 && lane == 0 && r >= 1 && r < N / 2) {  // c == N/2
+                float2 e_neg = make_float2(1.0f, 0.0f);
+                if constexpr (kSep) {
+                    float sn, cs;
+                    sincosf(2.0f * __ldg(q_row + N - r) * kq.u, &sn, &cs);
+                    e_neg = make_float2(cs, sn);
+                }
+                const float2 eqn = QUAD && !FULL ? __ldg(eqc + (N - r) * N + N / 2) : make_float2(1.0f, 0.0f);
+                delta[((size_t)cand * nb_chunk + bi) * (N / 2) + r] =
+                    cadd(cconj(v[t]), eval(N - r, N / 2, __ldg(q_row + N - r), qy[u],
+                                           load_g(N - r, N / 2), eqn, e_neg));
             }
-            delta[((size_t)cand * nb_chunk + bi) * (N / 2) + r] =
-                cadd(cconj(v[t]), eval(N - r, N / 2, e_neg));
         }
     }
     warp_fft<N, +1>(v, scr + warp * TP::scratch, tw, lane);
     float2* out = stage + (((size_t)cand * nb_chunk + bi) * TP::rows + r) * N;
 #pragma unroll
     for (int j = 0; j < RPL; ++j) out[warp_fft_index<N>(lane, j)] = v[j];
+}
+
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
 }
 
 template <int N, bool FULL>
@@ -564,8 +598,8 @@ __global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
     constexpr int kColTile = TP::tile;
     constexpr int NT = 32 * kColTile;
     extern __shared__ float4 smem4[];
-    float2* tile = reinterpret_cast<float2*>(smem4);
-    float2* tw = tile + kColTile * P;
+    float2* tiles = reinterpret_cast<float2*>(smem4);  // two strips: the next one arrives by cp.async
+    float2* tw = tiles + 2 * kColTile * P;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -574,20 +608,28 @@ __global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
     const int cand = blockIdx.z;
     const int x = x0 + warp;
     const float sign = (x & 1) ? -1.0f : 1.0f;
-    float2* line = tile + warp * P;
     fill_twiddles<N>(tw, tid, NT);
-    float as[RPL], aq[RPL];
-#pragma unroll
-    for (int t = 0; t < RPL; ++t) as[t] = aq[t] = 0.0f;
-    for (int bi = sub; bi < nb_chunk; bi += n_sub) {
+    auto issue = [&](int bi, float2* dst) {
         const float2* S = stage + ((size_t)cand * nb_chunk + bi) * TP::rows * N + x0;
-        __syncthreads();  // the previous pixel's columns are done (and tw is filled)
         for (int e = tid; e < TP::rows * kColTile; e += NT) {
             const int rr = e / kColTile;
             const int c = e - rr * kColTile;
-            tile[c * P + rr] = __ldcs(S + (size_t)rr * N + c);
+            cp_async8(dst + c * P + rr, S + (size_t)rr * N + c);
         }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    float as[RPL], aq[RPL];
+#pragma unroll
+    for (int t = 0; t < RPL; ++t) as[t] = aq[t] = 0.0f;
+    int buf = 0;
+    if (sub < nb_chunk) issue(sub, tiles);
+    for (int bi = sub; bi < nb_chunk; bi += n_sub) {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        // this strip has arrived everywhere; every warp is done with the other
+        // buffer (and tw is filled)
         __syncthreads();
+        if (bi + n_sub < nb_chunk) issue(bi + n_sub, tiles + (buf ^ 1) * kColTile * P);
+        float2* line = tiles + buf * kColTile * P + warp * P;
         if constexpr (!FULL) {
             const float2* d = delta + ((size_t)cand * nb_chunk + bi) * (N / 2);
 #pragma unroll
@@ -612,7 +654,9 @@ __global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
             as[j] += ph;
             aq[j] = fmaf(ph, ph, aq[j]);
         }
+        buf ^= 1;
     }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
     float* ps = part + ((size_t)(cand * n_sub + sub) * 2) * N * N + (size_t)x * N;
     float* pq = ps + (size_t)N * N;
 #pragma unroll
@@ -687,6 +731,12 @@ static int launch_two_pass(const float* g_half, const float* geom, const float* 
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP::row_smem));
     CUDA_TRY(cudaFuncSetAttribute(k_loss_cols<N, FULL>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP::col_smem));
+    CUDA_TRY(cudaFuncSetAttribute(k_loss_rows<N, CHI64, QUAD, FULL>,
+                                  cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared));
+    CUDA_TRY(cudaFuncSetAttribute(k_loss_cols<N, FULL>,
+                                  cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared));
     const auto* g = reinterpret_cast<const float2*>(g_half);
     for (int b0 = 0; b0 < cal.n_bf; b0 += pl.chunk_bf) {
         const int nb = cal.n_bf - b0 < pl.chunk_bf ? cal.n_bf - b0 : pl.chunk_bf;
@@ -741,7 +791,7 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
     k_loss_reduce<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(part, pl.n_chunks, cal.n_bf,
                                                                        var, mean_phase, N == 128 ? 1 : 0);
     CUDA_TRY(cudaGetLastError());
-    k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N, losses);
+    k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N / 256, N * N, losses);
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -903,7 +953,7 @@ static int launch_loss_full(const float* g_half, const float* geom, const float*
     k_loss_reduce<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(part, pl.n_chunks, cal.n_bf,
                                                                        var, mean_phase, 0);
     CUDA_TRY(cudaGetLastError());
-    k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N, losses);
+    k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N / 256, N * N, losses);
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
