@@ -447,7 +447,10 @@ extern "C" int qssb_mean_dp_u64(const uint16_t* counts, int64_t n_frames, int32_
 // tiles with the next tile's box arriving by cp.async into a second buffer
 // while the current tile is written out. (DRAM fetches whole 128-byte lines,
 // so the box rows are read in full either way: ~12.5 KB per 128^2 frame.) A
-// box larger than the tile buffer falls back to direct element loads.
+// box larger than the tile buffer is taken in row bands (work item = frame
+// tile x band); with ascending BF indices (the selection's order) each band
+// writes only its own contiguous BF range. Boxes wider than one buffer fall
+// back to direct element loads.
 constexpr int kGbF = 8;
 constexpr int kGbThreads = 256;
 constexpr int kGbMaxPix = 3072;  // box pixels per frame held in one buffer
@@ -457,18 +460,25 @@ __device__ __forceinline__ void gb_cp_async16(void* smem_dst, const void* gmem_s
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
 }
 
+constexpr int kGbMaxBands = 64;
+
 __global__ void __launch_bounds__(kGbThreads) k_gather_bbox(
     const uint16_t* __restrict__ counts, long long n_frames, int det_rows, int det_cols,
     const int32_t* __restrict__ bf_linear, int n_bf, uint16_t* __restrict__ columns) {
     extern __shared__ uint4 smem_u4[];
-    uint16_t* tiles = reinterpret_cast<uint16_t*>(smem_u4);  // [2][kGbF][area]
+    uint16_t* tiles = reinterpret_cast<uint16_t*>(smem_u4);  // [2][kGbF][band area]
     __shared__ int s_box[4][kGbThreads / 32];
+    __shared__ int s_band_lo[kGbMaxBands + 1];
+    __shared__ int s_unsorted;
     const int tid = threadIdx.x;
     const int lane = tid & 31, warp = tid >> 5;
     const int npix = det_rows * det_cols;
     int rmin = det_rows, rmax = -1, cmin = det_cols, cmax = -1;
+    if (tid == 0) s_unsorted = 0;
+    __syncthreads();
     for (int b = tid; b < n_bf; b += kGbThreads) {
         const int lin = __ldg(bf_linear + b);
+        if (b + 1 < n_bf && __ldg(bf_linear + b + 1) <= lin) s_unsorted = 1;
         if (lin < 0 || lin >= npix) continue;
         const int r = lin / det_cols, c = lin - (lin / det_cols) * det_cols;
         rmin = min(rmin, r); rmax = max(rmax, r); cmin = min(cmin, c); cmax = max(cmax, c);
@@ -494,8 +504,10 @@ __global__ void __launch_bounds__(kGbThreads) k_gather_bbox(
     const int c0 = cmin & ~7;
     const int width = rmax >= 0 ? ((cmax + 8) & ~7) - c0 : 0;   // multiple of 8 pixels
     const int nr = rmax >= 0 ? rmax - rmin + 1 : 0;
-    const int area = nr * width;
-    if (area == 0 || area > kGbMaxPix) {
+    // row bands of at most kGbMaxPix box pixels
+    const int band_rows = width > 0 ? min(nr, kGbMaxPix / width) : 0;
+    const int n_bands = band_rows > 0 ? (nr + band_rows - 1) / band_rows : 0;
+    if (width == 0 || band_rows == 0 || n_bands > kGbMaxBands) {
         // direct path: one element per (frame, BF pixel)
         for (long long t = blockIdx.x; t < n_tiles; t += gridDim.x) {
             const long long f0 = t * kGbF;
@@ -510,9 +522,31 @@ __global__ void __launch_bounds__(kGbThreads) k_gather_bbox(
         }
         return;
     }
+    // BF range of each band when bf_linear is ascending (the selection's
+    // row-major order): s_band_lo[k] = #{b : lin(b) < first pixel of band k}
+    const bool sorted = s_unsorted == 0;
+    if (sorted) {
+        for (int k = tid; k <= n_bands; k += kGbThreads) {
+            const int row = rmin + k * band_rows;
+            const int key = row > rmax ? 0x7fffffff : row * det_cols;
+            int lo = 0, hi = n_bf;  // first b with lin(b) >= key
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (__ldg(bf_linear + mid) < key) lo = mid + 1; else hi = mid;
+            }
+            s_band_lo[k] = lo;
+        }
+    }
+    __syncthreads();
     const int vpr = width / 8;
-    const int per_frame = nr * vpr;
-    auto stage = [&](long long t, uint16_t* dst) {
+    const long long n_items = n_tiles * n_bands;
+    auto stage = [&](long long item, uint16_t* dst) {
+        const long long t = item / n_bands;
+        const int k = (int)(item - t * n_bands);
+        const int r0 = rmin + k * band_rows;
+        const int rows = min(band_rows, rmax + 1 - r0);
+        const int per_frame = rows * vpr;
+        const int area = rows * width;
         const long long f0 = t * kGbF;
         const int nf = (int)min((long long)kGbF, n_frames - f0);
         for (int e = tid; e < nf * per_frame; e += kGbThreads) {
@@ -521,35 +555,48 @@ __global__ void __launch_bounds__(kGbThreads) k_gather_bbox(
             const int i = rem / vpr;
             const int v = rem - i * vpr;
             const uint4* src = reinterpret_cast<const uint4*>(
-                counts + (size_t)(f0 + f) * npix + (size_t)(rmin + i) * det_cols + c0) + v;
+                counts + (size_t)(f0 + f) * npix + (size_t)(r0 + i) * det_cols + c0) + v;
             gb_cp_async16(reinterpret_cast<uint4*>(dst + (size_t)f * area + i * width) + v, src);
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
     const bool vec_out = (n_frames & 7) == 0;
     int buf = 0;
-    if (blockIdx.x < n_tiles) stage(blockIdx.x, tiles);
-    for (long long t = blockIdx.x; t < n_tiles; t += gridDim.x) {
+    if (blockIdx.x < n_items) stage(blockIdx.x, tiles);
+    for (long long item = blockIdx.x; item < n_items; item += gridDim.x) {
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        __syncthreads();  // tile t is in; everyone is done with the other buffer
-        const long long tn = t + gridDim.x;
-        if (tn < n_tiles) stage(tn, tiles + (size_t)(buf ^ 1) * kGbF * kGbMaxPix);
+        __syncthreads();  // this item is in; everyone is done with the other buffer
+        const long long nxt = item + gridDim.x;
+        if (nxt < n_items) stage(nxt, tiles + (size_t)(buf ^ 1) * kGbF * kGbMaxPix);
         const uint16_t* tile = tiles + (size_t)buf * kGbF * kGbMaxPix;
+        const long long t = item / n_bands;
+        const int k = (int)(item - t * n_bands);
+        const int r0 = rmin + k * band_rows;
+        const int rows = min(band_rows, rmax + 1 - r0);
+        const int area = rows * width;
         const long long f0 = t * kGbF;
         const int nf = (int)min((long long)kGbF, n_frames - f0);
-        for (int b = tid; b < n_bf; b += kGbThreads) {
+        // sorted: the bands' BF ranges partition [0, n_bf) (out-of-detector
+        // entries sit at the ends and go to the first / last band); unsorted:
+        // every band scans all pixels and band 0 zero-fills invalid ones
+        const int b_lo = sorted && k > 0 ? s_band_lo[k] : 0;
+        const int b_hi = sorted && k + 1 < n_bands ? s_band_lo[k + 1] : n_bf;
+        const bool owns_invalid = sorted || k == 0;
+        for (int b = b_lo + tid; b < b_hi; b += kGbThreads) {
             const int lin = __ldg(bf_linear + b);
-            const bool ok = lin >= 0 && lin < npix;
-            const int r = ok ? lin / det_cols : rmin;
+            const bool valid = lin >= 0 && lin < npix;
+            const int r = valid ? lin / det_cols : -1;
+            if (valid ? (r < r0 || r >= r0 + rows) : !owns_invalid) continue;
+            const bool ok = valid;
             const int c = ok ? lin - r * det_cols : c0;
-            const int pos = (r - rmin) * width + (c - c0);
+            const int pos = ok ? (r - r0) * width + (c - c0) : 0;
             uint16_t* dst = columns + (size_t)b * n_frames + f0;
             if (vec_out && nf == kGbF) {
                 uint32_t w[4];
 #pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    w[k] = ok ? ((uint32_t)tile[(2 * k) * area + pos] |
-                                 ((uint32_t)tile[(2 * k + 1) * area + pos] << 16)) : 0u;
+                for (int q = 0; q < 4; ++q)
+                    w[q] = ok ? ((uint32_t)tile[(2 * q) * area + pos] |
+                                 ((uint32_t)tile[(2 * q + 1) * area + pos] << 16)) : 0u;
                 *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
             } else {
                 for (int f = 0; f < nf; ++f) dst[f] = ok ? tile[f * area + pos] : (uint16_t)0;
@@ -558,6 +605,142 @@ __global__ void __launch_bounds__(kGbThreads) k_gather_bbox(
         buf ^= 1;
     }
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// 64-frame tiles for outputs that do not stay in L2 (512^2 scans and up): a
+// work item is (64 frames, a row band of the bounding box). Lane pairs read a
+// 32-byte box segment of one frame (16 frames per warp load) and scatter the
+// pixels into a pixel-major shared tile (pitch 72 frames = 144 bytes, 16-byte
+// aligned rows); each BF column then receives its 64 frames as one 128-byte
+// line written by 8 lanes. Needs n_frames % 8 == 0 and 16-byte aligned rows.
+constexpr int kT64F = 64;
+constexpr int kT64P = 72;       // frames per smem pixel row (64 + 8)
+constexpr int kT64MaxPix = 704;  // band pixels per item: 704 x 144 B = 99 KB
+
+__global__ void __launch_bounds__(kGbThreads) k_gather_t64(
+    const uint16_t* __restrict__ counts, long long n_frames, int det_rows, int det_cols,
+    const int32_t* __restrict__ bf_linear, int n_bf, uint16_t* __restrict__ columns) {
+    extern __shared__ uint4 smem_u4[];
+    uint16_t* tile = reinterpret_cast<uint16_t*>(smem_u4);  // [band pixel][kT64P]
+    __shared__ int s_box[4][kGbThreads / 32];
+    __shared__ int s_band_lo[kGbMaxBands + 1];
+    __shared__ int s_unsorted;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int npix = det_rows * det_cols;
+    if (tid == 0) s_unsorted = 0;
+    __syncthreads();
+    int rmin = det_rows, rmax = -1, cmin = det_cols, cmax = -1;
+    for (int b = tid; b < n_bf; b += kGbThreads) {
+        const int lin = __ldg(bf_linear + b);
+        if (b + 1 < n_bf && __ldg(bf_linear + b + 1) <= lin) s_unsorted = 1;
+        if (lin < 0 || lin >= npix) continue;
+        const int r = lin / det_cols, c = lin - (lin / det_cols) * det_cols;
+        rmin = min(rmin, r); rmax = max(rmax, r); cmin = min(cmin, c); cmax = max(cmax, c);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        rmin = min(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+        rmax = max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+        cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
+        cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+    }
+    if (lane == 0) {
+        s_box[0][warp] = rmin; s_box[1][warp] = rmax; s_box[2][warp] = cmin; s_box[3][warp] = cmax;
+    }
+    __syncthreads();
+    rmin = det_rows; rmax = -1; cmin = det_cols; cmax = -1;
+#pragma unroll
+    for (int w = 0; w < kGbThreads / 32; ++w) {
+        rmin = min(rmin, s_box[0][w]); rmax = max(rmax, s_box[1][w]);
+        cmin = min(cmin, s_box[2][w]); cmax = max(cmax, s_box[3][w]);
+    }
+    const int c0 = cmin & ~15;
+    // multiple of 16 pixels (32-byte segments), inside the detector row
+    const int width = rmax >= 0 ? min(((cmax + 16) & ~15), det_cols) - c0 : 0;
+    const int nr = rmax >= 0 ? rmax - rmin + 1 : 0;
+    const int band_rows = width > 0 ? min(nr, kT64MaxPix / width) : 0;
+    const int n_bands = band_rows > 0 ? (nr + band_rows - 1) / band_rows : 0;
+    const long long n_tiles = (n_frames + kT64F - 1) / kT64F;
+    if (width == 0 || (width & 15) || band_rows == 0 || n_bands > kGbMaxBands) {
+        for (long long t = blockIdx.x; t < n_tiles; t += gridDim.x) {  // direct path
+            const long long f0 = t * kT64F;
+            const int nf = (int)min((long long)kT64F, n_frames - f0);
+            for (int e = tid; e < nf * n_bf; e += kGbThreads) {
+                const int f = e / n_bf, b = e - (e / n_bf) * n_bf;
+                const int lin = __ldg(bf_linear + b);
+                const bool ok = lin >= 0 && lin < npix;
+                columns[(size_t)b * n_frames + f0 + f] =
+                    ok ? __ldcs(counts + (size_t)(f0 + f) * npix + lin) : (uint16_t)0;
+            }
+        }
+        return;
+    }
+    const bool sorted = s_unsorted == 0;
+    if (sorted) {
+        for (int k = tid; k <= n_bands; k += kGbThreads) {
+            const int row = rmin + k * band_rows;
+            const int key = row > rmax ? 0x7fffffff : row * det_cols;
+            int lo = 0, hi = n_bf;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (__ldg(bf_linear + mid) < key) lo = mid + 1; else hi = mid;
+            }
+            s_band_lo[k] = lo;
+        }
+    }
+    __syncthreads();
+    const int segs_per_row = width / 16;
+    const long long n_items = n_tiles * n_bands;
+    const int grp = tid >> 3;  // write phase: 32 groups of 8 lanes, one BF column each
+    const int sub = tid & 7;
+    for (long long item = blockIdx.x; item < n_items; item += gridDim.x) {
+        const long long t = item / n_bands;
+        const int k = (int)(item - t * n_bands);
+        const int r0 = rmin + k * band_rows;
+        const int rows = min(band_rows, rmax + 1 - r0);
+        const long long f0 = t * kT64F;
+        const int nf = (int)min((long long)kT64F, n_frames - f0);
+        // load: e -> lane pair q = e / 2 (one 32-byte segment), half h
+        const int n_e = 2 * kT64F * rows * segs_per_row;
+#pragma unroll 4
+        for (int e = tid; e < n_e; e += kGbThreads) {
+            const int h = e & 1;
+            const int q = e >> 1;
+            const int f = q & (kT64F - 1);
+            const int seg = q >> 6;
+            const int i = seg / segs_per_row;
+            const int sg = seg - i * segs_per_row;
+            const int px = i * width + 16 * sg + 8 * h;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (f < nf)
+                v = __ldcs(reinterpret_cast<const uint4*>(
+                    counts + (size_t)(f0 + f) * npix + (size_t)(r0 + i) * det_cols + c0 + 16 * sg + 8 * h));
+            uint16_t* d = tile + (size_t)px * kT64P + f;
+            d[0 * kT64P] = (uint16_t)(v.x & 0xffffu); d[1 * kT64P] = (uint16_t)(v.x >> 16);
+            d[2 * kT64P] = (uint16_t)(v.y & 0xffffu); d[3 * kT64P] = (uint16_t)(v.y >> 16);
+            d[4 * kT64P] = (uint16_t)(v.z & 0xffffu); d[5 * kT64P] = (uint16_t)(v.z >> 16);
+            d[6 * kT64P] = (uint16_t)(v.w & 0xffffu); d[7 * kT64P] = (uint16_t)(v.w >> 16);
+        }
+        __syncthreads();
+        const int b_lo = sorted && k > 0 ? s_band_lo[k] : 0;
+        const int b_hi = sorted && k + 1 < n_bands ? s_band_lo[k + 1] : n_bf;
+        const bool owns_invalid = sorted || k == 0;
+        for (int b = b_lo + grp; b < b_hi; b += kGbThreads / 8) {
+            const int lin = __ldg(bf_linear + b);
+            const bool valid = lin >= 0 && lin < npix;
+            const int r = valid ? lin / det_cols : -1;
+            if (valid ? (r < r0 || r >= r0 + rows) : !owns_invalid) continue;
+            if (8 * sub >= nf) continue;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (valid) {
+                const int pos = (r - r0) * width + (lin - r * det_cols - c0);
+                v = *reinterpret_cast<const uint4*>(tile + (size_t)pos * kT64P + 8 * sub);
+            }
+            *reinterpret_cast<uint4*>(columns + (size_t)b * n_frames + f0 + 8 * sub) = v;
+        }
+        __syncthreads();  // the tile is rewritten by the next item
+    }
 }
 
 extern "C" int qssb_gather_bf_columns(const uint16_t* counts, int64_t n_frames, int32_t det_pixels,
@@ -591,6 +774,18 @@ extern "C" int qssb_gather_bf_columns_2d(const uint16_t* counts, int64_t n_frame
     if (!vec_ok)  // rows not 16-byte aligned: the tile gather
         return qssb_gather_bf_columns(counts, n_frames, det_rows * det_cols, bf_linear, n_bf,
                                       columns, stream);
+    if ((n_frames & 7) == 0 && (int64_t)n_frames * n_bf * 2 > ((int64_t)64 << 20)) {
+        // output larger than L2 can merge: full 128-byte column lines
+        const long long n_tiles64 = (n_frames + kT64F - 1) / kT64F;
+        long long gx = 2LL * device_sm_count();
+        if (gx > n_tiles64) gx = n_tiles64;
+        const int smem = (int)(sizeof(uint16_t) * kT64P * kT64MaxPix);
+        CUDA_TRY(cudaFuncSetAttribute(k_gather_t64, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+        k_gather_t64<<<(unsigned)gx, kGbThreads, smem, (cudaStream_t)stream>>>(
+            counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns);
+        CUDA_TRY(cudaGetLastError());
+        return QSSB_OK;
+    }
     const long long n_tiles = (n_frames + kGbF - 1) / kGbF;
     long long gx = 2LL * device_sm_count();
     if (gx > n_tiles) gx = n_tiles;

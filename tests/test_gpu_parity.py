@@ -193,25 +193,32 @@ def test_gather_is_bit_exact(n_frames, npix, n_bf):
     np.testing.assert_array_equal(cols.cpu().numpy(), data[:, lin].T)
 
 
-@pytest.mark.parametrize("n_frames,det,radius", [(16384, 128, 24.0), (1000, 64, 12.0),
-                                                 (77, 128, 40.0), (4096, 96, 70.0)])
-def test_bbox_gather_is_bit_exact(n_frames, det, radius):
+@pytest.mark.parametrize("n_frames,det,radius,shuffle", [
+    (16384, 128, 24.0, False), (1000, 64, 12.0, False), (77, 128, 40.0, False),
+    (4096, 96, 70.0, False), (4099, 192, 53.3, False), (2048, 192, 53.3, True),
+    (515, 96, 70.0, True), (8200, 192, 53.3, False), (8192, 192, 53.3, True)])
+def test_bbox_gather_is_bit_exact(n_frames, det, radius, shuffle):
     """The bounding-box gather (qssb_gather_bf_columns_2d) on disk-shaped BF
-    sets: full and ragged frame tiles, a box too large for the shared tile."""
+    sets: full and ragged frame tiles, boxes larger than the shared tile (row
+    bands; the 192^2 detector with a 53 px disk is the 512^2 workload's), BF
+    orders that are not ascending, and outputs above 64 MB (the 64-frame
+    transposed tiles)."""
     rng = np.random.default_rng(n_frames + det)
     counts = rng.integers(0, 65536, size=(n_frames, det, det), dtype=np.uint16)
     rr, cc = np.meshgrid(np.arange(det), np.arange(det), indexing="ij")
     disk = (rr - det / 2 + 0.3) ** 2 + (cc - det / 2 - 0.2) ** 2 <= radius ** 2
     lin = np.nonzero(disk.reshape(-1))[0].astype(np.int32)
+    if shuffle:
+        lin = rng.permutation(lin).astype(np.int32)
     cols = ops.gather_bf_columns(_dev(counts), _dev(lin)).cpu().numpy()
     np.testing.assert_array_equal(cols, counts.reshape(n_frames, -1)[:, lin].T)
 
 
 # -------------------------------------------------------------- scan FFT
-@pytest.mark.parametrize("n", [64, 128, 256])
+@pytest.mark.parametrize("n", [64, 128, 256, 512, 1024])
 def test_scan_fft_half_matches_fp64(n):
     rng = np.random.default_rng(n)
-    top = 4000 if n <= 128 else 256  # keeps every image sum below 2^24
+    top = {64: 4000, 128: 4000, 256: 256, 512: 64, 1024: 16}[n]  # every image sum below 2^24
     images = rng.integers(0, top, size=(9, n, n), dtype=np.uint16)
     g = ops.scan_fft_half(_dev(images.reshape(9, n * n)), (n, n)).cpu().numpy()
     ref = np.fft.rfft2(images.astype(np.float64))
