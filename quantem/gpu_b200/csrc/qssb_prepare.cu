@@ -801,27 +801,36 @@ extern "C" int qssb_gather_bf_columns_2d(const uint16_t* counts, int64_t n_frame
 // The half plane (264 KB per BF image at 256^2) does not fit one CTA's
 // shared memory, so the transform is two passes through G itself:
 //   k_scan_rows<N>: rows 2j, 2j+1 of a BF image as one complex line (one warp
-//     per pair), forward FFT, split into the two real rows' spectra
+//     per pair), forward warp FFT, split into the two real rows' spectra
 //     X_2j(c) = (Z(c) + conj Z(-c)) / 2, X_2j+1(c) = (Z(c) - conj Z(-c)) / 2i,
 //     c = 0..N/2, written to G[b][row][c];
-//   k_scan_cols<N>: T columns of G[b] staged in shared memory (pitch N+1:
-//     the T columns of one row land on distinct banks), forward FFT of each
-//     column along the rows, written back in place.
+//   k_scan_cols<N>: T columns of G[b] staged in shared memory (odd pitch:
+//     the T columns of one row land on distinct banks), forward warp FFT of
+//     each column along the rows, written back in place.
 template <int N>
 struct ScanLines {
     static constexpr int H = N / 2 + 1;
     static constexpr int kWarps = N >= 1024 ? 4 : 8;       // row pairs per block
     static constexpr int kTile = N >= 1024 ? 8 : 16;       // columns per block
-    static constexpr size_t cols_smem = sizeof(float2) * ((size_t)kTile * (N + 1) + N);
+    static constexpr int kScratch = warp_fft_scratch<N>();  // >= N: also holds a line
+    static constexpr int P = kScratch | 1;                  // column pitch, odd mod 16
+    static constexpr size_t rows_smem = sizeof(float2) * ((size_t)kWarps * kScratch + N);
+    static constexpr size_t cols_smem = sizeof(float2) * ((size_t)kTile * P + N);
 };
 
+// Rows: one warp per row pair, the line straight into registers
+// (v[t] = x[32 t + lane]), warp FFT, spectrum back to the warp's shared line
+// in natural order for the real-pair split.
 template <int N>
 __global__ void __launch_bounds__(32 * ScanLines<N>::kWarps) k_scan_rows(
     const uint16_t* __restrict__ columns, int n_bf, float2* __restrict__ g_half) {
-    constexpr int W = ScanLines<N>::kWarps;
-    constexpr int H = ScanLines<N>::H;
-    __shared__ float2 tw[N];
-    __shared__ float2 line[W][N];
+    using L = ScanLines<N>;
+    constexpr int W = L::kWarps;
+    constexpr int H = L::H;
+    constexpr int RPL = N / 32;
+    extern __shared__ float4 scan_rows_smem[];
+    float2* scr = reinterpret_cast<float2*>(scan_rows_smem);
+    float2* tw = scr + W * L::kScratch;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -833,10 +842,15 @@ __global__ void __launch_bounds__(32 * ScanLines<N>::kWarps) k_scan_rows(
     const uint16_t* img = columns + (size_t)b * N * N;
     const uint16_t* r0 = img + (size_t)(2 * pair) * N;
     const uint16_t* r1 = r0 + N;
-    float2* x = line[warp];
-    for (int i = lane; i < N; i += 32) x[i] = make_float2((float)__ldg(r0 + i), (float)__ldg(r1 + i));
+    float2 v[RPL];
+#pragma unroll
+    for (int t = 0; t < RPL; ++t)
+        v[t] = make_float2((float)__ldcs(r0 + 32 * t + lane), (float)__ldcs(r1 + 32 * t + lane));
+    float2* x = scr + warp * L::kScratch;
+    warp_fft<N, -1>(v, x, tw, lane);
+#pragma unroll
+    for (int j = 0; j < RPL; ++j) x[warp_fft_index<N>(lane, j)] = v[j];
     __syncwarp();
-    line_fft<N, -1>(x, 1, tw, lane);
     float2* g0 = g_half + ((size_t)b * N + 2 * pair) * H;
     float2* g1 = g0 + H;
     for (int c = lane; c < H; c += 32) {
@@ -847,11 +861,15 @@ __global__ void __launch_bounds__(32 * ScanLines<N>::kWarps) k_scan_rows(
     }
 }
 
+// Columns: T columns of G[b] staged in shared memory, one warp FFT per
+// column (the column's own line is the transpose scratch), written back.
 template <int N>
 __global__ void __launch_bounds__(256) k_scan_cols(int n_bf, float2* __restrict__ g_half) {
-    constexpr int P = N + 1;
-    constexpr int T = ScanLines<N>::kTile;
-    constexpr int H = ScanLines<N>::H;
+    using L = ScanLines<N>;
+    constexpr int P = L::P;
+    constexpr int T = L::kTile;
+    constexpr int H = L::H;
+    constexpr int RPL = N / 32;
     extern __shared__ float2 scan_cols_smem[];
     float2* tile = scan_cols_smem;
     float2* tw = tile + T * P;
@@ -870,7 +888,17 @@ __global__ void __launch_bounds__(256) k_scan_cols(int n_bf, float2* __restrict_
         if (c < nc) tile[c * P + r] = g[(size_t)r * H + c0 + c];
     }
     __syncthreads();
-    for (int c = warp; c < nc; c += 8) line_fft<N, -1>(tile + c * P, 1, tw, lane);
+    for (int c = warp; c < nc; c += 8) {
+        float2* line = tile + c * P;
+        float2 v[RPL];
+#pragma unroll
+        for (int t = 0; t < RPL; ++t) v[t] = line[lane + 32 * t];
+        __syncwarp();
+        warp_fft<N, -1>(v, line, tw, lane);
+#pragma unroll
+        for (int j = 0; j < RPL; ++j) line[warp_fft_index<N>(lane, j)] = v[j];
+        __syncwarp();
+    }
     __syncthreads();
     for (int e = tid; e < N * T; e += 256) {
         const int r = e / T;
@@ -883,8 +911,10 @@ template <int N>
 static int launch_scan_lines(const uint16_t* columns, int n_bf, float* g_half, cudaStream_t s) {
     using L = ScanLines<N>;
     auto* g = reinterpret_cast<float2*>(g_half);
-    k_scan_rows<N><<<dim3(n_bf, (N / 2 + L::kWarps - 1) / L::kWarps), 32 * L::kWarps, 0, s>>>(
-        columns, n_bf, g);
+    CUDA_TRY(cudaFuncSetAttribute(k_scan_rows<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)L::rows_smem));
+    k_scan_rows<N><<<dim3(n_bf, (N / 2 + L::kWarps - 1) / L::kWarps), 32 * L::kWarps,
+                     L::rows_smem, s>>>(columns, n_bf, g);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaFuncSetAttribute(k_scan_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)L::cols_smem));
