@@ -712,7 +712,7 @@ def run_b200(args, world, rank, local) -> None:
     print(json.dumps(line), flush=True)
 
 
-def run_profile_once(local: int, with_256: bool = False) -> None:
+def run_profile_once(local: int, with_256: bool = False, with_512: str | None = None) -> None:
     """One cold reconstruction, one warm object, one loss and one 64-candidate
     loss batch on the 128^4 workload, untimed: the launch sequence the ncu
     summaries under profiles/ are captured from."""
@@ -735,6 +735,24 @@ def run_profile_once(local: int, with_256: bool = False) -> None:
         be = B200SSBBackend(c256, device=dev, **KW)
         out["loss256"] = float(be.variance_loss_batch([spec.C10], [0.0], [0.0])[0])
         torch.cuda.synchronize(dev)
+    if with_512:
+        # "full": the 512^2 x 192^2 timing shape (19.3 GB); "small": 512^2 x 48^2
+        # (1.2 GB, ~440 BF) for multi-pass captures of the same kernels
+        from dataclasses import replace
+
+        del be
+        torch.cuda.empty_cache()
+        spec = CONFIGS["large_512x512_det192"]
+        if with_512 == "small":
+            spec = replace(spec, detector_shape=(48, 48), det_sampling_mrad=spec.semiangle_mrad / 20.0)
+        c512 = generate(spec, device=dev).counts
+        kw = dict(semiangle=spec.semiangle_mrad, scan_sampling=spec.scan_step_A,
+                  det_sampling=spec.det_sampling_mrad, voltage_kV=spec.voltage_kV)
+        be = B200SSBBackend(c512, device=dev, **kw)
+        be.object_and_phase(spec.C10, 0.0, 0.0)
+        _, out["loss512"] = be.reconstruct_with_loss(spec.C10, 0.0, 0.0)
+        out["n_bf512"] = be.num_bf
+        torch.cuda.synchronize(dev)
     print(json.dumps(out))
 
 
@@ -748,6 +766,8 @@ def main() -> None:
     ap.add_argument("--no-oracle", action="store_true")
     ap.add_argument("--with-256", action="store_true",
                     help="--profile-once: also one 256^2 scan loss evaluation")
+    ap.add_argument("--with-512", choices=["full", "small"], default=None,
+                    help="--profile-once: also one 512^2 cold preparation, object and loss")
     ap.add_argument("--no-large", action="store_true",
                     help="skip the 512^2 x 192^2 (19.3 GB) leg")
     ap.add_argument("--no-stress", action="store_true",
@@ -760,7 +780,7 @@ def main() -> None:
     world, rank, local = _dist()
     try:
         if args.profile_once:
-            run_profile_once(local, args.with_256)
+            run_profile_once(local, args.with_256, args.with_512)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         else:
