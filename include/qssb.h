@@ -54,7 +54,7 @@ extern "C" {
  * aperture evaluation at near-tied overlaps uses them as given. */
 typedef struct qssb_calibration {
     int32_t n_bf;                 /* selected BF pixels (B), >= 1 */
-    int32_t scan_rows;            /* R0: 64, 128 or 256 */
+    int32_t scan_rows;            /* R0: 64, 128, 256, 512 or 1024 */
     int32_t scan_cols;            /* R1: == scan_rows */
     int32_t reserved;             /* must be 0 */
     double wavelength_A;
@@ -264,6 +264,32 @@ int qssb_loss_batch_full(const float* g_half, const float* bf_geom, const float*
                          const qssb_full_aberrations_t* candidates, int32_t n_cand,
                          int32_t flags, void* workspace, size_t workspace_bytes,
                          float* losses, float* mean_phase, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Time series of object waves (ssb/temporal.py:77-257): drift correction by
+ * a Fourier phase ramp and the (phase-referenced) weighted complex mean.
+ *
+ * qssb_fourier_shift: out[t] = ifft2(fft2(in[t]) exp(-2 pi i (f_r s_r + f_c s_c))),
+ * f = fftfreq(n, 1), shifts [t] = (s_r, s_c) in pixels (fourier_shift_2d,
+ * temporal.py:77-107). in, out: device complex64 [n_frames][rows][cols]
+ * (may alias); shifts: device float32 [n_frames][2]; rows, cols powers of two
+ * in 64..1024. */
+int qssb_fourier_shift(const float* in, float* out, int32_t n_frames, int32_t rows,
+                       int32_t cols, const float* shifts, void* stream);
+
+/* Workspace bytes of qssb_join_object_waves with phase_reference = 1. */
+int qssb_join_workspace_bytes(int32_t n_frames, size_t* bytes);
+
+/* joined = sum_t w_t r_t frames[t] (join_object_waves, temporal.py:192-257):
+ * weights device float32 [n_frames], already normalised to sum 1
+ * (temporal.py:127-140); phase_reference 1 ("first"): r_t =
+ * exp(-i angle(sum_p frames[t] conj frames[0])) for t > 0, the overlap summed
+ * in FP64 in a fixed order (temporal.py:154-180); 0 ("none"): r_t = 1.
+ * write_back != 0 stores r_t frames[t] over frames (the aligned stack).
+ * frames: device complex64 [n_frames][n_pix]; joined: complex64 [n_pix]. */
+int qssb_join_object_waves(float* frames, const float* weights, int32_t n_frames, int64_t n_pix,
+                           int32_t phase_reference, void* workspace, size_t workspace_bytes,
+                           float* joined, int32_t write_back, void* stream);
 
 /* ------------------------------------------------------------------------
  * Learned aberration proposer (no counterpart in the reference, which has no

@@ -27,6 +27,8 @@ LAUNCHES_PER_CALL = {
     "qssb_object_ex": 4,
     "qssb_loss_batch": 3,
     "qssb_loss_batch_full": 3,
+    "qssb_fourier_shift": 3,
+    "qssb_join_object_waves": 1,
 }
 LAUNCH_COUNT = 0
 _PROFILE: list | None = None
@@ -376,3 +378,40 @@ def loss_batch(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
           _ptr(q_col), ctypes.byref(cal), _ptr(candidates), n, int(flags), _ptr(buf), buf.numel(),
           _ptr(losses), _ptr(mp), _stream(g_half))
     return losses, mp
+
+
+# ------------------------------------------------------------ time series
+def fourier_shift(frames: torch.Tensor, shifts: torch.Tensor, out: torch.Tensor | None = None
+                  ) -> torch.Tensor:
+    """Fourier-ramp shift of every frame (complex64 CUDA [T, R, C], shifts
+    float32 CUDA [T, 2] in pixels); R and C powers of two in 64..1024."""
+    _require_cuda(frames, "frames", torch.complex64)
+    _require_cuda(shifts, "shifts", torch.float32)
+    if frames.ndim != 3 or tuple(shifts.shape) != (frames.shape[0], 2):
+        raise ValueError("frames must be (T, R, C) and shifts (T, 2)")
+    t, r, c = (int(x) for x in frames.shape)
+    if out is None:
+        out = torch.empty_like(frames)
+    _call("qssb_fourier_shift", frames.device, _ptr(frames), _ptr(out), t, r, c, _ptr(shifts),
+          _stream(frames))
+    return out
+
+
+def join_frames(frames: torch.Tensor, weights: torch.Tensor, *, phase_reference: int,
+                write_back: bool, workspace: Workspace | None = None) -> torch.Tensor:
+    """Weighted complex mean of frames (complex64 CUDA [T, ...]) with optional
+    global-phase referencing to frame 0; weights float32 CUDA [T], summing to 1."""
+    _require_cuda(frames, "frames", torch.complex64)
+    _require_cuda(weights, "weights", torch.float32)
+    t = int(frames.shape[0])
+    n_pix = frames[0].numel()
+    joined = torch.empty(frames.shape[1:], dtype=torch.complex64, device=frames.device)
+    buf = None
+    if phase_reference:
+        n = ctypes.c_size_t(0)
+        check(_lib.load().qssb_join_workspace_bytes(t, ctypes.byref(n)))
+        buf = (workspace or Workspace(frames.device)).get(int(n.value))
+    _call("qssb_join_object_waves", frames.device, _ptr(frames), _ptr(weights), t, n_pix,
+          int(phase_reference), _ptr(buf), 0 if buf is None else buf.numel(), _ptr(joined),
+          1 if write_back else 0, _stream(frames))
+    return joined
