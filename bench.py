@@ -331,6 +331,48 @@ def large_512(dev: torch.device, steps: int = 5) -> dict:
     return out
 
 
+def temporal_join(dev: torch.device, steps: int = 10) -> dict:
+    """Time-series join (temporal.py's join_object_waves): T complex64 object
+    waves of N^2, subpixel drift correction by a Fourier ramp, phase reference
+    to frame 0, weighted mean; device-resident stack. Algorithmic bytes per
+    frame: three read+write passes of the shift (48 B/pixel) and the join's
+    overlap and mean reads (16 B/pixel) plus the aligned write-back (8 B)."""
+    from oracle import temporal_oracle as to
+    from quantem.gpu_b200.temporal import join_object_waves
+
+    out = {"workload": "complex64 object-wave stacks, random subpixel drifts, phase reference "
+                       "'first', weighted mean, aligned stack returned"}
+    stream = torch.cuda.current_stream(dev)
+    rng = np.random.default_rng(11)
+    for n, t in ((128, 256), (512, 64)):
+        g = torch.Generator(device=dev).manual_seed(n)
+        stack = torch.polar(1.0 + 0.05 * torch.randn((t, n, n), generator=g, device=dev),
+                            0.2 * torch.randn((t, n, n), generator=g, device=dev)).to(torch.complex64)
+        shifts = torch.as_tensor(rng.uniform(-4, 4, (t, 2)), dtype=torch.float32, device=dev)
+        weights = torch.as_tensor(rng.uniform(0.5, 1.0, t), dtype=torch.float32, device=dev)
+        fn = lambda: join_object_waves(stack, shifts=shifts, weights=weights,  # noqa: E731
+                                       phase_reference="first", return_aligned_stack=True)
+        fn()
+        torch.cuda.synchronize(dev)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record(stream)
+        for _ in range(steps):
+            fn()
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = s.elapsed_time(e) / steps
+        alg = 72.0 * n * n * t
+        # CPU: the FP64 oracle on 4 frames, scaled per frame (one host thread for numpy's FFT)
+        host = stack[:4].cpu().numpy()
+        t0 = time.perf_counter()
+        to.join_object_waves(host, shifts[:4].cpu().numpy(), weights[:4].cpu().numpy(), "first")
+        cpu_fps = 4 / (time.perf_counter() - t0)
+        out[f"{n}x{n}_T{t}"] = {"ms": ms, "frames_per_s": t * 1e3 / ms,
+                                "alg_gbs": alg / ms / 1e6, "cpu_oracle_frames_per_s": cpu_fps}
+        del stack
+    return out
+
+
 def sweep_3scans(dev: torch.device, steps: int) -> dict:
     """Batched aberration sweep: scans of 96^2, 128^2 and 160x120 positions
     (128^2 detector, padded by the reference's rule to 128^2, 128^2, 256^2),
@@ -697,6 +739,7 @@ def run_b200(args, world, rank, local) -> None:
         if not args.no_large:
             line["large_512"] = large_512(dev)
         line["sweep_3scans"] = sweep_3scans(dev, 5)
+        line["temporal_join"] = temporal_join(dev)
         line["learned_fits"] = learned_fits(dev)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(counts.cpu().numpy())
