@@ -292,6 +292,43 @@ int qssb_join_object_waves(float* frames, const float* weights, int32_t n_frames
                            float* joined, int32_t write_back, void* stream);
 
 /* ------------------------------------------------------------------------
+ * HDF5 bitshuffle + LZ4 chunks (filter 32008, element size 2, 8192-byte
+ * blocks) <-> u16 detector frames: the reference's acquisition decode
+ * (io/load.py:3271-3320, io/backends/cuda/decoder.py:258-403) and writer
+ * (io/save.py, decoder.py:496-1003). Chunk: big-endian u64 uncompressed bytes,
+ * big-endian u32 block bytes, then per block a big-endian u32 size and an LZ4
+ * block of the bit-shuffled elements; elements beyond the last multiple of 8
+ * follow raw. */
+#define QSSB_BSLZ4_OK 0
+#define QSSB_BSLZ4_BAD_HEADER 1   /* header size or block size wrong, chunk too short */
+#define QSSB_BSLZ4_BAD_CHAIN 2    /* a block runs past the chunk's end */
+#define QSSB_BSLZ4_BAD_LZ4 3      /* malformed LZ4 sequence or wrong decoded size */
+
+/* Decode n_chunks chunks: chunk c occupies compressed[chunk_offsets[c],
+ * chunk_offsets[c+1]) (the last ends at compressed_bytes) and decodes to
+ * chunk_bytes bytes at out + c * chunk_bytes / 2. compressed, chunk_offsets
+ * (int64), out: device. status: device int32 [n_chunks] (QSSB_BSLZ4_*) or
+ * NULL; a chunk that fails is zero-filled. Every offset and length is checked
+ * against the chunk's end. */
+int qssb_decode_bslz4_u16(const uint8_t* compressed, int64_t compressed_bytes,
+                          const int64_t* chunk_offsets, int32_t n_chunks, int64_t chunk_bytes,
+                          uint16_t* out, int32_t* status, void* stream);
+
+/* Scratch bytes of qssb_encode_bslz4_u16. */
+int qssb_encode_bslz4_scratch_bytes(int32_t n_chunks, int64_t chunk_bytes, size_t* bytes);
+
+/* Compress n_chunks frames (device u16, chunk_bytes each) into scratch and
+ * write each chunk's packed size (device int64 [n_chunks]). */
+int qssb_encode_bslz4_u16(const uint16_t* frames, int32_t n_chunks, int64_t chunk_bytes,
+                          uint8_t* scratch, int64_t* chunk_sizes, void* stream);
+
+/* Lay the chunks out at chunk_offsets (device int64, e.g. the exclusive sum
+ * of chunk_sizes) in packed (device u8, room for the total). */
+int qssb_pack_bslz4(const uint8_t* scratch, const uint16_t* frames, int32_t n_chunks,
+                    int64_t chunk_bytes, const int64_t* chunk_offsets, uint8_t* packed,
+                    void* stream);
+
+/* ------------------------------------------------------------------------
  * Learned aberration proposer (no counterpart in the reference, which has no
  * learned component). Features: trotter amplitudes |G_b(Q)| at n_q scan
  * frequencies, resampled onto a k grid through a caller-built CSR table

@@ -143,6 +143,11 @@ SIGNATURES = {
     "qssb_to_bf16": (ctypes.c_int, [_P, _I64, _P, _P]),
     "qssb_loss_batch": (ctypes.c_int, [
         _P, _P, _P, _P, ctypes.POINTER(Calibration), _P, _I32, _I32, _P, _SZ, _P, _P, _P]),
+    "qssb_decode_bslz4_u16": (ctypes.c_int, [_P, ctypes.c_int64, _P, _I32, ctypes.c_int64, _P, _P,
+                                             _P]),
+    "qssb_encode_bslz4_scratch_bytes": (ctypes.c_int, [_I32, ctypes.c_int64, ctypes.POINTER(_SZ)]),
+    "qssb_encode_bslz4_u16": (ctypes.c_int, [_P, _I32, ctypes.c_int64, _P, _P, _P]),
+    "qssb_pack_bslz4": (ctypes.c_int, [_P, _P, _I32, ctypes.c_int64, _P, _P, _P]),
     "qssb_fourier_shift": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _P, _P]),
     "qssb_join_workspace_bytes": (ctypes.c_int, [_I32, ctypes.POINTER(_SZ)]),
     "qssb_join_object_waves": (ctypes.c_int, [_P, _P, _I32, ctypes.c_int64, _I32, _P, _SZ, _P,
