@@ -373,6 +373,63 @@ def temporal_join(dev: torch.device, steps: int = 10) -> dict:
     return out
 
 
+def bslz4_decode(dev: torch.device, steps: int = 10) -> dict:
+    """The acquisition decode before the SSB path: the 128^4 synthetic counts
+    as HDF5 bitshuffle+LZ4 chunks (one 32 KB frame each, 16384 chunks, written
+    by qssb_encode_bslz4_u16) decoded into the u16 device tensor; beside it
+    the reference's own reader kernels on the same bytes (oracle/_ref) and the
+    pure-Python format oracle on a sample of frames (one host thread)."""
+    from oracle import bslz4_oracle as bo
+    from quantem.gpu_b200.decode import decode_bslz4, encode_bslz4
+    from quantem.gpu_b200.synthetic import CONFIGS, generate
+
+    counts = generate(CONFIGS[SPEC_NAME], device=dev).counts.reshape(-1, 128, 128)
+    packed, offsets = encode_bslz4(counts)
+    out_bytes = counts.numel() * 2
+    stream = torch.cuda.current_stream(dev)
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    decode_bslz4(packed, offsets, (128, 128))
+    torch.cuda.synchronize(dev)
+    s.record(stream)
+    for _ in range(steps):
+        decode_bslz4(packed, offsets, (128, 128), check=False)
+    e.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = s.elapsed_time(e) / steps
+    res = {"workload": "128^4 synthetic u16 counts as 16384 bitshuffle+LZ4 chunks of 32 KB",
+           "compressed_mb": packed.numel() / 1e6, "decoded_mb": out_bytes / 1e6,
+           "ratio": out_bytes / packed.numel(), "decode_ms": ms,
+           "decoded_gbs": out_bytes / ms / 1e6,
+           "compressed_gbs": packed.numel() / ms / 1e6}
+    try:
+        from oracle.ref_cuda.bslz4 import ReferenceBslz4
+
+        ref = ReferenceBslz4(dev)
+        # the reference reader walks block starts on the host first (not timed);
+        # its two kernels are timed like ours
+        run, got = ref.prepare_decode(packed, offsets, (128, 128))
+        run()
+        torch.cuda.synchronize(dev)
+        s.record(stream)
+        for _ in range(steps):
+            run()
+        e.record(stream)
+        torch.cuda.synchronize(dev)
+        res["reference_decode_ms"] = s.elapsed_time(e) / steps
+        res["speedup_vs_reference_kernels"] = res["reference_decode_ms"] / ms
+        res["reference_matches"] = bool(torch.equal(got.view(torch.int16), counts.view(torch.int16)))
+    except Exception as exc:  # noqa: BLE001 - the checker is optional on this leg
+        res["reference"] = f"unavailable: {exc}"
+    host = packed[: int(offsets[8])].cpu().numpy().tobytes()
+    offs = list(offsets[:8].cpu().numpy()) + [len(host)]
+    t0 = time.perf_counter()
+    for i in range(8):
+        bo.decode_chunk(host[offs[i]:offs[i + 1]])
+    res["cpu_oracle_frames_per_s"] = 8 / (time.perf_counter() - t0)
+    res["frames_per_s"] = counts.shape[0] * 1e3 / ms
+    return res
+
+
 def sweep_3scans(dev: torch.device, steps: int) -> dict:
     """Batched aberration sweep: scans of 96^2, 128^2 and 160x120 positions
     (128^2 detector, padded by the reference's rule to 128^2, 128^2, 256^2),
@@ -740,6 +797,7 @@ def run_b200(args, world, rank, local) -> None:
             line["large_512"] = large_512(dev)
         line["sweep_3scans"] = sweep_3scans(dev, 5)
         line["temporal_join"] = temporal_join(dev)
+        line["bslz4_decode"] = bslz4_decode(dev)
         line["learned_fits"] = learned_fits(dev)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(counts.cpu().numpy())

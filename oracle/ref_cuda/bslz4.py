@@ -81,6 +81,13 @@ class ReferenceBslz4:
     def decode(self, packed: torch.Tensor, offsets: torch.Tensor, frame_shape) -> torch.Tensor:
         """The reference reader: block starts walked on the host (as load.py
         does from the chunk headers), LZ4 blocks, then the u16 unshuffle."""
+        run, out = self.prepare_decode(packed, offsets, frame_shape)
+        run()
+        torch.cuda.synchronize(self.device)
+        return out
+
+    def prepare_decode(self, packed: torch.Tensor, offsets: torch.Tensor, frame_shape):
+        """Host walk and uploads once; returns (launch the two kernels, output)."""
         P, U32 = ctypes.c_void_p, ctypes.c_uint
         n = int(offsets.numel())
         frame_bytes = 2 * int(frame_shape[0]) * int(frame_shape[1])
@@ -101,12 +108,16 @@ class ReferenceBslz4:
         block_offsets = torch.arange(0, n * n_8kb, n_8kb, dtype=torch.int32, device=d)
         lz = torch.empty(n * frame_bytes, dtype=torch.uint8, device=d)
         out = torch.empty((n, *frame_shape), dtype=torch.uint16, device=d)
-        self._launch("h5lz4dc_batched", ((n_8kb + 1) // 2, 1, n), (32, 2, 1),
-                     [(packed.data_ptr(), P), (chunk_offsets.data_ptr(), P),
-                      (block_starts.data_ptr(), P), (counts.data_ptr(), P),
-                      (block_offsets.data_ptr(), P), (BLOCK, U32), (frame_bytes, U32),
-                      (lz.data_ptr(), P)])
-        self._launch("shuf_8192_16_batched", (n_8kb, 1, n), (256, 1, 1),
-                     [(lz.data_ptr(), P), (out.data_ptr(), P), (frame_bytes, U32)])
-        torch.cuda.synchronize(d)
-        return out
+        keep = (chunk_offsets, block_starts, counts, block_offsets, lz)
+
+        def run():
+            _ = keep
+            self._launch("h5lz4dc_batched", ((n_8kb + 1) // 2, 1, n), (32, 2, 1),
+                         [(packed.data_ptr(), P), (chunk_offsets.data_ptr(), P),
+                          (block_starts.data_ptr(), P), (counts.data_ptr(), P),
+                          (block_offsets.data_ptr(), P), (BLOCK, U32), (frame_bytes, U32),
+                          (lz.data_ptr(), P)])
+            self._launch("shuf_8192_16_batched", (n_8kb, 1, n), (256, 1, 1),
+                         [(lz.data_ptr(), P), (out.data_ptr(), P), (frame_bytes, U32)])
+
+        return run, out

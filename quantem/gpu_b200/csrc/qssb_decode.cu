@@ -12,12 +12,13 @@
 // the remaining < 8 elements follow raw.
 //
 // Decode: one CTA per chunk. Thread 0 walks the block chain (every offset
-// checked against the chunk's end); each warp stages a compressed block in
-// shared memory, decodes the LZ4 sequences (lane 0 parses, all lanes copy
-// literals and matches - a match byte j reads out[op - off + j mod off], so
-// overlapping matches need no serial copy) and bit-unshuffles the block with
-// 8x8 bit transposes straight into the u16 frame (16-byte stores). A
-// malformed chunk sets status[c] (the block is zero-filled); nothing traps.
+// checked against the chunk's end); each warp decodes a block's LZ4
+// sequences into shared memory (every lane parses the token stream through
+// L1, all lanes copy literals and matches - a match byte j reads
+// out[op - off + j mod off], so overlapping matches need no serial copy) and
+// bit-unshuffles the block with 8x8 bit transposes straight into the u16
+// frame (16-byte stores). A malformed chunk sets status[c] (the block is
+// zero-filled); nothing traps.
 // Encode: the same transposes forward, a greedy LZ4 compressor per block
 // (lane 0, a 4096-entry hash table in shared memory) into fixed-stride
 // slots, then a pack kernel that lays out the chunks at caller offsets.
@@ -29,7 +30,6 @@ constexpr int kDecWarps = 4;
 constexpr int kBlockBytes = 8192;                         // bytes per shuffled block
 constexpr int kBlockElems = kBlockBytes / 2;
 constexpr int kLz4Bound = kBlockBytes + kBlockBytes / 255 + 16;  // LZ4 worst case
-constexpr int kInPitch = (kLz4Bound + 15) & ~15;
 constexpr int kMaxBlocks = 512;                           // 4 MB frames
 constexpr int kEncHash = 4096;
 
@@ -54,74 +54,59 @@ __device__ __forceinline__ uint64_t transpose8(uint64_t x) {
     return x;
 }
 
-// Decode one LZ4 block from in[0, csz) into out[0, cap) by the whole warp.
-// Returns true when the stream is well formed and fills exactly cap bytes.
-__device__ bool lz4_block_warp(const uint8_t* in, int csz, uint8_t* out, int cap, int lane) {
+// Decode one LZ4 block from in[0, csz) (global memory, read through L1) into
+// out[0, cap) (shared memory) by the whole warp. Every lane parses the token
+// stream itself (the same bytes: broadcast reads, uniform control flow, no
+// shuffles); literal and match bytes are copied lane-parallel. Returns true
+// when the stream is well formed and fills exactly cap bytes.
+__device__ bool lz4_block_warp(const uint8_t* __restrict__ in, int csz, uint8_t* out, int cap,
+                               int lane) {
     int ip = 0, op = 0;
     for (int guard = 0; guard < kBlockBytes + 1; ++guard) {
-        int lit = 0, lit_at = 0, ml = 0, off = 0, next = 0, code = 0;  // code: 0 ok, 1 last, 2 error
-        if (lane == 0) {
-            int p = ip;
-            if (p >= csz) {
-                code = 2;
-            } else {
-                const int token = in[p++];
-                lit = token >> 4;
-                if (lit == 15) {
-                    int b;
-                    do {
-                        if (p >= csz) { code = 2; break; }
-                        b = in[p++];
-                        lit += b;
-                    } while (b == 255 && lit <= cap);
-                }
-                lit_at = p;
-                if (code == 0 && (lit > cap - op || lit > csz - p)) code = 2;
-                if (code == 0) {
-                    p += lit;
-                    if (p == csz) {
-                        code = 1;
-                    } else if (p + 2 > csz) {
-                        code = 2;
-                    } else {
-                        off = in[p] | (in[p + 1] << 8);
-                        p += 2;
-                        ml = (token & 15) + 4;
-                        if ((token & 15) == 15) {
-                            int b;
-                            do {
-                                if (p >= csz) { code = 2; break; }
-                                b = in[p++];
-                                ml += b;
-                            } while (b == 255 && ml <= cap);
-                        }
-                        if (code == 0 && (off == 0 || off > op + lit || ml > cap - op - lit)) code = 2;
-                    }
-                }
-                next = p;
-            }
+        if (ip >= csz) return false;
+        const int token = __ldg(in + ip++);
+        int lit = token >> 4;
+        if (lit == 15) {
+            int b;
+            do {
+                if (ip >= csz) return false;
+                b = __ldg(in + ip++);
+                lit += b;
+            } while (b == 255 && lit <= cap);
         }
-        code = __shfl_sync(0xffffffffu, code, 0);
-        if (code == 2) return false;
-        lit = __shfl_sync(0xffffffffu, lit, 0);
-        lit_at = __shfl_sync(0xffffffffu, lit_at, 0);
-        for (int j = lane; j < lit; j += 32) out[op + j] = in[lit_at + j];
+        if (lit > cap - op || lit > csz - ip) return false;
+        for (int j = lane; j < lit; j += 32) out[op + j] = __ldg(in + ip + j);
+        ip += lit;
         op += lit;
-        if (code == 1) {
+        if (ip == csz) {
             __syncwarp();
             return op == cap;
         }
-        ml = __shfl_sync(0xffffffffu, ml, 0);
-        off = __shfl_sync(0xffffffffu, off, 0);
-        ip = __shfl_sync(0xffffffffu, next, 0);
+        if (ip + 2 > csz) return false;
+        const int off = __ldg(in + ip) | (__ldg(in + ip + 1) << 8);
+        ip += 2;
+        int ml = (token & 15) + 4;
+        if ((token & 15) == 15) {
+            int b;
+            do {
+                if (ip >= csz) return false;
+                b = __ldg(in + ip++);
+                ml += b;
+            } while (b == 255 && ml <= cap);
+        }
+        if (off == 0 || off > op || ml > cap - op) return false;
         __syncwarp();  // literals (and earlier matches) visible to the match reads
-        // out[op + j] = out[op - off + (j mod off)]: reads only bytes before op
-        int r = lane % off;
-        const int step = 32 % off;
-        for (int j = lane; j < ml; j += 32) {
-            out[op + j] = out[op - off + r];
-            r += step;
-            if (r >= off) r -= off;
+        if (off >= ml) {  // no self-overlap: a plain copy
+            for (int j = lane; j < ml; j += 32) out[op + j] = out[op - off + j];
+        } else {
+            // out[op + j] = out[op - off + (j mod off)]: reads only bytes before op
+            int r = lane % off;
+            const int step = 32 % off;
+            for (int j = lane; j < ml; j += 32) {
+                out[op + j] = out[op - off + r];
+                r += step;
+                if (r >= off) r -= off;
+            }
         }
         op += ml;
         __syncwarp();
@@ -173,7 +158,7 @@ __global__ void __launch_bounds__(32 * kDecWarps) k_decode_bslz4_u16(
     const uint8_t* __restrict__ comp, long long comp_bytes, const long long* __restrict__ offsets,
     int n_chunks, long long chunk_bytes, uint16_t* __restrict__ out, int* __restrict__ status) {
     extern __shared__ uint4 dec_smem4[];
-    uint8_t* wbuf = reinterpret_cast<uint8_t*>(dec_smem4);  // per warp: input, then output
+    uint8_t* wbuf = reinterpret_cast<uint8_t*>(dec_smem4);  // per warp: one decoded block
     __shared__ DecSmem sh;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
@@ -186,6 +171,13 @@ __global__ void __launch_bounds__(32 * kDecWarps) k_decode_bslz4_u16(
     const long long c1 = c + 1 < n_chunks ? offsets[c + 1] : comp_bytes;
     const uint8_t* ch = comp + c0;
     const long long len = c1 - c0;
+    if (c0 >= 0 && c1 <= comp_bytes) {
+        // the chunk's bytes into L1 (one prefetch per 128-byte line) before the
+        // serial block-chain walk and the parses read them
+        for (long long i = (long long)tid * 128; i < len; i += 128LL * 32 * kDecWarps)
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(ch + i));
+    }
+    __syncthreads();
     if (tid == 0) {
         int st = kStOk;
         if (c0 < 0 || c1 > comp_bytes || len < 12) {
@@ -207,31 +199,25 @@ __global__ void __launch_bounds__(32 * kDecWarps) k_decode_bslz4_u16(
         if (st == kStOk && pos + (n_elem - n8) * 2 > len) st = kStChain;
         sh.tail_at = (int)pos;
         sh.status = st;
+        if (status) status[c] = st;  // blocks that fail raise it below
     }
     __syncthreads();
     uint16_t* frame = out + (size_t)c * n_elem;
     const bool vec = (n_elem & 7) == 0 && ((uintptr_t)out & 15u) == 0;
     if (sh.status != kStOk) {
         for (long long i = tid; i < n_elem; i += 32 * kDecWarps) frame[i] = 0;
-        if (tid == 0 && status) status[c] = sh.status;
         return;
     }
-    uint8_t* in_buf = wbuf + (size_t)warp * (kInPitch + kBlockBytes);
-    uint8_t* out_buf = in_buf + kInPitch;
-    bool ok = true;
+    uint8_t* out_buf = wbuf + (size_t)warp * kBlockBytes;
     for (int i = warp; i < n_blocks; i += kDecWarps) {
         const long long e0 = (long long)i * kBlockElems;
         const int cnt = (int)min((long long)kBlockElems, n8 - e0);
-        const int csz = sh.size[i];
-        const uint8_t* src = ch + sh.start[i];
-        for (int j = lane; j < csz; j += 32) in_buf[j] = src[j];
-        __syncwarp();
-        const bool good = lz4_block_warp(in_buf, csz, out_buf, 2 * cnt, lane);
+        const bool good = lz4_block_warp(ch + sh.start[i], sh.size[i], out_buf, 2 * cnt, lane);
         if (good) {
             unshuffle_store(out_buf, cnt, frame + e0, vec, lane);
         } else {
-            ok = false;
             for (int j = lane; j < cnt; j += 32) frame[e0 + j] = 0;
+            if (lane == 0 && status) atomicMax(status + c, kStLz4);
         }
         __syncwarp();
     }
@@ -242,9 +228,6 @@ __global__ void __launch_bounds__(32 * kDecWarps) k_decode_bslz4_u16(
             frame[j] = (uint16_t)(raw[b] | (raw[b + 1] << 8));
         }
     }
-    if (!ok) atomicExch(&sh.status, kStLz4);
-    __syncthreads();
-    if (tid == 0 && status) status[c] = sh.status;
 }
 
 // ------------------------------------------------------------------ encode
@@ -399,7 +382,7 @@ extern "C" int qssb_decode_bslz4_u16(const uint8_t* compressed, int64_t compress
     int rc = check_chunk_bytes(chunk_bytes, "qssb_decode_bslz4_u16: chunk_bytes must be even, "
                                             "at most 4 MB");
     if (rc) return rc;
-    const size_t smem = (size_t)kDecWarps * (kInPitch + kBlockBytes);
+    const size_t smem = (size_t)kDecWarps * kBlockBytes;
     CUDA_TRY(cudaFuncSetAttribute(k_decode_bslz4_u16, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));
     k_decode_bslz4_u16<<<n_chunks, 32 * kDecWarps, smem, (cudaStream_t)stream>>>(
