@@ -907,6 +907,77 @@ __global__ void __launch_bounds__(256) k_scan_cols(int n_bf, float2* __restrict_
     }
 }
 
+// Persistent column pass (N >= 512): one CTA per SM (a warp per column of
+// the strip) loops over (BF pixel, column strip) items; the next strip arrives by cp.async into
+// the second buffer while the current one is transformed (one warp per
+// column) and stored.
+__device__ __forceinline__ void scan_cp_async8(void* smem_dst, const void* gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+
+template <int N>
+__global__ void __launch_bounds__(32 * ScanLines<N>::kTile, 1) k_scan_cols_p(int n_bf,
+                                                                          float2* __restrict__ g_half) {
+    using L = ScanLines<N>;
+    constexpr int P = L::P;
+    constexpr int T = L::kTile;  // columns per strip, one warp each
+    constexpr int NT = 32 * T;
+    constexpr int H = L::H;
+    constexpr int RPL = N / 32;
+    constexpr int NS = (H + T - 1) / T;  // strips per BF image
+    extern __shared__ float2 scan_colsp_smem[];
+    float2* tiles = scan_colsp_smem;     // [2][T][P]
+    float2* tw = tiles + 2 * T * P;
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    fill_twiddles<N>(tw, tid, NT);
+    const long long n_items = (long long)n_bf * NS;
+    auto issue = [&](long long item, float2* dst) {
+        const int b = (int)(item / NS);
+        const int c0 = (int)(item - (long long)b * NS) * T;
+        const int nc = min(T, H - c0);
+        const float2* g = g_half + (size_t)b * N * H + c0;
+        for (int e = tid; e < N * T; e += NT) {
+            const int r = e / T;
+            const int c = e - r * T;
+            if (c < nc) scan_cp_async8(dst + c * P + r, g + (size_t)r * H + c);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    int buf = 0;
+    if (blockIdx.x < n_items) issue(blockIdx.x, tiles);
+    for (long long item = blockIdx.x; item < n_items; item += gridDim.x) {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();  // this strip is in; the other buffer's stores are done
+        if (item + gridDim.x < n_items) issue(item + gridDim.x, tiles + (buf ^ 1) * T * P);
+        float2* tile = tiles + buf * T * P;
+        const int b = (int)(item / NS);
+        const int c0 = (int)(item - (long long)b * NS) * T;
+        const int nc = min(T, H - c0);
+        if (warp < nc) {
+            float2* line = tile + warp * P;
+            float2 v[RPL];
+#pragma unroll
+            for (int t = 0; t < RPL; ++t) v[t] = line[lane + 32 * t];
+            __syncwarp();
+            warp_fft<N, -1>(v, line, tw, lane);
+#pragma unroll
+            for (int j = 0; j < RPL; ++j) line[warp_fft_index<N>(lane, j)] = v[j];
+        }
+        __syncthreads();
+        float2* g = g_half + (size_t)b * N * H + c0;
+        for (int e = tid; e < N * T; e += NT) {
+            const int r = e / T;
+            const int c = e - r * T;
+            if (c < nc) g[(size_t)r * H + c] = tile[c * P + r];
+        }
+        buf ^= 1;
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
 template <int N>
 static int launch_scan_lines(const uint16_t* columns, int n_bf, float* g_half, cudaStream_t s) {
     using L = ScanLines<N>;
@@ -918,7 +989,16 @@ static int launch_scan_lines(const uint16_t* columns, int n_bf, float* g_half, c
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaFuncSetAttribute(k_scan_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)L::cols_smem));
-    k_scan_cols<N><<<dim3(n_bf, (L::H + L::kTile - 1) / L::kTile), 256, L::cols_smem, s>>>(n_bf, g);
+    if constexpr (N >= 512) {
+        const size_t smem = sizeof(float2) * ((size_t)2 * L::kTile * L::P + N);
+        CUDA_TRY(cudaFuncSetAttribute(k_scan_cols_p<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+        const long long items = (long long)n_bf * ((L::H + L::kTile - 1) / L::kTile);
+        const int grid = items < device_sm_count() ? (int)items : device_sm_count();
+        k_scan_cols_p<N><<<grid, 32 * L::kTile, smem, s>>>(n_bf, g);
+    } else {
+        k_scan_cols<N><<<dim3(n_bf, (L::H + L::kTile - 1) / L::kTile), 256, L::cols_smem, s>>>(n_bf, g);
+    }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
