@@ -907,7 +907,7 @@ __global__ void __launch_bounds__(256) k_scan_cols(int n_bf, float2* __restrict_
     }
 }
 
-// Persistent column pass (N >= 512): one CTA per SM (a warp per column of
+// Persistent column pass (N >= 256): one CTA per SM (a warp per column of
 // the strip) loops over (BF pixel, column strip) items; the next strip arrives by cp.async into
 // the second buffer while the current one is transformed (one warp per
 // column) and stored.
@@ -989,7 +989,7 @@ static int launch_scan_lines(const uint16_t* columns, int n_bf, float* g_half, c
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaFuncSetAttribute(k_scan_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)L::cols_smem));
-    if constexpr (N >= 512) {
+    if constexpr (N >= 256) {
         const size_t smem = sizeof(float2) * ((size_t)2 * L::kTile * L::P + N);
         CUDA_TRY(cudaFuncSetAttribute(k_scan_cols_p<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
