@@ -88,9 +88,36 @@ class SSB:
         return cls(data, **kwargs)
 
     @classmethod
+    def from_chunks(cls, chunks, *, frame_shape: tuple[int, int], scan_shape: tuple[int, int],
+                    chunk_offsets=None, **kwargs) -> "SSB":
+        """Create a session from an acquisition stored one detector frame per
+        HDF5 bitshuffle+LZ4 chunk (the format ``SSB.open`` reads in the
+        reference, io/load.py:3271-3320): ``chunks`` is a list of raw chunk
+        bytes (e.g. from ``read_direct_chunk``), or a uint8 tensor of packed
+        chunks with ``chunk_offsets``; the chunks cross to the GPU compressed
+        and are decoded there."""
+        import torch
+
+        from .decode import decode_bslz4, from_chunks
+
+        r0, r1 = (int(x) for x in scan_shape)
+        k0, k1 = (int(x) for x in frame_shape)
+        if chunk_offsets is None:
+            counts = from_chunks(list(chunks), (k0, k1))
+        else:
+            dev = torch.device("cuda", torch.cuda.current_device())
+            data = torch.as_tensor(chunks).to(dev, non_blocking=True)
+            offs = torch.as_tensor(chunk_offsets, dtype=torch.int64).to(dev, non_blocking=True)
+            counts = decode_bslz4(data, offs, (k0, k1))
+        if counts.shape[0] != r0 * r1:
+            raise ValueError(f"{counts.shape[0]} chunks for a {r0}x{r1} scan")
+        return cls(counts.reshape(r0, r1, k0, k1), **kwargs)
+
+    @classmethod
     def open(cls, *args, **kwargs) -> "SSB":
-        raise NotImplementedError("SSB.open (HDF5 decode) is outside the B200 engine's scope; "
-                                  "load counts and use SSB.from_array.")
+        raise NotImplementedError("SSB.open needs an HDF5 reader (h5py), which this build does "
+                                  "not bundle: read the chunks with read_direct_chunk and use "
+                                  "SSB.from_chunks, or load counts and use SSB.from_array.")
 
     def _prepare(self) -> B200SSBBackend:
         if self._session is None:

@@ -108,3 +108,20 @@ def test_decoded_acquisition_reconstructs_identically():
     a = SSB.from_array(counts, **kw).reconstruct({"C10": 0.0, "C12": 0.0, "phi12": 0.0})
     b = SSB.from_array(decoded, **kw).reconstruct({"C10": 0.0, "C12": 0.0, "phi12": 0.0})
     assert torch.equal(a.object_wave, b.object_wave)
+
+
+def test_ssb_from_chunks_matches_from_array():
+    spec = CONFIGS["plain_32x32_det64"]
+    counts = generate(spec, DEV).counts  # [32, 32, 64, 64] -> padded to 128^2 scans by the session
+    kw = dict(voltage_kV=spec.voltage_kV, semiangle_mrad=spec.semiangle_mrad,
+              scan_sampling_A=spec.scan_step_A, det_sampling=spec.det_sampling_mrad)
+    packed, offsets = encode_bslz4(counts.reshape(-1, 64, 64))
+    host = packed.cpu().numpy().tobytes()
+    offs = list(offsets.cpu().numpy()) + [len(host)]
+    chunks = [host[offs[i]:offs[i + 1]] for i in range(len(offs) - 1)]
+    ab = {"C10": 50.0, "C12": 20.0, "phi12": 0.3}
+    want = SSB.from_array(counts, **kw).reconstruct(ab).object_wave
+    a = SSB.from_chunks(chunks, frame_shape=(64, 64), scan_shape=(32, 32), **kw).reconstruct(ab)
+    b = SSB.from_chunks(packed.cpu().pin_memory(), chunk_offsets=offsets.cpu(), frame_shape=(64, 64),
+                        scan_shape=(32, 32), **kw).reconstruct(ab)
+    assert torch.equal(a.object_wave, want) and torch.equal(b.object_wave, want)
