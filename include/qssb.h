@@ -236,6 +236,14 @@ int qssb_loss_batch(const float* g_half, const float* bf_geom, const float* q_ro
                     void* workspace, size_t workspace_bytes, float* losses,
                     float* mean_phase, void* stream);
 
+/* The phase function of qssb_loss_batch and qssb_loss_batch_full:
+ * out[i] = atan2(y[i], x[i]) by an octant reduction and a degree-17 odd
+ * polynomial, |error| <= 4e-7 rad against IEEE atan2 for finite
+ * |x|, |y| < 2^126, signed zeros and NaN as IEEE atan2. The reference's loss
+ * takes cupy.angle (engine.py:2120-2295); this entry exposes the GPU
+ * replacement so its error can be checked. y, x, out: device float32 [n]. */
+int qssb_phase_atan2(const float* y, const float* x, float* out, int64_t n, void* stream);
+
 /* The 14 Krivanek coefficients of one candidate, slots C10, C12, C21, C23,
  * C30, C32, C34, C41, C43, C45, C50, C52, C54, C56 (aberration.py:63,
  * engine.py:1244-1262): magnitudes in the length unit of C10 (Angstrom, as

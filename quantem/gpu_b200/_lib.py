@@ -156,6 +156,7 @@ SIGNATURES = {
         ctypes.c_int, [ctypes.POINTER(Calibration), _I32, _I32, ctypes.POINTER(_SZ)]),
     "qssb_loss_batch_full": (ctypes.c_int, [
         _P, _P, _P, _P, ctypes.POINTER(Calibration), _P, _I32, _I32, _P, _SZ, _P, _P, _P]),
+    "qssb_phase_atan2": (ctypes.c_int, [_P, _P, _P, ctypes.c_int64, _P]),
 }
 
 _lib = None

@@ -129,7 +129,7 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_moments(
 #pragma unroll
             for (int t = 0; t < RPL; ++t) {
                 const float2 v = plane[(lane + 32 * t) * P + col];
-                const float ph = atan2f(v.y, v.x);
+                const float ph = phase_atan2(v.y, v.x);
                 as[ci][t] += ph;
                 aq[ci][t] = fmaf(ph, ph, aq[ci][t]);
             }
@@ -249,9 +249,10 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
             pk = probe_at_bf<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
                                     __ldg(geom + 4 * n_bf + b), __ldg(geom + 5 * n_bf + b), p);
         const float2* gb = g + (size_t)b * N * H;
-        // A) rows 0..64 and the lower Nyquist column
-        for (int e = tid; e < 65 * N + 63; e += 512) {
-            int r, c;
+        // A) rows 0..64 and the lower Nyquist column; the G (and e^{iQ})
+        // values of a thread's next element are loaded one element ahead
+        constexpr int kNA = 65 * N + 63;
+        auto elem_rc = [](int e, int& r, int& c) {
             if (e < 65 * N) {
                 r = e >> 7;
                 c = e & 127;
@@ -259,17 +260,36 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
                 r = N - 1 - (e - 65 * N);  // 127 .. 65
                 c = 64;
             }
-            const float2 gv = c <= 64 ? __ldg(gb + r * H + c)
-                                      : cconj(__ldg(gb + ((N - r) & (N - 1)) * H + (N - c)));
+        };
+        auto g_at = [&](int r, int c) {
+            return c <= 64 ? __ldg(gb + r * H + c)
+                           : cconj(__ldg(gb + ((N - r) & (N - 1)) * H + (N - c)));
+        };
+        float2 g_nx = make_float2(0.f, 0.f), eq_nx = make_float2(1.f, 0.f);
+        if (tid < kNA) {
+            int r, c;
+            elem_rc(tid, r, c);
+            g_nx = g_at(r, c);
+            if constexpr (QUAD) eq_nx = __ldg(eqc + r * N + c);
+        }
+        for (int e = tid; e < kNA; e += 512) {
+            int r, c;
+            elem_rc(e, r, c);
+            const float2 gv = g_nx;
+            const float2 eqv = eq_nx;
+            if (e + 512 < kNA) {
+                int rn, cn;
+                elem_rc(e + 512, rn, cn);
+                g_nx = g_at(rn, cn);
+                if constexpr (QUAD) eq_nx = __ldg(eqc + rn * N + cn);
+            }
             float2 v;
             if constexpr (kSep) {
                 const float2 lo = make_float2(kq.kx_lo, kq.ky_lo);
-                v = corrected_quad_e(__ldg(q_row + r), __ldg(q_col + c), r, c,
-                                     __ldg(eqc + r * N + c), kq.kx, kq.ky, kq.ak, &lo,
-                                     cmul(s_phr[r], s_phc[c]), gv, p);
+                v = corrected_quad_e(__ldg(q_row + r), __ldg(q_col + c), r, c, eqv, kq.kx, kq.ky,
+                                     kq.ak, &lo, cmul(s_phr[r], s_phc[c]), gv, p);
             } else if constexpr (QUAD) {
-                v = corrected_quad<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c,
-                                          __ldg(eqc + r * N + c), kq, gv, p);
+                v = corrected_quad<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c, eqv, kq, gv, p);
             } else {
                 v = corrected<CHI64>(__ldg(q_row + r), __ldg(q_col + c), r, c, kq.kx, kq.ky,
                                      kq.kx_lo, kq.ky_lo, pk, gv, p);
@@ -329,7 +349,7 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
 #pragma unroll
             for (int t = 0; t < 16; ++t) {
                 const int y = fft128_g8_index(s, t);
-                const float ph = atan2f(v[t].y, v[t].x);
+                const float ph = phase_atan2(v[t].y, v[t].x);
                 acc[round][t] += ph;
                 float* q2 = sq + y * kL128P + x;
                 *q2 = fmaf(ph, ph, *q2);
@@ -650,7 +670,7 @@ __global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
         warp_fft<N, +1>(v, line, tw, lane);
 #pragma unroll
         for (int j = 0; j < RPL; ++j) {
-            const float ph = atan2f(v[j].y, v[j].x);
+            const float ph = phase_atan2(v[j].y, v[j].x);
             as[j] += ph;
             aq[j] = fmaf(ph, ph, aq[j]);
         }
@@ -909,7 +929,7 @@ __global__ void __launch_bounds__(kLossThreads, 1) k_loss_full(
 #pragma unroll
             for (int t = 0; t < RPL; ++t) {
                 const float2 v = plane[(lane + 32 * t) * P + col];
-                const float ph = atan2f(v.y, v.x);
+                const float ph = phase_atan2(v.y, v.x);
                 as[ci][t] += ph;
                 float* q2 = sq + col * N + lane + 32 * t;
                 *q2 = fmaf(ph, ph, *q2);
@@ -1063,4 +1083,26 @@ extern "C" int qssb_loss_batch_full(const float* g_half, const float* bf_geom, c
         default: return set_error(QSSB_ERR_UNSUPPORTED,
                                   "qssb_loss_batch_full: scan size must be 64, 128, 256, 512 or 1024");
     }
+}
+
+namespace qssb {
+__global__ void k_phase_atan2(const float* __restrict__ y, const float* __restrict__ x,
+                              float* __restrict__ out, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x)
+        out[i] = phase_atan2(__ldg(y + i), __ldg(x + i));
+}
+}  // namespace qssb
+
+extern "C" int qssb_phase_atan2(const float* y, const float* x, float* out, int64_t n,
+                                void* stream) {
+    if (n < 0 || (n > 0 && (!y || !x || !out)))
+        return set_error(QSSB_ERR_INVALID, "qssb_phase_atan2: null pointer or negative size");
+    if (n == 0) return QSSB_OK;
+    long long blocks = (n + 255) / 256;
+    const long long cap = 8LL * device_sm_count();
+    if (blocks > cap) blocks = cap;
+    k_phase_atan2<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(y, x, out, n);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
 }

@@ -29,6 +29,7 @@ LAUNCHES_PER_CALL = {
     "qssb_loss_batch_full": 3,
     "qssb_fourier_shift": 3,
     "qssb_join_object_waves": 1,
+    "qssb_phase_atan2": 1,
 }
 LAUNCH_COUNT = 0
 _PROFILE: list | None = None
@@ -378,6 +379,19 @@ def loss_batch(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
           _ptr(q_col), ctypes.byref(cal), _ptr(candidates), n, int(flags), _ptr(buf), buf.numel(),
           _ptr(losses), _ptr(mp), _stream(g_half))
     return losses, mp
+
+
+def phase_atan2(y: torch.Tensor, x: torch.Tensor) -> torch.Tensor:
+    """atan2(y, x) by the loss kernels' phase function (float32 CUDA tensors
+    of one shape; |error| <= 4e-7 rad against IEEE atan2)."""
+    _require_cuda(y, "y", torch.float32)
+    _require_cuda(x, "x", torch.float32)
+    if y.shape != x.shape:
+        raise ValueError("y and x must have the same shape")
+    y, x = y.contiguous(), x.contiguous()
+    out = torch.empty_like(y)
+    _call("qssb_phase_atan2", y.device, _ptr(y), _ptr(x), _ptr(out), y.numel(), _stream(y))
+    return out
 
 
 # ------------------------------------------------------------ time series
