@@ -191,106 +191,25 @@ __global__ void __launch_bounds__(512, 1) k_scan_fft_half(const uint16_t* __rest
     }
 }
 
-// 128 x 128 scan FFT, one CTA (16 warps = 64 groups of 8 lanes) per BF image.
-//  1. the u16 image is staged in shared memory (rows padded to 136 u16);
+// 128 x 128 scan FFT: persistent CTAs (one per SM, 16 warps = 64 groups of
+// 8 lanes) loop over BF images. Per image:
+//  1. the u16 image arrives in shared memory (rows padded to 136 u16) by
+//     cp.async (16-byte global -> shared copies, L1 bypassed) while the
+//     previous image is transformed, so the 32 KB load is off the critical
+//     path;
 //  2. group j transforms rows 2j and 2j+1 packed as one complex line
-//     (fft128_g8) and splits the two real spectra into the half plane H;
-//  3. 64 groups + 1 transform the 65 columns of H in place (fft128_g8), the
-//     column of group (w, grp) chosen so the two groups of each half-warp hit
-//     disjoint bank halves of H (pitch 65);
-//  4. H, which has G's [128][65] layout, is copied out with 16-byte stores.
-constexpr int kImgPitch = 136;                       // u16 per staged image row
+//     (fft128_g8) and splits the two real spectra into the half plane H
+//     ([128][65], pitch 65);
+//  3. the 65 columns of H are transformed in place by the 64 groups: columns
+//     0 and 64 (the DC and Nyquist bins of real rows) are real, so they go
+//     packed as Z = H(:,0) + i H(:,64) in one transform, stored in column 0;
+//     group (w, grp) takes a column chosen so the two groups of each
+//     half-warp hit disjoint bank halves of H;
+//  4. columns 0 and 64 are split from Z, F0(k) = (Z(k) + conj Z(-k)) / 2,
+//     F64(k) = (Z(k) - conj Z(-k)) / (2i), and H, which has G's [128][65]
+//     layout, is copied out with 16-byte stores.
+constexpr int kImgPitch = 136;  // u16 per staged image row
 constexpr int kScanHalf = 65;
-struct ScanFft128Smem {
-    static constexpr size_t a_bytes = sizeof(float2) * 64 * kG8Scratch;  // T, aliases the image
-    static constexpr size_t h_bytes = sizeof(float2) * 128 * kScanHalf;
-    static constexpr size_t bytes = a_bytes + h_bytes + sizeof(float2) * 128;
-    static_assert(sizeof(uint16_t) * 128 * kImgPitch <= a_bytes, "image fits in the T region");
-};
-
-__global__ void __launch_bounds__(512, 1) k_scan_fft128(const uint16_t* __restrict__ columns,
-                                                        int n_bf, float2* __restrict__ g_half) {
-    extern __shared__ float4 smem4[];
-    char* base = reinterpret_cast<char*>(smem4);
-    uint16_t* img = reinterpret_cast<uint16_t*>(base);
-    float2* T = reinterpret_cast<float2*>(base);
-    float2* H = reinterpret_cast<float2*>(base + ScanFft128Smem::a_bytes);
-    float2* tw = H + 128 * kScanHalf;
-    const int b = blockIdx.x;
-    if (b >= n_bf) return;
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    const int warp = tid >> 5;
-    const int g = tid >> 3;  // group 0..63
-    const int s = tid & 7;   // sub-lane
-    fill_twiddles<128>(tw, tid, 512);
-    // 1. stage the image
-    const uint4* src = reinterpret_cast<const uint4*>(columns + (size_t)b * 128 * 128);
-    for (int i = tid; i < 128 * 128 / 8; i += 512) {
-        const uint4 v = __ldcs(src + i);
-        const int row = i >> 4;
-        const int col = (i & 15) * 8;
-        *reinterpret_cast<uint4*>(img + row * kImgPitch + col) = v;
-    }
-    __syncthreads();
-    // 2. row pairs
-    float2 v[16];
-    {
-        const uint16_t* r0 = img + (2 * g) * kImgPitch + s;
-        const uint16_t* r1 = r0 + kImgPitch;
-#pragma unroll
-        for (int n1 = 0; n1 < 16; ++n1) v[n1] = make_float2((float)r0[8 * n1], (float)r1[8 * n1]);
-    }
-    __syncthreads();  // the image region becomes T
-    float2* Tg = T + g * kG8Scratch;
-    fft128_g8<-1>(v, Tg, s, tw);
-#pragma unroll
-    for (int t = 0; t < 16; ++t) Tg[fft128_g8_index(s, t)] = v[t];
-    __syncwarp();
-    // X_2g(c) = (Z(c) + conj Z(-c)) / 2, X_2g+1(c) = (Z(c) - conj Z(-c)) / (2i)
-#pragma unroll
-    for (int m = 0; m < 9; ++m) {
-        const int c = s + 8 * m;
-        if (c <= 64) {
-            const float2 z = Tg[c];
-            const float2 zm = Tg[(128 - c) & 127];
-            H[(2 * g) * kScanHalf + c] = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
-            H[(2 * g + 1) * kScanHalf + c] = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
-        }
-    }
-    __syncthreads();
-    // 3. columns: 64 in the first round, column 64 in the second
-    {
-        const int grp = lane >> 3;
-        const int col = 16 * (warp & 3) + 8 * (grp & 1) + 2 * (warp >> 2) + (grp >> 1);
-#pragma unroll
-        for (int n1 = 0; n1 < 16; ++n1) v[n1] = H[(s + 8 * n1) * kScanHalf + col];
-        fft128_g8<-1>(v, Tg, s, tw);
-#pragma unroll
-        for (int t = 0; t < 16; ++t) H[fft128_g8_index(s, t) * kScanHalf + col] = v[t];
-    }
-    if (warp == 0) {  // all 32 lanes of warp 0 take part in the group's syncwarps
-        const bool act = lane < 8;
-#pragma unroll
-        for (int n1 = 0; n1 < 16; ++n1) v[n1] = act ? H[(s + 8 * n1) * kScanHalf + 64] : make_float2(0.f, 0.f);
-        fft128_g8<-1>(v, Tg, s, tw);
-        if (act) {
-#pragma unroll
-            for (int t = 0; t < 16; ++t) H[fft128_g8_index(s, t) * kScanHalf + 64] = v[t];
-        }
-    }
-    __syncthreads();
-    // 4. copy out (H has G's layout; 128 * 65 float2 = 4160 float4)
-    const float4* h4 = reinterpret_cast<const float4*>(H);
-    float4* dst = reinterpret_cast<float4*>(g_half + (size_t)b * 128 * kScanHalf);
-    for (int i = tid; i < 128 * kScanHalf / 2; i += 512) dst[i] = h4[i];
-}
-
-// Persistent form of k_scan_fft128: one CTA per SM loops over BF images; the
-// next image is copied into a second staging buffer with cp.async (16-byte
-// global -> shared copies, L1 bypassed) while the current one is transformed,
-// so the 32 KB load of each image is off the critical path. Same arithmetic
-// and output as k_scan_fft128.
 struct ScanFft128PSmem {
     static constexpr size_t t_bytes = sizeof(float2) * 64 * kG8Scratch;
     static constexpr size_t h_bytes = sizeof(float2) * 128 * kScanHalf;
@@ -332,6 +251,9 @@ __global__ void __launch_bounds__(512, 1) k_scan_fft128p(const uint16_t* __restr
     const int g = tid >> 3;  // group 0..63
     const int s = tid & 7;   // sub-lane
     fill_twiddles<128>(tw, tid, 512);
+    // column job of this group: 0 = the packed DC / Nyquist pair, else the column
+    const int grp = lane >> 3;
+    const int col = 16 * (warp & 3) + 8 * (grp & 1) + 2 * (warp >> 2) + (grp >> 1);
     int buf = 0;
     if (blockIdx.x < n_bf) stage_image_async(imgs, columns, blockIdx.x, tid);
     for (int b = blockIdx.x; b < n_bf; b += gridDim.x) {
@@ -353,6 +275,7 @@ __global__ void __launch_bounds__(512, 1) k_scan_fft128p(const uint16_t* __restr
 #pragma unroll
         for (int t = 0; t < 16; ++t) Tg[fft128_g8_index(s, t)] = v[t];
         __syncwarp();
+        // X_2g(c) = (Z(c) + conj Z(-c)) / 2, X_2g+1(c) = (Z(c) - conj Z(-c)) / (2i)
 #pragma unroll
         for (int m = 0; m < 9; ++m) {
             const int c = s + 8 * m;
@@ -364,23 +287,33 @@ __global__ void __launch_bounds__(512, 1) k_scan_fft128p(const uint16_t* __restr
             }
         }
         __syncthreads();
-        {
-            const int grp = lane >> 3;
-            const int col = 16 * (warp & 3) + 8 * (grp & 1) + 2 * (warp >> 2) + (grp >> 1);
+        // columns (64 jobs: 1..63 and the packed 0 / 64 pair)
+        if (col == 0) {
+#pragma unroll
+            for (int n1 = 0; n1 < 16; ++n1) {
+                const float2* hr = H + (s + 8 * n1) * kScanHalf;
+                v[n1] = make_float2(hr[0].x, hr[64].x);  // both columns are real
+            }
+        } else {
 #pragma unroll
             for (int n1 = 0; n1 < 16; ++n1) v[n1] = H[(s + 8 * n1) * kScanHalf + col];
-            fft128_g8<-1>(v, Tg, s, tw);
-#pragma unroll
-            for (int t = 0; t < 16; ++t) H[fft128_g8_index(s, t) * kScanHalf + col] = v[t];
         }
-        if (warp == 0) {
-            const bool act = lane < 8;
+        fft128_g8<-1>(v, Tg, s, tw);
 #pragma unroll
-            for (int n1 = 0; n1 < 16; ++n1) v[n1] = act ? H[(s + 8 * n1) * kScanHalf + 64] : make_float2(0.f, 0.f);
-            fft128_g8<-1>(v, Tg, s, tw);
-            if (act) {
-#pragma unroll
-                for (int t = 0; t < 16; ++t) H[fft128_g8_index(s, t) * kScanHalf + 64] = v[t];
+        for (int t = 0; t < 16; ++t) H[fft128_g8_index(s, t) * kScanHalf + col] = v[t];
+        __syncthreads();
+        // split Z into columns 0 and 64: thread k <= 64 owns rows k and -k
+        if (tid <= 64) {
+            const int km = (128 - tid) & 127;
+            const float2 a = H[tid * kScanHalf];
+            const float2 m = H[km * kScanHalf];
+            const float2 f0 = make_float2(0.5f * (a.x + m.x), 0.5f * (a.y - m.y));
+            const float2 f64 = make_float2(0.5f * (a.y + m.y), -0.5f * (a.x - m.x));
+            H[tid * kScanHalf] = f0;
+            H[tid * kScanHalf + 64] = f64;
+            if (km != tid) {  // F(-k) = conj F(k) for real columns (k = 0, 64: real)
+                H[km * kScanHalf] = cconj(f0);
+                H[km * kScanHalf + 64] = cconj(f64);
             }
         }
         __syncthreads();
