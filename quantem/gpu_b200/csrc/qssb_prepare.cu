@@ -375,18 +375,28 @@ extern "C" int qssb_mean_dp_u64(const uint16_t* counts, int64_t n_frames, int32_
 
 // Bounding-box gather. The BF pixels' bounding box (rows x columns rounded
 // out to 8 pixels = 16 bytes) is read per frame with coalesced 16-byte copies
-// into shared memory, 8 frames per tile; each BF column then receives its 8
-// frames as one 16-byte store. Persistent CTAs (two per SM) loop over frame
-// tiles with the next tile's box arriving by cp.async into a second buffer
-// while the current tile is written out. (DRAM fetches whole 128-byte lines,
-// so the box rows are read in full either way: ~12.5 KB per 128^2 frame.) A
-// box larger than the tile buffer is taken in row bands (work item = frame
-// tile x band); with ascending BF indices (the selection's order) each band
-// writes only its own contiguous BF range. Boxes wider than one buffer fall
-// back to direct element loads.
-constexpr int kGbF = 8;
+// into shared memory, F frames per tile; each BF column then receives its F
+// frames as F/8 consecutive 16-byte stores. Persistent CTAs (two per SM) loop
+// over frame tiles with the next tile's box arriving by cp.async into a second
+// buffer while the current tile is written out. (DRAM fetches whole 128-byte
+// lines, so the box rows are read in full either way: ~12.5 KB per 128^2
+// frame.) A box larger than the tile buffer (MAXPIX pixels per frame) is taken
+// in row bands (work item = frame tile x band); with ascending BF indices (the
+// selection's order) each band writes only its own contiguous BF range. Boxes
+// wider than one buffer fall back to direct element loads.
+// Two shapes, same 98 KB of buffers: F = 32 frames x 768 pixels for detectors
+// up to 768 columns (64-byte column writes: at 128^4, 60 us against 70 us for
+// 16-byte ones), F = 8 x 3072 for wider ones.
+template <int F, int MAXPIX>
+struct GbShape {
+    static constexpr int kF = F;
+    static constexpr int kMaxPix = MAXPIX;
+    static constexpr size_t smem = sizeof(uint16_t) * 2 * F * MAXPIX;
+};
+using GbNarrow = GbShape<32, 768>;
+using GbWide = GbShape<8, 3072>;
 constexpr int kGbThreads = 256;
-constexpr int kGbMaxPix = 3072;  // box pixels per frame held in one buffer
+constexpr int kGbNarrowCols = 768;
 
 __device__ __forceinline__ void gb_cp_async16(void* smem_dst, const void* gmem_src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -395,9 +405,12 @@ __device__ __forceinline__ void gb_cp_async16(void* smem_dst, const void* gmem_s
 
 constexpr int kGbMaxBands = 64;
 
+template <typename SHAPE>
 __global__ void __launch_bounds__(kGbThreads) k_gather_bbox(
     const uint16_t* __restrict__ counts, long long n_frames, int det_rows, int det_cols,
     const int32_t* __restrict__ bf_linear, int n_bf, uint16_t* __restrict__ columns) {
+    constexpr int kGbF = SHAPE::kF;
+    constexpr int kGbMaxPix = SHAPE::kMaxPix;
     extern __shared__ uint4 smem_u4[];
     uint16_t* tiles = reinterpret_cast<uint16_t*>(smem_u4);  // [2][kGbF][band area]
     __shared__ int s_box[4][kGbThreads / 32];
@@ -525,12 +538,15 @@ __global__ void __launch_bounds__(kGbThreads) k_gather_bbox(
             const int pos = ok ? (r - r0) * width + (c - c0) : 0;
             uint16_t* dst = columns + (size_t)b * n_frames + f0;
             if (vec_out && nf == kGbF) {
-                uint32_t w[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    w[q] = ok ? ((uint32_t)tile[(2 * q) * area + pos] |
-                                 ((uint32_t)tile[(2 * q + 1) * area + pos] << 16)) : 0u;
-                *reinterpret_cast<uint4*>(dst) = make_uint4(w[0], w[1], w[2], w[3]);
+                for (int h = 0; h < kGbF / 8; ++h) {  // 8 frames per 16-byte store
+                    uint32_t w[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        w[q] = ok ? ((uint32_t)tile[(8 * h + 2 * q) * area + pos] |
+                                     ((uint32_t)tile[(8 * h + 2 * q + 1) * area + pos] << 16)) : 0u;
+                    reinterpret_cast<uint4*>(dst)[h] = make_uint4(w[0], w[1], w[2], w[3]);
+                }
             } else {
                 for (int f = 0; f < nf; ++f) dst[f] = ok ? tile[f * area + pos] : (uint16_t)0;
             }
@@ -693,6 +709,22 @@ extern "C" int qssb_gather_bf_columns(const uint16_t* counts, int64_t n_frames, 
     return QSSB_OK;
 }
 
+template <typename SHAPE>
+static int launch_gather_bbox(const uint16_t* counts, int64_t n_frames, int det_rows, int det_cols,
+                              const int32_t* bf_linear, int n_bf, uint16_t* columns,
+                              cudaStream_t stream) {
+    const long long n_tiles = (n_frames + SHAPE::kF - 1) / SHAPE::kF;
+    long long gx = 2LL * device_sm_count();
+    if (gx > n_tiles) gx = n_tiles;
+    const int smem = (int)SHAPE::smem;
+    CUDA_TRY(cudaFuncSetAttribute(k_gather_bbox<SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  smem));
+    k_gather_bbox<SHAPE><<<(unsigned)gx, kGbThreads, smem, stream>>>(
+        counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
 extern "C" int qssb_gather_bf_columns_2d(const uint16_t* counts, int64_t n_frames,
                                          int32_t det_rows, int32_t det_cols,
                                          const int32_t* bf_linear, int32_t n_bf,
@@ -719,15 +751,11 @@ extern "C" int qssb_gather_bf_columns_2d(const uint16_t* counts, int64_t n_frame
         CUDA_TRY(cudaGetLastError());
         return QSSB_OK;
     }
-    const long long n_tiles = (n_frames + kGbF - 1) / kGbF;
-    long long gx = 2LL * device_sm_count();
-    if (gx > n_tiles) gx = n_tiles;
-    const int smem = (int)(sizeof(uint16_t) * 2 * kGbF * kGbMaxPix);
-    CUDA_TRY(cudaFuncSetAttribute(k_gather_bbox, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    k_gather_bbox<<<(unsigned)gx, kGbThreads, smem, (cudaStream_t)stream>>>(
-        counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns);
-    CUDA_TRY(cudaGetLastError());
-    return QSSB_OK;
+    if (det_cols <= kGbNarrowCols)
+        return launch_gather_bbox<GbNarrow>(counts, n_frames, det_rows, det_cols, bf_linear, n_bf,
+                                            columns, (cudaStream_t)stream);
+    return launch_gather_bbox<GbWide>(counts, n_frames, det_rows, det_cols, bf_linear, n_bf,
+                                      columns, (cudaStream_t)stream);
 }
 
 // ------------------------------------------ 256^2 .. 1024^2 scan FFT
