@@ -214,6 +214,27 @@ def test_bbox_gather_is_bit_exact(n_frames, det, radius, shuffle):
     np.testing.assert_array_equal(cols, counts.reshape(n_frames, -1)[:, lin].T)
 
 
+@pytest.mark.parametrize("n_frames,det,shuffle", [
+    (2051, (16, 1024), False), (1000, (16, 1024), True), (300, (4, 4096), False),
+    (300, (96, 768), False), (64, (96, 768), True)])
+def test_bbox_gather_wide_detectors(n_frames, det, shuffle):
+    """Both tile shapes of the bounding-box gather and its direct fallback on
+    wide detectors: 32 x 768 at <= 768 columns (a 90-row box needs more than
+    64 one-row bands, hence the direct path), 8 x 3072 beyond (five row bands
+    of three 928-pixel box rows; a 3648-pixel box row does not fit and takes
+    the direct path)."""
+    rng = np.random.default_rng(n_frames + det[1])
+    k0, k1 = det
+    counts = rng.integers(0, 65536, size=(n_frames, k0, k1), dtype=np.uint16)
+    rr, cc = np.meshgrid(np.arange(k0), np.arange(k1), indexing="ij")
+    ell = ((rr - k0 / 2 + 0.3) / (0.47 * k0)) ** 2 + ((cc - k1 / 2 - 0.2) / (0.45 * k1)) ** 2 <= 1.0
+    lin = np.nonzero(ell.reshape(-1))[0].astype(np.int32)
+    if shuffle:
+        lin = rng.permutation(lin).astype(np.int32)
+    cols = ops.gather_bf_columns(_dev(counts), _dev(lin)).cpu().numpy()
+    np.testing.assert_array_equal(cols, counts.reshape(n_frames, -1)[:, lin].T)
+
+
 # -------------------------------------------------------------- scan FFT
 @pytest.mark.parametrize("n", [64, 128, 256, 512, 1024])
 def test_scan_fft_half_matches_fp64(n):
