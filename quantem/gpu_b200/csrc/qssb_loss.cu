@@ -380,10 +380,29 @@ __global__ void __launch_bounds__(256) k_loss_reduce(const float* __restrict__ p
     const int j = blockIdx.x * 256 + threadIdx.x;  // col * N + row, or row * N + col
     const int cand = blockIdx.y;
     double s1 = 0.0, s2 = 0.0;
-    for (int k = 0; k < n_chunks; ++k) {
-        const float* base = part + ((size_t)(cand * n_chunks + k) * 2) * N * N;
-        s1 += (double)base[j];
-        s2 += (double)base[(size_t)N * N + j];
+    // eight chunks' loads in flight before their (in-order) FP64 adds: a
+    // single candidate folds ~300 partial planes, which one load at a time
+    // leaves latency-bound
+    const float* cbase = part + (size_t)cand * n_chunks * 2 * N * N + j;
+    int k = 0;
+    for (; k + 8 <= n_chunks; k += 8) {
+        float a[8], b[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const float* base = cbase + (size_t)(k + u) * 2 * N * N;
+            a[u] = __ldg(base);
+            b[u] = __ldg(base + (size_t)N * N);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            s1 += (double)a[u];
+            s2 += (double)b[u];
+        }
+    }
+    for (; k < n_chunks; ++k) {
+        const float* base = cbase + (size_t)k * 2 * N * N;
+        s1 += (double)__ldg(base);
+        s2 += (double)__ldg(base + (size_t)N * N);
     }
     const double inv_b = 1.0 / (double)n_bf;
     const double mean = s1 * inv_b;
