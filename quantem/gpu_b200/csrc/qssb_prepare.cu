@@ -191,33 +191,30 @@ __global__ void __launch_bounds__(512, 1) k_scan_fft_half(const uint16_t* __rest
     }
 }
 
-// 128 x 128 scan FFT: persistent CTAs (one per SM, 16 warps = 64 groups of
-// 8 lanes) loop over BF images. Per image:
-//  1. the u16 image arrives in shared memory (rows padded to 136 u16) by
-//     cp.async (16-byte global -> shared copies, L1 bypassed) while the
-//     previous image is transformed, so the 32 KB load is off the critical
-//     path;
-//  2. group j transforms rows 2j and 2j+1 packed as one complex line
-//     (fft128_g8) and splits the two real spectra into the half plane H
+// 128 x 128 scan FFT: persistent CTAs of 256 threads (32 groups of 8 lanes),
+// two per SM (106 KB of shared memory each, so one CTA's barriers overlap
+// the other's work), loop over BF images. Per image:
+//  1. the u16 image is in shared memory (rows padded to 136 u16), copied in
+//     by cp.async (16-byte global -> shared copies, L1 bypassed) while the
+//     previous image's spectrum was stored; each group reads its two row
+//     pairs (j = g, g + 32) into registers, after which the image region
+//     serves as the groups' FFT scratch;
+//  2. row pairs 2j, 2j+1 are transformed packed as one complex line
+//     (fft128_g8) and split into the two real spectra of the half plane H
 //     ([128][65], pitch 65);
-//  3. the 65 columns of H are transformed in place by the 64 groups: columns
-//     0 and 64 (the DC and Nyquist bins of real rows) are real, so they go
-//     packed as Z = H(:,0) + i H(:,64) in one transform, stored in column 0;
-//     group (w, grp) takes a column chosen so the two groups of each
-//     half-warp hit disjoint bank halves of H;
+//  3. the 65 columns of H are transformed in place, two jobs per group:
+//     columns 0 and 64 (the DC and Nyquist bins of real rows) are real, so
+//     they go packed as Z = H(:,0) + i H(:,64) in one transform, stored in
+//     column 0; job (warp + 8 round, grp) takes a column chosen so the two
+//     groups of each half-warp hit disjoint bank halves of H;
 //  4. columns 0 and 64 are split from Z, F0(k) = (Z(k) + conj Z(-k)) / 2,
-//     F64(k) = (Z(k) - conj Z(-k)) / (2i), and H, which has G's [128][65]
-//     layout, is copied out with 16-byte stores.
+//     F64(k) = (Z(k) - conj Z(-k)) / (2i); the next image's copy is started
+//     and H, which has G's [128][65] layout, is copied out with 16-byte
+//     stores.
+// (The 512-thread form with a separate scratch and a double-buffered image,
+// one CTA per SM, took 80 us at 1781 BF pixels; this one 71 us.)
 constexpr int kImgPitch = 136;  // u16 per staged image row
 constexpr int kScanHalf = 65;
-struct ScanFft128PSmem {
-    static constexpr size_t t_bytes = sizeof(float2) * 64 * kG8Scratch;
-    static constexpr size_t h_bytes = sizeof(float2) * 128 * kScanHalf;
-    static constexpr size_t tw_bytes = sizeof(float2) * 128;
-    static constexpr size_t img_bytes = sizeof(uint16_t) * 128 * kImgPitch;
-    static constexpr size_t bytes = t_bytes + h_bytes + tw_bytes + 2 * img_bytes;
-};
-
 __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
@@ -225,10 +222,11 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+template <int NT>
 __device__ __forceinline__ void stage_image_async(uint16_t* img, const uint16_t* columns, int b,
                                                   int tid) {
     const uint4* src = reinterpret_cast<const uint4*>(columns + (size_t)b * 128 * 128);
-    for (int i = tid; i < 128 * 128 / 8; i += 512) {
+    for (int i = tid; i < 128 * 128 / 8; i += NT) {
         const int row = i >> 4;
         const int col = (i & 15) * 8;
         cp_async16(img + row * kImgPitch + col, src + i);
@@ -236,71 +234,90 @@ __device__ __forceinline__ void stage_image_async(uint16_t* img, const uint16_t*
     cp_async_commit();
 }
 
-__global__ void __launch_bounds__(512, 1) k_scan_fft128p(const uint16_t* __restrict__ columns,
+struct ScanFft128PSmem {
+    static constexpr size_t t_bytes = sizeof(float2) * 32 * kG8Scratch;
+    static constexpr size_t img_bytes = sizeof(uint16_t) * 128 * kImgPitch;
+    static constexpr size_t u_bytes = ((t_bytes > img_bytes ? t_bytes : img_bytes) + 15) & ~(size_t)15;
+    static constexpr size_t h_bytes = sizeof(float2) * 128 * kScanHalf;
+    static constexpr size_t tw_bytes = sizeof(float2) * 128;
+    static constexpr size_t bytes = u_bytes + h_bytes + tw_bytes;
+};
+
+__global__ void __launch_bounds__(256, 2) k_scan_fft128p(const uint16_t* __restrict__ columns,
                                                          int n_bf, float2* __restrict__ g_half) {
     extern __shared__ float4 smem4[];
     char* base = reinterpret_cast<char*>(smem4);
-    float2* T = reinterpret_cast<float2*>(base);
-    float2* H = reinterpret_cast<float2*>(base + ScanFft128PSmem::t_bytes);
+    float2* T = reinterpret_cast<float2*>(base);       // FFT scratch ...
+    uint16_t* img = reinterpret_cast<uint16_t*>(base);  // ... or the staged image
+    float2* H = reinterpret_cast<float2*>(base + ScanFft128PSmem::u_bytes);
     float2* tw = H + 128 * kScanHalf;
-    uint16_t* imgs = reinterpret_cast<uint16_t*>(base + ScanFft128PSmem::t_bytes +
-                                                 ScanFft128PSmem::h_bytes + ScanFft128PSmem::tw_bytes);
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
-    const int g = tid >> 3;  // group 0..63
+    const int g = tid >> 3;  // group 0..31
     const int s = tid & 7;   // sub-lane
-    fill_twiddles<128>(tw, tid, 512);
-    // column job of this group: 0 = the packed DC / Nyquist pair, else the column
     const int grp = lane >> 3;
-    const int col = 16 * (warp & 3) + 8 * (grp & 1) + 2 * (warp >> 2) + (grp >> 1);
-    int buf = 0;
-    if (blockIdx.x < n_bf) stage_image_async(imgs, columns, blockIdx.x, tid);
+    float2* Tg = T + g * kG8Scratch;
+    fill_twiddles<128>(tw, tid, 256);
+    if (blockIdx.x < n_bf) stage_image_async<256>(img, columns, blockIdx.x, tid);
     for (int b = blockIdx.x; b < n_bf; b += gridDim.x) {
-        uint16_t* img = imgs + buf * 128 * kImgPitch;
         cp_async_wait_all();
-        __syncthreads();  // the image is complete; the previous copy-out of H is done
-        const int nb = b + gridDim.x;
-        if (nb < n_bf) stage_image_async(imgs + (buf ^ 1) * 128 * kImgPitch, columns, nb, tid);
-        // row pairs
-        float2 v[16];
+        __syncthreads();  // the image is in; the previous copy-out of H is done
+        // row pairs j = g and g + 32 into registers
+        float2 v0[16], v1[16];
         {
             const uint16_t* r0 = img + (2 * g) * kImgPitch + s;
-            const uint16_t* r1 = r0 + kImgPitch;
-#pragma unroll
-            for (int n1 = 0; n1 < 16; ++n1) v[n1] = make_float2((float)r0[8 * n1], (float)r1[8 * n1]);
-        }
-        float2* Tg = T + g * kG8Scratch;
-        fft128_g8<-1>(v, Tg, s, tw);
-#pragma unroll
-        for (int t = 0; t < 16; ++t) Tg[fft128_g8_index(s, t)] = v[t];
-        __syncwarp();
-        // X_2g(c) = (Z(c) + conj Z(-c)) / 2, X_2g+1(c) = (Z(c) - conj Z(-c)) / (2i)
-#pragma unroll
-        for (int m = 0; m < 9; ++m) {
-            const int c = s + 8 * m;
-            if (c <= 64) {
-                const float2 z = Tg[c];
-                const float2 zm = Tg[(128 - c) & 127];
-                H[(2 * g) * kScanHalf + c] = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
-                H[(2 * g + 1) * kScanHalf + c] = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
-            }
-        }
-        __syncthreads();
-        // columns (64 jobs: 1..63 and the packed 0 / 64 pair)
-        if (col == 0) {
+            const uint16_t* r2 = r0 + 64 * kImgPitch;
 #pragma unroll
             for (int n1 = 0; n1 < 16; ++n1) {
-                const float2* hr = H + (s + 8 * n1) * kScanHalf;
-                v[n1] = make_float2(hr[0].x, hr[64].x);  // both columns are real
+                v0[n1] = make_float2((float)r0[8 * n1], (float)r0[kImgPitch + 8 * n1]);
+                v1[n1] = make_float2((float)r2[8 * n1], (float)r2[kImgPitch + 8 * n1]);
             }
-        } else {
-#pragma unroll
-            for (int n1 = 0; n1 < 16; ++n1) v[n1] = H[(s + 8 * n1) * kScanHalf + col];
         }
-        fft128_g8<-1>(v, Tg, s, tw);
+        __syncthreads();  // the image region becomes T
 #pragma unroll
-        for (int t = 0; t < 16; ++t) H[fft128_g8_index(s, t) * kScanHalf + col] = v[t];
+        for (int round = 0; round < 2; ++round) {
+            float2(&v)[16] = round == 0 ? v0 : v1;
+            const int j = g + 32 * round;
+            fft128_g8<-1>(v, Tg, s, tw);
+#pragma unroll
+            for (int t = 0; t < 16; ++t) Tg[fft128_g8_index(s, t)] = v[t];
+            __syncwarp();
+            // X_2j(c) = (Z(c) + conj Z(-c)) / 2, X_2j+1(c) = (Z(c) - conj Z(-c)) / (2i)
+#pragma unroll
+            for (int m = 0; m < 9; ++m) {
+                const int c = s + 8 * m;
+                if (c <= 64) {
+                    const float2 z = Tg[c];
+                    const float2 zm = Tg[(128 - c) & 127];
+                    H[(2 * j) * kScanHalf + c] = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+                    H[(2 * j + 1) * kScanHalf + c] = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+                }
+            }
+            __syncwarp();  // the group's reads of Tg precede its next transform
+        }
+        __syncthreads();
+        // columns: 64 jobs (1..63 and the packed 0 / 64 pair), two per group
+#pragma unroll
+        for (int round = 0; round < 2; ++round) {
+            const int w = warp + 8 * round;
+            const int col = 16 * (w & 3) + 8 * (grp & 1) + 2 * (w >> 2) + (grp >> 1);
+            float2 v[16];
+            if (col == 0) {
+#pragma unroll
+                for (int n1 = 0; n1 < 16; ++n1) {
+                    const float2* hr = H + (s + 8 * n1) * kScanHalf;
+                    v[n1] = make_float2(hr[0].x, hr[64].x);  // both columns are real
+                }
+            } else {
+#pragma unroll
+                for (int n1 = 0; n1 < 16; ++n1) v[n1] = H[(s + 8 * n1) * kScanHalf + col];
+            }
+            fft128_g8<-1>(v, Tg, s, tw);
+#pragma unroll
+            for (int t = 0; t < 16; ++t) H[fft128_g8_index(s, t) * kScanHalf + col] = v[t];
+            __syncwarp();
+        }
         __syncthreads();
         // split Z into columns 0 and 64: thread k <= 64 owns rows k and -k
         if (tid <= 64) {
@@ -316,11 +333,12 @@ __global__ void __launch_bounds__(512, 1) k_scan_fft128p(const uint16_t* __restr
                 H[km * kScanHalf + 64] = cconj(f64);
             }
         }
-        __syncthreads();
+        __syncthreads();  // T is free: the next image comes in during the copy-out
+        const int nb = b + gridDim.x;
+        if (nb < n_bf) stage_image_async<256>(img, columns, nb, tid);
         const float4* h4 = reinterpret_cast<const float4*>(H);
         float4* dst = reinterpret_cast<float4*>(g_half + (size_t)b * 128 * kScanHalf);
-        for (int i = tid; i < 128 * kScanHalf / 2; i += 512) dst[i] = h4[i];
-        buf ^= 1;
+        for (int i = tid; i < 128 * kScanHalf / 2; i += 256) dst[i] = h4[i];
     }
     cp_async_wait_all();  // nothing left in flight at exit
 }
@@ -991,8 +1009,9 @@ extern "C" int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t
             const size_t smem = ScanFft128PSmem::bytes;
             CUDA_TRY(cudaFuncSetAttribute(k_scan_fft128p, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
-            const int grid = n_bf < device_sm_count() ? n_bf : device_sm_count();
-            k_scan_fft128p<<<grid, 512, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half));
+            const int slots = 2 * device_sm_count();
+            const int grid = n_bf < slots ? n_bf : slots;
+            k_scan_fft128p<<<grid, 256, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half));
             CUDA_TRY(cudaGetLastError());
             return QSSB_OK;
         }
