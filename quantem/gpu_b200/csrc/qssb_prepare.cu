@@ -791,6 +791,12 @@ struct ScanLines {
     static constexpr int H = N / 2 + 1;
     static constexpr int kWarps = N >= 1024 ? 4 : 8;       // row pairs per block
     static constexpr int kTile = N >= 1024 ? 8 : 16;       // columns per block
+    // persistent column pass: columns per strip (one warp each) and CTAs per
+    // SM. At 256 three 8-warp CTAs per SM (0.63 ms for the two scan passes of
+    // 1783 BF pixels against 0.71 with one 16-warp CTA); at 512 and 1024 the
+    // 16/8-warp single CTA (8-warp pairs were within 1% at 512)
+    static constexpr int kTileP = N >= 1024 ? 8 : (N == 256 ? 8 : 16);
+    static constexpr int kCtasP = N == 256 ? 3 : 1;
     static constexpr int kScratch = warp_fft_scratch<N>();  // >= N: also holds a line
     static constexpr int P = kScratch | 1;                  // column pitch, odd mod 16
     static constexpr size_t rows_smem = sizeof(float2) * ((size_t)kWarps * kScratch + N);
@@ -886,21 +892,21 @@ __global__ void __launch_bounds__(256) k_scan_cols(int n_bf, float2* __restrict_
     }
 }
 
-// Persistent column pass (N >= 256): one CTA per SM (a warp per column of
-// the strip) loops over (BF pixel, column strip) items; the next strip arrives by cp.async into
-// the second buffer while the current one is transformed (one warp per
-// column) and stored.
+// Persistent column pass (N >= 256): kCtasP CTAs per SM (a warp per column
+// of the strip) loop over (BF pixel, column strip) items; the next strip
+// arrives by cp.async into the second buffer while the current one is
+// transformed (one warp per column) and stored.
 __device__ __forceinline__ void scan_cp_async8(void* smem_dst, const void* gmem_src) {
     const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
 }
 
 template <int N>
-__global__ void __launch_bounds__(32 * ScanLines<N>::kTile, 1) k_scan_cols_p(int n_bf,
-                                                                          float2* __restrict__ g_half) {
+__global__ void __launch_bounds__(32 * ScanLines<N>::kTileP, ScanLines<N>::kCtasP) k_scan_cols_p(
+    int n_bf, float2* __restrict__ g_half) {
     using L = ScanLines<N>;
     constexpr int P = L::P;
-    constexpr int T = L::kTile;  // columns per strip, one warp each
+    constexpr int T = L::kTileP;  // columns per strip, one warp each
     constexpr int NT = 32 * T;
     constexpr int H = L::H;
     constexpr int RPL = N / 32;
@@ -969,12 +975,13 @@ static int launch_scan_lines(const uint16_t* columns, int n_bf, float* g_half, c
     CUDA_TRY(cudaFuncSetAttribute(k_scan_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)L::cols_smem));
     if constexpr (N >= 256) {
-        const size_t smem = sizeof(float2) * ((size_t)2 * L::kTile * L::P + N);
+        const size_t smem = sizeof(float2) * ((size_t)2 * L::kTileP * L::P + N);
         CUDA_TRY(cudaFuncSetAttribute(k_scan_cols_p<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       (int)smem));
-        const long long items = (long long)n_bf * ((L::H + L::kTile - 1) / L::kTile);
-        const int grid = items < device_sm_count() ? (int)items : device_sm_count();
-        k_scan_cols_p<N><<<grid, 32 * L::kTile, smem, s>>>(n_bf, g);
+        const long long items = (long long)n_bf * ((L::H + L::kTileP - 1) / L::kTileP);
+        const long long slots = (long long)L::kCtasP * device_sm_count();
+        const int grid = (int)(items < slots ? items : slots);
+        k_scan_cols_p<N><<<grid, 32 * L::kTileP, smem, s>>>(n_bf, g);
     } else {
         k_scan_cols<N><<<dim3(n_bf, (L::H + L::kTile - 1) / L::kTile), 256, L::cols_smem, s>>>(n_bf, g);
     }
