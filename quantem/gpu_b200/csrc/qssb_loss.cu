@@ -369,55 +369,75 @@ __global__ void __launch_bounds__(512, 1) k_loss_moments128(
     for (int i = tid; i < N * N; i += 512) pq[i] = sq[(i >> 7) * kL128P + (i & 127)];
 }
 
-// Per pixel: fold the partial planes in FP64 (fixed order), write the mean
-// phase, and sum the variance over this block's 256 pixels (fixed tree):
-// block_var[cand][blockIdx.x]. N^2 is a multiple of 256 for every size.
+// Per pixel: fold the partial planes in FP64, write the mean phase, and sum
+// the variance over this block's 32 pixels: block_var[cand][blockIdx.x]. The
+// eight warps of a block take every 8th partial plane of the same 32 pixels
+// (four planes' loads in flight before their in-order adds), then warp 0
+// adds the eight slices in order - a fixed order for a given plan. N^2 is a
+// multiple of 32 for every size.
+constexpr int kReducePix = 32;
+constexpr int kReduceSlices = 8;
+
 template <int N>
-__global__ void __launch_bounds__(256) k_loss_reduce(const float* __restrict__ part, int n_chunks,
-                                                     int n_bf, double* __restrict__ block_var,
-                                                     float* __restrict__ mean_phase, int row_major) {
-    __shared__ double red[256];
-    const int j = blockIdx.x * 256 + threadIdx.x;  // col * N + row, or row * N + col
+__global__ void __launch_bounds__(kReducePix * kReduceSlices) k_loss_reduce(
+    const float* __restrict__ part, int n_chunks, int n_bf, double* __restrict__ block_var,
+    float* __restrict__ mean_phase, int row_major) {
+    __shared__ double r1[kReduceSlices][kReducePix];
+    __shared__ double r2[kReduceSlices][kReducePix];
+    __shared__ double rv[kReducePix];
+    const int px = threadIdx.x & (kReducePix - 1);
+    const int sl = threadIdx.x / kReducePix;
+    const int j = blockIdx.x * kReducePix + px;  // col * N + row, or row * N + col
     const int cand = blockIdx.y;
+    constexpr size_t NN = (size_t)N * N;
+    const float* cbase = part + (size_t)cand * n_chunks * 2 * NN + j;
     double s1 = 0.0, s2 = 0.0;
-    // eight chunks' loads in flight before their (in-order) FP64 adds: a
-    // single candidate folds ~300 partial planes, which one load at a time
-    // leaves latency-bound
-    const float* cbase = part + (size_t)cand * n_chunks * 2 * N * N + j;
-    int k = 0;
-    for (; k + 8 <= n_chunks; k += 8) {
-        float a[8], b[8];
+    int k = sl;
+    for (; k + 3 * kReduceSlices < n_chunks; k += 4 * kReduceSlices) {
+        float a[4], b[4];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-            const float* base = cbase + (size_t)(k + u) * 2 * N * N;
+        for (int u = 0; u < 4; ++u) {
+            const float* base = cbase + (size_t)(k + u * kReduceSlices) * 2 * NN;
             a[u] = __ldg(base);
-            b[u] = __ldg(base + (size_t)N * N);
+            b[u] = __ldg(base + NN);
         }
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
+        for (int u = 0; u < 4; ++u) {
             s1 += (double)a[u];
             s2 += (double)b[u];
         }
     }
-    for (; k < n_chunks; ++k) {
-        const float* base = cbase + (size_t)k * 2 * N * N;
+    for (; k < n_chunks; k += kReduceSlices) {
+        const float* base = cbase + (size_t)k * 2 * NN;
         s1 += (double)__ldg(base);
-        s2 += (double)__ldg(base + (size_t)N * N);
+        s2 += (double)__ldg(base + NN);
     }
-    const double inv_b = 1.0 / (double)n_bf;
-    const double mean = s1 * inv_b;
-    red[threadIdx.x] = s2 * inv_b - mean * mean;
-    if (mean_phase) {
-        const int hi = j / N;
-        const int lo = j - hi * N;
-        mean_phase[(size_t)cand * N * N + (row_major ? j : lo * N + hi)] = (float)mean;
+    r1[sl][px] = s1;
+    r2[sl][px] = s2;
+    __syncthreads();
+    if (sl == 0) {
+        double t1 = 0.0, t2 = 0.0;
+#pragma unroll
+        for (int w = 0; w < kReduceSlices; ++w) {
+            t1 += r1[w][px];
+            t2 += r2[w][px];
+        }
+        const double inv_b = 1.0 / (double)n_bf;
+        const double mean = t1 * inv_b;
+        rv[px] = t2 * inv_b - mean * mean;
+        if (mean_phase) {
+            const int hi = j / N;
+            const int lo = j - hi * N;
+            mean_phase[(size_t)cand * NN + (row_major ? j : lo * N + hi)] = (float)mean;
+        }
     }
     __syncthreads();
-    for (int w = 128; w > 0; w >>= 1) {
-        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-        __syncthreads();
+    if (threadIdx.x == 0) {
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < kReducePix; ++i) acc += rv[i];
+        block_var[(size_t)cand * (NN / kReducePix) + blockIdx.x] = acc;
     }
-    if (threadIdx.x == 0) block_var[(size_t)cand * (N * N / 256) + blockIdx.x] = red[0];
 }
 
 // L = (sum of the block sums, fixed order) / N^2.
@@ -827,10 +847,10 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
             pl.bf_per_chunk, pl.n_chunks, part);
     }
     CUDA_TRY(cudaGetLastError());
-    k_loss_reduce<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(part, pl.n_chunks, cal.n_bf,
-                                                                       var, mean_phase, N == 128 ? 1 : 0);
+    k_loss_reduce<N><<<dim3(N * N / kReducePix, n_cand), kReducePix * kReduceSlices, 0, s>>>(
+        part, pl.n_chunks, cal.n_bf, var, mean_phase, N == 128 ? 1 : 0);
     CUDA_TRY(cudaGetLastError());
-    k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N / 256, N * N, losses);
+    k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N / kReducePix, N * N, losses);
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -989,10 +1009,10 @@ static int launch_loss_full(const float* g_half, const float* geom, const float*
             pl.bf_per_chunk, pl.n_chunks, part);
         CUDA_TRY(cudaGetLastError());
     }
-    k_loss_reduce<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(part, pl.n_chunks, cal.n_bf,
-                                                                       var, mean_phase, 0);
+    k_loss_reduce<N><<<dim3(N * N / kReducePix, n_cand), kReducePix * kReduceSlices, 0, s>>>(
+        part, pl.n_chunks, cal.n_bf, var, mean_phase, 0);
     CUDA_TRY(cudaGetLastError());
-    k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N / 256, N * N, losses);
+    k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N / kReducePix, N * N, losses);
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
