@@ -216,13 +216,15 @@ def test_bbox_gather_is_bit_exact(n_frames, det, radius, shuffle):
 
 @pytest.mark.parametrize("n_frames,det,shuffle", [
     (2051, (16, 1024), False), (1000, (16, 1024), True), (300, (4, 4096), False),
-    (300, (96, 768), False), (64, (96, 768), True)])
+    (300, (96, 768), False), (64, (96, 768), True), (8192, (24, 512), False)])
 def test_bbox_gather_wide_detectors(n_frames, det, shuffle):
     """Both tile shapes of the bounding-box gather and its direct fallback on
     wide detectors: 32 x 768 at <= 768 columns (a 90-row box needs more than
     64 one-row bands, hence the direct path), 8 x 3072 beyond (five row bands
     of three 928-pixel box rows; a 3648-pixel box row does not fit and takes
-    the direct path)."""
+    the direct path); and, for outputs beyond 64 MB, the 64-frame gather's
+    704-pixel tiles (a 464-pixel box row per band on 512 columns; the
+    192-column cases above take its 320-pixel tiles)."""
     rng = np.random.default_rng(n_frames + det[1])
     k0, k1 = det
     counts = rng.integers(0, 65536, size=(n_frames, k0, k1), dtype=np.uint16)
