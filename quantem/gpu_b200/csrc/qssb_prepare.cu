@@ -405,10 +405,11 @@ extern "C" int qssb_mean_dp_u64(const uint16_t* counts, int64_t n_frames, int32_
 // Two shapes, same 98 KB of buffers: F = 32 frames x 768 pixels for detectors
 // up to 768 columns (64-byte column writes: at 128^4, 60 us against 70 us for
 // 16-byte ones), F = 8 x 3072 for wider ones.
-template <int F, int MAXPIX>
+template <int F, int MAXPIX, int CTAS = 2>
 struct GbShape {
     static constexpr int kF = F;
     static constexpr int kMaxPix = MAXPIX;
+    static constexpr int kCtas = CTAS;  // persistent CTAs per SM
     static constexpr size_t smem = sizeof(uint16_t) * 2 * F * MAXPIX;
 };
 using GbNarrow = GbShape<32, 768>;
@@ -754,7 +755,7 @@ static int launch_gather_bbox(const uint16_t* counts, int64_t n_frames, int det_
                               const int32_t* bf_linear, int n_bf, uint16_t* columns,
                               cudaStream_t stream) {
     const long long n_tiles = (n_frames + SHAPE::kF - 1) / SHAPE::kF;
-    long long gx = 2LL * device_sm_count();
+    long long gx = (long long)SHAPE::kCtas * device_sm_count();
     if (gx > n_tiles) gx = n_tiles;
     const int smem = (int)SHAPE::smem;
     CUDA_TRY(cudaFuncSetAttribute(k_gather_bbox<SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
