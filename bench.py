@@ -45,7 +45,24 @@ UNIT = "recon/s"
 SPEC_NAME = "plain_128x128_det128"
 KW = dict(semiangle=20.0, scan_sampling=0.5, det_sampling=20.0 / 24.0, voltage_kV=300)
 WORKLOAD = ("plain SSB, scan 128x128 x detector 128x128 uint16 (537 MB), ~1784 BF pixels, "
-            "cold u16->object phase per step (graph-launched ColdReconstructor)")
+            "cold u16->object phase per step")
+
+
+def _config(n_bf: int, world: int) -> dict:
+    """The workload dict both arms print (identical keys and values)."""
+    return {"workload": WORKLOAD, "n_bf": int(n_bf), "scan": [128, 128], "detector": [128, 128],
+            "l2": "inputs larger than L2 (537 MB u16 per step)", "parallelism": f"replicas x{world}"}
+
+
+def _sig(x, digits: int = 4):
+    """Round floats (recursively) to a few significant digits for the summary."""
+    if isinstance(x, float):
+        return float(f"{x:.{digits}g}")
+    if isinstance(x, dict):
+        return {k: _sig(v, digits) for k, v in x.items()}
+    if isinstance(x, (list, tuple)):
+        return [_sig(v, digits) for v in x]
+    return x
 
 
 def _dist():
@@ -87,8 +104,8 @@ class Clocks:
     """SM clock, power and throttle reasons sampled during the timed region.
 
     Polls NVML from a background thread every ~2 ms (the timed region of a
-    short run lasts only tens of milliseconds); falls back to nvidia-smi.
-    Reads settings only.
+    short run lasts only tens of milliseconds). Without NVML (pynvml missing
+    or failing) no clock record is produced. Reads settings only.
     """
 
     REASONS = {  # NVML clocks-event-reason bits
@@ -582,11 +599,12 @@ def run_reference(args, world, rank) -> None:
     counts = generate(CONFIGS[SPEC_NAME], device=dev).counts.cpu().numpy()
     kw = dict(voltage_kV=300, semiangle_mrad=KW["semiangle"], scan_sampling=KW["scan_sampling"],
               det_sampling=KW["det_sampling"])
+    n_bf = 0
     for _ in range(args.warmup):
-        spec.reconstruct(counts, **kw)
+        n_bf = spec.reconstruct(counts, **kw)[3]
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        spec.reconstruct(counts, **kw)
+        n_bf = spec.reconstruct(counts, **kw)[3]
     dt = time.perf_counter() - t0
     value = args.steps / dt
     line = {
@@ -594,7 +612,9 @@ def run_reference(args, world, rank) -> None:
         "warmup": args.warmup, "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "impl": "reference",
-        "config": {"workload": WORKLOAD, "path": "CPU torch restatement of docs/kernels/ssb.md"},
+        "config": _config(n_bf, args.gpus),
+        "reference_path": "CPU torch restatement of the reference's executable specification "
+                          "(docs/kernels/ssb.md), every host thread",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": spec.host_threads(), "kind": "port",
                          "sample": "one full 128^4 reconstruction per step"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -807,10 +827,10 @@ def run_b200(args, world, rank, local) -> None:
         "warmup": max(3, args.warmup), "ms_per_step": elapsed_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n_bf": n_bf, "scan": [128, 128], "detector": [128, 128],
-                   "l2": "inputs larger than L2 (537 MB u16 per step)",
-                   "parallelism": f"replicas x{world}"},
-        "roofline": {"bound": "hbm", "kernel": f"{dom['kernel']} ({dominant}), the step's longest stage",
+        "config": _config(n_bf, world),
+        "roofline": {"bound": LIMITER.get(dom["kernel"], "hbm"),
+                     "model": "algorithmic HBM bytes per launch / CUDA-event time vs measured copy bandwidth",
+                     "kernel": f"{dom['kernel']} ({dominant}), the step's longest stage",
                      "achieved": dom["achieved"], "peak": peak, "unit": "GB/s", "frac": dom["frac"],
                      "peak_kind": f"{peak_kind} hbm_gbs", "traffic": _traffic(dom["kernel"]),
                      "alg_bytes_per_launch": dom["alg_bytes_per_launch"],
@@ -854,7 +874,54 @@ def run_b200(args, world, rank, local) -> None:
         _, ref_ph = so.reconstruct(prep, so.Aberrations(0.0, 0.0, 0.0))
         err = so.wrapped_phase_error(ph.cpu().numpy(), ref_ph)
         line["phase_rms_rad_vs_fp64"] = float(np.sqrt(np.mean(err ** 2)))
+    line["headline"] = _headline(line)
     print(json.dumps(line), flush=True)
+
+
+# Measured limiter of each kernel the roofline can name (ncu: issue active,
+# warps active, DRAM throughput; the kernel summaries under profiles/)
+LIMITER = {"k_sum_frames_vec8": "hbm", "k_gather_bbox": "hbm", "k_scan_fft128p": "latency",
+           "k_trotter_quad4": "issue"}
+
+
+def _headline(line: dict) -> dict:
+    """The claims of the line in one compact object, printed last so that a
+    reader who keeps only the end of the output still has them."""
+    h = {"cold_recon_per_s": line["value"], "warm_recon_per_s": line.get("warm_recon_per_s"),
+         "e2e_recon_per_s": line["e2e"]["value"],
+         "e2e_from_chunks_recon_per_s": line.get("e2e_from_chunks", {}).get("value"),
+         "loss_evals_per_s": line.get("loss_evals_per_s_batch64"),
+         "stage_us": {k.replace("qssb_", ""): 1e3 * v for k, v in line.get("stage_ms", {}).items()},
+         "roofline": {"kernel": line["roofline"]["kernel"].split(" ")[0],
+                      "bound": line["roofline"]["bound"], "hbm_frac": line["roofline"]["frac"]}}
+    rc = line.get("reference_cuda", {})
+    if "cold_recon_per_s" in rc:
+        h["reference_cuda_recon_per_s"] = {"cold": rc["cold_recon_per_s"], "warm": rc["warm_recon_per_s"]}
+        h["speedup_vs_reference_cuda"] = line.get("speedup_vs_reference_cuda")
+    if "loss_evals_per_s" in rc:
+        h["reference_cuda_loss_evals_per_s"] = rc["loss_evals_per_s"]
+    if "phase_rms_rad_vs_fp64" in line:
+        h["phase_rms_rad_vs_fp64_128"] = line["phase_rms_rad_vs_fp64"]
+    st = line.get("stress_256")
+    if st:
+        h["stress_256_phase_rms_rad"] = {d: v["phase_rms_rad_vs_fp64_gpu"] for d, v in st["doses"].items()}
+    lg = line.get("large_512")
+    if lg:
+        h["large_512_ms"] = {"cold": lg["cold_u16_to_phase_ms"], "warm_object": lg["warm_complex_object_ms"],
+                             "phase_plus_loss": lg["exact_phase_plus_loss_ms"]}
+    sw = line.get("sweep_3scans")
+    if sw:
+        h["sweep_3scans"] = {"evals_per_s": sw["evals_per_s_graph"],
+                             "launches_per_graph": sw["kernel_launches_per_graph"],
+                             "truth_first": sw["truth_ranked_first"]}
+    lf = line.get("learned_fits")
+    if lf:
+        h["learned_fits"] = {k: lf[k] for k in ("tau_rad", "dose", "n_cases", "mean_evals_plain64",
+                                                "mean_evals_learned8", "evals_ratio") if k in lf}
+    cb = line.get("cpu_baseline")
+    if cb:
+        h["cpu_baseline"] = {"recon_per_s": cb["value"], "cores": cb["cores"]}
+    return _sig(h, 4)
 
 
 def run_profile_once(local: int, with_256: bool = False, with_512: str | None = None) -> None:

@@ -207,8 +207,11 @@ int qssb_object_ex(const float* g_half, const float* bf_geom, const float* q_row
  * that loads the library holds it until the process exits. Requests whose
  * qssb_object_workspace_bytes exceed it fail with QSSB_ERR_WORKSPACE (up to
  * 63488 BF pixels fit at 128^2 scans, 15616 at 256^2).
- * The first call on each device looks up the array's device address; make
- * that first call before any stream capture. All calls share the one array:
+ * The first call on each device looks up the array's device address and
+ * keeps it; make that first call before any stream capture. The kept address
+ * belongs to the device's current primary context: after cudaDeviceReset (or
+ * anything else that destroys that context) it is stale, so a process that
+ * resets a device must not call this entry on it again. All calls share the one array:
  * calls whose work overlaps on the GPU (other streams, other host threads)
  * race and corrupt each other's results, so serialise them. Each call writes
  * every scratch byte it reads, so nothing has to be cleared between calls.

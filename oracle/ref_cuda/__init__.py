@@ -6,7 +6,7 @@ modules and JIT-compiles them with NVRTC through CuPy
 (src/quantem/gpu/ssb/compute/cuda/kernels/common.py:620-622 assembles the
 module, :708 gives the compile options). CuPy is not installed here, so
 ``build_ref.py`` reads those strings with ``ast`` from the reference tree
-(``/root/reference``, present only in the build container), assembles the
+(``build_ref.reference_root()``, present only in the build container), assembles the
 module exactly as ``build_cuda_code`` does, and compiles it with nvcc and the
 reference's options into ``oracle/_ref/ssb_fft128.cubin`` (git-ignored; the
 built file travels to the GPU box, the source does not).

@@ -2,7 +2,9 @@
 
 Run in the build container, where the reference tree exists:
 
-    python -m oracle.ref_cuda.build_bslz4 [--reference /root/reference]
+    python -m oracle.ref_cuda.build_bslz4 [--reference PATH]
+
+(the checkout is found as in ``build_ref.reference_root()``)
 
 Reads the CUDA source string ``_CUDA_LZ4_SOURCE`` of
 ``src/quantem/gpu/io/backends/cuda/decoder.py`` with ``ast`` (the module

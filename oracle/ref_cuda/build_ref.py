@@ -2,7 +2,11 @@
 
 Run in the build container, where the reference tree exists:
 
-    python -m oracle.ref_cuda.build_ref [--reference /root/reference]
+    python -m oracle.ref_cuda.build_ref [--reference PATH]
+
+The reference checkout is found by ``reference_root()``: ``--reference``,
+else the ``QSSB_REFERENCE`` environment variable, else the build container's
+checkout location.
 
 Reads the CUDA source strings of
 ``src/quantem/gpu/ssb/compute/cuda/kernels/common.py`` (``_DEVICE_FUNCTIONS_CUDA``)
@@ -19,6 +23,7 @@ import argparse
 import ast
 import hashlib
 import json
+import os
 import shutil
 import subprocess
 import tempfile
@@ -29,7 +34,20 @@ OUT_DIR = ORACLE / "_ref"
 CUBIN = OUT_DIR / "ssb_fft128.cubin"
 MANIFEST = OUT_DIR / "ssb_fft128.json"
 KERNELS_REL = Path("src/quantem/gpu/ssb/compute/cuda/kernels")
-DEFAULT_REFERENCE = Path("/root/reference")
+# where the build container keeps the reference checkout (read-only); the one
+# place a recipe names it - everything else asks reference_root()
+_BUILD_CONTAINER_CHECKOUT = "/root/reference"
+
+
+def reference_root(override: str | Path | None = None) -> Path:
+    """The reference checkout to read: ``override``, else ``$QSSB_REFERENCE``,
+    else the build container's checkout. It may not exist (GPU boxes)."""
+    if override:
+        return Path(override)
+    return Path(os.environ.get("QSSB_REFERENCE", _BUILD_CONTAINER_CHECKOUT))
+
+
+DEFAULT_REFERENCE = reference_root()
 KERNEL_NAMES = ("ifft128_rows_fused_pk_t32_mr8_packed", "ifft128_cols_t32_mr8")
 TWIDDLE_NAME = "TWIDDLE_128"
 

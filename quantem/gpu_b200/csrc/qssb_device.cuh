@@ -877,7 +877,7 @@ __device__ __forceinline__ void kahan_add(float4& s, float2 v) {
 // atan2(y, x) of the phase-variance loss: octant reduction to
 // t = min(|x|, |y|) / max(|x|, |y|) in [0, 1], atan(t) = t P(t^2) with P of
 // degree 8 (coefficients fitted towards the minimax error on [0, 1] by
-// csrc/phase_atan2_fit.py), then pi/2 - r and pi - r (constants split hi +
+// tests/phase_atan2_fit.py), then pi/2 - r and pi - r (constants split hi +
 // lo) and the sign of y. |error| <= 4e-7 rad (rms < 1e-7) against IEEE
 // atan2 for finite |x|, |y| < 2^126 (the fast divide's range; 2.4e-7 of it
 // is the polynomial, the rest the divide's 2 ulp);

@@ -522,7 +522,9 @@ extern "C" int qssb_object(const float* g_half, const float* bf_geom, const floa
 // file-scope device array (see include/qssb.h for the callers it serves and
 // the sharing rules). The host must not pass the array's name to a kernel:
 // in host code it is a stand-in, not a device address. Its device address is
-// looked up once per device with cudaGetSymbolAddress and cached.
+// looked up once per device with cudaGetSymbolAddress and cached for the
+// life of the process (a device reset, which destroys the context the
+// address belongs to, makes it stale; the header says so).
 static __device__ __align__(256) unsigned char g_noalloc_scratch[QSSB_NOALLOC_SCRATCH_BYTES];
 
 namespace {

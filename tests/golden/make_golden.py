@@ -43,6 +43,10 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
+if str(REPO) not in sys.path:
+    sys.path.insert(0, str(REPO))
+
+from oracle.ref_cuda.build_ref import reference_root  # noqa: E402
 
 
 # ---------------------------------------------------------------------------
@@ -285,16 +289,18 @@ def run_spec(accel, g_half: np.ndarray, aberrations) -> dict:
             "spec_phase": phi.numpy()}
 
 
-REFERENCE = Path("/root/reference")
+REFERENCE = reference_root()
 
 
 def main() -> None:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--reference", default=None,
+                        help="reference checkout (default: $QSSB_REFERENCE, else the build "
+                             "container's checkout)")
     args = parser.parse_args()
     global REFERENCE
-    REFERENCE = Path(args.reference)
-    CudaSSBBackend, refmod = install(Path(args.reference))
+    REFERENCE = reference_root(args.reference)
+    CudaSSBBackend, refmod = install(REFERENCE)
 
     ab = (-120.0, 55.0, math.radians(17.0))
     # 1. The reference test's own end-to-end case (explicit bf_radius=3).

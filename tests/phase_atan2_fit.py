@@ -5,7 +5,7 @@ coefficients and the error of a float32 evaluation (fused multiply-adds
 emulated in float64, rounded to float32 at every step) of the whole atan2
 against numpy.arctan2.
 
-    python quantem/gpu_b200/csrc/phase_atan2_fit.py
+    python tests/phase_atan2_fit.py
 """
 import numpy as np
 

@@ -38,14 +38,15 @@ def _compare(backend: B200SSBBackend, host: np.ndarray, kw: dict, ab: so.Aberrat
     assert abs(backend.dc_value - prep.dc) <= 1e-14 * abs(prep.dc)
     g = backend.G_qk.cpu().numpy()
     assert np.abs(g - prep.g_half).max() <= 2e-6 * np.abs(prep.g_half).max()
-    obj, ph = backend.object_and_phase(ab.C10, ab.C12, ab.phi12)
+    obj, ph = backend.object_and_phase(ab.C10, ab.C12, ab.phi12, ab.C30)
     ref_obj, ref_ph = so.reconstruct(prep, ab)
     err = so.wrapped_phase_error(ph.cpu().numpy(), ref_ph)
     rms = float(np.sqrt(np.mean(err ** 2)))
     assert rms < 1e-4, rms
     if check_loss:
         ref_loss, _ = so.phase_variance_loss(prep.g_half, prep.geo, ab, prep.dc)
-        loss = backend.variance_loss(ab.C10, ab.C12, ab.phi12)
+        c30 = None if ab.C30 == 0.0 else [ab.C30]
+        loss = float(backend.variance_loss_batch([ab.C10], [ab.C12], [ab.phi12], C30=c30)[0])
         assert loss == pytest.approx(ref_loss, rel=1e-5, abs=1e-6)
     return rms
 
@@ -89,16 +90,33 @@ def test_uneven_96_scan_is_padded_like_the_reference():
     _compare(backend, counts, kw, so.Aberrations(10.0, 5.0, 0.1))
 
 
-def test_production_128x128_det128_end_to_end():
+@pytest.fixture(scope="module")
+def production_128():
+    """The 128x128 scan x 128x128 detector workload (537 MB u16), its backend
+    and the FP64 oracle's preparation of the same counts, shared by the cases
+    below."""
     spec = CONFIGS["plain_128x128_det128"]
-    data = generate(spec, device=DEV)
-    counts = data.counts
+    counts = generate(spec, device=DEV).counts
     host = counts.cpu().numpy()
     kw = dict(voltage_kV=300, semiangle_mrad=20.0, scan_sampling=0.5, det_sampling=20.0 / 24.0)
     backend = B200SSBBackend(counts, semiangle=20.0, scan_sampling=0.5, det_sampling=20.0 / 24.0,
                              voltage_kV=300)
+    yield backend, host, kw
+    backend.close()
+
+
+@pytest.mark.parametrize("ab", [
+    so.Aberrations(0.0, 0.0, 0.0),
+    so.Aberrations(-120.0, 55.0, math.radians(17.0)),
+    so.Aberrations(80.0, 30.0, 1.1, C30=3.0e4),
+], ids=["aberration_free", "C10_C12", "C10_C12_C30"])
+def test_production_128x128_det128_end_to_end(production_128, ab):
+    """Selection, G, dc, object phase (1e-4 rad RMS) and the phase-variance
+    loss (1e-5 relative) at 128^4 against the FP64 oracle, with and without
+    aberrations; the C30 case takes the direct (non-factorised) overlap."""
+    backend, host, kw = production_128
     assert 1700 <= backend.num_bf <= 1900
-    rms = _compare(backend, host, kw, so.Aberrations(0.0, 0.0, 0.0), check_loss=False)
+    rms = _compare(backend, host, kw, ab, check_loss=True)
     assert rms < 1e-4
 
 
@@ -121,7 +139,7 @@ def test_ssb_session_fit_recovers_defocus():
     assert res.loss is not None
 
 
-@pytest.mark.parametrize("dose", [1000.0])
+@pytest.mark.parametrize("dose", [50.0, 1000.0, 20000.0])
 def test_stress_256_matches_fp64_gpu_path(dose):
     """256^2 scan x 128^2 detector (2.1 GB u16), defocus 20 nm: the float32
     kernels (Kahan trotter sum) against the FP64 GPU restatement of the oracle,

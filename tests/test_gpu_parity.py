@@ -223,8 +223,9 @@ def test_bbox_gather_wide_detectors(n_frames, det, shuffle):
     64 one-row bands, hence the direct path), 8 x 3072 beyond (five row bands
     of three 928-pixel box rows; a 3648-pixel box row does not fit and takes
     the direct path); and, for outputs beyond 64 MB, the 64-frame gather's
-    704-pixel tiles (a 464-pixel box row per band on 512 columns; the
-    192-column cases above take its 320-pixel tiles)."""
+    704-pixel tiles (a 464-pixel box row per band on 512 columns; its
+    320-pixel tiles are exercised by the 192x192-detector cases of
+    test_bbox_gather_is_bit_exact)."""
     rng = np.random.default_rng(n_frames + det[1])
     k0, k1 = det
     counts = rng.integers(0, 65536, size=(n_frames, k0, k1), dtype=np.uint16)

@@ -177,7 +177,9 @@ def test_backend_class_has_every_protocol_member():
 
 
 def test_reference_protocol_members_match_when_reference_is_present():
-    ref = Path("/root/reference/src")
+    from oracle.ref_cuda.build_ref import reference_root
+
+    ref = reference_root() / "src"
     if not ref.exists():
         pytest.skip("reference checkout not present")
     sys.path.insert(0, str(ref))

@@ -14,7 +14,8 @@ CSRC = ROOT / "quantem" / "gpu_b200" / "csrc"
 
 
 def _fit_module():
-    spec = importlib.util.spec_from_file_location("phase_atan2_fit", CSRC / "phase_atan2_fit.py")
+    spec = importlib.util.spec_from_file_location("phase_atan2_fit",
+                                                  Path(__file__).resolve().parent / "phase_atan2_fit.py")
     mod = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mod)
     return mod
