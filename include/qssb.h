@@ -158,6 +158,24 @@ int qssb_gather_bf_columns_2d(const uint16_t* counts, int64_t n_frames, int32_t 
                               int32_t det_cols, const int32_t* bf_linear, int32_t n_bf,
                               uint16_t* columns, void* stream);
 
+/* Largest count of a whole loaded block of n u8 (elem_bytes 1) or u16
+ * (elem_bytes 2) detector counts, written to the device word *max_out (set
+ * to 0 first, on the stream). Replaces the cp.max(data) that decides whether
+ * the exact BF companion may be narrowed to u8 (engine.py:603-604). */
+int qssb_count_max(const void* counts, int32_t elem_bytes, int64_t n, uint32_t* max_out,
+                   void* stream);
+
+/* Exact BF companion columns: out[b][f] = (out type) counts[f][bf_linear[b]]
+ * for b < n_bf, f < n_scan; counts u8/u16 [n_scan][det_pixels] (in_bytes 1/2),
+ * out u8/u16 [n_bf][n_scan] (out_bytes 1/2). Narrowing u16 to u8 keeps the
+ * low byte, so callers narrow only when qssb_count_max says the block fits.
+ * An index outside [0, det_pixels) writes 0. Replaces the gather_transpose
+ * RawKernel of write_exact_bf_source (engine.py:620-660); callers pass a
+ * chunk's bf_linear + offset and its output rows. */
+int qssb_export_bf_columns(const void* counts, int32_t in_bytes, int64_t n_scan,
+                           int64_t det_pixels, const int32_t* bf_linear, int32_t n_bf, void* out,
+                           int32_t out_bytes, void* stream);
+
 /* Forward scan FFT of each BF image, Hermitian half plane:
  * g_half[b][r][c] = sum_R columns[b][R] exp(-2 pi i (r R_r/R0 + c R_c/R1)),
  * c in [0, R1/2]. Replaces cp.fft.fft2 + the half-plane slice of

@@ -511,13 +511,58 @@ class Prepared:
     geo: Geometry
 
 
+def detect_bf_radius(mean_dp: np.ndarray, threshold_ratio: float = 0.1
+                     ) -> tuple[tuple[int, int], int]:
+    """BF disk centre and half-maximum radius of the mean DP
+    (detector/compute/cuda/probe.py:12-119): centre of mass of the pixels
+    above ``threshold_ratio`` of the maximum, rounded; mean intensity per
+    integer-rounded radius out to the nearest edge; that profile smoothed by a
+    normalised 13-tap Gaussian (sigma 2, edge-padded); the radius is the first
+    bin below half the mean of the first five smoothed bins. Profile sums are
+    taken in FP64 and rounded once (the reference adds float32 atomically, in
+    no fixed order)."""
+    dp = np.asarray(mean_dp, dtype=np.float32)
+    if dp.ndim != 2 or 0 in dp.shape:
+        raise ValueError(f"Expected a non-empty 2D diffraction pattern, got shape {dp.shape}")
+    peak = float(np.nanmax(dp))
+    if not np.isfinite(peak) or peak <= 0:
+        raise ValueError("Diffraction pattern has no positive finite values")
+    above = dp > np.float32(threshold_ratio * peak)
+    if not above.any():
+        raise ValueError("No pixels above threshold")
+    n0, n1 = dp.shape
+    rr, cc = np.nonzero(above)
+    r0 = min(max(int(round(float(np.float32(rr.mean())))), 0), n0 - 1)
+    c0 = min(max(int(round(float(np.float32(cc.mean())))), 0), n1 - 1)
+    edge = min(r0, c0, n0 - r0, n1 - c0)
+    if edge < 2:
+        return (r0, c0), max(1, min(n0, n1) // 4)
+    dist = np.sqrt(np.add.outer((np.arange(n0) - r0) ** 2, (np.arange(n1) - c0) ** 2).astype(np.float32))
+    ring = np.rint(dist).astype(np.int64).ravel()
+    keep = ring < edge
+    total = np.bincount(ring[keep], weights=dp.ravel()[keep].astype(np.float64), minlength=edge)
+    count = np.bincount(ring[keep], minlength=edge)
+    prof = np.where(count > 0, total / np.maximum(count, 1), total).astype(np.float32)
+    if prof.size <= 5:
+        return (r0, c0), max(1, min(n0, n1) // 4)
+    taps = np.exp(-0.5 * ((np.arange(13, dtype=np.float32) - 6) / np.float32(2.0)) ** 2)
+    taps = (taps / taps.sum()).astype(np.float32)
+    ext = np.concatenate([np.full(6, prof[0]), prof, np.full(6, prof[-1])]).astype(np.float32)
+    smooth = np.array([np.dot(ext[i:i + 13].astype(np.float64), taps[::-1].astype(np.float64))
+                       for i in range(prof.size)], dtype=np.float32)
+    half = 0.5 * float(smooth[:5].mean())
+    low = np.nonzero(smooth < half)[0]
+    radius = int(low[0]) if low.size else prof.size // 2
+    return (r0, c0), max(1, radius)
+
+
 def prepare(
     data: np.ndarray,
     *,
     voltage_kV: float,
     semiangle_mrad: float,
     scan_sampling: float | tuple[float, float],
-    det_sampling: float | tuple[float, float],
+    det_sampling: float | tuple[float, float] | None,
     bf_intensity_threshold: float = 0.0,
     bf_radius: float | None = None,
     rotation_rad: float = 0.0,
@@ -535,11 +580,15 @@ def prepare(
         data = pad_or_crop_scan(data)
     if isinstance(scan_sampling, (int, float)):
         scan_sampling = (float(scan_sampling), float(scan_sampling))
-    if isinstance(det_sampling, (int, float)):
-        det_sampling = (float(det_sampling), float(det_sampling))
     lam = wavelength_angstrom(voltage_kV)
     det = (int(data.shape[2]), int(data.shape[3]))
     sums, mean_dp = mean_dp_u64(data)
+    if det_sampling is None:
+        # backend.py:276-285: det_sampling = 2 alpha / r from the detected radius
+        _, radius = detect_bf_radius(mean_dp)
+        det_sampling = (2.0 * semiangle_mrad) / radius
+    if isinstance(det_sampling, (int, float)):
+        det_sampling = (float(det_sampling), float(det_sampling))
     bf = select_bright_field(mean_dp, bf_intensity_threshold, bf_radius)
     g_half, dc = scan_fft_half(data, bf.rows, bf.cols)
     recip = (det_sampling[0] * 1e-3 / lam, det_sampling[1] * 1e-3 / lam)
@@ -576,3 +625,22 @@ def wrapped_phase_error(a: np.ndarray, b: np.ndarray) -> np.ndarray:
     tests/test_ssb_mps_cuda_reference.py:2016-2027.
     """
     return np.angle(np.exp(1j * (np.asarray(a, np.float64) - np.asarray(b, np.float64))))
+
+
+def bf_companion(data: np.ndarray, rows: np.ndarray, cols: np.ndarray) -> tuple[str, bytes]:
+    """The exact bright-field companion file (engine.py:577-701): suffix and
+    bytes of the selected BF pixels' counts, BF-major ``[bf, scan]``.
+
+    u8/u16 counts only (``TypeError`` otherwise, engine.py:598-602); u16 is
+    narrowed to u8 only when the largest count of the whole block is at most
+    255 (engine.py:603-604); BF order is the selection's (row-major).
+    """
+    data = np.asarray(data)
+    if data.dtype not in (np.uint8, np.uint16):
+        raise TypeError(f"Exact CUDA BF-source export supports uint8 or uint16 counts; got {data.dtype}.")
+    out_dtype = np.uint8 if int(data.max()) <= 255 else np.uint16
+    plane = data.shape[0] * data.shape[1]
+    flat = data.reshape(plane, data.shape[2] * data.shape[3])
+    lin = np.asarray(rows, np.int64) * data.shape[3] + np.asarray(cols, np.int64)
+    cols_bf = np.ascontiguousarray(flat[:, lin].T).astype(out_dtype)
+    return (".u8" if out_dtype == np.uint8 else ".u16"), cols_bf.tobytes()

@@ -116,6 +116,8 @@ SIGNATURES = {
     "qssb_bf_geometry": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, ctypes.POINTER(GeometryParams),
                                         _P, _P]),
     "qssb_scan_fft_half": (ctypes.c_int, [_P, _I32, _I32, _I32, _P, _P]),
+    "qssb_count_max": (ctypes.c_int, [_P, _I32, _I64, _P, _P]),
+    "qssb_export_bf_columns": (ctypes.c_int, [_P, _I32, _I64, _I64, _P, _I32, _P, _I32, _P]),
     "qssb_object_workspace_bytes": (
         ctypes.c_int, [ctypes.POINTER(Calibration), _I32, ctypes.POINTER(_SZ)]),
     "qssb_object": (ctypes.c_int, [

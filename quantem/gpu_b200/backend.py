@@ -77,6 +77,23 @@ def _as_device_counts(data, device: torch.device) -> torch.Tensor:
     return t.contiguous()
 
 
+def _as_device_counts_exact(data, device: torch.device) -> torch.Tensor:
+    """Counts on ``device`` in their own u8/u16 type (no widening), as the
+    exact BF companion writer needs them (engine.py:591-602)."""
+    if isinstance(data, np.ndarray):
+        dtype = data.dtype
+        t = torch.from_numpy(np.ascontiguousarray(data)) if dtype in (np.uint8, np.uint16) else None
+    elif isinstance(data, torch.Tensor):
+        dtype, t = data.dtype, data
+    else:
+        raise TypeError("data must be a numpy array or a torch tensor")
+    if t is None or t.dtype not in (torch.uint8, torch.uint16):
+        raise TypeError(f"Exact CUDA BF-source export supports uint8 or uint16 counts; got {dtype}.")
+    if not t.is_cuda or t.device != device:
+        t = t.to(device)
+    return t
+
+
 _FREQ_CACHE: dict = {}
 
 
@@ -522,7 +539,8 @@ class B200SSBBackend:
             phase = self.reconstruct_full(mags, angs)
             obj = torch.polar(torch.ones_like(phase), phase)
         else:
-            obj = self.reconstruct_object(C10, C12, phi12)
+            with self._oom_as_memory_error("reconstruction"):
+                obj = self.reconstruct_object(C10, C12, phi12)
         loss = None
         if compute_loss and not higher and self._scan_shape[0] in LOSS_SCAN_SIZES:
             try:
@@ -607,24 +625,99 @@ class B200SSBBackend:
             dc_value=complex(self.dc_value),
         )
 
+    _EXPORT_CHUNK_BF = 256  # BF pixels per device chunk (engine.py:662)
+
     def export_brightfield(self, data, path_stem) -> tuple[Path, float]:
-        """Exact BF detector counts, BF-major [bf, scan] (engine.py:577-701)."""
+        """Write the exact detector counts of the selected BF pixels, BF-major
+        ``[bf, scan]``, to ``path_stem`` + ``.u8`` or ``.u16``; returns the path
+        and the seconds it took (backend.py:693-702, engine.py:577-701).
+
+        The rules are the reference's: u8 or u16 counts only (``TypeError``
+        otherwise); the data must have the engine's scan shape (``ValueError``);
+        u16 is narrowed to u8 only when the largest count of the WHOLE block -
+        not just of the BF pixels - is at most 255. The device gathers and
+        transposes 256 BF pixels at a time (``qssb_export_bf_columns``) into
+        one of two pinned host buffers while a writer thread appends the
+        previous chunk to the file.
+        """
+        from concurrent.futures import ThreadPoolExecutor
+
         start = time.perf_counter()
-        counts = _as_device_counts(data, self.device)
-        if counts.ndim != 4 or tuple(counts.shape[:2]) != self.scan_shape:
-            raise ValueError(f"BF-source data must match the engine scan shape {self.scan_shape}.")
-        columns = ops.gather_bf_columns(counts, self._bf_linear)
-        max_value = int(columns.max().item()) if columns.numel() else 0
-        host = columns.cpu().numpy()
-        out = host.astype(np.uint8) if max_value <= 255 else host
-        suffix = ".u8" if out.dtype == np.uint8 else ".u16"
-        path = Path(path_stem).with_suffix(suffix).expanduser().resolve()
+        counts = _as_device_counts_exact(data, self.device)
+        if counts.ndim != 4 or tuple(int(v) for v in counts.shape[:2]) != self.scan_shape:
+            raise ValueError(
+                "CUDA BF-source data must match the engine scan shape; "
+                f"got {tuple(counts.shape)}, expected {self.scan_shape} + detector.")
+        counts = counts.contiguous()
+        max_value = int(ops.count_max(counts).cpu()[0]) & 0xFFFFFFFF
+        out_dtype = np.dtype(np.uint8 if max_value <= 255 else np.uint16)
+        torch_out = torch.uint8 if out_dtype == np.uint8 else torch.uint16
+        path = Path(path_stem).with_suffix(".u8" if out_dtype == np.uint8 else ".u16")
+        path = path.expanduser().resolve()
         path.parent.mkdir(parents=True, exist_ok=True)
-        out.tofile(path)
-        self._bf_source = (path, out.dtype, max_value)
-        return path, time.perf_counter() - start
+        path.unlink(missing_ok=True)
+
+        num_bf = self.num_bf
+        plane = int(self.scan_shape[0] * self.scan_shape[1])
+        cap = max(1, min(num_bf, self._EXPORT_CHUNK_BF))
+        row_bytes = plane * out_dtype.itemsize
+        device_cols = torch.empty((cap, plane), dtype=torch_out, device=self.device)
+        host = [torch.empty((cap, row_bytes), dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+        pending = [None, None]
+        stream = torch.cuda.current_stream(self.device)
+        with path.open("wb") as fh, ThreadPoolExecutor(max_workers=1) as writer:
+            for chunk, off in enumerate(range(0, num_bf, cap)):
+                slot = chunk % 2
+                if pending[slot] is not None:
+                    pending[slot].result()
+                n = min(cap, num_bf - off)
+                ops.export_bf_columns(counts, self._bf_linear[off:off + n], device_cols[:n])
+                host[slot][:n].copy_(device_cols[:n].view(torch.uint8), non_blocking=True)
+                done = torch.cuda.Event()
+                done.record(stream)
+                done.synchronize()
+                pending[slot] = writer.submit(host[slot][:n].numpy().tofile, fh)
+            for fut in pending:
+                if fut is not None:
+                    fut.result()
+        self._bf_source = (path, out_dtype, max_value)
+        self.bf_source_write_seconds = time.perf_counter() - start
+        return path, self.bf_source_write_seconds
 
     # ------------------------------------------------------------ fitting
+    @contextmanager
+    def _oom_as_memory_error(self, stage: str):
+        """A device allocation failure inside ``stage`` becomes the reference's
+        actionable ``MemoryError`` (backend.py:808-816, :1078-1086)."""
+        try:
+            yield
+        except torch.cuda.OutOfMemoryError:
+            free_gb = torch.cuda.mem_get_info(self.device)[0] / 1e9
+            raise MemoryError(
+                f"Out of GPU VRAM during SSB {stage} "
+                f"({self.num_bf} BF pixels, {free_gb:.1f} GB free).\n"
+                f"Try: SSB(..., bf_radius=<smaller>) to reduce BF pixel count, "
+                f"or restart the kernel to free stale GPU memory."
+            ) from None
+
+    def _evaluate_retrying(self, x: np.ndarray, verbose: bool = False) -> np.ndarray:
+        """Losses of a candidate batch; on a device allocation failure, free the
+        loss workspace and the allocator's cached blocks and score the batch
+        in halves (the reference halves its BF chunk, backend.py:1347-1354;
+        the B200 loss workspace scales with the candidate count instead)."""
+        try:
+            return self._evaluate(x)
+        except torch.cuda.OutOfMemoryError:
+            if len(x) <= 1:
+                raise
+            self._workspace.release()
+            torch.cuda.empty_cache()
+            half = (len(x) + 1) // 2
+            if verbose:
+                print(f"  OOM - retrying with {half}-candidate batches")
+            return np.concatenate([self._evaluate_retrying(x[:half], verbose),
+                                   self._evaluate_retrying(x[half:], verbose)])
+
     def _evaluate(self, x: np.ndarray) -> np.ndarray:
         x = np.atleast_2d(np.asarray(x, dtype=np.float64))
         return self.variance_loss_batch(x[:, 0], x[:, 1], x[:, 2]).double().cpu().numpy()
@@ -640,8 +733,9 @@ class B200SSBBackend:
             raise NotImplementedError("rotation search is not supported by the B200 sweep")
         ranges = dict(self._DEFAULT_OPTIMIZE_RANGES) if aberrations is None else dict(aberrations)
         keys, lo, hi = search_box(ranges, self.aberrations)
-        best_x, best_f, xs, fs = batch_sweep(self._evaluate, lo, hi, int(n_trials), seed=seed,
-                                             batch=self._SWEEP_BATCH)
+        with self._oom_as_memory_error("optimization"):
+            best_x, best_f, xs, fs = batch_sweep(self._evaluate, lo, hi, int(n_trials), seed=seed,
+                                                 batch=self._SWEEP_BATCH)
         self._optuna_trials = [
             {"params": {"C10_nm": float(x[0]), "C12_nm": float(x[1]), "phi12_deg": math.degrees(x[2])},
              "loss": float(f)} for x, f in zip(xs, fs)
@@ -666,7 +760,8 @@ class B200SSBBackend:
                 f"(locked: {', '.join(sorted(lock))})."
             )
         x0 = np.array([self.aberrations["C10"], self.aberrations["C12"], self.aberrations["phi12"]])
-        best_x, best_f, nfev = batch_nelder_mead(self._evaluate, x0, xatol=xatol, fatol=fatol)
+        with self._oom_as_memory_error("refinement"):
+            best_x, best_f, nfev = batch_nelder_mead(self._evaluate, x0, xatol=xatol, fatol=fatol)
         for i, k in enumerate(("C10", "C12", "phi12")):
             self.aberrations[k] = float(best_x[i])
         self._best_loss = best_f
@@ -689,7 +784,9 @@ class B200SSBBackend:
         p_deg = math.degrees(self.aberrations["phi12"])
         phi = np.radians(np.linspace(p_deg - hw["phi12_deg"], p_deg + hw["phi12_deg"], npts["phi12_deg"]))
         grid = np.array(np.meshgrid(c10, c12, phi, indexing="ij")).reshape(3, -1).T
-        losses = np.concatenate([self._evaluate(grid[s:s + 256]) for s in range(0, len(grid), 256)])
+        with self._oom_as_memory_error("grid search"):
+            losses = np.concatenate([self._evaluate_retrying(grid[s:s + 256], verbose)
+                                     for s in range(0, len(grid), 256)])
         best = int(np.argmin(losses))
         self.aberrations.update(C10=float(grid[best, 0]), C12=float(grid[best, 1]), phi12=float(grid[best, 2]))
         self._best_loss = float(losses[best])

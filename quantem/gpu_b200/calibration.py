@@ -87,7 +87,10 @@ def select_bf(mean_dp: np.ndarray, threshold: float = 0.0,
 
 def detect_bf_radius(mean_dp: np.ndarray, threshold_ratio: float = 0.1
                      ) -> tuple[tuple[int, int], int]:
-    """Half-max radius of the smoothed radial profile of the BF disk."""
+    """BF disk centre and half-max radius of the smoothed radial profile
+    (detector/compute/cuda/probe.py:12-119), on the host copy of the 64 KB
+    mean pattern; the backend sets det_sampling = 2 alpha / r from it
+    (backend.py:276-285)."""
     dp = np.asarray(mean_dp, dtype=np.float32)
     if dp.ndim != 2 or 0 in dp.shape:
         raise ValueError(f"Expected a non-empty 2D diffraction pattern, got {dp.shape}")
@@ -95,6 +98,10 @@ def detect_bf_radius(mean_dp: np.ndarray, threshold_ratio: float = 0.1
     if not np.isfinite(dp_max) or dp_max <= 0:
         raise ValueError("Diffraction pattern has no positive finite values.")
     mask = dp > threshold_ratio * dp_max
+    if not mask.any():
+        raise ValueError(
+            f"No pixels above threshold ({threshold_ratio:.0%} of max intensity). "
+            "The diffraction pattern may be too noisy or empty.")
     mask_f = mask.astype(np.float32)
     total = float(mask_f.sum())
     n0, n1 = dp.shape

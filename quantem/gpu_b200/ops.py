@@ -30,6 +30,8 @@ LAUNCHES_PER_CALL = {
     "qssb_fourier_shift": 3,
     "qssb_join_object_waves": 1,
     "qssb_phase_atan2": 1,
+    "qssb_count_max": 1,
+    "qssb_export_bf_columns": 1,
 }
 LAUNCH_COUNT = 0
 _PROFILE: list | None = None
@@ -251,6 +253,43 @@ def gather_bf_columns(counts: torch.Tensor, bf_linear: torch.Tensor, validate: b
     _call("qssb_gather_bf_columns_2d", counts.device, _ptr(counts), n_frames, k0, k1,
           _ptr(bf_linear), n_bf, _ptr(out), _stream(counts))
     return out
+
+
+_COUNT_BYTES = {torch.uint8: 1, torch.uint16: 2}
+
+
+def count_max(counts: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """Largest count of a u8/u16 CUDA block, as a device int32 scalar-like [1]
+    tensor holding the u32 result (read it with ``int(t[0])``)."""
+    if not isinstance(counts, torch.Tensor) or not counts.is_cuda:
+        raise ValueError("counts must be a CUDA tensor (the SSB engine has no CPU path)")
+    if counts.dtype not in _COUNT_BYTES:
+        raise TypeError(f"counts must be uint8 or uint16, got {counts.dtype}")
+    if not counts.is_contiguous():
+        raise ValueError("counts must be contiguous")
+    if out is None:
+        out = torch.empty(1, dtype=torch.int32, device=counts.device)
+    _call("qssb_count_max", counts.device, _ptr(counts), _COUNT_BYTES[counts.dtype],
+          counts.numel(), _ptr(out), _stream(counts))
+    return out
+
+
+def export_bf_columns(counts: torch.Tensor, bf_linear: torch.Tensor, out: torch.Tensor) -> None:
+    """out[b, f] = counts[f, bf_linear[b]] for the ``out.shape[0]`` BF pixels of
+    ``bf_linear`` (u8/u16 in, u8/u16 out; narrowing keeps the low byte)."""
+    if counts.dtype not in _COUNT_BYTES or out.dtype not in _COUNT_BYTES:
+        raise TypeError("counts and out must be uint8 or uint16")
+    for t, name in ((counts, "counts"), (out, "out")):
+        if not t.is_cuda or not t.is_contiguous():
+            raise ValueError(f"{name} must be a contiguous CUDA tensor")
+    _require_cuda(bf_linear, "bf_linear", torch.int32)
+    det = int(counts.shape[-2]) * int(counts.shape[-1])
+    n_scan = counts.numel() // det
+    n_bf = int(out.shape[0])
+    if out.ndim != 2 or out.shape[1] != n_scan or bf_linear.numel() < n_bf:
+        raise ValueError("out must be [n_bf, n_scan] with n_bf <= len(bf_linear)")
+    _call("qssb_export_bf_columns", counts.device, _ptr(counts), _COUNT_BYTES[counts.dtype],
+          n_scan, det, _ptr(bf_linear), n_bf, _ptr(out), _COUNT_BYTES[out.dtype], _stream(counts))
 
 
 def scan_fft_half(columns: torch.Tensor, scan_shape: tuple[int, int]) -> torch.Tensor:

@@ -66,6 +66,10 @@ class ShimArray(np.ndarray):
     def set(self, arr):
         self[...] = np.asarray(arr)
 
+    @property
+    def device(self):  # CuPy's array.device (numpy's own is the string "cpu")
+        return types.SimpleNamespace(id=0)
+
     def __array_wrap__(self, obj, context=None, return_scalar=False):
         return np.ndarray.__array_wrap__(self, obj, context, False)
 
@@ -103,6 +107,30 @@ class _InertKernel:
         return bytearray(1 << 16)
 
 
+class _GatherTransposeShim:
+    """Stands in for the one RawKernel whose effect the fixtures need: the BF
+    companion writer's ``gather_transpose`` (engine.py:620-660). Its
+    documented effect, for the chunk's BF pixels ``ob < num_bf`` and frames
+    ``s < num_scan``: ``output[ob * num_scan + s] = (out type)
+    input[s * detector_pixels + bf_linear[bf_offset + ob]]``. Everything
+    around it (dtype rule, narrowing on the whole block, file naming, chunk
+    order, writer thread) is the reference's own code."""
+
+    def __call__(self, grid, block, args):
+        inp, bf_linear, out, num_scan, bf_offset, num_bf, det = args
+        src = np.asarray(inp).reshape(int(num_scan), int(det))
+        idx = np.asarray(bf_linear)[int(bf_offset):int(bf_offset) + int(num_bf)]
+        dst = np.asarray(out).reshape(-1)
+        n = int(num_bf) * int(num_scan)
+        dst[:n] = src[:, idx].T.astype(dst.dtype).reshape(-1)
+
+
+def _raw_kernel(code=None, name=None, *args, **kwargs):
+    if name == "gather_transpose":
+        return _GatherTransposeShim()
+    return _InertKernel(code, name, *args, **kwargs)
+
+
 class _Pool:
     def free_all_blocks(self):
         return None
@@ -130,9 +158,11 @@ def build_cupy_shim() -> types.ModuleType:
         "arange", "meshgrid", "nonzero", "sqrt", "arctan2", "cos", "sin",
         "clip", "broadcast_to", "conj", "where", "angle", "mean", "abs",
         "maximum", "minimum", "exp", "divide", "percentile", "zeros_like",
-        "empty_like", "concatenate", "stack", "linspace", "round", "floor",
+        "empty_like", "concatenate", "stack", "linspace", "round", "floor", "max",
+        "nanmax", "any", "rint", "ones_like", "pad", "convolve",
     ):
         setattr(cp, name, _wrap(getattr(np, name)))
+    cp.add = np.add  # the ufunc: probe.py's radial profile uses cp.add.at
     cp.ndarray = ShimArray
     cp.asnumpy = lambda x, *a, **k: np.asarray(x).view(np.ndarray).copy()
     fft = types.ModuleType("cupy.fft")
@@ -141,7 +171,7 @@ def build_cupy_shim() -> types.ModuleType:
     fft.fftfreq = _wrap(np.fft.fftfreq)
     fft.fftshift = _wrap(np.fft.fftshift)
     cp.fft = fft
-    cp.RawKernel = _InertKernel
+    cp.RawKernel = _raw_kernel
     cp.ElementwiseKernel = _InertKernel
     cp.RawModule = _InertKernel
     cp.get_default_memory_pool = lambda: _Pool()
@@ -175,6 +205,12 @@ def install(reference: Path):
     sys.modules["cupy.cuda"] = sys.modules["cupy"].cuda
     sys.path.insert(0, str(reference / "src"))
     sys.path.insert(0, str(reference))
+    # quantem.gpu.detector's __init__ imports the HDF5 reader (h5py, absent
+    # here); the BF-radius detection needs only its compute/cuda/probe module,
+    # whose own package inits import nothing, so register the package bare
+    detector = types.ModuleType("quantem.gpu.detector")
+    detector.__path__ = [str(reference / "src" / "quantem" / "gpu" / "detector")]
+    sys.modules.setdefault("quantem.gpu.detector", detector)
     from quantem.gpu.ssb.compute.cuda.backend import CudaSSBBackend  # noqa: E402
     spec = importlib.util.spec_from_file_location(
         "ref_test_ssb_cuda_128", reference / "tests" / "test_ssb_cuda_128.py"
@@ -185,7 +221,7 @@ def install(reference: Path):
 
 
 sys.path.insert(0, str(HERE))
-from recipes import digest, disk_input, synthetic_plain_32  # noqa: E402
+from recipes import digest, disk_input, export_cases, synthetic_plain_32  # noqa: E402
 
 
 def run_case(CudaSSBBackend, refmod, name: str, data: np.ndarray, kwargs: dict,
@@ -226,11 +262,37 @@ def run_case(CudaSSBBackend, refmod, name: str, data: np.ndarray, kwargs: dict,
     if store_full_g:
         out["g_half_first3"] = g[:3].astype(np.complex64)
         out.update(run_spec(accel, g, aberrations))
+    if kwargs.get("det_sampling") is None:
+        # detected from the mean DP: det_sampling = 2 * semiangle / radius (backend.py:276-285)
+        out["angular_sampling"] = np.asarray(backend.angular_sampling, dtype=np.float64)
     for key in ("semiangle", "scan_sampling", "det_sampling", "voltage_kV", "bf_radius"):
         if kwargs.get(key) is not None:
             out["kw_" + key] = np.asarray(kwargs[key], dtype=np.float64)
     np.savez_compressed(HERE / f"{name}.npz", **out)
     print(f"{name}: B={out['rows'].size} center={tuple(out['center'])} loss={loss:.6g}")
+
+
+def run_export_cases(CudaSSBBackend) -> None:
+    """The reference's exact BF companion writer (engine.py:577-701) on three
+    blocks: u16 counts that fit u8, the same with one hot pixel outside the
+    disk, and u8 counts. Stores the file suffix, size and SHA-256."""
+    import tempfile
+
+    cp = sys.modules["cupy"]
+    kwargs = dict(voltage_kV=300, semiangle=21.4, scan_sampling=0.5, det_sampling=1.0, bf_radius=3)
+    backend = CudaSSBBackend(cp.asarray(disk_input(123)).view(ShimArray), **kwargs)
+    out = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, data in export_cases().items():
+            path, seconds = backend.export_brightfield(cp.asarray(data).view(ShimArray),
+                                                       Path(tmp) / name)
+            raw = Path(path).read_bytes()
+            out[name + "_suffix"] = np.asarray(Path(path).suffix)
+            out[name + "_bytes"] = np.asarray(len(raw))
+            out[name + "_sha256"] = np.asarray(hashlib.sha256(raw).hexdigest())
+            out[name + "_input_sha256"] = np.asarray(digest(data))
+            print(f"export {name}: {Path(path).suffix} {len(raw)} bytes")
+    np.savez_compressed(HERE / "ref_bf_export.npz", **out)
 
 
 def run_spec(accel, g_half: np.ndarray, aberrations) -> dict:
@@ -297,10 +359,29 @@ def main() -> None:
     parser.add_argument("--reference", default=None,
                         help="reference checkout (default: $QSSB_REFERENCE, else the build "
                              "container's checkout)")
+    parser.add_argument("--only", choices=["export", "detect"], default=None,
+                        help="write only the named fixture group")
     args = parser.parse_args()
     global REFERENCE
     REFERENCE = reference_root(args.reference)
     CudaSSBBackend, refmod = install(REFERENCE)
+    if args.only in (None, "export"):
+        run_export_cases(CudaSSBBackend)
+    if args.only in (None, "detect"):
+        # det_sampling=None: the reference detects the BF radius from the mean DP
+        # (detector/compute/cuda/probe.py:12-119) and sets det_sampling = 2 alpha / r
+        run_case(
+            CudaSSBBackend, refmod, "ref_plain32_detect", synthetic_plain_32(),
+            dict(voltage_kV=300, semiangle=20.0, scan_sampling=0.5, det_sampling=None),
+            (50.0, 20.0, 0.3), store_full_g=False,
+        )
+        run_case(
+            CudaSSBBackend, refmod, "ref_disk128_detect", disk_input(123),
+            dict(voltage_kV=300, semiangle=21.4, scan_sampling=0.5, det_sampling=None, bf_radius=3),
+            (-120.0, 55.0, math.radians(17.0)), store_full_g=False,
+        )
+    if args.only is not None:
+        return
 
     ab = (-120.0, 55.0, math.radians(17.0))
     # 1. The reference test's own end-to-end case (explicit bf_radius=3).

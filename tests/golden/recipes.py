@@ -26,6 +26,16 @@ def disk_input(seed: int, scan=(128, 128)) -> np.ndarray:
     return data
 
 
+def export_cases() -> dict[str, np.ndarray]:
+    """Inputs of the exact BF companion fixtures (the disk case above, 128x128
+    scan x 16x16 detector, bf_radius=3): u16 counts that fit u8, the same with
+    one hot pixel outside the BF disk, and the counts as u8."""
+    base = disk_input(123)
+    hot = base.copy()
+    hot[5, 7, 0, 0] = 300  # outside the BF disk: the block no longer fits u8
+    return {"u16_fits_u8": base, "u16_hot_pixel_outside_bf": hot, "u8": base.astype(np.uint8)}
+
+
 def synthetic_plain_32() -> np.ndarray:
     """The CPU-runnable plain workload (32x32 scan, 64x64 detector, u16)."""
     if str(REPO) not in sys.path:

@@ -81,6 +81,35 @@ def test_disk_case_matches_reference_golden():
     assert res.num_bf == 27
 
 
+@pytest.mark.parametrize("name", ["ref_plain32_detect", "ref_disk128_detect"])
+def test_detected_bf_radius_matches_reference(name):
+    """det_sampling=None: the backend detects the BF radius from the mean DP
+    (probe.py:12-119) and sets det_sampling = 2 alpha / r as the reference
+    does (backend.py:276-285, its factor 2 included); angular sampling,
+    selection, G and the reconstruction then follow the reference's golden
+    outputs and the FP64 oracle."""
+    from recipes import synthetic_plain_32
+
+    with np.load(f"tests/golden/{name}.npz") as z:
+        gold = {k: z[k] for k in z.files}
+    counts = synthetic_plain_32() if name == "ref_plain32_detect" else disk_input(123)
+    semi = float(gold["kw_semiangle"])
+    bf_radius = float(gold["kw_bf_radius"]) if "kw_bf_radius" in gold else None
+    backend = B200SSBBackend(torch.as_tensor(counts, device=DEV), semiangle=semi,
+                             scan_sampling=0.5, det_sampling=None, voltage_kV=300,
+                             bf_radius=bf_radius)
+    assert backend.angular_sampling == tuple(gold["angular_sampling"])
+    np.testing.assert_array_equal(backend.bf_inds_row, gold["rows"])
+    np.testing.assert_array_equal(backend.bf_inds_col, gold["cols"])
+    kw = dict(voltage_kV=300, semiangle_mrad=semi, scan_sampling=0.5, det_sampling=None,
+              bf_radius=bf_radius)
+    _compare(backend, counts, kw, so.Aberrations(*map(float, gold["aberrations"])))
+    c10, c12, phi12 = map(float, gold["aberrations"])
+    assert backend.variance_loss(c10, c12, phi12) == pytest.approx(float(gold["loss"]), rel=1e-4,
+                                                                   abs=1e-6)
+    backend.close()
+
+
 def test_uneven_96_scan_is_padded_like_the_reference():
     counts = disk_input(124, scan=(96, 96))
     kw = dict(voltage_kV=300, semiangle_mrad=21.4, scan_sampling=0.5, det_sampling=1.0, bf_radius=3)
