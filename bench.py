@@ -230,7 +230,26 @@ def reference_cuda_baseline(counts: torch.Tensor, be, steps: int, warmup: int) -
     ref_obj = ref.object(*wargs, 0.0, 0.0, 0.0, be.dc_value)
     our_obj, _ = be.object_and_phase(0.0, 0.0, 0.0)
     d = torch.angle(our_obj * torch.conj(ref_obj)).double()
+    del ref
+    loss = {}
+    if build_ref.sums_available():
+        # the reference's batched loss (variance_loss_batch: K12 + K13 over
+        # 1024-pixel BF chunks, K14) on the same G, 64 candidates like ours
+        from oracle.ref_cuda.harness import ReferenceLossBatch128
+
+        rl = ReferenceLossBatch128(dev)
+        c10 = np.linspace(-50.0, 50.0, 64)
+        lfn = lambda: rl.losses(be.G_qk, be._geom_dev, be._q_row, be._q_col,  # noqa: E731
+                                be.wavelength, semi, ang, ang, c10, 0.0, 0.0, be.dc_value)
+        loss_ms = timed(lfn, 3)
+        ours = be.variance_loss_batch(c10, 0.0, 0.0).double()
+        rel = ((lfn().double() - ours).abs() / ours.abs()).max()
+        loss = {"loss_evals_per_s": 64 * 1e3 / loss_ms, "loss_batch64_ms": loss_ms,
+                "loss_max_rel_diff_vs_ours": float(rel)}
+        del rl
+        torch.cuda.empty_cache()
     return {
+        **loss,
         "warm_recon_per_s": 1e3 / warm_ms, "cold_recon_per_s": 1e3 / cold_ms,
         "phase_rms_rad_vs_ours": float(torch.sqrt(torch.mean(d * d))),
         "kind": "reference CUDA kernels ifft128_rows_fused_pk_t32_mr8_packed + ifft128_cols_t32_mr8 "
@@ -855,6 +874,9 @@ def run_b200(args, world, rank, local) -> None:
             line["speedup_vs_reference_cuda"] = {
                 "cold": value / rc["cold_recon_per_s"],
                 "warm": line["warm_recon_per_s"] / rc["warm_recon_per_s"]}
+            if "loss_evals_per_s" in rc:
+                line["speedup_vs_reference_cuda"]["loss_batch64"] = (
+                    line["loss_evals_per_s_batch64"] / rc["loss_evals_per_s"])
     if world == 1 and not args.no_stress:
         line["stress_256"] = stress_256(dev, 5)
         if not args.no_large:

@@ -49,7 +49,18 @@ def reference_root(override: str | Path | None = None) -> Path:
 
 DEFAULT_REFERENCE = reference_root()
 KERNEL_NAMES = ("ifft128_rows_fused_pk_t32_mr8_packed", "ifft128_cols_t32_mr8")
+# the batched phase-variance loss of variance_loss_batch (engine.py:2120-2295):
+# rows + gamma + pk into the staging planes (K12), column IFFTs + atan2 +
+# sum / sum of squares (K13), both in the same module (fft128.py:152-351, 466-549)
+LOSS_KERNEL_NAMES = ("ifft128_rows_fused_pk_batch_t32_mr8_transpose_packed_b4",
+                     "ifft128_rows_var_g32_t32_mr1_batch")
 TWIDDLE_NAME = "TWIDDLE_128"
+# ... and the per-candidate loss from the sums (K14), a RawKernel string of
+# engine.py:96-137, compiled on its own (CuPy's RawKernel defaults: no fast math)
+SUMS_CUBIN = OUT_DIR / "ssb_loss_sums.cubin"
+SUMS_MANIFEST = OUT_DIR / "ssb_loss_sums.json"
+SUMS_KERNEL = "loss_from_sums_batch"
+ENGINE_REL = Path("src/quantem/gpu/ssb/compute/cuda/engine.py")
 
 
 def _string_constants(path: Path, names: set[str]) -> dict[str, str]:
@@ -88,6 +99,55 @@ __global__ void qref_full_chi_probe(
     out[2 * i + 1] = v.y;
 }
 """
+
+
+def _raw_kernel_sources(path: Path, names: set[str]) -> dict[str, str]:
+    """The source strings of module-level ``NAME = cp.RawKernel(r'''...''', ...)``
+    assignments (their first argument)."""
+    tree = ast.parse(path.read_text())
+    found = {}
+    for node in tree.body:
+        if isinstance(node, ast.Assign) and len(node.targets) == 1:
+            tgt = node.targets[0]
+            if isinstance(tgt, ast.Name) and tgt.id in names and isinstance(node.value, ast.Call) \
+                    and node.value.args and isinstance(node.value.args[0], ast.Constant):
+                found[tgt.id] = node.value.args[0].value
+    missing = names - set(found)
+    if missing:
+        raise RuntimeError(f"{path}: RawKernel sources not found: {sorted(missing)}")
+    return found
+
+
+def sums_available() -> bool:
+    return SUMS_CUBIN.exists() and SUMS_MANIFEST.exists()
+
+
+def build_sums(reference: Path = DEFAULT_REFERENCE, force: bool = False, verbose: bool = False
+               ) -> Path | None:
+    """Compile the reference's loss_from_sums_batch kernel into its own cubin."""
+    engine = reference / ENGINE_REL
+    if not engine.exists():
+        return SUMS_CUBIN if sums_available() else None
+    src = _raw_kernel_sources(engine, {"_loss_from_sums_batch_kernel"})["_loss_from_sums_batch_kernel"]
+    digest = hashlib.sha256(src.encode()).hexdigest()
+    if not force and sums_available():
+        if json.loads(SUMS_MANIFEST.read_text()).get("source_sha256") == digest:
+            return SUMS_CUBIN
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    OUT_DIR.mkdir(parents=True, exist_ok=True)
+    with tempfile.TemporaryDirectory() as td:
+        cu = Path(td) / "ssb_loss_sums.cu"
+        cu.write_text(src)
+        cmd = [nvcc, "-cubin", "-gencode", "arch=compute_100a,code=sm_100a", "-std=c++11",
+               "-o", str(SUMS_CUBIN) + ".tmp", str(cu)]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    Path(str(SUMS_CUBIN) + ".tmp").replace(SUMS_CUBIN)
+    SUMS_MANIFEST.write_text(json.dumps({
+        "source_sha256": digest, "reference_files": [str(ENGINE_REL)],
+        "options": "nvcc -cubin sm_100a -std=c++11", "kernels": [SUMS_KERNEL]}, indent=1))
+    return SUMS_CUBIN
 
 
 def module_source(reference: Path) -> str:
@@ -129,7 +189,7 @@ def build(reference: Path = DEFAULT_REFERENCE, force: bool = False, verbose: boo
         "source_sha256": digest,
         "reference_files": [str(KERNELS_REL / "common.py"), str(KERNELS_REL / "fft128.py")],
         "options": "nvcc -cubin sm_100a -std=c++11 --use_fast_math -maxrregcount=96 -Xptxas -dlcm=ca",
-        "kernels": list(KERNEL_NAMES) + [FULL_PROBE_NAME],
+        "kernels": list(KERNEL_NAMES) + list(LOSS_KERNEL_NAMES) + [FULL_PROBE_NAME],
         "twiddle": TWIDDLE_NAME,
     }, indent=1))
     return CUBIN
@@ -141,3 +201,4 @@ if __name__ == "__main__":
     ap.add_argument("--force", action="store_true")
     a = ap.parse_args()
     print(build(a.reference, force=a.force, verbose=True))
+    print(build_sums(a.reference, force=a.force, verbose=True))

@@ -173,3 +173,116 @@ def reference_cold_object(counts: torch.Tensor, ref: ReferenceObject128, *, wave
     obj = ref.object(g_half, geom, q_row, q_col, wavelength, semiangle_mrad * 1e-3,
                      det_sampling_mrad * 1e-3, det_sampling_mrad * 1e-3, C10, C12, phi12, dc)
     return obj, torch.angle(obj), n_bf
+
+
+class ReferenceLossBatch128:
+    """The reference's batched phase-variance loss for 128x128 scans, replayed
+    with its own kernels: ``SSBEngine.variance_loss_batch`` (engine.py:2120-2295)
+    -> the pk element-wise kernel (restated, engine.py:217-231) ->
+    ``ifft2_inplace_batch_fused_pk_variance`` streaming over BF chunks
+    (common.py:1006-1092: K12 ``ifft128_rows_fused_pk_batch_t32_mr8_transpose_packed_b4``
+    on grid (1, 8, quads * chunk) x (32, 16, 1) with 64 KB of dynamic shared
+    memory, then K13 ``ifft128_rows_var_g32_t32_mr1_batch`` on grid
+    (1, 128, ceil(chunk / 32) * batch) x (32, 1, 1) adding into the sums) ->
+    K14 ``loss_from_sums_batch`` (engine.py:96-137) on (batch,) x (256,).
+
+    The BF chunk is the engine's for 128x128 scans: every BF pixel at once when
+    the staging planes (batch x B x 128 x 128 complex64) fit 2 GiB, else
+    min(1024, B) (engine.py:2183-2200, with the memory-derived cap far above
+    1024 on a B200). Batches below 4 are padded with copies of the last
+    candidate (the reference loops them through its scalar path instead).
+    """
+
+    def __init__(self, device: torch.device | str = "cuda:0"):
+        from .build_ref import LOSS_KERNEL_NAMES, SUMS_CUBIN, SUMS_KERNEL, sums_available
+
+        if not (available() and sums_available()):
+            raise FileNotFoundError("reference loss cubins missing: run python -m oracle.ref_cuda.build_ref")
+        self.obj = ReferenceObject128(device)  # loads the module and its twiddles
+        cu = self.obj.cu
+        self.cu = cu
+        self.device = self.obj.device
+        (self.k12,) = _check(cu.cuModuleGetFunction(self.obj.module, LOSS_KERNEL_NAMES[0].encode()))
+        (self.k13,) = _check(cu.cuModuleGetFunction(self.obj.module, LOSS_KERNEL_NAMES[1].encode()))
+        _check(cu.cuFuncSetAttribute(
+            self.k12, cu.CUfunction_attribute.CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, 65536))
+        (self.sums_module,) = _check(cu.cuModuleLoad(str(SUMS_CUBIN).encode()))
+        (self.k14,) = _check(cu.cuModuleGetFunction(self.sums_module, SUMS_KERNEL.encode()))
+        self._bufs: dict = {}
+
+    def _buffers(self, batch: int, n_bf: int, chunk: int) -> dict:
+        key = (batch, n_bf, chunk)
+        if key not in self._bufs:
+            self._bufs.clear()
+            tail = n_bf % chunk
+            dev = self.device
+            self._bufs[key] = {
+                "staging": torch.empty((batch, chunk, N, N), dtype=torch.complex64, device=dev),
+                "tail": (torch.empty((batch, tail, N, N), dtype=torch.complex64, device=dev)
+                         if tail else None),
+                "sum": torch.empty((batch, N, N), dtype=torch.float32, device=dev),
+                "sumsq": torch.empty((batch, N, N), dtype=torch.float32, device=dev),
+                "loss": torch.empty(batch, dtype=torch.float32, device=dev),
+            }
+        return self._bufs[key]
+
+    def losses(self, g_half: torch.Tensor, geom: torch.Tensor, q_row: torch.Tensor,
+               q_col: torch.Tensor, wavelength: float, semiangle_rad: float, ang_y_rad: float,
+               ang_x_rad: float, C10, C12, phi12, dc: complex) -> torch.Tensor:
+        """float32 CUDA [batch] losses of the candidates (C10, C12, phi12 arrays)."""
+        n_bf = int(g_half.shape[0])
+        assert g_half.shape == (n_bf, N, N // 2 + 1) and g_half.dtype == torch.complex64
+        assert geom.shape[0] >= 6 and geom.shape[1] == n_bf
+        c10 = np.atleast_1d(np.asarray(C10, np.float32))
+        n = c10.size
+        c12 = np.broadcast_to(np.asarray(C12, np.float32), (n,))
+        phi = np.broadcast_to(np.asarray(phi12, np.float32), (n,))
+        batch = max(n, 4)
+        pad = lambda a: np.concatenate([a, np.repeat(a[-1:], batch - n)])  # noqa: E731
+        c10, c12, phi = pad(c10), pad(np.array(c12)), pad(np.array(phi))
+        dev = self.device
+        cos2 = np.cos(2.0 * phi).astype(np.float32)
+        sin2 = np.sin(2.0 * phi).astype(np.float32)
+        params = [torch.as_tensor(a, device=dev) for a in (c10, c12, cos2, sin2)]
+        factor = math.pi / wavelength
+        # pk [batch, B] = A(k) exp(-i chi(k)) per candidate (engine.py:217-231)
+        alpha2, c2k, s2k, ak = geom[2], geom[3], geom[4], geom[5]
+        chi = np.float32(factor) * alpha2[None, :] * (
+            params[1][:, None] * (c2k[None, :] * params[2][:, None] + s2k[None, :] * params[3][:, None])
+            + params[0][:, None])
+        pk = torch.complex(ak[None, :] * torch.cos(chi), -ak[None, :] * torch.sin(chi)).contiguous()
+        staging_bytes = batch * n_bf * N * N * 8
+        chunk = n_bf if staging_bytes <= 2 * 1024 ** 3 else min(1024, n_bf)
+        bufs = self._buffers(batch, n_bf, chunk)
+        bufs["sum"].zero_()
+        bufs["sumsq"].zero_()
+        g_half = g_half.contiguous()
+        kx, ky = geom[0].contiguous(), geom[1].contiguous()
+        stream = self.cu.CUstream(torch.cuda.current_stream(dev).cuda_stream)
+        P, F, I = ctypes.c_void_p, ctypes.c_float, ctypes.c_int
+        f32 = lambda x: float(np.float32(x))  # noqa: E731
+        quads = (batch + 3) // 4
+        for start in range(0, n_bf, chunk):
+            cnt = min(chunk, n_bf - start)
+            staging = bufs["staging"] if cnt == chunk else bufs["tail"]
+            pk_group = pk[:, start:start + cnt].contiguous()
+            args = [(kx.data_ptr() + 4 * start, P), (ky.data_ptr() + 4 * start, P),
+                    (q_row.data_ptr(), P), (q_col.data_ptr(), P),
+                    (f32(wavelength), F), (f32(semiangle_rad), F), (f32(ang_y_rad), F),
+                    (f32(ang_x_rad), F), *[(t.data_ptr(), P) for t in params], (f32(factor), F),
+                    (pk_group.data_ptr(), P), (g_half.data_ptr() + 8 * start * N * (N // 2 + 1), P),
+                    (staging.data_ptr(), P), (f32(dc.real), F), (f32(dc.imag), F),
+                    (cnt, I), (batch, I), (N // 2 + 1, I)]
+            _check(self.cu.cuLaunchKernel(self.k12, 1, 8, quads * cnt, 32, 16, 1, 65536, stream,
+                                          (tuple(a[0] for a in args), tuple(a[1] for a in args)), 0))
+            groups = (cnt + 31) // 32
+            args = [(staging.data_ptr(), P), (bufs["sum"].data_ptr(), P),
+                    (bufs["sumsq"].data_ptr(), P), (cnt, I), (batch, I), (f32(1.0 / (N * N)), F),
+                    (0, I)]
+            _check(self.cu.cuLaunchKernel(self.k13, 1, 128, groups * batch, 32, 1, 1, 0, stream,
+                                          (tuple(a[0] for a in args), tuple(a[1] for a in args)), 0))
+        args = [(bufs["sum"].data_ptr(), P), (bufs["sumsq"].data_ptr(), P),
+                (bufs["loss"].data_ptr(), P), (n_bf, I), (N, I), (N, I), (batch, I)]
+        _check(self.cu.cuLaunchKernel(self.k14, batch, 1, 1, 256, 1, 1, 0, stream,
+                                      (tuple(a[0] for a in args), tuple(a[1] for a in args)), 0))
+        return bufs["loss"][:n]

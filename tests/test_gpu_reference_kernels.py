@@ -88,3 +88,37 @@ def test_reference_cold_path_matches_ours(production):
     ours, theirs = ours.cpu().numpy(), ph.cpu().numpy()
     assert _rms(theirs, fp64) <= 1e-3
     assert _rms(ours, theirs) <= _rms(theirs, fp64) + _rms(ours, fp64) + 1e-6
+
+
+@pytest.mark.skipif(not build_ref.sums_available(), reason="oracle/_ref/ssb_loss_sums.cubin not built")
+def test_loss_batch_matches_reference_cuda_kernels(production):
+    """The reference's batched phase-variance loss (its K12 rows + gamma + pk
+    kernel, its K13 column + atan2 + sums kernel streaming over 1024-pixel BF
+    chunks, its K14 loss-from-sums kernel) on our resident G, against ours and
+    the FP64 oracle, for 16 candidates at 128^4 (their staging planes exceed
+    2 GiB, so the engine streams two BF chunks: 1024 + the 757-pixel tail).
+    The reference sums float32 phases with float32 atomics; ours sits within
+    1e-5 and its within 1e-4 relative of the oracle."""
+    from oracle.ref_cuda.harness import ReferenceLossBatch128
+
+    be, _, kw, _, prep = production
+    rng = np.random.default_rng(4)
+    c10 = rng.uniform(-150.0, 150.0, 16)
+    c12 = rng.uniform(0.0, 60.0, 16)
+    phi = rng.uniform(-np.pi / 2, np.pi / 2, 16)
+    c10[0], c12[0], phi[0] = -120.0, 55.0, math.radians(17.0)
+    semi, ang = kw["semiangle"] * 1e-3, kw["det_sampling"] * 1e-3
+    ref = ReferenceLossBatch128(DEV)
+    theirs = ref.losses(be.G_qk, be._geom_dev, be._q_row, be._q_col, be.wavelength, semi, ang,
+                        ang, c10, c12, phi, be.dc_value).cpu().numpy().astype(np.float64)
+    ours = be.variance_loss_batch(c10, c12, phi).cpu().numpy().astype(np.float64)
+    for i in (0, 3):
+        want, _ = so.phase_variance_loss(prep.g_half, prep.geo,
+                                         so.Aberrations(c10[i], c12[i], phi[i]), prep.dc)
+        assert abs(ours[i] - want) <= 1e-5 * abs(want), (i, ours[i], want)
+        assert abs(theirs[i] - want) <= 1e-4 * abs(want), (i, theirs[i], want)
+    np.testing.assert_allclose(theirs, ours, rtol=2e-4)
+    # a batch below 4 candidates is padded like the reference's minimum batch
+    two = ref.losses(be.G_qk, be._geom_dev, be._q_row, be._q_col, be.wavelength, semi, ang, ang,
+                     c10[:2], c12[:2], phi[:2], be.dc_value).cpu().numpy()
+    np.testing.assert_allclose(two, theirs[:2], rtol=1e-5)
