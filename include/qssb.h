@@ -257,6 +257,33 @@ int qssb_loss_batch(const float* g_half, const float* bf_geom, const float* q_ro
                     void* workspace, size_t workspace_bytes, float* losses,
                     float* mean_phase, void* stream);
 
+/* Bytes of the overlap table of a 128x128-scan dataset: float2 [n_bf][8383]. */
+int qssb_overlap_table_bytes(const qssb_calibration_t* cal, size_t* bytes);
+
+/* The candidate-independent part of the quadratic-chi overlap of a 128x128
+ * dataset: table[b][e] = A(k_b) (A(q - k_b) - A(q + k_b), A(q - k_b) + A(q + k_b))
+ * on the half set the loss evaluates (rows 0..64 x all columns, then
+ * (127 - j, 64) for j < 63), with the loss kernels' aperture rule (FP64 where
+ * the two apertures tie in the soft edge). The reference recomputes these
+ * apertures for every candidate inside gamma_mul_pk_onthefly
+ * (common.py:115-236); computing them once per dataset is this engine's own
+ * step. Depends on the geometry only: rebuild after cache_rotation. */
+int qssb_overlap_table(const float* bf_geom, const float* q_row, const float* q_col,
+                       const qssb_calibration_t* cal, float* table, void* stream);
+
+/* qssb_loss_batch with an optional overlap table (NULL: as qssb_loss_batch).
+ * With a table, 128x128 scans and QSSB_FLAG_QUADRATIC (C30 == 0), the loss
+ * runs two BF pixels per inverse 2D FFT (their anti-Hermitian parts packed
+ * as one complex plane, the Hermitian DC and Nyquist-line parts transformed
+ * on their own) from table reads; the workspace is the same. The reduction
+ * order is fixed for a given plan; the result differs from the table-free
+ * path by float32 rounding only. */
+int qssb_loss_batch_ex(const float* g_half, const float* bf_geom, const float* q_row,
+                       const float* q_col, const qssb_calibration_t* cal,
+                       const qssb_aberrations_t* candidates, int32_t n_cand, int32_t flags,
+                       const float* overlap, void* workspace, size_t workspace_bytes,
+                       float* losses, float* mean_phase, void* stream);
+
 /* The phase function of qssb_loss_batch and qssb_loss_batch_full:
  * out[i] = atan2(y[i], x[i]) by an octant reduction and a degree-17 odd
  * polynomial, |error| <= 4e-7 rad against IEEE atan2 for finite

@@ -425,14 +425,29 @@ class B200SSBBackend:
                                self._calibration(), Aberrations(C10, C12, phi12, C30),
                                flags=self._object_flags(), workspace=self._workspace)
 
+    # the 128x128 loss evaluates the candidate-independent overlap apertures
+    # once per geometry (qssb_overlap_table) instead of once per candidate
+    use_overlap_table = True
+
+    def _overlap_table(self) -> torch.Tensor | None:
+        if not self.use_overlap_table or self._scan_shape != (128, 128):
+            return None
+        if getattr(self, "_overlap_geom", None) is not self._geom_dev:
+            self._overlap = ops.overlap_table(self._geom_dev, self._q_row, self._q_col,
+                                              self._calibration())
+            self._overlap_geom = self._geom_dev
+        return self._overlap
+
     def variance_loss_batch(self, C10, C12, phi12, C30=None) -> torch.Tensor:
         """Phase-variance losses (float32 CUDA [n]) for a candidate batch."""
         self._require_loss_size()
         cands = self._candidates(C10, C12, phi12, C30)
-        flags = self._flags | (QSSB_FLAG_QUADRATIC if C30 is None or not np.any(np.asarray(C30)) else 0)
+        quad = C30 is None or not np.any(np.asarray(C30))
+        flags = self._flags | (QSSB_FLAG_QUADRATIC if quad else 0)
         losses, _ = ops.loss_batch(self.G_qk, self._geom_dev, self._q_row, self._q_col,
                                    self._calibration(), cands, flags=flags,
-                                   workspace=self._workspace)
+                                   workspace=self._workspace,
+                                   overlap=self._overlap_table() if quad else None)
         return losses
 
     def variance_loss(self, C10: float, C12: float, phi12: float) -> float:
@@ -445,7 +460,8 @@ class B200SSBBackend:
         losses, mp = ops.loss_batch(self.G_qk, self._geom_dev, self._q_row, self._q_col,
                                     self._calibration(), cands,
                                     flags=self._flags | QSSB_FLAG_QUADRATIC,
-                                    workspace=self._workspace, want_mean_phase=True)
+                                    workspace=self._workspace, want_mean_phase=True,
+                                    overlap=self._overlap_table())
         return mp[0], float(losses[0])
 
     def reconstruct(self, C10: float, C12: float, phi12: float) -> torch.Tensor:
@@ -809,6 +825,7 @@ class B200SSBBackend:
     def free(self) -> None:
         self.G_qk = None
         self._geom_dev = None
+        self._overlap = self._overlap_geom = None
         self._workspace.release()
 
     def close(self) -> None:

@@ -458,6 +458,391 @@ __global__ void __launch_bounds__(256) k_loss_final(const double* __restrict__ b
     if (threadIdx.x == 0) losses[cand] = (float)(red[0] / (double)npos);
 }
 
+// ---------------------------------------- N = 128 with the overlap table
+// For quadratic chi the overlap factorises (corrected_quad in
+// qssb_device.cuh): C_b(q) = G_b(q) e^{-i theta} (d cos Q + i s sin Q) / |.|,
+// where theta = 2 q^T M k_b and Q(q) depend on the candidate but
+//   (d, s) = A(k_b) (A(q - k_b) - A(q + k_b), A(q - k_b) + A(q + k_b))
+// does not. k_overlap_table128 evaluates (d, s) once per dataset on the
+// evaluated half set (rows 0..64 x 128 columns, then (127 - j, 64), j < 63),
+// with the kernels' aperture arithmetic and FP64 tie rule, so a candidate
+// costs a table read, a separable phase product and one reciprocal square
+// root per element.
+constexpr int kNE128 = 65 * 128 + 63;
+
+__device__ __forceinline__ void elem_rc128(int e, int& r, int& c) {
+    if (e < 65 * 128) {
+        r = e >> 7;
+        c = e & 127;
+    } else {
+        r = 127 - (e - 65 * 128);  // 127 .. 65
+        c = 64;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_overlap_table128(
+    const float* __restrict__ geom, int n_bf, const float* __restrict__ q_row,
+    const float* __restrict__ q_col, Probe p, float2* __restrict__ table) {
+    const int e = blockIdx.x * 256 + threadIdx.x;
+    const int b = blockIdx.y;
+    if (e >= kNE128 || b >= n_bf) return;
+    int r, c;
+    elem_rc128(e, r, c);
+    const float kx = __ldg(geom + b);
+    const float ky = __ldg(geom + n_bf + b);
+    const float ak = __ldg(geom + 5 * n_bf + b);
+    const float qx = __ldg(q_row + r);
+    const float qy = __ldg(q_col + c);
+    const float dxm = qx - kx, dym = qy - ky;
+    const float dxp = qx + kx, dyp = qy + ky;
+    const float r2m = fmaf(dxm, dxm, dym * dym);
+    const float r2p = fmaf(dxp, dxp, dyp * dyp);
+    float am = soft_aperture_fast(dxm, dym, r2m, p);
+    float ap = soft_aperture_fast(dxp, dyp, r2p, p);
+    if (fabsf(am - ap) < kApertureTie && (in_edge_band(r2m, p) || in_edge_band(r2p, p))) {
+        const double qx64 = fftfreq_d(r, p.n_r, p.qval_r);
+        const double qy64 = fftfreq_d(c, p.n_c, p.qval_c);
+        const double kx64 = (double)kx + (double)__ldg(geom + 6 * n_bf + b);
+        const double ky64 = (double)ky + (double)__ldg(geom + 7 * n_bf + b);
+        am = soft_aperture_fp64(qx64 - kx64, qy64 - ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
+        ap = soft_aperture_fp64(qx64 + kx64, qy64 + ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
+    }
+    table[(size_t)b * kNE128 + e] = make_float2(ak * (am - ap), ak * (am + ap));
+}
+
+// C = G conj(Gamma_hat) from the table entry ds = (d, s), e^{-i Q} = eq and
+// e^{i theta} = e (corrected_quad_e with A(k) folded into ds).
+__device__ __forceinline__ float2 corrected_table(float2 ds, float2 eq, float2 e, float2 g) {
+    const float dr = ds.x * eq.x;
+    const float di = -ds.y * eq.y;
+    float gr = fmaf(e.x, dr, -e.y * di);
+    float gi = fmaf(e.x, di, e.y * dr);
+    const float m2 = fmaf(gr, gr, gi * gi);
+    const float inv = m2 > 1e-16f ? rsqrtf(m2) : 1e8f;
+    gr *= inv;
+    gi *= inv;
+    return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
+}
+
+// Two BF pixels per inverse 2D FFT. Split each corrected spectrum into its
+// anti-Hermitian part A (C(-q) = -conj C(q): every scan frequency off the
+// Nyquist row and column, where the evaluated half set defines the other
+// half) and its Hermitian part E (DC and the two Nyquist lines). Then
+// IFFT2(A) = i a and IFFT2(E) = e with a, e real, so O_b = e_b + i a_b and
+// phi_b = atan2(a_b, e_b). The two pixels' A share one complex transform,
+//   S = A_2 - i A_1,  IFFT2(S) = a_1 + i a_2,
+// and E_b, nonzero on two lines only, gives
+//   e_b(y, x) = Re dc + (-1)^y E^row_b(x) + (-1)^x E^col_b(y)
+// from two 128-point transforms (one complex line per pixel: E^row + i E^col).
+// Per pixel pair: 2 x 8383 table evaluations, 128 row and 128 column FFTs
+// (the one-pixel kernel: 65 + 128 per pixel) and no shared-memory moments:
+// phi^2 is summed per thread in FP64 (the loss needs only its total, since
+// mean_R (1/B) sum_b phi_b^2 = (1/(N^2 B)) sum_{R,b} phi_b^2), phi per pixel
+// in registers as before.
+struct Pair128Smem {
+    static constexpr size_t s = sizeof(float2) * 128 * kL128P;    // packed plane S
+    static constexpr size_t t = sizeof(float2) * 64 * kG8Scratch;  // group transposes
+    static constexpr size_t tw = sizeof(float2) * 128;
+    static constexpr size_t ph = sizeof(float2) * 2 * 256;    // [bf][e^{2i q_r u} | e^{2i q_c v}]
+    static constexpr size_t ny = sizeof(float2) * 2 * 256;    // [bf][row 64 | column 64]: C, then A
+    static constexpr size_t eb = sizeof(float2) * 2 * 256;    // [bf][E row | E col]
+    static constexpr size_t el = sizeof(float) * 2 * 256;     // [bf][E^row(x) | E^col(y)]
+    static constexpr size_t bytes = s + t + tw + ph + ny + eb + el;
+};
+
+template <bool CHI64>
+__global__ void __launch_bounds__(512, 1) k_loss_pair128(
+    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
+    const float* __restrict__ q_row, const float* __restrict__ q_col,
+    const float2* __restrict__ overlap, const qssb_aberrations_t* __restrict__ cands,
+    qssb_calibration_t cal, const float2* __restrict__ eq_table, int bf_per_chunk, int n_chunks,
+    float* __restrict__ part, double* __restrict__ part_sq) {
+    constexpr int N = 128;
+    constexpr int H = N / 2 + 1;
+    constexpr int P = kL128P;
+    extern __shared__ float4 smem4[];
+    char* base = reinterpret_cast<char*>(smem4);
+    float2* S = reinterpret_cast<float2*>(base);
+    float2* T = reinterpret_cast<float2*>(base + Pair128Smem::s);
+    float2* tw = reinterpret_cast<float2*>(base + Pair128Smem::s + Pair128Smem::t);
+    float2* ph = tw + 128;
+    float2* ny = ph + 512;
+    float2* eb = ny + 512;
+    float* el = reinterpret_cast<float*>(eb + 512);
+    __shared__ Probe sp;
+    __shared__ double s_red[16];
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int grp = lane >> 3;
+    const int s = lane & 7;
+    float2* Tg = T + (warp * 4 + grp) * kG8Scratch;
+    const int chunk = blockIdx.x;
+    const int cand = blockIdx.y;
+    if (tid == 0) {
+        const qssb_aberrations_t ab = cands[cand];
+        sp = make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
+    }
+    fill_twiddles<N>(tw, tid, 512);
+    __syncthreads();
+    const Probe& p = sp;
+    const float2* eqc = eq_table + (size_t)cand * N * N;
+    // the line (row or column) of this group within a round of 64
+    const int line = (warp & 7) + 8 * grp + 32 * (warp >> 3);
+    float acc[2][16];
+#pragma unroll
+    for (int r = 0; r < 2; ++r)
+#pragma unroll
+        for (int t = 0; t < 16; ++t) acc[r][t] = 0.0f;
+    double sq = 0.0;
+    const int b0 = chunk * bf_per_chunk;
+    int nb = n_bf - b0;
+    if (nb > bf_per_chunk) nb = bf_per_chunk;
+    const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
+    for (int i = 0; i < nb; i += 2) {
+        const bool two = i + 1 < nb;
+        const int b1 = b0 + i;
+        const int b2 = two ? b1 + 1 : b1;
+        // e^{i 2 q_row(r) u_b}, e^{i 2 q_col(c) v_b} of both pixels, (u, v) = M k
+        {
+            const int bf = tid >> 8;
+            const int j = tid & 255;
+            const int b = bf ? b2 : b1;
+            const float kx = __ldg(geom + b);
+            const float ky = __ldg(geom + n_bf + b);
+            float sn, cs;
+            if constexpr (CHI64) {
+                const double kx64 = (double)kx + (double)__ldg(geom + 6 * n_bf + b);
+                const double ky64 = (double)ky + (double)__ldg(geom + 7 * n_bf + b);
+                const double u = j < 128 ? fma(p.mxx_d, kx64, p.mxy_d * ky64)
+                                         : fma(p.mxy_d, kx64, p.myy_d * ky64);
+                const double q = j < 128 ? fftfreq_d(j, N, p.qval_r) : fftfreq_d(j - 128, N, p.qval_c);
+                sincosf(reduce_angle(2.0 * q * u), &sn, &cs);
+            } else {
+                const float u = j < 128 ? fmaf(p.mxx, kx, p.mxy * ky) : fmaf(p.mxy, kx, p.myy * ky);
+                const float q = j < 128 ? __ldg(q_row + j) : __ldg(q_col + j - 128);
+                sincosf(2.0f * q * u, &sn, &cs);
+            }
+            ph[tid] = make_float2(cs, sn);
+        }
+        __syncthreads();
+        // A) both pixels' corrected spectra on the evaluated set, packed into S
+        {
+            const float2* g1 = g + (size_t)b1 * N * H;
+            const float2* g2 = g + (size_t)b2 * N * H;
+            const float2* t1 = overlap + (size_t)b1 * kNE128;
+            const float2* t2 = overlap + (size_t)b2 * kNE128;
+            for (int e = tid; e < kNE128; e += 512) {
+                int r, c;
+                elem_rc128(e, r, c);
+                const bool lo = c <= 64;
+                const int go = lo ? r * H + c : ((N - r) & (N - 1)) * H + (N - c);
+                float2 gv1 = __ldg(g1 + go);
+                float2 gv2 = __ldg(g2 + go);
+                if (!lo) {
+                    gv1.y = -gv1.y;
+                    gv2.y = -gv2.y;
+                }
+                const float2 eqv = __ldg(eqc + r * N + c);
+                const float2 v1 = corrected_table(__ldg(t1 + e), eqv, cmul(ph[r], ph[128 + c]), gv1);
+                float2 v2 = corrected_table(__ldg(t2 + e), eqv, cmul(ph[256 + r], ph[384 + c]), gv2);
+                if (!two) v2 = make_float2(0.0f, 0.0f);
+                if (r == 64 || c == 64) {
+                    if (r == 64) {
+                        ny[c] = v1;
+                        ny[256 + c] = v2;
+                    }
+                    if (c == 64) {
+                        ny[128 + r] = v1;
+                        ny[384 + r] = v2;
+                    }
+                } else if (r == 0 && c == 0) {
+                    // DC := dc; its anti-Hermitian part is i Im(dc)
+                    const float a2 = two ? dc.y : 0.0f;
+                    S[0] = make_float2(dc.y, a2);
+                } else {
+                    S[r * P + c] = make_float2(v2.x + v1.y, v2.y - v1.x);
+                    if (r != 0)
+                        S[(N - r) * P + ((N - c) & (N - 1))] = make_float2(v1.y - v2.x, v1.x + v2.y);
+                }
+            }
+        }
+        __syncthreads();
+        // A') the Nyquist lines: A into S, E transformed (thread: pixel, line, index)
+        {
+            const int bf = tid >> 8;
+            const int ln = (tid >> 7) & 1;
+            const int j = tid & 127;
+            const float2* cl = ny + bf * 256 + ln * 128;
+            const float2 c0 = cl[j];
+            const float2 c1 = cl[(N - j) & (N - 1)];
+            float2 a = make_float2(0.5f * (c0.x - c1.x), 0.5f * (c0.y + c1.y));
+            float2 ev = make_float2(0.5f * (c0.x + c1.x), 0.5f * (c0.y - c1.y));
+            if (ln == 1 && j == 64) a = ev = make_float2(0.0f, 0.0f);  // (64, 64): row line
+            __syncthreads();
+            ny[tid] = a;
+            eb[tid] = ev;
+        }
+        __syncthreads();
+        if (tid < 256) {
+            const int ln = tid >> 7;
+            const int j = tid & 127;
+            const float2 a1 = ny[ln * 128 + j];
+            const float2 a2 = ny[256 + ln * 128 + j];
+            const float2 v = make_float2(a2.x + a1.y, a2.y - a1.x);
+            if (ln == 0)
+                S[64 * P + j] = v;
+            else if (j != 64)
+                S[j * P + 64] = v;
+        } else if (tid < 320) {
+            // warps 8 and 9: E_row + i E_col of one pixel, inverse transform;
+            // real part = row line's E^row(x), imaginary = column line's E^col(y)
+            const int bf = warp - 8;
+            float2* x = eb + bf * 256;
+            for (int j = lane; j < 128; j += 32) {
+                const float2 er = x[j];
+                const float2 ec = x[128 + j];
+                x[j] = make_float2(er.x - ec.y, er.y + ec.x);
+            }
+            __syncwarp();
+            line_fft<N, +1>(x, 1, tw, lane);
+            for (int j = lane; j < 128; j += 32) {
+                el[bf * 256 + j] = x[j].x;
+                el[bf * 256 + 128 + j] = x[j].y;
+            }
+        }
+        __syncthreads();
+        // B) row IFFTs of S, two rounds of 64 rows
+#pragma unroll
+        for (int round = 0; round < 2; ++round) {
+            float2* rowp = S + (line + 64 * round) * P;
+            float2 v[16];
+#pragma unroll
+            for (int n1 = 0; n1 < 16; ++n1) v[n1] = rowp[s + 8 * n1];
+            fft128_g8<+1>(v, Tg, s, tw);
+#pragma unroll
+            for (int t = 0; t < 16; ++t) rowp[fft128_g8_index(s, t)] = v[t];
+        }
+        __syncthreads();
+        // C) column IFFTs: a_1 + i a_2 at (y, x); phases against e_b(y, x)
+#pragma unroll
+        for (int round = 0; round < 2; ++round) {
+            const int x = line + 64 * round;
+            const float sx = (x & 1) ? -1.0f : 1.0f;
+            const float er1 = el[x];
+            const float er2 = el[256 + x];
+            float2 v[16];
+#pragma unroll
+            for (int n1 = 0; n1 < 16; ++n1) v[n1] = S[(s + 8 * n1) * P + x];
+            fft128_g8<+1>(v, Tg, s, tw);
+#pragma unroll
+            for (int t = 0; t < 16; ++t) {
+                const int y = fft128_g8_index(s, t);
+                const float sy = (y & 1) ? -1.0f : 1.0f;
+                const float e1 = fmaf(sx, el[128 + y], fmaf(sy, er1, dc.x));
+                const float p1 = phase_atan2(v[t].x, e1);
+                float a = p1;
+                sq = fma((double)p1, (double)p1, sq);
+                if (two) {
+                    const float e2 = fmaf(sx, el[384 + y], fmaf(sy, er2, dc.x));
+                    const float p2 = phase_atan2(v[t].y, e2);
+                    a += p2;
+                    sq = fma((double)p2, (double)p2, sq);
+                }
+                acc[round][t] += a;
+            }
+        }
+        __syncthreads();
+    }
+    // row-major partial sum planes part[(cand * n_chunks + chunk) * N * N + y * N + x]
+    float* ps = part + (size_t)(cand * n_chunks + chunk) * N * N;
+#pragma unroll
+    for (int round = 0; round < 2; ++round) {
+        const int x = line + 64 * round;
+#pragma unroll
+        for (int t = 0; t < 16; ++t) ps[fft128_g8_index(s, t) * N + x] = acc[round][t];
+    }
+    // the CTA's sum of phi^2: lanes, then the 16 warps in order
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sq += __shfl_xor_sync(0xffffffffu, sq, off);
+    if (lane == 0) s_red[warp] = sq;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+#pragma unroll
+        for (int w = 0; w < 16; ++w) t += s_red[w];
+        part_sq[cand * n_chunks + chunk] = t;
+    }
+}
+
+// The pair kernel's fold: per pixel the FP64 sum of the chunks' phi planes,
+// the mean phase, and -mean^2 summed over the block's 32 pixels (the sum of
+// squares arrives as one FP64 number per chunk, added in k_loss_final_sq).
+template <int N>
+__global__ void __launch_bounds__(kReducePix * kReduceSlices) k_loss_reduce_sum(
+    const float* __restrict__ part, int n_chunks, int n_bf, double* __restrict__ block_var,
+    float* __restrict__ mean_phase) {
+    __shared__ double r1[kReduceSlices][kReducePix];
+    __shared__ double rv[kReducePix];
+    const int px = threadIdx.x & (kReducePix - 1);
+    const int sl = threadIdx.x / kReducePix;
+    const int j = blockIdx.x * kReducePix + px;  // y * N + x
+    const int cand = blockIdx.y;
+    constexpr size_t NN = (size_t)N * N;
+    const float* cbase = part + (size_t)cand * n_chunks * NN + j;
+    double s1 = 0.0;
+    int k = sl;
+    for (; k + 3 * kReduceSlices < n_chunks; k += 4 * kReduceSlices) {
+        float a[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) a[u] = __ldg(cbase + (size_t)(k + u * kReduceSlices) * NN);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) s1 += (double)a[u];
+    }
+    for (; k < n_chunks; k += kReduceSlices) s1 += (double)__ldg(cbase + (size_t)k * NN);
+    r1[sl][px] = s1;
+    __syncthreads();
+    if (sl == 0) {
+        double t1 = 0.0;
+#pragma unroll
+        for (int w = 0; w < kReduceSlices; ++w) t1 += r1[w][px];
+        const double mean = t1 / (double)n_bf;
+        rv[px] = -mean * mean;
+        if (mean_phase) mean_phase[(size_t)cand * NN + j] = (float)mean;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double acc = 0.0;
+#pragma unroll
+        for (int i = 0; i < kReducePix; ++i) acc += rv[i];
+        block_var[(size_t)cand * (NN / kReducePix) + blockIdx.x] = acc;
+    }
+}
+
+// L = (sum of the blocks' -mean^2 + (sum of phi^2) / B) / N^2, fixed order.
+__global__ void __launch_bounds__(256) k_loss_final_sq(const double* __restrict__ block_var,
+                                                       int n_blocks, const double* __restrict__ part_sq,
+                                                       int n_chunks, int n_bf, int npos,
+                                                       float* __restrict__ losses) {
+    __shared__ double red[256];
+    const int cand = blockIdx.x;
+    const double* v = block_var + (size_t)cand * n_blocks;
+    double acc = 0.0;
+    for (int i = threadIdx.x; i < n_blocks; i += 256) acc += v[i];
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        double q = 0.0;
+        for (int k = 0; k < n_chunks; ++k) q += part_sq[(size_t)cand * n_chunks + k];
+        losses[cand] = (float)((red[0] + q / (double)n_bf) / (double)npos);
+    }
+}
+
+
 // ---------------------------------------------- N >= 256: two passes
 // A 256^2 .. 1024^2 plane does not fit one CTA's shared memory. The BF pixels
 // are taken in chunks whose row-transformed planes stay in L2 (about 48 MB
@@ -754,6 +1139,35 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool 
         const size_t rows = full ? (size_t)n : (size_t)(n / 2 + 1);
         pl.stage_bytes = sizeof(float2) * rows * n * (size_t)tp.chunk_bf * n_cand;
         pl.delta_bytes = full ? 0 : sizeof(float2) * (size_t)(n / 2) * tp.chunk_bf * n_cand;
+    } else if (n == 128 && chunks_req <= 0) {
+        // one 512-thread CTA per SM: pick the chunking whose waves are
+        // fullest - minimise waves x (pairs per CTA + one pair's worth of
+        // per-CTA cost: set-up and its 64 KB partial plane), with an even BF
+        // count per chunk (the table kernel takes pixels in pairs), at most
+        // 4096 partial planes, fewest chunks on a tie. A fixed function of the
+        // problem (the B200's 148 SMs as a constant), so the bits do not
+        // depend on the device.
+        constexpr long kPlanSms = 148;
+        long best = -1;
+        int best_bpc = n_bf + (n_bf & 1);
+        const int cmax = n_bf < 8192 ? n_bf : 8192;
+        for (int c = 1; c <= cmax; ++c) {
+            int bpc = (n_bf + c - 1) / c;
+            bpc += bpc & 1;
+            const long chunks = (n_bf + bpc - 1) / bpc;
+            if (c > 1 && (long)n_cand * chunks > 4096) continue;
+            const long waves = ((long)n_cand * chunks + kPlanSms - 1) / kPlanSms;
+            const long cost = waves * (bpc / 2 + 1);
+            if (best < 0 || cost < best) {
+                best = cost;
+                best_bpc = bpc;
+            }
+        }
+        pl.bf_per_chunk = best_bpc;
+        pl.n_chunks = (n_bf + best_bpc - 1) / best_bpc;
+        pl.chunk_bf = 0;
+        pl.stage_bytes = 0;
+        pl.delta_bytes = 0;
     } else {
         int chunks = chunks_req > 0 ? chunks_req : (296 + n_cand - 1) / n_cand;
         if (chunks < 1) chunks = 1;
@@ -816,7 +1230,7 @@ template <int N, bool SYM, bool CHI64, bool QUAD>
 static int launch_loss(const float* g_half, const float* geom, const float* q_row,
                        const float* q_col, const qssb_calibration_t& cal,
                        const qssb_aberrations_t* cands, int n_cand, int chunks, char* ws,
-                       float* losses, float* mean_phase, cudaStream_t s) {
+                       float* losses, float* mean_phase, const float2* overlap, cudaStream_t s) {
     const LossPlan pl = plan_loss(N, cal.n_bf, n_cand, chunks);
     float* part = reinterpret_cast<float*>(ws);
     double* var = reinterpret_cast<double*>(ws + pl.part_bytes);
@@ -824,6 +1238,26 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
     if (QUAD) {
         k_eq_table<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(cands, cal, eq);
         CUDA_TRY(cudaGetLastError());
+    }
+    if constexpr (N == 128 && SYM && QUAD) {
+        if (overlap) {
+            // the pair kernel: sum planes (one per chunk) then one double per chunk
+            double* part_sq = reinterpret_cast<double*>(part + (size_t)n_cand * pl.n_chunks * N * N);
+            const size_t smem = Pair128Smem::bytes;
+            CUDA_TRY(cudaFuncSetAttribute(k_loss_pair128<CHI64>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            k_loss_pair128<CHI64><<<dim3(pl.n_chunks, n_cand), 512, smem, s>>>(
+                reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, overlap,
+                cands, cal, eq, pl.bf_per_chunk, pl.n_chunks, part, part_sq);
+            CUDA_TRY(cudaGetLastError());
+            k_loss_reduce_sum<N><<<dim3(N * N / kReducePix, n_cand), kReducePix * kReduceSlices, 0, s>>>(
+                part, pl.n_chunks, cal.n_bf, var, mean_phase);
+            CUDA_TRY(cudaGetLastError());
+            k_loss_final_sq<<<n_cand, 256, 0, s>>>(var, N * N / kReducePix, part_sq, pl.n_chunks,
+                                                   cal.n_bf, N * N, losses);
+            CUDA_TRY(cudaGetLastError());
+            return QSSB_OK;
+        }
     }
     if constexpr (N >= kL256) {
         static_assert(SYM, "the two-pass loss evaluates the half set");
@@ -859,19 +1293,19 @@ template <int N, bool QUAD>
 static int dispatch_loss_q(bool sym, bool chi64, const float* g_half, const float* geom,
                            const float* q_row, const float* q_col, const qssb_calibration_t& cal,
                            const qssb_aberrations_t* cands, int n_cand, int chunks, char* ws,
-                           float* losses, float* mean_phase, cudaStream_t s) {
+                           float* losses, float* mean_phase, const float2* ov, cudaStream_t s) {
     if constexpr (N >= kL256) {
         if (!sym)
             return set_error(QSSB_ERR_UNSUPPORTED,
                              "qssb_loss_batch: QSSB_FLAG_FULL_PLANE is offered up to 128^2");
-        return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s)
-                     : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
+        return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s)
+                     : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s);
     } else {
         if (sym)
-            return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s)
-                         : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
-        return chi64 ? launch_loss<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s)
-                     : launch_loss<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
+            return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s)
+                         : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s);
+        return chi64 ? launch_loss<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s)
+                     : launch_loss<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s);
     }
 }
 
@@ -881,10 +1315,10 @@ template <int N>
 static int dispatch_loss(bool sym, bool chi64, bool quad, const float* g_half, const float* geom,
                          const float* q_row, const float* q_col, const qssb_calibration_t& cal,
                          const qssb_aberrations_t* cands, int n_cand, int chunks, char* ws,
-                         float* losses, float* mean_phase, cudaStream_t s) {
+                         float* losses, float* mean_phase, const float2* ov, cudaStream_t s) {
     if (quad)
-        return dispatch_loss_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
-    return dispatch_loss_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, s);
+        return dispatch_loss_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s);
+    return dispatch_loss_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s);
 }
 
 // ------------------------------------------------------ 14-term chi
@@ -1050,6 +1484,42 @@ extern "C" int qssb_loss_batch(const float* g_half, const float* bf_geom, const 
                                const qssb_aberrations_t* candidates, int32_t n_cand, int32_t flags,
                                void* workspace, size_t workspace_bytes, float* losses,
                                float* mean_phase, void* stream) {
+    return qssb_loss_batch_ex(g_half, bf_geom, q_row, q_col, cal, candidates, n_cand, flags,
+                              nullptr, workspace, workspace_bytes, losses, mean_phase, stream);
+}
+
+extern "C" int qssb_overlap_table_bytes(const qssb_calibration_t* cal, size_t* bytes) {
+    int rc = validate_calibration(cal, "qssb_overlap_table_bytes: null calibration");
+    if (rc) return rc;
+    if (!bytes) return set_error(QSSB_ERR_INVALID, "qssb_overlap_table_bytes: null output");
+    if (cal->scan_rows != 128 || cal->scan_cols != 128)
+        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_overlap_table: 128x128 scans only");
+    *bytes = sizeof(float2) * (size_t)kNE128 * (size_t)cal->n_bf;
+    return QSSB_OK;
+}
+
+extern "C" int qssb_overlap_table(const float* bf_geom, const float* q_row, const float* q_col,
+                                  const qssb_calibration_t* cal, float* table, void* stream) {
+    size_t need = 0;
+    int rc = qssb_overlap_table_bytes(cal, &need);
+    if (rc) return rc;
+    if (!bf_geom || !q_row || !q_col || !table)
+        return set_error(QSSB_ERR_INVALID, "qssb_overlap_table: null pointer");
+    if (cal->n_bf > 65535)
+        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_overlap_table: more than 65535 BF pixels");
+    const Probe p = make_probe_common(*cal, 0.0f, 0.0f, 0.0f, 0.0f);
+    k_overlap_table128<<<dim3((kNE128 + 255) / 256, cal->n_bf), 256, 0, (cudaStream_t)stream>>>(
+        bf_geom, cal->n_bf, q_row, q_col, p, reinterpret_cast<float2*>(table));
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+extern "C" int qssb_loss_batch_ex(const float* g_half, const float* bf_geom, const float* q_row,
+                                  const float* q_col, const qssb_calibration_t* cal,
+                                  const qssb_aberrations_t* candidates, int32_t n_cand,
+                                  int32_t flags, const float* overlap, void* workspace,
+                                  size_t workspace_bytes, float* losses, float* mean_phase,
+                                  void* stream) {
     int rc = validate_calibration(cal, "qssb_loss_batch: null calibration");
     if (rc) return rc;
     if (!g_half || !bf_geom || !q_row || !q_col || !candidates || !workspace || !losses)
@@ -1065,14 +1535,17 @@ extern "C" int qssb_loss_batch(const float* g_half, const float* bf_geom, const 
     const bool chi64 = (flags & QSSB_FLAG_CHI_FP64) != 0;
     const bool quad = (flags & QSSB_FLAG_QUADRATIC) != 0;
     const int chunks = flag_chunks(flags);
+    if (overlap && (cal->scan_rows != 128 || cal->scan_cols != 128))
+        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch_ex: the overlap table is for 128x128 scans");
+    const float2* ov = reinterpret_cast<const float2*>(overlap);
     cudaStream_t s = (cudaStream_t)stream;
     char* ws = static_cast<char*>(workspace);
     switch (cal->scan_rows) {
-        case 64: return dispatch_loss<64>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
-        case 128: return dispatch_loss<128>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
-        case 256: return dispatch_loss<256>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
-        case 512: return dispatch_loss<512>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
-        case 1024: return dispatch_loss<1024>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, s);
+        case 64: return dispatch_loss<64>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, nullptr, s);
+        case 128: return dispatch_loss<128>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, ov, s);
+        case 256: return dispatch_loss<256>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, nullptr, s);
+        case 512: return dispatch_loss<512>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, nullptr, s);
+        case 1024: return dispatch_loss<1024>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, nullptr, s);
         default: return set_error(QSSB_ERR_UNSUPPORTED,
                                   "qssb_loss_batch: scan size must be 64, 128, 256, 512 or 1024");
     }

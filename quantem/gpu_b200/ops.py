@@ -26,6 +26,8 @@ LAUNCHES_PER_CALL = {
     "qssb_object": 4,
     "qssb_object_ex": 4,
     "qssb_loss_batch": 3,
+    "qssb_loss_batch_ex": 3,
+    "qssb_overlap_table": 1,
     "qssb_loss_batch_full": 3,
     "qssb_fourier_shift": 3,
     "qssb_join_object_waves": 1,
@@ -389,12 +391,30 @@ def loss_batch_full(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Te
     return losses, mp
 
 
+def overlap_table(bf_geom: torch.Tensor, q_row: torch.Tensor, q_col: torch.Tensor,
+                  cal: Calibration) -> torch.Tensor:
+    """The candidate-independent overlap apertures of a 128x128-scan dataset
+    (float32 CUDA [n_bf, 8383, 2]) for ``loss_batch(..., overlap=...)``."""
+    _require_cuda(bf_geom, "bf_geom", torch.float32)
+    if tuple(bf_geom.shape) != (_lib.GEOM_ROWS, cal.n_bf):
+        raise ValueError("bf_geom shape does not match the calibration")
+    nbytes = ctypes.c_size_t(0)
+    check(_lib.load().qssb_overlap_table_bytes(ctypes.byref(cal), ctypes.byref(nbytes)))
+    table = torch.empty(nbytes.value // 4, dtype=torch.float32, device=bf_geom.device)
+    _call("qssb_overlap_table", bf_geom.device, _ptr(bf_geom), _ptr(q_row), _ptr(q_col),
+          ctypes.byref(cal), _ptr(table), _stream(bf_geom))
+    return table.view(cal.n_bf, -1, 2)
+
+
 def loss_batch(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
                q_col: torch.Tensor, cal: Calibration, candidates: torch.Tensor, *,
                flags: int = 0, workspace: Workspace | None = None, want_mean_phase: bool = False,
-               out: torch.Tensor | None = None
+               out: torch.Tensor | None = None, overlap: torch.Tensor | None = None
                ) -> tuple[torch.Tensor, torch.Tensor | None]:
-    """Phase-variance losses for ``candidates`` (float32 CUDA [n, 4]: C10, C12, phi12, C30)."""
+    """Phase-variance losses for ``candidates`` (float32 CUDA [n, 4]: C10, C12, phi12, C30).
+
+    ``overlap`` (from ``overlap_table``, 128x128 scans) selects the
+    table-driven kernel for quadratic candidates (``QSSB_FLAG_QUADRATIC``)."""
     _require_cuda(g_half, "g_half", torch.complex64)
     _require_cuda(bf_geom, "bf_geom", torch.float32)
     _require_cuda(candidates, "candidates", torch.float32)
@@ -414,9 +434,17 @@ def loss_batch(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
     losses = out if out is not None else torch.empty(n, dtype=torch.float32, device=g_half.device)
     mp = (torch.empty((n, r0, r1), dtype=torch.float32, device=g_half.device)
           if want_mean_phase else None)
-    _call("qssb_loss_batch", g_half.device, _ptr(g_half), _ptr(bf_geom), _ptr(q_row),
-          _ptr(q_col), ctypes.byref(cal), _ptr(candidates), n, int(flags), _ptr(buf), buf.numel(),
-          _ptr(losses), _ptr(mp), _stream(g_half))
+    if overlap is None:
+        _call("qssb_loss_batch", g_half.device, _ptr(g_half), _ptr(bf_geom), _ptr(q_row),
+              _ptr(q_col), ctypes.byref(cal), _ptr(candidates), n, int(flags), _ptr(buf),
+              buf.numel(), _ptr(losses), _ptr(mp), _stream(g_half))
+    else:
+        _require_cuda(overlap, "overlap", torch.float32)
+        if overlap.shape[0] != cal.n_bf:
+            raise ValueError("overlap table does not match the calibration")
+        _call("qssb_loss_batch_ex", g_half.device, _ptr(g_half), _ptr(bf_geom), _ptr(q_row),
+              _ptr(q_col), ctypes.byref(cal), _ptr(candidates), n, int(flags), _ptr(overlap),
+              _ptr(buf), buf.numel(), _ptr(losses), _ptr(mp), _stream(g_half))
     return losses, mp
 
 

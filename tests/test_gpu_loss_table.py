@@ -1,0 +1,110 @@
+"""The table-driven 128x128 phase-variance loss (``qssb_overlap_table`` +
+``qssb_loss_batch_ex``): two BF pixels per inverse 2D FFT, their
+anti-Hermitian parts packed into one complex plane and the Hermitian DC and
+Nyquist-line parts transformed on their own.
+
+Checked against the FP64 oracle (loss 1e-5 relative, mean phase 2e-4 rad at
+the 99.9th percentile, as the other loss tests) and against the table-free
+kernel (float32 rounding only), on the reference test's 27-pixel disk case
+and on the CPU-runnable workload padded to 128^2 (437 pixels: an odd count,
+so the last pixel of a chunk is transformed alone); plus the table itself
+against an FP64 evaluation of the apertures, repeatability, and the
+single-candidate, three-candidate and 64-candidate plans.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import ssb_oracle as so
+from quantem.gpu_b200 import ops
+from quantem.gpu_b200._lib import QSSB_FLAG_CHI_FP64, QSSB_FLAG_QUADRATIC
+from recipes import disk_input, synthetic_plain_32
+from test_gpu_parity import DISK_KW, _prep_case
+
+pytestmark = pytest.mark.gpu
+DEV = torch.device("cuda:0")
+LOSS_RTOL, LOSS_ATOL, PHASE_ATOL = 1e-5, 1e-6, 2e-4
+CANDS = [(-120.0, 55.0, math.radians(17.0)), (-80.0, 30.0, math.radians(-5.0)),
+         (20.0, 40.0, math.radians(11.0)), (100.0, 10.0, math.radians(43.0)),
+         (0.0, 0.0, 0.0)]
+
+
+@pytest.fixture(scope="module", params=["disk27", "plain437"])
+def case(request):
+    if request.param == "disk27":
+        return _prep_case(disk_input(123), **DISK_KW)
+    kw = dict(voltage_kV=300, semiangle_mrad=20.0, scan_sampling=0.5, det_sampling=20.0 / 12.0)
+    return _prep_case(synthetic_plain_32(), **kw)
+
+
+def _cands(rows) -> torch.Tensor:
+    return torch.tensor([[a, b, c, 0.0] for a, b, c in rows], dtype=torch.float32, device=DEV)
+
+
+@pytest.mark.parametrize("flags", [QSSB_FLAG_QUADRATIC, QSSB_FLAG_QUADRATIC | QSSB_FLAG_CHI_FP64])
+def test_table_loss_matches_oracle_and_table_free_kernel(case, flags):
+    prep, cal, d = case
+    table = ops.overlap_table(d["geom"], d["q_row"], d["q_col"], cal)
+    cands = _cands(CANDS)
+    losses, mp = ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands,
+                                flags=flags, want_mean_phase=True, overlap=table)
+    plain, mp_plain = ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands,
+                                     flags=flags, want_mean_phase=True)
+    losses, mp, plain = losses.cpu().numpy(), mp.cpu().numpy(), plain.cpu().numpy()
+    for i, (a, b, c) in enumerate(CANDS):
+        ref_loss, ref_mean = so.phase_variance_loss(prep.g_half, prep.geo, so.Aberrations(a, b, c),
+                                                    prep.dc)
+        assert losses[i] == pytest.approx(ref_loss, rel=LOSS_RTOL, abs=LOSS_ATOL), (i, flags)
+        assert losses[i] == pytest.approx(plain[i], rel=2e-6, abs=1e-7)
+        err = np.abs(so.wrapped_phase_error(mp[i], ref_mean))
+        assert np.percentile(err, 99.9) < PHASE_ATOL
+    np.testing.assert_allclose(mp, mp_plain.cpu().numpy(), rtol=0, atol=2e-5)
+
+
+def test_table_matches_fp64_apertures(case):
+    """table[b][e] = A(k)(A(q-k) -+ A(q+k)) on the evaluated half set: the
+    float32 fast aperture with the FP64 tie rule, within float32 rounding of
+    an FP64 evaluation except where the rule itself switched to FP64."""
+    prep, cal, d = case
+    table = ops.overlap_table(d["geom"], d["q_row"], d["q_col"], cal).cpu().numpy().astype(np.float64)
+    n = prep.scan_shape[0]
+    rows = np.concatenate([np.repeat(np.arange(65), n), np.arange(127, 64, -1)])
+    cols = np.concatenate([np.tile(np.arange(n), 65), np.full(63, 64)])
+    geo = prep.geo
+    qx = geo.q_row.astype(np.float64)[rows][None, :]
+    qy = geo.q_col.astype(np.float64)[cols][None, :]
+    kx = geo.kx[:, None].astype(np.float64)
+    ky = geo.ky[:, None].astype(np.float64)
+    am = so._aperture_and_angles(qx - kx, qy - ky, geo)[3]
+    ap = so._aperture_and_angles(qx + kx, qy + ky, geo)[3]
+    ak = geo.aperture_k[:, None]
+    want = np.stack([ak * (am - ap), ak * (am + ap)], axis=-1)
+    assert table.shape == want.shape
+    assert np.abs(table - want).max() <= 2e-5
+
+
+def test_table_loss_plans_and_repeatability(case):
+    """One, three and 64 candidates (different chunk plans) agree per
+    candidate with each other within float32 rounding; a call repeated gives
+    identical bits."""
+    prep, cal, d = case
+    table = ops.overlap_table(d["geom"], d["q_row"], d["q_col"], cal)
+    rng = np.random.default_rng(9)
+    rows = [(float(a), float(b), float(c)) for a, b, c in
+            zip(rng.uniform(-150, 150, 64), rng.uniform(0, 60, 64), rng.uniform(-1.5, 1.5, 64))]
+    run = lambda r: ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, _cands(r),  # noqa: E731
+                                   flags=QSSB_FLAG_QUADRATIC, overlap=table)[0]
+    big = run(rows)
+    assert torch.equal(big, run(rows))
+    big = big.cpu().numpy()
+    three = run(rows[:3]).cpu().numpy()
+    one = run(rows[:1]).cpu().numpy()
+    np.testing.assert_allclose(three, big[:3], rtol=2e-6)
+    np.testing.assert_allclose(one, big[:1], rtol=2e-6)
+    for i in (0, 37):
+        ref, _ = so.phase_variance_loss(prep.g_half, prep.geo, so.Aberrations(*rows[i]), prep.dc)
+        assert big[i] == pytest.approx(ref, rel=LOSS_RTOL, abs=LOSS_ATOL)
