@@ -544,10 +544,11 @@ struct Pair128Smem {
     static constexpr size_t t = sizeof(float2) * 64 * kG8Scratch;  // group transposes
     static constexpr size_t tw = sizeof(float2) * 128;
     static constexpr size_t ph = sizeof(float2) * 2 * 256;    // [bf][e^{2i q_r u} | e^{2i q_c v}]
-    static constexpr size_t ny = sizeof(float2) * 2 * 256;    // [bf][row 64 | column 64]: C, then A
+    static constexpr size_t ny = sizeof(float2) * 2 * 256;    // [bf][row 64 | column 64]: C
     static constexpr size_t eb = sizeof(float2) * 2 * 256;    // [bf][E row | E col]
+    static constexpr size_t na = sizeof(float2) * 2 * 256;    // [bf][row 64 | column 64]: A
     static constexpr size_t el = sizeof(float) * 2 * 256;     // [bf][E^row(x) | E^col(y)]
-    static constexpr size_t bytes = s + t + tw + ph + ny + eb + el;
+    static constexpr size_t bytes = s + t + tw + ph + ny + eb + na + el;
 };
 
 template <bool CHI64>
@@ -568,7 +569,8 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
     float2* ph = tw + 128;
     float2* ny = ph + 512;
     float2* eb = ny + 512;
-    float* el = reinterpret_cast<float*>(eb + 512);
+    float2* na = eb + 512;
+    float* el = reinterpret_cast<float*>(na + 512);
     __shared__ Probe sp;
     __shared__ double s_red[16];
     const int tid = threadIdx.x;
@@ -599,11 +601,11 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
     int nb = n_bf - b0;
     if (nb > bf_per_chunk) nb = bf_per_chunk;
     const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
-    for (int i = 0; i < nb; i += 2) {
-        const bool two = i + 1 < nb;
+    // e^{i 2 q_row(r) u_b}, e^{i 2 q_col(c) v_b} of the pair starting at pixel
+    // i of the chunk, (u, v) = M k; written during the previous pair's row pass
+    auto fill_phase = [&](int i) {
         const int b1 = b0 + i;
-        const int b2 = two ? b1 + 1 : b1;
-        // e^{i 2 q_row(r) u_b}, e^{i 2 q_col(c) v_b} of both pixels, (u, v) = M k
+        const int b2 = i + 1 < nb ? b1 + 1 : b1;
         {
             const int bf = tid >> 8;
             const int j = tid & 255;
@@ -625,27 +627,55 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
             }
             ph[tid] = make_float2(cs, sn);
         }
-        __syncthreads();
+    };
+    if (nb > 0) fill_phase(0);
+    __syncthreads();
+    for (int i = 0; i < nb; i += 2) {
+        const bool two = i + 1 < nb;
+        const int b1 = b0 + i;
+        const int b2 = two ? b1 + 1 : b1;
         // A) both pixels' corrected spectra on the evaluated set, packed into S
         {
             const float2* g1 = g + (size_t)b1 * N * H;
             const float2* g2 = g + (size_t)b2 * N * H;
             const float2* t1 = overlap + (size_t)b1 * kNE128;
             const float2* t2 = overlap + (size_t)b2 * kNE128;
+            // the next element's five loads are issued before this one's math
+            auto gofs = [](int r, int c) {
+                return c <= 64 ? r * H + c : ((N - r) & (N - 1)) * H + (N - c);
+            };
+            float2 ng1, ng2, nt1, nt2, neq;
+            {
+                int r, c;
+                elem_rc128(tid, r, c);  // tid < 512 < kNE128
+                const int go = gofs(r, c);
+                ng1 = __ldg(g1 + go);
+                ng2 = __ldg(g2 + go);
+                nt1 = __ldg(t1 + tid);
+                nt2 = __ldg(t2 + tid);
+                neq = __ldg(eqc + r * N + c);
+            }
             for (int e = tid; e < kNE128; e += 512) {
                 int r, c;
                 elem_rc128(e, r, c);
-                const bool lo = c <= 64;
-                const int go = lo ? r * H + c : ((N - r) & (N - 1)) * H + (N - c);
-                float2 gv1 = __ldg(g1 + go);
-                float2 gv2 = __ldg(g2 + go);
-                if (!lo) {
+                float2 gv1 = ng1, gv2 = ng2;
+                const float2 d1 = nt1, d2 = nt2, eqv = neq;
+                if (e + 512 < kNE128) {
+                    int rn, cn;
+                    elem_rc128(e + 512, rn, cn);
+                    const int go = gofs(rn, cn);
+                    ng1 = __ldg(g1 + go);
+                    ng2 = __ldg(g2 + go);
+                    nt1 = __ldg(t1 + e + 512);
+                    nt2 = __ldg(t2 + e + 512);
+                    neq = __ldg(eqc + rn * N + cn);
+                }
+                if (c > 64) {
                     gv1.y = -gv1.y;
                     gv2.y = -gv2.y;
                 }
-                const float2 eqv = __ldg(eqc + r * N + c);
-                const float2 v1 = corrected_table(__ldg(t1 + e), eqv, cmul(ph[r], ph[128 + c]), gv1);
-                float2 v2 = corrected_table(__ldg(t2 + e), eqv, cmul(ph[256 + r], ph[384 + c]), gv2);
+                const float2 v1 = corrected_table(d1, eqv, cmul(ph[r], ph[128 + c]), gv1);
+                float2 v2 = corrected_table(d2, eqv, cmul(ph[256 + r], ph[384 + c]), gv2);
                 if (!two) v2 = make_float2(0.0f, 0.0f);
                 if (r == 64 || c == 64) {
                     if (r == 64) {
@@ -679,16 +709,15 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
             float2 a = make_float2(0.5f * (c0.x - c1.x), 0.5f * (c0.y + c1.y));
             float2 ev = make_float2(0.5f * (c0.x + c1.x), 0.5f * (c0.y - c1.y));
             if (ln == 1 && j == 64) a = ev = make_float2(0.0f, 0.0f);  // (64, 64): row line
-            __syncthreads();
-            ny[tid] = a;
+            na[tid] = a;
             eb[tid] = ev;
         }
         __syncthreads();
         if (tid < 256) {
             const int ln = tid >> 7;
             const int j = tid & 127;
-            const float2 a1 = ny[ln * 128 + j];
-            const float2 a2 = ny[256 + ln * 128 + j];
+            const float2 a1 = na[ln * 128 + j];
+            const float2 a2 = na[256 + ln * 128 + j];
             const float2 v = make_float2(a2.x + a1.y, a2.y - a1.x);
             if (ln == 0)
                 S[64 * P + j] = v;
@@ -723,6 +752,8 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
 #pragma unroll
             for (int t = 0; t < 16; ++t) rowp[fft128_g8_index(s, t)] = v[t];
         }
+        // A of this pair is done with ph: the next pair's phase rows go in now
+        if (i + 2 < nb) fill_phase(i + 2);
         __syncthreads();
         // C) column IFFTs: a_1 + i a_2 at (y, x); phases against e_b(y, x)
 #pragma unroll
