@@ -272,12 +272,14 @@ int qssb_overlap_table(const float* bf_geom, const float* q_row, const float* q_
                        const qssb_calibration_t* cal, float* table, void* stream);
 
 /* qssb_loss_batch with an optional overlap table (NULL: as qssb_loss_batch).
- * With a table, 128x128 scans and QSSB_FLAG_QUADRATIC (C30 == 0), the loss
- * runs two BF pixels per inverse 2D FFT (their anti-Hermitian parts packed
- * as one complex plane, the Hermitian DC and Nyquist-line parts transformed
- * on their own) from table reads; the workspace is the same. The reduction
- * order is fixed for a given plan; the result differs from the table-free
- * path by float32 rounding only. */
+ * With a table and 128x128 scans (symmetric half set, i.e. without
+ * QSSB_FLAG_FULL_PLANE) the loss runs two BF pixels per inverse 2D FFT (their
+ * anti-Hermitian parts packed as one complex plane, the Hermitian DC and
+ * Nyquist-line parts transformed on their own) with the apertures read from
+ * the table: for QSSB_FLAG_QUADRATIC batches through the factorised overlap,
+ * otherwise (C30) through the direct probe phases. The workspace is the same.
+ * The reduction order is fixed for a given plan; the result differs from the
+ * table-free path by float32 rounding only. */
 int qssb_loss_batch_ex(const float* g_half, const float* bf_geom, const float* q_row,
                        const float* q_col, const qssb_calibration_t* cal,
                        const qssb_aberrations_t* candidates, int32_t n_cand, int32_t flags,

@@ -86,21 +86,27 @@ def loss_chunk_options(n_bf: int, n_cand: int, sms: int, scan: int = 128) -> lis
 
 
 def tune_loss(g_half, bf_geom, q_row, q_col, cal, candidates: torch.Tensor, flags: int,
-              workspace: ops.Workspace, reps: int = 2) -> int:
-    """Best chunks-per-candidate for this batch shape (cached)."""
+              workspace: ops.Workspace, reps: int = 2, overlap: torch.Tensor | None = None) -> int:
+    """Best chunks-per-candidate for this batch shape (cached); 0 keeps the
+    built-in plan when it is the fastest."""
     dev = g_half.device
     n_cand = int(candidates.shape[0])
-    key = _key("loss", dev, int(cal.scan_rows), int(cal.n_bf), n_cand, flags & 0xFFFF)
+    key = _key("loss" if overlap is None else "loss_table", dev, int(cal.scan_rows), int(cal.n_bf),
+               n_cand, flags & 0xFFFF)
     hit = _cache().get(key)
     if hit is not None:
         return hit
     sms = torch.cuda.get_device_properties(dev).multi_processor_count
     out = torch.empty(n_cand, dtype=torch.float32, device=dev)
     timings = {}
-    for c in loss_chunk_options(int(cal.n_bf), n_cand, sms, int(cal.scan_rows)):
+    opts = loss_chunk_options(int(cal.n_bf), n_cand, sms, int(cal.scan_rows))
+    if int(cal.scan_rows) == 128:
+        opts = [0] + opts  # the built-in wave-aware plan competes too
+    for c in opts:
         f = flags | _lib.flag_chunks(c)
         timings[c] = _time_ms(lambda: ops.loss_batch(g_half, bf_geom, q_row, q_col, cal, candidates,
-                                                     flags=f, workspace=workspace, out=out), dev, reps)
+                                                     flags=f, workspace=workspace, out=out,
+                                                     overlap=overlap), dev, reps)
     best = min(timings, key=timings.get)
     _store(key, best)
     return best

@@ -446,8 +446,7 @@ class B200SSBBackend:
         flags = self._flags | (QSSB_FLAG_QUADRATIC if quad else 0)
         losses, _ = ops.loss_batch(self.G_qk, self._geom_dev, self._q_row, self._q_col,
                                    self._calibration(), cands, flags=flags,
-                                   workspace=self._workspace,
-                                   overlap=self._overlap_table() if quad else None)
+                                   workspace=self._workspace, overlap=self._overlap_table())
         return losses
 
     def variance_loss(self, C10: float, C12: float, phi12: float) -> float:

@@ -524,6 +524,35 @@ __device__ __forceinline__ float2 corrected_table(float2 ds, float2 eq, float2 e
     return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
 }
 
+// The same from the table without the quadratic factorisation (C30 != 0):
+// with m = A(k) A(q-k) = (s + d) / 2 and l = A(k) A(q+k) = (s - d) / 2,
+//   Gamma = m e^{-i chi(q-k)} e^{i chi(k)} - l e^{i chi(q+k)} e^{-i chi(k)}
+// (corrected with the apertures from the table); ek = e^{i chi(k)}.
+template <bool CHI64>
+__device__ __forceinline__ float2 corrected_table_direct(float2 ds, float qx, float qy, float kx,
+                                                         float ky, float2 ek, float2 g,
+                                                         const Probe& p) {
+    const float m = 0.5f * (ds.y + ds.x);
+    const float l = 0.5f * (ds.y - ds.x);
+    const Disp dm = displacement(qx - kx, qy - ky, p);
+    const Disp dp = displacement(qx + kx, qy + ky, p);
+    float sm, cm, sp, cp;
+    __sincosf(chi_value<CHI64>(dm.alpha2, dm.cos2, dm.sin2, p), &sm, &cm);
+    __sincosf(chi_value<CHI64>(dp.alpha2, dp.cos2, dp.sin2, p), &sp, &cp);
+    // t1 = m (cm - i sm)(ck + i sk), t2 = l (cp + i sp)(ck - i sk)
+    const float t1r = m * fmaf(cm, ek.x, sm * ek.y);
+    const float t1i = m * fmaf(cm, ek.y, -sm * ek.x);
+    const float t2r = l * fmaf(cp, ek.x, sp * ek.y);
+    const float t2i = l * fmaf(sp, ek.x, -cp * ek.y);
+    float gr = t1r - t2r;
+    float gi = t1i - t2i;
+    const float m2 = fmaf(gr, gr, gi * gi);
+    const float inv = m2 > 1e-16f ? rsqrtf(m2) : 1e8f;
+    gr *= inv;
+    gi *= inv;
+    return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
+}
+
 // Two BF pixels per inverse 2D FFT. Split each corrected spectrum into its
 // anti-Hermitian part A (C(-q) = -conj C(q): every scan frequency off the
 // Nyquist row and column, where the evaluated half set defines the other
@@ -551,7 +580,7 @@ struct Pair128Smem {
     static constexpr size_t bytes = s + t + tw + ph + ny + eb + na + el;
 };
 
-template <bool CHI64>
+template <bool CHI64, bool QUAD>
 __global__ void __launch_bounds__(512, 1) k_loss_pair128(
     const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
     const float* __restrict__ q_row, const float* __restrict__ q_col,
@@ -613,7 +642,15 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
             const float kx = __ldg(geom + b);
             const float ky = __ldg(geom + n_bf + b);
             float sn, cs;
-            if constexpr (CHI64) {
+            if constexpr (!QUAD) {
+                // e^{i chi(k_b)} (the reference's pk without A(k), which the table holds)
+                if (j == 0) {
+                    __sincosf(chi_value<CHI64>(__ldg(geom + 2 * n_bf + b), __ldg(geom + 3 * n_bf + b),
+                                               __ldg(geom + 4 * n_bf + b), p), &sn, &cs);
+                    ph[bf * 256] = make_float2(cs, sn);
+                }
+                return;
+            } else if constexpr (CHI64) {
                 const double kx64 = (double)kx + (double)__ldg(geom + 6 * n_bf + b);
                 const double ky64 = (double)ky + (double)__ldg(geom + 7 * n_bf + b);
                 const double u = j < 128 ? fma(p.mxx_d, kx64, p.mxy_d * ky64)
@@ -644,7 +681,7 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
             auto gofs = [](int r, int c) {
                 return c <= 64 ? r * H + c : ((N - r) & (N - 1)) * H + (N - c);
             };
-            float2 ng1, ng2, nt1, nt2, neq;
+            float2 ng1, ng2, nt1, nt2, neq = make_float2(1.0f, 0.0f);
             {
                 int r, c;
                 elem_rc128(tid, r, c);  // tid < 512 < kNE128
@@ -653,7 +690,14 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
                 ng2 = __ldg(g2 + go);
                 nt1 = __ldg(t1 + tid);
                 nt2 = __ldg(t2 + tid);
-                neq = __ldg(eqc + r * N + c);
+                if constexpr (QUAD) neq = __ldg(eqc + r * N + c);
+            }
+            float k1x = 0.f, k1y = 0.f, k2x = 0.f, k2y = 0.f;
+            if constexpr (!QUAD) {
+                k1x = __ldg(geom + b1);
+                k1y = __ldg(geom + n_bf + b1);
+                k2x = __ldg(geom + b2);
+                k2y = __ldg(geom + n_bf + b2);
             }
             for (int e = tid; e < kNE128; e += 512) {
                 int r, c;
@@ -668,14 +712,22 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
                     ng2 = __ldg(g2 + go);
                     nt1 = __ldg(t1 + e + 512);
                     nt2 = __ldg(t2 + e + 512);
-                    neq = __ldg(eqc + rn * N + cn);
+                    if constexpr (QUAD) neq = __ldg(eqc + rn * N + cn);
                 }
                 if (c > 64) {
                     gv1.y = -gv1.y;
                     gv2.y = -gv2.y;
                 }
-                const float2 v1 = corrected_table(d1, eqv, cmul(ph[r], ph[128 + c]), gv1);
-                float2 v2 = corrected_table(d2, eqv, cmul(ph[256 + r], ph[384 + c]), gv2);
+                float2 v1, v2;
+                if constexpr (QUAD) {
+                    v1 = corrected_table(d1, eqv, cmul(ph[r], ph[128 + c]), gv1);
+                    v2 = corrected_table(d2, eqv, cmul(ph[256 + r], ph[384 + c]), gv2);
+                } else {
+                    const float qx = __ldg(q_row + r);
+                    const float qy = __ldg(q_col + c);
+                    v1 = corrected_table_direct<CHI64>(d1, qx, qy, k1x, k1y, ph[0], gv1, p);
+                    v2 = corrected_table_direct<CHI64>(d2, qx, qy, k2x, k2y, ph[256], gv2, p);
+                }
                 if (!two) v2 = make_float2(0.0f, 0.0f);
                 if (r == 64 || c == 64) {
                     if (r == 64) {
@@ -1270,14 +1322,14 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
         k_eq_table<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(cands, cal, eq);
         CUDA_TRY(cudaGetLastError());
     }
-    if constexpr (N == 128 && SYM && QUAD) {
+    if constexpr (N == 128 && SYM) {
         if (overlap) {
             // the pair kernel: sum planes (one per chunk) then one double per chunk
             double* part_sq = reinterpret_cast<double*>(part + (size_t)n_cand * pl.n_chunks * N * N);
             const size_t smem = Pair128Smem::bytes;
-            CUDA_TRY(cudaFuncSetAttribute(k_loss_pair128<CHI64>,
+            CUDA_TRY(cudaFuncSetAttribute(k_loss_pair128<CHI64, QUAD>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            k_loss_pair128<CHI64><<<dim3(pl.n_chunks, n_cand), 512, smem, s>>>(
+            k_loss_pair128<CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), 512, smem, s>>>(
                 reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, overlap,
                 cands, cal, eq, pl.bf_per_chunk, pl.n_chunks, part, part_sq);
             CUDA_TRY(cudaGetLastError());

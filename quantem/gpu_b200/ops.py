@@ -414,7 +414,7 @@ def loss_batch(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
     """Phase-variance losses for ``candidates`` (float32 CUDA [n, 4]: C10, C12, phi12, C30).
 
     ``overlap`` (from ``overlap_table``, 128x128 scans) selects the
-    table-driven kernel for quadratic candidates (``QSSB_FLAG_QUADRATIC``)."""
+    table-driven kernel (two BF pixels per inverse 2D FFT)."""
     _require_cuda(g_half, "g_half", torch.complex64)
     _require_cuda(bf_geom, "bf_geom", torch.float32)
     _require_cuda(candidates, "candidates", torch.float32)

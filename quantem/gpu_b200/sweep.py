@@ -42,15 +42,16 @@ class MultiScanSweep:
             cands = torch.zeros((n, 4), dtype=torch.float32, device=self.device)
             cands[:, 0] = torch.linspace(-100.0, 100.0, n, device=self.device)
             ws = ops.Workspace(self.device)
+            overlap = be._overlap_table()  # 128x128 scans: the table-driven pair kernel
             chunks = 0
             if tune:
                 chunks = autotune.tune_loss(be.G_qk, be._geom_dev, be._q_row, be._q_col, cal,
-                                            cands, flags, ws)
+                                            cands, flags, ws, overlap=overlap)
             flags |= _lib.flag_chunks(chunks)
             ws.get(ops.loss_workspace_bytes(cal, n, flags))
             out = torch.empty(n, dtype=torch.float32, device=self.device)
             self._slots.append(dict(be=be, cal=cal, flags=flags, cands=cands, ws=ws, out=out,
-                                    chunks=chunks))
+                                    chunks=chunks, overlap=overlap))
         self.host_cands = [torch.empty((s["cands"].shape[0], 4), dtype=torch.float32).pin_memory()
                            for s in self._slots]
         self.host_out = [torch.empty(s["out"].shape[0], dtype=torch.float32).pin_memory()
@@ -62,7 +63,8 @@ class MultiScanSweep:
         for s in self._slots:
             be = s["be"]
             ops.loss_batch(be.G_qk, be._geom_dev, be._q_row, be._q_col, s["cal"], s["cands"],
-                           flags=s["flags"], workspace=s["ws"], out=s["out"])
+                           flags=s["flags"], workspace=s["ws"], out=s["out"],
+                           overlap=s["overlap"])
 
     def capture(self) -> None:
         """Record every scan's loss launches into one CUDA graph."""

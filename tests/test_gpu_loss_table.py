@@ -108,3 +108,26 @@ def test_table_loss_plans_and_repeatability(case):
     for i in (0, 37):
         ref, _ = so.phase_variance_loss(prep.g_half, prep.geo, so.Aberrations(*rows[i]), prep.dc)
         assert big[i] == pytest.approx(ref, rel=LOSS_RTOL, abs=LOSS_ATOL)
+
+
+@pytest.mark.parametrize("flags", [0, QSSB_FLAG_CHI_FP64])
+def test_table_loss_with_spherical_aberration(case, flags):
+    """C30 != 0 (no quadratic factorisation): the pair kernel takes the probe
+    phases directly and only the apertures from the table; against the FP64
+    oracle and the table-free kernel."""
+    prep, cal, d = case
+    table = ops.overlap_table(d["geom"], d["q_row"], d["q_col"], cal)
+    rows = [(-120.0, 55.0, math.radians(17.0), 3.0e4), (40.0, 20.0, 0.4, 8.0e4),
+            (0.0, 0.0, 0.0, 1.0e4)]
+    cands = torch.tensor(rows, dtype=torch.float32, device=DEV)
+    losses, mp = ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands,
+                                flags=flags, want_mean_phase=True, overlap=table)
+    plain, _ = ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands, flags=flags)
+    losses, mp, plain = losses.cpu().numpy(), mp.cpu().numpy(), plain.cpu().numpy()
+    for i, (a, b, c, c30) in enumerate(rows):
+        ref_loss, ref_mean = so.phase_variance_loss(prep.g_half, prep.geo,
+                                                    so.Aberrations(a, b, c, C30=c30), prep.dc)
+        assert losses[i] == pytest.approx(ref_loss, rel=LOSS_RTOL, abs=LOSS_ATOL), (i, flags)
+        assert losses[i] == pytest.approx(plain[i], rel=5e-6, abs=1e-7)
+        err = np.abs(so.wrapped_phase_error(mp[i], ref_mean))
+        assert np.percentile(err, 99.9) < PHASE_ATOL
