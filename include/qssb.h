@@ -260,9 +260,9 @@ int qssb_loss_batch(const float* g_half, const float* bf_geom, const float* q_ro
 /* Bytes of the overlap table of a 128x128-scan dataset: float2 [n_bf][8383]. */
 int qssb_overlap_table_bytes(const qssb_calibration_t* cal, size_t* bytes);
 
-/* The candidate-independent part of the quadratic-chi overlap of a 128x128
- * dataset: table[b][e] = A(k_b) (A(q - k_b) - A(q + k_b), A(q - k_b) + A(q + k_b))
- * on the half set the loss evaluates (rows 0..64 x all columns, then
+/* The candidate-independent part of the overlap of a 128x128 dataset, the
+ * aperture pair table[b][e] = (A(q - k_b), A(q + k_b)) on the half set the
+ * loss evaluates (rows 0..64 x all columns, then
  * (127 - j, 64) for j < 63), with the loss kernels' aperture rule (FP64 where
  * the two apertures tie in the soft edge). The reference recomputes these
  * apertures for every candidate inside gamma_mul_pk_onthefly

@@ -461,13 +461,12 @@ __global__ void __launch_bounds__(256) k_loss_final(const double* __restrict__ b
 // ---------------------------------------- N = 128 with the overlap table
 // For quadratic chi the overlap factorises (corrected_quad in
 // qssb_device.cuh): C_b(q) = G_b(q) e^{-i theta} (d cos Q + i s sin Q) / |.|,
-// where theta = 2 q^T M k_b and Q(q) depend on the candidate but
-//   (d, s) = A(k_b) (A(q - k_b) - A(q + k_b), A(q - k_b) + A(q + k_b))
-// does not. k_overlap_table128 evaluates (d, s) once per dataset on the
-// evaluated half set (rows 0..64 x 128 columns, then (127 - j, 64), j < 63),
-// with the kernels' aperture arithmetic and FP64 tie rule, so a candidate
-// costs a table read, a separable phase product and one reciprocal square
-// root per element.
+// where theta = 2 q^T M k_b and Q(q) depend on the candidate but the
+// aperture pair (A(q - k_b), A(q + k_b)) does not. k_overlap_table128
+// evaluates the pair once per dataset on the evaluated half set (rows
+// 0..64 x 128 columns, then (127 - j, 64), j < 63), with the kernels'
+// aperture arithmetic and FP64 tie rule, so a candidate costs a table read,
+// a separable phase product and one reciprocal square root per element.
 constexpr int kNE128 = 65 * 128 + 63;
 
 __device__ __forceinline__ void elem_rc128(int e, int& r, int& c) {
@@ -490,7 +489,6 @@ __global__ void __launch_bounds__(256) k_overlap_table128(
     elem_rc128(e, r, c);
     const float kx = __ldg(geom + b);
     const float ky = __ldg(geom + n_bf + b);
-    const float ak = __ldg(geom + 5 * n_bf + b);
     const float qx = __ldg(q_row + r);
     const float qy = __ldg(q_col + c);
     const float dxm = qx - kx, dym = qy - ky;
@@ -507,16 +505,16 @@ __global__ void __launch_bounds__(256) k_overlap_table128(
         am = soft_aperture_fp64(qx64 - kx64, qy64 - ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
         ap = soft_aperture_fp64(qx64 + kx64, qy64 + ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
     }
-    table[(size_t)b * kNE128 + e] = make_float2(ak * (am - ap), ak * (am + ap));
+    table[(size_t)b * kNE128 + e] = make_float2(am, ap);
 }
 
-// C = G conj(Gamma_hat) from the table entry ds = (d, s), e^{-i Q} = eq and
-// e^{i theta} = e (corrected_quad_e with A(k) folded into ds).
-__device__ __forceinline__ float2 corrected_table(float2 ds, float2 eq, float2 e, float2 g) {
-    const float dr = ds.x * eq.x;
-    const float di = -ds.y * eq.y;
-    float gr = fmaf(e.x, dr, -e.y * di);
-    float gi = fmaf(e.x, di, e.y * dr);
+// C = G conj(Gamma_hat) from the table entry a = (A(q - k), A(q + k)),
+// e^{-i Q} = eq, e^{i theta} = e and A(k) = ak: corrected_quad_e's arithmetic.
+__device__ __forceinline__ float2 corrected_table(float2 a, float2 eq, float2 e, float ak, float2 g) {
+    const float dr = (a.x - a.y) * eq.x;
+    const float di = -(a.x + a.y) * eq.y;
+    float gr = ak * fmaf(e.x, dr, -e.y * di);
+    float gi = ak * fmaf(e.x, di, e.y * dr);
     const float m2 = fmaf(gr, gr, gi * gi);
     const float inv = m2 > 1e-16f ? rsqrtf(m2) : 1e8f;
     gr *= inv;
@@ -525,15 +523,15 @@ __device__ __forceinline__ float2 corrected_table(float2 ds, float2 eq, float2 e
 }
 
 // The same from the table without the quadratic factorisation (C30 != 0):
-// with m = A(k) A(q-k) = (s + d) / 2 and l = A(k) A(q+k) = (s - d) / 2,
+// with m = A(k) A(q-k) and l = A(k) A(q+k),
 //   Gamma = m e^{-i chi(q-k)} e^{i chi(k)} - l e^{i chi(q+k)} e^{-i chi(k)}
 // (corrected with the apertures from the table); ek = e^{i chi(k)}.
 template <bool CHI64>
-__device__ __forceinline__ float2 corrected_table_direct(float2 ds, float qx, float qy, float kx,
-                                                         float ky, float2 ek, float2 g,
+__device__ __forceinline__ float2 corrected_table_direct(float2 a, float qx, float qy, float kx,
+                                                         float ky, float ak, float2 ek, float2 g,
                                                          const Probe& p) {
-    const float m = 0.5f * (ds.y + ds.x);
-    const float l = 0.5f * (ds.y - ds.x);
+    const float m = ak * a.x;
+    const float l = ak * a.y;
     const Disp dm = displacement(qx - kx, qy - ky, p);
     const Disp dp = displacement(qx + kx, qy + ky, p);
     float sm, cm, sp, cp;
@@ -692,6 +690,8 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
                 nt2 = __ldg(t2 + tid);
                 if constexpr (QUAD) neq = __ldg(eqc + r * N + c);
             }
+            const float ak1 = __ldg(geom + 5 * n_bf + b1);
+            const float ak2 = __ldg(geom + 5 * n_bf + b2);
             float k1x = 0.f, k1y = 0.f, k2x = 0.f, k2y = 0.f;
             if constexpr (!QUAD) {
                 k1x = __ldg(geom + b1);
@@ -720,13 +720,13 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
                 }
                 float2 v1, v2;
                 if constexpr (QUAD) {
-                    v1 = corrected_table(d1, eqv, cmul(ph[r], ph[128 + c]), gv1);
-                    v2 = corrected_table(d2, eqv, cmul(ph[256 + r], ph[384 + c]), gv2);
+                    v1 = corrected_table(d1, eqv, cmul(ph[r], ph[128 + c]), ak1, gv1);
+                    v2 = corrected_table(d2, eqv, cmul(ph[256 + r], ph[384 + c]), ak2, gv2);
                 } else {
                     const float qx = __ldg(q_row + r);
                     const float qy = __ldg(q_col + c);
-                    v1 = corrected_table_direct<CHI64>(d1, qx, qy, k1x, k1y, ph[0], gv1, p);
-                    v2 = corrected_table_direct<CHI64>(d2, qx, qy, k2x, k2y, ph[256], gv2, p);
+                    v1 = corrected_table_direct<CHI64>(d1, qx, qy, k1x, k1y, ak1, ph[0], gv1, p);
+                    v2 = corrected_table_direct<CHI64>(d2, qx, qy, k2x, k2y, ak2, ph[256], gv2, p);
                 }
                 if (!two) v2 = make_float2(0.0f, 0.0f);
                 if (r == 64 || c == 64) {

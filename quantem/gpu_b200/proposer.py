@@ -511,3 +511,133 @@ def compass_search(be, start: np.ndarray, steps: np.ndarray, rounds: int, done=N
         if done is not None and done(from_x(x)[0]):
             return from_x(x)[0], evals, r + 1
     return from_x(x)[0], evals, rounds
+
+
+def _quadratic_design(u: np.ndarray, kind: str) -> np.ndarray:
+    """Columns of a quadratic model in u [n, d]: 1, u_i, then u_i u_j (i <= j,
+    kind "full") or u_i^2 (kind "diag"); kind "linear" stops after u_i."""
+    n, d = u.shape
+    cols = [np.ones(n), *u.T]
+    if kind == "full":
+        cols += [u[:, i] * u[:, j] for i in range(d) for j in range(i, d)]
+    elif kind == "diag":
+        cols += [u[:, i] * u[:, i] for i in range(d)]
+    return np.stack(cols, axis=1)
+
+
+def _model_step(coef: np.ndarray, d: int, kind: str, radius: float) -> np.ndarray:
+    """Minimiser of the fitted quadratic within |u| <= radius: the Newton step
+    when the Hessian is positive definite and the step fits, else the
+    trust-region step (H + lambda I) u = -g with lambda found by bisection."""
+    g = coef[1:1 + d]
+    h = np.zeros((d, d))
+    if kind == "full":
+        k = 1 + d
+        for i in range(d):
+            for j in range(i, d):
+                if i == j:
+                    h[i, i] = 2.0 * coef[k]
+                else:
+                    h[i, j] = h[j, i] = coef[k]
+                k += 1
+    elif kind == "diag":
+        h = np.diag(2.0 * coef[1 + d:1 + 2 * d])
+    gn = float(np.linalg.norm(g))
+    if kind == "linear" or gn == 0.0:
+        return -radius * g / gn if gn > 0 else np.zeros(d)
+    lam_min = float(np.linalg.eigvalsh(h).min())
+    if lam_min > 0:
+        u = np.linalg.solve(h, -g)
+        if np.linalg.norm(u) <= radius:
+            return u
+    lo_l, hi_l = max(0.0, -lam_min) + 1e-12, max(0.0, -lam_min) + gn / radius + 1.0
+    for _ in range(60):
+        lam = 0.5 * (lo_l + hi_l)
+        u = np.linalg.solve(h + lam * np.eye(d), -g)
+        if np.linalg.norm(u) > radius:
+            lo_l = lam
+        else:
+            hi_l = lam
+    return np.linalg.solve(h + hi_l * np.eye(d), -g)
+
+
+def surrogate_search(be, starts: np.ndarray, widths: np.ndarray, batch: int, rounds: int,
+                     rng: np.random.Generator, done=None, lo=None, hi=None,
+                     radius0: float = 0.5, min_radius: float = 1e-4):
+    """Trust-region refinement with a quadratic surrogate of the
+    phase-variance loss, ``batch`` SSB evaluations per round (one
+    ``qssb_loss_batch`` call), in x = (C10, a, b, C30) scaled by ``widths``.
+
+    Round 0 scores the start points (a proposal's two sign hypotheses) and
+    draws around the first. Each later round fits a weighted least-squares
+    quadratic (full, then diagonal, then linear as the points allow) to the
+    scored points nearest the incumbent, takes its minimiser within the trust
+    radius, and scores it, half of that step, and points at half the radius
+    around it (which keep the next fit well posed). The radius doubles when
+    the full step hits the boundary and wins, and halves when nothing beats
+    the incumbent. ``done(best_aberrations)`` ends it early. Returns
+    (best (C10, C12, phi12, C30), SSB evaluations, rounds)."""
+    lo = BOX_LO if lo is None else np.asarray(lo, np.float64)
+    hi = BOX_HI if hi is None else np.asarray(hi, np.float64)
+    w = np.asarray(widths, np.float64)
+    d = 4
+    xs: list[np.ndarray] = []
+    fs: list[float] = []
+
+    def score(cand: np.ndarray) -> None:
+        cand = np.clip(cand, lo, hi)
+        ab = from_x(cand)
+        losses = be.variance_loss_batch(ab[:, 0], ab[:, 1], ab[:, 2], ab[:, 3]).cpu().numpy()
+        xs.extend(cand)
+        fs.extend(float(v) for v in losses)
+
+    starts = np.clip(np.array(starts, np.float64, ndmin=2).reshape(-1, d), lo, hi)[:batch]
+    extra = batch - len(starts)
+    cand = starts
+    if extra > 0:
+        cand = np.vstack([starts, starts[0] + rng.normal(0.0, radius0, (extra, d)) * w])
+    score(cand)
+    best = int(np.argmin(fs))
+    c, fc = xs[best].copy(), fs[best]
+    radius = radius0
+    if done is not None and done(from_x(c)[0]):
+        return from_x(c)[0], len(fs), 0
+    for r in range(1, rounds):
+        X = np.asarray(xs)
+        F = np.asarray(fs)
+        U = (X - c) / w
+        dist = np.linalg.norm(U, axis=1)
+        order = np.argsort(dist)
+        near = order[dist[order] <= 2.0 * radius]
+        if len(near) < 24:
+            near = order[:min(len(order), 24)]
+        n = len(near)
+        kind = "full" if n >= 18 else ("diag" if n >= 11 else "linear")
+        A = _quadratic_design(U[near], kind)
+        wt = 1.0 / (1.0 + (dist[near] / radius) ** 2)
+        coef = np.linalg.lstsq(A * wt[:, None], (F[near] - fc) * wt, rcond=None)[0]
+        u = _model_step(coef, d, kind, radius)
+        step = c + u * w
+        v = rng.normal(size=(batch - 2, d))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        cand = np.vstack([step, c + 0.5 * u * w, step + 0.5 * radius * v * w])
+        n0 = len(fs)
+        score(cand)
+        j = n0 + int(np.argmin(fs[n0:]))
+        if fs[j] < fc:
+            moved = float(np.linalg.norm((xs[j] - c) / w))
+            c, fc = xs[j].copy(), fs[j]
+            # the radius follows the step: doubled when a full step to the
+            # boundary won, else twice the distance moved (at most a quarter
+            # of the old radius less)
+            if j == n0 and np.linalg.norm(u) >= 0.9 * radius:
+                radius = min(2.0 * radius, 2.0)
+            else:
+                radius = min(radius, max(2.0 * moved, 0.25 * radius))
+        else:
+            radius *= 0.5
+        if done is not None and done(from_x(c)[0]):
+            return from_x(c)[0], len(fs), r + 1
+        if radius < min_radius:
+            break
+    return from_x(c)[0], len(fs), rounds

@@ -56,6 +56,9 @@ class SyntheticSpec:
     lattice_A: float = 4.0
     vacancy_fraction: float = 0.05
     seed: int = 0
+    # False: counts are the expected intensities rounded to integers (no
+    # Poisson noise), for studies whose error floor must not be shot noise
+    poisson: bool = True
 
     def aberrations(self) -> dict[str, float]:
         """Aberrations in the reference's numeric convention (Angstrom, rad)."""
@@ -211,7 +214,7 @@ def generate(spec: SyntheticSpec, device: torch.device | str = "cpu",
             intens[s:e] = intensities(s, e)
         scale = spec.dose / intens.sum(dim=(1, 2)).mean()
         intens *= scale
-        counts = torch.poisson(intens, generator=gen)
+        counts = torch.poisson(intens, generator=gen) if spec.poisson else torch.round(intens)
         counts = torch.clamp(counts, max=65535).to(torch.int32).to(torch.uint16)
     else:
         # large acquisitions: two streaming passes (frame totals, then counts
@@ -224,7 +227,7 @@ def generate(spec: SyntheticSpec, device: torch.device | str = "cpu",
         for s in range(0, n_frames, batch):
             e = min(n_frames, s + batch)
             lam_b = intensities(s, e) * scale.to(torch.float32)
-            c = torch.poisson(lam_b, generator=gen)
+            c = torch.poisson(lam_b, generator=gen) if spec.poisson else torch.round(lam_b)
             counts[s:e] = torch.clamp(c, max=65535).to(torch.int32).to(torch.uint16)
     counts = counts.reshape(r0, r1, k0, k1)
     return SyntheticData(counts=counts, spec=spec, object_phase=phi,

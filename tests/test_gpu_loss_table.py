@@ -66,9 +66,9 @@ def test_table_loss_matches_oracle_and_table_free_kernel(case, flags):
 
 
 def test_table_matches_fp64_apertures(case):
-    """table[b][e] = A(k)(A(q-k) -+ A(q+k)) on the evaluated half set: the
-    float32 fast aperture with the FP64 tie rule, within float32 rounding of
-    an FP64 evaluation except where the rule itself switched to FP64."""
+    """table[b][e] = (A(q-k), A(q+k)) on the evaluated half set: the float32
+    fast aperture with the FP64 tie rule, within float32 rounding of an FP64
+    evaluation except where the rule itself switched to FP64."""
     prep, cal, d = case
     table = ops.overlap_table(d["geom"], d["q_row"], d["q_col"], cal).cpu().numpy().astype(np.float64)
     n = prep.scan_shape[0]
@@ -81,8 +81,7 @@ def test_table_matches_fp64_apertures(case):
     ky = geo.ky[:, None].astype(np.float64)
     am = so._aperture_and_angles(qx - kx, qy - ky, geo)[3]
     ap = so._aperture_and_angles(qx + kx, qy + ky, geo)[3]
-    ak = geo.aperture_k[:, None]
-    want = np.stack([ak * (am - ap), ak * (am + ap)], axis=-1)
+    want = np.stack([am, ap], axis=-1)
     assert table.shape == want.shape
     assert np.abs(table - want).max() <= 2e-5
 
