@@ -184,6 +184,44 @@ int qssb_export_bf_columns(const void* counts, int32_t in_bytes, int64_t n_scan,
 int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t scan_rows,
                        int32_t scan_cols, float* g_half, void* stream);
 
+/* The BF columns written by the frame-sum pass (no counterpart as one step in
+ * the reference, whose _extract_gqk gathers after the selection,
+ * backend.py:520-589). A cold reconstruction then reads the counts once:
+ *
+ * qssb_bf_box_estimate: from u64 sums of some frames (e.g. the first 512, by
+ * qssb_mean_dp_u64 on that prefix), a superset box of the BF disk: the
+ * bounding box of the pixels at >= 1/4 of the largest sum (or, with
+ * radius_px > 0, their centroid +- radius_px), widened by margin, columns
+ * rounded out to multiples of 8. box: device int32[8] = r0, r1, c0, c1
+ * (half-open), width, pixel count, valid (pixel count <= capacity), unused. */
+int qssb_bf_box_estimate(const uint64_t* sums, int32_t det_rows, int32_t det_cols,
+                         float radius_px, int32_t margin, int64_t capacity, int32_t* box,
+                         void* stream);
+
+/* qssb_mean_dp_u64 (sums only) that also writes, when the box is valid and
+ * consistent (inside the detector, 8-pixel columns, at most capacity
+ * pixels), the box's columns box_cols[(r - r0) * width + (c - c0)][f] =
+ * counts[f][r][c] (u16, capacity x n_frames). det_cols and n_frames multiples
+ * of 8, counts and box_cols 16-byte aligned. */
+int qssb_mean_dp_u64_box(const uint16_t* counts, int64_t n_frames, int32_t det_rows,
+                         int32_t det_cols, uint64_t* sums, const int32_t* box, int64_t capacity,
+                         uint16_t* box_cols, void* stream);
+
+/* After qssb_select_bf: map[b] = box column of BF pixel b (-1 outside the
+ * box) for b < min(n_bf, capacity), and *ok = 1 when every BF pixel lies in
+ * a valid box of at most box_capacity pixels (else the caller gathers with
+ * qssb_gather_bf_columns_2d). */
+int qssb_bf_box_map(const int32_t* bf_linear, const qssb_bf_info_t* info, int32_t det_rows,
+                    int32_t det_cols, int32_t capacity, int64_t box_capacity,
+                    const int32_t* box, int32_t* map, int32_t* ok, void* stream);
+
+/* qssb_scan_fft_half for 128x128 scans reading BF pixel b's image from
+ * column map[b] of the n_cols columns [n_cols][R0*R1] (the box columns);
+ * map entries must come from a qssb_bf_box_map whose ok flag was set. */
+int qssb_scan_fft_half_mapped(const uint16_t* columns, int64_t n_cols, const int32_t* map,
+                              int32_t n_bf, int32_t scan_rows, int32_t scan_cols, float* g_half,
+                              void* stream);
+
 /* Workspace bytes needed by qssb_object for this calibration. */
 int qssb_object_workspace_bytes(const qssb_calibration_t* cal, int32_t flags, size_t* bytes);
 

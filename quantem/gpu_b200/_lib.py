@@ -117,6 +117,10 @@ SIGNATURES = {
                                         _P, _P]),
     "qssb_scan_fft_half": (ctypes.c_int, [_P, _I32, _I32, _I32, _P, _P]),
     "qssb_count_max": (ctypes.c_int, [_P, _I32, _I64, _P, _P]),
+    "qssb_bf_box_estimate": (ctypes.c_int, [_P, _I32, _I32, ctypes.c_float, _I32, _I64, _P, _P]),
+    "qssb_mean_dp_u64_box": (ctypes.c_int, [_P, _I64, _I32, _I32, _P, _P, _I64, _P, _P]),
+    "qssb_bf_box_map": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _I64, _P, _P, _P, _P]),
+    "qssb_scan_fft_half_mapped": (ctypes.c_int, [_P, _I64, _P, _I32, _I32, _I32, _P, _P]),
     "qssb_export_bf_columns": (ctypes.c_int, [_P, _I32, _I64, _I64, _P, _I32, _P, _I32, _P]),
     "qssb_object_workspace_bytes": (
         ctypes.c_int, [ctypes.POINTER(Calibration), _I32, ctypes.POINTER(_SZ)]),

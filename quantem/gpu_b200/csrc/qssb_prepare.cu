@@ -243,8 +243,19 @@ struct ScanFft128PSmem {
     static constexpr size_t bytes = u_bytes + h_bytes + tw_bytes;
 };
 
+// map (optional): BF pixel b's image is column map[b] of the n_cols in
+// `columns` (the box columns of qssb_mean_dp_u64_box); an index outside
+// [0, n_cols) is clamped (callers pass only maps whose ok flag was set).
+__device__ __forceinline__ int scan_column(const int32_t* map, int b, int n_cols) {
+    if (!map) return b;
+    const int c = __ldg(map + b);
+    return c < 0 ? 0 : (c >= n_cols ? n_cols - 1 : c);
+}
+
 __global__ void __launch_bounds__(256, 2) k_scan_fft128p(const uint16_t* __restrict__ columns,
-                                                         int n_bf, float2* __restrict__ g_half) {
+                                                         int n_bf, float2* __restrict__ g_half,
+                                                         const int32_t* __restrict__ map,
+                                                         int n_cols) {
     extern __shared__ float4 smem4[];
     char* base = reinterpret_cast<char*>(smem4);
     float2* T = reinterpret_cast<float2*>(base);       // FFT scratch ...
@@ -259,7 +270,7 @@ __global__ void __launch_bounds__(256, 2) k_scan_fft128p(const uint16_t* __restr
     const int grp = lane >> 3;
     float2* Tg = T + g * kG8Scratch;
     fill_twiddles<128>(tw, tid, 256);
-    if (blockIdx.x < n_bf) stage_image_async<256>(img, columns, blockIdx.x, tid);
+    if (blockIdx.x < n_bf) stage_image_async<256>(img, columns, scan_column(map, blockIdx.x, n_cols), tid);
     for (int b = blockIdx.x; b < n_bf; b += gridDim.x) {
         cp_async_wait_all();
         __syncthreads();  // the image is in; the previous copy-out of H is done
@@ -335,7 +346,7 @@ __global__ void __launch_bounds__(256, 2) k_scan_fft128p(const uint16_t* __restr
         }
         __syncthreads();  // T is free: the next image comes in during the copy-out
         const int nb = b + gridDim.x;
-        if (nb < n_bf) stage_image_async<256>(img, columns, nb, tid);
+        if (nb < n_bf) stage_image_async<256>(img, columns, scan_column(map, nb, n_cols), tid);
         const float4* h4 = reinterpret_cast<const float4*>(H);
         float4* dst = reinterpret_cast<float4*>(g_half + (size_t)b * 128 * kScanHalf);
         for (int i = tid; i < 128 * kScanHalf / 2; i += 256) dst[i] = h4[i];
@@ -1037,7 +1048,8 @@ extern "C" int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t
                                           (int)smem));
             const int slots = 2 * device_sm_count();
             const int grid = n_bf < slots ? n_bf : slots;
-            k_scan_fft128p<<<grid, 256, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half));
+            k_scan_fft128p<<<grid, 256, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half),
+                                                   nullptr, n_bf);
             CUDA_TRY(cudaGetLastError());
             return QSSB_OK;
         }
@@ -1048,4 +1060,27 @@ extern "C" int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t
             return set_error(QSSB_ERR_UNSUPPORTED,
                              "qssb_scan_fft_half: scan size must be 64, 128, 256, 512 or 1024");
     }
+}
+
+extern "C" int qssb_scan_fft_half_mapped(const uint16_t* columns, int64_t n_cols,
+                                         const int32_t* map, int32_t n_bf, int32_t scan_rows,
+                                         int32_t scan_cols, float* g_half, void* stream) {
+    if (!columns || !map || !g_half || n_bf <= 0 || n_cols <= 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_scan_fft_half_mapped: null pointer or empty shape");
+    if (scan_rows != 128 || scan_cols != 128)
+        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_scan_fft_half_mapped: 128x128 scans only");
+    if (((uintptr_t)columns & 15u) != 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_scan_fft_half_mapped: columns must be 16-byte aligned");
+    if (n_cols > 0x7fffffff)
+        return set_error(QSSB_ERR_INVALID, "qssb_scan_fft_half_mapped: too many columns");
+    cudaStream_t s = (cudaStream_t)stream;
+    const size_t smem = ScanFft128PSmem::bytes;
+    CUDA_TRY(cudaFuncSetAttribute(k_scan_fft128p, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem));
+    const int slots = 2 * device_sm_count();
+    const int grid = n_bf < slots ? n_bf : slots;
+    k_scan_fft128p<<<grid, 256, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half), map,
+                                           (int)n_cols);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
 }

@@ -33,6 +33,10 @@ LAUNCHES_PER_CALL = {
     "qssb_join_object_waves": 1,
     "qssb_phase_atan2": 1,
     "qssb_count_max": 1,
+    "qssb_bf_box_estimate": 1,
+    "qssb_mean_dp_u64_box": 1,
+    "qssb_bf_box_map": 1,
+    "qssb_scan_fft_half_mapped": 1,
     "qssb_export_bf_columns": 1,
 }
 LAUNCH_COUNT = 0
@@ -235,6 +239,72 @@ def bf_geometry(sel: DeviceSelection, det_shape: tuple[int, int], k_step: tuple[
     _call("qssb_bf_geometry", sel.bf_linear.device, _ptr(sel.bf_linear), _ptr(sel.info), k0, k1,
           cap, ctypes.byref(gp), _ptr(geom), _stream(geom))
     return geom
+
+
+BOX_WORDS = 8  # the device box record: r0, r1, c0, c1, width, pixels, valid, unused
+
+
+def bf_box_estimate(sample_sums: torch.Tensor, det_shape: tuple[int, int], capacity: int,
+                    radius_px: float = 0.0, margin: int = 2,
+                    out: torch.Tensor | None = None) -> torch.Tensor:
+    """Superset box of the BF disk from u64 sums of some frames (device int32[8])."""
+    _require_cuda(sample_sums, "sample_sums", torch.int64)
+    box = out if out is not None else torch.empty(BOX_WORDS, dtype=torch.int32,
+                                                  device=sample_sums.device)
+    _call("qssb_bf_box_estimate", sample_sums.device, _ptr(sample_sums), int(det_shape[0]),
+          int(det_shape[1]), float(radius_px), int(margin), int(capacity), _ptr(box),
+          _stream(sample_sums))
+    return box
+
+
+def mean_dp_u64_box(counts: torch.Tensor, box: torch.Tensor, box_cols: torch.Tensor,
+                    sums: torch.Tensor | None = None) -> torch.Tensor:
+    """Exact u64 frame sums (int64 [K0, K1]) that also write the box's columns."""
+    _require_cuda(counts, "counts", torch.uint16)
+    _require_cuda(box, "box", torch.int32)
+    _require_cuda(box_cols, "box_cols", torch.uint16)
+    k0, k1 = int(counts.shape[-2]), int(counts.shape[-1])
+    n_frames = counts.numel() // (k0 * k1)
+    if box_cols.ndim != 2 or box_cols.shape[1] != n_frames:
+        raise ValueError("box_cols must be [capacity, n_frames]")
+    if sums is None:
+        sums = torch.empty((k0, k1), dtype=torch.int64, device=counts.device)
+    _call("qssb_mean_dp_u64_box", counts.device, _ptr(counts), n_frames, k0, k1, _ptr(sums),
+          _ptr(box), int(box_cols.shape[0]), _ptr(box_cols), _stream(counts))
+    return sums
+
+
+def bf_box_map(sel: DeviceSelection, det_shape: tuple[int, int], box: torch.Tensor,
+               capacity: int, out: tuple[torch.Tensor, torch.Tensor] | None = None
+               ) -> tuple[torch.Tensor, torch.Tensor]:
+    """(map int32 [capacity]: BF pixel -> box column, ok int32 [1]); capacity
+    is the box columns' row count (the map holds as many entries)."""
+    dev = sel.bf_linear.device
+    if out is None:
+        out = (torch.empty(capacity, dtype=torch.int32, device=dev),
+               torch.empty(1, dtype=torch.int32, device=dev))
+    bmap, ok = out
+    _call("qssb_bf_box_map", dev, _ptr(sel.bf_linear), _ptr(sel.info), int(det_shape[0]),
+          int(det_shape[1]), int(min(capacity, bmap.numel())), int(capacity), _ptr(box), _ptr(bmap),
+          _ptr(ok), _stream(box))
+    return bmap, ok
+
+
+def scan_fft_half_mapped(box_cols: torch.Tensor, bf_map: torch.Tensor, n_bf: int,
+                         scan_shape: tuple[int, int], out: torch.Tensor | None = None
+                         ) -> torch.Tensor:
+    """Hermitian half-plane scan spectra of BF pixels whose images are box
+    columns ``bf_map[b]`` (128x128 scans)."""
+    _require_cuda(box_cols, "box_cols", torch.uint16)
+    _require_cuda(bf_map, "bf_map", torch.int32)
+    r0, r1 = int(scan_shape[0]), int(scan_shape[1])
+    if box_cols.shape[1] != r0 * r1 or bf_map.numel() < n_bf:
+        raise ValueError("box_cols must be [capacity, R0*R1] and bf_map hold n_bf entries")
+    g = out if out is not None else torch.empty((n_bf, r0, r1 // 2 + 1), dtype=torch.complex64,
+                                                device=box_cols.device)
+    _call("qssb_scan_fft_half_mapped", box_cols.device, _ptr(box_cols), int(box_cols.shape[0]),
+          _ptr(bf_map), int(n_bf), r0, r1, _ptr(g), _stream(box_cols))
+    return g
 
 
 def gather_bf_columns(counts: torch.Tensor, bf_linear: torch.Tensor, validate: bool = True

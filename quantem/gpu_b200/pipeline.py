@@ -13,6 +13,16 @@ one shape and calibration (a detector feeding scans, a benchmark loop),
   ``qssb_object_ex`` (dc read from the device selection result), one graph
   per BF count, with buffers sized for it.
 
+At 128x128 scans (detector columns and frame count multiples of 8) the
+counts are read once: stage A first sums the first 512 frames and estimates
+a superset box of the BF disk (``qssb_bf_box_estimate``), the frame-sum pass
+writes the box's columns as it streams (``qssb_mean_dp_u64_box``), and after
+the selection ``qssb_bf_box_map`` maps every BF pixel to its box column;
+stage B then transforms straight from the box (``qssb_scan_fft_half_mapped``).
+When a BF pixel falls outside the box (the map's ok flag, read with the
+selection result) that run takes the gathering stage B instead, so results
+never depend on the estimate.
+
 Every ``run`` recomputes everything from the counts in the input buffer; only
 allocation and launch overhead are shared. The one host sync reads the BF
 count between the stages (the buffers of stage B depend on it).
@@ -37,7 +47,8 @@ class ColdReconstructor:
     def __init__(self, counts: torch.Tensor, *, semiangle: float, scan_sampling: float,
                  det_sampling: float, voltage_kV: float, bf_intensity_threshold: float = 0.0,
                  bf_radius: float | None = None, rotation_angle_deg: float = 0.0,
-                 aberrations: tuple = (0.0, 0.0, 0.0, 0.0), use_graphs: bool = True):
+                 aberrations: tuple = (0.0, 0.0, 0.0, 0.0), use_graphs: bool = True,
+                 use_box: bool = True):
         if counts.ndim != 4 or counts.dtype != torch.uint16 or not counts.is_cuda:
             raise ValueError("counts must be a CUDA uint16 tensor [R0, R1, K0, K1]")
         r0, r1, k0, k1 = (int(x) for x in counts.shape)
@@ -61,6 +72,18 @@ class ColdReconstructor:
         self.use_graphs = bool(use_graphs)
         self.q_row, self.q_col = _device_frequencies(self.scan_shape, self.scan_sampling, self.device)
         self.info_host = torch.empty(ops.BF_INFO_BYTES, dtype=torch.uint8, pin_memory=True)
+        # the box path: BF columns written by the frame-sum pass
+        self.use_box = (use_box and r0 == 128 and k1 % 8 == 0 and self.n_frames % 8 == 0
+                        and counts.data_ptr() % 16 == 0)
+        if self.use_box:
+            self.box_capacity = max(1, (k0 * k1) // 2)
+            self.box_cols = torch.empty((self.box_capacity, self.n_frames), dtype=torch.uint16,
+                                        device=self.device)
+            self.box = torch.empty(ops.BOX_WORDS, dtype=torch.int32, device=self.device)
+            self.box_map = (torch.empty(self.box_capacity, dtype=torch.int32, device=self.device),
+                            torch.empty(1, dtype=torch.int32, device=self.device))
+            self.ok_host = torch.zeros(1, dtype=torch.int32, pin_memory=True)
+        self.box_runs = 0  # runs that used the box columns
         self._graph_a = None
         self._b: dict[int, dict] = {}
         self.last_info = None
@@ -74,11 +97,24 @@ class ColdReconstructor:
                           non_blocking=True)
 
     # ------------------------------------------------------------ stage A
+    SAMPLE_FRAMES = 512  # frames whose sums place the box
+
     def _stage_a(self) -> None:
-        sums, _ = ops.mean_dp_u64(self.counts, want_mean=False)
+        if self.use_box:
+            frames = self.counts.view(-1, *self.det_shape)
+            sample, _ = ops.mean_dp_u64(frames[: min(self.SAMPLE_FRAMES, self.n_frames)],
+                                        want_mean=False)
+            ops.bf_box_estimate(sample, self.det_shape, self.box_capacity,
+                                radius_px=float(self.bf_radius or 0.0), out=self.box)
+            sums = ops.mean_dp_u64_box(self.counts, self.box, self.box_cols)
+        else:
+            sums, _ = ops.mean_dp_u64(self.counts, want_mean=False)
         sel = ops.select_bf(sums, self.det_shape, self.n_frames, self.threshold, self.bf_radius)
         geom = ops.bf_geometry(sel, self.det_shape, self.k_step, self.rotation, self.wavelength,
                                self.semiangle * 1e-3, (self.ang[0] * 1e-3, self.ang[1] * 1e-3))
+        if self.use_box:
+            ops.bf_box_map(sel, self.det_shape, self.box, self.box_capacity, out=self.box_map)
+            self.ok_host.copy_(self.box_map[1], non_blocking=True)
         self.info_host.copy_(sel.info, non_blocking=True)
         self._a = (sums, sel, geom)
 
@@ -91,7 +127,7 @@ class ColdReconstructor:
             dc_re=0.0, dc_im=0.0)
 
     # ------------------------------------------------------------ stage B
-    def _make_b(self, n_bf: int) -> dict:
+    def _make_b(self, n_bf: int, mapped: bool = False) -> dict:
         _, sel, geom_buf = self._a
         lin = sel.bf_linear[:n_bf]
         geom = geom_buf[: 8 * n_bf].view(8, n_bf)
@@ -103,8 +139,12 @@ class ColdReconstructor:
         st["ws"].get(ops.object_workspace_bytes(st["cal"]))
 
         def launch():
-            columns = ops.gather_bf_columns(self.counts, lin, validate=False)
-            g = ops.scan_fft_half(columns, self.scan_shape)
+            if mapped:
+                columns = None
+                g = ops.scan_fft_half_mapped(self.box_cols, self.box_map[0], n_bf, self.scan_shape)
+            else:
+                columns = ops.gather_bf_columns(self.counts, lin, validate=False)
+                g = ops.scan_fft_half(columns, self.scan_shape)
             ops.object_wave(g, geom, self.q_row, self.q_col, st["cal"], self.ab, workspace=st["ws"],
                             dc_device=dc_dev, out=(st["obj"], st["phase"]))
             st["keep"] = (columns, g)
@@ -145,10 +185,13 @@ class ColdReconstructor:
         self.last_info = info
         if info.n_bf <= 0:
             raise ValueError("No bright-field pixels selected.")
-        st = self._b.get(int(info.n_bf))
+        mapped = bool(self.use_box and int(self.ok_host[0]) == 1)
+        self.box_runs += int(mapped)
+        key = (int(info.n_bf), mapped)
+        st = self._b.get(key)
         if st is None:
-            st = self._make_b(int(info.n_bf))
-            self._b[int(info.n_bf)] = st
+            st = self._make_b(int(info.n_bf), mapped)
+            self._b[key] = st
         if self.use_graphs:
             st["graph"].replay()
             ops.LAUNCH_COUNT += st["launches"]

