@@ -295,6 +295,17 @@ int qssb_loss_batch(const float* g_half, const float* bf_geom, const float* q_ro
                     void* workspace, size_t workspace_bytes, float* losses,
                     float* mean_phase, void* stream);
 
+/* Registers a cancel flag: a device int32 (device memory, or pinned host
+ * memory mapped into the device address space for a live cancel) that the
+ * table-driven loss kernel (qssb_loss_batch_ex with a table) reads once per
+ * BF-pixel pair. Nonzero stops every CTA at its next pair; the batch's losses
+ * come back NaN. NULL unregisters. The pointer is a launch argument, so a
+ * CUDA graph keeps the one registered when it was captured. The reference
+ * cancels a remote job between stages (remote/ssb_api.py:624-679); this
+ * reaches into a running loss batch. The kernels have no unbounded loop: a
+ * flag that is never set changes nothing. */
+int qssb_set_cancel(const int32_t* flag);
+
 /* Bytes of the overlap table of a 128x128-scan dataset: float2 [n_bf][8383]. */
 int qssb_overlap_table_bytes(const qssb_calibration_t* cal, size_t* bytes);
 

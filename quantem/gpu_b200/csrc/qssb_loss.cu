@@ -459,6 +459,13 @@ __global__ void __launch_bounds__(256) k_loss_final(const double* __restrict__ b
 }
 
 // ---------------------------------------- N = 128 with the overlap table
+// The registered cancel flag (qssb_set_cancel): a device int the table
+// kernel polls once per BF pixel pair; nonzero stops every CTA at its next
+// pair and makes the losses NaN.
+static const int* g_cancel_flag = nullptr;
+static const int* cancel_flag() { return g_cancel_flag; }
+constexpr int kFusedFoldChunks = 32;
+
 // For quadratic chi the overlap factorises (corrected_quad in
 // qssb_device.cuh): C_b(q) = G_b(q) e^{-i theta} (d cos Q + i s sin Q) / |.|,
 // where theta = 2 q^T M k_b and Q(q) depend on the candidate but the
@@ -584,7 +591,8 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
     const float* __restrict__ q_row, const float* __restrict__ q_col,
     const float2* __restrict__ overlap, const qssb_aberrations_t* __restrict__ cands,
     qssb_calibration_t cal, const float2* __restrict__ eq_table, int bf_per_chunk, int n_chunks,
-    float* __restrict__ part, double* __restrict__ part_sq) {
+    float* __restrict__ part, double* __restrict__ part_sq, const int* __restrict__ cancel,
+    unsigned int* __restrict__ arrivals, float* __restrict__ losses, float* __restrict__ mean_phase) {
     constexpr int N = 128;
     constexpr int H = N / 2 + 1;
     constexpr int P = kL128P;
@@ -600,6 +608,7 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
     float* el = reinterpret_cast<float*>(na + 512);
     __shared__ Probe sp;
     __shared__ double s_red[16];
+    __shared__ int s_stop, s_last;
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
@@ -611,6 +620,7 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
     if (tid == 0) {
         const qssb_aberrations_t ab = cands[cand];
         sp = make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
+        s_stop = 0;
     }
     fill_twiddles<N>(tw, tid, 512);
     __syncthreads();
@@ -835,8 +845,12 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
                 acc[round][t] += a;
             }
         }
+        // the cancel flag, read by one thread so the whole CTA stops together
+        if (tid == 0 && cancel && *reinterpret_cast<const volatile int*>(cancel) != 0) s_stop = 1;
         __syncthreads();
+        if (s_stop) break;
     }
+    if (s_stop) sq = __longlong_as_double(0x7ff8000000000000LL);  // NaN: the loss reports it
     // row-major partial sum planes part[(cand * n_chunks + chunk) * N * N + y * N + x]
     float* ps = part + (size_t)(cand * n_chunks + chunk) * N * N;
 #pragma unroll
@@ -855,6 +869,39 @@ __global__ void __launch_bounds__(512, 1) k_loss_pair128(
 #pragma unroll
         for (int w = 0; w < 16; ++w) t += s_red[w];
         part_sq[cand * n_chunks + chunk] = t;
+    }
+    if (!arrivals) return;  // the fold runs as its own kernels
+    // In-kernel fold: the last of the candidate's chunks to finish folds them
+    // all (no CTA waits for another). Writers make their partials visible
+    // before counting in; the counter is left at 0 for the next launch.
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(arrivals + cand, 1u) == (unsigned)(n_chunks - 1);
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    constexpr int NN = N * N;
+    const float* pc = part + (size_t)cand * n_chunks * NN;
+    double neg = 0.0;
+    for (int j = tid; j < NN; j += 512) {
+        double t = 0.0;
+        for (int k = 0; k < n_chunks; ++k) t += (double)__ldcg(pc + (size_t)k * NN + j);
+        const double mean = t / (double)n_bf;
+        if (mean_phase) mean_phase[(size_t)cand * NN + j] = (float)mean;
+        neg -= mean * mean;
+    }
+    double* red = reinterpret_cast<double*>(S);  // S is free now
+    red[tid] = neg;
+    __syncthreads();
+    for (int w = 256; w > 0; w >>= 1) {
+        if (tid < w) red[tid] += red[tid + w];
+        __syncthreads();
+    }
+    if (tid == 0) {
+        double q = 0.0;
+        for (int k = 0; k < n_chunks; ++k) q += __ldcg(part_sq + (size_t)cand * n_chunks + k);
+        losses[cand] = (float)((red[0] + q / (double)n_bf) / (double)NN);
+        arrivals[cand] = 0u;
     }
 }
 
@@ -1326,13 +1373,20 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
         if (overlap) {
             // the pair kernel: sum planes (one per chunk) then one double per chunk
             double* part_sq = reinterpret_cast<double*>(part + (size_t)n_cand * pl.n_chunks * N * N);
+            // a candidate's chunks folded by its last CTA when they are few
+            // (one launch); many chunks fold faster in the parallel kernels
+            const bool fused = pl.n_chunks <= kFusedFoldChunks;
+            unsigned int* arrivals = reinterpret_cast<unsigned int*>(part_sq + (size_t)n_cand * pl.n_chunks);
+            if (fused) CUDA_TRY(cudaMemsetAsync(arrivals, 0, sizeof(unsigned int) * n_cand, s));
             const size_t smem = Pair128Smem::bytes;
             CUDA_TRY(cudaFuncSetAttribute(k_loss_pair128<CHI64, QUAD>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
             k_loss_pair128<CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), 512, smem, s>>>(
                 reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, overlap,
-                cands, cal, eq, pl.bf_per_chunk, pl.n_chunks, part, part_sq);
+                cands, cal, eq, pl.bf_per_chunk, pl.n_chunks, part, part_sq, cancel_flag(),
+                fused ? arrivals : nullptr, losses, mean_phase);
             CUDA_TRY(cudaGetLastError());
+            if (fused) return QSSB_OK;
             k_loss_reduce_sum<N><<<dim3(N * N / kReducePix, n_cand), kReducePix * kReduceSlices, 0, s>>>(
                 part, pl.n_chunks, cal.n_bf, var, mean_phase);
             CUDA_TRY(cudaGetLastError());
@@ -1699,5 +1753,10 @@ extern "C" int qssb_phase_atan2(const float* y, const float* x, float* out, int6
     if (blocks > cap) blocks = cap;
     k_phase_atan2<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(y, x, out, n);
     CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+extern "C" int qssb_set_cancel(const int32_t* flag) {
+    g_cancel_flag = flag;
     return QSSB_OK;
 }

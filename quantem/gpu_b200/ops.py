@@ -461,6 +461,20 @@ def loss_batch_full(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Te
     return losses, mp
 
 
+_CANCEL: torch.Tensor | None = None
+
+
+def set_cancel_flag(flag: torch.Tensor | None) -> None:
+    """Register (or with None clear) the device int32 flag the table-driven
+    loss kernel polls between BF-pixel pairs; nonzero stops a batch and its
+    losses come back NaN. The tensor is kept referenced while registered."""
+    global _CANCEL
+    if flag is not None:
+        _require_cuda(flag, "flag", torch.int32)
+    _CANCEL = flag
+    check(_lib.load().qssb_set_cancel(_ptr(flag)))
+
+
 def overlap_table(bf_geom: torch.Tensor, q_row: torch.Tensor, q_col: torch.Tensor,
                   cal: Calibration) -> torch.Tensor:
     """The candidate-independent overlap apertures of a 128x128-scan dataset

@@ -134,3 +134,28 @@ def test_table_loss_with_spherical_aberration(case, flags):
         assert losses[i] == pytest.approx(plain[i], rel=5e-6, abs=1e-7)
         err = np.abs(so.wrapped_phase_error(mp[i], ref_mean))
         assert np.percentile(err, 99.9) < PHASE_ATOL
+
+
+def test_cancel_flag_stops_a_batch_without_hanging(case):
+    """A registered cancel flag that is already set stops every CTA of the
+    table kernel at its first BF-pixel pair: the call returns (no hang) with
+    NaN losses; cleared, the next call gives the normal losses again; a flag
+    that is never set changes nothing."""
+    prep, cal, d = case
+    table = ops.overlap_table(d["geom"], d["q_row"], d["q_col"], cal)
+    cands = _cands(CANDS * 8)  # 40 candidates: the one-launch fold
+    run = lambda: ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands,  # noqa: E731
+                                 flags=QSSB_FLAG_QUADRATIC, overlap=table)[0].cpu().numpy()
+    want = run()
+    flag = torch.zeros(1, dtype=torch.int32, device=DEV)
+    try:
+        ops.set_cancel_flag(flag)
+        np.testing.assert_array_equal(run(), want)
+        flag.fill_(1)
+        got = run()
+        assert np.all(np.isnan(got))
+        flag.fill_(0)
+        np.testing.assert_array_equal(run(), want)
+    finally:
+        ops.set_cancel_flag(None)
+    np.testing.assert_array_equal(run(), want)
