@@ -13,15 +13,18 @@ one shape and calibration (a detector feeding scans, a benchmark loop),
   ``qssb_object_ex`` (dc read from the device selection result), one graph
   per BF count, with buffers sized for it.
 
-At 128x128 scans (detector columns and frame count multiples of 8) the
-counts are read once: stage A first sums the first 512 frames and estimates
+With ``use_box`` (128x128 scans, detector columns and frame count multiples
+of 8) the counts are read once: stage A first sums the first 512 frames and estimates
 a superset box of the BF disk (``qssb_bf_box_estimate``), the frame-sum pass
 writes the box's columns as it streams (``qssb_mean_dp_u64_box``), and after
 the selection ``qssb_bf_box_map`` maps every BF pixel to its box column;
 stage B then transforms straight from the box (``qssb_scan_fft_half_mapped``).
 When a BF pixel falls outside the box (the map's ok flag, read with the
 selection result) that run takes the gathering stage B instead, so results
-never depend on the estimate.
+never depend on the estimate. Off by default: on a B200 at 128^4 the sum
+pass's scattered 16-byte box-column stores (107 MB) add ~50 us, more than the
+gather (~60 us) they replace saves once the sample sums, the estimate and the
+map are counted (0.374 against 0.330 ms per reconstruction).
 
 Every ``run`` recomputes everything from the counts in the input buffer; only
 allocation and launch overhead are shared. The one host sync reads the BF
@@ -48,7 +51,7 @@ class ColdReconstructor:
                  det_sampling: float, voltage_kV: float, bf_intensity_threshold: float = 0.0,
                  bf_radius: float | None = None, rotation_angle_deg: float = 0.0,
                  aberrations: tuple = (0.0, 0.0, 0.0, 0.0), use_graphs: bool = True,
-                 use_box: bool = True):
+                 use_box: bool = False):
         if counts.ndim != 4 or counts.dtype != torch.uint16 or not counts.is_cuda:
             raise ValueError("counts must be a CUDA uint16 tensor [R0, R1, K0, K1]")
         r0, r1, k0, k1 = (int(x) for x in counts.shape)

@@ -58,7 +58,7 @@ def test_box_sums_and_columns_are_exact(counts128):
 
 
 def test_cold_reconstruction_through_the_box_is_bit_identical(counts128):
-    boxed = ColdReconstructor(counts128, **KW)
+    boxed = ColdReconstructor(counts128, use_box=True, **KW)
     plain = ColdReconstructor(counts128, use_box=False, **KW)
     assert boxed.use_box and not plain.use_box
     for _ in range(2):
@@ -77,7 +77,7 @@ def test_missed_disk_falls_back_to_the_gather(counts128):
     frames = shifted.view(-1, 128, 128)
     f16 = shifted.view(torch.int16).view(-1, 128, 128)
     f16[:512] = torch.roll(f16[:512], 12, dims=2)
-    boxed = ColdReconstructor(shifted, **KW)
+    boxed = ColdReconstructor(shifted, use_box=True, **KW)
     plain = ColdReconstructor(shifted, use_box=False, **KW)
     a = boxed.run().clone()
     b = plain.run().clone()
