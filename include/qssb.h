@@ -476,6 +476,20 @@ int qssb_gemm_bf16(const void* A, int32_t lda, int32_t trans_a, const void* B, i
                    int32_t trans_b, int32_t M, int32_t N, int32_t K, const float* bias,
                    int32_t accumulate, float* C, int32_t ldc, void* act_bf16, int32_t ld_act,
                    void* stream);
+
+/* The same GEMM on the 5th-generation tensor cores (tcgen05.mma kind::f16,
+ * FP32 accumulator in tensor memory), split over K: 128 x 128 output tiles,
+ * splits K ranges each, partial tiles in the workspace summed in split order
+ * (deterministic), then the epilogue of qssb_gemm_bf16. M and N multiples of
+ * 128, K a multiple of 64 x splits, leading dimensions multiples of 8, A and
+ * B 16-byte aligned, workspace 256-byte aligned and at least
+ * qssb_gemm_tc_workspace_bytes; its last 256 bytes hold an int set to 1 when
+ * a bounded wait inside the kernel gave up (the result is then invalid). */
+int qssb_gemm_tc_workspace_bytes(int32_t M, int32_t N, int32_t K, int32_t splits, size_t* bytes);
+int qssb_gemm_bf16_tc(const void* A, int32_t lda, int32_t trans_a, const void* B, int32_t ldb,
+                      int32_t trans_b, int32_t M, int32_t N, int32_t K, int32_t splits,
+                      const float* bias, int32_t accumulate, float* C, int32_t ldc, void* act_bf16,
+                      int32_t ld_act, void* workspace, size_t workspace_bytes, void* stream);
 /* dz = dy * GELU'(pre) (FP32 and BF16 copies), n elements. */
 int qssb_gelu_backward(const float* dy, const float* pre, int64_t n, void* dz_bf16, float* dz,
                        void* stream);

@@ -152,6 +152,9 @@ SIGNATURES = {
     "qssb_loss_batch_ex": (ctypes.c_int, [
         _P, _P, _P, _P, ctypes.POINTER(Calibration), _P, _I32, _I32, _P, _P, _SZ, _P, _P, _P]),
     "qssb_set_cancel": (ctypes.c_int, [_P]),
+    "qssb_gemm_tc_workspace_bytes": (ctypes.c_int, [_I32, _I32, _I32, _I32, ctypes.POINTER(_SZ)]),
+    "qssb_gemm_bf16_tc": (ctypes.c_int, [_P, _I32, _I32, _P, _I32, _I32, _I32, _I32, _I32, _I32, _P,
+                                         _I32, _P, _I32, _P, _I32, _P, _SZ, _P]),
     "qssb_overlap_table_bytes": (ctypes.c_int, [ctypes.POINTER(Calibration), ctypes.POINTER(_SZ)]),
     "qssb_overlap_table": (ctypes.c_int, [_P, _P, _P, ctypes.POINTER(Calibration), _P, _P]),
     "qssb_decode_bslz4_u16": (ctypes.c_int, [_P, ctypes.c_int64, _P, _I32, ctypes.c_int64, _P, _P,

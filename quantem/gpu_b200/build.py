@@ -16,7 +16,7 @@ PKG = Path(__file__).resolve().parent
 CSRC = PKG / "csrc"
 OUT = PKG / "libqssb.so"
 SOURCES = ["qssb_errors.cu", "qssb_prepare.cu", "qssb_select.cu", "qssb_object.cu", "qssb_loss.cu", "qssb_features.cu", "qssb_mlp.cu",
-           "qssb_temporal.cu", "qssb_decode.cu", "qssb_export.cu", "qssb_box.cu"]
+           "qssb_temporal.cu", "qssb_decode.cu", "qssb_export.cu", "qssb_box.cu", "qssb_gemm_tc.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared"]
 

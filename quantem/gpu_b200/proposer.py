@@ -436,7 +436,8 @@ def from_x(x: np.ndarray) -> np.ndarray:
 
 
 def zoom_search(be, centres: np.ndarray | None, half_widths: np.ndarray, batch: int, rounds: int,
-                shrink: float, rng: np.random.Generator, done=None, lo=None, hi=None):
+                shrink: float, rng: np.random.Generator, done=None, lo=None, hi=None,
+                history: tuple[list, list] | None = None):
     """Batched zoom search on the phase-variance loss in x = (C10, a, b, C30):
     each round scores ``batch`` candidates in one ``qssb_loss_batch`` call (the
     current best plus uniform draws in a box around it; the first round splits
@@ -469,6 +470,9 @@ def zoom_search(be, centres: np.ndarray | None, half_widths: np.ndarray, batch: 
         ab = from_x(cand)
         losses = be.variance_loss_batch(ab[:, 0], ab[:, 1], ab[:, 2], ab[:, 3]).cpu().numpy()
         evals += batch
+        if history is not None:
+            history[0].extend(cand)
+            history[1].extend(float(v) for v in losses)
         j = int(np.argmin(losses))
         if losses[j] < best_loss:
             best_x, best_loss = cand[j].copy(), float(losses[j])
@@ -563,7 +567,7 @@ def _model_step(coef: np.ndarray, d: int, kind: str, radius: float) -> np.ndarra
 
 def surrogate_search(be, starts: np.ndarray, widths: np.ndarray, batch: int, rounds: int,
                      rng: np.random.Generator, done=None, lo=None, hi=None,
-                     radius0: float = 0.5, min_radius: float = 1e-4):
+                     radius0: float = 0.5, min_radius: float = 1e-4, history=None):
     """Trust-region refinement with a quadratic surrogate of the
     phase-variance loss, ``batch`` SSB evaluations per round (one
     ``qssb_loss_batch`` call), in x = (C10, a, b, C30) scaled by ``widths``.
@@ -576,13 +580,16 @@ def surrogate_search(be, starts: np.ndarray, widths: np.ndarray, batch: int, rou
     around it (which keep the next fit well posed). The radius doubles when
     the full step hits the boundary and wins, and halves when nothing beats
     the incumbent. ``done(best_aberrations)`` ends it early. Returns
-    (best (C10, C12, phi12, C30), SSB evaluations, rounds)."""
+    (best (C10, C12, phi12, C30), SSB evaluations, rounds). ``history``
+    (scored points (xs, losses) of an earlier search on the same data) seeds
+    the fits; its evaluations are not counted again."""
     lo = BOX_LO if lo is None else np.asarray(lo, np.float64)
     hi = BOX_HI if hi is None else np.asarray(hi, np.float64)
     w = np.asarray(widths, np.float64)
     d = 4
-    xs: list[np.ndarray] = []
-    fs: list[float] = []
+    xs: list[np.ndarray] = [] if history is None else [np.asarray(x, np.float64) for x in history[0]]
+    fs: list[float] = [] if history is None else [float(f) for f in history[1]]
+    n_prior = len(fs)
 
     def score(cand: np.ndarray) -> None:
         cand = np.clip(cand, lo, hi)
@@ -601,7 +608,7 @@ def surrogate_search(be, starts: np.ndarray, widths: np.ndarray, batch: int, rou
     c, fc = xs[best].copy(), fs[best]
     radius = radius0
     if done is not None and done(from_x(c)[0]):
-        return from_x(c)[0], len(fs), 0
+        return from_x(c)[0], len(fs) - n_prior, 0
     for r in range(1, rounds):
         X = np.asarray(xs)
         F = np.asarray(fs)
@@ -637,7 +644,26 @@ def surrogate_search(be, starts: np.ndarray, widths: np.ndarray, batch: int, rou
         else:
             radius *= 0.5
         if done is not None and done(from_x(c)[0]):
-            return from_x(c)[0], len(fs), r + 1
+            return from_x(c)[0], len(fs) - n_prior, r + 1
         if radius < min_radius:
             break
-    return from_x(c)[0], len(fs), rounds
+    return from_x(c)[0], len(fs) - n_prior, rounds
+
+
+def learned_refine(be, hypotheses: np.ndarray, widths: np.ndarray, batch: int, rounds: int,
+                   rng: np.random.Generator, done=None, zoom_rounds: int = 6,
+                   zoom_shrink: float = 0.8, min_radius: float = 1e-7):
+    """The refinement after a proposal, ``batch`` evaluations per round: a
+    zoom over the two sign hypotheses (robust into the right basin), then the
+    trust-region quadratic surrogate from its best point, fitted to every
+    point scored so far (fast to a precise minimum). Returns (best (C10, C12,
+    phi12, C30), SSB evaluations, rounds)."""
+    hist: tuple[list, list] = ([], [])
+    best, ev1, r1 = zoom_search(be, hypotheses, widths, batch, zoom_rounds, zoom_shrink, rng,
+                                done=done, history=hist)
+    if done is not None and r1 < zoom_rounds:
+        return best, ev1, r1
+    w = np.asarray(widths, np.float64) * zoom_shrink ** zoom_rounds
+    best2, ev2, r2 = surrogate_search(be, to_x(best[None]), w, batch, max(1, rounds - r1), rng,
+                                      done=done, radius0=1.0, min_radius=min_radius, history=hist)
+    return best2, ev1 + ev2, r1 + r2
