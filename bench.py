@@ -519,23 +519,26 @@ def sweep_3scans(dev: torch.device, steps: int) -> dict:
     }
 
 
-# Box shrink per round of the 8-candidate refinement: the fastest of 0.9, 0.85,
-# 0.8, 0.75, 0.7 and 0.6 that reached tau on all of 16 simulated cases (mean
-# 71 evaluations; 0.75 missed one case, 0.7 five)
-LEARNED_SHRINK = 0.8
-
-
-def learned_fits(dev: torch.device, n_cases: int = 4, tau: float = 1e-3) -> dict:
+def learned_fits(dev: torch.device, n_cases: int = 12) -> dict:
     """Learned proposal + 8-candidate refinement vs the plain 64-candidate sweep.
 
     The proposer is trained here (50k forward-model samples of the 64^2 x 64^2
-    lattice) with the library's own kernels. Each case is a fully simulated
-    64^2-scan x 64^2-detector dataset (padded to 128^2 by the reference rule)
-    with aberrations drawn from the sweep ranges at 1e6 e per position. A fit
-    is done when the phase reconstructed at its current best estimate is
-    within ``tau`` rad RMS of the FP64-oracle phase at the true aberrations;
-    SSB evaluations (candidates scored) are counted to that point, and fits/s
-    is timed by replaying the same search without the checks."""
+    lattice, 40 epochs) with the library's own kernels (its large GEMMs on the
+    tcgen05 tensor cores). Each case is a fully simulated 64^2-scan x
+    64^2-detector dataset (padded to 128^2 by the reference rule) with
+    aberrations drawn from the sweep ranges at 1e6 e per position. Two
+    targets, with SSB evaluations (candidates scored) counted until the
+    current best estimate meets them:
+      * 1e-4 rad RMS from the FP64-oracle phase at the loss optimum (the
+        phase a converged fit returns; its aberrations are found by a long
+        refinement from the truth first);
+      * 1e-3 rad RMS from the FP64-oracle phase at the true aberrations (the
+        loss optimum of a 0.3 rad object sits 2-6e-4 rad from it even without
+        noise, so 1e-4 from the truth is out of reach of any loss minimiser).
+    plain = a 64-candidate zoom sweep over the whole range (at most 200
+    rounds); learned = the proposal's two sign hypotheses, then
+    ``proposer.learned_refine`` (8 per round). Fits/s come from replaying the
+    same searches without the checks."""
     from oracle import ssb_oracle as so
     from oracle import ssb_torch_fp64 as tf
     from quantem.gpu_b200 import B200SSBBackend
@@ -547,6 +550,12 @@ def learned_fits(dev: torch.device, n_cases: int = 4, tau: float = 1e-3) -> dict
     info = prop.train(n_samples=50_000, epochs=40)
     torch.cuda.synchronize(dev)
     train_s = time.perf_counter() - t0
+    # FLOPs of a training step at batch 256: forward 2 m n k per layer, backward
+    # the weight gradients of every layer and the input gradients of layers 2-4
+    dims = [pr.N_IN, pr.HIDDEN, pr.HIDDEN, pr.HIDDEN, pr.N_OUT_PAD]
+    fwd = sum(2 * 256 * dims[i] * dims[i + 1] for i in range(4))
+    bwd = fwd + sum(2 * 256 * dims[i] * dims[i + 1] for i in range(1, 4))
+    steps = info["epochs"] * (50_000 // 256)
     val = prop.validate(2048)
     rng = np.random.default_rng(77)
     w0 = np.array([120.0, 40.0, 40.0, 5000.0])
@@ -562,19 +571,16 @@ def learned_fits(dev: torch.device, n_cases: int = 4, tau: float = 1e-3) -> dict
         padded = torch.as_tensor(so.pad_or_crop_scan(counts.cpu().numpy()), device=dev)
         prep = tf.prepare(padded, voltage_kV=300, semiangle_mrad=20.0, scan_sampling=0.5,
                           det_sampling=20.0 / 12.0)
-        truth = tf.reconstruct(prep, so.Aberrations(*map(float, ab)))[1].cpu().numpy()
+        x_opt, _, _ = pr.surrogate_search(be, pr.to_x(ab[None]), w0 / 16, 8, 300,
+                                          np.random.default_rng(5), min_radius=1e-7)
+        ref = {"opt": tf.reconstruct(prep, so.Aberrations(*map(float, x_opt)))[1].cpu().numpy(),
+               "truth": tf.reconstruct(prep, so.Aberrations(*map(float, ab)))[1].cpu().numpy()}
         del padded, prep
 
-        def ok(est):
+        def within(est, target, tau):
             ph = be.object_and_phase(*map(float, est))[1].cpu().numpy()
-            e = so.wrapped_phase_error(ph, truth)
+            e = so.wrapped_phase_error(ph, ref[target])
             return float(np.sqrt(np.mean(e ** 2))) <= tau
-
-        plain = pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64, 30, 0.75,
-                               np.random.default_rng(1), done=ok)
-        hyp = prop.propose(be)
-        learned = pr.zoom_search(be, pr.to_x(hyp), w0, 8, 60, LEARNED_SHRINK, np.random.default_rng(2),
-                                 done=ok)
 
         def timed(fn):
             torch.cuda.synchronize(dev)
@@ -583,28 +589,43 @@ def learned_fits(dev: torch.device, n_cases: int = 4, tau: float = 1e-3) -> dict
             torch.cuda.synchronize(dev)
             return time.perf_counter() - t
 
-        t_plain = timed(lambda: pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64,
-                                               plain[2], 0.75, np.random.default_rng(1)))
-        t_learned = timed(lambda: pr.zoom_search(be, pr.to_x(prop.propose(be)), w0, 8, learned[2],
-                                                 LEARNED_SHRINK, np.random.default_rng(2)))
-        rows.append({"truth": [round(float(v), 1) for v in ab],
-                     "proposal": [round(float(v), 1) for v in hyp[0]],
-                     "plain_evals": plain[1], "learned_evals": learned[1],
-                     "plain_done": ok(plain[0]), "learned_done": ok(learned[0]),
-                     "plain_s": t_plain, "learned_s": t_learned})
+        row = {}
+        for key, target, tau in (("opt_1e-4", "opt", 1e-4), ("truth_1e-3", "truth", 1e-3)):
+            ok = lambda est: within(est, target, tau)  # noqa: E731
+            bp, pe, pr_rounds = pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64, 200, 0.75,
+                                               np.random.default_rng(1), done=ok)
+            hyp = prop.propose(be)
+            bl, le, lr_rounds = pr.learned_refine(be, pr.to_x(hyp), w0, 8, 120,
+                                                  np.random.default_rng(2), done=ok)
+            t_plain = timed(lambda: pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64,
+                                                   pr_rounds, 0.75, np.random.default_rng(1)))
+            t_learned = timed(lambda: pr.learned_refine(be, pr.to_x(prop.propose(be)), w0, 8,
+                                                        lr_rounds, np.random.default_rng(2)))
+            row[key] = {"plain": pe, "learned": le, "plain_done": ok(bp), "learned_done": ok(bl),
+                        "plain_s": t_plain, "learned_s": t_learned}
+        rows.append(row)
         del be, counts
-    pe = float(np.mean([r["plain_evals"] for r in rows]))
-    le = float(np.mean([r["learned_evals"] for r in rows]))
+
+    def summary(key):
+        rs = [r[key] for r in rows]
+        pe = float(np.mean([r["plain"] for r in rs]))
+        le = float(np.mean([r["learned"] for r in rs]))
+        return {"mean_evals_plain64": pe, "mean_evals_learned8": le, "evals_ratio": pe / le,
+                "plain_reached": sum(r["plain_done"] for r in rs),
+                "learned_reached": sum(r["learned_done"] for r in rs), "n_cases": len(rs),
+                "fits_per_s_plain64": len(rs) / sum(r["plain_s"] for r in rs),
+                "fits_per_s_learned8": len(rs) / sum(r["learned_s"] for r in rs),
+                "evals_per_case": [[r["plain"], r["learned"]] for r in rs]}
+
     return {
         "workload": "64^2 scan x 64^2 detector (padded to 128^2), 1e6 e/position, aberrations "
-                    "in the sweep ranges; done = phase within tau rad RMS of the FP64 oracle at truth",
-        "tau_rad": tau, "train_s": train_s, "train_samples": 50_000, "train_epochs": info["epochs"],
+                    "in the sweep ranges (C1, A1, C3)",
+        "train_s": train_s, "train_samples": 50_000, "train_epochs": info["epochs"],
+        "train_tflops": (fwd + bwd) * steps / train_s / 1e12,
         "val_rmse": {"C1_A": val["rmse_units"][0], "A1a_A": val["rmse_units"][1],
                      "A1b_A": val["rmse_units"][2], "C3_A": val["rmse_units"][3]},
-        "mean_evals_plain64": pe, "mean_evals_learned8": le, "evals_ratio": pe / le,
-        "fits_per_s_plain64": len(rows) / sum(r["plain_s"] for r in rows),
-        "fits_per_s_learned8": len(rows) / sum(r["learned_s"] for r in rows),
-        "cases": rows,
+        "tau_1e-4_vs_loss_optimum": summary("opt_1e-4"),
+        "tau_1e-3_vs_truth": summary("truth_1e-3"),
     }
 
 
@@ -981,8 +1002,11 @@ def _headline(line: dict) -> dict:
                              "truth_first": sw["truth_ranked_first"]}
     lf = line.get("learned_fits")
     if lf:
-        h["learned_fits"] = {k: lf[k] for k in ("tau_rad", "dose", "n_cases", "mean_evals_plain64",
-                                                "mean_evals_learned8", "evals_ratio") if k in lf}
+        h["learned_fits"] = {
+            k: {q: lf[k][q] for q in ("mean_evals_plain64", "mean_evals_learned8", "evals_ratio",
+                                      "plain_reached", "learned_reached", "n_cases")}
+            for k in ("tau_1e-4_vs_loss_optimum", "tau_1e-3_vs_truth") if k in lf}
+        h["learned_fits"]["train_tflops"] = lf.get("train_tflops")
     cb = line.get("cpu_baseline")
     if cb:
         h["cpu_baseline"] = {"recon_per_s": cb["value"], "cores": cb["cores"]}

@@ -277,6 +277,7 @@ class MLP:
         self.v = [torch.zeros_like(t) for t in self.w + self.b]
         self.t = 0
         self._bufs: dict = {}
+        self._tc_ws: torch.Tensor | None = None
 
     # buffers per batch size
     def _buf(self, m: int) -> dict:
@@ -298,8 +299,30 @@ class MLP:
             self._bufs[m] = b
         return b
 
+    # the large GEMMs (M, N multiples of 128, K of 64) run on the tcgen05
+    # kernel, split over K until about two CTAs per SM; the rest on the warp MMA
+    use_tc = True
+
+    @staticmethod
+    def _tc_splits(m: int, n: int, k: int) -> int:
+        tiles = (m // 128) * (n // 128)
+        splits = 1
+        while tiles * splits * 2 <= 296 and k % (64 * splits * 2) == 0 and k // (splits * 2) >= 256:
+            splits *= 2
+        return splits
+
     def _gemm(self, a, lda, ta, bmat, ldb, tb, m, n, k, bias=None, c=None, ldc=0, act=None,
               ld_act=0, accumulate=False):
+        if self.use_tc and m % 128 == 0 and n % 128 == 0 and k % 64 == 0:
+            splits = self._tc_splits(m, n, k)
+            need = ctypes.c_size_t(0)
+            _lib.check(_lib.load().qssb_gemm_tc_workspace_bytes(m, n, k, splits, ctypes.byref(need)))
+            if self._tc_ws is None or self._tc_ws.numel() < need.value:
+                self._tc_ws = torch.empty(need.value, dtype=torch.uint8, device=self.device)
+            _call("qssb_gemm_bf16_tc", self.device, _ptr(a), lda, int(ta), _ptr(bmat), ldb, int(tb),
+                  m, n, k, splits, _ptr(bias), int(accumulate), _ptr(c), ldc, _ptr(act), ld_act,
+                  _ptr(self._tc_ws), need.value, _stream(self.device))
+            return
         _call("qssb_gemm_bf16", self.device, _ptr(a), lda, int(ta), _ptr(bmat), ldb, int(tb), m, n,
               k, _ptr(bias), int(accumulate), _ptr(c), ldc, _ptr(act), ld_act, _stream(self.device))
 

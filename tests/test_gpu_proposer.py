@@ -148,3 +148,36 @@ def test_learned_proposal_needs_fewer_evaluations_than_plain_sweep():
         plain_total += pe
         learned_total += le
     assert learned_total * 2 <= plain_total, (learned_total, plain_total)
+
+
+def test_forward_model_features_match_simulated_scans():
+    """Held-out check of the training data: for four aberration draws the
+    network never saw, the forward model's maps at the lattice reflections
+    ((8, 0), (16, 0), (0, 8), (0, 16) in units of 1/32 A^-1, where a crystal's
+    signal lies) match the maps measured from fully simulated 64^2 x 64^2
+    scans at 1e6 e per position (the SSB forward model with Poisson counts):
+    cosine similarity of every reflection map >= 0.9, mean >= 0.95. (The
+    other twelve maps carry noise in both.)"""
+    from quantem.gpu_b200 import B200SSBBackend
+    from quantem.gpu_b200.synthetic import SyntheticSpec, generate
+
+    lat = pr.TrainingLattice(DEV)
+    rng = np.random.default_rng(2024)
+    cos_all = []
+    for i in range(4):
+        ab = draw_aberrations(rng, 1)
+        spec = SyntheticSpec(scan_shape=(64, 64), detector_shape=(64, 64),
+                             det_sampling_mrad=20.0 / 12.0, dose=1e6, C10=float(ab[0, 0]),
+                             C12=float(ab[0, 1]), phi12=float(ab[0, 2]), C30=float(ab[0, 3]),
+                             seed=500 + i)
+        be = B200SSBBackend(generate(spec, DEV).counts, semiangle=20.0, scan_sampling=0.5,
+                            det_sampling=20.0 / 12.0, voltage_kV=300, device=DEV)
+        got = pr.backend_features(be).float().view(16, -1).cpu().numpy()
+        want = lat.features(ab, np.random.default_rng(i), sigma=(1e-6, 1e-6)).float().view(16, -1)
+        want = want.cpu().numpy()
+        for q in (1, 3, 5, 7):
+            a, b = got[q], want[q]
+            cos_all.append(float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b))))
+        be.close()
+    assert min(cos_all) >= 0.9, cos_all
+    assert np.mean(cos_all) >= 0.95, cos_all
