@@ -526,15 +526,16 @@ def learned_fits(dev: torch.device, n_cases: int = 12) -> dict:
     lattice, 40 epochs) with the library's own kernels (its large GEMMs on the
     tcgen05 tensor cores). Each case is a fully simulated 64^2-scan x
     64^2-detector dataset (padded to 128^2 by the reference rule) with
-    aberrations drawn from the sweep ranges at 1e6 e per position. Two
-    targets, with SSB evaluations (candidates scored) counted until the
-    current best estimate meets them:
-      * 1e-4 rad RMS from the FP64-oracle phase at the loss optimum (the
-        phase a converged fit returns; its aberrations are found by a long
-        refinement from the truth first);
-      * 1e-3 rad RMS from the FP64-oracle phase at the true aberrations (the
-        loss optimum of a 0.3 rad object sits 2-6e-4 rad from it even without
-        noise, so 1e-4 from the truth is out of reach of any loss minimiser).
+    aberrations drawn from the sweep ranges at 1e6 e per position. SSB
+    evaluations (candidates scored) are counted until the current best
+    estimate's phase is within tau rad RMS of the FP64-oracle phase at the
+    true aberrations:
+      * tau = 1e-4 on weak-phase objects (0.03 rad atoms): their loss optimum
+        lies 3e-6 .. 9e-5 rad from that phase;
+      * tau = 1e-3 on the configs' 0.3 rad objects, whose loss optimum lies
+        2e-4 .. 6e-4 rad from it even without noise (the phase-variance
+        objective, not the search, sets that floor), so 1e-4 is out of reach
+        there for any minimiser of the loss.
     plain = a 64-candidate zoom sweep over the whole range (at most 200
     rounds); learned = the proposal's two sign hypotheses, then
     ``proposer.learned_refine`` (8 per round). Fits/s come from replaying the
@@ -560,27 +561,29 @@ def learned_fits(dev: torch.device, n_cases: int = 12) -> dict:
     rng = np.random.default_rng(77)
     w0 = np.array([120.0, 40.0, 40.0, 5000.0])
     rows = []
-    for i in range(n_cases):
+    cases = [(i, 0.03, "weak_1e-4", 1e-4) for i in range(n_cases)] + \
+            [(i, 0.3, "std_1e-3", 1e-3) for i in range(n_cases // 2)]
+    for i, peak, key, tau in cases:
         ab = draw_aberrations(rng, 1)[0]
         spec = SyntheticSpec(scan_shape=(64, 64), detector_shape=(64, 64),
                              det_sampling_mrad=20.0 / 12.0, dose=1e6, C10=float(ab[0]),
-                             C12=float(ab[1]), phi12=float(ab[2]), C30=float(ab[3]), seed=100 + i)
+                             C12=float(ab[1]), phi12=float(ab[2]), C30=float(ab[3]),
+                             atom_peak_rad=peak, seed=100 + i)
         counts = generate(spec, dev).counts
         be = B200SSBBackend(counts, semiangle=20.0, scan_sampling=0.5, det_sampling=20.0 / 12.0,
                             voltage_kV=300, device=dev)
         padded = torch.as_tensor(so.pad_or_crop_scan(counts.cpu().numpy()), device=dev)
         prep = tf.prepare(padded, voltage_kV=300, semiangle_mrad=20.0, scan_sampling=0.5,
                           det_sampling=20.0 / 12.0)
+        truth = tf.reconstruct(prep, so.Aberrations(*map(float, ab)))[1].cpu().numpy()
+        # the objective's own floor: the loss optimum, refined from the truth
         x_opt, _, _ = pr.surrogate_search(be, pr.to_x(ab[None]), w0 / 16, 8, 300,
                                           np.random.default_rng(5), min_radius=1e-7)
-        ref = {"opt": tf.reconstruct(prep, so.Aberrations(*map(float, x_opt)))[1].cpu().numpy(),
-               "truth": tf.reconstruct(prep, so.Aberrations(*map(float, ab)))[1].cpu().numpy()}
         del padded, prep
 
-        def within(est, target, tau):
+        def rms(est):
             ph = be.object_and_phase(*map(float, est))[1].cpu().numpy()
-            e = so.wrapped_phase_error(ph, ref[target])
-            return float(np.sqrt(np.mean(e ** 2))) <= tau
+            return float(np.sqrt(np.mean(so.wrapped_phase_error(ph, truth) ** 2)))
 
         def timed(fn):
             torch.cuda.synchronize(dev)
@@ -589,25 +592,23 @@ def learned_fits(dev: torch.device, n_cases: int = 12) -> dict:
             torch.cuda.synchronize(dev)
             return time.perf_counter() - t
 
-        row = {}
-        for key, target, tau in (("opt_1e-4", "opt", 1e-4), ("truth_1e-3", "truth", 1e-3)):
-            ok = lambda est: within(est, target, tau)  # noqa: E731
-            bp, pe, pr_rounds = pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64, 200, 0.75,
-                                               np.random.default_rng(1), done=ok)
-            hyp = prop.propose(be)
-            bl, le, lr_rounds = pr.learned_refine(be, pr.to_x(hyp), w0, 8, 120,
-                                                  np.random.default_rng(2), done=ok)
-            t_plain = timed(lambda: pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64,
-                                                   pr_rounds, 0.75, np.random.default_rng(1)))
-            t_learned = timed(lambda: pr.learned_refine(be, pr.to_x(prop.propose(be)), w0, 8,
-                                                        lr_rounds, np.random.default_rng(2)))
-            row[key] = {"plain": pe, "learned": le, "plain_done": ok(bp), "learned_done": ok(bl),
-                        "plain_s": t_plain, "learned_s": t_learned}
-        rows.append(row)
+        ok = lambda est: rms(est) <= tau  # noqa: E731
+        bp, pe, pr_rounds = pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64, 200, 0.75,
+                                           np.random.default_rng(1), done=ok)
+        hyp = prop.propose(be)
+        bl, le, lr_rounds = pr.learned_refine(be, pr.to_x(hyp), w0, 8, 120,
+                                              np.random.default_rng(2), done=ok)
+        t_plain = timed(lambda: pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64,
+                                               pr_rounds, 0.75, np.random.default_rng(1)))
+        t_learned = timed(lambda: pr.learned_refine(be, pr.to_x(prop.propose(be)), w0, 8,
+                                                    lr_rounds, np.random.default_rng(2)))
+        rows.append({"key": key, "plain": pe, "learned": le, "plain_done": ok(bp),
+                     "learned_done": ok(bl), "plain_s": t_plain, "learned_s": t_learned,
+                     "loss_optimum_rms_rad": rms(x_opt)})
         del be, counts
 
     def summary(key):
-        rs = [r[key] for r in rows]
+        rs = [r for r in rows if r["key"] == key]
         pe = float(np.mean([r["plain"] for r in rs]))
         le = float(np.mean([r["learned"] for r in rs]))
         return {"mean_evals_plain64": pe, "mean_evals_learned8": le, "evals_ratio": pe / le,
@@ -615,17 +616,18 @@ def learned_fits(dev: torch.device, n_cases: int = 12) -> dict:
                 "learned_reached": sum(r["learned_done"] for r in rs), "n_cases": len(rs),
                 "fits_per_s_plain64": len(rs) / sum(r["plain_s"] for r in rs),
                 "fits_per_s_learned8": len(rs) / sum(r["learned_s"] for r in rs),
+                "loss_optimum_rms_rad_max": max(r["loss_optimum_rms_rad"] for r in rs),
                 "evals_per_case": [[r["plain"], r["learned"]] for r in rs]}
 
     return {
         "workload": "64^2 scan x 64^2 detector (padded to 128^2), 1e6 e/position, aberrations "
-                    "in the sweep ranges (C1, A1, C3)",
+                    "in the sweep ranges (C1, A1, C3); weak-phase (0.03 rad) and 0.3 rad atoms",
         "train_s": train_s, "train_samples": 50_000, "train_epochs": info["epochs"],
         "train_tflops": (fwd + bwd) * steps / train_s / 1e12,
         "val_rmse": {"C1_A": val["rmse_units"][0], "A1a_A": val["rmse_units"][1],
                      "A1b_A": val["rmse_units"][2], "C3_A": val["rmse_units"][3]},
-        "tau_1e-4_vs_loss_optimum": summary("opt_1e-4"),
-        "tau_1e-3_vs_truth": summary("truth_1e-3"),
+        "tau_1e-4_weak_phase": summary("weak_1e-4"),
+        "tau_1e-3_0.3rad": summary("std_1e-3"),
     }
 
 
@@ -1005,7 +1007,7 @@ def _headline(line: dict) -> dict:
         h["learned_fits"] = {
             k: {q: lf[k][q] for q in ("mean_evals_plain64", "mean_evals_learned8", "evals_ratio",
                                       "plain_reached", "learned_reached", "n_cases")}
-            for k in ("tau_1e-4_vs_loss_optimum", "tau_1e-3_vs_truth") if k in lf}
+            for k in ("tau_1e-4_weak_phase", "tau_1e-3_0.3rad") if k in lf}
         h["learned_fits"]["train_tflops"] = lf.get("train_tflops")
     cb = line.get("cpu_baseline")
     if cb:

@@ -111,9 +111,12 @@ def test_short_training_cuts_validation_error():
 
 
 def test_learned_proposal_needs_fewer_evaluations_than_plain_sweep():
-    """What the trained network gains: proposal + 8-candidate refinement reaches
-    a phase within 1e-3 rad RMS of the FP64 oracle (at the true aberrations)
-    with fewer SSB evaluations than the plain 64-candidate sweep."""
+    """What the trained network gains: on weak-phase datasets (0.03 rad atoms,
+    64^2 scans, 1e6 e per position) the proposal plus the 8-candidate
+    refinement reaches a phase within 1e-4 rad RMS of the FP64 oracle at the
+    true aberrations with at least 6x fewer SSB evaluations, in total over
+    three cases, than the plain 64-candidate zoom sweep over the whole range
+    (measured on a B200: about 8x); every learned fit reaches the target."""
     from oracle import ssb_torch_fp64 as tf
     from quantem.gpu_b200 import B200SSBBackend
     from quantem.gpu_b200.synthetic import SyntheticSpec, generate
@@ -122,11 +125,13 @@ def test_learned_proposal_needs_fewer_evaluations_than_plain_sweep():
     prop.train(n_samples=50_000, epochs=40)
     rng = np.random.default_rng(77)
     plain_total = learned_total = 0
-    for i in range(2):
+    w0 = np.array([120.0, 40.0, 40.0, 5000.0])
+    for i in range(3):
         ab = draw_aberrations(rng, 1)[0]
         spec = SyntheticSpec(scan_shape=(64, 64), detector_shape=(64, 64),
                              det_sampling_mrad=20.0 / 12.0, dose=1e6, C10=float(ab[0]),
-                             C12=float(ab[1]), phi12=float(ab[2]), C30=float(ab[3]), seed=100 + i)
+                             C12=float(ab[1]), phi12=float(ab[2]), C30=float(ab[3]),
+                             atom_peak_rad=0.03, seed=100 + i)
         counts = generate(spec, DEV).counts
         be = B200SSBBackend(counts, semiangle=20.0, scan_sampling=0.5, det_sampling=20.0 / 12.0,
                             voltage_kV=300, device=DEV)
@@ -137,17 +142,16 @@ def test_learned_proposal_needs_fewer_evaluations_than_plain_sweep():
 
         def ok(est):
             ph = be.object_and_phase(*map(float, est))[1].cpu().numpy()
-            return float(np.sqrt(np.mean(so.wrapped_phase_error(ph, truth) ** 2))) <= 1e-3
+            return float(np.sqrt(np.mean(so.wrapped_phase_error(ph, truth) ** 2))) <= 1e-4
 
-        _, pe, _ = pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64, 30, 0.75,
+        _, pe, _ = pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64, 200, 0.75,
                                   np.random.default_rng(1), done=ok)
-        best, le, _ = pr.zoom_search(be, pr.to_x(prop.propose(be)),
-                                     np.array([120.0, 40.0, 40.0, 5000.0]), 8, 60, 0.9,
-                                     np.random.default_rng(2), done=ok)
-        assert ok(best)
+        best, le, _ = pr.learned_refine(be, pr.to_x(prop.propose(be)), w0, 8, 120,
+                                        np.random.default_rng(2), done=ok)
+        assert ok(best), i
         plain_total += pe
         learned_total += le
-    assert learned_total * 2 <= plain_total, (learned_total, plain_total)
+    assert learned_total * 6 <= plain_total, (learned_total, plain_total)
 
 
 def test_forward_model_features_match_simulated_scans():
