@@ -519,27 +519,34 @@ def sweep_3scans(dev: torch.device, steps: int) -> dict:
     }
 
 
-def learned_fits(dev: torch.device, n_cases: int = 12) -> dict:
+def learned_fits(dev: torch.device, n_cases: int = 16) -> dict:
     """Learned proposal + 8-candidate refinement vs the plain 64-candidate sweep.
 
     The proposer is trained here (50k forward-model samples of the 64^2 x 64^2
     lattice, 40 epochs) with the library's own kernels (its large GEMMs on the
     tcgen05 tensor cores). Each case is a fully simulated 64^2-scan x
     64^2-detector dataset (padded to 128^2 by the reference rule) with
-    aberrations drawn from the sweep ranges at 1e6 e per position. SSB
-    evaluations (candidates scored) are counted until the current best
-    estimate's phase is within tau rad RMS of the FP64-oracle phase at the
-    true aberrations:
-      * tau = 1e-4 on weak-phase objects (0.03 rad atoms): their loss optimum
-        lies 3e-6 .. 9e-5 rad from that phase;
-      * tau = 1e-3 on the configs' 0.3 rad objects, whose loss optimum lies
-        2e-4 .. 6e-4 rad from it even without noise (the phase-variance
-        objective, not the search, sets that floor), so 1e-4 is out of reach
-        there for any minimiser of the loss.
+    aberrations drawn from the sweep ranges at 1e6 e per position:
+    ``n_cases`` weak-phase objects (0.03 rad atoms) and ``n_cases // 2`` of
+    the configs' 0.3 rad objects. SSB evaluations (candidates scored) are
+    counted until the current best estimate's phase is within tau rad RMS
+    (1e-4 on the weak-phase objects, 1e-3 on the 0.3 rad ones, whose phase
+    moves ten times as much per A of aberration, finer than the float32
+    loss resolves at 1e-4) of an FP64-oracle phase:
+      * ``..._vs_loss_optimum_...``: the FP64 phase at the loss optimum (the
+        minimiser's goal, refined from the truth), which both searches
+        converge to, so this measures the search alone;
+      * ``..._vs_truth_...``: the FP64 phase at the true aberrations. The loss
+        optimum lies 1e-5 .. 1.6e-4 rad from it on the weak-phase objects and
+        1e-4 .. 1.6e-3 rad on the 0.3 rad ones (the phase-variance objective,
+        not the search, sets that floor; listed per case); a case whose floor
+        exceeds tau is reached only by passing through on the way, so it is
+        counted, not compared.
     plain = a 64-candidate zoom sweep over the whole range (at most 200
-    rounds); learned = the proposal's two sign hypotheses, then
-    ``proposer.learned_refine`` (8 per round). Fits/s come from replaying the
-    same searches without the checks."""
+    rounds); learned = the proposal's eight hypotheses (four heads, two
+    signs), then ``proposer.learned_refine`` (8 per round; the plain sweep as
+    its fallback, evaluations added). Fits/s time the same searches with the
+    oracle checks' own time taken out."""
     from oracle import ssb_oracle as so
     from oracle import ssb_torch_fp64 as tf
     from quantem.gpu_b200 import B200SSBBackend
@@ -561,9 +568,9 @@ def learned_fits(dev: torch.device, n_cases: int = 12) -> dict:
     rng = np.random.default_rng(77)
     w0 = np.array([120.0, 40.0, 40.0, 5000.0])
     rows = []
-    cases = [(i, 0.03, "weak_1e-4", 1e-4) for i in range(n_cases)] + \
-            [(i, 0.3, "std_1e-3", 1e-3) for i in range(n_cases // 2)]
-    for i, peak, key, tau in cases:
+    cases = [(i, 0.03, "weak") for i in range(n_cases)] + \
+            [(i, 0.3, "0.3rad") for i in range(n_cases // 2)]
+    for i, peak, obj in cases:
         ab = draw_aberrations(rng, 1)[0]
         spec = SyntheticSpec(scan_shape=(64, 64), detector_shape=(64, 64),
                              det_sampling_mrad=20.0 / 12.0, dose=1e6, C10=float(ab[0]),
@@ -576,58 +583,82 @@ def learned_fits(dev: torch.device, n_cases: int = 12) -> dict:
         prep = tf.prepare(padded, voltage_kV=300, semiangle_mrad=20.0, scan_sampling=0.5,
                           det_sampling=20.0 / 12.0)
         truth = tf.reconstruct(prep, so.Aberrations(*map(float, ab)))[1].cpu().numpy()
-        # the objective's own floor: the loss optimum, refined from the truth
+        # the objective's own optimum, refined from the truth, and its FP64 phase
         x_opt, _, _ = pr.surrogate_search(be, pr.to_x(ab[None]), w0 / 16, 8, 300,
                                           np.random.default_rng(5), min_radius=1e-7)
+        at_opt = tf.reconstruct(prep, so.Aberrations(*map(float, x_opt)))[1].cpu().numpy()
         del padded, prep
+        check_s = [0.0]
 
-        def rms(est):
+        def rms(est, ref):
             ph = be.object_and_phase(*map(float, est))[1].cpu().numpy()
-            return float(np.sqrt(np.mean(so.wrapped_phase_error(ph, truth) ** 2)))
+            return float(np.sqrt(np.mean(so.wrapped_phase_error(ph, ref) ** 2)))
 
         def timed(fn):
+            check_s[0] = 0.0
             torch.cuda.synchronize(dev)
             t = time.perf_counter()
-            fn()
+            out = fn()
             torch.cuda.synchronize(dev)
-            return time.perf_counter() - t
+            return out, time.perf_counter() - t - check_s[0]
 
-        ok = lambda est: rms(est) <= tau  # noqa: E731
-        bp, pe, pr_rounds = pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64, 200, 0.75,
-                                           np.random.default_rng(1), done=ok)
-        hyp = prop.propose(be)
-        bl, le, lr_rounds = pr.learned_refine(be, pr.to_x(hyp), w0, 8, 120,
-                                              np.random.default_rng(2), done=ok)
-        t_plain = timed(lambda: pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64,
-                                               pr_rounds, 0.75, np.random.default_rng(1)))
-        t_learned = timed(lambda: pr.learned_refine(be, pr.to_x(prop.propose(be)), w0, 8,
-                                                    lr_rounds, np.random.default_rng(2)))
-        rows.append({"key": key, "plain": pe, "learned": le, "plain_done": ok(bp),
-                     "learned_done": ok(bl), "plain_s": t_plain, "learned_s": t_learned,
-                     "loss_optimum_rms_rad": rms(x_opt)})
+        floor = rms(x_opt, truth)
+        tau_obj = 1e-4 if obj == "weak" else 1e-3
+        for crit, ref in (("opt", at_opt), ("truth", truth)):
+            def ok(est, ref=ref):
+                torch.cuda.synchronize(dev)
+                t = time.perf_counter()
+                r = rms(est, ref) <= tau_obj
+                check_s[0] += time.perf_counter() - t
+                return r
+
+            (bp, pe, _), t_plain = timed(lambda: pr.zoom_search(
+                be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64, 200, 0.75, np.random.default_rng(1),
+                done=ok))
+            (bl, le, _, fell), t_learned = timed(lambda: pr.learned_refine(
+                be, pr.to_x(prop.propose(be)), rng=np.random.default_rng(2), done=ok))
+            rows.append({"crit": crit, "obj": obj, "tau": tau_obj, "plain": pe, "learned": le,
+                         "plain_done": ok(bp), "learned_done": ok(bl), "fell_back": fell,
+                         "plain_s": t_plain, "learned_s": t_learned,
+                         "floor": floor if crit == "truth" else 0.0})
         del be, counts
 
-    def summary(key):
-        rs = [r for r in rows if r["key"] == key]
-        pe = float(np.mean([r["plain"] for r in rs]))
-        le = float(np.mean([r["learned"] for r in rs]))
+    def summary(crit, obj):
+        """Means, the ratio and fits/s over the cases whose loss optimum lies
+        within tau of the reference phase (a converging minimiser cannot stay
+        inside the target otherwise; those are counted, not compared) and that
+        both searches reached (one that ran out of rounds has no count to
+        compare); every case is listed as (plain, learned, plain reached,
+        learned reached, floor)."""
+        rs = [r for r in rows if r["crit"] == crit and r["obj"] == obj]
+        ok_floor = [r for r in rs if r["floor"] <= r["tau"]]
+        both = [r for r in ok_floor if r["plain_done"] and r["learned_done"]] or ok_floor or rs
+        pe = float(np.mean([r["plain"] for r in both]))
+        le = float(np.mean([r["learned"] for r in both]))
         return {"mean_evals_plain64": pe, "mean_evals_learned8": le, "evals_ratio": pe / le,
+                "ratio_over": "cases with floor <= tau that both reached",
+                "both_reached": len(both), "n_cases": len(rs),
+                "floor_above_tau": len(rs) - len(ok_floor),
                 "plain_reached": sum(r["plain_done"] for r in rs),
-                "learned_reached": sum(r["learned_done"] for r in rs), "n_cases": len(rs),
-                "fits_per_s_plain64": len(rs) / sum(r["plain_s"] for r in rs),
-                "fits_per_s_learned8": len(rs) / sum(r["learned_s"] for r in rs),
-                "loss_optimum_rms_rad_max": max(r["loss_optimum_rms_rad"] for r in rs),
-                "evals_per_case": [[r["plain"], r["learned"]] for r in rs]}
+                "learned_reached": sum(r["learned_done"] for r in rs),
+                "learned_fell_back": sum(r["fell_back"] for r in rs),
+                "fits_per_s_plain64": len(both) / sum(r["plain_s"] for r in both),
+                "fits_per_s_learned8": len(both) / sum(r["learned_s"] for r in both),
+                "cases": [[r["plain"], r["learned"], int(r["plain_done"]), int(r["learned_done"]),
+                           float("%.3g" % r["floor"])] for r in rs]}
 
     return {
         "workload": "64^2 scan x 64^2 detector (padded to 128^2), 1e6 e/position, aberrations "
                     "in the sweep ranges (C1, A1, C3); weak-phase (0.03 rad) and 0.3 rad atoms",
         "train_s": train_s, "train_samples": 50_000, "train_epochs": info["epochs"],
         "train_tflops": (fwd + bwd) * steps / train_s / 1e12,
-        "val_rmse": {"C1_A": val["rmse_units"][0], "A1a_A": val["rmse_units"][1],
-                     "A1b_A": val["rmse_units"][2], "C3_A": val["rmse_units"][3]},
-        "tau_1e-4_weak_phase": summary("weak_1e-4"),
-        "tau_1e-3_0.3rad": summary("std_1e-3"),
+        "val_best_head_A": {"rmse": [round(v, 1) for v in val["rmse_units"]],
+                            "median_abs": [round(v, 1) for v in val["median_abs_units"]],
+                            "order": "C1, A1a, A1b, C3"},
+        "tau_1e-4_vs_loss_optimum_weak_phase": summary("opt", "weak"),
+        "tau_1e-4_vs_truth_weak_phase": summary("truth", "weak"),
+        "tau_1e-3_vs_loss_optimum_0.3rad": summary("opt", "0.3rad"),
+        "tau_1e-3_vs_truth_0.3rad": summary("truth", "0.3rad"),
     }
 
 
@@ -1004,10 +1035,13 @@ def _headline(line: dict) -> dict:
                              "truth_first": sw["truth_ranked_first"]}
     lf = line.get("learned_fits")
     if lf:
+        keys = ("tau_1e-4_vs_loss_optimum_weak_phase", "tau_1e-4_vs_truth_weak_phase",
+                "tau_1e-3_vs_loss_optimum_0.3rad", "tau_1e-3_vs_truth_0.3rad")
         h["learned_fits"] = {
             k: {q: lf[k][q] for q in ("mean_evals_plain64", "mean_evals_learned8", "evals_ratio",
-                                      "plain_reached", "learned_reached", "n_cases")}
-            for k in ("tau_1e-4_weak_phase", "tau_1e-3_0.3rad") if k in lf}
+                                      "both_reached", "floor_above_tau", "learned_fell_back",
+                                      "n_cases")}
+            for k in keys if k in lf}
         h["learned_fits"]["train_tflops"] = lf.get("train_tflops")
     cb = line.get("cpu_baseline")
     if cb:

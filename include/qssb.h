@@ -499,6 +499,18 @@ int qssb_bias_grad(const float* dz, int32_t rows, int32_t cols, float* db, void*
  * (zero in columns n_out..ld-1); loss (device float) may be NULL. */
 int qssb_mse(const float* y, const float* target, int32_t rows, int32_t n_out, int32_t ld,
              float* dy, float* loss, void* stream);
+/* Multi-head (winner-takes-all) MSE: row r of y (ld columns) holds `heads`
+ * groups of n_out outputs against target[r][0..n_out). Per row the winner is
+ * the head with the least squared error over its first n_select outputs
+ * (ties: lowest index; written to winner[r] when winner is not NULL); loss =
+ * mean over rows of sum_c w_c (y_win,c - t_c)^2 / n_out, w = out_weight
+ * (n_out floats, NULL = all 1); dy_h,c = 2 s_h w_c (y_h,c - t_c) / (rows
+ * n_out) with s = 1 - eps for the winner and eps / (heads - 1) for the others
+ * (1 with one head), zero in the padding columns. heads * n_out <= ld,
+ * 1 <= n_select <= n_out, 0 <= eps < 1. */
+int qssb_mse_heads(const float* y, const float* target, int32_t rows, int32_t n_out,
+                   int32_t heads, int32_t ld, const float* out_weight, int32_t n_select,
+                   float eps, float* dy, float* loss, int32_t* winner, void* stream);
 /* Adam (bias-corrected, decoupled weight decay) on FP32 master weights; the
  * BF16 copy w_bf16 (may be NULL) is refreshed. step counts from 1. */
 int qssb_adam(float* w, float* m, float* v, const float* grad, int64_t n, float lr, float beta1,

@@ -144,6 +144,8 @@ SIGNATURES = {
     "qssb_gelu_backward": (ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
     "qssb_bias_grad": (ctypes.c_int, [_P, _I32, _I32, _P, _P]),
     "qssb_mse": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _P, _P, _P]),
+    "qssb_mse_heads": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _I32, _P, _I32, ctypes.c_float,
+                                      _P, _P, _P, _P]),
     "qssb_adam": (ctypes.c_int, [_P, _P, _P, _P, _I64, ctypes.c_float, ctypes.c_float,
                                  ctypes.c_float, ctypes.c_float, ctypes.c_float, _I32, _P, _P]),
     "qssb_to_bf16": (ctypes.c_int, [_P, _I64, _P, _P]),

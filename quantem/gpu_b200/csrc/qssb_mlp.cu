@@ -156,6 +156,59 @@ __global__ void __launch_bounds__(256) k_mse(const float* __restrict__ y, const 
     if (threadIdx.x == 0 && loss) *loss = (float)(red[0] * scale);
 }
 
+// Multi-head (winner-takes-all) MSE. Row r of y holds `heads` groups of n_out
+// outputs (columns h n_out .. h n_out + n_out - 1, padding up to ld). The
+// winning head of a row is the one with the least squared error over its
+// first n_select outputs (ties: the lowest index); the loss is the mean over
+// rows of sum_c w_c (y_win,c - t_c)^2 / n_out and the gradient of head h is
+// dy_h,c = 2 s_h w_c (y_h,c - t_c) / (rows n_out), with s = 1 - eps for the
+// winner and eps / (heads - 1) for the others (s = 1 with one head). One
+// thread per row; the loss sums in FP64 in a fixed order.
+__global__ void __launch_bounds__(256) k_mse_heads(
+    const float* __restrict__ y, const float* __restrict__ t, int rows, int n_out, int heads,
+    int ld, const float* __restrict__ w_out, int n_select, float eps, float* __restrict__ dy,
+    float* __restrict__ loss, int* __restrict__ winner) {
+    __shared__ double red[256];
+    const double scale = 1.0 / ((double)rows * n_out);
+    double acc = 0.0;
+    for (int r = threadIdx.x; r < rows; r += 256) {
+        const float* yr = y + (size_t)r * ld;
+        const float* tr = t + (size_t)r * n_out;
+        int win = 0;
+        float best = 0.0f;
+        for (int h = 0; h < heads; ++h) {
+            float e = 0.0f;
+            for (int c = 0; c < n_select; ++c) {
+                const float d = yr[h * n_out + c] - tr[c];
+                e = fmaf(d, d, e);
+            }
+            if (h == 0 || e < best) {
+                best = e;
+                win = h;
+            }
+        }
+        if (winner) winner[r] = win;
+        float* dr = dy + (size_t)r * ld;
+        for (int c = heads * n_out; c < ld; ++c) dr[c] = 0.0f;
+        for (int h = 0; h < heads; ++h) {
+            const float s = heads == 1 ? 1.0f : (h == win ? 1.0f - eps : eps / (float)(heads - 1));
+            for (int c = 0; c < n_out; ++c) {
+                const float wc = w_out ? w_out[c] : 1.0f;
+                const float d = yr[h * n_out + c] - tr[c];
+                if (h == win) acc += (double)wc * d * d;
+                dr[h * n_out + c] = (float)(2.0 * scale) * s * wc * d;
+            }
+        }
+    }
+    red[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = 128; w > 0; w >>= 1) {
+        if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && loss) *loss = (float)(red[0] * scale);
+}
+
 // Adam on FP32 master weights (bias-corrected), then the BF16 copy.
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
                        const float* __restrict__ g, long long n, float lr, float b1, float b2,
@@ -246,6 +299,22 @@ extern "C" int qssb_mse(const float* y, const float* target, int32_t rows, int32
     if (!y || !target || !dy || rows <= 0 || n_out <= 0 || ld < n_out)
         return set_error(QSSB_ERR_INVALID, "qssb_mse: null pointer or bad shape");
     k_mse<<<1, 256, 0, (cudaStream_t)stream>>>(y, target, rows, n_out, ld, dy, loss);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+extern "C" int qssb_mse_heads(const float* y, const float* target, int32_t rows, int32_t n_out,
+                              int32_t heads, int32_t ld, const float* out_weight,
+                              int32_t n_select, float eps, float* dy, float* loss,
+                              int32_t* winner, void* stream) {
+    if (!y || !target || !dy || rows <= 0 || n_out <= 0 || heads <= 0 ||
+        (int64_t)heads * n_out > ld || n_select <= 0 || n_select > n_out)
+        return set_error(QSSB_ERR_INVALID, "qssb_mse_heads: null pointer or bad shape");
+    if (!(eps >= 0.0f && eps < 1.0f))
+        return set_error(QSSB_ERR_INVALID, "qssb_mse_heads: eps must be in [0, 1)");
+    k_mse_heads<<<1, 256, 0, (cudaStream_t)stream>>>(y, target, rows, n_out, heads, ld,
+                                                      out_weight, n_select, eps, dy, loss,
+                                                      winner);
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

@@ -6,24 +6,32 @@ No counterpart in the reference, whose fits search the whole prior box
 (Optuna TPE + Nelder-Mead, backend.py:958-1374). The pieces:
 
 * Features (``qssb_trotter_features`` / ``qssb_synth_features``): |G_b(Q)|
-  at 16 fixed scan frequencies Q = (m, n) / 32 A^-1 (on the fftfreq grid of
-  every scan whose extent N d is a multiple of 32 A), resampled onto a 32x32
-  grid over the aperture disk with a tent of the training detector's pitch
-  and normalised per Q: 16384 inputs, independent of dose and object contrast.
+  at 16 fixed scan frequencies Q = (m, n) / 32 A^-1 on the reciprocal
+  lattice of the synthetic 4 A square crystal (multiples of 1/4 A^-1 along
+  eight directions, where its signal lies; on the fftfreq grid of every scan
+  whose extent N d is a multiple of 32 A), resampled onto a 32x32 grid over
+  the aperture disk with a tent of the training detector's pitch and
+  normalised per Q: 16384 inputs, independent of dose and object contrast.
 * Training data: the SSB forward model of a weak-phase object,
   G_b(Q) = Gamma(Q, k_b) Phi(Q) + noise, on a 64x64-scan x 64x64-detector
   lattice (300 kV, 20 mrad, 20/12 mrad per pixel), aberrations uniform in the
   sweep ranges (C1 +-50 nm, |A1| <= 10 nm, C3 <= 1 um), random Phi and noise;
-  each sample leaves a random subset of its 16 maps noise-dominated, as a
-  crystal does between its reflections.
-* Network: 16384 -> 512 -> 512 -> 512 -> 4, GELU, BF16 weights and
-  activations on the tensor cores with FP32 accumulation, FP32 master weights
-  and Adam (``qssb_gemm_bf16``, ``qssb_gelu_backward``, ``qssb_bias_grad``,
-  ``qssb_mse``, ``qssb_adam``). Outputs (C1, |A1| cos 2phi, |A1| sin 2phi, C3)
-  scaled to O(1).
+  each sample leaves a random 0 .. 8 of its 16 maps noise-dominated.
+* Network: 16384 -> 512 -> 512 -> 512 -> 4 heads x 4, GELU, BF16 weights
+  and activations on the tensor cores with FP32 accumulation, FP32 master
+  weights and Adam (``qssb_gemm_bf16_tc`` / ``qssb_gemm_bf16``,
+  ``qssb_gelu_backward``, ``qssb_bias_grad``, ``qssb_mse_heads``,
+  ``qssb_adam``). Each head outputs (C1, |A1| cos 2phi, |A1| sin 2phi, C3),
+  C1 and A1 on one scale (an error of 1 A costs the same in either). The
+  heads train winner-takes-all on (C1, A1): the amplitudes fix
+  c(phi) = C1 + |A1| cos 2(phi - phi_A1) per direction only up to
+  |sin(pi lambda |Q|^2 c)|, whose aliases differ by 16/lambda (812 A at
+  300 kV) on this lattice, so one input can have several answers and each
+  head learns one.
 * Sign: trotter amplitudes are unchanged when every aberration flips sign
   (Gamma -> conj Gamma), so targets are canonical (C1 >= 0) and a proposal
-  is two hypotheses, p and -p; the refinement tests both.
+  is eight hypotheses (four heads, each sign), scored together as the
+  refinement's first 8-candidate batch.
 """
 from __future__ import annotations
 
@@ -40,8 +48,8 @@ from .calibration import bf_geometry
 from .physics import electron_wavelength_angstrom
 from .synthetic import SWEEP_RANGES
 
-Q_UNITS = np.array([(4, 0), (8, 0), (12, 0), (16, 0), (0, 4), (0, 8), (0, 12), (0, 16),
-                    (3, 3), (6, 6), (9, 9), (12, 12), (3, -3), (6, -6), (9, -9), (12, -12)],
+Q_UNITS = np.array([(8, 0), (16, 0), (24, 0), (0, 8), (0, 16), (0, 24), (8, 8), (16, 16),
+                    (8, -8), (16, -16), (16, 8), (8, 16), (16, -8), (8, -16), (24, 8), (8, 24)],
                    dtype=np.int32)
 Q_PERIOD_A = 32.0          # Q = units / 32 A^-1
 GRID = 32
@@ -51,8 +59,11 @@ CELL_RADIUS_FACTOR = 0.9   # cells beyond 0.9 alpha/lambda stay empty: the BF se
 N_IN = len(Q_UNITS) * GRID * GRID
 HIDDEN = 512
 N_OUT = 4
-N_OUT_PAD = 16
-OUT_SCALE = np.array([500.0, 100.0, 100.0, 1.0e4], dtype=np.float32)
+HEADS = 4
+N_OUT_PAD = 16             # HEADS x N_OUT
+OUT_SCALE = np.array([200.0, 200.0, 200.0, 1.0e4], dtype=np.float32)
+OUT_WEIGHT = np.array([1.0, 1.0, 1.0, 0.1], dtype=np.float32)  # C3 is barely visible
+WTA_EPS = 0.05             # share of the gradient the losing heads keep
 
 # the training lattice (64x64 detector)
 TRAIN_VOLTAGE_KV = 300.0
@@ -192,8 +203,14 @@ class TrainingLattice:
 
     def features(self, aberrations: np.ndarray, rng: np.random.Generator,
                  sigma: tuple[float, float] = (0.02, 1.0), seed: int = 0,
-                 chunk: int = 4096) -> torch.Tensor:
-        """BF16 features [n, N_IN] of the forward model at ``aberrations`` [n, 4]."""
+                 chunk: int = 4096, informative: tuple[int, int] | None = None,
+                 amplitude_contrast: tuple[float, float] = (0.0, 0.5)) -> torch.Tensor:
+        """BF16 features [n, N_IN] of the forward model at ``aberrations`` [n, 4].
+        Each sample keeps between ``informative`` = (lo, hi) of its maps at a
+        noise level drawn log-uniformly in ``sigma`` (default half .. all of
+        them: the crystal's reflections all carry signal, some weakly) and
+        drowns the rest; its amplitude part is a fraction of the phase part
+        drawn uniformly in ``amplitude_contrast``, with a random phase."""
         n = int(aberrations.shape[0])
         nq = len(Q_UNITS)
         out = torch.empty((n, N_IN), dtype=torch.bfloat16, device=self.device)
@@ -204,16 +221,16 @@ class TrainingLattice:
             ab = torch.as_tensor(np.ascontiguousarray(aberrations[s:e], np.float32), device=self.device)
             amp = np.exp(rng.uniform(np.log(0.2), np.log(5.0), size=(m, nq)))
             ph = rng.uniform(0, 2 * np.pi, size=(m, nq))
-            # amplitude contrast: 0 .. 0.5 of the phase part, random phase
-            amp_a = amp * rng.uniform(0.0, 0.5, size=(m, nq))
+            amp_a = amp * rng.uniform(*amplitude_contrast, size=(m, nq))
             ph_a = rng.uniform(0, 2 * np.pi, size=(m, nq))
             phi = np.stack([np.stack([amp * np.cos(ph), amp * np.sin(ph)], axis=-1),
                             np.stack([amp_a * np.cos(ph_a), amp_a * np.sin(ph_a)], axis=-1)],
                            axis=2).astype(np.float32)     # [m, nq, 2, 2]
-            # one noise level per map: a crystal puts its signal into a few
-            # frequencies (reflections) and leaves the others noise-dominated,
-            # so each sample has 2..16 informative maps, the rest drowned
-            n_good = rng.integers(2, nq + 1, size=m)
+            # one noise level per map: a crystal's reflections differ in
+            # strength, so each sample keeps a random number of informative
+            # maps and drowns the rest
+            lo_n, hi_n = (nq // 2, nq) if informative is None else informative
+            n_good = rng.integers(lo_n, hi_n + 1, size=m)
             good = rng.random((m, nq)).argsort(axis=1) < n_good[:, None]
             lo = rng.uniform(np.log(sigma[0]), np.log(sigma[1]), size=(m, nq))
             hi = rng.uniform(np.log(2.0), np.log(50.0), size=(m, nq))
@@ -255,7 +272,7 @@ def flipped(ab: np.ndarray) -> np.ndarray:
 
 # -------------------------------------------------------------------- MLP
 class MLP:
-    """16384 -> 512 -> 512 -> 512 -> 4 (padded to 16), GELU, BF16 weights on the
+    """16384 -> 512 -> 512 -> 512 -> HEADS x 4, GELU, BF16 weights on the
     tensor cores, FP32 master weights and Adam; every step in the C ABI."""
 
     def __init__(self, device, seed: int = 0):
@@ -266,11 +283,14 @@ class MLP:
         for i in range(4):
             fan_in = dims[i]
             w = torch.randn((dims[i], dims[i + 1]), generator=g, device=self.device) * math.sqrt(2.0 / fan_in)
+            b = torch.zeros(dims[i + 1], device=self.device)
             if i == 3:
-                w[:, N_OUT:] = 0.0
+                # small output weights; the heads start from spread biases so
+                # that they split the winners from the first steps
                 w *= 0.1
+                b = torch.linspace(-0.5, 0.5, dims[i + 1], device=self.device)
             self.w.append(w.contiguous())
-            self.b.append(torch.zeros(dims[i + 1], device=self.device))
+            self.b.append(b)
         self.dims = dims
         self.w_bf = [w.to(torch.bfloat16).contiguous() for w in self.w]
         self.m = [torch.zeros_like(t) for t in self.w + self.b]
@@ -278,6 +298,7 @@ class MLP:
         self.t = 0
         self._bufs: dict = {}
         self._tc_ws: torch.Tensor | None = None
+        self._out_weight = torch.as_tensor(OUT_WEIGHT, device=self.device)
 
     # buffers per batch size
     def _buf(self, m: int) -> dict:
@@ -295,6 +316,7 @@ class MLP:
                 "gw": [torch.empty_like(w) for w in self.w],
                 "gb": [torch.empty_like(x) for x in self.b],
                 "loss": torch.empty(1, device=dev),
+                "winner": torch.empty(m, dtype=torch.int32, device=dev),
             }
             self._bufs[m] = b
         return b
@@ -343,12 +365,15 @@ class MLP:
         return bf["z"][3]
 
     def backward_and_step(self, target: torch.Tensor, lr: float, wd: float = 1e-5) -> torch.Tensor:
-        """MSE against target [m, N_OUT] (FP32), gradients, one Adam step; returns the loss (device)."""
+        """Winner-takes-all MSE of the heads against target [m, N_OUT] (FP32;
+        winner by (C1, A1), C3 weighted by OUT_WEIGHT), gradients, one Adam
+        step; returns the loss (device)."""
         bf = self._buf(int(target.shape[0]))
         m = int(target.shape[0])
         dev = self.device
-        _call("qssb_mse", dev, _ptr(bf["z"][3]), _ptr(target), m, N_OUT, N_OUT_PAD, _ptr(bf["dy"]),
-              _ptr(bf["loss"]), _stream(dev))
+        _call("qssb_mse_heads", dev, _ptr(bf["z"][3]), _ptr(target), m, N_OUT, HEADS, N_OUT_PAD,
+              _ptr(self._out_weight), 3, ctypes.c_float(WTA_EPS), _ptr(bf["dy"]), _ptr(bf["loss"]),
+              _ptr(bf["winner"]), _stream(dev))
         _call("qssb_to_bf16", dev, _ptr(bf["dy"]), m * N_OUT_PAD, _ptr(bf["dy_bf"]), _stream(dev))
         grad_bf, grad_f = bf["dy_bf"], bf["dy"]
         for i in (3, 2, 1, 0):
@@ -375,11 +400,12 @@ class MLP:
         return bf["loss"]
 
     def predict(self, x: torch.Tensor) -> np.ndarray:
+        """Scaled outputs [m, HEADS, N_OUT] of x [m, N_IN]."""
         m = int(x.shape[0])
         pad = (-m) % 16
         if pad:
             x = torch.cat([x, torch.zeros((pad, N_IN), dtype=x.dtype, device=x.device)])
-        return self.forward(x)[:m, :N_OUT].cpu().numpy()
+        return self.forward(x)[:m, :HEADS * N_OUT].cpu().numpy().reshape(m, HEADS, N_OUT)
 
 
 class Proposer:
@@ -425,16 +451,28 @@ class Proposer:
         return {"epochs": epochs, "steps": step, "final_train_mse": losses[-1] if losses else None}
 
     def validate(self, n: int = 2048, seed: int = 12345) -> dict:
+        """Errors of the best head per sample (the head nearest the target in
+        (C1, A1), as the refinement's first batch picks it by loss) on fresh
+        forward-model samples: RMS and median, scaled and in A."""
         x, t, _ = self.make_data(n, seed)
         pred = self.mlp.predict(x)
-        err = pred - t.cpu().numpy()
-        return {"rmse_scaled": np.sqrt(np.mean(err ** 2, axis=0)).tolist(),
-                "rmse_units": (np.sqrt(np.mean(err ** 2, axis=0)) * OUT_SCALE).tolist()}
+        tt = t.cpu().numpy()
+        d = pred - tt[:, None, :]
+        win = np.argmin(np.sum(d[..., :3] ** 2, axis=-1), axis=1)
+        err = d[np.arange(len(d)), win]
+        rmse = np.sqrt(np.mean(err ** 2, axis=0))
+        return {"rmse_scaled": rmse.tolist(), "rmse_units": (rmse * OUT_SCALE).tolist(),
+                "median_abs_units": (np.median(np.abs(err), axis=0) * OUT_SCALE).tolist()}
 
     def propose(self, be) -> np.ndarray:
-        """Two hypotheses [2, 4] (C10, C12, phi12, C30): the canonical proposal and its flip."""
-        p = decode(self.mlp.predict(backend_features(be)))[0]
-        return np.stack([p, flipped(p)[0]])
+        """2 x HEADS hypotheses [8, 4] (C10, C12, phi12, C30): each head's
+        canonical proposal followed by its sign flip."""
+        z = self.mlp.predict(backend_features(be))[0]
+        out = []
+        for h in range(HEADS):
+            p = decode(z[h][None])
+            out += [p[0], flipped(p)[0]]
+        return np.stack(out)
 
 
 # ------------------------------------------------------------- refinement
@@ -673,20 +711,122 @@ def surrogate_search(be, starts: np.ndarray, widths: np.ndarray, batch: int, rou
     return from_x(c)[0], len(fs) - n_prior, rounds
 
 
-def learned_refine(be, hypotheses: np.ndarray, widths: np.ndarray, batch: int, rounds: int,
-                   rng: np.random.Generator, done=None, zoom_rounds: int = 6,
-                   zoom_shrink: float = 0.8, min_radius: float = 1e-7):
-    """The refinement after a proposal, ``batch`` evaluations per round: a
-    zoom over the two sign hypotheses (robust into the right basin), then the
-    trust-region quadratic surrogate from its best point, fitted to every
-    point scored so far (fast to a precise minimum). Returns (best (C10, C12,
-    phi12, C30), SSB evaluations, rounds)."""
-    hist: tuple[list, list] = ([], [])
-    best, ev1, r1 = zoom_search(be, hypotheses, widths, batch, zoom_rounds, zoom_shrink, rng,
-                                done=done, history=hist)
-    if done is not None and r1 < zoom_rounds:
-        return best, ev1, r1
-    w = np.asarray(widths, np.float64) * zoom_shrink ** zoom_rounds
-    best2, ev2, r2 = surrogate_search(be, to_x(best[None]), w, batch, max(1, rounds - r1), rng,
-                                      done=done, radius0=1.0, min_radius=min_radius, history=hist)
-    return best2, ev1 + ev2, r1 + r2
+REFINE_MARGIN = 0.1  # the refinement may step this share of each range beyond the sweep box
+
+
+def refine_box() -> tuple[np.ndarray, np.ndarray]:
+    """Bounds of the refinement: the sweep box widened by REFINE_MARGIN of its
+    span on each side (a truth on the box's edge stays inside the designs)."""
+    span = BOX_HI - BOX_LO
+    return BOX_LO - REFINE_MARGIN * span, BOX_HI + REFINE_MARGIN * span
+
+
+def _local_design(centre: np.ndarray, r: float, dims: int, batch: int,
+                  with_centre: bool) -> np.ndarray:
+    """The centre (optional), centre +- r e_i (i < dims), then centre + r (e_i +- e_k)/sqrt 2
+    until ``batch`` points."""
+    eye = np.eye(4)[:dims]
+    pts = [centre] if with_centre else []
+    pts += [centre + s * r * e for e in eye for s in (1.0, -1.0)]
+    pairs = [(i, k) for i in range(dims) for k in range(i + 1, dims)]
+    for sign in (1.0, -1.0):
+        for i, k in pairs:
+            pts.append(centre + r * (eye[i] + sign * eye[k]) / math.sqrt(2.0))
+    while len(pts) < batch:  # more points than the patterns: a wider axial ring
+        j = len(pts)
+        pts.append(centre + 2.0 * r * (1.0 if j % 2 else -1.0) * eye[(j // 2) % dims])
+    return np.asarray(pts[:batch])
+
+
+def quadratic_refine(be, hypotheses: np.ndarray, step: float, batch: int, rounds: int,
+                     done=None, lo=None, hi=None, dims: int = 3, min_step: float = 0.05):
+    """The short refinement a proposal seeds: ``batch`` SSB evaluations per
+    round, each round one ``qssb_loss_batch`` call, in x = (C10, a, b, C30).
+
+    Round 0 scores the hypotheses (the proposal's heads and signs; spare
+    slots take the design below around the first) and keeps the best as the
+    centre c. Later rounds move the first ``dims`` coordinates
+    (C1, A1; C3 stays at the hypothesis's value - it shifts the phase by about
+    1e-5 rad per 1000 A on the 64^2 test scans): while fewer than 1 + 2 dims
+    scored points lie within 3 rho of c, a round scores the design
+    c +- rho e_i plus diagonals; after that it fits a quadratic in (x - c) /
+    rho (diagonal Hessian below 1 + dims + dims (dims + 1) / 2 + 2 points,
+    full above; weights 1 / (1 + d^2)) to those points, steps to the model's
+    minimiser within 2 rho and scores that point with a design of radius
+    rho / 2 around it (which keeps the next fit posed). rho starts at
+    ``step`` (A), follows accepted moves (twice the move, at least half the
+    old rho, never more) and halves when a round finds nothing better.
+    Returns (best (C10, C12, phi12, C30), SSB evaluations, rounds, ok): ok
+    means ``done(best)`` held, or, without ``done``, that rho fell below
+    ``min_step`` within ``rounds``."""
+    if lo is None or hi is None:
+        lo, hi = refine_box()
+    xs: list[np.ndarray] = []
+    fs: list[float] = []
+
+    def score(cand: np.ndarray) -> None:
+        cand = np.clip(np.asarray(cand, np.float64), lo, hi)
+        ab = from_x(cand)
+        losses = be.variance_loss_batch(ab[:, 0], ab[:, 1], ab[:, 2], ab[:, 3]).cpu().numpy()
+        xs.extend(cand)
+        fs.extend(float(v) for v in losses)
+
+    rho = float(step)
+    hyp = np.array(hypotheses, np.float64, ndmin=2).reshape(-1, 4)[:batch]
+    if len(hyp) < batch:  # spare slots: the design around the first hypothesis
+        hyp = np.vstack([hyp, _local_design(hyp[0], rho, dims, batch - len(hyp), False)])
+    score(hyp)
+    j = int(np.argmin(fs))
+    c, fc = xs[j].copy(), fs[j]
+    if done is not None and done(from_x(c)[0]):
+        return from_x(c)[0], len(fs), 1, True
+    n_diag = 1 + 2 * dims
+    n_full = 1 + dims + dims * (dims + 1) // 2
+    for r in range(1, rounds):
+        X = np.asarray(xs)
+        F = np.asarray(fs)
+        U = (X[:, :dims] - c[:dims]) / rho
+        dist = np.linalg.norm(U, axis=1)
+        near = np.nonzero(dist <= 3.0)[0]
+        if len(near) >= n_diag:
+            kind = "full" if len(near) >= n_full + 2 else "diag"
+            A = _quadratic_design(U[near], kind)
+            wt = 1.0 / (1.0 + dist[near] ** 2)
+            coef = np.linalg.lstsq(A * wt[:, None], (F[near] - fc) * wt, rcond=None)[0]
+            u = np.zeros(4)
+            u[:dims] = _model_step(coef, dims, kind, 2.0) * rho
+            cand = _local_design(c + u, 0.5 * rho, dims, batch, with_centre=True)
+        else:
+            cand = _local_design(c, rho, dims, batch, with_centre=False)
+        n0 = len(fs)
+        score(cand)
+        k = n0 + int(np.argmin(fs[n0:]))
+        if fs[k] < fc:
+            moved = float(np.linalg.norm(xs[k][:dims] - c[:dims]))
+            c, fc = xs[k].copy(), fs[k]
+            rho = min(rho, max(2.0 * moved, 0.5 * rho))
+        else:
+            rho *= 0.5
+        if done is not None and done(from_x(c)[0]):
+            return from_x(c)[0], len(fs), r + 1, True
+        if rho < min_step:
+            return from_x(c)[0], len(fs), r + 1, done is None
+    return from_x(c)[0], len(fs), rounds, False
+
+
+def learned_refine(be, hypotheses: np.ndarray, step: float = 8.0, batch: int = 8,
+                   rounds: int = 12, rng: np.random.Generator | None = None, done=None,
+                   fallback_rounds: int = 200):
+    """Proposal + refinement with the plain sweep as the fallback:
+    ``quadratic_refine`` from the hypotheses, and when it does not end ok
+    (``done`` unmet, or no convergence within ``rounds``) the plain
+    64-candidate zoom sweep over the whole box, whose evaluations are added.
+    Returns (best (C10, C12, phi12, C30), SSB evaluations, rounds,
+    fell_back)."""
+    best, ev, r, ok = quadratic_refine(be, hypotheses, step, batch, rounds, done=done)
+    if ok:
+        return best, ev, r, False
+    rng = np.random.default_rng(0) if rng is None else rng
+    best2, ev2, r2 = zoom_search(be, None, (BOX_HI - BOX_LO) / 2, 64, fallback_rounds, 0.75, rng,
+                                 done=done)
+    return best2, ev + ev2, r + r2, True

@@ -1,7 +1,9 @@
 """The learned proposer's CUDA kernels against the FP64 oracle
 (oracle/proposer_oracle.py): forward-model features, features from a
-resident G, and the MLP's outputs and gradients; plus a short training run
-that must cut the validation error."""
+resident G, the winner-takes-all loss, and the MLP's outputs and gradients;
+a short training run that must cut the validation error; what the trained
+network gains over the plain sweep; and a held-out check of the training
+data against fully simulated scans."""
 from __future__ import annotations
 
 import ctypes
@@ -80,21 +82,58 @@ def test_backend_features_match_oracle():
     np.testing.assert_allclose(got, want, rtol=1e-2, atol=1e-2)  # BF16 output
 
 
+def test_mse_heads_matches_oracle():
+    """``qssb_mse_heads`` on given FP32 outputs: loss, gradient and winners
+    equal the FP64 oracle's (one head reduces to the plain MSE)."""
+    rng = np.random.default_rng(11)
+    m, n_out, heads, ld = 64, 4, 4, 16
+    y = torch.as_tensor(rng.normal(size=(m, ld)).astype(np.float32), device=DEV)
+    t = torch.as_tensor(rng.normal(size=(m, n_out)).astype(np.float32), device=DEV)
+    w = torch.as_tensor(np.array([1.0, 1.0, 1.0, 0.1], np.float32), device=DEV)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for h, n_sel, eps in ((4, 3, 0.05), (4, 4, 0.0), (1, 4, 0.0)):
+        dy = torch.full((m, ld), 7.0, device=DEV)
+        loss = torch.empty(1, device=DEV)
+        win = torch.empty(m, dtype=torch.int32, device=DEV)
+        _lib.check(_lib.load().qssb_mse_heads(_ptr(y), _ptr(t), m, n_out, h, ld, _ptr(w), n_sel,
+                                              ctypes.c_float(eps), _ptr(dy), _ptr(loss), _ptr(win),
+                                              stream))
+        l_ref, dy_ref, win_ref = po.heads_loss_and_grad(y.cpu().numpy(), t.cpu().numpy(), n_out, h,
+                                                        w.cpu().numpy(), n_sel, eps)
+        np.testing.assert_array_equal(win.cpu().numpy(), win_ref)
+        np.testing.assert_allclose(dy.cpu().numpy(), dy_ref, rtol=1e-5, atol=1e-9)
+        assert abs(loss.item() - l_ref) <= 1e-6 * l_ref
+    bad = _lib.load().qssb_mse_heads(_ptr(y), _ptr(t), m, n_out, 5, ld, None, 3,
+                                     ctypes.c_float(0.0), _ptr(dy), None, None, stream)
+    assert bad != 0  # 5 heads x 4 outputs do not fit 16 columns
+
+
 def test_mlp_outputs_and_gradients_match_oracle():
+    """Forward outputs and every gradient of the winner-takes-all training
+    step against the FP64 oracle. Row r's target lies within 0.01 of head
+    r mod 4 in (C1, A1), which select the winner, so that the winners do not
+    hang on BF16 rounding, and is drawn freely in C3, which then carries most
+    of the loss."""
     mlp = pr.MLP(DEV, seed=3)
     rng = np.random.default_rng(4)
     m = 32
     x = torch.as_tensor(rng.uniform(0, 2, size=(m, pr.N_IN)).astype(np.float32), device=DEV).to(torch.bfloat16)
-    t = torch.as_tensor(rng.normal(size=(m, pr.N_OUT)).astype(np.float32), device=DEV)
     ws = [w.float().cpu().numpy().astype(np.float64) for w in mlp.w_bf]
     bs = [b.cpu().numpy().astype(np.float64) for b in mlp.b]
-    loss_ref, y_ref, dws, dbs = po.mlp_loss_and_grads(x.float().cpu().numpy(), ws, bs,
-                                                       t.cpu().numpy(), pr.N_OUT)
     y = mlp.forward(x).cpu().numpy()
-    np.testing.assert_allclose(y[:, :pr.N_OUT], y_ref[:, :pr.N_OUT], rtol=2e-2, atol=2e-2)
+    heads = y[:, :pr.HEADS * pr.N_OUT].reshape(m, pr.HEADS, pr.N_OUT)
+    t_np = heads[np.arange(m), np.arange(m) % pr.HEADS] + 0.01 * rng.normal(size=(m, pr.N_OUT))
+    t_np[:, 3] = rng.normal(size=m)
+    t_np = t_np.astype(np.float32)
+    t = torch.as_tensor(t_np, device=DEV)
+    loss_ref, y_ref, dws, dbs = po.mlp_loss_and_grads(x.float().cpu().numpy(), ws, bs, t_np,
+                                                       pr.N_OUT, pr.HEADS, pr.OUT_WEIGHT, 3,
+                                                       pr.WTA_EPS)
+    np.testing.assert_allclose(y, y_ref, rtol=2e-2, atol=2e-2)
     loss = mlp.backward_and_step(t, lr=0.0).item()
-    assert abs(loss - loss_ref) <= 2e-2 * loss_ref
     bufs = mlp._buf(m)
+    np.testing.assert_array_equal(bufs["winner"].cpu().numpy(), np.arange(m) % pr.HEADS)
+    assert abs(loss - loss_ref) <= 2e-2 * loss_ref
     for i in range(4):
         for got, want in ((bufs["gw"][i].cpu().numpy(), dws[i]), (bufs["gb"][i].cpu().numpy(), dbs[i])):
             rel = np.linalg.norm(got - want) / max(np.linalg.norm(want), 1e-30)
@@ -114,9 +153,9 @@ def test_learned_proposal_needs_fewer_evaluations_than_plain_sweep():
     """What the trained network gains: on weak-phase datasets (0.03 rad atoms,
     64^2 scans, 1e6 e per position) the proposal plus the 8-candidate
     refinement reaches a phase within 1e-4 rad RMS of the FP64 oracle at the
-    true aberrations with at least 6x fewer SSB evaluations, in total over
-    three cases, than the plain 64-candidate zoom sweep over the whole range
-    (measured on a B200: about 8x); every learned fit reaches the target."""
+    true aberrations with at least 15x fewer SSB evaluations, in total over
+    six cases, than the plain 64-candidate zoom sweep over the whole range;
+    every learned fit reaches the target without the plain fallback."""
     from oracle import ssb_torch_fp64 as tf
     from quantem.gpu_b200 import B200SSBBackend
     from quantem.gpu_b200.synthetic import SyntheticSpec, generate
@@ -125,8 +164,7 @@ def test_learned_proposal_needs_fewer_evaluations_than_plain_sweep():
     prop.train(n_samples=50_000, epochs=40)
     rng = np.random.default_rng(77)
     plain_total = learned_total = 0
-    w0 = np.array([120.0, 40.0, 40.0, 5000.0])
-    for i in range(3):
+    for i in range(6):
         ab = draw_aberrations(rng, 1)[0]
         spec = SyntheticSpec(scan_shape=(64, 64), detector_shape=(64, 64),
                              det_sampling_mrad=20.0 / 12.0, dose=1e6, C10=float(ab[0]),
@@ -146,42 +184,47 @@ def test_learned_proposal_needs_fewer_evaluations_than_plain_sweep():
 
         _, pe, _ = pr.zoom_search(be, None, (pr.BOX_HI - pr.BOX_LO) / 2, 64, 200, 0.75,
                                   np.random.default_rng(1), done=ok)
-        best, le, _ = pr.learned_refine(be, pr.to_x(prop.propose(be)), w0, 8, 120,
-                                        np.random.default_rng(2), done=ok)
-        assert ok(best), i
+        best, le, _, fell_back = pr.learned_refine(be, pr.to_x(prop.propose(be)), done=ok)
+        assert ok(best) and not fell_back, (i, le)
         plain_total += pe
         learned_total += le
-    assert learned_total * 6 <= plain_total, (learned_total, plain_total)
+    assert learned_total * 15 <= plain_total, (learned_total, plain_total)
 
 
 def test_forward_model_features_match_simulated_scans():
     """Held-out check of the training data: for four aberration draws the
-    network never saw, the forward model's maps at the lattice reflections
-    ((8, 0), (16, 0), (0, 8), (0, 16) in units of 1/32 A^-1, where a crystal's
-    signal lies) match the maps measured from fully simulated 64^2 x 64^2
-    scans at 1e6 e per position (the SSB forward model with Poisson counts):
-    cosine similarity of every reflection map >= 0.9, mean >= 0.95. (The
-    other twelve maps carry noise in both.)"""
+    network never saw, the forward model's 16 maps (all at reflections of the
+    synthetic crystal; phase part only) match the maps measured from fully
+    simulated 64^2 x 64^2 scans at 1e6 e per position (|FFT(probe x
+    exp(i phi))|^2 per probe position, Poisson counts). Cosine similarity
+    per map: on the
+    configs' 0.3 rad objects every map >= 0.85 and the mean >= 0.97; on
+    weak-phase (0.03 rad) objects, whose maps carry ten times less signal
+    over the same counting noise, every map >= 0.8 and the mean >= 0.95.
+    The lowest maps are those at the largest |Q| (24 / 32 A^-1), whose
+    double-overlap lens is narrowest."""
     from quantem.gpu_b200 import B200SSBBackend
     from quantem.gpu_b200.synthetic import SyntheticSpec, generate
 
     lat = pr.TrainingLattice(DEV)
-    rng = np.random.default_rng(2024)
-    cos_all = []
-    for i in range(4):
-        ab = draw_aberrations(rng, 1)
-        spec = SyntheticSpec(scan_shape=(64, 64), detector_shape=(64, 64),
-                             det_sampling_mrad=20.0 / 12.0, dose=1e6, C10=float(ab[0, 0]),
-                             C12=float(ab[0, 1]), phi12=float(ab[0, 2]), C30=float(ab[0, 3]),
-                             seed=500 + i)
-        be = B200SSBBackend(generate(spec, DEV).counts, semiangle=20.0, scan_sampling=0.5,
-                            det_sampling=20.0 / 12.0, voltage_kV=300, device=DEV)
-        got = pr.backend_features(be).float().view(16, -1).cpu().numpy()
-        want = lat.features(ab, np.random.default_rng(i), sigma=(1e-6, 1e-6)).float().view(16, -1)
-        want = want.cpu().numpy()
-        for q in (1, 3, 5, 7):
-            a, b = got[q], want[q]
-            cos_all.append(float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b))))
-        be.close()
-    assert min(cos_all) >= 0.9, cos_all
-    assert np.mean(cos_all) >= 0.95, cos_all
+    for peak, lo, mean in ((0.3, 0.85, 0.97), (0.03, 0.8, 0.95)):
+        rng = np.random.default_rng(2024)
+        cos_all = []
+        for i in range(4):
+            ab = draw_aberrations(rng, 1)
+            spec = SyntheticSpec(scan_shape=(64, 64), detector_shape=(64, 64),
+                                 det_sampling_mrad=20.0 / 12.0, dose=1e6, C10=float(ab[0, 0]),
+                                 C12=float(ab[0, 1]), phi12=float(ab[0, 2]), C30=float(ab[0, 3]),
+                                 atom_peak_rad=peak, seed=500 + i)
+            be = B200SSBBackend(generate(spec, DEV).counts, semiangle=20.0, scan_sampling=0.5,
+                                det_sampling=20.0 / 12.0, voltage_kV=300, device=DEV)
+            got = pr.backend_features(be).float().view(16, -1).cpu().numpy()
+            want = lat.features(ab, np.random.default_rng(i), sigma=(1e-6, 1e-6),
+                                informative=(16, 16), amplitude_contrast=(0.0, 0.0))
+            want = want.float().view(16, -1).cpu().numpy()
+            for q in range(16):
+                a, b = got[q], want[q]
+                cos_all.append(float(a @ b / (np.linalg.norm(a) * np.linalg.norm(b))))
+            be.close()
+        assert min(cos_all) >= lo, (peak, cos_all)
+        assert np.mean(cos_all) >= mean, (peak, np.mean(cos_all))

@@ -126,3 +126,83 @@ def test_surrogate_search_step_stays_in_the_trust_region():
     u = pr._model_step(coef, d, "full", 10.0)
     np.testing.assert_allclose(u, -np.array([1.0, -2.0, 0.5, 0.0]) / np.array([4.0, 2.0, 3.0, 1.0]),
                                rtol=1e-9)
+
+
+def test_heads_loss_gradient_is_the_derivative_of_the_loss():
+    """The oracle of ``qssb_mse_heads``: with eps = 0 its gradient is the
+    derivative of its loss (central differences, away from winner changes);
+    one head is the plain MSE; the losing heads get eps / (heads - 1) of
+    their own MSE gradient."""
+    rng = np.random.default_rng(3)
+    m, n_out, heads = 5, 4, 4
+    y = rng.normal(size=(m, 16))
+    t = rng.normal(size=(m, n_out))
+    w = np.array([1.0, 1.0, 1.0, 0.1])
+    loss, dy, win = po.heads_loss_and_grad(y, t, n_out, heads, w, 3, 0.0)
+    h = 1e-6
+    for r in range(m):
+        for c in range(16):
+            yp, ym = y.copy(), y.copy()
+            yp[r, c] += h
+            ym[r, c] -= h
+            lp = po.heads_loss_and_grad(yp, t, n_out, heads, w, 3, 0.0)[0]
+            lm = po.heads_loss_and_grad(ym, t, n_out, heads, w, 3, 0.0)[0]
+            assert abs((lp - lm) / (2 * h) - dy[r, c]) < 1e-6
+    l1, dy1, _ = po.heads_loss_and_grad(y, t, n_out, 1)
+    np.testing.assert_allclose(l1, np.mean((y[:, :4] - t) ** 2))
+    np.testing.assert_allclose(dy1[:, :4], 2 * (y[:, :4] - t) / (m * n_out))
+    assert not dy1[:, 4:].any()
+    _, dye, _ = po.heads_loss_and_grad(y, t, n_out, heads, w, 3, 0.3)
+    for r in range(m):
+        for hh in range(heads):
+            d = 2 * w * (y[r, 4 * hh:4 * hh + 4] - t[r]) / (m * n_out)
+            s = 0.7 if hh == win[r] else 0.1
+            np.testing.assert_allclose(dye[r, 4 * hh:4 * hh + 4], s * d, rtol=1e-12)
+
+
+def test_quadratic_refine_converges_from_a_proposal_in_few_rounds():
+    """From the best of eight hypotheses (one within ~15 A of the truth in C1
+    and A1, seven decoys) the refinement reaches 0.05 A of the truth of a
+    quadratic-plus-quartic bowl within 6 rounds of 8 evaluations, one loss
+    batch per round, C3 held at the hypothesis's (true) value."""
+    rng = np.random.default_rng(0)
+    widths = np.array([20.0, 20.0, 20.0, 3000.0])
+    for trial in range(5):
+        truth = np.array([rng.uniform(-400, 400), rng.uniform(10, 90), rng.uniform(0, 3),
+                          rng.uniform(500, 9000)])
+        be = _QuarticLoss(truth, widths, seed=trial)
+        tx = pr.to_x(truth[None])[0]
+        good = tx + np.append(rng.normal(0.0, 8.0, 3), 0.0)
+        decoys = tx + rng.normal(0.0, 1.0, (7, 4)) * np.array([300.0, 80.0, 80.0, 4000.0])
+        hyps = np.vstack([decoys[:3], good, decoys[3:]])
+
+        def done(est):
+            return np.linalg.norm(pr.to_x(est[None])[0][:3] - tx[:3]) < 0.05
+
+        best, evals, rounds, ok = pr.quadratic_refine(be, hyps, 8.0, 8, 12, done=done)
+        assert ok and done(best), trial
+        assert evals == 8 * rounds and be.calls == rounds
+        assert rounds <= 6, (trial, rounds)
+        # without a stopping rule it converges on its own (the step falls below 0.05 A)
+        be2 = _QuarticLoss(truth, widths, seed=trial)
+        best2, _, _, ok2 = pr.quadratic_refine(be2, hyps, 8.0, 8, 40)
+        assert ok2 and np.linalg.norm(pr.to_x(best2[None])[0][:3] - tx[:3]) < 0.5
+
+
+def test_learned_refine_falls_back_to_the_plain_sweep():
+    """When the refinement cannot meet the target within its rounds, the
+    plain 64-candidate sweep runs and its evaluations are added."""
+    truth = np.array([120.0, 30.0, 0.4, 4000.0])
+    be = _QuarticLoss(truth, np.array([20.0, 20.0, 20.0, 3000.0]))
+    tx = pr.to_x(truth[None])[0]
+    calls = {"n": 0}
+
+    def done(est):  # met only once the plain sweep has scored a few batches
+        calls["n"] += 1
+        return be.calls > 8 and np.linalg.norm(pr.to_x(est[None])[0][:3] - tx[:3]) < 40.0
+
+    best, evals, rounds, fell_back = pr.learned_refine(be, tx[None] + 200.0, rounds=4, done=done)
+    assert fell_back
+    assert evals == 8 * 4 + 64 * (be.calls - 4)
+    lo, hi = pr.refine_box()
+    assert np.all(lo < pr.BOX_LO) and np.all(hi > pr.BOX_HI)
