@@ -1049,10 +1049,13 @@ def _headline(line: dict) -> dict:
     return _sig(h, 4)
 
 
-def run_profile_once(local: int, with_256: bool = False, with_512: str | None = None) -> None:
+def run_profile_once(local: int, with_256: bool = False, with_512: str | None = None,
+                     with_mlp: bool = False) -> None:
     """One cold reconstruction, one warm object, one loss and one 64-candidate
     loss batch on the 128^4 workload, untimed: the launch sequence the ncu
-    summaries under profiles/ are captured from."""
+    summaries under profiles/ are captured from. ``with_mlp``: then two
+    training steps of the proposer's MLP at batch 256 on random inputs (its
+    first tcgen05 launch is the 256 x 512 x 16384 input layer)."""
     from quantem.gpu_b200 import B200SSBBackend
     from quantem.gpu_b200.synthetic import CONFIGS, generate
 
@@ -1090,6 +1093,17 @@ def run_profile_once(local: int, with_256: bool = False, with_512: str | None = 
         _, out["loss512"] = be.reconstruct_with_loss(spec.C10, 0.0, 0.0)
         out["n_bf512"] = be.num_bf
         torch.cuda.synchronize(dev)
+    if with_mlp:
+        from quantem.gpu_b200 import proposer as pr
+
+        mlp = pr.MLP(dev, seed=0)
+        g = torch.Generator(device=dev).manual_seed(1)
+        x = torch.rand((256, pr.N_IN), generator=g, device=dev).to(torch.bfloat16)
+        t = torch.rand((256, pr.N_OUT), generator=g, device=dev)
+        for _ in range(2):
+            mlp.forward(x)
+            loss_t = mlp.backward_and_step(t, 1e-4)
+        out["mlp_loss"] = float(loss_t.item())
     print(json.dumps(out))
 
 
@@ -1105,6 +1119,8 @@ def main() -> None:
                     help="--profile-once: also one 256^2 scan loss evaluation")
     ap.add_argument("--with-512", choices=["full", "small"], default=None,
                     help="--profile-once: also one 512^2 cold preparation, object and loss")
+    ap.add_argument("--with-mlp", action="store_true",
+                    help="--profile-once: also two proposer MLP training steps (batch 256)")
     ap.add_argument("--no-large", action="store_true",
                     help="skip the 512^2 x 192^2 (19.3 GB) leg")
     ap.add_argument("--no-stress", action="store_true",
@@ -1117,7 +1133,7 @@ def main() -> None:
     world, rank, local = _dist()
     try:
         if args.profile_once:
-            run_profile_once(local, args.with_256, args.with_512)
+            run_profile_once(local, args.with_256, args.with_512, args.with_mlp)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         else:

@@ -479,12 +479,15 @@ int qssb_gemm_bf16(const void* A, int32_t lda, int32_t trans_a, const void* B, i
 
 /* The same GEMM on the 5th-generation tensor cores (tcgen05.mma kind::f16,
  * FP32 accumulator in tensor memory), split over K: 128 x 128 output tiles,
- * splits K ranges each, partial tiles in the workspace summed in split order
- * (deterministic), then the epilogue of qssb_gemm_bf16. M and N multiples of
- * 128, K a multiple of 64 x splits, leading dimensions multiples of 8, A and
- * B 16-byte aligned, workspace 256-byte aligned and at least
- * qssb_gemm_tc_workspace_bytes; its last 256 bytes hold an int set to 1 when
- * a bounded wait inside the kernel gave up (the result is then invalid). */
+ * splits K ranges each; with splits > 1 the partial tiles go to the workspace
+ * and are summed in split order (deterministic), then the epilogue of
+ * qssb_gemm_bf16; with splits == 1 the MMA kernel applies that epilogue and
+ * writes C itself (C then 16-byte aligned, ldc a multiple of 4). M and N
+ * multiples of 128, K a multiple of 64 x splits, leading dimensions multiples
+ * of 8, A and B 16-byte aligned, workspace 256-byte aligned and at least
+ * qssb_gemm_tc_workspace_bytes (4 splits M N + 256 bytes with split K, 256
+ * without); its last 256 bytes hold an int set to 1 when a bounded wait
+ * inside the kernel gave up (the result is then invalid). */
 int qssb_gemm_tc_workspace_bytes(int32_t M, int32_t N, int32_t K, int32_t splits, size_t* bytes);
 int qssb_gemm_bf16_tc(const void* A, int32_t lda, int32_t trans_a, const void* B, int32_t ldb,
                       int32_t trans_b, int32_t M, int32_t N, int32_t K, int32_t splits,
@@ -493,7 +496,8 @@ int qssb_gemm_bf16_tc(const void* A, int32_t lda, int32_t trans_a, const void* B
 /* dz = dy * GELU'(pre) (FP32 and BF16 copies), n elements. */
 int qssb_gelu_backward(const float* dy, const float* pre, int64_t n, void* dz_bf16, float* dz,
                        void* stream);
-/* db[c] = sum over rows of dz[r][c] (fixed order, FP64 accumulation). */
+/* db[c] = sum over rows of dz[r][c] (FP64 accumulation: eight interleaved
+ * row slices folded in a fixed order). */
 int qssb_bias_grad(const float* dz, int32_t rows, int32_t cols, float* db, void* stream);
 /* Mean squared error over the first n_out of ld columns and its gradient dy
  * (zero in columns n_out..ld-1); loss (device float) may be NULL. */

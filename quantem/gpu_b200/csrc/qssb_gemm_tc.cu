@@ -2,20 +2,23 @@
 // tensor cores (tcgen05): C[M][N] (+)= op(A)[M][K] op(B)[K][N], BF16 operands,
 // FP32 accumulation in tensor memory. No counterpart in the reference.
 //
-// One CTA (4 warps) per 128 x 128 output tile and K range (split K): the
-// tile's operands are staged in shared memory 64 K-elements at a time, two
-// stages deep, in the no-swizzle canonical layouts of the MMA's shared-memory
-// descriptors (8 x 16-byte core matrices; a K-major operand keeps 8
-// consecutive k of a row in one 16-byte unit, an MN-major one 8 consecutive
-// rows of one k), so every global load and shared store is 16 bytes. One
-// thread issues the four 128 x 128 x 16 MMAs of a stage (tcgen05.mma
-// kind::f16) and commits them to the stage's mbarrier, which the CTA waits on
-// before refilling that stage. The accumulator lives in 128 TMEM columns;
-// the epilogue reads it with tcgen05.ld (each warp its 32 lanes = rows) and
-// writes FP32 partial tiles [split][M][N]; k_gemm_tc_reduce adds the splits
-// in a fixed order and applies bias / accumulate / GELU as qssb_gemm_bf16.
-// Every mbarrier wait is bounded; a wait that runs out sets *status and the
-// CTA skips its epilogue.
+// One CTA (4 warps, two CTAs per SM) per 128 x 128 output tile and K range
+// (split K): the tile's operands are staged in shared memory 64 K-elements at
+// a time by cp.async in a three-stage ring, in the no-swizzle canonical
+// layouts of the MMA's shared-memory descriptors (8 x 16-byte core matrices;
+// a K-major operand keeps 8 consecutive k of a row in one 16-byte unit, an
+// MN-major one 8 consecutive rows of one k). Each thread's copies are
+// ordered so that a quarter-warp writes eight different 16-byte bank groups.
+// One thread issues the four 128 x 128 x 16 MMAs of a stage (tcgen05.mma
+// kind::f16) and commits them to the stage's mbarrier; a stage is refilled
+// once that barrier shows its MMAs done, so loads of the next two k-tiles
+// overlap the MMAs of the current one. The accumulator lives in 128 TMEM
+// columns; the epilogue reads it with tcgen05.ld (each warp its 32 lanes =
+// rows). Without split K it applies bias / accumulate / GELU and writes C
+// directly; with it, FP32 partial tiles [split][M][N] go to the workspace and
+// k_gemm_tc_reduce adds the splits in a fixed order and applies them. Every
+// mbarrier wait is bounded; a wait that runs out sets *status and the CTA
+// skips its epilogue.
 #include <cuda_bf16.h>
 #include <math.h>
 
@@ -25,7 +28,7 @@ namespace qssb {
 
 namespace tc {
 
-constexpr int BM = 128, BN = 128, BK = 64, STAGES = 2, THREADS = 128;
+constexpr int BM = 128, BN = 128, BK = 64, STAGES = 3, THREADS = 128;
 constexpr int TILE_BYTES = BM * BK * 2;          // 16 KB per operand per stage (BM == BN)
 constexpr int SMEM_BYTES = STAGES * 2 * TILE_BYTES;
 constexpr long long kWaitLimit = 1LL << 26;      // try_wait polls before giving up
@@ -73,35 +76,57 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
 constexpr uint32_t kLbo = BM / 8 * 128;
 constexpr uint32_t kSbo = 128;
 
-// Stage one operand tile: rows [r0, r0 + 128) of op(X) (M or N side), k in
-// [k0, k0 + 64). X is row-major with leading dimension ld; kmajor: X[row][k]
-// (k contiguous), else X[k][row] (rows contiguous). 16-byte units only.
-__device__ __forceinline__ void stage_tile(char* dst, const __nv_bfloat16* __restrict__ X, int ld,
-                                           bool kmajor, int r0, int k0, int tid) {
+// Stage one operand tile by cp.async: rows [r0, r0 + 128) of op(X) (M or N
+// side), k in [k0, k0 + 64). X is row-major with leading dimension ld;
+// kmajor: X[row][k] (k contiguous), else X[k][row] (rows contiguous). Unit u
+// of the 1024 16-byte units goes to shared offset 16 u in both layouts'
+// orders (conflict-free stores): K-major u = kg * 128 + row (a thread walks
+// one row's eight 16-byte pieces over its eight units, so the L1-allocating
+// copies reuse each line), MN-major u = kg * 128 + rowgroup * 8 + k % 8.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" :: "r"(dst), "l"(src) : "memory");
+}
+
+__device__ __forceinline__ void stage_tile_async(uint32_t dst, const __nv_bfloat16* __restrict__ X,
+                                                 int ld, bool kmajor, int r0, int k0, int tid) {
 #pragma unroll
     for (int it = 0; it < (BM * BK / 8) / THREADS; ++it) {
-        const int u = tid + it * THREADS;  // 16-byte unit of the 128 x 64 tile
-        int row, kk;
-        if (kmajor) {            // unit = 8 consecutive k of one row
-            row = u >> 3;        // 0..127
-            kk = (u & 7) * 8;    // 0..56
-        } else {                 // unit = 8 consecutive rows of one k
-            kk = u >> 4;         // 0..63
-            row = (u & 15) * 8;  // 0..120
+        const int u = tid + it * THREADS;  // 16-byte unit, in shared-memory order
+        const int kg = u >> 7;             // which 8 k
+        const __nv_bfloat16* src;
+        if (kmajor) {
+            const int row = u & 127;
+            src = X + (size_t)(r0 + row) * ld + (k0 + kg * 8);
+        } else {
+            const int rg = (u >> 3) & 15;  // which 8 rows
+            const int kk = kg * 8 + (u & 7);
+            src = X + (size_t)(k0 + kk) * ld + (r0 + rg * 8);
         }
-        const __nv_bfloat16* src = kmajor ? X + (size_t)(r0 + row) * ld + (k0 + kk)
-                                          : X + (size_t)(k0 + kk) * ld + (r0 + row);
-        const uint4 v = __ldg(reinterpret_cast<const uint4*>(src));
-        const uint32_t off = kmajor ? (kk >> 3) * kLbo + (row >> 3) * kSbo + (row & 7) * 16
-                                    : (kk >> 3) * kLbo + (row >> 3) * kSbo + (kk & 7) * 16;
-        *reinterpret_cast<uint4*>(dst + off) = v;
+        cp_async16(dst + 16u * (uint32_t)u, src);
     }
 }
 
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" :: "n"(N) : "memory");
+}
+
+__device__ __forceinline__ float gelu_tc(float x) {
+    const float s = 0.7978845608028654f;
+    const float u = s * fmaf(0.044715f * x * x, x, x);
+    return 0.5f * x * (1.0f + tanhf(u));
+}
+
 template <bool TA, bool TB>
-__global__ void __launch_bounds__(THREADS, 1) k_gemm_tc(
+__global__ void __launch_bounds__(THREADS, 2) k_gemm_tc(
     const __nv_bfloat16* __restrict__ A, int lda, const __nv_bfloat16* __restrict__ B, int ldb,
-    int M, int N, int k_per_split, float* __restrict__ part, int* __restrict__ status) {
+    int M, int N, int k_per_split, float* __restrict__ part, int* __restrict__ status,
+    const float* __restrict__ bias, int accumulate, float* __restrict__ C, int ldc,
+    __nv_bfloat16* __restrict__ act, int ld_act) {
     extern __shared__ __align__(128) char smem[];
     __shared__ __align__(8) uint64_t bars[STAGES];
     __shared__ uint32_t s_tmem;
@@ -124,22 +149,27 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm_tc(
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&bars[s])));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
+    const uint32_t smem_base = smem_u32(smem);
+    auto load_tile = [&](int kt) {
+        const uint32_t a_addr = smem_base + (kt % STAGES) * 2 * TILE_BYTES;
+        const int k0 = kbeg + kt * BK;
+        stage_tile_async(a_addr, A, lda, a_kmajor, m0, k0, tid);
+        stage_tile_async(a_addr + TILE_BYTES, B, ldb, b_kmajor, n0, k0, tid);
+    };
+    // prologue: the first STAGES - 1 tiles in flight (one commit group each)
+#pragma unroll
+    for (int kt = 0; kt < STAGES - 1; ++kt) {
+        if (kt < ktiles) load_tile(kt);
+        cp_async_commit();
+    }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = s_tmem;
-    const uint32_t smem_base = smem_u32(smem);
     for (int kt = 0; kt < ktiles; ++kt) {
         const int st = kt % STAGES;
-        char* a_tile = smem + st * 2 * TILE_BYTES;
-        char* b_tile = a_tile + TILE_BYTES;
-        if (kt >= STAGES) {  // the MMAs that read this stage two tiles ago are done
-            if (!mbar_wait(smem_u32(&bars[st]), ((kt - STAGES) / STAGES) & 1)) s_fail = 1;
-        }
-        const int k0 = kbeg + kt * BK;
-        stage_tile(a_tile, A, lda, a_kmajor, m0, k0, tid);
-        stage_tile(b_tile, B, ldb, b_kmajor, n0, k0, tid);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // stores -> tensor core
+        cp_async_wait<STAGES - 2>();  // this thread's copies of tile kt have landed
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // -> the tensor core
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();
         if (s_fail) break;
@@ -151,17 +181,28 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm_tc(
             for (int ks = 0; ks < BK / 16; ++ks) {  // 16 k per MMA = two 8-k core columns
                 const uint64_t ad = smem_desc(a_addr + ks * 2 * kLbo, kLbo, kSbo);
                 const uint64_t bd = smem_desc(b_addr + ks * 2 * kLbo, kLbo, kSbo);
-                const uint32_t accumulate = (kt > 0 || ks > 0) ? 1u : 0u;
+                const uint32_t acc = (kt > 0 || ks > 0) ? 1u : 0u;
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
                     "setp.ne.b32 p, %4, 0;\n\t"
                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}"
-                    :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(accumulate), "r"(0u));
+                    :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u));
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                          :: "r"(smem_u32(&bars[st])) : "memory");
         }
+        // refill: tile kt + STAGES - 1 goes to the stage tile kt - 1 used, once
+        // the MMAs that read it are done
+        const int nt = kt + STAGES - 1;
+        if (nt < ktiles) {
+            if (kt >= 1 && !mbar_wait(smem_u32(&bars[(kt - 1) % STAGES]), ((kt - 1) / STAGES) & 1))
+                s_fail = 1;
+            else
+                load_tile(nt);
+        }
+        cp_async_commit();
     }
+    cp_async_wait<0>();
     // the last commit covers every MMA issued before it
     if (!s_fail && ktiles > 0) {
         const int last = ktiles - 1;
@@ -173,6 +214,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm_tc(
     if (!s_fail) {
         // warp w reads TMEM lanes 32 w .. 32 w + 31 (rows), 32 columns at a time
         const int row = m0 + warp * 32 + (tid & 31);
+        const bool direct = gridDim.z == 1;
         float* out = part + ((size_t)split * M + row) * N + n0;
 #pragma unroll 1
         for (int c = 0; c < BN; c += 32) {
@@ -190,11 +232,35 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm_tc(
                   "=r"(r[30]), "=r"(r[31])
                 : "r"(taddr));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (direct) {
+                const int col0 = n0 + c;
 #pragma unroll
-            for (int j = 0; j < 32; j += 4)
-                *reinterpret_cast<float4*>(out + c + j) =
-                    make_float4(__uint_as_float(r[j]), __uint_as_float(r[j + 1]),
-                                __uint_as_float(r[j + 2]), __uint_as_float(r[j + 3]));
+                for (int j = 0; j < 32; j += 4) {
+                    float v[4];
+#pragma unroll
+                    for (int q = 0; q < 4; ++q)
+                        v[q] = __uint_as_float(r[j + q]) + (bias ? bias[col0 + j + q] : 0.0f);
+                    if (C) {
+                        float4* pc = reinterpret_cast<float4*>(C + (size_t)row * ldc + col0 + j);
+                        if (accumulate) {
+                            const float4 o = *pc;
+                            v[0] += o.x; v[1] += o.y; v[2] += o.z; v[3] += o.w;
+                        }
+                        *pc = make_float4(v[0], v[1], v[2], v[3]);
+                    }
+                    if (act) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            act[(size_t)row * ld_act + col0 + j + q] = __float2bfloat16_rn(gelu_tc(v[q]));
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 32; j += 4)
+                    *reinterpret_cast<float4*>(out + c + j) =
+                        make_float4(__uint_as_float(r[j]), __uint_as_float(r[j + 1]),
+                                    __uint_as_float(r[j + 2]), __uint_as_float(r[j + 3]));
+            }
         }
     } else if (tid == 0 && status) {
         atomicExch(status, 1);
@@ -208,11 +274,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_gemm_tc(
 
 }  // namespace tc
 
-__device__ __forceinline__ float gelu_tc(float x) {
-    const float s = 0.7978845608028654f;
-    const float u = s * fmaf(0.044715f * x * x, x, x);
-    return 0.5f * x * (1.0f + tanhf(u));
-}
+using tc::gelu_tc;
 
 // Sum of the split partials in split order, then bias / accumulate / GELU.
 __global__ void k_gemm_tc_reduce(const float* __restrict__ part, int splits, int M, int N,
@@ -242,7 +304,7 @@ extern "C" int qssb_gemm_tc_workspace_bytes(int32_t M, int32_t N, int32_t K, int
                                             size_t* bytes) {
     if (!bytes || M <= 0 || N <= 0 || K <= 0 || splits <= 0)
         return set_error(QSSB_ERR_INVALID, "qssb_gemm_tc_workspace_bytes: invalid sizes");
-    *bytes = sizeof(float) * (size_t)splits * M * N + 256;
+    *bytes = (splits > 1 ? sizeof(float) * (size_t)splits * M * N : 0) + 256;
     return QSSB_OK;
 }
 
@@ -263,6 +325,9 @@ extern "C" int qssb_gemm_bf16_tc(const void* A, int32_t lda, int32_t trans_a, co
         return set_error(QSSB_ERR_INVALID, "qssb_gemm_bf16_tc: leading dimensions");
     if (((uintptr_t)A & 15u) || ((uintptr_t)B & 15u) || ((uintptr_t)workspace & 255u))
         return set_error(QSSB_ERR_INVALID, "qssb_gemm_bf16_tc: A, B 16-byte and workspace 256-byte aligned");
+    if (splits == 1 && C && (((uintptr_t)C & 15u) || (ldc % 4)))
+        return set_error(QSSB_ERR_INVALID,
+                         "qssb_gemm_bf16_tc: without split K, C 16-byte aligned and ldc a multiple of 4");
     size_t need = 0;
     int rc = qssb_gemm_tc_workspace_bytes(M, N, K, splits, &need);
     if (rc) return rc;
@@ -281,7 +346,9 @@ extern "C" int qssb_gemm_bf16_tc(const void* A, int32_t lda, int32_t trans_a, co
     const int kps = K / splits;
     auto launch = [&](auto kern) -> int {
         CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-        kern<<<grid, THREADS, SMEM_BYTES, s>>>(a, lda, b, ldb, M, N, kps, part, status);
+        kern<<<grid, THREADS, SMEM_BYTES, s>>>(a, lda, b, ldb, M, N, kps, part, status, bias,
+                                               accumulate, C, ldc,
+                                               static_cast<__nv_bfloat16*>(act_bf16), ld_act);
         CUDA_TRY(cudaGetLastError());
         return QSSB_OK;
     };
@@ -291,6 +358,7 @@ extern "C" int qssb_gemm_bf16_tc(const void* A, int32_t lda, int32_t trans_a, co
         rc = trans_b ? launch(k_gemm_tc<false, true>) : launch(k_gemm_tc<false, false>);
     }
     if (rc) return rc;
+    if (splits == 1) return QSSB_OK;  // the MMA kernel wrote C / act itself
     const long long total = (long long)M * N;
     long long blocks = (total + 255) / 256;
     const long long cap = 8LL * device_sm_count();

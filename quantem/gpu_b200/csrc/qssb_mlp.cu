@@ -118,14 +118,26 @@ __global__ void k_gelu_backward(const float* __restrict__ dy, const float* __res
     }
 }
 
-// db[c] = sum over rows of dz[r][c] (fixed order: one thread per column).
-__global__ void k_bias_grad(const float* __restrict__ dz, int rows, int cols,
-                            float* __restrict__ db) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= cols) return;
+// db[c] = sum over rows of dz[r][c]: 32 columns per CTA (one per lane, so a
+// warp reads 128 contiguous bytes of a row), eight warps over interleaved row
+// slices in FP64, folded in warp order (a fixed order).
+constexpr int kBiasWarps = 8;
+__global__ void __launch_bounds__(32 * kBiasWarps) k_bias_grad(const float* __restrict__ dz,
+                                                               int rows, int cols,
+                                                               float* __restrict__ db) {
+    __shared__ double part[kBiasWarps][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int c = blockIdx.x * 32 + lane;
     double s = 0.0;
-    for (int r = 0; r < rows; ++r) s += (double)dz[(size_t)r * cols + c];
-    db[c] = (float)s;
+    if (c < cols)
+        for (int r = w; r < rows; r += kBiasWarps) s += (double)dz[(size_t)r * cols + c];
+    part[w][lane] = s;
+    __syncthreads();
+    if (w == 0 && c < cols) {
+        double t = 0.0;
+        for (int k = 0; k < kBiasWarps; ++k) t += part[k][lane];
+        db[c] = (float)t;
+    }
 }
 
 // MSE over the first n_out of ld columns: loss = mean (y - t)^2 over rows x n_out,
@@ -289,7 +301,7 @@ extern "C" int qssb_gelu_backward(const float* dy, const float* pre, int64_t n, 
 extern "C" int qssb_bias_grad(const float* dz, int32_t rows, int32_t cols, float* db, void* stream) {
     if (!dz || !db || rows <= 0 || cols <= 0)
         return set_error(QSSB_ERR_INVALID, "qssb_bias_grad: null pointer or empty");
-    k_bias_grad<<<(cols + 127) / 128, 128, 0, (cudaStream_t)stream>>>(dz, rows, cols, db);
+    k_bias_grad<<<(cols + 31) / 32, 32 * kBiasWarps, 0, (cudaStream_t)stream>>>(dz, rows, cols, db);
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

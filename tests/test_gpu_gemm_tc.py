@@ -1,7 +1,8 @@
 """The proposer MLP's GEMM on the tcgen05 tensor cores (``qssb_gemm_bf16_tc``)
 against an FP32 product of the same BF16 operands: all four transpose
 combinations, one and several K splits, the bias / accumulate / GELU
-epilogue, and the training step's shapes. BF16 products are exact in FP32;
+epilogue (in the reduce pass with split K, in the MMA kernel without), and
+the training step's shapes. BF16 products are exact in FP32;
 only the summation order differs (FP32 accumulation in the tensor core, the
 splits added in order), hence the 1e-5 relative bound on the largest
 element, and two calls give identical bits."""
@@ -69,6 +70,20 @@ def test_gemm_tc_epilogue_and_training_shapes():
     _gemm_tc(x, True, dz, False, 16384, 512, 256, 1, c=c, accumulate=True)
     ref = c0 + x.float().T @ dz.float()
     assert (c - ref).abs().max().item() <= 1e-5 * ref.abs().max().item() + 1e-6
+    # without split K the MMA kernel applies bias and GELU itself (layer 2's shape)
+    a2 = (0.1 * torch.randn((256, 512), generator=g, device=DEV)).to(torch.bfloat16)
+    w2 = (0.05 * torch.randn((512, 512), generator=g, device=DEV)).to(torch.bfloat16)
+    z2 = torch.empty((256, 512), device=DEV)
+    act2 = torch.empty((256, 512), dtype=torch.bfloat16, device=DEV)
+    _gemm_tc(a2, False, w2, False, 256, 512, 512, 1, bias=bias, c=z2, act=act2)
+    ref2 = a2.float() @ w2.float() + bias
+    assert (z2 - ref2).abs().max().item() <= 1e-5 * ref2.abs().max().item() + 1e-6
+    gelu2 = 0.5 * ref2 * (1 + torch.tanh(0.7978845608028654 * (ref2 + 0.044715 * ref2 ** 3)))
+    assert (act2.float() - gelu2).abs().max().item() <= 1e-2 * gelu2.abs().max().item()
+    # and the same with only the BF16 activation written
+    act3 = torch.empty_like(act2)
+    _gemm_tc(a2, False, w2, False, 256, 512, 512, 1, bias=bias, act=act3)
+    assert torch.equal(act3, act2)
 
 
 def test_gemm_tc_rejects_unsupported_shapes():
@@ -82,3 +97,9 @@ def test_gemm_tc_rejects_unsupported_shapes():
                                1, 128, 128, 96, 1, None, 0, ctypes.c_void_p(c.data_ptr()), 128, None, 0,
                                ctypes.c_void_p(ws.data_ptr()), ws.numel(), None)
     assert rc == _lib.QSSB_ERR_UNSUPPORTED
+    # without split K, C must take 16-byte stores
+    rc = lib.qssb_gemm_bf16_tc(ctypes.c_void_p(a.data_ptr()), 64, 0, ctypes.c_void_p(a.data_ptr()), 64,
+                               1, 128, 128, 64, 1, None, 0, ctypes.c_void_p(c.data_ptr() + 4), 128,
+                               None, 0, ctypes.c_void_p(ws.data_ptr()), ws.numel(), None)
+    assert rc == _lib.QSSB_ERR_INVALID
+    assert nbytes.value == 256  # no partial tiles without split K
