@@ -523,8 +523,10 @@ def learned_fits(dev: torch.device, n_cases: int = 16) -> dict:
     """Learned proposal + 8-candidate refinement vs the plain 64-candidate sweep.
 
     The proposer is trained here (50k forward-model samples of the 64^2 x 64^2
-    lattice, 40 epochs) with the library's own kernels (its large GEMMs on the
-    tcgen05 tensor cores). Each case is a fully simulated 64^2-scan x
+    lattice, 40 epochs, after a one-epoch warm-up on a throwaway model) with
+    the library's own kernels (its large GEMMs on the tcgen05 tensor cores,
+    each step replayed as one CUDA graph); train_s includes synthesising the
+    samples. Each case is a fully simulated 64^2-scan x
     64^2-detector dataset (padded to 128^2 by the reference rule) with
     aberrations drawn from the sweep ranges at 1e6 e per position:
     ``n_cases`` weak-phase objects (0.03 rad atoms) and ``n_cases // 2`` of
@@ -553,6 +555,9 @@ def learned_fits(dev: torch.device, n_cases: int = 16) -> dict:
     from quantem.gpu_b200 import proposer as pr
     from quantem.gpu_b200.synthetic import SyntheticSpec, draw_aberrations, generate
 
+    # warm-up (module loading, first launches, graph capture) on a throwaway model
+    pr.Proposer(dev, seed=99).train(n_samples=2048, epochs=1)
+    torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     prop = pr.Proposer(dev, seed=0)
     info = prop.train(n_samples=50_000, epochs=40)

@@ -520,6 +520,17 @@ int qssb_mse_heads(const float* y, const float* target, int32_t rows, int32_t n_
 int qssb_adam(float* w, float* m, float* v, const float* grad, int64_t n, float lr, float beta1,
               float beta2, float eps, float weight_decay, int32_t step, void* w_bf16,
               void* stream);
+/* The training schedule on the device, for graph-replayed steps: *step += 1,
+ * then hyper[0..2] = {lr0 (1 + cos(pi (step - 1 - first_step) / total_steps))
+ * / 2, 1 - beta1^step, 1 - beta2^step} (device float[3], device int32 step;
+ * first_step: the step count when this cosine run began). */
+int qssb_adam_schedule(float* hyper, int32_t* step, int32_t first_step, int32_t total_steps,
+                       float lr0, float beta1, float beta2, void* stream);
+/* qssb_adam with the learning rate and bias corrections read from hyper
+ * (device {lr, c1, c2}, as qssb_adam_schedule writes them). */
+int qssb_adam_dev(float* w, float* m, float* v, const float* grad, int64_t n, const float* hyper,
+                  float beta1, float beta2, float eps, float weight_decay, void* w_bf16,
+                  void* stream);
 /* y = BF16(x), n elements. */
 int qssb_to_bf16(const float* x, int64_t n, void* y, void* stream);
 

@@ -148,6 +148,10 @@ SIGNATURES = {
                                       _P, _P, _P, _P]),
     "qssb_adam": (ctypes.c_int, [_P, _P, _P, _P, _I64, ctypes.c_float, ctypes.c_float,
                                  ctypes.c_float, ctypes.c_float, ctypes.c_float, _I32, _P, _P]),
+    "qssb_adam_schedule": (ctypes.c_int, [_P, _P, _I32, _I32, ctypes.c_float, ctypes.c_float,
+                                          ctypes.c_float, _P]),
+    "qssb_adam_dev": (ctypes.c_int, [_P, _P, _P, _P, _I64, _P, ctypes.c_float, ctypes.c_float,
+                                     ctypes.c_float, ctypes.c_float, _P, _P]),
     "qssb_to_bf16": (ctypes.c_int, [_P, _I64, _P, _P]),
     "qssb_loss_batch": (ctypes.c_int, [
         _P, _P, _P, _P, ctypes.POINTER(Calibration), _P, _I32, _I32, _P, _SZ, _P, _P, _P]),

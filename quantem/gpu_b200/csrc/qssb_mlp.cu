@@ -221,10 +221,18 @@ __global__ void __launch_bounds__(256) k_mse_heads(
     if (threadIdx.x == 0 && loss) *loss = (float)(red[0] * scale);
 }
 
-// Adam on FP32 master weights (bias-corrected), then the BF16 copy.
+// Adam on FP32 master weights (bias-corrected), then the BF16 copy. With
+// `hyper` the learning rate and the bias corrections come from the device
+// ({lr, c1, c2}, written by k_adam_schedule) instead of the arguments.
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
                        const float* __restrict__ g, long long n, float lr, float b1, float b2,
-                       float eps, float wd, float c1, float c2, __nv_bfloat16* __restrict__ w_bf) {
+                       float eps, float wd, float c1, float c2, __nv_bfloat16* __restrict__ w_bf,
+                       const float* __restrict__ hyper) {
+    if (hyper) {
+        lr = hyper[0];
+        c1 = hyper[1];
+        c2 = hyper[2];
+    }
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
          i += (long long)gridDim.x * blockDim.x) {
         const float gi = g[i];
@@ -237,6 +245,22 @@ __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __re
         w[i] = wi;
         if (w_bf) w_bf[i] = __float2bfloat16_rn(wi);
     }
+}
+
+// One training step's schedule on the device (for graph-replayed steps):
+// step += 1; hyper = {lr0 (1 + cos(pi (step - 1 - first) / total)) / 2,
+// 1 - beta1^step, 1 - beta2^step} (the cosine schedule of a run that began
+// after step `first`, and Adam's bias corrections, as the host computes them
+// for qssb_adam).
+__global__ void k_adam_schedule(float* __restrict__ hyper, int* __restrict__ step, int first,
+                                int total, float lr0, float beta1, float beta2) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const int t = *step + 1;
+    *step = t;
+    const double frac = (double)(t - 1 - first) / (double)total;
+    hyper[0] = (float)((double)lr0 * 0.5 * (1.0 + cos(3.141592653589793 * frac)));
+    hyper[1] = 1.0f - powf(beta1, (float)t);
+    hyper[2] = 1.0f - powf(beta2, (float)t);
 }
 
 __global__ void k_to_bf16(const float* __restrict__ x, long long n, __nv_bfloat16* __restrict__ y) {
@@ -340,7 +364,31 @@ extern "C" int qssb_adam(float* w, float* m, float* v, const float* grad, int64_
     const float c2 = 1.0f - powf(beta2, (float)step);
     k_adam<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
         w, m, v, grad, n, lr, beta1, beta2, eps, weight_decay, c1, c2,
-        static_cast<__nv_bfloat16*>(w_bf16));
+        static_cast<__nv_bfloat16*>(w_bf16), nullptr);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+extern "C" int qssb_adam_schedule(float* hyper, int32_t* step, int32_t first_step,
+                                  int32_t total_steps, float lr0, float beta1, float beta2,
+                                  void* stream) {
+    if (!hyper || !step || total_steps <= 0 || first_step < 0)
+        return set_error(QSSB_ERR_INVALID,
+                         "qssb_adam_schedule: null pointer, total_steps < 1 or first_step < 0");
+    k_adam_schedule<<<1, 32, 0, (cudaStream_t)stream>>>(hyper, step, first_step, total_steps, lr0,
+                                                         beta1, beta2);
+    CUDA_TRY(cudaGetLastError());
+    return QSSB_OK;
+}
+
+extern "C" int qssb_adam_dev(float* w, float* m, float* v, const float* grad, int64_t n,
+                             const float* hyper, float beta1, float beta2, float eps,
+                             float weight_decay, void* w_bf16, void* stream) {
+    if (!w || !m || !v || !grad || !hyper || n <= 0)
+        return set_error(QSSB_ERR_INVALID, "qssb_adam_dev: null pointer or empty");
+    k_adam<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+        w, m, v, grad, n, 0.0f, beta1, beta2, eps, weight_decay, 1.0f, 1.0f,
+        static_cast<__nv_bfloat16*>(w_bf16), hyper);
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

@@ -64,6 +64,7 @@ N_OUT_PAD = 16             # HEADS x N_OUT
 OUT_SCALE = np.array([200.0, 200.0, 200.0, 1.0e4], dtype=np.float32)
 OUT_WEIGHT = np.array([1.0, 1.0, 1.0, 0.1], dtype=np.float32)  # C3 is barely visible
 WTA_EPS = 0.05             # share of the gradient the losing heads keep
+ADAM_BETAS = (0.9, 0.999)
 
 # the training lattice (64x64 detector)
 TRAIN_VOLTAGE_KV = 300.0
@@ -364,10 +365,13 @@ class MLP:
         self._x = x
         return bf["z"][3]
 
-    def backward_and_step(self, target: torch.Tensor, lr: float, wd: float = 1e-5) -> torch.Tensor:
+    def backward_and_step(self, target: torch.Tensor, lr: float, wd: float = 1e-5,
+                          hyper: torch.Tensor | None = None) -> torch.Tensor:
         """Winner-takes-all MSE of the heads against target [m, N_OUT] (FP32;
         winner by (C1, A1), C3 weighted by OUT_WEIGHT), gradients, one Adam
-        step; returns the loss (device)."""
+        step; returns the loss (device). With ``hyper`` (device {lr, c1, c2}
+        from ``qssb_adam_schedule``) the step takes its learning rate and bias
+        corrections from there, so that it can be replayed from a graph."""
         bf = self._buf(int(target.shape[0]))
         m = int(target.shape[0])
         dev = self.device
@@ -393,10 +397,16 @@ class MLP:
         grads = bf["gw"] + bf["gb"]
         for j, (p, gr) in enumerate(zip(params, grads)):
             wbf = self.w_bf[j] if j < 4 else None
-            _call("qssb_adam", dev, _ptr(p), _ptr(self.m[j]), _ptr(self.v[j]), _ptr(gr), p.numel(),
-                  ctypes.c_float(lr), ctypes.c_float(0.9), ctypes.c_float(0.999),
-                  ctypes.c_float(1e-8), ctypes.c_float(wd if j < 4 else 0.0), self.t, _ptr(wbf),
-                  _stream(dev))
+            if hyper is None:
+                _call("qssb_adam", dev, _ptr(p), _ptr(self.m[j]), _ptr(self.v[j]), _ptr(gr),
+                      p.numel(), ctypes.c_float(lr), ctypes.c_float(ADAM_BETAS[0]),
+                      ctypes.c_float(ADAM_BETAS[1]), ctypes.c_float(1e-8),
+                      ctypes.c_float(wd if j < 4 else 0.0), self.t, _ptr(wbf), _stream(dev))
+            else:
+                _call("qssb_adam_dev", dev, _ptr(p), _ptr(self.m[j]), _ptr(self.v[j]), _ptr(gr),
+                      p.numel(), _ptr(hyper), ctypes.c_float(ADAM_BETAS[0]),
+                      ctypes.c_float(ADAM_BETAS[1]), ctypes.c_float(1e-8),
+                      ctypes.c_float(wd if j < 4 else 0.0), _ptr(wbf), _stream(dev))
         return bf["loss"]
 
     def predict(self, x: torch.Tensor) -> np.ndarray:
@@ -428,27 +438,65 @@ class Proposer:
         return x, t, ab
 
     def train(self, n_samples: int = 50_000, epochs: int = 40, batch: int = 256,
-              lr: float = 1e-3) -> dict:
+              lr: float = 1e-3, use_graph: bool = True) -> dict:
+        """Adam with a cosine learning rate over ``epochs`` shuffled passes.
+
+        Every step gathers its batch through a device index (this epoch's
+        permutation at a device cursor), runs forward, the winner-takes-all
+        loss, backward and the Adam update with the schedule computed on the
+        device (``qssb_adam_schedule``). The first step runs eagerly; the
+        rest replay it as one CUDA graph (``use_graph``), so the ~45 launches
+        of a step cost one host call. The per-epoch losses are read after
+        each epoch's last step."""
         x, t, _ = self.make_data(n_samples, self.seed)
+        dev = self.device
         steps_per_epoch = n_samples // batch
         total = epochs * steps_per_epoch
-        g = torch.Generator(device=self.device).manual_seed(self.seed + 1)
-        step = 0
+        g = torch.Generator(device=dev).manual_seed(self.seed + 1)
+        perm = torch.empty(n_samples, dtype=torch.int64, device=dev)
+        base = torch.arange(batch, dtype=torch.int64, device=dev)
+        pos = torch.empty_like(base)
+        idx = torch.empty_like(base)
+        xb = torch.empty((batch, N_IN), dtype=x.dtype, device=dev)
+        tb = torch.empty((batch, N_OUT), dtype=t.dtype, device=dev)
+        hyper = torch.zeros(4, device=dev)
+        step_ctr = torch.zeros(1, dtype=torch.int32, device=dev)
+        mlp = self.mlp
+        t0 = mlp.t
+        step_ctr.fill_(t0)
+
+        def one_step() -> torch.Tensor:
+            torch.index_select(perm, 0, pos, out=idx)
+            torch.index_select(x, 0, idx, out=xb)
+            torch.index_select(t, 0, idx, out=tb)
+            pos.add_(batch)
+            _call("qssb_adam_schedule", dev, _ptr(hyper), _ptr(step_ctr), t0, total,
+                  ctypes.c_float(lr), ctypes.c_float(ADAM_BETAS[0]), ctypes.c_float(ADAM_BETAS[1]),
+                  _stream(dev))
+            mlp.forward(xb)
+            return mlp.backward_and_step(tb, lr, hyper=hyper)
+
+        graph = None
+        loss_t = None
         losses = []
         for _ in range(epochs):
-            perm = torch.randperm(n_samples, generator=g, device=self.device)
-            for s in range(steps_per_epoch):
-                sel = perm[s * batch:(s + 1) * batch]
-                xb = x.index_select(0, sel).contiguous()
-                tb = t.index_select(0, sel).contiguous()
-                self.mlp.forward(xb)
-                cur = lr * 0.5 * (1.0 + math.cos(math.pi * step / total))
-                loss = self.mlp.backward_and_step(tb, cur)
-                step += 1
-                if s == steps_per_epoch - 1:
-                    losses.append(float(loss.item()))
+            perm.copy_(torch.randperm(n_samples, generator=g, device=dev))
+            pos.copy_(base)
+            for _s in range(steps_per_epoch):
+                if graph is not None:
+                    graph.replay()
+                    continue
+                loss_t = one_step()
+                if use_graph:
+                    torch.cuda.synchronize(dev)
+                    graph = torch.cuda.CUDAGraph()
+                    with torch.cuda.graph(graph, capture_error_mode="relaxed"):
+                        loss_t = one_step()
+            losses.append(float(loss_t.item()))
+        mlp.t = int(step_ctr.item())
         self.history = losses
-        return {"epochs": epochs, "steps": step, "final_train_mse": losses[-1] if losses else None}
+        return {"epochs": epochs, "steps": mlp.t - t0, "graph": graph is not None,
+                "final_train_mse": losses[-1] if losses else None}
 
     def validate(self, n: int = 2048, seed: int = 12345) -> dict:
         """Errors of the best head per sample (the head nearest the target in

@@ -140,6 +140,58 @@ def test_mlp_outputs_and_gradients_match_oracle():
             assert rel <= 3e-2, (i, rel)
 
 
+def test_device_schedule_matches_host_adam():
+    """``qssb_adam_schedule`` + ``qssb_adam_dev`` give the update ``qssb_adam``
+    gives with the host's cosine learning rate and bias corrections."""
+    import math
+
+    lib = _lib.load()
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    g = torch.Generator(device=DEV).manual_seed(9)
+    n, total, first, lr = 4096, 50, 3, 1e-3
+    w = torch.randn(n, generator=g, device=DEV)
+    grad = torch.randn(n, generator=g, device=DEV)
+    m0 = 0.1 * torch.randn(n, generator=g, device=DEV)
+    v0 = torch.rand(n, generator=g, device=DEV)
+    hyper = torch.zeros(4, device=DEV)
+    step = torch.full((1,), first + 6, dtype=torch.int32, device=DEV)  # 7th step of the run
+    _lib.check(lib.qssb_adam_schedule(_ptr(hyper), _ptr(step), first, total, ctypes.c_float(lr),
+                                      ctypes.c_float(0.9), ctypes.c_float(0.999), stream))
+    t = first + 7
+    assert int(step.item()) == t
+    want_lr = lr * 0.5 * (1.0 + math.cos(math.pi * (t - 1 - first) / total))
+    h = hyper.cpu().numpy()
+    np.testing.assert_allclose(h[0], want_lr, rtol=1e-6)
+    # 1 - powf(beta, t) in float32, as qssb_adam forms it: the float32 betas,
+    # and a powf error of an ulp or two magnified by the cancellation
+    b1, b2 = float(np.float32(0.9)), float(np.float32(0.999))
+    np.testing.assert_allclose(h[1:3], [1 - b1 ** t, 1 - b2 ** t], rtol=3e-5)
+    w1, m1, v1 = w.clone(), m0.clone(), v0.clone()
+    w2, m2, v2 = w.clone(), m0.clone(), v0.clone()
+    _lib.check(lib.qssb_adam_dev(_ptr(w1), _ptr(m1), _ptr(v1), _ptr(grad), n, _ptr(hyper),
+                                 ctypes.c_float(0.9), ctypes.c_float(0.999), ctypes.c_float(1e-8),
+                                 ctypes.c_float(1e-5), None, stream))
+    _lib.check(lib.qssb_adam(_ptr(w2), _ptr(m2), _ptr(v2), _ptr(grad), n, ctypes.c_float(h[0]),
+                             ctypes.c_float(0.9), ctypes.c_float(0.999), ctypes.c_float(1e-8),
+                             ctypes.c_float(1e-5), t, None, stream))
+    assert torch.equal(m1, m2) and torch.equal(v1, v2)
+    torch.testing.assert_close(w1, w2, rtol=1e-6, atol=1e-9)
+
+
+def test_graph_replayed_training_equals_eager_steps():
+    """Training replayed from the captured step graph gives the same weights,
+    bit for bit, as the same steps launched one by one."""
+    a = pr.Proposer(DEV, seed=4)
+    b = pr.Proposer(DEV, seed=4)
+    ia = a.train(n_samples=2048, epochs=3, use_graph=True)
+    ib = b.train(n_samples=2048, epochs=3, use_graph=False)
+    assert ia["graph"] and not ib["graph"] and ia["steps"] == ib["steps"] == 3 * 8
+    assert a.mlp.t == b.mlp.t == 24
+    for wa, wb in zip(a.mlp.w + a.mlp.b, b.mlp.w + b.mlp.b):
+        assert torch.equal(wa, wb)
+    assert a.history == b.history
+
+
 def test_short_training_cuts_validation_error():
     prop = pr.Proposer(DEV, seed=5)
     before = prop.validate(1024)["rmse_scaled"]
