@@ -37,6 +37,13 @@ extern "C" {
 #define QSSB_FLAG_QUADRATIC 4     /* qssb_loss_batch: every candidate has C30 == 0, so the
                                      factorised quadratic-chi overlap applies (qssb_object
                                      decides this itself from its host-side candidate) */
+/* Tile-shape variant (another tuning knob): bits 8..11 of flags. qssb_object
+ * on the quadratic-chi path: 1 = 2 adjacent frequencies per thread, 2 or 0
+ * (the default) = 4, 3 = 8. Results agree to float32 rounding across
+ * variants; each variant repeats its own bits. */
+#define QSSB_FLAG_VARIANT_SHIFT 8
+#define QSSB_FLAG_VARIANT(v) ((int32_t)(v) << QSSB_FLAG_VARIANT_SHIFT)
+#define QSSB_FLAG_VARIANT_MAX 15
 /* Work partition (the tuning knob of an autotuner): bits 16..30 of flags hold
  * the number of BF chunks - per candidate for qssb_loss_batch, in total for
  * qssb_object. 0 keeps the built-in plan. Any value gives the same result up
@@ -157,6 +164,14 @@ int qssb_bf_geometry(const int32_t* bf_linear, const qssb_bf_info_t* info, int32
 int qssb_gather_bf_columns_2d(const uint16_t* counts, int64_t n_frames, int32_t det_rows,
                               int32_t det_cols, const int32_t* bf_linear, int32_t n_bf,
                               uint16_t* columns, void* stream);
+/* The same with the tile shape named (the autotuner's knob; every variant
+ * copies the same bits): 0 = the built-in rule above; bounding-box tiles of
+ * (frames x band pixels) 1 = 32 x 768, 2 = 16 x 1536, 3 = 64 x 384,
+ * 4 = 8 x 3072; 64-frame pixel-major tiles of 5 = 320 and 6 = 704 band pixels
+ * (5 and 6 need n_frames % 8 == 0, else the built-in rule applies). */
+int qssb_gather_bf_columns_2d_ex(const uint16_t* counts, int64_t n_frames, int32_t det_rows,
+                                 int32_t det_cols, const int32_t* bf_linear, int32_t n_bf,
+                                 uint16_t* columns, int32_t variant, void* stream);
 
 /* Largest count of a whole loaded block of n u8 (elem_bytes 1) or u16
  * (elem_bytes 2) detector counts, written to the device word *max_out (set
@@ -183,6 +198,16 @@ int qssb_export_bf_columns(const void* counts, int32_t in_bytes, int64_t n_scan,
  * g_half: complex64 [n_bf][R0][R1/2+1]. */
 int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t scan_rows,
                        int32_t scan_cols, float* g_half, void* stream);
+/* The same with the launch shape named (the autotuner's knob; every variant
+ * gives the same bits): 0 = built-in, 1 .. qssb_scan_fft_variants(scan_rows).
+ * 128: persistent CTAs per SM, 1 = two (built-in), 2 = one. 256 / 512 / 1024:
+ * the column pass's (columns per strip = warps per CTA, CTAs per SM) -
+ * 256: 1 = (8, 3) built-in, 2 = (16, 1), 3 = (8, 2), 4 = (16, 2);
+ * 512: 1 = (16, 1) built-in, 2 = (8, 1), 3 = (8, 2); 1024: 1 = (8, 1)
+ * built-in, 2 = (4, 2). 64: one shape. */
+int qssb_scan_fft_half_ex(const uint16_t* columns, int32_t n_bf, int32_t scan_rows,
+                          int32_t scan_cols, float* g_half, int32_t variant, void* stream);
+int qssb_scan_fft_variants(int32_t scan_rows, int32_t* count);
 
 /* The BF columns written by the frame-sum pass (no counterpart as one step in
  * the reference, whose _extract_gqk gathers after the selection,

@@ -24,6 +24,10 @@ QSSB_FLAG_QUADRATIC = 4
 QSSB_NOALLOC_SCRATCH_BYTES = 16 << 20
 QSSB_FLAG_CHUNKS_SHIFT = 16
 QSSB_FLAG_CHUNKS_MAX = 32767
+QSSB_FLAG_VARIANT_SHIFT = 8
+QSSB_FLAG_VARIANT_MAX = 15
+GATHER_VARIANTS = 6  # qssb_gather_bf_columns_2d_ex: 1..6 (0 = built-in rule)
+OBJECT_VARIANTS = 3  # QSSB_FLAG_VARIANT on qssb_object: 1..3 (0 = built-in)
 
 
 def flag_chunks(n: int) -> int:
@@ -31,6 +35,13 @@ def flag_chunks(n: int) -> int:
     if not 0 <= int(n) <= QSSB_FLAG_CHUNKS_MAX:
         raise ValueError(f"chunk count must be in [0, {QSSB_FLAG_CHUNKS_MAX}]")
     return int(n) << QSSB_FLAG_CHUNKS_SHIFT
+
+
+def flag_variant(v: int) -> int:
+    """``QSSB_FLAG_VARIANT(v)``: the tile-shape knob (0 = built-in shape)."""
+    if not 0 <= int(v) <= QSSB_FLAG_VARIANT_MAX:
+        raise ValueError(f"variant must be in [0, {QSSB_FLAG_VARIANT_MAX}]")
+    return int(v) << QSSB_FLAG_VARIANT_SHIFT
 
 
 class Calibration(ctypes.Structure):
@@ -111,11 +122,14 @@ SIGNATURES = {
     "qssb_mean_dp_u64": (ctypes.c_int, [_P, _I64, _I32, _P, _P, _P]),
     "qssb_gather_bf_columns": (ctypes.c_int, [_P, _I64, _I32, _P, _I32, _P, _P]),
     "qssb_gather_bf_columns_2d": (ctypes.c_int, [_P, _I64, _I32, _I32, _P, _I32, _P, _P]),
+    "qssb_gather_bf_columns_2d_ex": (ctypes.c_int, [_P, _I64, _I32, _I32, _P, _I32, _P, _I32, _P]),
     "qssb_select_bf": (ctypes.c_int, [_P, _I32, _I32, _I64, ctypes.c_float, ctypes.c_float,
                                       _P, _P, _P, _P]),
     "qssb_bf_geometry": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, ctypes.POINTER(GeometryParams),
                                         _P, _P]),
     "qssb_scan_fft_half": (ctypes.c_int, [_P, _I32, _I32, _I32, _P, _P]),
+    "qssb_scan_fft_half_ex": (ctypes.c_int, [_P, _I32, _I32, _I32, _P, _I32, _P]),
+    "qssb_scan_fft_variants": (ctypes.c_int, [_I32, _P]),
     "qssb_count_max": (ctypes.c_int, [_P, _I32, _I64, _P, _P]),
     "qssb_bf_box_estimate": (ctypes.c_int, [_P, _I32, _I32, ctypes.c_float, _I32, _I64, _P, _P]),
     "qssb_mean_dp_u64_box": (ctypes.c_int, [_P, _I64, _I32, _I32, _P, _P, _I64, _P, _P]),

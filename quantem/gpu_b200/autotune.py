@@ -1,16 +1,23 @@
-"""Autotuner for the work partition of the SSB kernels.
+"""Autotuner for the work partition and tile shapes of the SSB kernels.
 
 The loss kernel's CTAs each own one (candidate, BF chunk); with one CTA per
 SM resident, the number of chunks per candidate decides how many waves the
 batch takes and how full the last one is. The trotter kernel's BF chunk count
-trades grid size against the cost of folding the partial sums. Both are set
-through ``QSSB_FLAG_CHUNKS`` (bits 16..30 of the flags). The tuner times a
-small set of candidate partitions with CUDA events on the real inputs, keeps
-the fastest and caches it per (device, kind, scan size, BF count, batch size,
-chi path) in memory and in a JSON file (``$QSSB_TUNING_CACHE``, default
-``~/.cache/quantem_gpu_b200/tuning.json``) so later processes skip the search.
-A cached partition gives identical bits on every call; different partitions
-differ only in float32 summation order.
+trades grid size against the cost of folding the partial sums, and its tile
+shape (2, 4 or 8 adjacent frequencies per thread) trades registers against
+one sincos per tile. Both go through the flags (``QSSB_FLAG_CHUNKS``, bits
+16..30; ``QSSB_FLAG_VARIANT``, bits 8..11). The BF gather's tile shape
+(frames x band pixels, bounding-box or pixel-major tiles) and the scan FFT's
+launch shape (persistent CTAs per SM; at 256^2 and up the column pass's
+strip width and CTAs per SM) are named by the ``_ex`` entry points'
+``variant`` argument; every gather and FFT variant gives the same bits.
+
+The tuner times a small set of candidates with CUDA events on the real
+inputs, keeps the fastest and caches it per (device, kind, shape) in memory
+and in a JSON file (``$QSSB_TUNING_CACHE``, default
+``~/.cache/quantem_gpu_b200/tuning.json``) so later processes skip the
+search. A cached choice gives identical bits on every call; different
+partitions or trotter tiles differ only in float32 rounding.
 """
 from __future__ import annotations
 
@@ -112,25 +119,81 @@ def tune_loss(g_half, bf_geom, q_row, q_col, cal, candidates: torch.Tensor, flag
     return best
 
 
-def cached_object(device: torch.device, scan_rows: int, n_bf: int, flags: int) -> int:
-    """The cached object partition for this shape, or 0 (built-in plan); no search."""
-    return _cache().get(_key("object", device, int(scan_rows), int(n_bf), flags & 0xFFFF), 0)
+def _object_key(device, scan_rows: int, n_bf: int, flags: int, quadratic: bool) -> str:
+    return _key("object", device, int(scan_rows), int(n_bf), flags & 0xFF, int(quadratic))
+
+
+def cached_object(device: torch.device, scan_rows: int, n_bf: int, flags: int,
+                  quadratic: bool = True) -> int:
+    """The cached object tuning for this shape as flag bits (QSSB_FLAG_CHUNKS |
+    QSSB_FLAG_VARIANT), or 0 (built-in plan and tile); no search."""
+    return _cache().get(_object_key(device, scan_rows, n_bf, flags, quadratic), 0)
+
+
+def object_options(scan_rows: int, n_bf: int, quadratic: bool) -> list[tuple[int, int]]:
+    """(total BF chunks, trotter tile variant) pairs the object tuner times:
+    chunk counts around the built-in plan's, each with 2, 4 and 8 frequencies
+    per thread on the quadratic-chi path (variants 1, 0, 3; 0 is the built-in
+    4) and the built-in tile elsewhere."""
+    base = 32 if int(scan_rows) >= 256 else 128
+    chunks = sorted({min(max(1, c), int(n_bf)) for c in (base // 2, base, 3 * base // 2, 2 * base)})
+    variants = (0, 1, 3) if quadratic else (0,)
+    return [(c, v) for c in chunks for v in variants]
 
 
 def tune_object(g_half, bf_geom, q_row, q_col, cal, ab, flags: int, workspace: ops.Workspace,
                 reps: int = 3) -> int:
-    """Best total BF chunk count for the object (trotter) kernel (cached)."""
+    """Best (BF chunk count, trotter tile) for the object kernels, as flag bits
+    to OR into ``flags`` (cached). ``ab`` decides the path: C30 == 0 is the
+    quadratic-chi path that has tile variants."""
     dev = g_half.device
-    key = _key("object", dev, int(cal.scan_rows), int(cal.n_bf), flags & 0xFFFF)
+    quadratic = float(ab.C30) == 0.0
+    key = _object_key(dev, int(cal.scan_rows), int(cal.n_bf), flags, quadratic)
     hit = _cache().get(key)
     if hit is not None:
         return hit
-    base = 32 if int(cal.scan_rows) >= 256 else 128
     timings = {}
-    for c in sorted({max(1, base // 2), base, 3 * base // 2, 2 * base}):
-        f = flags | _lib.flag_chunks(min(c, int(cal.n_bf)))
-        timings[c] = _time_ms(lambda: ops.object_wave(g_half, bf_geom, q_row, q_col, cal, ab,
-                                                      flags=f, workspace=workspace), dev, reps)
+    for c, v in object_options(int(cal.scan_rows), int(cal.n_bf), quadratic):
+        bits = _lib.flag_chunks(c) | _lib.flag_variant(v)
+        f = flags | bits
+        timings[bits] = _time_ms(lambda: ops.object_wave(g_half, bf_geom, q_row, q_col, cal, ab,
+                                                         flags=f, workspace=workspace), dev, reps)
+    best = min(timings, key=timings.get)
+    _store(key, best)
+    return best
+
+
+def tune_gather(counts: torch.Tensor, bf_linear: torch.Tensor, reps: int = 3) -> int:
+    """Best tile shape of the BF gather for this detector, frame count and BF
+    count (``qssb_gather_bf_columns_2d_ex`` variant, cached; 0 = built-in)."""
+    dev = counts.device
+    k0, k1 = int(counts.shape[-2]), int(counts.shape[-1])
+    n_frames = counts.numel() // (k0 * k1)
+    key = _key("gather", dev, k0, k1, n_frames, int(bf_linear.numel()))
+    hit = _cache().get(key)
+    if hit is not None:
+        return hit
+    timings = {}
+    for v in range(_lib.GATHER_VARIANTS + 1):
+        timings[v] = _time_ms(lambda: ops.gather_bf_columns(counts, bf_linear, validate=False,
+                                                            variant=v), dev, reps)
+    best = min(timings, key=timings.get)
+    _store(key, best)
+    return best
+
+
+def tune_scan_fft(columns: torch.Tensor, scan_shape: tuple[int, int], reps: int = 3) -> int:
+    """Best launch shape of the scan FFT for this scan size and BF count
+    (``qssb_scan_fft_half_ex`` variant, cached; 0 = built-in)."""
+    dev = columns.device
+    r0 = int(scan_shape[0])
+    key = _key("scan_fft", dev, r0, int(scan_shape[1]), int(columns.shape[0]))
+    hit = _cache().get(key)
+    if hit is not None:
+        return hit
+    timings = {}
+    for v in range(ops.scan_fft_variants(r0) + 1):
+        timings[v] = _time_ms(lambda: ops.scan_fft_half(columns, scan_shape, variant=v), dev, reps)
     best = min(timings, key=timings.get)
     _store(key, best)
     return best

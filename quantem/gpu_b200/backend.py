@@ -31,7 +31,7 @@ from typing import Literal
 import numpy as np
 import torch
 
-from . import autotune, ops
+from . import _lib, autotune, ops
 from ._lib import (
     FULL_TERM_NAMES,
     FULL_TERMS,
@@ -40,7 +40,6 @@ from ._lib import (
     QSSB_FLAG_QUADRATIC,
     Aberrations,
     Calibration,
-    flag_chunks,
 )
 from .calibration import (
     BFGeometry,
@@ -335,20 +334,21 @@ class B200SSBBackend:
     def _geometry(self, value) -> None:
         self._geometry_host = value
 
-    def _object_flags(self) -> int:
+    def _object_flags(self, quadratic: bool = True) -> int:
         """Flags of the object kernels: the session's, plus the autotuned work
-        partition when one is cached for this scan size and BF count."""
-        chunks = autotune.cached_object(self.device, self._scan_shape[0], int(self.G_qk.shape[0]),
-                                        self._flags)
-        return self._flags | flag_chunks(chunks)
+        partition and trotter tile when cached for this scan size and BF count."""
+        return self._flags | autotune.cached_object(self.device, self._scan_shape[0],
+                                                    int(self.G_qk.shape[0]), self._flags, quadratic)
 
     def autotune(self) -> dict:
-        """Time the object kernels' work partitions on this dataset and cache the
-        fastest for every later session with the same scan size and BF count."""
-        c = autotune.tune_object(self.G_qk, self._geom_dev, self._q_row, self._q_col,
-                                 self._calibration(), Aberrations(0.0, 0.0, 0.0, 0.0), self._flags,
-                                 self._workspace)
-        return {"object_chunks": c}
+        """Time the object kernels' work partitions and trotter tiles on this
+        dataset and cache the fastest for every later session with the same
+        scan size and BF count."""
+        bits = autotune.tune_object(self.G_qk, self._geom_dev, self._q_row, self._q_col,
+                                    self._calibration(), Aberrations(0.0, 0.0, 0.0, 0.0),
+                                    self._flags, self._workspace)
+        return {"object_chunks": (bits >> _lib.QSSB_FLAG_CHUNKS_SHIFT) & _lib.QSSB_FLAG_CHUNKS_MAX,
+                "object_tile_variant": (bits >> _lib.QSSB_FLAG_VARIANT_SHIFT) & _lib.QSSB_FLAG_VARIANT_MAX}
 
     def _calibration(self) -> Calibration:
         return Calibration(
@@ -414,7 +414,7 @@ class B200SSBBackend:
             self.cache_rotation(rotation_angle_rad)
         obj, _ = ops.object_wave(self.G_qk, self._geom_dev, self._q_row, self._q_col,
                                  self._calibration(), Aberrations(C10, C12, phi12, C30),
-                                 flags=self._object_flags(), workspace=self._workspace,
+                                 flags=self._object_flags(C30 == 0.0), workspace=self._workspace,
                                  want_phase=False)
         return obj
 
@@ -423,7 +423,7 @@ class B200SSBBackend:
         """Object wave and its float32 phase from one launch sequence."""
         return ops.object_wave(self.G_qk, self._geom_dev, self._q_row, self._q_col,
                                self._calibration(), Aberrations(C10, C12, phi12, C30),
-                               flags=self._object_flags(), workspace=self._workspace)
+                               flags=self._object_flags(C30 == 0.0), workspace=self._workspace)
 
     # the 128x128 loss evaluates the candidate-independent overlap apertures
     # once per geometry (qssb_overlap_table) instead of once per candidate

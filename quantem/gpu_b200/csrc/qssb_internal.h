@@ -19,6 +19,10 @@ Probe make_probe(const qssb_calibration_t& cal, const qssb_aberrations_t& ab);
 // Validates a calibration; returns QSSB_OK or an error code (message set).
 int validate_calibration(const qssb_calibration_t* cal, const char* who);
 // Requested chunk count carried in flags (QSSB_FLAG_CHUNKS); 0 = built-in plan.
+inline int flag_variant(int32_t flags) {
+    return (int)((flags >> QSSB_FLAG_VARIANT_SHIFT) & QSSB_FLAG_VARIANT_MAX);
+}
+
 inline int flag_chunks(int32_t flags) {
     return (int)((flags >> QSSB_FLAG_CHUNKS_SHIFT) & QSSB_FLAG_CHUNKS_MAX);
 }

@@ -126,10 +126,11 @@ __global__ void __launch_bounds__(kTrotterThreads) k_trotter_partial(
     partial[(size_t)chunk * NQ + qi] = make_float2(sr, si);
 }
 
-// The C10/C12 (quadratic chi, FP32) path with four adjacent frequencies per
-// thread. theta = 2 q^T M k is linear in q, so along a row of the stored half
-// plane e^{i theta} advances by the per-BF factor w = e^{i 2 dq v}: one sincos
-// per four overlap evaluations. Threads t < N * N/8 take (r, 4j .. 4j+3) of
+// The C10/C12 (quadratic chi, FP32) path with Q adjacent frequencies per
+// thread (the tile shape the autotuner picks: 2, 4 - the default - or 8).
+// theta = 2 q^T M k is linear in q, so along a row of the stored half plane
+// e^{i theta} advances by the per-BF factor w = e^{i 2 dq v}: one sincos per Q
+// overlap evaluations. Threads t < N * N/(2Q) take (r, Qj .. Qj+Q-1) of
 // columns 0..N/2-1; the rest take column N/2 of every row and the Nyquist
 // row's columns N/2+1..N-1 one at a time. The partial layout is the same as
 // k_trotter_partial's.
@@ -138,14 +139,15 @@ struct BFRow {
     float4 b;  // A(k), w.x, w.y, unused
 };
 
-template <int N>
+template <int N, int Q = 4>
 __global__ void __launch_bounds__(kTrotterThreads) k_trotter_quad4(
     const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
     const float* __restrict__ q_row, const float* __restrict__ q_col, Probe p, int bf_per_chunk,
     float2* __restrict__ partial) {
+    static_assert(Q == 2 || Q == 4 || Q == 8, "2, 4 or 8 frequencies per thread");
     constexpr int H = N / 2 + 1;
     constexpr int NQ = n_eval_q<N, true>();
-    constexpr int GPR = N / 8;   // groups of four per row
+    constexpr int GPR = N / (2 * Q);  // groups of Q per row
     constexpr int NG = N * GPR;
     constexpr int NT = N + N / 2 - 1;
     __shared__ BFRow s_bf[kMaxBfChunk];
@@ -172,28 +174,28 @@ __global__ void __launch_bounds__(kTrotterThreads) k_trotter_quad4(
     const int t = blockIdx.x * kTrotterThreads + tid;
     if (t < NG) {
         const int r = t / GPR;
-        const int c0 = 4 * (t - r * GPR);
+        const int c0 = Q * (t - r * GPR);
         const float qx = __ldg(q_row + r);
-        float qy[4];
-        float2 eq[4];
+        float qy[Q];
+        float2 eq[Q];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < Q; ++j) {
             qy[j] = __ldg(q_col + c0 + j);
             eq[j] = eq_value(r, c0 + j, p);
         }
         const float2* gp = g + (size_t)b0 * N * H + r * H + c0;
-        float4 acc[4];
-        float2 gc[4];
+        float4 acc[Q];
+        float2 gc[Q];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
+        for (int j = 0; j < Q; ++j) {
             acc[j] = make_float4(0.f, 0.f, 0.f, 0.f);
             gc[j] = nb > 0 ? __ldg(gp + j) : make_float2(0.f, 0.f);
         }
         for (int i = 0; i < nb; ++i) {
-            float2 gn[4];
+            float2 gn[Q];
             const bool more = i + 1 < nb;
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
+            for (int j = 0; j < Q; ++j)
                 gn[j] = more ? __ldg(gp + (size_t)(i + 1) * N * H + j) : make_float2(0.f, 0.f);
             const float4 a = s_bf[i].a;
             const float4 bb = s_bf[i].b;
@@ -202,18 +204,18 @@ __global__ void __launch_bounds__(kTrotterThreads) k_trotter_quad4(
             float2 e = make_float2(ct, st);
             const float2 w = make_float2(bb.y, bb.z);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
+            for (int j = 0; j < Q; ++j) {
                 const float2 v = corrected_quad_e(qx, qy[j], r, c0 + j, eq[j], a.x, a.y, bb.x,
                                                   &s_lo[i], e, gc[j], p);
                 kahan_add(acc[j], v);
-                if (j < 3) e = cmul(e, w);
+                if (j < Q - 1) e = cmul(e, w);
             }
 #pragma unroll
-            for (int j = 0; j < 4; ++j) gc[j] = gn[j];
+            for (int j = 0; j < Q; ++j) gc[j] = gn[j];
         }
         float2* out = partial + (size_t)chunk * NQ + r * H + c0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) out[j] = make_float2(acc[j].x, acc[j].y);
+        for (int j = 0; j < Q; ++j) out[j] = make_float2(acc[j].x, acc[j].y);
     } else if (t < NG + NT) {
         const int tt = t - NG;
         int r, c, gr, gcol, qi;
@@ -242,9 +244,9 @@ __global__ void __launch_bounds__(kTrotterThreads) k_trotter_quad4(
     }
 }
 
-template <int N>
+template <int N, int Q = 4>
 __host__ __device__ constexpr int quad4_threads() {
-    return N * (N / 8) + N + N / 2 - 1;
+    return N * (N / (2 * Q)) + N + N / 2 - 1;
 }
 
 // Full N x N corrected-mean plane from the chunk partials. A block takes 32
@@ -399,19 +401,32 @@ int validate_calibration(const qssb_calibration_t* cal, const char* who) {
     return QSSB_OK;
 }
 
+template <int N, int Q>
+static void launch_quad(const float* g_half, const float* geom, const float* q_row,
+                        const float* q_col, const qssb_calibration_t& cal, const Probe& p,
+                        const ObjectPlan& pl, float2* partial, cudaStream_t s) {
+    const dim3 grid((quad4_threads<N, Q>() + kTrotterThreads - 1) / kTrotterThreads, pl.n_chunks);
+    k_trotter_quad4<N, Q><<<grid, kTrotterThreads, 0, s>>>(
+        reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, p, pl.bf_per_chunk,
+        partial);
+}
+
 template <int N, bool SYM, bool CHI64, bool QUAD>
 static int launch_object(const float* g_half, const float* geom, const float* q_row,
                          const float* q_col, const qssb_calibration_t& cal, const Probe& p,
-                         int chunks, const double* dc_dev, char* ws, float* object, float* phase,
-                         cudaStream_t s) {
+                         int chunks, int variant, const double* dc_dev, char* ws, float* object,
+                         float* phase, cudaStream_t s) {
     const ObjectPlan pl = plan_object(N, cal.n_bf, SYM, chunks);
     float2* partial = reinterpret_cast<float2*>(ws);
     float2* plane = reinterpret_cast<float2*>(ws + pl.partial_bytes);
     if constexpr (SYM && QUAD && !CHI64) {
-        const dim3 grid((quad4_threads<N>() + kTrotterThreads - 1) / kTrotterThreads, pl.n_chunks);
-        k_trotter_quad4<N><<<grid, kTrotterThreads, 0, s>>>(
-            reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, p,
-            pl.bf_per_chunk, partial);
+        // tile shape: variant 1 -> 2 frequencies per thread, 3 -> 8, else 4
+        if (variant == 1)
+            launch_quad<N, 2>(g_half, geom, q_row, q_col, cal, p, pl, partial, s);
+        else if (variant == 3)
+            launch_quad<N, 8>(g_half, geom, q_row, q_col, cal, p, pl, partial, s);
+        else
+            launch_quad<N, 4>(g_half, geom, q_row, q_col, cal, p, pl, partial, s);
     } else {
         const dim3 grid((pl.n_q + kTrotterThreads - 1) / kTrotterThreads, pl.n_chunks);
         k_trotter_partial<N, SYM, CHI64, QUAD><<<grid, kTrotterThreads, 0, s>>>(
@@ -434,24 +449,24 @@ static int launch_object(const float* g_half, const float* geom, const float* q_
 template <int N, bool QUAD>
 static int dispatch_object_q(bool sym, bool chi64, const float* g_half, const float* geom,
                              const float* q_row, const float* q_col, const qssb_calibration_t& cal,
-                             const Probe& p, int chunks, const double* dc_dev, char* ws,
-                             float* object, float* phase, cudaStream_t s) {
+                             const Probe& p, int chunks, int variant, const double* dc_dev,
+                             char* ws, float* object, float* phase, cudaStream_t s) {
     if (sym) {
-        return chi64 ? launch_object<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, dc_dev, ws, object, phase, s)
-                     : launch_object<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, dc_dev, ws, object, phase, s);
+        return chi64 ? launch_object<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, variant, dc_dev, ws, object, phase, s)
+                     : launch_object<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, variant, dc_dev, ws, object, phase, s);
     }
-    return chi64 ? launch_object<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, dc_dev, ws, object, phase, s)
-                 : launch_object<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, dc_dev, ws, object, phase, s);
+    return chi64 ? launch_object<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, variant, dc_dev, ws, object, phase, s)
+                 : launch_object<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, p, chunks, variant, dc_dev, ws, object, phase, s);
 }
 
 template <int N>
 static int dispatch_object(bool sym, bool chi64, const float* g_half, const float* geom,
                            const float* q_row, const float* q_col, const qssb_calibration_t& cal,
-                           const Probe& p, int chunks, const double* dc_dev, char* ws,
+                           const Probe& p, int chunks, int variant, const double* dc_dev, char* ws,
                            float* object, float* phase, cudaStream_t s) {
     if (p.quadratic)
-        return dispatch_object_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, p, chunks, dc_dev, ws, object, phase, s);
-    return dispatch_object_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, p, chunks, dc_dev, ws, object, phase, s);
+        return dispatch_object_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, p, chunks, variant, dc_dev, ws, object, phase, s);
+    return dispatch_object_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, p, chunks, variant, dc_dev, ws, object, phase, s);
 }
 
 }  // namespace qssb
@@ -499,11 +514,11 @@ extern "C" int qssb_object_ex(const float* g_half, const float* bf_geom, const f
     cudaStream_t s = (cudaStream_t)stream;
     char* ws = static_cast<char*>(workspace);
     switch (cal->scan_rows) {
-        case 64: return dispatch_object<64>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
-        case 128: return dispatch_object<128>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
-        case 256: return dispatch_object<256>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
-        case 512: return dispatch_object<512>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
-        case 1024: return dispatch_object<1024>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, dc_dev, ws, object, phase, s);
+        case 64: return dispatch_object<64>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, flag_variant(flags), dc_dev, ws, object, phase, s);
+        case 128: return dispatch_object<128>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, flag_variant(flags), dc_dev, ws, object, phase, s);
+        case 256: return dispatch_object<256>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, flag_variant(flags), dc_dev, ws, object, phase, s);
+        case 512: return dispatch_object<512>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, flag_variant(flags), dc_dev, ws, object, phase, s);
+        case 1024: return dispatch_object<1024>(sym, chi64, g_half, bf_geom, q_row, q_col, *cal, p, chunks, flag_variant(flags), dc_dev, ws, object, phase, s);
         default: return set_error(QSSB_ERR_UNSUPPORTED,
                                   "qssb_object: scan size must be 64, 128, 256, 512 or 1024");
     }

@@ -777,21 +777,45 @@ static int launch_gather_bbox(const uint16_t* counts, int64_t n_frames, int det_
     return QSSB_OK;
 }
 
-extern "C" int qssb_gather_bf_columns_2d(const uint16_t* counts, int64_t n_frames,
-                                         int32_t det_rows, int32_t det_cols,
-                                         const int32_t* bf_linear, int32_t n_bf,
-                                         uint16_t* columns, void* stream) {
+// Tile shapes the autotuner may pick (qssb_gather_bf_columns_2d_ex); all
+// copy the same bits.
+using GbF16 = GbShape<16, 1536>;
+using GbF64 = GbShape<64, 384>;
+constexpr int kGatherVariants = 7;
+
+extern "C" int qssb_gather_bf_columns_2d_ex(const uint16_t* counts, int64_t n_frames,
+                                            int32_t det_rows, int32_t det_cols,
+                                            const int32_t* bf_linear, int32_t n_bf,
+                                            uint16_t* columns, int32_t variant, void* stream) {
     if (!counts || !bf_linear || !columns || n_frames <= 0 || det_rows <= 0 || det_cols <= 0 ||
         n_bf <= 0)
         return set_error(QSSB_ERR_INVALID, "qssb_gather_bf_columns_2d: null pointer or empty shape");
     if ((int64_t)det_rows * det_cols > 0x7fffffff)
         return set_error(QSSB_ERR_INVALID, "qssb_gather_bf_columns_2d: detector too large");
+    if (variant < 0 || variant >= kGatherVariants)
+        return set_error(QSSB_ERR_INVALID, "qssb_gather_bf_columns_2d_ex: unknown variant");
     const bool vec_ok = (det_cols % 8) == 0 && ((uintptr_t)counts & 15u) == 0 &&
                         ((uintptr_t)columns & 15u) == 0;
     if (!vec_ok)  // rows not 16-byte aligned: the tile gather
         return qssb_gather_bf_columns(counts, n_frames, det_rows * det_cols, bf_linear, n_bf,
                                       columns, stream);
-    if ((n_frames & 7) == 0 && (int64_t)n_frames * n_bf * 2 > ((int64_t)64 << 20)) {
+    cudaStream_t st = (cudaStream_t)stream;
+    const bool t64_ok = (n_frames & 7) == 0;
+    switch (variant) {
+        case 1: return launch_gather_bbox<GbNarrow>(counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns, st);
+        case 2: return launch_gather_bbox<GbF16>(counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns, st);
+        case 3: return launch_gather_bbox<GbF64>(counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns, st);
+        case 4: return launch_gather_bbox<GbWide>(counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns, st);
+        case 5:
+            if (t64_ok) return launch_gather_t64<320, 4>(counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns, st);
+            break;
+        case 6:
+            if (t64_ok) return launch_gather_t64<704, 2>(counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns, st);
+            break;
+        default:
+            break;
+    }
+    if (t64_ok && (int64_t)n_frames * n_bf * 2 > ((int64_t)64 << 20)) {
         // output larger than L2 can merge: full 128-byte column lines
         if (det_cols <= kT64SmallCols)
             return launch_gather_t64<320, 4>(counts, n_frames, det_rows, det_cols, bf_linear, n_bf,
@@ -804,6 +828,14 @@ extern "C" int qssb_gather_bf_columns_2d(const uint16_t* counts, int64_t n_frame
                                             columns, (cudaStream_t)stream);
     return launch_gather_bbox<GbWide>(counts, n_frames, det_rows, det_cols, bf_linear, n_bf,
                                       columns, (cudaStream_t)stream);
+}
+
+extern "C" int qssb_gather_bf_columns_2d(const uint16_t* counts, int64_t n_frames,
+                                         int32_t det_rows, int32_t det_cols,
+                                         const int32_t* bf_linear, int32_t n_bf,
+                                         uint16_t* columns, void* stream) {
+    return qssb_gather_bf_columns_2d_ex(counts, n_frames, det_rows, det_cols, bf_linear, n_bf,
+                                        columns, 0, stream);
 }
 
 // ------------------------------------------ 256^2 .. 1024^2 scan FFT
@@ -931,12 +963,10 @@ __device__ __forceinline__ void scan_cp_async8(void* smem_dst, const void* gmem_
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(gmem_src) : "memory");
 }
 
-template <int N>
-__global__ void __launch_bounds__(32 * ScanLines<N>::kTileP, ScanLines<N>::kCtasP) k_scan_cols_p(
-    int n_bf, float2* __restrict__ g_half) {
+template <int N, int T = ScanLines<N>::kTileP, int CTAS = ScanLines<N>::kCtasP>
+__global__ void __launch_bounds__(32 * T, CTAS) k_scan_cols_p(int n_bf, float2* __restrict__ g_half) {
     using L = ScanLines<N>;
-    constexpr int P = L::P;
-    constexpr int T = L::kTileP;  // columns per strip, one warp each
+    constexpr int P = L::P;  // T: columns per strip, one warp each; CTAS: CTAs per SM
     constexpr int NT = 32 * T;
     constexpr int H = L::H;
     constexpr int RPL = N / 32;
@@ -993,8 +1023,25 @@ __global__ void __launch_bounds__(32 * ScanLines<N>::kTileP, ScanLines<N>::kCtas
     asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
+template <int N, int T, int CTAS>
+static int launch_scan_cols_p(int n_bf, float2* g, cudaStream_t s) {
+    using L = ScanLines<N>;
+    const size_t smem = sizeof(float2) * ((size_t)2 * T * L::P + N);
+    CUDA_TRY(cudaFuncSetAttribute(k_scan_cols_p<N, T, CTAS>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const long long items = (long long)n_bf * ((L::H + T - 1) / T);
+    const long long slots = (long long)CTAS * device_sm_count();
+    const int grid = (int)(items < slots ? items : slots);
+    k_scan_cols_p<N, T, CTAS><<<grid, 32 * T, smem, s>>>(n_bf, g);
+    return QSSB_OK;
+}
+
+// Column-pass shapes (columns per strip = warps per CTA, CTAs per SM) the
+// autotuner may pick through qssb_scan_fft_half_ex: variant 1 is the
+// built-in choice, 2.. the alternatives; all give the same bits.
 template <int N>
-static int launch_scan_lines(const uint16_t* columns, int n_bf, float* g_half, cudaStream_t s) {
+static int launch_scan_lines(const uint16_t* columns, int n_bf, float* g_half, int variant,
+                             cudaStream_t s) {
     using L = ScanLines<N>;
     auto* g = reinterpret_cast<float2*>(g_half);
     CUDA_TRY(cudaFuncSetAttribute(k_scan_rows<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -1004,17 +1051,29 @@ static int launch_scan_lines(const uint16_t* columns, int n_bf, float* g_half, c
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaFuncSetAttribute(k_scan_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)L::cols_smem));
-    if constexpr (N >= 256) {
-        const size_t smem = sizeof(float2) * ((size_t)2 * L::kTileP * L::P + N);
-        CUDA_TRY(cudaFuncSetAttribute(k_scan_cols_p<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-        const long long items = (long long)n_bf * ((L::H + L::kTileP - 1) / L::kTileP);
-        const long long slots = (long long)L::kCtasP * device_sm_count();
-        const int grid = (int)(items < slots ? items : slots);
-        k_scan_cols_p<N><<<grid, 32 * L::kTileP, smem, s>>>(n_bf, g);
+    int rc = QSSB_OK;
+    if constexpr (N == 256) {
+        switch (variant) {
+            case 2: rc = launch_scan_cols_p<N, 16, 1>(n_bf, g, s); break;
+            case 3: rc = launch_scan_cols_p<N, 8, 2>(n_bf, g, s); break;
+            case 4: rc = launch_scan_cols_p<N, 16, 2>(n_bf, g, s); break;
+            default: rc = launch_scan_cols_p<N, L::kTileP, L::kCtasP>(n_bf, g, s); break;
+        }
+    } else if constexpr (N == 512) {
+        switch (variant) {
+            case 2: rc = launch_scan_cols_p<N, 8, 1>(n_bf, g, s); break;
+            case 3: rc = launch_scan_cols_p<N, 8, 2>(n_bf, g, s); break;
+            default: rc = launch_scan_cols_p<N, L::kTileP, L::kCtasP>(n_bf, g, s); break;
+        }
+    } else if constexpr (N >= 1024) {
+        switch (variant) {
+            case 2: rc = launch_scan_cols_p<N, 4, 2>(n_bf, g, s); break;
+            default: rc = launch_scan_cols_p<N, L::kTileP, L::kCtasP>(n_bf, g, s); break;
+        }
     } else {
         k_scan_cols<N><<<dim3(n_bf, (L::H + L::kTile - 1) / L::kTile), 256, L::cols_smem, s>>>(n_bf, g);
     }
+    if (rc) return rc;
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -1029,10 +1088,29 @@ static int launch_scan_fft(const uint16_t* columns, int n_bf, float* g_half, cud
     return QSSB_OK;
 }
 
-extern "C" int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t scan_rows,
-                                  int32_t scan_cols, float* g_half, void* stream) {
+extern "C" int qssb_scan_fft_variants(int32_t scan_rows, int32_t* count) {
+    if (!count) return set_error(QSSB_ERR_INVALID, "qssb_scan_fft_variants: null output");
+    switch (scan_rows) {
+        case 64: *count = 1; return QSSB_OK;
+        case 128: *count = 2; return QSSB_OK;
+        case 256: *count = 4; return QSSB_OK;
+        case 512: *count = 3; return QSSB_OK;
+        case 1024: *count = 2; return QSSB_OK;
+        default:
+            return set_error(QSSB_ERR_UNSUPPORTED,
+                             "qssb_scan_fft_variants: scan size must be 64, 128, 256, 512 or 1024");
+    }
+}
+
+extern "C" int qssb_scan_fft_half_ex(const uint16_t* columns, int32_t n_bf, int32_t scan_rows,
+                                     int32_t scan_cols, float* g_half, int32_t variant,
+                                     void* stream) {
     if (!columns || !g_half || n_bf <= 0)
         return set_error(QSSB_ERR_INVALID, "qssb_scan_fft_half: null pointer or empty shape");
+    int32_t n_var = 0;
+    if (scan_rows == scan_cols && qssb_scan_fft_variants(scan_rows, &n_var) == QSSB_OK &&
+        (variant < 0 || variant > n_var))
+        return set_error(QSSB_ERR_INVALID, "qssb_scan_fft_half_ex: unknown variant");
     if (scan_rows != scan_cols)
         return set_error(QSSB_ERR_UNSUPPORTED, "qssb_scan_fft_half: square scans only");
     if (((uintptr_t)columns & 15u) != 0)
@@ -1043,23 +1121,29 @@ extern "C" int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t
     switch (scan_rows) {
         case 64: return launch_scan_fft<64>(columns, n_bf, g_half, s);
         case 128: {
+            // persistent CTAs: two per SM (variant 1, the default), or one (variant 2)
             const size_t smem = ScanFft128PSmem::bytes;
             CUDA_TRY(cudaFuncSetAttribute(k_scan_fft128p, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
-            const int slots = 2 * device_sm_count();
+            const int slots = (variant == 2 ? 1 : 2) * device_sm_count();
             const int grid = n_bf < slots ? n_bf : slots;
             k_scan_fft128p<<<grid, 256, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half),
                                                    nullptr, n_bf);
             CUDA_TRY(cudaGetLastError());
             return QSSB_OK;
         }
-        case 256: return launch_scan_lines<256>(columns, n_bf, g_half, s);
-        case 512: return launch_scan_lines<512>(columns, n_bf, g_half, s);
-        case 1024: return launch_scan_lines<1024>(columns, n_bf, g_half, s);
+        case 256: return launch_scan_lines<256>(columns, n_bf, g_half, variant, s);
+        case 512: return launch_scan_lines<512>(columns, n_bf, g_half, variant, s);
+        case 1024: return launch_scan_lines<1024>(columns, n_bf, g_half, variant, s);
         default:
             return set_error(QSSB_ERR_UNSUPPORTED,
                              "qssb_scan_fft_half: scan size must be 64, 128, 256, 512 or 1024");
     }
+}
+
+extern "C" int qssb_scan_fft_half(const uint16_t* columns, int32_t n_bf, int32_t scan_rows,
+                                  int32_t scan_cols, float* g_half, void* stream) {
+    return qssb_scan_fft_half_ex(columns, n_bf, scan_rows, scan_cols, g_half, 0, stream);
 }
 
 extern "C" int qssb_scan_fft_half_mapped(const uint16_t* columns, int64_t n_cols,

@@ -22,7 +22,9 @@ LAUNCHES_PER_CALL = {
     "qssb_bf_geometry": 1,
     "qssb_gather_bf_columns": 1,
     "qssb_gather_bf_columns_2d": 1,
+    "qssb_gather_bf_columns_2d_ex": 1,
     "qssb_scan_fft_half": 1,
+    "qssb_scan_fft_half_ex": 1,
     "qssb_object": 4,
     "qssb_object_ex": 4,
     "qssb_loss_batch": 3,
@@ -307,12 +309,13 @@ def scan_fft_half_mapped(box_cols: torch.Tensor, bf_map: torch.Tensor, n_bf: int
     return g
 
 
-def gather_bf_columns(counts: torch.Tensor, bf_linear: torch.Tensor, validate: bool = True
-                      ) -> torch.Tensor:
+def gather_bf_columns(counts: torch.Tensor, bf_linear: torch.Tensor, validate: bool = True,
+                      variant: int = 0) -> torch.Tensor:
     """columns[b, f] = counts[f, bf_linear[b]] (u16, BF-major).
 
     ``validate`` checks the index range on the device (two host syncs); the
-    backend passes indices it built itself and skips it.
+    backend passes indices it built itself and skips it. ``variant`` names
+    the tile shape (``qssb_gather_bf_columns_2d_ex``; 0 = built-in rule).
     """
     _require_cuda(counts, "counts", torch.uint16)
     _require_cuda(bf_linear, "bf_linear", torch.int32)
@@ -322,8 +325,8 @@ def gather_bf_columns(counts: torch.Tensor, bf_linear: torch.Tensor, validate: b
     if validate and n_bf and (int(bf_linear.min()) < 0 or int(bf_linear.max()) >= k0 * k1):
         raise ValueError("bf_linear indices must lie in [0, K0*K1)")
     out = torch.empty((n_bf, n_frames), dtype=torch.uint16, device=counts.device)
-    _call("qssb_gather_bf_columns_2d", counts.device, _ptr(counts), n_frames, k0, k1,
-          _ptr(bf_linear), n_bf, _ptr(out), _stream(counts))
+    _call("qssb_gather_bf_columns_2d_ex", counts.device, _ptr(counts), n_frames, k0, k1,
+          _ptr(bf_linear), n_bf, _ptr(out), int(variant), _stream(counts))
     return out
 
 
@@ -364,16 +367,26 @@ def export_bf_columns(counts: torch.Tensor, bf_linear: torch.Tensor, out: torch.
           n_scan, det, _ptr(bf_linear), n_bf, _ptr(out), _COUNT_BYTES[out.dtype], _stream(counts))
 
 
-def scan_fft_half(columns: torch.Tensor, scan_shape: tuple[int, int]) -> torch.Tensor:
-    """Hermitian half-plane scan spectra G[b, r, c], c in [0, R1/2] (complex64)."""
+def scan_fft_variants(scan_rows: int) -> int:
+    """Launch shapes ``qssb_scan_fft_half_ex`` offers at this scan size (1..n)."""
+    n = ctypes.c_int32(0)
+    check(_lib.load().qssb_scan_fft_variants(int(scan_rows), ctypes.byref(n)))
+    return int(n.value)
+
+
+def scan_fft_half(columns: torch.Tensor, scan_shape: tuple[int, int], variant: int = 0
+                  ) -> torch.Tensor:
+    """Hermitian half-plane scan spectra G[b, r, c], c in [0, R1/2] (complex64).
+    ``variant`` names the launch shape (0 = built-in; every shape gives the
+    same bits)."""
     _require_cuda(columns, "columns", torch.uint16)
     r0, r1 = int(scan_shape[0]), int(scan_shape[1])
     n_bf = int(columns.shape[0])
     if columns.shape[1] != r0 * r1:
         raise ValueError("columns must hold R0*R1 frames per BF pixel")
     g = torch.empty((n_bf, r0, r1 // 2 + 1), dtype=torch.complex64, device=columns.device)
-    _call("qssb_scan_fft_half", columns.device, _ptr(columns), n_bf, r0, r1, _ptr(g),
-          _stream(columns))
+    _call("qssb_scan_fft_half_ex", columns.device, _ptr(columns), n_bf, r0, r1, _ptr(g),
+          int(variant), _stream(columns))
     if r0 >= 256:
         global LAUNCH_COUNT
         LAUNCH_COUNT += 1  # rows pass + columns pass

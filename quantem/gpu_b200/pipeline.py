@@ -26,6 +26,11 @@ pass's scattered 16-byte box-column stores (107 MB) add ~50 us, more than the
 gather (~60 us) they replace saves once the sample sums, the estimate and the
 map are counted (0.374 against 0.330 ms per reconstruction).
 
+With ``tune`` (the default) the first run of a BF count asks the autotuner
+for the gather's tile shape, the scan FFT's launch shape and the object's
+work partition and trotter tile (timed on the real inputs, then cached), and
+stage B is recorded with them.
+
 Every ``run`` recomputes everything from the counts in the input buffer; only
 allocation and launch overhead are shared. The one host sync reads the BF
 count between the stages (the buffers of stage B depend on it).
@@ -37,7 +42,7 @@ import math
 import numpy as np
 import torch
 
-from . import ops
+from . import autotune, ops
 from ._lib import Aberrations, Calibration
 from .backend import _device_frequencies
 from .calibration import scan_frequencies  # noqa: F401  (re-exported for callers)
@@ -51,7 +56,7 @@ class ColdReconstructor:
                  det_sampling: float, voltage_kV: float, bf_intensity_threshold: float = 0.0,
                  bf_radius: float | None = None, rotation_angle_deg: float = 0.0,
                  aberrations: tuple = (0.0, 0.0, 0.0, 0.0), use_graphs: bool = True,
-                 use_box: bool = False):
+                 use_box: bool = False, tune: bool = True):
         if counts.ndim != 4 or counts.dtype != torch.uint16 or not counts.is_cuda:
             raise ValueError("counts must be a CUDA uint16 tensor [R0, R1, K0, K1]")
         r0, r1, k0, k1 = (int(x) for x in counts.shape)
@@ -73,6 +78,7 @@ class ColdReconstructor:
         self.k_step = (recip, recip)
         self.ab = Aberrations(*(float(a) for a in aberrations))
         self.use_graphs = bool(use_graphs)
+        self.tune = bool(tune)
         self.q_row, self.q_col = _device_frequencies(self.scan_shape, self.scan_sampling, self.device)
         self.info_host = torch.empty(ops.BF_INFO_BYTES, dtype=torch.uint8, pin_memory=True)
         # the box path: BF columns written by the frame-sum pass
@@ -138,18 +144,36 @@ class ColdReconstructor:
         r0, r1 = self.scan_shape
         st = {"cal": self._calibration(n_bf), "ws": ops.Workspace(self.device),
               "obj": torch.empty((r0, r1), dtype=torch.complex64, device=self.device),
-              "phase": torch.empty((r0, r1), dtype=torch.float32, device=self.device)}
-        st["ws"].get(ops.object_workspace_bytes(st["cal"]))
+              "phase": torch.empty((r0, r1), dtype=torch.float32, device=self.device),
+              "gather_variant": 0, "fft_variant": 0, "obj_flags": 0}
+        if self.tune:
+            # the autotuner's shapes for this detector, scan and BF count
+            # (cached after the first search; timed on these very inputs)
+            if mapped:
+                g = ops.scan_fft_half_mapped(self.box_cols, self.box_map[0], n_bf, self.scan_shape)
+            else:
+                st["gather_variant"] = autotune.tune_gather(self.counts, lin)
+                columns = ops.gather_bf_columns(self.counts, lin, validate=False,
+                                                variant=st["gather_variant"])
+                st["fft_variant"] = autotune.tune_scan_fft(columns, self.scan_shape)
+                g = ops.scan_fft_half(columns, self.scan_shape, variant=st["fft_variant"])
+                del columns
+            st["obj_flags"] = autotune.tune_object(g, geom, self.q_row, self.q_col, st["cal"],
+                                                   self.ab, 0, st["ws"])
+            del g
+        st["ws"].get(ops.object_workspace_bytes(st["cal"], st["obj_flags"]))
 
         def launch():
             if mapped:
                 columns = None
                 g = ops.scan_fft_half_mapped(self.box_cols, self.box_map[0], n_bf, self.scan_shape)
             else:
-                columns = ops.gather_bf_columns(self.counts, lin, validate=False)
-                g = ops.scan_fft_half(columns, self.scan_shape)
-            ops.object_wave(g, geom, self.q_row, self.q_col, st["cal"], self.ab, workspace=st["ws"],
-                            dc_device=dc_dev, out=(st["obj"], st["phase"]))
+                columns = ops.gather_bf_columns(self.counts, lin, validate=False,
+                                                variant=st["gather_variant"])
+                g = ops.scan_fft_half(columns, self.scan_shape, variant=st["fft_variant"])
+            ops.object_wave(g, geom, self.q_row, self.q_col, st["cal"], self.ab,
+                            flags=st["obj_flags"], workspace=st["ws"], dc_device=dc_dev,
+                            out=(st["obj"], st["phase"]))
             st["keep"] = (columns, g)
 
         st["launch"] = launch
