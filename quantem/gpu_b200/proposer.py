@@ -110,25 +110,36 @@ def resample_table(kx: np.ndarray, ky: np.ndarray, kmax: float, h: float,
     wy = 1.0 - np.abs(ky[None, :] - centres[:, None]) / h
     wx = np.where(wx > 0, wx, 0.0)
     wy = np.where(wy > 0, wy, 0.0)
-    off = [0]
-    idx, wts = [], []
-    for i in range(grid):
-        nzx = np.nonzero(wx[i])[0]
-        for j in range(grid):
-            if centres[i] ** 2 + centres[j] ** 2 > rmax2:
-                off.append(off[-1])
-                continue
-            w = wx[i, nzx] * wy[j, nzx]
-            keep = w > 0
-            b = nzx[keep]
-            w = w[keep]
-            if w.size:
-                idx.append(b)
-                wts.append(w / w.sum())
-            off.append(off[-1] + int(w.size))
-    idx = np.concatenate(idx) if idx else np.zeros(0, np.int64)
-    wts = np.concatenate(wts) if wts else np.zeros(0)
-    return (np.asarray(off, np.int32), idx.astype(np.int32), wts.astype(np.float32))
+    # each tent spans a few cells per axis: (pixel, cell) pairs from the cells
+    # near each pixel only, then ordered cell-major with pixels ascending
+    reach = int(np.ceil(h / step)) + 1
+    n_bf = kx.size
+    base_i = np.floor((kx + kmax) / step).astype(np.int64)
+    base_j = np.floor((ky + kmax) / step).astype(np.int64)
+    d = np.arange(-reach, reach + 1)
+    ci = base_i[:, None] + d[None, :]                                # [B, 2R+1]
+    cj = base_j[:, None] + d[None, :]
+    ok_i = (ci >= 0) & (ci < grid)
+    ok_j = (cj >= 0) & (cj < grid)
+    ci_c = np.clip(ci, 0, grid - 1)
+    cj_c = np.clip(cj, 0, grid - 1)
+    pix = np.arange(n_bf)[:, None]
+    wxi = np.where(ok_i, wx[ci_c, pix], 0.0)
+    wyj = np.where(ok_j, wy[cj_c, pix], 0.0)
+    w = wxi[:, :, None] * wyj[:, None, :]                           # [B, 2R+1, 2R+1]
+    cells = ci_c[:, :, None] * grid + cj_c[:, None, :]
+    inside = (centres[:, None] ** 2 + centres[None, :] ** 2 <= rmax2).ravel()
+    keep = (w > 0) & inside[cells]
+    cell = cells[keep]
+    b = np.broadcast_to(np.arange(n_bf)[:, None, None], w.shape)[keep]
+    vals = w[keep]
+    order = np.lexsort((b, cell))
+    cell, b, vals = cell[order], b[order], vals[order]
+    counts = np.bincount(cell, minlength=grid * grid)
+    sums = np.bincount(cell, weights=vals, minlength=grid * grid)
+    off = np.concatenate([[0], np.cumsum(counts)])
+    wts = vals / sums[cell]
+    return off.astype(np.int32), b.astype(np.int32), wts.astype(np.float32)
 
 
 @dataclass
@@ -141,14 +152,26 @@ class Lattice:
     w: torch.Tensor
 
 
+_LATTICES: dict = {}  # device CSR tables by (device, geometry): datasets share detectors
+
+
 def _lattice(kx: np.ndarray, ky: np.ndarray, kmax: float, device) -> Lattice:
+    key = (str(device), float(kmax), np.asarray(kx, np.float32).tobytes(),
+           np.asarray(ky, np.float32).tobytes())
+    hit = _LATTICES.get(key)
+    if hit is not None:
+        return hit
     off, idx, w = resample_table(kx, ky, kmax, tent_half_width(),
                                  cell_radius=CELL_RADIUS_FACTOR * kmax / K_MAX_FACTOR)
     if idx.size == 0:
         idx = np.zeros(1, np.int32)
         w = np.zeros(1, np.float32)
     t = lambda a: torch.as_tensor(a, device=device)  # noqa: E731
-    return Lattice(int(len(kx)), t(off), t(idx), t(w))
+    lat = Lattice(int(len(kx)), t(off), t(idx), t(w))
+    if len(_LATTICES) >= 8:
+        _LATTICES.pop(next(iter(_LATTICES)))
+    _LATTICES[key] = lat
+    return lat
 
 
 def backend_features(be) -> torch.Tensor:

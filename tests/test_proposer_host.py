@@ -30,6 +30,31 @@ def test_resample_table_rows_are_normalised_tents():
         assert np.all(np.abs(kx[b] - cx) < 0.2) and np.all(np.abs(ky[b] - cy) < 0.2)
 
 
+def test_resample_table_equals_the_dense_definition():
+    """The sparse build (cells near each pixel only) gives exactly the table of
+    the definition: every (cell, pixel) tent weight product, cells beyond the
+    radius empty, pixels ascending within a cell, rows normalised."""
+    rng = np.random.default_rng(3)
+    kx = rng.uniform(-1, 1, 700)
+    ky = rng.uniform(-1, 1, 700)
+    kmax, h, grid, rad = 1.05, 0.09, 16, 0.9
+    off, idx, w = pr.resample_table(kx, ky, kmax, h, grid=grid, cell_radius=rad)
+    step = 2 * kmax / grid
+    centres = -kmax + (np.arange(grid) + 0.5) * step
+    for i in range(grid):
+        for j in range(grid):
+            c = i * grid + j
+            tent = (np.clip(1 - np.abs(kx - centres[i]) / h, 0, None)
+                    * np.clip(1 - np.abs(ky - centres[j]) / h, 0, None))
+            if centres[i] ** 2 + centres[j] ** 2 > rad ** 2:
+                tent[:] = 0
+            want = np.nonzero(tent > 0)[0]
+            np.testing.assert_array_equal(idx[off[c]:off[c + 1]], want)
+            if want.size:
+                np.testing.assert_allclose(w[off[c]:off[c + 1]], tent[want] / tent[want].sum(),
+                                           rtol=1e-6)
+
+
 def test_targets_round_trip_and_flip():
     rng = np.random.default_rng(1)
     from quantem.gpu_b200.synthetic import draw_aberrations
