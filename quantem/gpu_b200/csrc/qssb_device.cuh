@@ -18,11 +18,23 @@
 namespace qssb {
 
 // ---------------------------------------------------------------- complex
-__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
-__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
-    return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+// On sm_100 the FP32 pipe executes two-wide packed instructions (FADD2,
+// FMUL2, FFMA2), each lane rounded exactly as its scalar counterpart, so the
+// (re, im) pairs below cost one instruction where two scalar ones did, with
+// the same bits. Negation and the exact subtraction a - b == a + (-b) keep
+// every result identical to the scalar forms.
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) {
+    return __fadd2_rn(a, make_float2(-b.x, -b.y));
 }
+// (a.x b.x - a.y b.y, a.x b.y + a.y b.x) with the products of a.y rounded
+// first: fma(a.x, b.x, -(a.y b.y)), fma(a.x, b.y, a.y b.x)
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+    const float2 t = __fmul2_rn(make_float2(a.y, a.y), make_float2(-b.y, b.x));
+    return __ffma2_rn(make_float2(a.x, a.x), b, t);
+}
+// a * s for a real s
+__device__ __forceinline__ float2 cscale(float2 a, float s) { return __fmul2_rn(a, make_float2(s, s)); }
 __device__ __forceinline__ float2 cconj(float2 a) { return make_float2(a.x, -a.y); }
 __device__ __forceinline__ float2 cneg_conj(float2 a) { return make_float2(-a.x, a.y); }
 // multiply by DIR * i  (DIR = -1: -i, DIR = +1: +i)
@@ -433,6 +445,26 @@ __device__ __forceinline__ float soft_aperture_fast(float dx, float dy, float r2
     return a;
 }
 
+// The apertures at two displacements at once, (A(dm), A(dp)) for squared
+// radii r2 = (|dm|^2, |dp|^2): the isotropic form in packed FP32 (lane by
+// lane the same operations as soft_aperture_fast), the other form per lane.
+__device__ __forceinline__ float2 soft_aperture_fast2(float2 dm, float2 dp, float2 r2,
+                                                      const Probe& p) {
+    if (!p.iso)
+        return make_float2(soft_aperture_fast(dm.x, dm.y, r2.x, p),
+                           soft_aperture_fast(dp.x, dp.y, r2.y, p));
+    const float2 r = __fmul2_rn(r2, make_float2(rsqrtf(r2.x), rsqrtf(r2.y)));
+    const float2 num = __ffma2_rn(make_float2(-r.x, -r.y), make_float2(p.wavelength, p.wavelength),
+                                  make_float2(p.semiangle, p.semiangle));
+    const float2 edge = __ffma2_rn(num, make_float2(p.inv_ang, p.inv_ang), make_float2(0.5f, 0.5f));
+    float am = __saturatef(edge.x), ap = __saturatef(edge.y);
+    am = r2.x >= p.outer2 ? 0.0f : am;
+    ap = r2.y >= p.outer2 ? 0.0f : ap;
+    am = r2.x <= p.inner2 ? 1.0f : am;
+    ap = r2.y <= p.inner2 ? 1.0f : ap;
+    return make_float2(am, ap);
+}
+
 __device__ __forceinline__ bool in_edge_band(float r2, const Probe& p) {
     return !(p.inner2 > 0.0f && r2 <= p.inner2) && r2 < p.outer2;
 }
@@ -690,30 +722,34 @@ __device__ __forceinline__ float2 corrected_quad_e(float qx, float qy, int r, in
                                                    float kx, float ky, float ak,
                                                    const float2* lo, float2 e, float2 g,
                                                    const Probe& p) {
-    const float dxm = qx - kx, dym = qy - ky;
-    const float dxp = qx + kx, dyp = qy + ky;
-    const float r2m = fmaf(dxm, dxm, dym * dym);
-    const float r2p = fmaf(dxp, dxp, dyp * dyp);
-    float am = soft_aperture_fast(dxm, dym, r2m, p);
-    float ap = soft_aperture_fast(dxp, dyp, r2p, p);
-    if (fabsf(am - ap) < kApertureTie && (in_edge_band(r2m, p) || in_edge_band(r2p, p))) {
+    // packed (re, im) / (m, p) pairs throughout; lane by lane the scalar
+    // operations of the definition, so the bits do not depend on the packing
+    const float2 q2 = make_float2(qx, qy), k2 = make_float2(kx, ky);
+    const float2 dm = csub(q2, k2);  // q - k
+    const float2 dp = cadd(q2, k2);  // q + k
+    const float2 yy = __fmul2_rn(make_float2(dm.y, dp.y), make_float2(dm.y, dp.y));
+    const float2 r2 = __ffma2_rn(make_float2(dm.x, dp.x), make_float2(dm.x, dp.x), yy);
+    float2 a = soft_aperture_fast2(dm, dp, r2, p);
+    if (fabsf(a.x - a.y) < kApertureTie && (in_edge_band(r2.x, p) || in_edge_band(r2.y, p))) {
         const float2 l = *lo;
         const double qx64 = fftfreq_d(r, p.n_r, p.qval_r);
         const double qy64 = fftfreq_d(c, p.n_c, p.qval_c);
         const double kx64 = (double)kx + (double)l.x;
         const double ky64 = (double)ky + (double)l.y;
-        am = soft_aperture_fp64(qx64 - kx64, qy64 - ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
-        ap = soft_aperture_fp64(qx64 + kx64, qy64 + ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
+        a.x = soft_aperture_fp64(qx64 - kx64, qy64 - ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
+        a.y = soft_aperture_fp64(qx64 + kx64, qy64 + ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
     }
-    const float dr = (am - ap) * eq.x;
-    const float di = -(am + ap) * eq.y;
-    float gr = ak * fmaf(e.x, dr, -e.y * di);
-    float gi = ak * fmaf(e.x, di, e.y * dr);
-    const float m2 = fmaf(gr, gr, gi * gi);
+    // (dr, di) = ((am - ap) eq.x, -(am + ap) eq.y)
+    const float2 d = __fmul2_rn(__fadd2_rn(make_float2(a.x, a.x), make_float2(-a.y, a.y)),
+                                make_float2(eq.x, -eq.y));
+    // (gr, gi) = ak (e.x dr - e.y di, e.x di + e.y dr)
+    float2 gg = cscale(cmul(e, d), ak);
+    const float m2 = fmaf(gg.x, gg.x, gg.y * gg.y);
     const float inv = m2 > 1e-16f ? rsqrtf(m2) : 1e8f;
-    gr *= inv;
-    gi *= inv;
-    return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
+    gg = cscale(gg, inv);
+    // G conj(Gamma_hat) = (g.x gr + g.y gi, g.y gr - g.x gi)
+    const float2 t = __fmul2_rn(make_float2(g.y, -g.x), make_float2(gg.y, gg.y));
+    return __ffma2_rn(g, make_float2(gg.x, gg.x), t);
 }
 
 // ------------------------------------------------ 14-term Krivanek chi
@@ -864,14 +900,12 @@ __device__ __forceinline__ float2 probe_full_at_bf(double kx, double ky, float a
 
 // Kahan-compensated complex accumulation: (s.x, s.y) sums, (s.z, s.w) compensations.
 __device__ __forceinline__ void kahan_add(float4& s, float2 v) {
-    const float yr = v.x - s.z;
-    const float tr = s.x + yr;
-    s.z = (tr - s.x) - yr;
-    s.x = tr;
-    const float yi = v.y - s.w;
-    const float ti = s.y + yi;
-    s.w = (ti - s.y) - yi;
-    s.y = ti;
+    // (re, im) in step: y = v - c, t = sum + y, c = (t - sum) - y, sum = t
+    const float2 sum = make_float2(s.x, s.y);
+    const float2 y = csub(v, make_float2(s.z, s.w));
+    const float2 t = cadd(sum, y);
+    const float2 c = csub(csub(t, sum), y);
+    s = make_float4(t.x, t.y, c.x, c.y);
 }
 
 // atan2(y, x) of the phase-variance loss: octant reduction to

@@ -518,15 +518,16 @@ __global__ void __launch_bounds__(256) k_overlap_table128(
 // C = G conj(Gamma_hat) from the table entry a = (A(q - k), A(q + k)),
 // e^{-i Q} = eq, e^{i theta} = e and A(k) = ak: corrected_quad_e's arithmetic.
 __device__ __forceinline__ float2 corrected_table(float2 a, float2 eq, float2 e, float ak, float2 g) {
-    const float dr = (a.x - a.y) * eq.x;
-    const float di = -(a.x + a.y) * eq.y;
-    float gr = ak * fmaf(e.x, dr, -e.y * di);
-    float gi = ak * fmaf(e.x, di, e.y * dr);
-    const float m2 = fmaf(gr, gr, gi * gi);
+    // packed (re, im) pairs; lane by lane the scalar operations of
+    // corrected_quad_e, so the bits are the same
+    const float2 d = __fmul2_rn(__fadd2_rn(make_float2(a.x, a.x), make_float2(-a.y, a.y)),
+                                make_float2(eq.x, -eq.y));  // (dr, di)
+    float2 gg = cscale(cmul(e, d), ak);
+    const float m2 = fmaf(gg.x, gg.x, gg.y * gg.y);
     const float inv = m2 > 1e-16f ? rsqrtf(m2) : 1e8f;
-    gr *= inv;
-    gi *= inv;
-    return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
+    gg = cscale(gg, inv);
+    const float2 t = __fmul2_rn(make_float2(g.y, -g.x), make_float2(gg.y, gg.y));
+    return __ffma2_rn(g, make_float2(gg.x, gg.x), t);
 }
 
 // The same from the table without the quadratic factorisation (C30 != 0):
