@@ -92,6 +92,11 @@ typedef struct qssb_aberrations {
 
 int qssb_version(void);
 const char* qssb_last_error(void);
+/* Kernel launches this library has made in this process, all threads and
+ * devices (launches recorded into a CUDA graph count once, at capture; its
+ * replays run them again without host calls). No reference counterpart: the
+ * count behind the bench's launch figures. */
+int64_t qssb_kernel_launches(void);
 
 /* Mean diffraction pattern: sums[k] = sum over frames of counts[f][k] in
  * exact u64 arithmetic, mean_dp[k] = float32(sums[k]) / n_frames (IEEE

@@ -157,6 +157,7 @@ SIGNATURES = {
                                       _P, _I32, _P, _I32, _P]),
     "qssb_gelu_backward": (ctypes.c_int, [_P, _P, _I64, _P, _P, _P]),
     "qssb_bias_grad": (ctypes.c_int, [_P, _I32, _I32, _P, _P]),
+    "qssb_kernel_launches": (ctypes.c_int64, []),
     "qssb_mse": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _P, _P, _P]),
     "qssb_mse_heads": (ctypes.c_int, [_P, _P, _I32, _I32, _I32, _I32, _P, _I32, ctypes.c_float,
                                       _P, _P, _P, _P]),

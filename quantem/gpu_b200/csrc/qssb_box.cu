@@ -240,9 +240,9 @@ extern "C" int qssb_bf_box_estimate(const uint64_t* sums, int32_t det_rows, int3
         return set_error(QSSB_ERR_INVALID, "qssb_bf_box_estimate: invalid arguments");
     if ((int64_t)det_rows * det_cols > (1 << 26))
         return set_error(QSSB_ERR_UNSUPPORTED, "qssb_bf_box_estimate: detector too large");
-    k_box_estimate<<<1, kBoxThreads, 0, (cudaStream_t)stream>>>(
+    { k_box_estimate<<<1, kBoxThreads, 0, (cudaStream_t)stream>>>(
         reinterpret_cast<const unsigned long long*>(sums), det_rows, det_cols, radius_px, margin,
-        capacity, box);
+        capacity, box); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -273,9 +273,9 @@ extern "C" int qssb_mean_dp_u64_box(const uint16_t* counts, int64_t n_frames, in
     if (chunk < 8) chunk = 8;
     const long long gy = (n_frames + chunk - 1) / chunk;
     if (gy > 65535) return set_error(QSSB_ERR_INVALID, "qssb_mean_dp_u64_box: too many frames");
-    k_sum_frames_box<<<dim3(gx, (unsigned)gy), kSumBoxThreads, 0, s>>>(
+    { k_sum_frames_box<<<dim3(gx, (unsigned)gy), kSumBoxThreads, 0, s>>>(
         reinterpret_cast<const uint4*>(counts), n_frames, nvec, det_rows, det_cols, (int)chunk,
-        reinterpret_cast<unsigned long long*>(sums), box, (long long)capacity, box_cols);
+        reinterpret_cast<unsigned long long*>(sums), box, (long long)capacity, box_cols); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -287,9 +287,9 @@ extern "C" int qssb_bf_box_map(const int32_t* bf_linear, const qssb_bf_info_t* i
     if (!bf_linear || !info || !box || !map || !ok || det_rows <= 0 || det_cols <= 0 ||
         capacity <= 0 || box_capacity < 0)
         return set_error(QSSB_ERR_INVALID, "qssb_bf_box_map: invalid arguments");
-    k_box_map<<<1, kBoxThreads, 0, (cudaStream_t)stream>>>(bf_linear, info, det_rows, det_cols,
+    { k_box_map<<<1, kBoxThreads, 0, (cudaStream_t)stream>>>(bf_linear, info, det_rows, det_cols,
                                                            capacity, (long long)box_capacity, box,
-                                                           map, ok);
+                                                           map, ok); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

@@ -385,9 +385,9 @@ extern "C" int qssb_decode_bslz4_u16(const uint8_t* compressed, int64_t compress
     const size_t smem = (size_t)kDecWarps * kBlockBytes;
     CUDA_TRY(cudaFuncSetAttribute(k_decode_bslz4_u16, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));
-    k_decode_bslz4_u16<<<n_chunks, 32 * kDecWarps, smem, (cudaStream_t)stream>>>(
+    { k_decode_bslz4_u16<<<n_chunks, 32 * kDecWarps, smem, (cudaStream_t)stream>>>(
         compressed, compressed_bytes, reinterpret_cast<const long long*>(chunk_offsets), n_chunks,
-        chunk_bytes, out, status);
+        chunk_bytes, out, status); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -416,10 +416,10 @@ extern "C" int qssb_encode_bslz4_u16(const uint16_t* frames, int32_t n_chunks, i
     const size_t smem = (size_t)kDecWarps * (kBlockBytes + 2 * kEncHash);
     CUDA_TRY(cudaFuncSetAttribute(k_encode_bslz4_u16, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));
-    k_encode_bslz4_u16<<<n_chunks, 32 * kDecWarps, smem, s>>>(frames, n_chunks, chunk_bytes, scratch);
+    { k_encode_bslz4_u16<<<n_chunks, 32 * kDecWarps, smem, s>>>(frames, n_chunks, chunk_bytes, scratch); note_launch(); }
     CUDA_TRY(cudaGetLastError());
-    k_bslz4_chunk_sizes<<<(n_chunks + 255) / 256, 256, 0, s>>>(
-        scratch, n_chunks, chunk_bytes, reinterpret_cast<long long*>(chunk_sizes));
+    { k_bslz4_chunk_sizes<<<(n_chunks + 255) / 256, 256, 0, s>>>(
+        scratch, n_chunks, chunk_bytes, reinterpret_cast<long long*>(chunk_sizes)); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -431,9 +431,9 @@ extern "C" int qssb_pack_bslz4(const uint8_t* scratch, const uint16_t* frames, i
         return set_error(QSSB_ERR_INVALID, "qssb_pack_bslz4: null pointer or empty input");
     int rc = check_chunk_bytes(chunk_bytes, "qssb_pack_bslz4: chunk_bytes must be even, at most 4 MB");
     if (rc) return rc;
-    k_bslz4_pack<<<n_chunks, 256, 0, (cudaStream_t)stream>>>(
+    { k_bslz4_pack<<<n_chunks, 256, 0, (cudaStream_t)stream>>>(
         scratch, frames, n_chunks, chunk_bytes, reinterpret_cast<const long long*>(chunk_offsets),
-        packed);
+        packed); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

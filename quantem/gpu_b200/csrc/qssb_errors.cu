@@ -2,6 +2,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <atomic>
+
 #include "qssb_internal.h"
 
 namespace qssb {
@@ -18,6 +20,10 @@ int set_cuda_error(cudaError_t err, const char* where) {
              cudaGetErrorString(err), where);
     return QSSB_ERR_CUDA;
 }
+
+static std::atomic<long long> g_kernel_launches{0};
+
+void note_launch() { g_kernel_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int device_sm_count() {
     static int cached[64] = {0};
@@ -38,3 +44,7 @@ int device_sm_count() {
 extern "C" int qssb_version(void) { return QSSB_VERSION; }
 
 extern "C" const char* qssb_last_error(void) { return qssb::g_last_error; }
+
+extern "C" int64_t qssb_kernel_launches(void) {
+    return (int64_t)qssb::g_kernel_launches.load(std::memory_order_relaxed);
+}

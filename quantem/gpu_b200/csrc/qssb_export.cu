@@ -99,9 +99,9 @@ cudaError_t launch_export(const void* counts, int64_t n_scan, int64_t det_pixels
                           const int32_t* bf_linear, int n_bf, void* out, cudaStream_t st) {
     const dim3 grid((unsigned)((n_scan + kExportFrames - 1) / kExportFrames),
                     (unsigned)((n_bf + kExportBf - 1) / kExportBf));
-    k_export_bf<Tin, Tout><<<grid, 256, 0, st>>>(static_cast<const Tin*>(counts), n_scan,
+    { k_export_bf<Tin, Tout><<<grid, 256, 0, st>>>(static_cast<const Tin*>(counts), n_scan,
                                                  det_pixels, bf_linear, n_bf,
-                                                 static_cast<Tout*>(out));
+                                                 static_cast<Tout*>(out)); note_launch(); }
     return cudaGetLastError();
 }
 
@@ -131,10 +131,10 @@ extern "C" int qssb_count_max(const void* counts, int32_t elem_bytes, int64_t n,
     int64_t blocks = (n_vec + 255) / 256;
     if (blocks > (int64_t)sms * 8) blocks = (int64_t)sms * 8;
     if (blocks < 1) blocks = 1;
-    k_count_max<<<(unsigned)blocks, 256, 0, st>>>(
+    { k_count_max<<<(unsigned)blocks, 256, 0, st>>>(
         reinterpret_cast<const uint4*>(bytes_p + head_bytes), n_vec, bytes_p,
         (int)(head_bytes / elem_bytes), bytes_p + head_bytes + n_vec * 16,
-        (int)(tail_bytes / elem_bytes), elem_bytes, max_out);
+        (int)(tail_bytes / elem_bytes), elem_bytes, max_out); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

@@ -179,12 +179,12 @@ extern "C" int qssb_trotter_features(const float* g_half, int32_t n_bf, int32_t 
     int rc = check_csr(csr_off, csr_idx, csr_w, cells);
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
-    k_values_from_g<<<dim3((n_bf + 255) / 256, n_q), 256, 0, s>>>(
-        reinterpret_cast<const float2*>(g_half), n_bf, scan_n, q_idx, n_q, scratch);
+    { k_values_from_g<<<dim3((n_bf + 255) / 256, n_q), 256, 0, s>>>(
+        reinterpret_cast<const float2*>(g_half), n_bf, scan_n, q_idx, n_q, scratch); note_launch(); }
     CUDA_TRY(cudaGetLastError());
-    k_resample<<<dim3(n_q, 1), kFeatThreads, 0, s>>>(scratch, n_bf, n_q, csr_off, csr_idx, csr_w,
+    { k_resample<<<dim3(n_q, 1), kFeatThreads, 0, s>>>(scratch, n_bf, n_q, csr_off, csr_idx, csr_w,
                                                       cells, out_f32,
-                                                      static_cast<__nv_bfloat16*>(out_bf16));
+                                                      static_cast<__nv_bfloat16*>(out_bf16)); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -204,13 +204,13 @@ extern "C" int qssb_synth_features(const float* bf_geom, int32_t n_bf, const flo
     int rc = check_csr(csr_off, csr_idx, csr_w, cells);
     if (rc) return rc;
     cudaStream_t s = (cudaStream_t)stream;
-    k_values_synth<<<dim3(n_q, n_samples), kFeatThreads, 0, s>>>(
+    { k_values_synth<<<dim3(n_q, n_samples), kFeatThreads, 0, s>>>(
         bf_geom, n_bf, q_vec, n_q, aberrations, reinterpret_cast<const float2*>(phi), sigma, *cal,
-        (unsigned long long)seed, scratch);
+        (unsigned long long)seed, scratch); note_launch(); }
     CUDA_TRY(cudaGetLastError());
-    k_resample<<<dim3(n_q, n_samples), kFeatThreads, 0, s>>>(
+    { k_resample<<<dim3(n_q, n_samples), kFeatThreads, 0, s>>>(
         scratch, n_bf, n_q, csr_off, csr_idx, csr_w, cells, out_f32,
-        static_cast<__nv_bfloat16*>(out_bf16));
+        static_cast<__nv_bfloat16*>(out_bf16)); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

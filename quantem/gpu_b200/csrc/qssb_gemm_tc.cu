@@ -346,9 +346,9 @@ extern "C" int qssb_gemm_bf16_tc(const void* A, int32_t lda, int32_t trans_a, co
     const int kps = K / splits;
     auto launch = [&](auto kern) -> int {
         CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES));
-        kern<<<grid, THREADS, SMEM_BYTES, s>>>(a, lda, b, ldb, M, N, kps, part, status, bias,
+        { kern<<<grid, THREADS, SMEM_BYTES, s>>>(a, lda, b, ldb, M, N, kps, part, status, bias,
                                                accumulate, C, ldc,
-                                               static_cast<__nv_bfloat16*>(act_bf16), ld_act);
+                                               static_cast<__nv_bfloat16*>(act_bf16), ld_act); note_launch(); }
         CUDA_TRY(cudaGetLastError());
         return QSSB_OK;
     };
@@ -363,8 +363,8 @@ extern "C" int qssb_gemm_bf16_tc(const void* A, int32_t lda, int32_t trans_a, co
     long long blocks = (total + 255) / 256;
     const long long cap = 8LL * device_sm_count();
     if (blocks > cap) blocks = cap;
-    k_gemm_tc_reduce<<<(unsigned)blocks, 256, 0, s>>>(part, splits, M, N, bias, accumulate, C, ldc,
-                                                     static_cast<__nv_bfloat16*>(act_bf16), ld_act);
+    { k_gemm_tc_reduce<<<(unsigned)blocks, 256, 0, s>>>(part, splits, M, N, bias, accumulate, C, ldc,
+                                                     static_cast<__nv_bfloat16*>(act_bf16), ld_act); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

@@ -18,14 +18,19 @@ int device_sm_count();
 Probe make_probe(const qssb_calibration_t& cal, const qssb_aberrations_t& ab);
 // Validates a calibration; returns QSSB_OK or an error code (message set).
 int validate_calibration(const qssb_calibration_t* cal, const char* who);
-// Requested chunk count carried in flags (QSSB_FLAG_CHUNKS); 0 = built-in plan.
+// Tile-shape variant carried in flags (QSSB_FLAG_VARIANT); 0 = built-in shape.
 inline int flag_variant(int32_t flags) {
     return (int)((flags >> QSSB_FLAG_VARIANT_SHIFT) & QSSB_FLAG_VARIANT_MAX);
 }
 
+// Requested chunk count carried in flags (QSSB_FLAG_CHUNKS); 0 = built-in plan.
 inline int flag_chunks(int32_t flags) {
     return (int)((flags >> QSSB_FLAG_CHUNKS_SHIFT) & QSSB_FLAG_CHUNKS_MAX);
 }
+
+// Counts one kernel launch made by this library (every <<< >>> site calls it
+// right after the launch): qssb_kernel_launches reports the running total.
+void note_launch();
 
 }  // namespace qssb
 

@@ -1344,14 +1344,14 @@ static int launch_two_pass(const float* g_half, const float* geom, const float* 
     const auto* g = reinterpret_cast<const float2*>(g_half);
     for (int b0 = 0; b0 < cal.n_bf; b0 += pl.chunk_bf) {
         const int nb = cal.n_bf - b0 < pl.chunk_bf ? cal.n_bf - b0 : pl.chunk_bf;
-        k_loss_rows<N, CHI64, QUAD, FULL>
+        { k_loss_rows<N, CHI64, QUAD, FULL>
             <<<dim3((TP::rows + TP::rwarps - 1) / TP::rwarps, nb, n_cand), 32 * TP::rwarps,
                TP::row_smem, s>>>(g, cal.n_bf, geom, q_row, q_col, cands, cal, eq, b0, nb, stage,
-                                  delta);
+                                  delta); note_launch(); }
         CUDA_TRY(cudaGetLastError());
-        k_loss_cols<N, FULL><<<dim3(N / TP::tile, pl.n_chunks, n_cand), 32 * TP::tile,
+        { k_loss_cols<N, FULL><<<dim3(N / TP::tile, pl.n_chunks, n_cand), 32 * TP::tile,
                                TP::col_smem, s>>>(stage, delta, nb, pl.n_chunks, b0 == 0 ? 1 : 0,
-                                                  part);
+                                                  part); note_launch(); }
         CUDA_TRY(cudaGetLastError());
     }
     return QSSB_OK;
@@ -1367,7 +1367,7 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
     double* var = reinterpret_cast<double*>(ws + pl.part_bytes);
     float2* eq = reinterpret_cast<float2*>(ws + pl.part_bytes + pl.var_bytes);
     if (QUAD) {
-        k_eq_table<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(cands, cal, eq);
+        { k_eq_table<N><<<dim3((N * N + 255) / 256, n_cand), 256, 0, s>>>(cands, cal, eq); note_launch(); }
         CUDA_TRY(cudaGetLastError());
     }
     if constexpr (N == 128 && SYM) {
@@ -1382,17 +1382,17 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
             const size_t smem = Pair128Smem::bytes;
             CUDA_TRY(cudaFuncSetAttribute(k_loss_pair128<CHI64, QUAD>,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            k_loss_pair128<CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), 512, smem, s>>>(
+            { k_loss_pair128<CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), 512, smem, s>>>(
                 reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, overlap,
                 cands, cal, eq, pl.bf_per_chunk, pl.n_chunks, part, part_sq, cancel_flag(),
-                fused ? arrivals : nullptr, losses, mean_phase);
+                fused ? arrivals : nullptr, losses, mean_phase); note_launch(); }
             CUDA_TRY(cudaGetLastError());
             if (fused) return QSSB_OK;
-            k_loss_reduce_sum<N><<<dim3(N * N / kReducePix, n_cand), kReducePix * kReduceSlices, 0, s>>>(
-                part, pl.n_chunks, cal.n_bf, var, mean_phase);
+            { k_loss_reduce_sum<N><<<dim3(N * N / kReducePix, n_cand), kReducePix * kReduceSlices, 0, s>>>(
+                part, pl.n_chunks, cal.n_bf, var, mean_phase); note_launch(); }
             CUDA_TRY(cudaGetLastError());
-            k_loss_final_sq<<<n_cand, 256, 0, s>>>(var, N * N / kReducePix, part_sq, pl.n_chunks,
-                                                   cal.n_bf, N * N, losses);
+            { k_loss_final_sq<<<n_cand, 256, 0, s>>>(var, N * N / kReducePix, part_sq, pl.n_chunks,
+                                                   cal.n_bf, N * N, losses); note_launch(); }
             CUDA_TRY(cudaGetLastError());
             return QSSB_OK;
         }
@@ -1407,22 +1407,22 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
         const size_t smem = Loss128Smem::bytes;
         CUDA_TRY(cudaFuncSetAttribute(k_loss_moments128<CHI64, QUAD>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_loss_moments128<CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), 512, smem, s>>>(
+        { k_loss_moments128<CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), 512, smem, s>>>(
             reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal, eq,
-            pl.bf_per_chunk, pl.n_chunks, part);
+            pl.bf_per_chunk, pl.n_chunks, part); note_launch(); }
     } else {
         const size_t smem = LossSmem<N>::bytes;
         CUDA_TRY(cudaFuncSetAttribute(k_loss_moments<N, SYM, CHI64, QUAD>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_loss_moments<N, SYM, CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
+        { k_loss_moments<N, SYM, CHI64, QUAD><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
             reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal, eq,
-            pl.bf_per_chunk, pl.n_chunks, part);
+            pl.bf_per_chunk, pl.n_chunks, part); note_launch(); }
     }
     CUDA_TRY(cudaGetLastError());
-    k_loss_reduce<N><<<dim3(N * N / kReducePix, n_cand), kReducePix * kReduceSlices, 0, s>>>(
-        part, pl.n_chunks, cal.n_bf, var, mean_phase, N == 128 ? 1 : 0);
+    { k_loss_reduce<N><<<dim3(N * N / kReducePix, n_cand), kReducePix * kReduceSlices, 0, s>>>(
+        part, pl.n_chunks, cal.n_bf, var, mean_phase, N == 128 ? 1 : 0); note_launch(); }
     CUDA_TRY(cudaGetLastError());
-    k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N / kReducePix, N * N, losses);
+    { k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N / kReducePix, N * N, losses); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -1576,15 +1576,15 @@ static int launch_loss_full(const float* g_half, const float* geom, const float*
         const size_t smem = LossSmem<N>::bytes + sizeof(float) * N * N;
         CUDA_TRY(cudaFuncSetAttribute(k_loss_full<N, CHI64>,
                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_loss_full<N, CHI64><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
+        { k_loss_full<N, CHI64><<<dim3(pl.n_chunks, n_cand), kLossThreads, smem, s>>>(
             reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, cands, cal,
-            pl.bf_per_chunk, pl.n_chunks, part);
+            pl.bf_per_chunk, pl.n_chunks, part); note_launch(); }
         CUDA_TRY(cudaGetLastError());
     }
-    k_loss_reduce<N><<<dim3(N * N / kReducePix, n_cand), kReducePix * kReduceSlices, 0, s>>>(
-        part, pl.n_chunks, cal.n_bf, var, mean_phase, 0);
+    { k_loss_reduce<N><<<dim3(N * N / kReducePix, n_cand), kReducePix * kReduceSlices, 0, s>>>(
+        part, pl.n_chunks, cal.n_bf, var, mean_phase, 0); note_launch(); }
     CUDA_TRY(cudaGetLastError());
-    k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N / kReducePix, N * N, losses);
+    { k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N / kReducePix, N * N, losses); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -1646,8 +1646,8 @@ extern "C" int qssb_overlap_table(const float* bf_geom, const float* q_row, cons
     if (cal->n_bf > 65535)
         return set_error(QSSB_ERR_UNSUPPORTED, "qssb_overlap_table: more than 65535 BF pixels");
     const Probe p = make_probe_common(*cal, 0.0f, 0.0f, 0.0f, 0.0f);
-    k_overlap_table128<<<dim3((kNE128 + 255) / 256, cal->n_bf), 256, 0, (cudaStream_t)stream>>>(
-        bf_geom, cal->n_bf, q_row, q_col, p, reinterpret_cast<float2*>(table));
+    { k_overlap_table128<<<dim3((kNE128 + 255) / 256, cal->n_bf), 256, 0, (cudaStream_t)stream>>>(
+        bf_geom, cal->n_bf, q_row, q_col, p, reinterpret_cast<float2*>(table)); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -1752,7 +1752,7 @@ extern "C" int qssb_phase_atan2(const float* y, const float* x, float* out, int6
     long long blocks = (n + 255) / 256;
     const long long cap = 8LL * device_sm_count();
     if (blocks > cap) blocks = cap;
-    k_phase_atan2<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(y, x, out, n);
+    { k_phase_atan2<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(y, x, out, n); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

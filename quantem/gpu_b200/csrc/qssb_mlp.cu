@@ -302,11 +302,11 @@ extern "C" int qssb_gemm_bf16(const void* A, int32_t lda, int32_t trans_a, const
     auto* act = static_cast<__nv_bfloat16*>(act_bf16);
     cudaStream_t s = (cudaStream_t)stream;
     if (trans_a) {
-        if (trans_b) k_gemm_bf16<true, true><<<grid, 128, 0, s>>>(a, lda, b, ldb, M, N, K, bias, accumulate, C, ldc, act, ld_act);
-        else k_gemm_bf16<true, false><<<grid, 128, 0, s>>>(a, lda, b, ldb, M, N, K, bias, accumulate, C, ldc, act, ld_act);
+        if (trans_b) { k_gemm_bf16<true, true><<<grid, 128, 0, s>>>(a, lda, b, ldb, M, N, K, bias, accumulate, C, ldc, act, ld_act); note_launch(); }
+        else { k_gemm_bf16<true, false><<<grid, 128, 0, s>>>(a, lda, b, ldb, M, N, K, bias, accumulate, C, ldc, act, ld_act); note_launch(); }
     } else {
-        if (trans_b) k_gemm_bf16<false, true><<<grid, 128, 0, s>>>(a, lda, b, ldb, M, N, K, bias, accumulate, C, ldc, act, ld_act);
-        else k_gemm_bf16<false, false><<<grid, 128, 0, s>>>(a, lda, b, ldb, M, N, K, bias, accumulate, C, ldc, act, ld_act);
+        if (trans_b) { k_gemm_bf16<false, true><<<grid, 128, 0, s>>>(a, lda, b, ldb, M, N, K, bias, accumulate, C, ldc, act, ld_act); note_launch(); }
+        else { k_gemm_bf16<false, false><<<grid, 128, 0, s>>>(a, lda, b, ldb, M, N, K, bias, accumulate, C, ldc, act, ld_act); note_launch(); }
     }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
@@ -316,8 +316,8 @@ extern "C" int qssb_gelu_backward(const float* dy, const float* pre, int64_t n, 
                                   float* dz, void* stream) {
     if (!dy || !pre || !dz_bf16 || !dz || n <= 0)
         return set_error(QSSB_ERR_INVALID, "qssb_gelu_backward: null pointer or empty");
-    k_gelu_backward<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
-        dy, pre, n, static_cast<__nv_bfloat16*>(dz_bf16), dz);
+    { k_gelu_backward<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+        dy, pre, n, static_cast<__nv_bfloat16*>(dz_bf16), dz); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -325,7 +325,7 @@ extern "C" int qssb_gelu_backward(const float* dy, const float* pre, int64_t n, 
 extern "C" int qssb_bias_grad(const float* dz, int32_t rows, int32_t cols, float* db, void* stream) {
     if (!dz || !db || rows <= 0 || cols <= 0)
         return set_error(QSSB_ERR_INVALID, "qssb_bias_grad: null pointer or empty");
-    k_bias_grad<<<(cols + 31) / 32, 32 * kBiasWarps, 0, (cudaStream_t)stream>>>(dz, rows, cols, db);
+    { k_bias_grad<<<(cols + 31) / 32, 32 * kBiasWarps, 0, (cudaStream_t)stream>>>(dz, rows, cols, db); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -334,7 +334,7 @@ extern "C" int qssb_mse(const float* y, const float* target, int32_t rows, int32
                         int32_t ld, float* dy, float* loss, void* stream) {
     if (!y || !target || !dy || rows <= 0 || n_out <= 0 || ld < n_out)
         return set_error(QSSB_ERR_INVALID, "qssb_mse: null pointer or bad shape");
-    k_mse<<<1, 256, 0, (cudaStream_t)stream>>>(y, target, rows, n_out, ld, dy, loss);
+    { k_mse<<<1, 256, 0, (cudaStream_t)stream>>>(y, target, rows, n_out, ld, dy, loss); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -348,9 +348,9 @@ extern "C" int qssb_mse_heads(const float* y, const float* target, int32_t rows,
         return set_error(QSSB_ERR_INVALID, "qssb_mse_heads: null pointer or bad shape");
     if (!(eps >= 0.0f && eps < 1.0f))
         return set_error(QSSB_ERR_INVALID, "qssb_mse_heads: eps must be in [0, 1)");
-    k_mse_heads<<<1, 256, 0, (cudaStream_t)stream>>>(y, target, rows, n_out, heads, ld,
+    { k_mse_heads<<<1, 256, 0, (cudaStream_t)stream>>>(y, target, rows, n_out, heads, ld,
                                                       out_weight, n_select, eps, dy, loss,
-                                                      winner);
+                                                      winner); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -362,9 +362,9 @@ extern "C" int qssb_adam(float* w, float* m, float* v, const float* grad, int64_
         return set_error(QSSB_ERR_INVALID, "qssb_adam: null pointer, empty or step < 1");
     const float c1 = 1.0f - powf(beta1, (float)step);
     const float c2 = 1.0f - powf(beta2, (float)step);
-    k_adam<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+    { k_adam<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
         w, m, v, grad, n, lr, beta1, beta2, eps, weight_decay, c1, c2,
-        static_cast<__nv_bfloat16*>(w_bf16), nullptr);
+        static_cast<__nv_bfloat16*>(w_bf16), nullptr); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -375,8 +375,8 @@ extern "C" int qssb_adam_schedule(float* hyper, int32_t* step, int32_t first_ste
     if (!hyper || !step || total_steps <= 0 || first_step < 0)
         return set_error(QSSB_ERR_INVALID,
                          "qssb_adam_schedule: null pointer, total_steps < 1 or first_step < 0");
-    k_adam_schedule<<<1, 32, 0, (cudaStream_t)stream>>>(hyper, step, first_step, total_steps, lr0,
-                                                         beta1, beta2);
+    { k_adam_schedule<<<1, 32, 0, (cudaStream_t)stream>>>(hyper, step, first_step, total_steps, lr0,
+                                                         beta1, beta2); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -386,16 +386,16 @@ extern "C" int qssb_adam_dev(float* w, float* m, float* v, const float* grad, in
                              float weight_decay, void* w_bf16, void* stream) {
     if (!w || !m || !v || !grad || !hyper || n <= 0)
         return set_error(QSSB_ERR_INVALID, "qssb_adam_dev: null pointer or empty");
-    k_adam<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
+    { k_adam<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(
         w, m, v, grad, n, 0.0f, beta1, beta2, eps, weight_decay, 1.0f, 1.0f,
-        static_cast<__nv_bfloat16*>(w_bf16), hyper);
+        static_cast<__nv_bfloat16*>(w_bf16), hyper); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
 
 extern "C" int qssb_to_bf16(const float* x, int64_t n, void* y, void* stream) {
     if (!x || !y || n <= 0) return set_error(QSSB_ERR_INVALID, "qssb_to_bf16: null pointer or empty");
-    k_to_bf16<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(x, n, static_cast<__nv_bfloat16*>(y));
+    { k_to_bf16<<<grid_for(n), 256, 0, (cudaStream_t)stream>>>(x, n, static_cast<__nv_bfloat16*>(y)); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

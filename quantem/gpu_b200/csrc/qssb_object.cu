@@ -406,9 +406,9 @@ static void launch_quad(const float* g_half, const float* geom, const float* q_r
                         const float* q_col, const qssb_calibration_t& cal, const Probe& p,
                         const ObjectPlan& pl, float2* partial, cudaStream_t s) {
     const dim3 grid((quad4_threads<N, Q>() + kTrotterThreads - 1) / kTrotterThreads, pl.n_chunks);
-    k_trotter_quad4<N, Q><<<grid, kTrotterThreads, 0, s>>>(
+    { k_trotter_quad4<N, Q><<<grid, kTrotterThreads, 0, s>>>(
         reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, p, pl.bf_per_chunk,
-        partial);
+        partial); note_launch(); }
 }
 
 template <int N, bool SYM, bool CHI64, bool QUAD>
@@ -429,19 +429,19 @@ static int launch_object(const float* g_half, const float* geom, const float* q_
             launch_quad<N, 4>(g_half, geom, q_row, q_col, cal, p, pl, partial, s);
     } else {
         const dim3 grid((pl.n_q + kTrotterThreads - 1) / kTrotterThreads, pl.n_chunks);
-        k_trotter_partial<N, SYM, CHI64, QUAD><<<grid, kTrotterThreads, 0, s>>>(
+        { k_trotter_partial<N, SYM, CHI64, QUAD><<<grid, kTrotterThreads, 0, s>>>(
             reinterpret_cast<const float2*>(g_half), cal.n_bf, geom, q_row, q_col, p,
-            pl.bf_per_chunk, partial);
+            pl.bf_per_chunk, partial); note_launch(); }
     }
     CUDA_TRY(cudaGetLastError());
-    k_trotter_plane<N, SYM><<<(N * N + 31) / 32, 32 * kFoldSlices, 0, s>>>(
+    { k_trotter_plane<N, SYM><<<(N * N + 31) / 32, 32 * kFoldSlices, 0, s>>>(
         partial, pl.n_chunks, cal.n_bf, make_float2((float)cal.dc_re, (float)cal.dc_im), dc_dev,
-        plane);
+        plane); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     constexpr int W = ifft_lines<N>();
-    k_ifft_rows<N><<<N / W, 32 * W, 0, s>>>(plane);
+    { k_ifft_rows<N><<<N / W, 32 * W, 0, s>>>(plane); note_launch(); }
     CUDA_TRY(cudaGetLastError());
-    k_ifft_cols_phase<N><<<N / W, 32 * W, 0, s>>>(plane, reinterpret_cast<float2*>(object), phase);
+    { k_ifft_cols_phase<N><<<N / W, 32 * W, 0, s>>>(plane, reinterpret_cast<float2*>(object), phase); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

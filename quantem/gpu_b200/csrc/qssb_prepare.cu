@@ -379,9 +379,9 @@ extern "C" int qssb_mean_dp_u64(const uint16_t* counts, int64_t n_frames, int32_
         if (chunk < 4) chunk = 4;
         const long long gy = (n_frames + chunk - 1) / chunk;
         if (gy > 65535) return set_error(QSSB_ERR_INVALID, "qssb_mean_dp_u64: too many frames");
-        k_sum_frames_vec8<<<dim3(gx, (unsigned)gy), kSumThreads, 0, s>>>(
+        { k_sum_frames_vec8<<<dim3(gx, (unsigned)gy), kSumThreads, 0, s>>>(
             reinterpret_cast<const uint4*>(counts), n_frames, nvec, (int)chunk,
-            reinterpret_cast<unsigned long long*>(sums));
+            reinterpret_cast<unsigned long long*>(sums)); note_launch(); }
     } else {
         const int gx = (det_pixels + 255) / 256;
         long long want = (long long)sms * 16 / gx;
@@ -390,13 +390,13 @@ extern "C" int qssb_mean_dp_u64(const uint16_t* counts, int64_t n_frames, int32_
         if (chunk > 32768) chunk = 32768;
         const long long gy = (n_frames + chunk - 1) / chunk;
         if (gy > 65535) return set_error(QSSB_ERR_INVALID, "qssb_mean_dp_u64: too many frames");
-        k_sum_frames_scalar<<<dim3(gx, (unsigned)gy), 256, 0, s>>>(
-            counts, n_frames, det_pixels, (int)chunk, reinterpret_cast<unsigned long long*>(sums));
+        { k_sum_frames_scalar<<<dim3(gx, (unsigned)gy), 256, 0, s>>>(
+            counts, n_frames, det_pixels, (int)chunk, reinterpret_cast<unsigned long long*>(sums)); note_launch(); }
     }
     CUDA_TRY(cudaGetLastError());
     if (mean_dp) {
-        k_mean_from_sums<<<(det_pixels + 255) / 256, 256, 0, s>>>(
-            reinterpret_cast<const unsigned long long*>(sums), det_pixels, (float)n_frames, mean_dp);
+        { k_mean_from_sums<<<(det_pixels + 255) / 256, 256, 0, s>>>(
+            reinterpret_cast<const unsigned long long*>(sums), det_pixels, (float)n_frames, mean_dp); note_launch(); }
         CUDA_TRY(cudaGetLastError());
     }
     return QSSB_OK;
@@ -739,8 +739,8 @@ extern "C" int qssb_gather_bf_columns(const uint16_t* counts, int64_t n_frames, 
     const int gy = (n_bf + kGatherB - 1) / kGatherB;
     if (gx > 0x7fffffffLL || gy > 65535)
         return set_error(QSSB_ERR_INVALID, "qssb_gather_bf_columns: grid too large");
-    k_gather_columns<<<dim3((unsigned)gx, gy), 256, 0, (cudaStream_t)stream>>>(
-        counts, n_frames, det_pixels, bf_linear, n_bf, columns);
+    { k_gather_columns<<<dim3((unsigned)gx, gy), 256, 0, (cudaStream_t)stream>>>(
+        counts, n_frames, det_pixels, bf_linear, n_bf, columns); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -755,8 +755,8 @@ static int launch_gather_t64(const uint16_t* counts, int64_t n_frames, int det_r
     const int smem = (int)(sizeof(uint16_t) * kT64P * MAXPIX);
     CUDA_TRY(cudaFuncSetAttribute(k_gather_t64<MAXPIX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   smem));
-    k_gather_t64<MAXPIX><<<(unsigned)gx, kGbThreads, smem, stream>>>(
-        counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns);
+    { k_gather_t64<MAXPIX><<<(unsigned)gx, kGbThreads, smem, stream>>>(
+        counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -771,8 +771,8 @@ static int launch_gather_bbox(const uint16_t* counts, int64_t n_frames, int det_
     const int smem = (int)SHAPE::smem;
     CUDA_TRY(cudaFuncSetAttribute(k_gather_bbox<SHAPE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   smem));
-    k_gather_bbox<SHAPE><<<(unsigned)gx, kGbThreads, smem, stream>>>(
-        counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns);
+    { k_gather_bbox<SHAPE><<<(unsigned)gx, kGbThreads, smem, stream>>>(
+        counts, n_frames, det_rows, det_cols, bf_linear, n_bf, columns); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -1032,7 +1032,7 @@ static int launch_scan_cols_p(int n_bf, float2* g, cudaStream_t s) {
     const long long items = (long long)n_bf * ((L::H + T - 1) / T);
     const long long slots = (long long)CTAS * device_sm_count();
     const int grid = (int)(items < slots ? items : slots);
-    k_scan_cols_p<N, T, CTAS><<<grid, 32 * T, smem, s>>>(n_bf, g);
+    { k_scan_cols_p<N, T, CTAS><<<grid, 32 * T, smem, s>>>(n_bf, g); note_launch(); }
     return QSSB_OK;
 }
 
@@ -1046,8 +1046,8 @@ static int launch_scan_lines(const uint16_t* columns, int n_bf, float* g_half, i
     auto* g = reinterpret_cast<float2*>(g_half);
     CUDA_TRY(cudaFuncSetAttribute(k_scan_rows<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)L::rows_smem));
-    k_scan_rows<N><<<dim3(n_bf, (N / 2 + L::kWarps - 1) / L::kWarps), 32 * L::kWarps,
-                     L::rows_smem, s>>>(columns, n_bf, g);
+    { k_scan_rows<N><<<dim3(n_bf, (N / 2 + L::kWarps - 1) / L::kWarps), 32 * L::kWarps,
+                     L::rows_smem, s>>>(columns, n_bf, g); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaFuncSetAttribute(k_scan_cols<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)L::cols_smem));
@@ -1071,7 +1071,7 @@ static int launch_scan_lines(const uint16_t* columns, int n_bf, float* g_half, i
             default: rc = launch_scan_cols_p<N, L::kTileP, L::kCtasP>(n_bf, g, s); break;
         }
     } else {
-        k_scan_cols<N><<<dim3(n_bf, (L::H + L::kTile - 1) / L::kTile), 256, L::cols_smem, s>>>(n_bf, g);
+        { k_scan_cols<N><<<dim3(n_bf, (L::H + L::kTile - 1) / L::kTile), 256, L::cols_smem, s>>>(n_bf, g); note_launch(); }
     }
     if (rc) return rc;
     CUDA_TRY(cudaGetLastError());
@@ -1083,7 +1083,7 @@ static int launch_scan_fft(const uint16_t* columns, int n_bf, float* g_half, cud
     const size_t smem = ScanFftSmem<N>::bytes;
     CUDA_TRY(cudaFuncSetAttribute(k_scan_fft_half<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)smem));
-    k_scan_fft_half<N><<<n_bf, 512, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half));
+    { k_scan_fft_half<N><<<n_bf, 512, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half)); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -1127,8 +1127,8 @@ extern "C" int qssb_scan_fft_half_ex(const uint16_t* columns, int32_t n_bf, int3
                                           (int)smem));
             const int slots = (variant == 2 ? 1 : 2) * device_sm_count();
             const int grid = n_bf < slots ? n_bf : slots;
-            k_scan_fft128p<<<grid, 256, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half),
-                                                   nullptr, n_bf);
+            { k_scan_fft128p<<<grid, 256, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half),
+                                                   nullptr, n_bf); note_launch(); }
             CUDA_TRY(cudaGetLastError());
             return QSSB_OK;
         }
@@ -1163,8 +1163,8 @@ extern "C" int qssb_scan_fft_half_mapped(const uint16_t* columns, int64_t n_cols
                                   (int)smem));
     const int slots = 2 * device_sm_count();
     const int grid = n_bf < slots ? n_bf : slots;
-    k_scan_fft128p<<<grid, 256, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half), map,
-                                           (int)n_cols);
+    { k_scan_fft128p<<<grid, 256, smem, s>>>(columns, n_bf, reinterpret_cast<float2*>(g_half), map,
+                                           (int)n_cols); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

@@ -572,18 +572,18 @@ extern "C" int qssb_select_bf(const uint64_t* sums, int32_t det_rows, int32_t de
         return set_error(QSSB_ERR_INVALID, "qssb_select_bf: sums and info must be 8-byte aligned");
     const int npix = det_rows * det_cols;
     if (npix <= kSelCluster * kSelCThreads * kSelPer) {  // every pixel has a register slot
-        k_select_bf_cluster<<<kSelCluster, kSelCThreads, 0, (cudaStream_t)stream>>>(
+        { k_select_bf_cluster<<<kSelCluster, kSelCThreads, 0, (cudaStream_t)stream>>>(
             reinterpret_cast<const unsigned long long*>(sums), det_rows, det_cols,
-            (float)n_frames, threshold, bf_radius, mean_dp, bf_linear, info);
+            (float)n_frames, threshold, bf_radius, mean_dp, bf_linear, info); note_launch(); }
         CUDA_TRY(cudaGetLastError());
         return QSSB_OK;
     }
     const size_t smem = npix <= kSelSmemPixels ? sizeof(float) * (size_t)npix : 0;
     CUDA_TRY(cudaFuncSetAttribute(k_select_bf, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)(sizeof(float) * kSelSmemPixels)));
-    k_select_bf<<<1, kSelThreads, smem, (cudaStream_t)stream>>>(
+    { k_select_bf<<<1, kSelThreads, smem, (cudaStream_t)stream>>>(
         reinterpret_cast<const unsigned long long*>(sums), det_rows, det_cols, (float)n_frames,
-        threshold, bf_radius, mean_dp, bf_linear, info);
+        threshold, bf_radius, mean_dp, bf_linear, info); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -603,8 +603,8 @@ extern "C" int qssb_bf_geometry(const int32_t* bf_linear, const qssb_bf_info_t* 
         !(params->det_sampling_col_rad > 0.0) || !isfinite(params->rot_cos) ||
         !isfinite(params->rot_sin) || !isfinite(params->semiangle_rad))
         return set_error(QSSB_ERR_INVALID, "qssb_bf_geometry: invalid geometry parameters");
-    k_bf_geometry<<<(capacity + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
-        bf_linear, info, det_cols, capacity, *params, bf_geom);
+    { k_bf_geometry<<<(capacity + 255) / 256, 256, 0, (cudaStream_t)stream>>>(
+        bf_linear, info, det_cols, capacity, *params, bf_geom); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

@@ -198,8 +198,8 @@ static void launch_rows(const float2* in, float2* out, int n_frames, int rows, f
                         cudaStream_t s) {
     const size_t smem = sizeof(float2) * ((size_t)kTmpWarps * tmp_line<C>() + C);
     cudaFuncSetAttribute(k_tmp_rows<C, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_tmp_rows<C, DIR><<<dim3((rows + kTmpWarps - 1) / kTmpWarps, n_frames), 32 * kTmpWarps, smem, s>>>(
-        in, out, rows, scale);
+    { k_tmp_rows<C, DIR><<<dim3((rows + kTmpWarps - 1) / kTmpWarps, n_frames), 32 * kTmpWarps, smem, s>>>(
+        in, out, rows, scale); note_launch(); }
 }
 
 static int rows_pass(int cols, int dir, const float2* in, float2* out, int n_frames, int rows,
@@ -227,8 +227,8 @@ template <int R>
 static int launch_cols(float2* data, int n_frames, int cols, const float* shifts, cudaStream_t s) {
     const size_t smem = sizeof(float2) * ((size_t)kTmpWarps * (tmp_line<R>() | 1) + R);
     CUDA_TRY(cudaFuncSetAttribute(k_tmp_cols<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_tmp_cols<R><<<dim3((cols + kTmpWarps - 1) / kTmpWarps, n_frames), 32 * kTmpWarps, smem, s>>>(
-        data, cols, shifts);
+    { k_tmp_cols<R><<<dim3((cols + kTmpWarps - 1) / kTmpWarps, n_frames), 32 * kTmpWarps, smem, s>>>(
+        data, cols, shifts); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -292,15 +292,15 @@ extern "C" int qssb_join_object_waves(float* frames, const float* weights, int32
         auto* partial = static_cast<double2*>(workspace);
         const size_t part = (sizeof(double2) * (size_t)n_frames * kJoinBlocks + 255) & ~(size_t)255;
         rot = reinterpret_cast<float2*>(static_cast<char*>(workspace) + part);
-        k_overlap_partial<<<dim3(kJoinBlocks, n_frames), kJoinThreads, 0, s>>>(a, n_pix, partial);
+        { k_overlap_partial<<<dim3(kJoinBlocks, n_frames), kJoinThreads, 0, s>>>(a, n_pix, partial); note_launch(); }
         CUDA_TRY(cudaGetLastError());
-        k_overlap_rotation<<<(n_frames + 127) / 128, 128, 0, s>>>(partial, n_frames, rot);
+        { k_overlap_rotation<<<(n_frames + 127) / 128, 128, 0, s>>>(partial, n_frames, rot); note_launch(); }
         CUDA_TRY(cudaGetLastError());
     }
     const long long blocks = (n_pix + kJoinThreads - 1) / kJoinThreads;
     if (blocks > 0x7fffffffLL) return set_error(QSSB_ERR_INVALID, "qssb_join_object_waves: too many pixels");
-    k_join<<<(unsigned)blocks, kJoinThreads, 0, s>>>(a, weights, rot, n_frames, n_pix,
-                                                     reinterpret_cast<float2*>(joined), write_back);
+    { k_join<<<(unsigned)blocks, kJoinThreads, 0, s>>>(a, weights, rot, n_frames, n_pix,
+                                                     reinterpret_cast<float2*>(joined), write_back); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }

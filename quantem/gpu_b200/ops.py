@@ -16,31 +16,9 @@ from . import _lib
 from ._lib import Aberrations, Calibration, check
 
 # Kernel launches each entry point enqueues (the evidence counted by bench.py).
-LAUNCHES_PER_CALL = {
-    "qssb_mean_dp_u64": 2,
-    "qssb_select_bf": 1,
-    "qssb_bf_geometry": 1,
-    "qssb_gather_bf_columns": 1,
-    "qssb_gather_bf_columns_2d": 1,
-    "qssb_gather_bf_columns_2d_ex": 1,
-    "qssb_scan_fft_half": 1,
-    "qssb_scan_fft_half_ex": 1,
-    "qssb_object": 4,
-    "qssb_object_ex": 4,
-    "qssb_loss_batch": 3,
-    "qssb_loss_batch_ex": 3,
-    "qssb_overlap_table": 1,
-    "qssb_loss_batch_full": 3,
-    "qssb_fourier_shift": 3,
-    "qssb_join_object_waves": 1,
-    "qssb_phase_atan2": 1,
-    "qssb_count_max": 1,
-    "qssb_bf_box_estimate": 1,
-    "qssb_mean_dp_u64_box": 1,
-    "qssb_bf_box_map": 1,
-    "qssb_scan_fft_half_mapped": 1,
-    "qssb_export_bf_columns": 1,
-}
+# Kernel launches made through this module, counted by the library itself
+# (qssb_kernel_launches before and after each call); graph replays add their
+# captured count where they are issued.
 LAUNCH_COUNT = 0
 _PROFILE: list | None = None
 
@@ -64,6 +42,7 @@ def profile_ops():
 def _call(name: str, device: torch.device, *args) -> None:
     global LAUNCH_COUNT
     fn = getattr(_lib.load(), name)
+    before = int(_lib.load().qssb_kernel_launches())
     if _PROFILE is None:
         check(fn(*args))
     else:
@@ -74,7 +53,7 @@ def _call(name: str, device: torch.device, *args) -> None:
         check(fn(*args))
         end.record(stream)
         _PROFILE.append((name, start, end))
-    LAUNCH_COUNT += LAUNCHES_PER_CALL.get(name, 0)
+    LAUNCH_COUNT += int(_lib.load().qssb_kernel_launches()) - before
 
 
 def _require_cuda(t: torch.Tensor, name: str, dtype: torch.dtype) -> None:
@@ -167,9 +146,6 @@ def mean_dp_u64(counts: torch.Tensor, want_mean: bool = True
     mean = torch.empty((k0, k1), dtype=torch.float32, device=counts.device) if want_mean else None
     _call("qssb_mean_dp_u64", counts.device, _ptr(counts), n_frames, k0 * k1, _ptr(sums),
           _ptr(mean), _stream(counts))
-    if not want_mean:
-        global LAUNCH_COUNT
-        LAUNCH_COUNT -= 1  # the mean kernel is skipped
     return sums, mean
 
 
@@ -387,9 +363,6 @@ def scan_fft_half(columns: torch.Tensor, scan_shape: tuple[int, int], variant: i
     g = torch.empty((n_bf, r0, r1 // 2 + 1), dtype=torch.complex64, device=columns.device)
     _call("qssb_scan_fft_half_ex", columns.device, _ptr(columns), n_bf, r0, r1, _ptr(g),
           int(variant), _stream(columns))
-    if r0 >= 256:
-        global LAUNCH_COUNT
-        LAUNCH_COUNT += 1  # rows pass + columns pass
     return g
 
 

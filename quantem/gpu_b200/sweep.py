@@ -4,9 +4,12 @@ The reference scores candidates scan by scan, one CuPy launch sequence (and
 host sync) per batch (backend.py:1261-1374, engine.py:2120-2295). Here the
 prepared scans (each a resident ``B200SSBBackend``, uneven sizes padded by the
 reference's rule to 128^2 or 256^2) get fixed device buffers for their
-candidates, losses and workspaces; every scan's loss launches (chi-phase
-table, moments, reduction, mean) are captured once into one CUDA graph, and a
-sweep step is: copy the candidates in, replay the graph, read the losses out.
+candidates, losses and workspaces; every scan's loss launches (at 128^2 the
+chi-phase table and the pair kernel, which folds in its last CTA; at 256^2 the
+table, a row and a column pass per L2-sized BF chunk, and the fold) are
+captured once into one CUDA graph, and a sweep step is: copy the candidates
+in, replay the graph, read the losses out. ``launches_per_replay`` is the
+library's own count of the kernels captured (``qssb_kernel_launches``).
 The work partition of each scan's loss kernel is chosen by the autotuner
 (``autotune.tune_loss``) before capture.
 """

@@ -17,7 +17,7 @@ import torch
 
 from oracle import ssb_oracle as so
 from oracle import ssb_torch_fp64 as tf
-from quantem.gpu_b200 import B200SSBBackend, ops
+from quantem.gpu_b200 import B200SSBBackend, _lib, ops
 from quantem.gpu_b200.sweep import MultiScanSweep
 from quantem.gpu_b200.synthetic import draw_aberrations, generate, sweep_specs
 
@@ -57,13 +57,26 @@ def test_graph_sweep_matches_direct_calls_and_repeats(scans, candidates):
     sw = MultiScanSweep([be for _, _, be in scans], N_CAND)
     first = sw(candidates)
     second = sw(candidates)
-    assert sw.launches_per_replay == 3 * len(scans)  # moments, reduce, mean per scan
     for a, b in zip(first, second):
         np.testing.assert_array_equal(a, b)
+    # the graph holds exactly the kernels the direct calls launch (the library
+    # counts every launch): at 128^2 the phase table and the pair kernel, at
+    # 256^2 the table and a row and a column pass per L2-sized BF chunk, then
+    # the fold
+    lib = _lib.load()
+    direct_launches = 0
     for (_, _, be), slot, c, got in zip(scans, sw._slots, candidates, first):
+        n0 = lib.qssb_kernel_launches()
+        ops.loss_batch(be.G_qk, be._geom_dev, be._q_row, be._q_col, slot["cal"],
+                       torch.as_tensor(c, device=DEV), flags=slot["flags"],
+                       overlap=slot["overlap"])
+        direct_launches += lib.qssb_kernel_launches() - n0
         direct, _ = ops.loss_batch(be.G_qk, be._geom_dev, be._q_row, be._q_col, slot["cal"],
                                    torch.as_tensor(c, device=DEV), flags=slot["flags"])
         np.testing.assert_array_equal(direct.cpu().numpy(), got)
+    assert sw.launches_per_replay == direct_launches
+    assert sw._slots[0]["overlap"] is not None  # 128^2: two launches
+    assert direct_launches > 2 * 2
 
 
 def test_sweep_losses_match_fp64_and_find_the_truth(scans, candidates):

@@ -108,3 +108,26 @@ def test_tuned_cold_reconstruction_matches_untuned(counts128):
     st = tuned._b[(tuned.last_info.n_bf, False)]
     assert 0 <= st["gather_variant"] <= _lib.GATHER_VARIANTS
     assert torch.equal(tuned.run(), a)
+
+
+def test_library_counts_its_own_kernel_launches(counts128):
+    """``qssb_kernel_launches``: one launch for a gather, two for a fused 128^2
+    loss batch (the phase table and the pair kernel, whose last CTA folds),
+    four for an object (trotter, fold, row and column inverse FFTs)."""
+    from quantem.gpu_b200 import B200SSBBackend
+
+    lib = _lib.load()
+    lin = _disk(128, 26.0)
+    n0 = lib.qssb_kernel_launches()
+    ops.gather_bf_columns(counts128, lin, validate=False)
+    assert lib.qssb_kernel_launches() - n0 == 1
+    be = B200SSBBackend(counts128, device=DEV, **KW)
+    be.variance_loss_batch([0.0] * 64, [0.0] * 64, [0.0] * 64)  # builds the overlap table
+    n0, c0 = lib.qssb_kernel_launches(), ops.LAUNCH_COUNT
+    be.variance_loss_batch(list(np.linspace(-50, 50, 64)), [0.0] * 64, [0.0] * 64)
+    assert lib.qssb_kernel_launches() - n0 == 2
+    assert ops.LAUNCH_COUNT - c0 == 2
+    n0 = lib.qssb_kernel_launches()
+    be.object_and_phase(10.0, 5.0, 0.1)
+    assert lib.qssb_kernel_launches() - n0 == 4
+    be.close()

@@ -26,7 +26,7 @@ GOLDEN = REPO / "tests" / "golden"
 # ------------------------------------------------------------------ C ABI
 def _declared_symbols() -> list[str]:
     text = (REPO / "include" / "qssb.h").read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(qssb_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|const char\*)\s+(qssb_\w+)\s*\(", text, re.M)))
 
 
 def test_library_exports_every_declared_symbol():
