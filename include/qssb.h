@@ -336,17 +336,22 @@ int qssb_loss_batch(const float* g_half, const float* bf_geom, const float* q_ro
  * flag that is never set changes nothing. */
 int qssb_set_cancel(const int32_t* flag);
 
-/* Bytes of the overlap table of a 128x128-scan dataset: float2 [n_bf][8383]. */
+/* Bytes of the overlap table of a square scan of side N: float2 [n_bf][E],
+ * E = 8383 at N = 128, (N/2 + 1) N + N/2 at N = 256, 512, 1024 (1.05 MB per
+ * BF pixel at 512, 4.2 MB at 1024: check the size against the device). */
 int qssb_overlap_table_bytes(const qssb_calibration_t* cal, size_t* bytes);
 
-/* The candidate-independent part of the overlap of a 128x128 dataset, the
- * aperture pair table[b][e] = (A(q - k_b), A(q + k_b)) on the half set the
- * loss evaluates (rows 0..64 x all columns, then
- * (127 - j, 64) for j < 63), with the loss kernels' aperture rule (FP64 where
- * the two apertures tie in the soft edge). The reference recomputes these
- * apertures for every candidate inside gamma_mul_pk_onthefly
- * (common.py:115-236); computing them once per dataset is this engine's own
- * step. Depends on the geometry only: rebuild after cache_rotation. */
+/* The candidate-independent part of the overlap, the aperture pair
+ * table[b][e] = (A(q - k_b), A(q + k_b)) at the frequencies the loss
+ * evaluates, with the loss kernels' aperture rule (FP64 where the two
+ * apertures tie in the soft edge). N = 128: the half set (rows 0..64 x all
+ * columns, then (127 - j, 64) for j < 63) in the pair kernel's order; N >= 256:
+ * the two-pass row kernel's, rows 0 .. N/2 x all N columns row-major, then
+ * at (N/2 + 1) N + r the partner (N - r, N/2) of its Nyquist-column relation
+ * (r = 1 .. N/2 - 1). The reference recomputes these apertures for every
+ * candidate inside gamma_mul_pk_onthefly (common.py:115-236); computing them
+ * once per dataset is this engine's own step. Depends on the geometry only:
+ * rebuild after cache_rotation. */
 int qssb_overlap_table(const float* bf_geom, const float* q_row, const float* q_col,
                        const qssb_calibration_t* cal, float* table, void* stream);
 
@@ -356,9 +361,12 @@ int qssb_overlap_table(const float* bf_geom, const float* q_row, const float* q_
  * anti-Hermitian parts packed as one complex plane, the Hermitian DC and
  * Nyquist-line parts transformed on their own) with the apertures read from
  * the table: for QSSB_FLAG_QUADRATIC batches through the factorised overlap,
- * otherwise (C30) through the direct probe phases. The workspace is the same.
- * The reduction order is fixed for a given plan; the result differs from the
- * table-free path by float32 rounding only. */
+ * otherwise (C30) through the direct probe phases. With a table and 256 .. 1024
+ * scans, the row pass of QSSB_FLAG_QUADRATIC batches (without
+ * QSSB_FLAG_CHI_FP64) reads the apertures instead of evaluating them; other
+ * batches there ignore the table. The workspace is the same. The reduction
+ * order is fixed for a given plan; the result differs from the table-free path
+ * by float32 rounding only. */
 int qssb_loss_batch_ex(const float* g_half, const float* bf_geom, const float* q_row,
                        const float* q_col, const qssb_calibration_t* cal,
                        const qssb_aberrations_t* candidates, int32_t n_cand, int32_t flags,

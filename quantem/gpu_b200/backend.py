@@ -425,17 +425,27 @@ class B200SSBBackend:
                                self._calibration(), Aberrations(C10, C12, phi12, C30),
                                flags=self._object_flags(C30 == 0.0), workspace=self._workspace)
 
-    # the 128x128 loss evaluates the candidate-independent overlap apertures
-    # once per geometry (qssb_overlap_table) instead of once per candidate
+    # the loss of a square 128..1024 scan evaluates the candidate-independent
+    # overlap apertures once per geometry (qssb_overlap_table) instead of once
+    # per candidate; the table is float2 per (BF pixel, retained scan
+    # frequency), so it is built only while it stays below this share of the
+    # free device memory and below OVERLAP_TABLE_MAX_BYTES
     use_overlap_table = True
+    OVERLAP_TABLE_MAX_BYTES = 16 << 30
+    OVERLAP_TABLE_FREE_SHARE = 0.25
 
     def _overlap_table(self) -> torch.Tensor | None:
-        if not self.use_overlap_table or self._scan_shape != (128, 128):
+        rows, cols = self._scan_shape
+        if not self.use_overlap_table or rows != cols or rows not in (128, 256, 512, 1024):
             return None
         if getattr(self, "_overlap_geom", None) is not self._geom_dev:
-            self._overlap = ops.overlap_table(self._geom_dev, self._q_row, self._q_col,
-                                              self._calibration())
+            self._overlap = None
             self._overlap_geom = self._geom_dev
+            need = ops.overlap_table_bytes(self._calibration())
+            free, _ = torch.cuda.mem_get_info(self.device)
+            if need <= min(self.OVERLAP_TABLE_MAX_BYTES, self.OVERLAP_TABLE_FREE_SHARE * free):
+                self._overlap = ops.overlap_table(self._geom_dev, self._q_row, self._q_col,
+                                                  self._calibration())
         return self._overlap
 
     def variance_loss_batch(self, C10, C12, phi12, C30=None) -> torch.Tensor:

@@ -486,14 +486,13 @@ __device__ __forceinline__ void elem_rc128(int e, int& r, int& c) {
     }
 }
 
-__global__ void __launch_bounds__(256) k_overlap_table128(
-    const float* __restrict__ geom, int n_bf, const float* __restrict__ q_row,
-    const float* __restrict__ q_col, Probe p, float2* __restrict__ table) {
-    const int e = blockIdx.x * 256 + threadIdx.x;
-    const int b = blockIdx.y;
-    if (e >= kNE128 || b >= n_bf) return;
-    int r, c;
-    elem_rc128(e, r, c);
+// (A(q - k_b), A(q + k_b)) at scan frequency (r, c) for BF pixel b: the fast
+// float32 aperture, recomputed in FP64 where the pair ties in the soft edge
+// (corrected_quad_e's rule and arithmetic).
+__device__ __forceinline__ float2 aperture_pair(const float* __restrict__ geom, int n_bf, int b,
+                                                const float* __restrict__ q_row,
+                                                const float* __restrict__ q_col, int r, int c,
+                                                const Probe& p) {
     const float kx = __ldg(geom + b);
     const float ky = __ldg(geom + n_bf + b);
     const float qx = __ldg(q_row + r);
@@ -512,7 +511,44 @@ __global__ void __launch_bounds__(256) k_overlap_table128(
         am = soft_aperture_fp64(qx64 - kx64, qy64 - ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
         ap = soft_aperture_fp64(qx64 + kx64, qy64 + ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
     }
-    table[(size_t)b * kNE128 + e] = make_float2(am, ap);
+    return make_float2(am, ap);
+}
+
+__global__ void __launch_bounds__(256) k_overlap_table128(
+    const float* __restrict__ geom, int n_bf, const float* __restrict__ q_row,
+    const float* __restrict__ q_col, Probe p, float2* __restrict__ table) {
+    const int e = blockIdx.x * 256 + threadIdx.x;
+    const int b = blockIdx.y;
+    if (e >= kNE128 || b >= n_bf) return;
+    int r, c;
+    elem_rc128(e, r, c);
+    table[(size_t)b * kNE128 + e] = aperture_pair(geom, n_bf, b, q_row, q_col, r, c, p);
+}
+
+// The two-pass (256^2 .. 1024^2) table: per BF pixel the frequencies the row
+// pass evaluates - rows 0 .. N/2 over all N columns, row-major - then the
+// partners (N - r, N/2) of its Nyquist-column relation at index
+// (N/2 + 1) N + r, r = 1 .. N/2 - 1 (index r = 0 unused).
+template <int N>
+__host__ __device__ constexpr size_t two_pass_table_elems() {
+    return (size_t)(N / 2 + 1) * N + N / 2;
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_overlap_table_rows(
+    const float* __restrict__ geom, int n_bf, const float* __restrict__ q_row,
+    const float* __restrict__ q_col, Probe p, float2* __restrict__ table) {
+    constexpr int kMain = (N / 2 + 1) * N;
+    const int e = blockIdx.x * 256 + threadIdx.x;
+    const int b = blockIdx.y;
+    if (e >= (int)two_pass_table_elems<N>() || b >= n_bf) return;
+    float2 v = make_float2(0.0f, 0.0f);
+    if (e < kMain) {
+        v = aperture_pair(geom, n_bf, b, q_row, q_col, e / N, e % N, p);
+    } else if (e > kMain) {
+        v = aperture_pair(geom, n_bf, b, q_row, q_col, N - (e - kMain), N / 2, p);
+    }
+    table[(size_t)b * two_pass_table_elems<N>() + e] = v;
 }
 
 // C = G conj(Gamma_hat) from the table entry a = (A(q - k), A(q + k)),
@@ -1036,7 +1072,7 @@ __global__ void __launch_bounds__(32 * row_warps(N)) k_loss_rows(
     const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
     const float* __restrict__ q_row, const float* __restrict__ q_col, const void* __restrict__ cands,
     qssb_calibration_t cal, const float2* __restrict__ eq_table, int b0, int nb_chunk,
-    float2* __restrict__ stage, float2* __restrict__ delta) {
+    float2* __restrict__ stage, float2* __restrict__ delta, const float2* __restrict__ overlap) {
     using TP = TwoPass<N, FULL>;
     constexpr int H = N / 2 + 1;
     constexpr int RW = TP::rwarps;
@@ -1120,11 +1156,14 @@ __global__ void __launch_bounds__(32 * row_warps(N)) k_loss_rows(
     };
     const float2 e_row = kSep ? s_phr[warp] : make_float2(1.0f, 0.0f);
     const float qx = __ldg(q_row + r);
+    // with the per-geometry table the apertures are read, not evaluated
+    const bool tab = kSep && overlap != nullptr;
+    const float2* ovb = tab ? overlap + (size_t)b * two_pass_table_elems<N>() : nullptr;
     float2 v[RPL];
     constexpr int kBatch = 8;  // loads of 8 elements issued before their math
 #pragma unroll
     for (int t0 = 0; t0 < RPL; t0 += kBatch) {
-        float2 gv[kBatch], eq[kBatch];
+        float2 gv[kBatch], eq[kBatch], ov[kBatch];
         float qy[kBatch];
 #pragma unroll
         for (int u = 0; u < kBatch; ++u) {
@@ -1132,12 +1171,19 @@ __global__ void __launch_bounds__(32 * row_warps(N)) k_loss_rows(
             gv[u] = load_g(r, c);
             qy[u] = __ldg(q_col + c);
             eq[u] = QUAD && !FULL ? __ldg(eqc + r * N + c) : make_float2(1.0f, 0.0f);
+            ov[u] = tab ? __ldg(ovb + r * N + c) : make_float2(0.0f, 0.0f);
         }
 #pragma unroll
         for (int u = 0; u < kBatch; ++u) {
             const int t = t0 + u;
             const int c = lane + 32 * t;
-            v[t] = (r == 0 && c == 0) ? dc : eval(r, c, qx, qy[u], gv[u], eq[u], e_row);
+            if (tab) {
+                v[t] = (r == 0 && c == 0)
+                           ? dc
+                           : corrected_table(ov[u], eq[u], cmul(e_row, s_phc[c]), kq.ak, gv[u]);
+            } else {
+                v[t] = (r == 0 && c == 0) ? dc : eval(r, c, qx, qy[u], gv[u], eq[u], e_row);
+            }
             if (!FULL && t == N / 64 && lane == 0 && r >= 1 && r < N / 2) {  // c == N/2
                 float2 e_neg = make_float2(1.0f, 0.0f);
                 if constexpr (kSep) {
@@ -1146,9 +1192,12 @@ __global__ void __launch_bounds__(32 * row_warps(N)) k_loss_rows(
                     e_neg = make_float2(cs, sn);
                 }
                 const float2 eqn = QUAD && !FULL ? __ldg(eqc + (N - r) * N + N / 2) : make_float2(1.0f, 0.0f);
-                delta[((size_t)cand * nb_chunk + bi) * (N / 2) + r] =
-                    cadd(cconj(v[t]), eval(N - r, N / 2, __ldg(q_row + N - r), qy[u],
-                                           load_g(N - r, N / 2), eqn, e_neg));
+                const float2 partner =
+                    tab ? corrected_table(__ldg(ovb + (N / 2 + 1) * N + r), eqn,
+                                          cmul(e_neg, s_phc[N / 2]), kq.ak, load_g(N - r, N / 2))
+                        : eval(N - r, N / 2, __ldg(q_row + N - r), qy[u], load_g(N - r, N / 2),
+                               eqn, e_neg);
+                delta[((size_t)cand * nb_chunk + bi) * (N / 2) + r] = cadd(cconj(v[t]), partner);
             }
         }
     }
@@ -1327,7 +1376,7 @@ template <int N, bool CHI64, bool QUAD, bool FULL>
 static int launch_two_pass(const float* g_half, const float* geom, const float* q_row,
                            const float* q_col, const qssb_calibration_t& cal, const void* cands,
                            int n_cand, const LossPlan& pl, const float2* eq, float* part,
-                           char* stage_base, cudaStream_t s) {
+                           char* stage_base, cudaStream_t s, const float2* overlap = nullptr) {
     using TP = TwoPass<N, FULL>;
     float2* stage = reinterpret_cast<float2*>(stage_base);
     float2* delta = reinterpret_cast<float2*>(stage_base + pl.stage_bytes);
@@ -1347,7 +1396,7 @@ static int launch_two_pass(const float* g_half, const float* geom, const float* 
         { k_loss_rows<N, CHI64, QUAD, FULL>
             <<<dim3((TP::rows + TP::rwarps - 1) / TP::rwarps, nb, n_cand), 32 * TP::rwarps,
                TP::row_smem, s>>>(g, cal.n_bf, geom, q_row, q_col, cands, cal, eq, b0, nb, stage,
-                                  delta); note_launch(); }
+                                  delta, overlap); note_launch(); }
         CUDA_TRY(cudaGetLastError());
         { k_loss_cols<N, FULL><<<dim3(N / TP::tile, pl.n_chunks, n_cand), 32 * TP::tile,
                                TP::col_smem, s>>>(stage, delta, nb, pl.n_chunks, b0 == 0 ? 1 : 0,
@@ -1401,7 +1450,7 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
         static_assert(SYM, "the two-pass loss evaluates the half set");
         const int rc = launch_two_pass<N, CHI64, QUAD, false>(
             g_half, geom, q_row, q_col, cal, cands, n_cand, pl, eq, part,
-            ws + pl.part_bytes + pl.var_bytes + pl.eq_bytes, s);
+            ws + pl.part_bytes + pl.var_bytes + pl.eq_bytes, s, overlap);
         if (rc) return rc;
     } else if constexpr (N == 128) {
         const size_t smem = Loss128Smem::bytes;
@@ -1626,13 +1675,25 @@ extern "C" int qssb_loss_batch(const float* g_half, const float* bf_geom, const 
                               nullptr, workspace, workspace_bytes, losses, mean_phase, stream);
 }
 
+static size_t overlap_table_elems(int n) {
+    switch (n) {
+        case 128: return (size_t)kNE128;
+        case 256: return two_pass_table_elems<256>();
+        case 512: return two_pass_table_elems<512>();
+        case 1024: return two_pass_table_elems<1024>();
+        default: return 0;
+    }
+}
+
 extern "C" int qssb_overlap_table_bytes(const qssb_calibration_t* cal, size_t* bytes) {
     int rc = validate_calibration(cal, "qssb_overlap_table_bytes: null calibration");
     if (rc) return rc;
     if (!bytes) return set_error(QSSB_ERR_INVALID, "qssb_overlap_table_bytes: null output");
-    if (cal->scan_rows != 128 || cal->scan_cols != 128)
-        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_overlap_table: 128x128 scans only");
-    *bytes = sizeof(float2) * (size_t)kNE128 * (size_t)cal->n_bf;
+    const size_t elems = overlap_table_elems(cal->scan_rows);
+    if (elems == 0 || cal->scan_cols != cal->scan_rows)
+        return set_error(QSSB_ERR_UNSUPPORTED,
+                         "qssb_overlap_table: square 128, 256, 512 or 1024 scans only");
+    *bytes = sizeof(float2) * elems * (size_t)cal->n_bf;
     return QSSB_OK;
 }
 
@@ -1646,8 +1707,15 @@ extern "C" int qssb_overlap_table(const float* bf_geom, const float* q_row, cons
     if (cal->n_bf > 65535)
         return set_error(QSSB_ERR_UNSUPPORTED, "qssb_overlap_table: more than 65535 BF pixels");
     const Probe p = make_probe_common(*cal, 0.0f, 0.0f, 0.0f, 0.0f);
-    { k_overlap_table128<<<dim3((kNE128 + 255) / 256, cal->n_bf), 256, 0, (cudaStream_t)stream>>>(
-        bf_geom, cal->n_bf, q_row, q_col, p, reinterpret_cast<float2*>(table)); note_launch(); }
+    auto* t = reinterpret_cast<float2*>(table);
+    cudaStream_t st = (cudaStream_t)stream;
+    const unsigned gx = (unsigned)((overlap_table_elems(cal->scan_rows) + 255) / 256);
+    switch (cal->scan_rows) {
+        case 128: { k_overlap_table128<<<dim3(gx, cal->n_bf), 256, 0, st>>>(bf_geom, cal->n_bf, q_row, q_col, p, t); note_launch(); } break;
+        case 256: { k_overlap_table_rows<256><<<dim3(gx, cal->n_bf), 256, 0, st>>>(bf_geom, cal->n_bf, q_row, q_col, p, t); note_launch(); } break;
+        case 512: { k_overlap_table_rows<512><<<dim3(gx, cal->n_bf), 256, 0, st>>>(bf_geom, cal->n_bf, q_row, q_col, p, t); note_launch(); } break;
+        default: { k_overlap_table_rows<1024><<<dim3(gx, cal->n_bf), 256, 0, st>>>(bf_geom, cal->n_bf, q_row, q_col, p, t); note_launch(); } break;
+    }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -1673,17 +1741,18 @@ extern "C" int qssb_loss_batch_ex(const float* g_half, const float* bf_geom, con
     const bool chi64 = (flags & QSSB_FLAG_CHI_FP64) != 0;
     const bool quad = (flags & QSSB_FLAG_QUADRATIC) != 0;
     const int chunks = flag_chunks(flags);
-    if (overlap && (cal->scan_rows != 128 || cal->scan_cols != 128))
-        return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch_ex: the overlap table is for 128x128 scans");
+    if (overlap && (cal->scan_rows < 128 || cal->scan_cols != cal->scan_rows))
+        return set_error(QSSB_ERR_UNSUPPORTED,
+                         "qssb_loss_batch_ex: the overlap table is for square 128 .. 1024 scans");
     const float2* ov = reinterpret_cast<const float2*>(overlap);
     cudaStream_t s = (cudaStream_t)stream;
     char* ws = static_cast<char*>(workspace);
     switch (cal->scan_rows) {
         case 64: return dispatch_loss<64>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, nullptr, s);
         case 128: return dispatch_loss<128>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, ov, s);
-        case 256: return dispatch_loss<256>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, nullptr, s);
-        case 512: return dispatch_loss<512>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, nullptr, s);
-        case 1024: return dispatch_loss<1024>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, nullptr, s);
+        case 256: return dispatch_loss<256>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, ov, s);
+        case 512: return dispatch_loss<512>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, ov, s);
+        case 1024: return dispatch_loss<1024>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, ov, s);
         default: return set_error(QSSB_ERR_UNSUPPORTED,
                                   "qssb_loss_batch: scan size must be 64, 128, 256, 512 or 1024");
     }

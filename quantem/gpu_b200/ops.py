@@ -461,16 +461,25 @@ def set_cancel_flag(flag: torch.Tensor | None) -> None:
     check(_lib.load().qssb_set_cancel(_ptr(flag)))
 
 
+def overlap_table_bytes(cal: Calibration) -> int:
+    """Bytes of the overlap table of a square 128, 256, 512 or 1024 scan."""
+    nbytes = ctypes.c_size_t(0)
+    check(_lib.load().qssb_overlap_table_bytes(ctypes.byref(cal), ctypes.byref(nbytes)))
+    return int(nbytes.value)
+
+
 def overlap_table(bf_geom: torch.Tensor, q_row: torch.Tensor, q_col: torch.Tensor,
                   cal: Calibration) -> torch.Tensor:
-    """The candidate-independent overlap apertures of a 128x128-scan dataset
-    (float32 CUDA [n_bf, 8383, 2]) for ``loss_batch(..., overlap=...)``."""
+    """The candidate-independent overlap apertures of a square-scan dataset
+    (float32 CUDA [n_bf, E, 2]) for ``loss_batch(..., overlap=...)``.
+
+    E is 8383 at 128x128 (the pair kernel's retained-frequency order) and
+    (N/2+1)*N + N/2 at N = 256, 512, 1024 (rows 0..N/2 of the scan-frequency
+    plane, then the partner (N-r, N/2) of each row r)."""
     _require_cuda(bf_geom, "bf_geom", torch.float32)
     if tuple(bf_geom.shape) != (_lib.GEOM_ROWS, cal.n_bf):
         raise ValueError("bf_geom shape does not match the calibration")
-    nbytes = ctypes.c_size_t(0)
-    check(_lib.load().qssb_overlap_table_bytes(ctypes.byref(cal), ctypes.byref(nbytes)))
-    table = torch.empty(nbytes.value // 4, dtype=torch.float32, device=bf_geom.device)
+    table = torch.empty(overlap_table_bytes(cal) // 4, dtype=torch.float32, device=bf_geom.device)
     _call("qssb_overlap_table", bf_geom.device, _ptr(bf_geom), _ptr(q_row), _ptr(q_col),
           ctypes.byref(cal), _ptr(table), _stream(bf_geom))
     return table.view(cal.n_bf, -1, 2)
@@ -483,8 +492,10 @@ def loss_batch(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
                ) -> tuple[torch.Tensor, torch.Tensor | None]:
     """Phase-variance losses for ``candidates`` (float32 CUDA [n, 4]: C10, C12, phi12, C30).
 
-    ``overlap`` (from ``overlap_table``, 128x128 scans) selects the
-    table-driven kernel (two BF pixels per inverse 2D FFT)."""
+    ``overlap`` (from ``overlap_table``, square 128 .. 1024 scans) supplies
+    the candidate-independent apertures: at 128x128 it selects the pair
+    kernel (two BF pixels per inverse 2D FFT); at 256 .. 1024 the row pass
+    of the quadratic-chi loss reads them instead of evaluating them."""
     _require_cuda(g_half, "g_half", torch.complex64)
     _require_cuda(bf_geom, "bf_geom", torch.float32)
     _require_cuda(candidates, "candidates", torch.float32)
@@ -510,7 +521,7 @@ def loss_batch(g_half: torch.Tensor, bf_geom: torch.Tensor, q_row: torch.Tensor,
               buf.numel(), _ptr(losses), _ptr(mp), _stream(g_half))
     else:
         _require_cuda(overlap, "overlap", torch.float32)
-        if overlap.shape[0] != cal.n_bf:
+        if overlap.shape[0] != cal.n_bf or overlap.numel() * 4 != overlap_table_bytes(cal):
             raise ValueError("overlap table does not match the calibration")
         _call("qssb_loss_batch_ex", g_half.device, _ptr(g_half), _ptr(bf_geom), _ptr(q_row),
               _ptr(q_col), ctypes.byref(cal), _ptr(candidates), n, int(flags), _ptr(overlap),

@@ -10,6 +10,10 @@ and on the CPU-runnable workload padded to 128^2 (437 pixels: an odd count,
 so the last pixel of a chunk is transformed alone); plus the table itself
 against an FP64 evaluation of the apertures, repeatability, and the
 single-candidate, three-candidate and 64-candidate plans.
+
+At 256^2 and 512^2 the two-pass loss reads the same apertures from its own
+table order; there the table layout, the losses against the oracle and the
+table-free kernel, and the backend's table switch are checked.
 """
 from __future__ import annotations
 
@@ -20,7 +24,7 @@ import pytest
 import torch
 
 from oracle import ssb_oracle as so
-from quantem.gpu_b200 import ops
+from quantem.gpu_b200 import B200SSBBackend, ops
 from quantem.gpu_b200._lib import QSSB_FLAG_CHI_FP64, QSSB_FLAG_QUADRATIC
 from recipes import disk_input, synthetic_plain_32
 from test_gpu_parity import DISK_KW, _prep_case
@@ -159,3 +163,84 @@ def test_cancel_flag_stops_a_batch_without_hanging(case):
     finally:
         ops.set_cancel_flag(None)
     np.testing.assert_array_equal(run(), want)
+
+
+# ---------------------------------------------------------------- 256^2 .. 1024^2
+# The two-pass loss (row pass, then column pass) reads the same apertures from
+# a per-geometry table in its own order: rows 0 .. N/2 of the scan-frequency
+# plane over all N columns, then the partner (N - r, N/2) of each row r of the
+# Nyquist-column relation at index (N/2 + 1) N + r.
+
+
+@pytest.fixture(scope="module", params=[256, 512])
+def big_case(request):
+    n = request.param
+    return _prep_case(disk_input(123, scan=(n, n)), **DISK_KW)
+
+
+def test_two_pass_table_layout_matches_fp64_apertures(big_case):
+    prep, cal, d = big_case
+    n = prep.scan_shape[0]
+    table = ops.overlap_table(d["geom"], d["q_row"], d["q_col"], cal)
+    assert ops.overlap_table_bytes(cal) == 8 * cal.n_bf * ((n // 2 + 1) * n + n // 2)
+    table = table.cpu().numpy().astype(np.float64)
+    assert table.shape == (cal.n_bf, (n // 2 + 1) * n + n // 2, 2)
+    main = (n // 2 + 1) * n
+    np.testing.assert_array_equal(table[:, main], 0.0)  # index r = 0 of the partners: unused
+    rows = np.concatenate([np.repeat(np.arange(n // 2 + 1), n), np.arange(n - 1, n // 2, -1)])
+    cols = np.concatenate([np.tile(np.arange(n), n // 2 + 1), np.full(n // 2 - 1, n // 2)])
+    geo = prep.geo
+    qx = geo.q_row.astype(np.float64)[rows][None, :]
+    qy = geo.q_col.astype(np.float64)[cols][None, :]
+    kx = geo.kx[:, None].astype(np.float64)
+    ky = geo.ky[:, None].astype(np.float64)
+    am = so._aperture_and_angles(qx - kx, qy - ky, geo)[3]
+    ap = so._aperture_and_angles(qx + kx, qy + ky, geo)[3]
+    got = np.delete(table, main, axis=1)
+    assert np.abs(got - np.stack([am, ap], axis=-1)).max() <= 2e-5
+
+
+@pytest.mark.parametrize("flags", [QSSB_FLAG_QUADRATIC, QSSB_FLAG_QUADRATIC | QSSB_FLAG_CHI_FP64, 0])
+def test_two_pass_table_loss_matches_oracle_and_table_free_kernel(big_case, flags):
+    """The quadratic float32 path reads the table; the FP64-chi and C30 paths
+    accept it and evaluate as before. Losses against the FP64 oracle and the
+    table-free kernel, mean phases against the table-free kernel."""
+    prep, cal, d = big_case
+    table = ops.overlap_table(d["geom"], d["q_row"], d["q_col"], cal)
+    rows = CANDS if flags else [(-120.0, 55.0, math.radians(17.0)), (40.0, 20.0, 0.4)]
+    c30 = 0.0 if flags else 3.0e4
+    cands = torch.tensor([[a, b, c, c30] for a, b, c in rows], dtype=torch.float32, device=DEV)
+    losses, mp = ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands,
+                                flags=flags, want_mean_phase=True, overlap=table)
+    plain, mp_plain = ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands,
+                                     flags=flags, want_mean_phase=True)
+    losses, mp, plain = losses.cpu().numpy(), mp.cpu().numpy(), plain.cpu().numpy()
+    for i, (a, b, c) in enumerate(rows):
+        ref_loss, _ = so.phase_variance_loss(prep.g_half, prep.geo,
+                                             so.Aberrations(a, b, c, C30=c30), prep.dc)
+        assert losses[i] == pytest.approx(ref_loss, rel=LOSS_RTOL, abs=LOSS_ATOL), (i, flags)
+        assert losses[i] == pytest.approx(plain[i], rel=2e-6, abs=1e-7)
+    np.testing.assert_allclose(mp, mp_plain.cpu().numpy(), rtol=0, atol=2e-5)
+
+
+def test_two_pass_table_rejects_a_wrong_size(big_case):
+    prep, cal, d = big_case
+    table = ops.overlap_table(d["geom"], d["q_row"], d["q_col"], cal)
+    cands = _cands(CANDS[:1])
+    with pytest.raises(ValueError):
+        ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands,
+                       flags=QSSB_FLAG_QUADRATIC, overlap=table[:, :-1].contiguous())
+
+
+def test_backend_builds_the_256_table_and_agrees_without_it():
+    counts = disk_input(123, scan=(256, 256))
+    be = B200SSBBackend(torch.as_tensor(counts, device=DEV), semiangle=21.4, scan_sampling=0.5,
+                        det_sampling=1.0, voltage_kV=300, bf_radius=3)
+    c1 = np.linspace(-100.0, 100.0, 9)
+    with_table = be.variance_loss_batch(c1, 20.0, 0.3).cpu().numpy()
+    assert be._overlap_table() is not None
+    be.use_overlap_table = False
+    assert be._overlap_table() is None
+    without = be.variance_loss_batch(c1, 20.0, 0.3).cpu().numpy()
+    np.testing.assert_allclose(with_table, without, rtol=2e-6, atol=1e-7)
+    be.close()
