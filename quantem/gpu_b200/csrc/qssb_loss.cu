@@ -1030,13 +1030,23 @@ constexpr size_t kStageBudget = 32u << 20;
 
 // Rows per CTA of the row pass and columns per CTA of the column pass (one
 // warp each): 16, or 8 at 1024 where a lane holds 32 values of its line.
-__host__ __device__ constexpr int row_warps(int n) { return n >= 1024 ? 8 : 16; }
+// Row pass shape: warps per CTA, CTAs per SM asked of the compiler, and the
+// elements whose loads are issued before their math. At 256^2 three 8-warp
+// CTAs per SM (80 registers) hide more latency than one 16-warp CTA at 128.
+__host__ __device__ constexpr int row_warps(int n) { return n >= 1024 ? 8 : (n == 256 ? 8 : 16); }
+__host__ __device__ constexpr int row_min_ctas(int n) { return n == 256 ? 3 : 1; }
+__host__ __device__ constexpr int row_load_batch(int n) { return n == 256 ? 4 : 8; }
 __host__ __device__ constexpr int col_tile(int n) { return n >= 1024 ? 8 : 16; }
 
 template <int N, bool FULL>
 struct TwoPass {
     static constexpr int rows = FULL ? N : N / 2 + 1;
     static constexpr int rwarps = row_warps(N);
+    // at 256^2 the half set's Nyquist row N/2 is taken by warp 0 of the first
+    // CTA after its row 0, so the rows 0 .. N/2 - 1 fill whole CTAs (17 CTAs
+    // of 8 warps would leave one CTA a single row)
+    static constexpr bool fold_nyquist = !FULL && N == 256;
+    static constexpr int row_ctas = fold_nyquist ? N / 2 / rwarps : (rows + rwarps - 1) / rwarps;
     static constexpr int tile = col_tile(N);
     static constexpr int scratch = warp_fft_scratch<N>();
     // column line pitch: odd mod 16 (conflict-free strip loads), and room for
@@ -1068,11 +1078,12 @@ static TwoPassPlan plan_two_pass(int n, bool full, int n_bf, int n_cand, int chu
 }
 
 template <int N, bool CHI64, bool QUAD, bool FULL>
-__global__ void __launch_bounds__(32 * row_warps(N)) k_loss_rows(
+__global__ void __launch_bounds__(32 * row_warps(N), row_min_ctas(N)) k_loss_rows(
     const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
     const float* __restrict__ q_row, const float* __restrict__ q_col, const void* __restrict__ cands,
-    qssb_calibration_t cal, const float2* __restrict__ eq_table, int b0, int nb_chunk,
-    float2* __restrict__ stage, float2* __restrict__ delta, const float2* __restrict__ overlap) {
+    qssb_calibration_t cal, const Probe* __restrict__ probes, const float2* __restrict__ twg,
+    const float2* __restrict__ eq_table, int b0, int nb_chunk, float2* __restrict__ stage,
+    float2* __restrict__ delta, const float2* __restrict__ overlap) {
     using TP = TwoPass<N, FULL>;
     constexpr int H = N / 2 + 1;
     constexpr int RW = TP::rwarps;
@@ -1093,18 +1104,18 @@ __global__ void __launch_bounds__(32 * row_warps(N)) k_loss_rows(
     const int b = b0 + bi;
     const int cand = blockIdx.z;
     const int r0 = blockIdx.x * RW;
-    const int r = r0 + warp;
-    if (tid == 0) {
-        if constexpr (FULL) {
+    {  // the candidate's probe and the twiddles, from k_two_pass_setup
+        const auto* src = reinterpret_cast<const unsigned int*>(probes + cand);
+        auto* dst = reinterpret_cast<unsigned int*>(&sp);
+        for (int i = tid; i < (int)(sizeof(Probe) / 4); i += 32 * RW) dst[i] = __ldg(src + i);
+        for (int i = tid; i < N; i += 32 * RW) tw[i] = __ldg(twg + i);
+    }
+    if constexpr (FULL) {
+        if (tid == 0) {
             const auto* fc = static_cast<const qssb_full_aberrations_t*>(cands) + cand;
-            sp = make_probe_common(cal, 0.0f, 0.0f, 0.0f, 0.0f);
             make_full_chi(fc->magnitude, fc->angle_rad, cal.wavelength_A, sf, sd);
-        } else {
-            const qssb_aberrations_t ab = static_cast<const qssb_aberrations_t*>(cands)[cand];
-            sp = make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
         }
     }
-    fill_twiddles<N>(tw, tid, 32 * RW);
     __syncthreads();
     const Probe& p = sp;
     const BFQuad kq = bf_quad(geom, n_bf, b, p);
@@ -1129,7 +1140,6 @@ __global__ void __launch_bounds__(32 * row_warps(N)) k_loss_rows(
         }
         __syncthreads();
     }
-    if (r >= TP::rows) return;  // warp-uniform; no block barrier follows
     const float2* gb = g + (size_t)b * N * H;
     const float2* eqc = eq_table + (size_t)cand * N * N;
     const float2 dc = make_float2((float)cal.dc_re, (float)cal.dc_im);
@@ -1154,57 +1164,78 @@ __global__ void __launch_bounds__(32 * row_warps(N)) k_loss_rows(
             return corrected<CHI64>(qx, qy, rr, c, kq.kx, kq.ky, kq.kx_lo, kq.ky_lo, pk, gv, p);
         }
     };
-    const float2 e_row = kSep ? s_phr[warp] : make_float2(1.0f, 0.0f);
-    const float qx = __ldg(q_row + r);
     // with the per-geometry table the apertures are read, not evaluated
     const bool tab = kSep && overlap != nullptr;
     const float2* ovb = tab ? overlap + (size_t)b * two_pass_table_elems<N>() : nullptr;
-    float2 v[RPL];
-    constexpr int kBatch = 8;  // loads of 8 elements issued before their math
+    // one row per warp (e_row: the row's separable phase factor)
+    auto row = [&](const int r, const float2 e_row) {
+        const float qx = __ldg(q_row + r);
+        float2 v[RPL];
+        constexpr int kBatch = row_load_batch(N);  // loads issued before their math
 #pragma unroll
-    for (int t0 = 0; t0 < RPL; t0 += kBatch) {
-        float2 gv[kBatch], eq[kBatch], ov[kBatch];
-        float qy[kBatch];
+        for (int t0 = 0; t0 < RPL; t0 += kBatch) {
+            float2 gv[kBatch], eq[kBatch], ov[kBatch];
+            float qy[kBatch];
 #pragma unroll
-        for (int u = 0; u < kBatch; ++u) {
-            const int c = lane + 32 * (t0 + u);
-            gv[u] = load_g(r, c);
-            qy[u] = __ldg(q_col + c);
-            eq[u] = QUAD && !FULL ? __ldg(eqc + r * N + c) : make_float2(1.0f, 0.0f);
-            ov[u] = tab ? __ldg(ovb + r * N + c) : make_float2(0.0f, 0.0f);
-        }
-#pragma unroll
-        for (int u = 0; u < kBatch; ++u) {
-            const int t = t0 + u;
-            const int c = lane + 32 * t;
-            if (tab) {
-                v[t] = (r == 0 && c == 0)
-                           ? dc
-                           : corrected_table(ov[u], eq[u], cmul(e_row, s_phc[c]), kq.ak, gv[u]);
-            } else {
-                v[t] = (r == 0 && c == 0) ? dc : eval(r, c, qx, qy[u], gv[u], eq[u], e_row);
+            for (int u = 0; u < kBatch; ++u) {
+                const int c = lane + 32 * (t0 + u);
+                gv[u] = load_g(r, c);
+                qy[u] = __ldg(q_col + c);
+                eq[u] = QUAD && !FULL ? __ldg(eqc + r * N + c) : make_float2(1.0f, 0.0f);
+                ov[u] = tab ? __ldg(ovb + r * N + c) : make_float2(0.0f, 0.0f);
             }
-            if (!FULL && t == N / 64 && lane == 0 && r >= 1 && r < N / 2) {  // c == N/2
-                float2 e_neg = make_float2(1.0f, 0.0f);
-                if constexpr (kSep) {
-                    float sn, cs;
-                    sincosf(2.0f * __ldg(q_row + N - r) * kq.u, &sn, &cs);
-                    e_neg = make_float2(cs, sn);
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u) {
+                const int t = t0 + u;
+                const int c = lane + 32 * t;
+                if (tab) {
+                    v[t] = (r == 0 && c == 0)
+                               ? dc
+                               : corrected_table(ov[u], eq[u], cmul(e_row, s_phc[c]), kq.ak,
+                                                 gv[u]);
+                } else {
+                    v[t] = (r == 0 && c == 0) ? dc : eval(r, c, qx, qy[u], gv[u], eq[u], e_row);
                 }
-                const float2 eqn = QUAD && !FULL ? __ldg(eqc + (N - r) * N + N / 2) : make_float2(1.0f, 0.0f);
-                const float2 partner =
-                    tab ? corrected_table(__ldg(ovb + (N / 2 + 1) * N + r), eqn,
-                                          cmul(e_neg, s_phc[N / 2]), kq.ak, load_g(N - r, N / 2))
-                        : eval(N - r, N / 2, __ldg(q_row + N - r), qy[u], load_g(N - r, N / 2),
-                               eqn, e_neg);
-                delta[((size_t)cand * nb_chunk + bi) * (N / 2) + r] = cadd(cconj(v[t]), partner);
+                if (!FULL && t == N / 64 && lane == 0 && r >= 1 && r < N / 2) {  // c == N/2
+                    float2 e_neg = make_float2(1.0f, 0.0f);
+                    if constexpr (kSep) {
+                        float sn, cs;
+                        sincosf(2.0f * __ldg(q_row + N - r) * kq.u, &sn, &cs);
+                        e_neg = make_float2(cs, sn);
+                    }
+                    const float2 eqn = QUAD && !FULL ? __ldg(eqc + (N - r) * N + N / 2)
+                                                     : make_float2(1.0f, 0.0f);
+                    const float2 partner =
+                        tab ? corrected_table(__ldg(ovb + (N / 2 + 1) * N + r), eqn,
+                                              cmul(e_neg, s_phc[N / 2]), kq.ak,
+                                              load_g(N - r, N / 2))
+                            : eval(N - r, N / 2, __ldg(q_row + N - r), qy[u], load_g(N - r, N / 2),
+                                   eqn, e_neg);
+                    delta[((size_t)cand * nb_chunk + bi) * (N / 2) + r] =
+                        cadd(cconj(v[t]), partner);
+                }
             }
+        }
+        warp_fft<N, +1>(v, scr + warp * TP::scratch, tw, lane);
+        float2* out = stage + (((size_t)cand * nb_chunk + bi) * TP::rows + r) * N;
+#pragma unroll
+        for (int j = 0; j < RPL; ++j) out[warp_fft_index<N>(lane, j)] = v[j];
+    };
+    const int r = r0 + warp;
+    if (r < TP::rows) row(r, kSep ? s_phr[warp] : make_float2(1.0f, 0.0f));
+    if constexpr (TP::fold_nyquist) {
+        static_assert(TP::row_ctas * RW == N / 2, "whole CTAs of rows");
+        if (blockIdx.x == 0 && warp == 0) {
+            __syncwarp();  // the FFT scratch is reused by the Nyquist row
+            float2 e_row = make_float2(1.0f, 0.0f);
+            if constexpr (kSep) {
+                float sn, cs;
+                sincosf(2.0f * __ldg(q_row + N / 2) * kq.u, &sn, &cs);
+                e_row = make_float2(cs, sn);
+            }
+            row(N / 2, e_row);
         }
     }
-    warp_fft<N, +1>(v, scr + warp * TP::scratch, tw, lane);
-    float2* out = stage + (((size_t)cand * nb_chunk + bi) * TP::rows + r) * N;
-#pragma unroll
-    for (int j = 0; j < RPL; ++j) out[warp_fft_index<N>(lane, j)] = v[j];
 }
 
 __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
@@ -1214,8 +1245,8 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) 
 
 template <int N, bool FULL>
 __global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
-    const float2* __restrict__ stage, const float2* __restrict__ delta, int nb_chunk, int n_sub,
-    int first, float* __restrict__ part) {
+    const float2* __restrict__ stage, const float2* __restrict__ delta,
+    const float2* __restrict__ twg, int nb_chunk, int n_sub, int first, float* __restrict__ part) {
     using TP = TwoPass<N, FULL>;
     constexpr int P = TP::pitch;
     constexpr int RPL = N / 32;
@@ -1232,7 +1263,7 @@ __global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
     const int cand = blockIdx.z;
     const int x = x0 + warp;
     const float sign = (x & 1) ? -1.0f : 1.0f;
-    fill_twiddles<N>(tw, tid, NT);
+    for (int i = tid; i < N; i += NT) tw[i] = __ldg(twg + i);
     auto issue = [&](int bi, float2* dst) {
         const float2* S = stage + ((size_t)cand * nb_chunk + bi) * TP::rows * N + x0;
         for (int e = tid; e < TP::rows * kColTile; e += NT) {
@@ -1305,6 +1336,7 @@ struct LossPlan {
     size_t eq_bytes;
     size_t stage_bytes;  // N >= 256: row-transformed planes of one chunk
     size_t delta_bytes;  // N >= 256, half set: Nyquist-column deviations
+    size_t setup_bytes;  // N >= 256: per-candidate probes and the N twiddles
 };
 
 // Deterministic: about 296 CTAs in total (two per B200 SM), at least one BF
@@ -1319,6 +1351,9 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool 
         const size_t rows = full ? (size_t)n : (size_t)(n / 2 + 1);
         pl.stage_bytes = sizeof(float2) * rows * n * (size_t)tp.chunk_bf * n_cand;
         pl.delta_bytes = full ? 0 : sizeof(float2) * (size_t)(n / 2) * tp.chunk_bf * n_cand;
+        pl.delta_bytes = (pl.delta_bytes + 255) & ~(size_t)255;
+        pl.setup_bytes = ((sizeof(Probe) * (size_t)n_cand + 255) & ~(size_t)255) +
+                         sizeof(float2) * (size_t)n;
     } else if (n == 128 && chunks_req <= 0) {
         // one 512-thread CTA per SM: pick the chunking whose waves are
         // fullest - minimise waves x (pairs per CTA + one pair's worth of
@@ -1348,6 +1383,7 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool 
         pl.chunk_bf = 0;
         pl.stage_bytes = 0;
         pl.delta_bytes = 0;
+        pl.setup_bytes = 0;
     } else {
         int chunks = chunks_req > 0 ? chunks_req : (296 + n_cand - 1) / n_cand;
         if (chunks < 1) chunks = 1;
@@ -1357,6 +1393,7 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool 
         pl.chunk_bf = 0;
         pl.stage_bytes = 0;
         pl.delta_bytes = 0;
+        pl.setup_bytes = 0;
     }
     pl.part_bytes = sizeof(float) * 2 * (size_t)n * n * pl.n_chunks * n_cand;
     pl.part_bytes = (pl.part_bytes + 255) & ~(size_t)255;
@@ -1367,7 +1404,28 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool 
 }
 
 static size_t loss_workspace(const LossPlan& pl) {
-    return pl.part_bytes + pl.var_bytes + pl.eq_bytes + pl.stage_bytes + pl.delta_bytes;
+    return pl.part_bytes + pl.var_bytes + pl.eq_bytes + pl.stage_bytes + pl.delta_bytes +
+           pl.setup_bytes;
+}
+
+// Once per batch: every candidate's probe parameters (FP64 divisions and the
+// FP64 cos/sin of 2 phi12) and the N FFT twiddles, so that the row and column
+// CTAs start by copying them instead of evaluating them in a serial prologue.
+template <int N, bool FULL>
+__global__ void __launch_bounds__(128) k_two_pass_setup(const void* __restrict__ cands,
+                                                         qssb_calibration_t cal, int n_cand,
+                                                         Probe* __restrict__ probes,
+                                                         float2* __restrict__ tw) {
+    const int i = blockIdx.x * 128 + threadIdx.x;
+    if (i < n_cand) {
+        if constexpr (FULL) {
+            probes[i] = make_probe_common(cal, 0.0f, 0.0f, 0.0f, 0.0f);
+        } else {
+            const qssb_aberrations_t ab = static_cast<const qssb_aberrations_t*>(cands)[i];
+            probes[i] = make_probe_common(cal, ab.C10, ab.C12, ab.phi12, ab.C30);
+        }
+    }
+    fill_twiddles<N>(tw, i, (int)(gridDim.x * 128));
 }
 
 // The N >= 256 launch sequence after the eq table: row and column passes per
@@ -1380,6 +1438,9 @@ static int launch_two_pass(const float* g_half, const float* geom, const float* 
     using TP = TwoPass<N, FULL>;
     float2* stage = reinterpret_cast<float2*>(stage_base);
     float2* delta = reinterpret_cast<float2*>(stage_base + pl.stage_bytes);
+    Probe* probes = reinterpret_cast<Probe*>(stage_base + pl.stage_bytes + pl.delta_bytes);
+    float2* twg = reinterpret_cast<float2*>(stage_base + pl.stage_bytes + pl.delta_bytes +
+                                            pl.setup_bytes - sizeof(float2) * N);
     CUDA_TRY(cudaFuncSetAttribute(k_loss_rows<N, CHI64, QUAD, FULL>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP::row_smem));
     CUDA_TRY(cudaFuncSetAttribute(k_loss_cols<N, FULL>,
@@ -1391,16 +1452,21 @@ static int launch_two_pass(const float* g_half, const float* geom, const float* 
                                   cudaFuncAttributePreferredSharedMemoryCarveout,
                                   (int)cudaSharedmemCarveoutMaxShared));
     const auto* g = reinterpret_cast<const float2*>(g_half);
+    {
+        const int n = n_cand > N ? n_cand : N;
+        { k_two_pass_setup<N, FULL><<<(n + 127) / 128, 128, 0, s>>>(cands, cal, n_cand, probes, twg); note_launch(); }
+        CUDA_TRY(cudaGetLastError());
+    }
     for (int b0 = 0; b0 < cal.n_bf; b0 += pl.chunk_bf) {
         const int nb = cal.n_bf - b0 < pl.chunk_bf ? cal.n_bf - b0 : pl.chunk_bf;
         { k_loss_rows<N, CHI64, QUAD, FULL>
-            <<<dim3((TP::rows + TP::rwarps - 1) / TP::rwarps, nb, n_cand), 32 * TP::rwarps,
-               TP::row_smem, s>>>(g, cal.n_bf, geom, q_row, q_col, cands, cal, eq, b0, nb, stage,
-                                  delta, overlap); note_launch(); }
+            <<<dim3(TP::row_ctas, nb, n_cand), 32 * TP::rwarps,
+               TP::row_smem, s>>>(g, cal.n_bf, geom, q_row, q_col, cands, cal, probes, twg, eq, b0,
+                                  nb, stage, delta, overlap); note_launch(); }
         CUDA_TRY(cudaGetLastError());
         { k_loss_cols<N, FULL><<<dim3(N / TP::tile, pl.n_chunks, n_cand), 32 * TP::tile,
-                               TP::col_smem, s>>>(stage, delta, nb, pl.n_chunks, b0 == 0 ? 1 : 0,
-                                                  part); note_launch(); }
+                               TP::col_smem, s>>>(stage, delta, twg, nb, pl.n_chunks,
+                                                  b0 == 0 ? 1 : 0, part); note_launch(); }
         CUDA_TRY(cudaGetLastError());
     }
     return QSSB_OK;
