@@ -1057,20 +1057,30 @@ struct TwoPass {
 };
 
 struct TwoPassPlan {
+    int group;     // candidates per launch sequence
     int chunk_bf;  // BF pixels per (rows, columns) launch pair
     int n_sub;     // column-pass interleave = partial planes per candidate
 };
 
+// Candidates go through the passes in groups whose column pass is about 256
+// CTAs (16 candidates at 256^2, 8 at 512^2), so that a chunk of the staging
+// budget holds several BF pixels per candidate and each column CTA folds them
+// into its moments before one read-modify-write of its partial planes (a
+// whole 64-candidate batch at once leaves one pixel per chunk).
 static TwoPassPlan plan_two_pass(int n, bool full, int n_bf, int n_cand, int chunks_req) {
     TwoPassPlan tp;
+    const int strips = n / col_tile(n);
+    int group = 256 / strips;
+    if (group < 1) group = 1;
+    if (group > n_cand) group = n_cand;
+    tp.group = group;
     const size_t per_bf = sizeof(float2) * (size_t)(full ? n : n / 2 + 1) * n;
-    long long c = (long long)(kStageBudget / (per_bf * (size_t)n_cand));
+    long long c = (long long)(kStageBudget / (per_bf * (size_t)group));
     if (c < 1) c = 1;
     if (c > n_bf) c = n_bf;
     tp.chunk_bf = (int)c;
-    const int strips = n / col_tile(n);
     // whole waves of two CTAs per SM (148 SMs), not a last partial wave
-    int sub = chunks_req > 0 ? chunks_req : 296 / (strips * n_cand);
+    int sub = chunks_req > 0 ? chunks_req : 296 / (strips * group);
     if (sub < 1) sub = 1;
     if (sub > tp.chunk_bf) sub = tp.chunk_bf;
     tp.n_sub = sub;
@@ -1082,8 +1092,8 @@ __global__ void __launch_bounds__(32 * row_warps(N), row_min_ctas(N)) k_loss_row
     const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
     const float* __restrict__ q_row, const float* __restrict__ q_col, const void* __restrict__ cands,
     qssb_calibration_t cal, const Probe* __restrict__ probes, const float2* __restrict__ twg,
-    const float2* __restrict__ eq_table, int b0, int nb_chunk, float2* __restrict__ stage,
-    float2* __restrict__ delta, const float2* __restrict__ overlap) {
+    const float2* __restrict__ eq_table, int cand0, int b0, int nb_chunk,
+    float2* __restrict__ stage, float2* __restrict__ delta, const float2* __restrict__ overlap) {
     using TP = TwoPass<N, FULL>;
     constexpr int H = N / 2 + 1;
     constexpr int RW = TP::rwarps;
@@ -1102,7 +1112,8 @@ __global__ void __launch_bounds__(32 * row_warps(N), row_min_ctas(N)) k_loss_row
     const int warp = tid >> 5;
     const int bi = blockIdx.y;
     const int b = b0 + bi;
-    const int cand = blockIdx.z;
+    const int zc = blockIdx.z;  // the candidate within the group (staging index)
+    const int cand = cand0 + zc;
     const int r0 = blockIdx.x * RW;
     {  // the candidate's probe and the twiddles, from k_two_pass_setup
         const auto* src = reinterpret_cast<const unsigned int*>(probes + cand);
@@ -1211,13 +1222,13 @@ __global__ void __launch_bounds__(32 * row_warps(N), row_min_ctas(N)) k_loss_row
                                               load_g(N - r, N / 2))
                             : eval(N - r, N / 2, __ldg(q_row + N - r), qy[u], load_g(N - r, N / 2),
                                    eqn, e_neg);
-                    delta[((size_t)cand * nb_chunk + bi) * (N / 2) + r] =
+                    delta[((size_t)zc * nb_chunk + bi) * (N / 2) + r] =
                         cadd(cconj(v[t]), partner);
                 }
             }
         }
         warp_fft<N, +1>(v, scr + warp * TP::scratch, tw, lane);
-        float2* out = stage + (((size_t)cand * nb_chunk + bi) * TP::rows + r) * N;
+        float2* out = stage + (((size_t)zc * nb_chunk + bi) * TP::rows + r) * N;
 #pragma unroll
         for (int j = 0; j < RPL; ++j) out[warp_fft_index<N>(lane, j)] = v[j];
     };
@@ -1246,7 +1257,8 @@ __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) 
 template <int N, bool FULL>
 __global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
     const float2* __restrict__ stage, const float2* __restrict__ delta,
-    const float2* __restrict__ twg, int nb_chunk, int n_sub, int first, float* __restrict__ part) {
+    const float2* __restrict__ twg, int cand0, int nb_chunk, int n_sub, int first,
+    float* __restrict__ part) {
     using TP = TwoPass<N, FULL>;
     constexpr int P = TP::pitch;
     constexpr int RPL = N / 32;
@@ -1260,12 +1272,13 @@ __global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
     const int warp = tid >> 5;
     const int x0 = blockIdx.x * kColTile;
     const int sub = blockIdx.y;
-    const int cand = blockIdx.z;
+    const int zc = blockIdx.z;  // the candidate within the group (staging index)
+    const int cand = cand0 + zc;
     const int x = x0 + warp;
     const float sign = (x & 1) ? -1.0f : 1.0f;
     for (int i = tid; i < N; i += NT) tw[i] = __ldg(twg + i);
     auto issue = [&](int bi, float2* dst) {
-        const float2* S = stage + ((size_t)cand * nb_chunk + bi) * TP::rows * N + x0;
+        const float2* S = stage + ((size_t)zc * nb_chunk + bi) * TP::rows * N + x0;
         for (int e = tid; e < TP::rows * kColTile; e += NT) {
             const int rr = e / kColTile;
             const int c = e - rr * kColTile;
@@ -1286,7 +1299,7 @@ __global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
         if (bi + n_sub < nb_chunk) issue(bi + n_sub, tiles + (buf ^ 1) * kColTile * P);
         float2* line = tiles + buf * kColTile * P + warp * P;
         if constexpr (!FULL) {
-            const float2* d = delta + ((size_t)cand * nb_chunk + bi) * (N / 2);
+            const float2* d = delta + ((size_t)zc * nb_chunk + bi) * (N / 2);
 #pragma unroll
             for (int t = 0; t < RPL; ++t) {
                 const int rr = lane + 32 * t;
@@ -1331,6 +1344,7 @@ struct LossPlan {
     int bf_per_chunk;
     int n_chunks;      // partial planes per candidate
     int chunk_bf;      // N >= 256: BF pixels per row/column launch pair
+    int group;         // N >= 256: candidates per row/column launch pair
     size_t part_bytes;
     size_t var_bytes;
     size_t eq_bytes;
@@ -1349,8 +1363,9 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool 
         pl.n_chunks = tp.n_sub;
         pl.bf_per_chunk = 0;
         const size_t rows = full ? (size_t)n : (size_t)(n / 2 + 1);
-        pl.stage_bytes = sizeof(float2) * rows * n * (size_t)tp.chunk_bf * n_cand;
-        pl.delta_bytes = full ? 0 : sizeof(float2) * (size_t)(n / 2) * tp.chunk_bf * n_cand;
+        pl.group = tp.group;
+        pl.stage_bytes = sizeof(float2) * rows * n * (size_t)tp.chunk_bf * tp.group;
+        pl.delta_bytes = full ? 0 : sizeof(float2) * (size_t)(n / 2) * tp.chunk_bf * tp.group;
         pl.delta_bytes = (pl.delta_bytes + 255) & ~(size_t)255;
         pl.setup_bytes = ((sizeof(Probe) * (size_t)n_cand + 255) & ~(size_t)255) +
                          sizeof(float2) * (size_t)n;
@@ -1381,6 +1396,7 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool 
         pl.bf_per_chunk = best_bpc;
         pl.n_chunks = (n_bf + best_bpc - 1) / best_bpc;
         pl.chunk_bf = 0;
+        pl.group = 0;
         pl.stage_bytes = 0;
         pl.delta_bytes = 0;
         pl.setup_bytes = 0;
@@ -1391,6 +1407,7 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool 
         pl.bf_per_chunk = (n_bf + chunks - 1) / chunks;
         pl.n_chunks = (n_bf + pl.bf_per_chunk - 1) / pl.bf_per_chunk;
         pl.chunk_bf = 0;
+        pl.group = 0;
         pl.stage_bytes = 0;
         pl.delta_bytes = 0;
         pl.setup_bytes = 0;
@@ -1457,17 +1474,20 @@ static int launch_two_pass(const float* g_half, const float* geom, const float* 
         { k_two_pass_setup<N, FULL><<<(n + 127) / 128, 128, 0, s>>>(cands, cal, n_cand, probes, twg); note_launch(); }
         CUDA_TRY(cudaGetLastError());
     }
-    for (int b0 = 0; b0 < cal.n_bf; b0 += pl.chunk_bf) {
-        const int nb = cal.n_bf - b0 < pl.chunk_bf ? cal.n_bf - b0 : pl.chunk_bf;
-        { k_loss_rows<N, CHI64, QUAD, FULL>
-            <<<dim3(TP::row_ctas, nb, n_cand), 32 * TP::rwarps,
-               TP::row_smem, s>>>(g, cal.n_bf, geom, q_row, q_col, cands, cal, probes, twg, eq, b0,
-                                  nb, stage, delta, overlap); note_launch(); }
-        CUDA_TRY(cudaGetLastError());
-        { k_loss_cols<N, FULL><<<dim3(N / TP::tile, pl.n_chunks, n_cand), 32 * TP::tile,
-                               TP::col_smem, s>>>(stage, delta, twg, nb, pl.n_chunks,
-                                                  b0 == 0 ? 1 : 0, part); note_launch(); }
-        CUDA_TRY(cudaGetLastError());
+    for (int c0 = 0; c0 < n_cand; c0 += pl.group) {
+        const int nc = n_cand - c0 < pl.group ? n_cand - c0 : pl.group;
+        for (int b0 = 0; b0 < cal.n_bf; b0 += pl.chunk_bf) {
+            const int nb = cal.n_bf - b0 < pl.chunk_bf ? cal.n_bf - b0 : pl.chunk_bf;
+            { k_loss_rows<N, CHI64, QUAD, FULL>
+                <<<dim3(TP::row_ctas, nb, nc), 32 * TP::rwarps, TP::row_smem, s>>>(
+                    g, cal.n_bf, geom, q_row, q_col, cands, cal, probes, twg, eq, c0, b0, nb,
+                    stage, delta, overlap); note_launch(); }
+            CUDA_TRY(cudaGetLastError());
+            { k_loss_cols<N, FULL><<<dim3(N / TP::tile, pl.n_chunks, nc), 32 * TP::tile,
+                                   TP::col_smem, s>>>(stage, delta, twg, c0, nb, pl.n_chunks,
+                                                      b0 == 0 ? 1 : 0, part); note_launch(); }
+            CUDA_TRY(cudaGetLastError());
+        }
     }
     return QSSB_OK;
 }
