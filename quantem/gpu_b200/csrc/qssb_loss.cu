@@ -1054,6 +1054,15 @@ struct TwoPass {
     static constexpr int pitch = (scratch > N ? scratch : N) | 1;
     static constexpr size_t row_smem = sizeof(float2) * ((size_t)rwarps * scratch + N);
     static constexpr size_t col_smem = sizeof(float2) * ((size_t)2 * tile * pitch + N);
+    // half set at 256^2: column pairs (k_loss_cols_pair), a warp per pair of
+    // the strip's columns; two adjacent lines hold one warp FFT's scratch
+    static constexpr bool pair_cols = !FULL && N == 256;
+    static constexpr int pair_warps = tile / 2;
+    static constexpr int pair_pitch = (rows > (scratch + 1) / 2 ? rows : (scratch + 1) / 2) | 1;
+    static constexpr size_t col_pair_smem =
+        sizeof(float2) * ((size_t)2 * tile * pair_pitch + N) + sizeof(float) * (size_t)pair_warps * N;
+    // CTAs per SM of the column pass, for the plan's wave arithmetic
+    static constexpr int col_ctas_per_sm = pair_cols ? 3 : 2;
 };
 
 struct TwoPassPlan {
@@ -1062,15 +1071,19 @@ struct TwoPassPlan {
     int n_sub;     // column-pass interleave = partial planes per candidate
 };
 
-// Candidates go through the passes in groups whose column pass is about 256
-// CTAs (16 candidates at 256^2, 8 at 512^2), so that a chunk of the staging
-// budget holds several BF pixels per candidate and each column CTA folds them
-// into its moments before one read-modify-write of its partial planes (a
-// whole 64-candidate batch at once leaves one pixel per chunk).
+// Candidates go through the passes in groups whose column pass fills one wave
+// of its CTA slots (64 candidates at 256^2: 27, 27 and 10; 16 at 512^2: 9 and
+// 7), so that a chunk of the staging budget holds several BF pixels per
+// candidate and each column CTA folds them into its moments before one
+// read-modify-write of its partial planes (a whole 64-candidate batch at once
+// leaves one pixel per chunk). Full waves beat equal groups: 27/27/10 takes
+// 1.14 ms per candidate at 256^2 against 1.24 for 22/22/20.
 static TwoPassPlan plan_two_pass(int n, bool full, int n_bf, int n_cand, int chunks_req) {
     TwoPassPlan tp;
     const int strips = n / col_tile(n);
-    int group = 256 / strips;
+    // column-pass CTA slots of the B200 (148 SMs); groups of equal size
+    const int slots = 148 * ((!full && n == 256) ? TwoPass<256, false>::col_ctas_per_sm : 2);
+    int group = slots / strips;
     if (group < 1) group = 1;
     if (group > n_cand) group = n_cand;
     tp.group = group;
@@ -1079,8 +1092,8 @@ static TwoPassPlan plan_two_pass(int n, bool full, int n_bf, int n_cand, int chu
     if (c < 1) c = 1;
     if (c > n_bf) c = n_bf;
     tp.chunk_bf = (int)c;
-    // whole waves of two CTAs per SM (148 SMs), not a last partial wave
-    int sub = chunks_req > 0 ? chunks_req : 296 / (strips * group);
+    // whole waves of the column pass's CTA slots, not a last partial wave
+    int sub = chunks_req > 0 ? chunks_req : slots / (strips * group);
     if (sub < 1) sub = 1;
     if (sub > tp.chunk_bf) sub = tp.chunk_bf;
     tp.n_sub = sub;
@@ -1340,6 +1353,139 @@ __global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
     }
 }
 
+// The column pass of the half set two columns at a time (256^2). A column
+// line L of the row-transformed half plane, completed by the +-q relation
+// L[N - r] = -conj(L[r]) + s delta_r (s = (-1)^x, delta_r the Nyquist-column
+// deviation of row r), splits into an anti-Hermitian part
+//   AL[r] = L[r] - (s/2) conj(delta_r), AL[N - r] = -conj(AL[r]),
+//   AL[0] = i Im L[0], AL[N/2] = i Im L[N/2],
+// whose transform is purely imaginary, and a Hermitian part whose transform
+// is real: Re L[0] + (-1)^y Re L[N/2] + s Dhat(y), with
+// Dhat(y) = Re sum_r delta_r w^{-r y} the same for every column of the BF
+// pixel. So one complex FFT of AL_a + i AL_b gives both columns' imaginary
+// parts (i Y_a - Y_b), and one FFT per BF pixel gives Dhat: about half the
+// column FFTs of k_loss_cols. Dhat is computed W pixels ahead, one per warp,
+// with the idle strip buffer as scratch.
+template <int N>
+__global__ void __launch_bounds__(16 * col_tile(N), TwoPass<N, false>::col_ctas_per_sm)
+    k_loss_cols_pair(const float2* __restrict__ stage, const float2* __restrict__ delta,
+                     const float2* __restrict__ twg, int cand0, int nb_chunk, int n_sub,
+                     int first, float* __restrict__ part) {
+    using TP = TwoPass<N, false>;
+    constexpr int P = TP::pair_pitch;
+    constexpr int RPL = N / 32;
+    constexpr int kColTile = TP::tile;
+    constexpr int W = TP::pair_warps;
+    constexpr int NT = 32 * W;
+    static_assert(TP::pair_cols && 2 * P >= TP::scratch, "pair lines hold the FFT scratch");
+    extern __shared__ float4 smem4[];
+    float2* tiles = reinterpret_cast<float2*>(smem4);  // two strips: the next one arrives by cp.async
+    float2* tw = tiles + 2 * kColTile * P;
+    float* dh = reinterpret_cast<float*>(tw + N);  // [W][N]: Dhat of the next W pixels
+    const int tid = threadIdx.x;
+    const int lane = tid & 31;
+    const int warp = tid >> 5;
+    const int x0 = blockIdx.x * kColTile;
+    const int sub = blockIdx.y;
+    const int zc = blockIdx.z;  // the candidate within the group (staging index)
+    const int cand = cand0 + zc;
+    const int xa = x0 + 2 * warp;  // even: s = +1 for column xa, -1 for xa + 1
+    for (int i = tid; i < N; i += NT) tw[i] = __ldg(twg + i);
+    auto issue = [&](int bi, float2* dst) {
+        const float2* S = stage + ((size_t)zc * nb_chunk + bi) * TP::rows * N + x0;
+        for (int e = tid; e < TP::rows * kColTile; e += NT) {
+            const int rr = e / kColTile;
+            const int c = e - rr * kColTile;
+            cp_async8(dst + c * P + rr, S + (size_t)rr * N + c);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    float asa[RPL], aqa[RPL], asb[RPL], aqb[RPL];
+#pragma unroll
+    for (int t = 0; t < RPL; ++t) asa[t] = aqa[t] = asb[t] = aqb[t] = 0.0f;
+    int buf = 0;
+    if (sub < nb_chunk) issue(sub, tiles);
+    int step = 0;
+    for (int bi = sub; bi < nb_chunk; bi += n_sub, ++step) {
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        // this strip has arrived everywhere; every warp is done with the other
+        // buffer (and tw is filled)
+        __syncthreads();
+        const int slot = step % W;
+        if (slot == 0) {  // CTA-uniform
+            const int bj = bi + warp * n_sub;
+            if (bj < nb_chunk) {
+                const float2* d = delta + ((size_t)zc * nb_chunk + bj) * (N / 2);
+                float2 v[RPL];
+#pragma unroll
+                for (int t = 0; t < RPL; ++t) {
+                    const int rr = lane + 32 * t;
+                    v[t] = rr > N / 2 ? __ldg(d + N - rr) : make_float2(0.0f, 0.0f);
+                }
+                warp_fft<N, +1>(v, tiles + (buf ^ 1) * kColTile * P + 2 * warp * P, tw, lane);
+#pragma unroll
+                for (int j = 0; j < RPL; ++j) dh[warp * N + warp_fft_index<N>(lane, j)] = v[j].x;
+            }
+            __syncthreads();
+        }
+        if (bi + n_sub < nb_chunk) issue(bi + n_sub, tiles + (buf ^ 1) * kColTile * P);
+        float2* la = tiles + buf * kColTile * P + 2 * warp * P;
+        const float2* lb = la + P;
+        const float2* d = delta + ((size_t)zc * nb_chunk + bi) * (N / 2);
+        float2 v[RPL];
+#pragma unroll
+        for (int t = 0; t < RPL; ++t) {
+            const int rr = lane + 32 * t;
+            if (rr == 0 || rr == N / 2) {
+                v[t] = make_float2(-lb[rr].y, la[rr].y);
+            } else {
+                const int rp = rr < N / 2 ? rr : N - rr;
+                const float2 dd = __ldg(d + rp);
+                const float2 a = la[rp];
+                const float2 bv = lb[rp];
+                const float ax = fmaf(-0.5f, dd.x, a.x), ay = fmaf(0.5f, dd.y, a.y);
+                const float bx = fmaf(0.5f, dd.x, bv.x), by = fmaf(-0.5f, dd.y, bv.y);
+                v[t] = rr < N / 2 ? make_float2(ax - by, ay + bx) : make_float2(-ax - by, ay - bx);
+            }
+        }
+        const float ha0 = la[0].x, haN = la[N / 2].x, hb0 = lb[0].x, hbN = lb[N / 2].x;
+        __syncwarp();  // the two lines become the FFT's transpose scratch
+        warp_fft<N, +1>(v, la, tw, lane);
+        const float* dhs = dh + slot * N;
+#pragma unroll
+        for (int j = 0; j < RPL; ++j) {
+            const int y = warp_fft_index<N>(lane, j);
+            const float sy = (y & 1) ? -1.0f : 1.0f;
+            const float dv = dhs[y];
+            const float pa = phase_atan2(v[j].y, fmaf(sy, haN, ha0) + dv);
+            const float pb = phase_atan2(-v[j].x, fmaf(sy, hbN, hb0) - dv);
+            asa[j] += pa;
+            aqa[j] = fmaf(pa, pa, aqa[j]);
+            asb[j] += pb;
+            aqb[j] = fmaf(pb, pb, aqb[j]);
+        }
+        buf ^= 1;
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    float* ps = part + ((size_t)(cand * n_sub + sub) * 2) * N * N + (size_t)xa * N;
+    float* pq = ps + (size_t)N * N;
+#pragma unroll
+    for (int j = 0; j < RPL; ++j) {
+        const int y = warp_fft_index<N>(lane, j);
+        if (first) {
+            ps[y] = asa[j];
+            pq[y] = aqa[j];
+            ps[N + y] = asb[j];
+            pq[N + y] = aqb[j];
+        } else {
+            ps[y] += asa[j];
+            pq[y] += aqa[j];
+            ps[N + y] += asb[j];
+            pq[N + y] += aqb[j];
+        }
+    }
+}
+
 struct LossPlan {
     int bf_per_chunk;
     int n_chunks;      // partial planes per candidate
@@ -1462,6 +1608,14 @@ static int launch_two_pass(const float* g_half, const float* geom, const float* 
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP::row_smem));
     CUDA_TRY(cudaFuncSetAttribute(k_loss_cols<N, FULL>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TP::col_smem));
+    if constexpr (TP::pair_cols) {
+        CUDA_TRY(cudaFuncSetAttribute(k_loss_cols_pair<N>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)TP::col_pair_smem));
+        CUDA_TRY(cudaFuncSetAttribute(k_loss_cols_pair<N>,
+                                      cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      (int)cudaSharedmemCarveoutMaxShared));
+    }
     CUDA_TRY(cudaFuncSetAttribute(k_loss_rows<N, CHI64, QUAD, FULL>,
                                   cudaFuncAttributePreferredSharedMemoryCarveout,
                                   (int)cudaSharedmemCarveoutMaxShared));
@@ -1476,16 +1630,26 @@ static int launch_two_pass(const float* g_half, const float* geom, const float* 
     }
     for (int c0 = 0; c0 < n_cand; c0 += pl.group) {
         const int nc = n_cand - c0 < pl.group ? n_cand - c0 : pl.group;
-        for (int b0 = 0; b0 < cal.n_bf; b0 += pl.chunk_bf) {
-            const int nb = cal.n_bf - b0 < pl.chunk_bf ? cal.n_bf - b0 : pl.chunk_bf;
+        // a smaller last group takes more BF pixels per chunk in the same staging
+        int chunk = pl.chunk_bf * pl.group / nc;
+        if (chunk > cal.n_bf) chunk = cal.n_bf;
+        for (int b0 = 0; b0 < cal.n_bf; b0 += chunk) {
+            const int nb = cal.n_bf - b0 < chunk ? cal.n_bf - b0 : chunk;
             { k_loss_rows<N, CHI64, QUAD, FULL>
                 <<<dim3(TP::row_ctas, nb, nc), 32 * TP::rwarps, TP::row_smem, s>>>(
                     g, cal.n_bf, geom, q_row, q_col, cands, cal, probes, twg, eq, c0, b0, nb,
                     stage, delta, overlap); note_launch(); }
             CUDA_TRY(cudaGetLastError());
-            { k_loss_cols<N, FULL><<<dim3(N / TP::tile, pl.n_chunks, nc), 32 * TP::tile,
-                                   TP::col_smem, s>>>(stage, delta, twg, c0, nb, pl.n_chunks,
-                                                      b0 == 0 ? 1 : 0, part); note_launch(); }
+            if constexpr (TP::pair_cols) {
+                { k_loss_cols_pair<N><<<dim3(N / TP::tile, pl.n_chunks, nc), 32 * TP::pair_warps,
+                                        TP::col_pair_smem, s>>>(stage, delta, twg, c0, nb,
+                                                                pl.n_chunks, b0 == 0 ? 1 : 0,
+                                                                part); note_launch(); }
+            } else {
+                { k_loss_cols<N, FULL><<<dim3(N / TP::tile, pl.n_chunks, nc), 32 * TP::tile,
+                                       TP::col_smem, s>>>(stage, delta, twg, c0, nb, pl.n_chunks,
+                                                          b0 == 0 ? 1 : 0, part); note_launch(); }
+            }
             CUDA_TRY(cudaGetLastError());
         }
     }
