@@ -1056,13 +1056,13 @@ struct TwoPass {
     static constexpr size_t col_smem = sizeof(float2) * ((size_t)2 * tile * pitch + N);
     // half set at 256^2: column pairs (k_loss_cols_pair), a warp per pair of
     // the strip's columns; two adjacent lines hold one warp FFT's scratch
-    static constexpr bool pair_cols = !FULL && N == 256;
+    static constexpr bool pair_cols = !FULL && (N == 256 || N == 512);
     static constexpr int pair_warps = tile / 2;
     static constexpr int pair_pitch = (rows > (scratch + 1) / 2 ? rows : (scratch + 1) / 2) | 1;
     static constexpr size_t col_pair_smem =
         sizeof(float2) * ((size_t)2 * tile * pair_pitch + N) + sizeof(float) * (size_t)pair_warps * N;
     // CTAs per SM of the column pass, for the plan's wave arithmetic
-    static constexpr int col_ctas_per_sm = pair_cols ? 3 : 2;
+    static constexpr int col_ctas_per_sm = pair_cols && N == 256 ? 3 : 2;
 };
 
 struct TwoPassPlan {
