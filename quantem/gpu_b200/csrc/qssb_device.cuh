@@ -549,6 +549,28 @@ __device__ __forceinline__ float2 probe_at_bf(float alpha2, float cos2, float si
 // from FP64 q and k (k = kx + kx_lo) reproduces the FP64 result there.
 constexpr float kApertureTie = 1.0e-4f;
 
+// G conj(Gamma_hat) from the displacements and apertures of q - k and q + k:
+// Gamma = P(q - k) conj(P(k)) - conj(P(q + k)) P(k), unit-normalised.
+template <bool CHI64>
+__device__ __forceinline__ float2 corrected_from_apertures(const Disp& dm, const Disp& dp, float am,
+                                                           float ap, float2 pk, float2 g,
+                                                           const Probe& p) {
+    const float2 pm = probe_from<CHI64>(dm, am, p);
+    const float2 pp = probe_from<CHI64>(dp, ap, p);
+    // t1 = pm * conj(pk); t2 = conj(pp) * pk
+    const float t1r = fmaf(pm.x, pk.x, pm.y * pk.y);
+    const float t1i = fmaf(pm.y, pk.x, -pm.x * pk.y);
+    const float t2r = fmaf(pp.x, pk.x, pp.y * pk.y);
+    const float t2i = fmaf(pp.x, pk.y, -pp.y * pk.x);
+    float gr = t1r - t2r;
+    float gi = t1i - t2i;
+    const float m2 = fmaf(gr, gr, gi * gi);
+    const float inv = m2 > 1e-16f ? rsqrtf(m2) : 1e8f;
+    gr *= inv;
+    gi *= inv;
+    return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
+}
+
 // C = G conj(Gamma_hat), Gamma = P(q-k) conj(P(k)) - conj(P(q+k)) P(k),
 // Gamma_hat = Gamma * (|Gamma|^2 > 1e-16 ? 1/|Gamma| : 1e8)
 // (gamma_mul_pk_onthefly, common.py:173-236). (r, c) index the scan
@@ -569,20 +591,7 @@ __device__ __forceinline__ float2 corrected(float qx, float qy, int r, int c, fl
         am = soft_aperture_fp64(qx64 - kx64, qy64 - ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
         ap = soft_aperture_fp64(qx64 + kx64, qy64 + ky64, p.semi_d, p.lam_d, p.ang_r_d, p.ang_c_d);
     }
-    const float2 pm = probe_from<CHI64>(dm, am, p);
-    const float2 pp = probe_from<CHI64>(dp, ap, p);
-    // t1 = pm * conj(pk); t2 = conj(pp) * pk
-    const float t1r = fmaf(pm.x, pk.x, pm.y * pk.y);
-    const float t1i = fmaf(pm.y, pk.x, -pm.x * pk.y);
-    const float t2r = fmaf(pp.x, pk.x, pp.y * pk.y);
-    const float t2i = fmaf(pp.x, pk.y, -pp.y * pk.x);
-    float gr = t1r - t2r;
-    float gi = t1i - t2i;
-    const float m2 = fmaf(gr, gr, gi * gi);
-    const float inv = m2 > 1e-16f ? rsqrtf(m2) : 1e8f;
-    gr *= inv;
-    gi *= inv;
-    return make_float2(fmaf(g.x, gr, g.y * gi), fmaf(g.y, gr, -g.x * gi));
+    return corrected_from_apertures<CHI64>(dm, dp, am, ap, pk, g, p);
 }
 
 // Probe constants of one candidate from the calibration (FP64 trig of phi12).

@@ -1173,24 +1173,32 @@ __global__ void __launch_bounds__(32 * row_warps(N), row_min_ctas(N)) k_loss_row
         return c <= N / 2 ? __ldcs(gb + rr * H + c)
                           : cconj(__ldcs(gb + ((N - rr) & (N - 1)) * H + (N - c)));
     };
-    auto eval = [&](int rr, int c, float qx, float qy, float2 gv, float2 eq,
-                    float2 e_row) -> float2 {
+    // with the per-geometry table the apertures are read, not evaluated
+    // (float32 quadratic chi, and the general chi with C30)
+    constexpr bool kTab = kSep || (!FULL && !QUAD);
+    const bool tab = kTab && overlap != nullptr;
+    const float2* ovb = tab ? overlap + (size_t)b * two_pass_table_elems<N>() : nullptr;
+    auto eval = [&](int rr, int c, float qx, float qy, float2 gv, float2 eq, float2 e_row,
+                    float2 ov) -> float2 {
         if constexpr (FULL) {
             return corrected_full<CHI64>(qx, qy, rr, c, kq.kx, kq.ky, kq.kx_lo, kq.ky_lo, pk, gv, p,
                                          sf, sd);
         } else if constexpr (kSep) {
+            if (tab) return corrected_table(ov, eq, cmul(e_row, s_phc[c]), kq.ak, gv);
             const float2 lo = make_float2(kq.kx_lo, kq.ky_lo);
             return corrected_quad_e(qx, qy, rr, c, eq, kq.kx, kq.ky, kq.ak, &lo,
                                     cmul(e_row, s_phc[c]), gv, p);
         } else if constexpr (QUAD) {
             return corrected_quad<CHI64>(qx, qy, rr, c, eq, kq, gv, p);
         } else {
+            if (tab) {
+                const Disp dm = displacement(qx - kq.kx, qy - kq.ky, p);
+                const Disp dp = displacement(qx + kq.kx, qy + kq.ky, p);
+                return corrected_from_apertures<CHI64>(dm, dp, ov.x, ov.y, pk, gv, p);
+            }
             return corrected<CHI64>(qx, qy, rr, c, kq.kx, kq.ky, kq.kx_lo, kq.ky_lo, pk, gv, p);
         }
     };
-    // with the per-geometry table the apertures are read, not evaluated
-    const bool tab = kSep && overlap != nullptr;
-    const float2* ovb = tab ? overlap + (size_t)b * two_pass_table_elems<N>() : nullptr;
     // one row per warp (e_row: the row's separable phase factor)
     auto row = [&](const int r, const float2 e_row) {
         const float qx = __ldg(q_row + r);
@@ -1212,14 +1220,7 @@ __global__ void __launch_bounds__(32 * row_warps(N), row_min_ctas(N)) k_loss_row
             for (int u = 0; u < kBatch; ++u) {
                 const int t = t0 + u;
                 const int c = lane + 32 * t;
-                if (tab) {
-                    v[t] = (r == 0 && c == 0)
-                               ? dc
-                               : corrected_table(ov[u], eq[u], cmul(e_row, s_phc[c]), kq.ak,
-                                                 gv[u]);
-                } else {
-                    v[t] = (r == 0 && c == 0) ? dc : eval(r, c, qx, qy[u], gv[u], eq[u], e_row);
-                }
+                v[t] = (r == 0 && c == 0) ? dc : eval(r, c, qx, qy[u], gv[u], eq[u], e_row, ov[u]);
                 if (!FULL && t == N / 64 && lane == 0 && r >= 1 && r < N / 2) {  // c == N/2
                     float2 e_neg = make_float2(1.0f, 0.0f);
                     if constexpr (kSep) {
@@ -1229,12 +1230,10 @@ __global__ void __launch_bounds__(32 * row_warps(N), row_min_ctas(N)) k_loss_row
                     }
                     const float2 eqn = QUAD && !FULL ? __ldg(eqc + (N - r) * N + N / 2)
                                                      : make_float2(1.0f, 0.0f);
-                    const float2 partner =
-                        tab ? corrected_table(__ldg(ovb + (N / 2 + 1) * N + r), eqn,
-                                              cmul(e_neg, s_phc[N / 2]), kq.ak,
-                                              load_g(N - r, N / 2))
-                            : eval(N - r, N / 2, __ldg(q_row + N - r), qy[u], load_g(N - r, N / 2),
-                                   eqn, e_neg);
+                    const float2 ovn =
+                        tab ? __ldg(ovb + (N / 2 + 1) * N + r) : make_float2(0.0f, 0.0f);
+                    const float2 partner = eval(N - r, N / 2, __ldg(q_row + N - r), qy[u],
+                                                load_g(N - r, N / 2), eqn, e_neg, ovn);
                     delta[((size_t)zc * nb_chunk + bi) * (N / 2) + r] =
                         cadd(cconj(v[t]), partner);
                 }
