@@ -37,6 +37,11 @@ extern "C" {
 #define QSSB_FLAG_QUADRATIC 4     /* qssb_loss_batch: every candidate has C30 == 0, so the
                                      factorised quadratic-chi overlap applies (qssb_object
                                      decides this itself from its host-side candidate) */
+#define QSSB_FLAG_PERSISTENT 8    /* qssb_loss_batch at 256^2 (float32 chi): one persistent
+                                     launch runs every row and column item of the batch
+                                     instead of a row and a column launch per BF chunk
+                                     (the same plan; the same bits with
+                                     QSSB_FLAG_QUADRATIC, float32 rounding without); slower */
 /* Tile-shape variant (another tuning knob): bits 8..11 of flags. qssb_object
  * on the quadratic-chi path: 1 = 2 adjacent frequencies per thread, 2 or 0
  * (the default) = 4, 3 = 8. Results agree to float32 rounding across

@@ -21,6 +21,7 @@ QSSB_ERR_WORKSPACE = -4
 QSSB_FLAG_CHI_FP64 = 1
 QSSB_FLAG_FULL_PLANE = 2
 QSSB_FLAG_QUADRATIC = 4
+QSSB_FLAG_PERSISTENT = 8
 QSSB_NOALLOC_SCRATCH_BYTES = 16 << 20
 QSSB_FLAG_CHUNKS_SHIFT = 16
 QSSB_FLAG_CHUNKS_MAX = 32767

@@ -15,6 +15,7 @@
 // Partial moment planes per chunk are folded in a fixed order in FP64
 // (k_loss_reduce), and the per-pixel variance is averaged (k_loss_final):
 // repeated calls give identical bits.
+#include <limits.h>
 #include <math.h>
 
 #include "qssb_internal.h"
@@ -440,10 +441,12 @@ __global__ void __launch_bounds__(kReducePix * kReduceSlices) k_loss_reduce(
     }
 }
 
-// L = (sum of the block sums, fixed order) / N^2.
+// L = (sum of the block sums, fixed order) / N^2; NaN when status (the
+// persistent loss's abort word, or null) is set.
 __global__ void __launch_bounds__(256) k_loss_final(const double* __restrict__ block_var,
                                                     int n_blocks, int npos,
-                                                    float* __restrict__ losses) {
+                                                    float* __restrict__ losses,
+                                                    const int* __restrict__ status = nullptr) {
     __shared__ double red[256];
     const int cand = blockIdx.x;
     const double* v = block_var + (size_t)cand * n_blocks;
@@ -455,7 +458,9 @@ __global__ void __launch_bounds__(256) k_loss_final(const double* __restrict__ b
         if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
         __syncthreads();
     }
-    if (threadIdx.x == 0) losses[cand] = (float)(red[0] / (double)npos);
+    if (threadIdx.x == 0)
+        losses[cand] = (status && *status != 0) ? __int_as_float(0x7fc00000)
+                                                : (float)(red[0] / (double)npos);
 }
 
 // ---------------------------------------- N = 128 with the overlap table
@@ -1027,6 +1032,19 @@ __global__ void __launch_bounds__(256) k_loss_final_sq(const double* __restrict_
 //     own partial planes (column-major), so every element has one writer.
 constexpr int kL256 = 256;
 constexpr size_t kStageBudget = 32u << 20;
+// The persistent one-launch loss (k_loss_queue, QSSB_FLAG_PERSISTENT): 256^2,
+// half set, float32 chi, at most this many candidate groups (27 candidates each).
+constexpr int kQueueN = 256;
+constexpr int kQueueMaxGroups = 16;
+// Queue words: the ticket, the abort word, then per chunk the completed row
+// and column items.
+__host__ __device__ constexpr int queue_words(int K) { return 2 + 2 * K; }
+constexpr int kQueueAbortWord = 1;
+
+static bool loss_queue_requested(int n, int flags) {
+    return n == kQueueN && (flags & QSSB_FLAG_PERSISTENT) &&
+           !(flags & (QSSB_FLAG_CHI_FP64 | QSSB_FLAG_FULL_PLANE));
+}
 
 // Rows per CTA of the row pass and columns per CTA of the column pass (one
 // warp each): 16, or 8 at 1024 where a lane holds 32 values of its line.
@@ -1054,13 +1072,16 @@ struct TwoPass {
     static constexpr int pitch = (scratch > N ? scratch : N) | 1;
     static constexpr size_t row_smem = sizeof(float2) * ((size_t)rwarps * scratch + N);
     static constexpr size_t col_smem = sizeof(float2) * ((size_t)2 * tile * pitch + N);
-    // half set at 256^2: column pairs (k_loss_cols_pair), a warp per pair of
-    // the strip's columns; two adjacent lines hold one warp FFT's scratch
+    // half set at 256^2 and 512^2: column pairs (k_loss_cols_pair), a warp
+    // per pair of the strip's columns, staged as one float4 per row (the two
+    // columns' values side by side); a pair's lines hold one warp FFT's scratch
     static constexpr bool pair_cols = !FULL && (N == 256 || N == 512);
     static constexpr int pair_warps = tile / 2;
     static constexpr int pair_pitch = (rows > (scratch + 1) / 2 ? rows : (scratch + 1) / 2) | 1;
-    static constexpr size_t col_pair_smem =
-        sizeof(float2) * ((size_t)2 * tile * pair_pitch + N) + sizeof(float) * (size_t)pair_warps * N;
+    // + two buffers of the BF pixel's N/2 Nyquist-column deviations
+    static constexpr size_t col_pair_smem = sizeof(float4) * (size_t)2 * pair_warps * pair_pitch +
+                                            sizeof(float2) * N + sizeof(float) * (size_t)pair_warps * N +
+                                            sizeof(float2) * (size_t)N;
     // CTAs per SM of the column pass, for the plan's wave arithmetic
     static constexpr int col_ctas_per_sm = pair_cols && N == 256 ? 3 : 2;
 };
@@ -1100,21 +1121,22 @@ static TwoPassPlan plan_two_pass(int n, bool full, int n_bf, int n_cand, int chu
     return tp;
 }
 
+// One row-pass work item: rows rowblock * RW .. + RW - 1 of BF pixel b0 + bi
+// for candidate cand0 + zc. scr: RW warp FFT scratches; tw: the twiddles
+// (filled before the item's first barrier).
 template <int N, bool CHI64, bool QUAD, bool FULL>
-__global__ void __launch_bounds__(32 * row_warps(N), row_min_ctas(N)) k_loss_rows(
+__device__ __forceinline__ void loss_rows_item(
     const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
     const float* __restrict__ q_row, const float* __restrict__ q_col, const void* __restrict__ cands,
-    qssb_calibration_t cal, const Probe* __restrict__ probes, const float2* __restrict__ twg,
+    const qssb_calibration_t& cal, const Probe* __restrict__ probes,
     const float2* __restrict__ eq_table, int cand0, int b0, int nb_chunk,
-    float2* __restrict__ stage, float2* __restrict__ delta, const float2* __restrict__ overlap) {
+    float2* __restrict__ stage, float2* __restrict__ delta, const float2* __restrict__ overlap,
+    int rowblock, int bi, int zc, float2* scr, const float2* tw) {
     using TP = TwoPass<N, FULL>;
     constexpr int H = N / 2 + 1;
     constexpr int RW = TP::rwarps;
     constexpr int RPL = N / 32;
     constexpr bool kSep = !FULL && QUAD && !CHI64;
-    extern __shared__ float4 smem4[];
-    float2* scr = reinterpret_cast<float2*>(smem4);
-    float2* tw = scr + RW * TP::scratch;
     __shared__ Probe sp;
     __shared__ FullChi sf;
     __shared__ FullChi64 sd;
@@ -1123,16 +1145,13 @@ __global__ void __launch_bounds__(32 * row_warps(N), row_min_ctas(N)) k_loss_row
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
-    const int bi = blockIdx.y;
     const int b = b0 + bi;
-    const int zc = blockIdx.z;  // the candidate within the group (staging index)
     const int cand = cand0 + zc;
-    const int r0 = blockIdx.x * RW;
-    {  // the candidate's probe and the twiddles, from k_two_pass_setup
+    const int r0 = rowblock * RW;
+    {  // the candidate's probe, from k_two_pass_setup
         const auto* src = reinterpret_cast<const unsigned int*>(probes + cand);
         auto* dst = reinterpret_cast<unsigned int*>(&sp);
         for (int i = tid; i < (int)(sizeof(Probe) / 4); i += 32 * RW) dst[i] = __ldg(src + i);
-        for (int i = tid; i < N; i += 32 * RW) tw[i] = __ldg(twg + i);
     }
     if constexpr (FULL) {
         if (tid == 0) {
@@ -1248,7 +1267,7 @@ __global__ void __launch_bounds__(32 * row_warps(N), row_min_ctas(N)) k_loss_row
     if (r < TP::rows) row(r, kSep ? s_phr[warp] : make_float2(1.0f, 0.0f));
     if constexpr (TP::fold_nyquist) {
         static_assert(TP::row_ctas * RW == N / 2, "whole CTAs of rows");
-        if (blockIdx.x == 0 && warp == 0) {
+        if (rowblock == 0 && warp == 0) {
             __syncwarp();  // the FFT scratch is reused by the Nyquist row
             float2 e_row = make_float2(1.0f, 0.0f);
             if constexpr (kSep) {
@@ -1259,6 +1278,23 @@ __global__ void __launch_bounds__(32 * row_warps(N), row_min_ctas(N)) k_loss_row
             row(N / 2, e_row);
         }
     }
+}
+
+template <int N, bool CHI64, bool QUAD, bool FULL>
+__global__ void __launch_bounds__(32 * row_warps(N), row_min_ctas(N)) k_loss_rows(
+    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
+    const float* __restrict__ q_row, const float* __restrict__ q_col, const void* __restrict__ cands,
+    qssb_calibration_t cal, const Probe* __restrict__ probes, const float2* __restrict__ twg,
+    const float2* __restrict__ eq_table, int cand0, int b0, int nb_chunk,
+    float2* __restrict__ stage, float2* __restrict__ delta, const float2* __restrict__ overlap) {
+    using TP = TwoPass<N, FULL>;
+    extern __shared__ float4 smem4[];
+    float2* scr = reinterpret_cast<float2*>(smem4);
+    float2* tw = scr + TP::rwarps * TP::scratch;
+    for (int i = threadIdx.x; i < N; i += 32 * TP::rwarps) tw[i] = __ldg(twg + i);
+    loss_rows_item<N, CHI64, QUAD, FULL>(g, n_bf, geom, q_row, q_col, cands, cal, probes,
+                                         eq_table, cand0, b0, nb_chunk, stage, delta, overlap,
+                                         blockIdx.x, blockIdx.y, blockIdx.z, scr, tw);
 }
 
 __device__ __forceinline__ void cp_async8(void* smem_dst, const void* gmem_src) {
@@ -1352,10 +1388,21 @@ __global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
     }
 }
 
-// The column pass of the half set two columns at a time (256^2). A column
-// line L of the row-transformed half plane, completed by the +-q relation
-// L[N - r] = -conj(L[r]) + s delta_r (s = (-1)^x, delta_r the Nyquist-column
-// deviation of row r), splits into an anti-Hermitian part
+// 16-byte cp.async: through L2 only (L2ONLY, for data written earlier in the
+// same launch by other SMs) or allocating in L1 as well
+template <bool L2ONLY>
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    if constexpr (L2ONLY)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+
+// The column pass of the half set two columns at a time (256^2, 512^2). A
+// column line L of the row-transformed half plane, completed by the +-q
+// relation L[N - r] = -conj(L[r]) + s delta_r (s = (-1)^x, delta_r the
+// Nyquist-column deviation of row r), splits into an anti-Hermitian part
 //   AL[r] = L[r] - (s/2) conj(delta_r), AL[N - r] = -conj(AL[r]),
 //   AL[0] = i Im L[0], AL[N/2] = i Im L[N/2],
 // whose transform is purely imaginary, and a Hermitian part whose transform
@@ -1364,38 +1411,40 @@ __global__ void __launch_bounds__(32 * col_tile(N)) k_loss_cols(
 // pixel. So one complex FFT of AL_a + i AL_b gives both columns' imaginary
 // parts (i Y_a - Y_b), and one FFT per BF pixel gives Dhat: about half the
 // column FFTs of k_loss_cols. Dhat is computed W pixels ahead, one per warp,
-// with the idle strip buffer as scratch.
-template <int N>
-__global__ void __launch_bounds__(16 * col_tile(N), TwoPass<N, false>::col_ctas_per_sm)
-    k_loss_cols_pair(const float2* __restrict__ stage, const float2* __restrict__ delta,
-                     const float2* __restrict__ twg, int cand0, int nb_chunk, int n_sub,
-                     int first, float* __restrict__ part) {
+// with the idle strip buffer as scratch. L2ONLY (the persistent queue kernel,
+// whose producers write in the same launch): staged rows, deviations and
+// partial planes are read through L2 only (cp.async.cg, ld.global.cg).
+template <int N, bool L2ONLY>
+__device__ __forceinline__ void loss_cols_pair_item(
+    const float2* __restrict__ stage, const float2* __restrict__ delta, int cand0, int nb_chunk,
+    int n_sub, int first, float* __restrict__ part, int strip, int sub, int zc, float4* tiles,
+    const float2* tw, float* dh, float2* dsm) {
     using TP = TwoPass<N, false>;
     constexpr int P = TP::pair_pitch;
     constexpr int RPL = N / 32;
     constexpr int kColTile = TP::tile;
     constexpr int W = TP::pair_warps;
     constexpr int NT = 32 * W;
-    static_assert(TP::pair_cols && 2 * P >= TP::scratch, "pair lines hold the FFT scratch");
-    extern __shared__ float4 smem4[];
-    float2* tiles = reinterpret_cast<float2*>(smem4);  // two strips: the next one arrives by cp.async
-    float2* tw = tiles + 2 * kColTile * P;
-    float* dh = reinterpret_cast<float*>(tw + N);  // [W][N]: Dhat of the next W pixels
+    static_assert(TP::pair_cols && 2 * P >= TP::scratch, "a pair's lines hold the FFT scratch");
     const int tid = threadIdx.x;
     const int lane = tid & 31;
     const int warp = tid >> 5;
-    const int x0 = blockIdx.x * kColTile;
-    const int sub = blockIdx.y;
-    const int zc = blockIdx.z;  // the candidate within the group (staging index)
+    const int x0 = strip * kColTile;
     const int cand = cand0 + zc;
     const int xa = x0 + 2 * warp;  // even: s = +1 for column xa, -1 for xa + 1
-    for (int i = tid; i < N; i += NT) tw[i] = __ldg(twg + i);
-    auto issue = [&](int bi, float2* dst) {
+    // the strip of BF pixel bi and its deviations (dsm: two buffers of N/2)
+    auto issue = [&](int bi, int into) {
+        float4* dst = tiles + into * W * P;
         const float2* S = stage + ((size_t)zc * nb_chunk + bi) * TP::rows * N + x0;
-        for (int e = tid; e < TP::rows * kColTile; e += NT) {
-            const int rr = e / kColTile;
-            const int c = e - rr * kColTile;
-            cp_async8(dst + c * P + rr, S + (size_t)rr * N + c);
+        for (int e = tid; e < TP::rows * W; e += NT) {
+            const int rr = e / W;
+            const int pp = e - rr * W;
+            cp_async16<L2ONLY>(dst + pp * P + rr, S + (size_t)rr * N + 2 * pp);
+        }
+        if constexpr (L2ONLY) {  // else read from global through L1
+            const float2* D = delta + ((size_t)zc * nb_chunk + bi) * (N / 2);
+            for (int e = tid; e < N / 4; e += NT)
+                cp_async16<true>(dsm + into * (N / 2) + 2 * e, D + 2 * e);
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
@@ -1403,7 +1452,7 @@ __global__ void __launch_bounds__(16 * col_tile(N), TwoPass<N, false>::col_ctas_
 #pragma unroll
     for (int t = 0; t < RPL; ++t) asa[t] = aqa[t] = asb[t] = aqb[t] = 0.0f;
     int buf = 0;
-    if (sub < nb_chunk) issue(sub, tiles);
+    if (sub < nb_chunk) issue(sub, 0);
     int step = 0;
     for (int bi = sub; bi < nb_chunk; bi += n_sub, ++step) {
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -1419,45 +1468,47 @@ __global__ void __launch_bounds__(16 * col_tile(N), TwoPass<N, false>::col_ctas_
 #pragma unroll
                 for (int t = 0; t < RPL; ++t) {
                     const int rr = lane + 32 * t;
-                    v[t] = rr > N / 2 ? __ldg(d + N - rr) : make_float2(0.0f, 0.0f);
+                    v[t] = rr > N / 2 ? (L2ONLY ? __ldcg(d + N - rr) : __ldg(d + N - rr))
+                                      : make_float2(0.0f, 0.0f);
                 }
-                warp_fft<N, +1>(v, tiles + (buf ^ 1) * kColTile * P + 2 * warp * P, tw, lane);
+                warp_fft<N, +1>(v, reinterpret_cast<float2*>(tiles + ((buf ^ 1) * W + warp) * P),
+                                tw, lane);
 #pragma unroll
                 for (int j = 0; j < RPL; ++j) dh[warp * N + warp_fft_index<N>(lane, j)] = v[j].x;
             }
             __syncthreads();
         }
-        if (bi + n_sub < nb_chunk) issue(bi + n_sub, tiles + (buf ^ 1) * kColTile * P);
-        float2* la = tiles + buf * kColTile * P + 2 * warp * P;
-        const float2* lb = la + P;
-        const float2* d = delta + ((size_t)zc * nb_chunk + bi) * (N / 2);
+        if (bi + n_sub < nb_chunk) issue(bi + n_sub, buf ^ 1);
+        float4* pr = tiles + (buf * W + warp) * P;
+        const float2* d =
+            L2ONLY ? dsm + buf * (N / 2) : delta + ((size_t)zc * nb_chunk + bi) * (N / 2);
         float2 v[RPL];
 #pragma unroll
         for (int t = 0; t < RPL; ++t) {
             const int rr = lane + 32 * t;
             if (rr == 0 || rr == N / 2) {
-                v[t] = make_float2(-lb[rr].y, la[rr].y);
+                const float4 q = pr[rr];
+                v[t] = make_float2(-q.w, q.y);
             } else {
                 const int rp = rr < N / 2 ? rr : N - rr;
-                const float2 dd = __ldg(d + rp);
-                const float2 a = la[rp];
-                const float2 bv = lb[rp];
-                const float ax = fmaf(-0.5f, dd.x, a.x), ay = fmaf(0.5f, dd.y, a.y);
-                const float bx = fmaf(0.5f, dd.x, bv.x), by = fmaf(-0.5f, dd.y, bv.y);
+                const float2 dd = L2ONLY ? d[rp] : __ldg(d + rp);
+                const float4 q = pr[rp];
+                const float ax = fmaf(-0.5f, dd.x, q.x), ay = fmaf(0.5f, dd.y, q.y);
+                const float bx = fmaf(0.5f, dd.x, q.z), by = fmaf(-0.5f, dd.y, q.w);
                 v[t] = rr < N / 2 ? make_float2(ax - by, ay + bx) : make_float2(-ax - by, ay - bx);
             }
         }
-        const float ha0 = la[0].x, haN = la[N / 2].x, hb0 = lb[0].x, hbN = lb[N / 2].x;
-        __syncwarp();  // the two lines become the FFT's transpose scratch
-        warp_fft<N, +1>(v, la, tw, lane);
+        const float4 h0 = pr[0], hN = pr[N / 2];
+        __syncwarp();  // the pair's lines become the FFT's transpose scratch
+        warp_fft<N, +1>(v, reinterpret_cast<float2*>(pr), tw, lane);
         const float* dhs = dh + slot * N;
 #pragma unroll
         for (int j = 0; j < RPL; ++j) {
             const int y = warp_fft_index<N>(lane, j);
             const float sy = (y & 1) ? -1.0f : 1.0f;
             const float dv = dhs[y];
-            const float pa = phase_atan2(v[j].y, fmaf(sy, haN, ha0) + dv);
-            const float pb = phase_atan2(-v[j].x, fmaf(sy, hbN, hb0) - dv);
+            const float pa = phase_atan2(v[j].y, fmaf(sy, hN.x, h0.x) + dv);
+            const float pb = phase_atan2(-v[j].x, fmaf(sy, hN.z, h0.z) - dv);
             asa[j] += pa;
             aqa[j] = fmaf(pa, pa, aqa[j]);
             asb[j] += pb;
@@ -1476,6 +1527,11 @@ __global__ void __launch_bounds__(16 * col_tile(N), TwoPass<N, false>::col_ctas_
             pq[y] = aqa[j];
             ps[N + y] = asb[j];
             pq[N + y] = aqb[j];
+        } else if constexpr (L2ONLY) {
+            ps[y] = __ldcg(ps + y) + asa[j];
+            pq[y] = __ldcg(pq + y) + aqa[j];
+            ps[N + y] = __ldcg(ps + N + y) + asb[j];
+            pq[N + y] = __ldcg(pq + N + y) + aqb[j];
         } else {
             ps[y] += asa[j];
             pq[y] += aqa[j];
@@ -1483,6 +1539,22 @@ __global__ void __launch_bounds__(16 * col_tile(N), TwoPass<N, false>::col_ctas_
             pq[N + y] += aqb[j];
         }
     }
+}
+
+template <int N>
+__global__ void __launch_bounds__(16 * col_tile(N), TwoPass<N, false>::col_ctas_per_sm)
+    k_loss_cols_pair(const float2* __restrict__ stage, const float2* __restrict__ delta,
+                     const float2* __restrict__ twg, int cand0, int nb_chunk, int n_sub,
+                     int first, float* __restrict__ part) {
+    using TP = TwoPass<N, false>;
+    extern __shared__ float4 smem4[];
+    float4* tiles = smem4;  // two strips: the next one arrives by cp.async
+    float2* tw = reinterpret_cast<float2*>(tiles + 2 * TP::pair_warps * TP::pair_pitch);
+    float* dh = reinterpret_cast<float*>(tw + N);  // [W][N]: Dhat of the next W pixels
+    float2* dsm = reinterpret_cast<float2*>(dh + TP::pair_warps * N);
+    for (int i = threadIdx.x; i < N; i += 32 * TP::pair_warps) tw[i] = __ldg(twg + i);
+    loss_cols_pair_item<N, false>(stage, delta, cand0, nb_chunk, n_sub, first, part, blockIdx.x,
+                           blockIdx.y, blockIdx.z, tiles, tw, dh, dsm);
 }
 
 struct LossPlan {
@@ -1496,12 +1568,21 @@ struct LossPlan {
     size_t stage_bytes;  // N >= 256: row-transformed planes of one chunk
     size_t delta_bytes;  // N >= 256, half set: Nyquist-column deviations
     size_t setup_bytes;  // N >= 256: per-candidate probes and the N twiddles
+    bool queue;          // 256^2 half set: one persistent launch (k_loss_queue)
+    int n_groups;        // queue: candidate groups
+    int n_phase_chunks;  // queue: BF chunks over all groups
+    size_t queue_bytes;  // queue: ticket, abort word and per-chunk completion counts
 };
 
 // Deterministic: about 296 CTAs in total (two per B200 SM), at least one BF
 // pixel each. N >= 256: the two-pass plan (n_chunks = its column interleave).
-static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool full = false) {
+static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool full = false,
+                          bool queue = false) {
     LossPlan pl;
+    pl.queue = false;
+    pl.n_groups = 0;
+    pl.n_phase_chunks = 0;
+    pl.queue_bytes = 0;
     if (n >= kL256) {
         const TwoPassPlan tp = plan_two_pass(n, full, n_bf, n_cand, chunks_req);
         pl.chunk_bf = tp.chunk_bf;
@@ -1514,6 +1595,23 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool 
         pl.delta_bytes = (pl.delta_bytes + 255) & ~(size_t)255;
         pl.setup_bytes = ((sizeof(Probe) * (size_t)n_cand + 255) & ~(size_t)255) +
                          sizeof(float2) * (size_t)n;
+        const int n_groups = (n_cand + tp.group - 1) / tp.group;
+        if (queue && !full && n == kQueueN && n_groups <= kQueueMaxGroups) {
+            // two staging slots (rows of chunk k + 1 while columns of chunk k)
+            pl.queue = true;
+            pl.n_groups = n_groups;
+            int k = 0;
+            for (int g = 0; g < n_groups; ++g) {
+                const int nc = n_cand - g * tp.group < tp.group ? n_cand - g * tp.group : tp.group;
+                int chunk = tp.chunk_bf * tp.group / nc;
+                if (chunk > n_bf) chunk = n_bf;
+                k += (n_bf + chunk - 1) / chunk;
+            }
+            pl.n_phase_chunks = k;
+            pl.stage_bytes = 2 * ((pl.stage_bytes + 255) & ~(size_t)255);
+            pl.delta_bytes = 2 * pl.delta_bytes;
+            pl.queue_bytes = (sizeof(int) * (size_t)queue_words(k) + 255) & ~(size_t)255;
+        }
     } else if (n == 128 && chunks_req <= 0) {
         // one 512-thread CTA per SM: pick the chunking whose waves are
         // fullest - minimise waves x (pairs per CTA + one pair's worth of
@@ -1567,8 +1665,176 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool 
 
 static size_t loss_workspace(const LossPlan& pl) {
     return pl.part_bytes + pl.var_bytes + pl.eq_bytes + pl.stage_bytes + pl.delta_bytes +
-           pl.setup_bytes;
+           pl.setup_bytes + pl.queue_bytes;
 }
+
+// ------------------------------------- the persistent one-launch loss (256^2)
+// With QSSB_FLAG_PERSISTENT one launch runs every row and column item of the
+// batch (all candidate groups, all BF chunks) from a global ticket, in the
+// order
+//   R(0), R(1), C(0), R(2), C(1), ..., R(K-1), C(K-2), C(K-1)
+// (R(k): the row items of chunk k, C(k): its column items), with two staging
+// slots. An item waits (thread 0, bounded) only for items with smaller
+// tickets: C(k) for R(k) and, within a candidate group, for C(k - 1) (the
+// partial planes' read-modify-write order); R(k) for C(k - 2) (its slot).
+// A waiting CTA holds a ticket taken after the ones it waits on, and every
+// ticket taken is held by a running CTA, so the batch drains whatever the
+// number of resident CTAs. Producers write through L2 and fence before their
+// counts; consumers read staged rows, deviations and partial planes through
+// L2 only. The chunking is the launch sequence's, and so are the bits on the
+// quadratic path (the general-chi arithmetic, inlined into another kernel,
+// may contract differently: float32 rounding). A wait that runs out, or a set
+// cancel flag, sets the abort word: later items only count themselves and
+// k_loss_final writes NaN losses. CTAs that wait hold their slots, so this is
+// slower than the launch sequence (the default), which it replaces where
+// one launch per batch matters more than time.
+struct QueuePlan {
+    int K;       // BF chunks over all candidate groups
+    int SR, SC;  // items of one row phase, of one column phase
+    int n_sub;
+    int n_groups;
+    int kstart[kQueueMaxGroups + 1];
+    int c0[kQueueMaxGroups];
+    int nc[kQueueMaxGroups];
+    int chunk[kQueueMaxGroups];
+    size_t stage_slot;  // float2 elements per staging slot
+    size_t delta_slot;
+};
+
+constexpr long long kQueueSpinLimit = 1ll << 22;  // polls 128 ns apart: over half a second
+
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Thread 0 of an item: wait until *count reaches target. Nonzero: the batch
+// is aborted (the cancel flag is set, this wait ran out, or another did).
+__device__ int queue_wait(const int* count, int target, int* abort_word, const int* cancel) {
+    for (long long it = 0;; ++it) {
+        if (ld_acquire_gpu(count) >= target) return 0;
+        if (*reinterpret_cast<volatile int*>(abort_word) != 0) return 1;
+        if (cancel && *reinterpret_cast<const volatile int*>(cancel) != 0) {
+            atomicCAS(abort_word, 0, 1);
+            return 1;
+        }
+        if (it >= kQueueSpinLimit) {
+            atomicCAS(abort_word, 0, 2);
+            return 1;
+        }
+        __nanosleep(128);
+    }
+}
+
+template <int N, bool QUAD>
+__global__ void __launch_bounds__(32 * TwoPass<N, false>::rwarps, 3) k_loss_queue(
+    const float2* __restrict__ g, int n_bf, const float* __restrict__ geom,
+    const float* __restrict__ q_row, const float* __restrict__ q_col, const void* __restrict__ cands,
+    qssb_calibration_t cal, const Probe* __restrict__ probes, const float2* __restrict__ twg,
+    const float2* __restrict__ eq_table, float2* __restrict__ stage, float2* __restrict__ delta,
+    const float2* __restrict__ overlap, float* __restrict__ part, QueuePlan qp,
+    int* __restrict__ queue, const int* __restrict__ cancel) {
+    using TP = TwoPass<N, false>;
+    static_assert(TP::pair_cols && TP::rwarps == TP::pair_warps, "one CTA shape for both items");
+    constexpr int NT = 32 * TP::rwarps;
+    constexpr int kStrips = N / TP::tile;
+    extern __shared__ float4 smem4[];
+    float2* tw = reinterpret_cast<float2*>(smem4);
+    float4* area = smem4 + N / 2;  // row items: warp FFT scratches; column items: strips, Dhat
+    float2* scr = reinterpret_cast<float2*>(area);
+    float4* tiles = area;
+    float* dh = reinterpret_cast<float*>(tiles + 2 * TP::pair_warps * TP::pair_pitch);
+    float2* dsm = reinterpret_cast<float2*>(dh + TP::pair_warps * N);
+    __shared__ int s_item;
+    __shared__ int s_skip;
+    int* ticket = queue;
+    int* abort_word = queue + kQueueAbortWord;
+    int* done_r = queue + 2;
+    int* done_c = done_r + qp.K;
+    for (int i = threadIdx.x; i < N; i += NT) tw[i] = __ldg(twg + i);
+    const int total = qp.K * (qp.SR + qp.SC);
+    for (;;) {
+        __syncthreads();  // the previous item is done with shared memory
+        if (threadIdx.x == 0) s_item = atomicAdd(ticket, 1);
+        __syncthreads();
+        const int t = s_item;
+        if (t >= total) break;
+        bool row;
+        int k, w;
+        if (t < qp.SR) {
+            row = true;
+            k = 0;
+            w = t;
+        } else {
+            const int tp = t - qp.SR;
+            const int q = 1 + tp / (qp.SR + qp.SC);
+            w = tp - (q - 1) * (qp.SR + qp.SC);
+            if (q < qp.K && w < qp.SR) {
+                row = true;
+                k = q;
+            } else {
+                row = false;
+                k = q - 1;
+                if (q < qp.K) w -= qp.SR;
+            }
+        }
+        int gi = 0;
+        while (gi + 1 < qp.n_groups && k >= qp.kstart[gi + 1]) ++gi;
+        const int kg = k - qp.kstart[gi];
+        const int ch = qp.chunk[gi];
+        const int b0 = kg * ch;
+        const int nb = n_bf - b0 < ch ? n_bf - b0 : ch;
+        float2* st = stage + (size_t)(k & 1) * qp.stage_slot;
+        float2* dl = delta + (size_t)(k & 1) * qp.delta_slot;
+        if (threadIdx.x == 0) {
+            if (cancel && *reinterpret_cast<const volatile int*>(cancel) != 0)
+                atomicCAS(abort_word, 0, 1);
+            int skip = 0;
+            if (row) {
+                if (k >= 2) skip = queue_wait(done_c + k - 2, qp.SC, abort_word, cancel);
+            } else {
+                skip = queue_wait(done_r + k, qp.SR, abort_word, cancel);
+                if (!skip && kg >= 1) skip = queue_wait(done_c + k - 1, qp.SC, abort_word, cancel);
+            }
+            s_skip = skip | (*reinterpret_cast<volatile int*>(abort_word) != 0);
+        }
+        __syncthreads();
+        if (!s_skip) {  // CTA-uniform, as is every branch below
+            if (row) {
+                const int rb = w % TP::row_ctas;
+                const int pl = w / TP::row_ctas;
+                const int zc = pl / ch;
+                const int bi = pl - zc * ch;
+                if (zc < qp.nc[gi] && bi < nb)
+                    loss_rows_item<N, false, QUAD, false>(g, n_bf, geom, q_row, q_col, cands, cal,
+                                                          probes, eq_table, qp.c0[gi], b0, nb, st,
+                                                          dl, overlap, rb, bi, zc, scr, tw);
+            } else {
+                const int strip = w % kStrips;
+                const int rest = w / kStrips;
+                const int sub = rest % qp.n_sub;
+                const int zc = rest / qp.n_sub;
+                if (zc < qp.nc[gi])
+                    loss_cols_pair_item<N, true>(st, dl, qp.c0[gi], nb, qp.n_sub, kg == 0 ? 1 : 0,
+                                                 part, strip, sub, zc, tiles, tw, dh, dsm);
+            }
+        }
+        __threadfence();  // this thread's writes of the item, before its count
+        __syncthreads();
+        if (threadIdx.x == 0) atomicAdd(row ? done_r + k : done_c + k, 1);
+    }
+}
+
+template <int N>
+struct QueueSmem {
+    using TP = TwoPass<N, false>;
+    static constexpr size_t scr = sizeof(float2) * (size_t)TP::rwarps * TP::scratch;
+    static constexpr size_t cols = sizeof(float4) * (size_t)2 * TP::pair_warps * TP::pair_pitch +
+                                   sizeof(float) * (size_t)TP::pair_warps * N +
+                                   sizeof(float2) * (size_t)N;
+    static constexpr size_t bytes = sizeof(float2) * N + (scr > cols ? scr : cols);
+};
 
 // Once per batch: every candidate's probe parameters (FP64 divisions and the
 // FP64 cos/sin of 2 phi12) and the N FFT twiddles, so that the row and column
@@ -1577,8 +1843,10 @@ template <int N, bool FULL>
 __global__ void __launch_bounds__(128) k_two_pass_setup(const void* __restrict__ cands,
                                                          qssb_calibration_t cal, int n_cand,
                                                          Probe* __restrict__ probes,
-                                                         float2* __restrict__ tw) {
+                                                         float2* __restrict__ tw,
+                                                         int* __restrict__ queue, int n_queue) {
     const int i = blockIdx.x * 128 + threadIdx.x;
+    if (i < n_queue) queue[i] = 0;  // the queue kernel's ticket, abort word and counts
     if (i < n_cand) {
         if constexpr (FULL) {
             probes[i] = make_probe_common(cal, 0.0f, 0.0f, 0.0f, 0.0f);
@@ -1622,10 +1890,57 @@ static int launch_two_pass(const float* g_half, const float* geom, const float* 
                                   cudaFuncAttributePreferredSharedMemoryCarveout,
                                   (int)cudaSharedmemCarveoutMaxShared));
     const auto* g = reinterpret_cast<const float2*>(g_half);
+    int* queue = reinterpret_cast<int*>(stage_base + pl.stage_bytes + pl.delta_bytes +
+                                        pl.setup_bytes);
+    const int n_queue = pl.queue ? queue_words(pl.n_phase_chunks) : 0;
     {
-        const int n = n_cand > N ? n_cand : N;
-        { k_two_pass_setup<N, FULL><<<(n + 127) / 128, 128, 0, s>>>(cands, cal, n_cand, probes, twg); note_launch(); }
+        int n = n_cand > N ? n_cand : N;
+        if (n_queue > n) n = n_queue;
+        { k_two_pass_setup<N, FULL><<<(n + 127) / 128, 128, 0, s>>>(cands, cal, n_cand, probes, twg,
+                                                                   queue, n_queue); note_launch(); }
         CUDA_TRY(cudaGetLastError());
+    }
+    if constexpr (N == kQueueN && !FULL && !CHI64) {
+        if (pl.queue) {
+            QueuePlan qp = {};
+            qp.n_sub = pl.n_chunks;
+            qp.n_groups = pl.n_groups;
+            qp.SR = TP::row_ctas * pl.chunk_bf * pl.group;
+            qp.SC = (N / TP::tile) * pl.n_chunks * pl.group;
+            int k = 0;
+            for (int gi = 0; gi < pl.n_groups; ++gi) {
+                const int c0 = gi * pl.group;
+                const int nc = n_cand - c0 < pl.group ? n_cand - c0 : pl.group;
+                int chunk = pl.chunk_bf * pl.group / nc;
+                if (chunk > cal.n_bf) chunk = cal.n_bf;
+                qp.kstart[gi] = k;
+                qp.c0[gi] = c0;
+                qp.nc[gi] = nc;
+                qp.chunk[gi] = chunk;
+                k += (cal.n_bf + chunk - 1) / chunk;
+            }
+            qp.kstart[pl.n_groups] = k;
+            qp.K = k;
+            qp.stage_slot = pl.stage_bytes / 2 / sizeof(float2);
+            qp.delta_slot = pl.delta_bytes / 2 / sizeof(float2);
+            if (k != pl.n_phase_chunks || (long long)k * (qp.SR + qp.SC) > INT_MAX)
+                return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: queue plan mismatch");
+            const size_t smem = QueueSmem<N>::bytes;
+            CUDA_TRY(cudaFuncSetAttribute(k_loss_queue<N, QUAD>,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            CUDA_TRY(cudaFuncSetAttribute(k_loss_queue<N, QUAD>,
+                                          cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          (int)cudaSharedmemCarveoutMaxShared));
+            int per_sm = 0;
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &per_sm, k_loss_queue<N, QUAD>, 32 * TP::rwarps, smem));
+            if (per_sm < 1) per_sm = 1;
+            { k_loss_queue<N, QUAD><<<device_sm_count() * per_sm, 32 * TP::rwarps, smem, s>>>(
+                g, cal.n_bf, geom, q_row, q_col, cands, cal, probes, twg, eq, stage, delta, overlap,
+                part, qp, queue, cancel_flag()); note_launch(); }
+            CUDA_TRY(cudaGetLastError());
+            return QSSB_OK;
+        }
     }
     for (int c0 = 0; c0 < n_cand; c0 += pl.group) {
         const int nc = n_cand - c0 < pl.group ? n_cand - c0 : pl.group;
@@ -1658,9 +1973,10 @@ static int launch_two_pass(const float* g_half, const float* geom, const float* 
 template <int N, bool SYM, bool CHI64, bool QUAD>
 static int launch_loss(const float* g_half, const float* geom, const float* q_row,
                        const float* q_col, const qssb_calibration_t& cal,
-                       const qssb_aberrations_t* cands, int n_cand, int chunks, char* ws,
+                       const qssb_aberrations_t* cands, int n_cand, int flags, char* ws,
                        float* losses, float* mean_phase, const float2* overlap, cudaStream_t s) {
-    const LossPlan pl = plan_loss(N, cal.n_bf, n_cand, chunks);
+    const LossPlan pl = plan_loss(N, cal.n_bf, n_cand, flag_chunks(flags), false,
+                                  loss_queue_requested(N, flags));
     float* part = reinterpret_cast<float*>(ws);
     double* var = reinterpret_cast<double*>(ws + pl.part_bytes);
     float2* eq = reinterpret_cast<float2*>(ws + pl.part_bytes + pl.var_bytes);
@@ -1720,7 +2036,13 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
     { k_loss_reduce<N><<<dim3(N * N / kReducePix, n_cand), kReducePix * kReduceSlices, 0, s>>>(
         part, pl.n_chunks, cal.n_bf, var, mean_phase, N == 128 ? 1 : 0); note_launch(); }
     CUDA_TRY(cudaGetLastError());
-    { k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N / kReducePix, N * N, losses); note_launch(); }
+    // the persistent loss's abort word (cancel or a wait that ran out): NaN losses
+    const int* status = nullptr;
+    if (pl.queue)
+        status = reinterpret_cast<const int*>(ws + pl.part_bytes + pl.var_bytes + pl.eq_bytes +
+                                              pl.stage_bytes + pl.delta_bytes + pl.setup_bytes) +
+                 kQueueAbortWord;
+    { k_loss_final<<<n_cand, 256, 0, s>>>(var, N * N / kReducePix, N * N, losses, status); note_launch(); }
     CUDA_TRY(cudaGetLastError());
     return QSSB_OK;
 }
@@ -1728,20 +2050,20 @@ static int launch_loss(const float* g_half, const float* geom, const float* q_ro
 template <int N, bool QUAD>
 static int dispatch_loss_q(bool sym, bool chi64, const float* g_half, const float* geom,
                            const float* q_row, const float* q_col, const qssb_calibration_t& cal,
-                           const qssb_aberrations_t* cands, int n_cand, int chunks, char* ws,
+                           const qssb_aberrations_t* cands, int n_cand, int flags, char* ws,
                            float* losses, float* mean_phase, const float2* ov, cudaStream_t s) {
     if constexpr (N >= kL256) {
         if (!sym)
             return set_error(QSSB_ERR_UNSUPPORTED,
                              "qssb_loss_batch: QSSB_FLAG_FULL_PLANE is offered up to 128^2");
-        return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s)
-                     : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s);
+        return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, flags, ws, losses, mean_phase, ov, s)
+                     : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, flags, ws, losses, mean_phase, ov, s);
     } else {
         if (sym)
-            return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s)
-                         : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s);
-        return chi64 ? launch_loss<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s)
-                     : launch_loss<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s);
+            return chi64 ? launch_loss<N, true, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, flags, ws, losses, mean_phase, ov, s)
+                         : launch_loss<N, true, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, flags, ws, losses, mean_phase, ov, s);
+        return chi64 ? launch_loss<N, false, true, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, flags, ws, losses, mean_phase, ov, s)
+                     : launch_loss<N, false, false, QUAD>(g_half, geom, q_row, q_col, cal, cands, n_cand, flags, ws, losses, mean_phase, ov, s);
     }
 }
 
@@ -1750,11 +2072,11 @@ static int dispatch_loss_q(bool sym, bool chi64, const float* g_half, const floa
 template <int N>
 static int dispatch_loss(bool sym, bool chi64, bool quad, const float* g_half, const float* geom,
                          const float* q_row, const float* q_col, const qssb_calibration_t& cal,
-                         const qssb_aberrations_t* cands, int n_cand, int chunks, char* ws,
+                         const qssb_aberrations_t* cands, int n_cand, int flags, char* ws,
                          float* losses, float* mean_phase, const float2* ov, cudaStream_t s) {
     if (quad)
-        return dispatch_loss_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s);
-    return dispatch_loss_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, chunks, ws, losses, mean_phase, ov, s);
+        return dispatch_loss_q<N, true>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, flags, ws, losses, mean_phase, ov, s);
+    return dispatch_loss_q<N, false>(sym, chi64, g_half, geom, q_row, q_col, cal, cands, n_cand, flags, ws, losses, mean_phase, ov, s);
 }
 
 // ------------------------------------------------------ 14-term chi
@@ -1910,7 +2232,8 @@ extern "C" int qssb_loss_workspace_bytes(const qssb_calibration_t* cal, int32_t 
     if (n != 64 && n != 128 && n != 256 && n != 512 && n != 1024)
         return set_error(QSSB_ERR_UNSUPPORTED,
                          "qssb_loss_batch: scan size must be 64, 128, 256, 512 or 1024");
-    const LossPlan pl = plan_loss(n, cal->n_bf, n_cand, flag_chunks(flags));
+    const LossPlan pl =
+        plan_loss(n, cal->n_bf, n_cand, flag_chunks(flags), false, loss_queue_requested(n, flags));
     *bytes = loss_workspace(pl);
     return QSSB_OK;
 }
@@ -1989,7 +2312,6 @@ extern "C" int qssb_loss_batch_ex(const float* g_half, const float* bf_geom, con
     const bool sym = !(flags & QSSB_FLAG_FULL_PLANE);
     const bool chi64 = (flags & QSSB_FLAG_CHI_FP64) != 0;
     const bool quad = (flags & QSSB_FLAG_QUADRATIC) != 0;
-    const int chunks = flag_chunks(flags);
     if (overlap && (cal->scan_rows < 128 || cal->scan_cols != cal->scan_rows))
         return set_error(QSSB_ERR_UNSUPPORTED,
                          "qssb_loss_batch_ex: the overlap table is for square 128 .. 1024 scans");
@@ -1997,11 +2319,11 @@ extern "C" int qssb_loss_batch_ex(const float* g_half, const float* bf_geom, con
     cudaStream_t s = (cudaStream_t)stream;
     char* ws = static_cast<char*>(workspace);
     switch (cal->scan_rows) {
-        case 64: return dispatch_loss<64>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, nullptr, s);
-        case 128: return dispatch_loss<128>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, ov, s);
-        case 256: return dispatch_loss<256>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, ov, s);
-        case 512: return dispatch_loss<512>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, ov, s);
-        case 1024: return dispatch_loss<1024>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, chunks, ws, losses, mean_phase, ov, s);
+        case 64: return dispatch_loss<64>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, flags, ws, losses, mean_phase, nullptr, s);
+        case 128: return dispatch_loss<128>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, flags, ws, losses, mean_phase, ov, s);
+        case 256: return dispatch_loss<256>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, flags, ws, losses, mean_phase, ov, s);
+        case 512: return dispatch_loss<512>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, flags, ws, losses, mean_phase, ov, s);
+        case 1024: return dispatch_loss<1024>(sym, chi64, quad, g_half, bf_geom, q_row, q_col, *cal, candidates, n_cand, flags, ws, losses, mean_phase, ov, s);
         default: return set_error(QSSB_ERR_UNSUPPORTED,
                                   "qssb_loss_batch: scan size must be 64, 128, 256, 512 or 1024");
     }

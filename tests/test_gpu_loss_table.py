@@ -25,7 +25,8 @@ import torch
 
 from oracle import ssb_oracle as so
 from quantem.gpu_b200 import B200SSBBackend, ops
-from quantem.gpu_b200._lib import QSSB_FLAG_CHI_FP64, QSSB_FLAG_QUADRATIC
+from quantem.gpu_b200._lib import (QSSB_FLAG_CHI_FP64, QSSB_FLAG_PERSISTENT,
+                                   QSSB_FLAG_QUADRATIC)
 from recipes import disk_input, synthetic_plain_32
 from test_gpu_parity import DISK_KW, _prep_case
 
@@ -244,3 +245,90 @@ def test_backend_builds_the_256_table_and_agrees_without_it():
     without = be.variance_loss_batch(c1, 20.0, 0.3).cpu().numpy()
     np.testing.assert_allclose(with_table, without, rtol=2e-6, atol=1e-7)
     be.close()
+
+
+# ------------------------------------------- the persistent one-launch loss
+# At 256^2 (half set, float32 chi) QSSB_FLAG_PERSISTENT runs every row and
+# column item of the batch in one k_loss_queue launch from a ticket queue,
+# with bounded waits on per-chunk completion counts, instead of a row and a
+# column launch per BF chunk. Same plan, so the same bits on the quadratic
+# path (float32 rounding on the C30 path).
+
+
+@pytest.fixture(scope="module")
+def case256():
+    return _prep_case(disk_input(123, scan=(256, 256)), **DISK_KW)
+
+
+def _rows(n, seed=3, c30=False):
+    rng = np.random.default_rng(seed)
+    out = np.stack([rng.uniform(-150, 150, n), rng.uniform(0, 60, n), rng.uniform(-1.5, 1.5, n),
+                    rng.uniform(0.0, 5e4, n) if c30 else np.zeros(n)], axis=1)
+    return torch.tensor(out, dtype=torch.float32, device=DEV)
+
+
+@pytest.mark.parametrize("n_cand,c30", [(1, False), (5, True), (27, False), (64, False),
+                                        (64, True), (70, False)])
+def test_persistent_launch_matches_the_launch_sequence(case256, n_cand, c30):
+    """1 .. 70 candidates: one group, a full group of 27, 64 = 27 + 27 + 10
+    and 70 = 27 + 27 + 16 (a last group with larger chunks); quadratic and C30."""
+    prep, cal, d = case256
+    table = ops.overlap_table(d["geom"], d["q_row"], d["q_col"], cal)
+    cands = _rows(n_cand, seed=n_cand, c30=c30)
+    fl = 0 if c30 else QSSB_FLAG_QUADRATIC
+    n0 = ops.LAUNCH_COUNT
+    q, mq = ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands,
+                           flags=fl | QSSB_FLAG_PERSISTENT, want_mean_phase=True, overlap=table)
+    launches = ops.LAUNCH_COUNT - n0
+    seq, ms = ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands, flags=fl,
+                             want_mean_phase=True, overlap=table)
+    if c30:
+        # the general-chi arithmetic, inlined into two different kernels, is
+        # contracted into FMAs differently: float32 rounding, not the plan
+        torch.testing.assert_close(q, seq, rtol=1e-6, atol=0)
+        torch.testing.assert_close(mq, ms, rtol=0, atol=2e-6)
+    else:
+        assert torch.equal(q, seq)
+        assert torch.equal(mq, ms)
+    # eq table (quadratic), setup, the queue kernel, reduce, final
+    assert launches == (4 if c30 else 5)
+    # the sequence: the same plus a row and a column launch per BF chunk
+    assert ops.LAUNCH_COUNT - n0 - launches > launches
+    if n_cand <= 5:
+        for i in range(n_cand):
+            a, b, c, c3 = (float(v) for v in cands[i].cpu())
+            ref, _ = so.phase_variance_loss(prep.g_half, prep.geo, so.Aberrations(a, b, c, C30=c3),
+                                            prep.dc)
+            assert float(q[i]) == pytest.approx(ref, rel=LOSS_RTOL, abs=LOSS_ATOL)
+
+
+def test_persistent_launch_repeats_its_bits_without_the_table(case256):
+    prep, cal, d = case256
+    cands = _rows(30)
+    run = lambda fl: ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands,  # noqa: E731
+                                    flags=fl)[0]
+    a = run(QSSB_FLAG_QUADRATIC | QSSB_FLAG_PERSISTENT)
+    assert torch.equal(a, run(QSSB_FLAG_QUADRATIC | QSSB_FLAG_PERSISTENT))
+    assert torch.equal(a, run(QSSB_FLAG_QUADRATIC))
+
+
+def test_persistent_launch_cancel_flag_gives_nan_without_hanging(case256):
+    """A set cancel flag makes every queue wait give up at once: the launch
+    drains (no hang) and the losses are NaN; cleared, the losses come back."""
+    prep, cal, d = case256
+    table = ops.overlap_table(d["geom"], d["q_row"], d["q_col"], cal)
+    cands = _rows(40)
+    run = lambda: ops.loss_batch(d["g"], d["geom"], d["q_row"], d["q_col"], cal, cands,  # noqa: E731
+                                 flags=QSSB_FLAG_QUADRATIC | QSSB_FLAG_PERSISTENT,
+                                 overlap=table)[0].cpu().numpy()
+    want = run()
+    flag = torch.zeros(1, dtype=torch.int32, device=DEV)
+    try:
+        ops.set_cancel_flag(flag)
+        np.testing.assert_array_equal(run(), want)
+        flag.fill_(1)
+        assert np.all(np.isnan(run()))
+        flag.fill_(0)
+        np.testing.assert_array_equal(run(), want)
+    finally:
+        ops.set_cancel_flag(None)
