@@ -506,6 +506,10 @@ def sweep_3scans(dev: torch.device, steps: int) -> dict:
 
     graph_ms = timed(sw.replay)
     direct_ms = timed(sw._launch_all)
+    # the same sweep with each 256^2 scan's passes in one persistent launch
+    swp = MultiScanSweep(backends, 64, persistent=True)
+    lp = swp(cands)
+    persistent_ms = timed(swp.replay)
     n = sum(c.shape[0] for c in cands)
     return {
         "workload": "scans 96x96, 128x128, 160x120 (padded to 128, 128, 256) x 128^2 detector, "
@@ -514,6 +518,10 @@ def sweep_3scans(dev: torch.device, steps: int) -> dict:
         "graph_launch_ms": graph_ms, "evals_per_s_graph": n * 1e3 / graph_ms,
         "evals_per_s_direct": n * 1e3 / direct_ms,
         "kernel_launches_per_graph": sw.launches_per_replay,
+        "persistent": {"evals_per_s_graph": n * 1e3 / persistent_ms,
+                       "kernel_launches_per_graph": swp.launches_per_replay,
+                       "max_rel_diff_vs_sequence": float(max(
+                           np.max(np.abs(a - b) / np.abs(b)) for a, b in zip(lp, losses)))},
         "autotuned_chunks_per_candidate": [s["chunks"] for s in sw._slots],
         "truth_ranked_first": [bool(int(np.argmin(l)) == 17) for l in losses],
     }
@@ -1083,7 +1091,10 @@ def _headline(line: dict) -> dict:
     if sw:
         h["sweep_3scans"] = {"evals_per_s": sw["evals_per_s_graph"],
                              "launches_per_graph": sw["kernel_launches_per_graph"],
-                             "truth_first": sw["truth_ranked_first"]}
+                             "truth_first": sw["truth_ranked_first"],
+                             "persistent_evals_per_s": sw["persistent"]["evals_per_s_graph"],
+                             "persistent_launches_per_graph":
+                                 sw["persistent"]["kernel_launches_per_graph"]}
     lf = line.get("learned_fits")
     if lf:
         keys = ("tau_1e-4_vs_loss_optimum_weak_phase", "tau_1e-4_vs_truth_weak_phase",

@@ -11,7 +11,10 @@ captured once into one CUDA graph, and a sweep step is: copy the candidates
 in, replay the graph, read the losses out. ``launches_per_replay`` is the
 library's own count of the kernels captured (``qssb_kernel_launches``).
 The work partition of each scan's loss kernel is chosen by the autotuner
-(``autotune.tune_loss``) before capture.
+(``autotune.tune_loss``) before capture. ``persistent=True`` runs each 256^2
+scan's row and column passes as one persistent launch
+(``QSSB_FLAG_PERSISTENT``: a handful of kernels per scan instead of two per
+BF chunk, the same losses on the quadratic path, but slower).
 """
 from __future__ import annotations
 
@@ -19,7 +22,7 @@ import numpy as np
 import torch
 
 from . import _lib, autotune, ops
-from ._lib import QSSB_FLAG_QUADRATIC
+from ._lib import QSSB_FLAG_PERSISTENT, QSSB_FLAG_QUADRATIC
 
 
 class MultiScanSweep:
@@ -27,7 +30,7 @@ class MultiScanSweep:
     in one graph replay."""
 
     def __init__(self, backends, n_cand: int | list[int], *, quadratic: bool = False,
-                 tune: bool = True):
+                 tune: bool = True, persistent: bool = False):
         if not backends:
             raise ValueError("at least one prepared scan is needed")
         self.backends = list(backends)
@@ -41,7 +44,8 @@ class MultiScanSweep:
         self._slots = []
         for be, n in zip(self.backends, counts):
             cal = be._calibration()
-            flags = be._flags | (QSSB_FLAG_QUADRATIC if quadratic else 0)
+            flags = (be._flags | (QSSB_FLAG_QUADRATIC if quadratic else 0)
+                     | (QSSB_FLAG_PERSISTENT if persistent else 0))
             cands = torch.zeros((n, 4), dtype=torch.float32, device=self.device)
             cands[:, 0] = torch.linspace(-100.0, 100.0, n, device=self.device)
             ws = ops.Workspace(self.device)

@@ -90,3 +90,21 @@ def test_sweep_losses_match_fp64_and_find_the_truth(scans, candidates):
         for j in (i % N_CAND, (i + 3) % N_CAND):
             want, _ = tf.phase_variance_loss(prep, so.Aberrations(*map(float, c[j])))
             assert abs(losses[j] - want) <= 1e-5 * abs(want) + 1e-6, (spec.scan_shape, j, losses[j], want)
+
+
+def test_persistent_sweep_is_a_few_kernels_per_scan(scans, candidates):
+    """persistent=True: the 256^2 scan's row and column passes in one launch.
+    With C30 candidates there is no quadratic phase table, so the graph holds
+    one kernel per 128^2 scan (the pair kernel, which folds in its last CTA)
+    and four for the 256^2 scan (setup, queue, reduce, final); the losses
+    agree with the launch-sequence sweep to float32 rounding (the C30 path)
+    and still rank the truth first."""
+    seq = MultiScanSweep([be for _, _, be in scans], N_CAND, tune=False)
+    per = MultiScanSweep([be for _, _, be in scans], N_CAND, tune=False, persistent=True)
+    want = seq(candidates)
+    got = per(candidates)
+    assert per.launches_per_replay == 1 + 1 + 4
+    assert seq.launches_per_replay > per.launches_per_replay
+    for i, (w, g) in enumerate(zip(want, got)):
+        np.testing.assert_allclose(g, w, rtol=1e-6, atol=0)
+        assert int(np.argmin(g)) == i % N_CAND
