@@ -1035,6 +1035,7 @@ constexpr size_t kStageBudget = 32u << 20;
 // The persistent one-launch loss (k_loss_queue, QSSB_FLAG_PERSISTENT): 256^2,
 // half set, float32 chi, at most this many candidate groups (27 candidates each).
 constexpr int kQueueN = 256;
+constexpr int kQueueSlots = 3;  // staging slots of the persistent loss
 constexpr int kQueueMaxGroups = 16;
 // Queue words: the ticket, the abort word, then per chunk the completed row
 // and column items.
@@ -1597,7 +1598,7 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool 
                          sizeof(float2) * (size_t)n;
         const int n_groups = (n_cand + tp.group - 1) / tp.group;
         if (queue && !full && n == kQueueN && n_groups <= kQueueMaxGroups) {
-            // two staging slots (rows of chunk k + 1 while columns of chunk k)
+            // kQueueSlots staging slots (rows of later chunks while columns of chunk k)
             pl.queue = true;
             pl.n_groups = n_groups;
             int k = 0;
@@ -1608,8 +1609,8 @@ static LossPlan plan_loss(int n, int n_bf, int n_cand, int chunks_req = 0, bool 
                 k += (n_bf + chunk - 1) / chunk;
             }
             pl.n_phase_chunks = k;
-            pl.stage_bytes = 2 * ((pl.stage_bytes + 255) & ~(size_t)255);
-            pl.delta_bytes = 2 * pl.delta_bytes;
+            pl.stage_bytes = kQueueSlots * ((pl.stage_bytes + 255) & ~(size_t)255);
+            pl.delta_bytes = kQueueSlots * pl.delta_bytes;
             pl.queue_bytes = (sizeof(int) * (size_t)queue_words(k) + 255) & ~(size_t)255;
         }
     } else if (n == 128 && chunks_req <= 0) {
@@ -1673,10 +1674,10 @@ static size_t loss_workspace(const LossPlan& pl) {
 // batch (all candidate groups, all BF chunks) from a global ticket, in the
 // order
 //   R(0), R(1), C(0), R(2), C(1), ..., R(K-1), C(K-2), C(K-1)
-// (R(k): the row items of chunk k, C(k): its column items), with two staging
-// slots. An item waits (thread 0, bounded) only for items with smaller
-// tickets: C(k) for R(k) and, within a candidate group, for C(k - 1) (the
-// partial planes' read-modify-write order); R(k) for C(k - 2) (its slot).
+// (R(k): the row items of chunk k, C(k): its column items), with three
+// staging slots. An item waits (thread 0, bounded) only for items with
+// smaller tickets: C(k) for R(k) and, within a candidate group, for C(k - 1)
+// (the partial planes' read-modify-write order); R(k) for C(k - 3) (its slot).
 // A waiting CTA holds a ticket taken after the ones it waits on, and every
 // ticket taken is held by a running CTA, so the batch drains whatever the
 // number of resident CTAs. Producers write through L2 and fence before their
@@ -1685,9 +1686,10 @@ static size_t loss_workspace(const LossPlan& pl) {
 // quadratic path (the general-chi arithmetic, inlined into another kernel,
 // may contract differently: float32 rounding). A wait that runs out, or a set
 // cancel flag, sets the abort word: later items only count themselves and
-// k_loss_final writes NaN losses. CTAs that wait hold their slots, so this is
-// slower than the launch sequence (the default), which it replaces where
-// one launch per batch matters more than time.
+// k_loss_final writes NaN losses. CTAs that wait hold their slots; with two
+// staging slots that cost 16% against the launch sequence, with three (96 MB
+// of L2-resident staging at 27 candidates per group) it is 3% faster with C30
+// and 2.5% slower with quadratic chi.
 struct QueuePlan {
     int K;       // BF chunks over all candidate groups
     int SR, SC;  // items of one row phase, of one column phase
@@ -1785,14 +1787,15 @@ __global__ void __launch_bounds__(32 * TwoPass<N, false>::rwarps, 3) k_loss_queu
         const int ch = qp.chunk[gi];
         const int b0 = kg * ch;
         const int nb = n_bf - b0 < ch ? n_bf - b0 : ch;
-        float2* st = stage + (size_t)(k & 1) * qp.stage_slot;
-        float2* dl = delta + (size_t)(k & 1) * qp.delta_slot;
+        float2* st = stage + (size_t)(k % kQueueSlots) * qp.stage_slot;
+        float2* dl = delta + (size_t)(k % kQueueSlots) * qp.delta_slot;
         if (threadIdx.x == 0) {
             if (cancel && *reinterpret_cast<const volatile int*>(cancel) != 0)
                 atomicCAS(abort_word, 0, 1);
             int skip = 0;
             if (row) {
-                if (k >= 2) skip = queue_wait(done_c + k - 2, qp.SC, abort_word, cancel);
+                if (k >= kQueueSlots)
+                    skip = queue_wait(done_c + k - kQueueSlots, qp.SC, abort_word, cancel);
             } else {
                 skip = queue_wait(done_r + k, qp.SR, abort_word, cancel);
                 if (!skip && kg >= 1) skip = queue_wait(done_c + k - 1, qp.SC, abort_word, cancel);
@@ -1921,8 +1924,8 @@ static int launch_two_pass(const float* g_half, const float* geom, const float* 
             }
             qp.kstart[pl.n_groups] = k;
             qp.K = k;
-            qp.stage_slot = pl.stage_bytes / 2 / sizeof(float2);
-            qp.delta_slot = pl.delta_bytes / 2 / sizeof(float2);
+            qp.stage_slot = pl.stage_bytes / kQueueSlots / sizeof(float2);
+            qp.delta_slot = pl.delta_bytes / kQueueSlots / sizeof(float2);
             if (k != pl.n_phase_chunks || (long long)k * (qp.SR + qp.SC) > INT_MAX)
                 return set_error(QSSB_ERR_UNSUPPORTED, "qssb_loss_batch: queue plan mismatch");
             const size_t smem = QueueSmem<N>::bytes;

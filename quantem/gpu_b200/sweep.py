@@ -6,15 +6,17 @@ prepared scans (each a resident ``B200SSBBackend``, uneven sizes padded by the
 reference's rule to 128^2 or 256^2) get fixed device buffers for their
 candidates, losses and workspaces; every scan's loss launches (at 128^2 the
 chi-phase table and the pair kernel, which folds in its last CTA; at 256^2 the
-table, a row and a column pass per L2-sized BF chunk, and the fold) are
+set-up, one persistent kernel for the row and column passes over every
+L2-sized BF chunk, and the fold) are
 captured once into one CUDA graph, and a sweep step is: copy the candidates
 in, replay the graph, read the losses out. ``launches_per_replay`` is the
 library's own count of the kernels captured (``qssb_kernel_launches``).
 The work partition of each scan's loss kernel is chosen by the autotuner
-(``autotune.tune_loss``) before capture. ``persistent=True`` runs each 256^2
-scan's row and column passes as one persistent launch
-(``QSSB_FLAG_PERSISTENT``: a handful of kernels per scan instead of two per
-BF chunk, the same losses on the quadratic path, but slower).
+(``autotune.tune_loss``) before capture. By default (``persistent=True``)
+each 256^2 scan's row and column passes run as one persistent launch
+(``QSSB_FLAG_PERSISTENT``): four kernels for that scan instead of two per BF
+chunk, the same losses to float32 rounding, and faster with C30 candidates;
+``persistent=False`` keeps the launch sequence.
 """
 from __future__ import annotations
 
@@ -30,7 +32,7 @@ class MultiScanSweep:
     in one graph replay."""
 
     def __init__(self, backends, n_cand: int | list[int], *, quadratic: bool = False,
-                 tune: bool = True, persistent: bool = False):
+                 tune: bool = True, persistent: bool = True):
         if not backends:
             raise ValueError("at least one prepared scan is needed")
         self.backends = list(backends)

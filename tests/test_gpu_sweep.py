@@ -93,14 +93,14 @@ def test_sweep_losses_match_fp64_and_find_the_truth(scans, candidates):
 
 
 def test_persistent_sweep_is_a_few_kernels_per_scan(scans, candidates):
-    """persistent=True: the 256^2 scan's row and column passes in one launch.
+    """By default the 256^2 scan's row and column passes run in one launch.
     With C30 candidates there is no quadratic phase table, so the graph holds
     one kernel per 128^2 scan (the pair kernel, which folds in its last CTA)
     and four for the 256^2 scan (setup, queue, reduce, final); the losses
     agree with the launch-sequence sweep to float32 rounding (the C30 path)
     and still rank the truth first."""
-    seq = MultiScanSweep([be for _, _, be in scans], N_CAND, tune=False)
-    per = MultiScanSweep([be for _, _, be in scans], N_CAND, tune=False, persistent=True)
+    seq = MultiScanSweep([be for _, _, be in scans], N_CAND, tune=False, persistent=False)
+    per = MultiScanSweep([be for _, _, be in scans], N_CAND, tune=False)
     want = seq(candidates)
     got = per(candidates)
     assert per.launches_per_replay == 1 + 1 + 4
