@@ -41,7 +41,8 @@ extern "C" {
                                      launch runs every row and column item of the batch
                                      instead of a row and a column launch per BF chunk
                                      (the same plan; the same bits with
-                                     QSSB_FLAG_QUADRATIC, float32 rounding without); slower */
+                                     QSSB_FLAG_QUADRATIC, float32 rounding without;
+                                     within 3% of the sequence's time) */
 /* Tile-shape variant (another tuning knob): bits 8..11 of flags. qssb_object
  * on the quadratic-chi path: 1 = 2 adjacent frequencies per thread, 2 or 0
  * (the default) = 4, 3 = 8. Results agree to float32 rounding across
