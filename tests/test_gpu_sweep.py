@@ -108,3 +108,22 @@ def test_persistent_sweep_is_a_few_kernels_per_scan(scans, candidates):
     for i, (w, g) in enumerate(zip(want, got)):
         np.testing.assert_allclose(g, w, rtol=1e-6, atol=0)
         assert int(np.argmin(g)) == i % N_CAND
+
+
+def test_cancel_flag_registered_before_capture_stops_a_replay(scans, candidates):
+    """The graph captures the registered flag's address: set, a replay ends
+    with NaN losses for every scan (the 128^2 pair kernels and the 256^2
+    persistent kernel both poll it) and no hang; cleared, the losses return."""
+    flag = torch.zeros(1, dtype=torch.int32, device=DEV)
+    try:
+        ops.set_cancel_flag(flag)
+        sw = MultiScanSweep([be for _, _, be in scans], N_CAND, tune=False)
+        want = sw(candidates)
+        flag.fill_(1)
+        got = sw(candidates)
+        assert all(np.all(np.isnan(g)) for g in got)
+        flag.fill_(0)
+        for w, g in zip(want, sw(candidates)):
+            np.testing.assert_array_equal(g, w)
+    finally:
+        ops.set_cancel_flag(None)
