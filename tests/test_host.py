@@ -250,3 +250,30 @@ def test_synthetic_generator_dose_and_bf_radius():
     assert abs(sel.radius - 12.0) < 1.0
     again = generate(spec, device="cpu").counts.numpy()
     np.testing.assert_array_equal(counts, again)
+
+
+def test_persistent_loss_plan_without_gpu():
+    """The workspace query is host arithmetic: at 256^2 (float32 chi)
+    QSSB_FLAG_PERSISTENT adds two more staging slots (three in all) and the
+    queue words (ticket, abort word, two counts per BF chunk); elsewhere the
+    flag changes nothing. The sizes follow the plan: 27-candidate groups
+    (444 column CTA slots / 16 strips), 4 BF pixels per chunk in the 32 MB
+    staging budget, 10 for the last group of 10 candidates."""
+    cal = _lib.Calibration(n_bf=1783, scan_rows=256, scan_cols=256, reserved=0,
+                           wavelength_A=0.0197, semiangle_rad=0.02, det_sampling_row_rad=1e-3,
+                           det_sampling_col_rad=1e-3, scan_sampling_row_A=0.5,
+                           scan_sampling_col_A=0.5, dc_re=1.0, dc_im=0.0)
+    q, per, f64 = _lib.QSSB_FLAG_QUADRATIC, _lib.QSSB_FLAG_PERSISTENT, _lib.QSSB_FLAG_CHI_FP64
+    from quantem.gpu_b200 import ops
+    seq = ops.loss_workspace_bytes(cal, 64, q)
+    pst = ops.loss_workspace_bytes(cal, 64, q | per)
+    slot = 8 * 129 * 256 * 4 * 27          # staged half rows of a chunk
+    dslot = 8 * 128 * 4 * 27               # its Nyquist-column deviations
+    chunks = 2 * -(-1783 // 4) + -(-1783 // 10)
+    words = (4 * (2 + 2 * chunks) + 255) // 256 * 256
+    assert chunks == 1071
+    assert pst - seq == 2 * slot + 2 * dslot + words
+    assert ops.loss_workspace_bytes(cal, 64, q | per | f64) == ops.loss_workspace_bytes(cal, 64, q | f64)
+    for n in (128, 512):
+        cal.scan_rows = cal.scan_cols = n
+        assert ops.loss_workspace_bytes(cal, 64, q | per) == ops.loss_workspace_bytes(cal, 64, q)
